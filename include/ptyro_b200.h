@@ -1,0 +1,108 @@
+/*
+ * ptyro_b200 — C-ABI of the B200 multislice 4D-STEM engine.
+ *
+ * Plain pointers and sizes only. Every array argument is a DEVICE pointer unless
+ * its comment says HOST; every call only enqueues work on `stream` (a
+ * cudaStream_t passed as void*), never synchronises and never allocates: scratch
+ * comes from the caller's `workspace`, sized by ptyro_ms_workspace_bytes().
+ * Complex arrays are interleaved complex64 (re, im float pairs).
+ *
+ * Each entry point replaces one step of the reference's JAX path
+ * (ptyrodactyl 2026.5.31, paths relative to its project root); the citation
+ * names the function whose arithmetic and argument meaning it keeps.
+ *
+ * Return value: PTYRO_OK or an error code; ptyro_last_error() gives the message
+ * of the last failure on the calling host thread.
+ */
+#ifndef PTYRO_B200_H
+#define PTYRO_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PTYRO_OK 0
+#define PTYRO_ERR_INVALID 1     /* bad shape, size or scalar (reference: ValueError) */
+#define PTYRO_ERR_WORKSPACE 2   /* workspace too small or misaligned */
+#define PTYRO_ERR_CUDA 3        /* a launch failed */
+#define PTYRO_ERR_UNSUPPORTED 4 /* grid size outside the compiled set */
+
+/* Geometry and physics scalars of one multislice job.
+ * The potential is V[y][x][s] with element strides pot_stride_{y,x,s} (the
+ * reference stores slices last, PotentialSlices.slices (H, W, S)); the beam is
+ * modes[y][x][m] with complex-element strides mode_stride_{y,x,m}
+ * (ProbeModes.modes (H, W, M)). */
+typedef struct ptyro_ms_params {
+  int32_t n;                   /* grid edge H == W; power of two in [16, 1024] */
+  int32_t num_slices;          /* S >= 1 */
+  int32_t num_modes;           /* M >= 1 */
+  int32_t num_probes;          /* P >= 0 scan positions */
+  int32_t batch;               /* probes in flight per batch; 0 = automatic */
+  int32_t reserved;
+  double voltage_kv;           /* MicroscopeConfig.voltage_kv */
+  double slice_thickness_ang;  /* PotentialSlices.slice_thickness */
+  double calib_ang;            /* min(PotentialSlices.calib, ProbeModes.calib): propagator grid */
+  double shift_calib_ang;      /* DetectorConfig.real_space_calib_ang: shift-ramp grid */
+  int64_t pot_stride_y, pot_stride_x, pot_stride_s;
+  int64_t mode_stride_y, mode_stride_x, mode_stride_m;
+} ptyro_ms_params;
+
+/* Library version, major*10000 + minor*100 + patch. */
+int ptyro_version(void);
+
+/* Message of the last failed call on this host thread ("" if none). */
+const char* ptyro_last_error(void);
+
+/* Workspace bytes ptyro_ms_forward / ptyro_ms_forward_plain need for `p`. */
+size_t ptyro_ms_workspace_bytes(const ptyro_ms_params* p);
+
+/* Batched fused 4D-STEM forward model.
+ * Replaces stem_4d (src/ptyrodactyl/multislice/simulations.py:1330-1443) with its
+ * shift_beam_fourier (:1236-1327), the slice loop of
+ * _cbed_amplitude_from_slice_provider (:501-603) and the incoherent mode sum of
+ * apply_distribution (src/ptyrodactyl/multislice/reduce.py:29-89).
+ *   potential  float32 V[y][x][s] (strided, see ptyro_ms_params), volt-Angstrom
+ *   modes      complex64 beam modes[y][x][m] (strided)
+ *   weights    float32 (M) normalised mode weights
+ *   positions  float64 (P, 2) (y, x) shifts; the reference passes
+ *              DetectorConfig.scan_positions_px here and its q grid makes them
+ *              act as Angstrom
+ *   patterns   float32 (P, N, N) out: fftshifted sum_m w_m |A_m|^2 per position */
+int ptyro_ms_forward(const ptyro_ms_params* p, const float* potential, const float* modes,
+                     const float* weights, const double* positions, float* patterns,
+                     void* workspace, size_t workspace_bytes, void* stream);
+
+/* The same model run the plain way: one scan position at a time, one kernel per
+ * stage (shift, and per slice transmission multiply, FFT2, propagator multiply,
+ * IFFT2, then FFT2 and |.|^2), the way the reference's vmap body reads
+ * (simulations.py:1396-1427 around :501-603). Kept as the comparison baseline. */
+int ptyro_ms_forward_plain(const ptyro_ms_params* p, const float* potential, const float* modes,
+                           const float* weights, const double* positions, float* patterns,
+                           void* workspace, size_t workspace_bytes, void* stream);
+
+/* Probe formation. Replaces make_probe (src/ptyrodactyl/multislice/simulations.py:334-431)
+ * with aberration (:434-498): aperture |q| <= alpha/lambda times exp(-i chi),
+ * ifftshift(ifft2(.)). Writes a complex64 (n, n) probe to `probe`.
+ * Workspace: ptyro_fft_workspace_bytes(n). */
+int ptyro_make_probe(int32_t n, double voltage_kv, double aperture_mrad, double probe_calibration_pm,
+                     double defocus_ang, double c3_ang, double c5_ang, float* probe,
+                     void* workspace, size_t workspace_bytes, void* stream);
+
+/* Workspace bytes for ptyro_fft2 / ptyro_make_probe at edge n. */
+size_t ptyro_fft_workspace_bytes(int32_t n);
+
+/* In-place batched 2-D FFT of `count` contiguous complex64 (n, n) planes, with
+ * numpy/JAX conventions: inverse != 0 gives ifft2 (1/n^2 scaling), else fft2.
+ * Stands in for the jnp.fft.fft2/ifft2 calls of the path (simulations.py:429,
+ * :585-589, :601, :1287, :1319). */
+int ptyro_fft2(int32_t n, int32_t count, int32_t inverse, float* data, void* workspace,
+               size_t workspace_bytes, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PTYRO_B200_H */

@@ -1,0 +1,259 @@
+"""Oracle (test infrastructure only): NumPy restatement of ptyrodactyl's multislice path.
+
+This module is the CPU checker for the CUDA kernels in ``ptyrodactyl_b200``. It
+is never called by the product path: only ``tests/``, ``__graft_entry__.smoke``
+and the CPU-baseline leg of ``bench.py`` import it.
+
+Every function follows the reference's arithmetic in operation order. Paths
+are relative to the reference project root. ``dtype`` selects the wave
+precision: ``np.complex128`` restates the reference as shipped (the package
+forces x64, ``src/ptyrodactyl/__init__.py:96``); ``np.complex64`` restates its
+float32 path (wave, propagator and transmission held in complex64; physics
+scalars evaluated in float64 and rounded where they enter an array).
+
+Pinned against the reference's golden file
+``tests/test_data/plan01_ug_reference.npz`` (see ``tests/golden/make_golden.py``
+and ``tests/test_oracle_golden.py``).
+"""
+
+from __future__ import annotations
+
+import numpy as np
+
+# CODATA 2018 exact/recommended values, types/constants.py:60-96
+H_PLANCK = 6.62607015e-34
+M_E = 9.1093837015e-31
+E_CHARGE = 1.602176634e-19
+C_LIGHT = 2.99792458e8
+
+
+def relativistic_wavelength_ang(voltage_kv: float) -> float:
+    """lambda = h c / sqrt(eV (2 m c^2 + eV)) in Angstrom (types/constants.py:291-340)."""
+    ev = float(voltage_kv) * 1000.0 * E_CHARGE
+    numerator = (H_PLANCK * H_PLANCK) * (C_LIGHT * C_LIGHT)
+    denominator = ev * (2.0 * M_E * (C_LIGHT * C_LIGHT) + ev)
+    return 1e10 * np.sqrt(numerator / denominator)
+
+
+def interaction_sigma(voltage_kv: float) -> float:
+    """sigma = 2 pi / (lambda V) (m c^2 + eV) / (2 m c^2 + eV) (multislice/simulations.py:150-157)."""
+    voltage = float(voltage_kv) * 1000.0
+    ev = E_CHARGE * voltage
+    lam = relativistic_wavelength_ang(voltage_kv)
+    einstein = M_E * (C_LIGHT * C_LIGHT)
+    return ((2 * np.pi / (lam * voltage)) * (einstein + ev)) / ((2 * einstein) + ev)
+
+
+def transmission_func(pot_slice: np.ndarray, voltage_kv: float, dtype=np.complex128) -> np.ndarray:
+    """T = exp(i sigma V) (multislice/simulations.py:105-159)."""
+    sigma = interaction_sigma(voltage_kv)
+    return np.exp(1j * sigma * np.asarray(pot_slice, dtype=np.float64)).astype(dtype)
+
+
+def propagation_func(h: int, w: int, thickness_ang: float, voltage_kv: float, calib_ang: float,
+                     dtype=np.complex128) -> np.ndarray:
+    """P(q) = exp(-i pi lambda dz |q|^2), q = fftfreq(n, d=calib) (multislice/simulations.py:162-225)."""
+    qy = np.fft.fftfreq(int(h), d=float(calib_ang))
+    qx = np.fft.fftfreq(int(w), d=float(calib_ang))
+    lya, lxa = np.meshgrid(qy, qx, indexing="ij")
+    l_sq = np.square(lxa) + np.square(lya)
+    lam = relativistic_wavelength_ang(voltage_kv)
+    prop = np.exp((-1j) * np.pi * lam * float(thickness_ang) * l_sq)
+    return prop.astype(dtype)
+
+
+def aberration(fourier_coord: np.ndarray, lambda_angstrom: float, defocus: float = 0.0,
+               c3: float = 0.0, c5: float = 0.0) -> np.ndarray:
+    """chi = 2 pi / lambda (C1 p^2/2 + 1e7 C3 p^4/4 + 1e7 C5 p^6/6), p = lambda q
+    (multislice/simulations.py:434-498). The 1e7 factor makes the C3/C5 fields act as mm."""
+    p = lambda_angstrom * fourier_coord
+    chi = ((defocus * np.power(p, 2)) / 2) + ((c3 * 1e7 * np.power(p, 4)) / 4) + \
+        ((c5 * 1e7 * np.power(p, 6)) / 6)
+    return (2 * np.pi * chi) / lambda_angstrom
+
+
+def probe_fourier_radius(probe_shape, probe_calibration_pm: float) -> np.ndarray:
+    """|q| on the unshifted grid that make_probe builds (multislice/simulations.py:400-416)."""
+    image_y, image_x = int(probe_shape[0]), int(probe_shape[1])
+    x_fov = image_x * 0.01 * float(probe_calibration_pm)
+    y_fov = image_y * 0.01 * float(probe_calibration_pm)
+    qx = np.arange(-image_x / 2, image_x / 2, 1) / x_fov
+    qy = np.arange(-image_y / 2, image_y / 2, 1) / y_fov
+    lx = np.roll(qx, image_x // 2)
+    ly = np.roll(qy, image_y // 2)
+    lya, lxa = np.meshgrid(lx, ly)  # 'xy' indexing, as the reference
+    l2 = np.multiply(lxa, lxa) + np.multiply(lya, lya)
+    return l2 ** 0.5
+
+
+def make_probe(voltage_kv: float, aperture_mrad: float, probe_shape, probe_calibration_pm: float,
+               defocus_ang: float = 0.0, c3_ang: float = 0.0, c5_ang: float = 0.0,
+               dtype=np.complex128) -> np.ndarray:
+    """Aperture mask |q| <= alpha/lambda times exp(-i chi), then ifftshift(ifft2(.))
+    (multislice/simulations.py:334-431). The result is unnormalised:
+    sum |psi|^2 = n_aperture / (H W)."""
+    aperture = aperture_mrad / 1000.0
+    wavelength = relativistic_wavelength_ang(voltage_kv)
+    l_max = aperture / wavelength
+    q = probe_fourier_radius(probe_shape, probe_calibration_pm)
+    a_dist = np.asarray(q <= l_max, dtype=np.complex128)
+    chi = aberration(q, wavelength, defocus_ang, c3_ang, c5_ang)
+    a_dist = a_dist * np.exp(-1j * chi)
+    return np.fft.ifftshift(np.fft.ifft2(a_dist)).astype(dtype)
+
+
+def shift_beam_fourier(beam: np.ndarray, pos: np.ndarray, calib_ang: float,
+                       dtype=np.complex128) -> np.ndarray:
+    """psi_p = ifft2(fft2(psi) exp(-2 pi i (qy y_p + qx x_p))), q in 1/Angstrom, pos in
+    Angstrom (multislice/simulations.py:1236-1327). (H,W,M) + (P,2) -> (P,H,W,M)."""
+    our_beam = np.asarray(beam).astype(dtype)
+    if our_beam.ndim == 2:
+        our_beam = our_beam[..., None]
+    hh, ww = our_beam.shape[0], our_beam.shape[1]
+    pos = np.atleast_2d(np.asarray(pos, dtype=np.float64))
+    qy = np.fft.fftfreq(hh, d=float(calib_ang))
+    qx = np.fft.fftfreq(ww, d=float(calib_ang))
+    qya, qxa = np.meshgrid(qy, qx, indexing="ij")
+    beam_k = np.fft.fft2(our_beam, axes=(0, 1))
+    out = np.empty((pos.shape[0], hh, ww, our_beam.shape[2]), dtype=dtype)
+    for i in range(pos.shape[0]):
+        phase = -2.0 * np.pi * ((qya * pos[i, 0]) + (qxa * pos[i, 1]))
+        ramp = np.exp(1j * phase).astype(dtype)
+        out[i] = np.fft.ifft2(beam_k * ramp[..., None], axes=(0, 1))
+    return out
+
+
+def cbed_amplitude(slices: np.ndarray, slice_thickness: float, voltage_kv: float,
+                   calib_ang: float, beam_modes: np.ndarray, dtype=np.complex128) -> np.ndarray:
+    """The slice loop (multislice/simulations.py:501-603): per slice wave *= T_s, then,
+    unless it is the last slice, wave = ifft2(fft2(wave) * P); finally
+    fftshift(fft2(wave)). slices (H,W,S), beam_modes (H,W,M) -> (H,W,M)."""
+    slices = np.atleast_3d(np.asarray(slices, dtype=np.float64))
+    wave = np.atleast_3d(np.asarray(beam_modes)).astype(dtype)
+    h, w, num_slices = slices.shape
+    prop = propagation_func(wave.shape[0], wave.shape[1], slice_thickness, voltage_kv,
+                            calib_ang, dtype)
+    for s in range(num_slices):
+        trans = transmission_func(slices[:, :, s], voltage_kv, dtype)
+        wave = wave * trans[..., None]
+        if s != num_slices - 1:
+            w_k = np.fft.fft2(wave, axes=(0, 1)) * prop[..., None]
+            wave = np.fft.ifft2(w_k, axes=(0, 1)).astype(dtype)
+    return np.fft.fftshift(np.fft.fft2(wave, axes=(0, 1)), axes=(0, 1))
+
+
+def incoherent_intensity(amplitudes: np.ndarray, weights: np.ndarray) -> np.ndarray:
+    """I = sum_m w_m |A_m|^2 (multislice/reduce.py:81-86); amplitudes (H,W,M)."""
+    return np.einsum("n,hwn->hw", np.asarray(weights, np.float64), np.abs(amplitudes) ** 2)
+
+
+def normalized_weights(weights) -> np.ndarray:
+    """Weights divided by their sum (types/electron_types.py:1318-1324)."""
+    w = np.asarray(weights, dtype=np.float64)
+    return w / np.sum(w)
+
+
+def cbed_image(slices, slice_thickness, pot_calib, beam_modes, weights, beam_calib,
+               voltage_kv, dtype=np.complex128) -> np.ndarray:
+    """Plain (no-ensemble) branch of cbed_image (multislice/simulations.py:1195-1233)."""
+    calib = min(float(pot_calib), float(beam_calib))
+    amps = cbed_amplitude(slices, slice_thickness, voltage_kv, calib, beam_modes, dtype)
+    return incoherent_intensity(amps, weights)
+
+
+def stem_4d(slices, slice_thickness, pot_calib, beam_modes, weights, beam_calib, voltage_kv,
+            scan_positions_px, real_space_calib_ang, dtype=np.complex128) -> dict:
+    """stem_4d (multislice/simulations.py:1330-1443).
+
+    ``scan_positions_px`` is passed unchanged to ``shift_beam_fourier`` whose q is in
+    1/Angstrom, so each position acts as Angstrom relative to the probe's own place
+    (periodic); the output ``scan_positions`` claims ``pos * calib`` Angstrom.
+    Returns a dict with the STEM4D fields; ``data`` is (P,H,W) float64.
+    """
+    positions = np.atleast_2d(np.asarray(scan_positions_px, dtype=np.float64))
+    shifted = shift_beam_fourier(beam_modes, positions, real_space_calib_ang, dtype)
+    calib = min(float(pot_calib), float(beam_calib))
+    data = np.empty((positions.shape[0], shifted.shape[1], shifted.shape[2]), np.float64)
+    for i in range(positions.shape[0]):
+        amps = cbed_amplitude(slices, slice_thickness, voltage_kv, calib, shifted[i], dtype)
+        data[i] = incoherent_intensity(amps, weights)
+    return {
+        "data": data,
+        "real_space_calib": float(real_space_calib_ang),
+        "fourier_space_calib": 1.0 / (shifted.shape[1] * calib),
+        "scan_positions": positions * float(real_space_calib_ang),
+        "voltage_kv": float(voltage_kv),
+    }
+
+
+# ---------------------------------------------------------------------------
+# Adjoint (hand-derived), the checker for the gradient kernels.
+#
+# Forward per probe p and mode m:  phi_s = psi_s * T_s,  psi_{s+1} = U phi_s
+# (U = ifft2 diag(P) fft2, unitary), A = fftshift(fft2(phi_{S-1})), I = sum_m w_m |A_m|^2.
+# With g = dL/dI (real) and lam = dL/dconj(.) :
+#   lam_A   = w_m g A
+#   lam_phi = N^2 ifft2(ifftshift(lam_A))          (adjoint of fftshift o fft2)
+#   dL/dV_s = 2 sigma Im(conj(phi_s) lam_phi_s)     (T = exp(i sigma V))
+#   lam_psi = conj(T_s) lam_phi ;  lam_phi_{s-1} = U^H lam_psi = ifft2(conj(P) fft2(lam_psi))
+#   lam_beam = sum_p N^2 ifft2? -> via shift adjoint below.
+# JAX's gradient of a real loss w.r.t. a complex input z is 2 dL/dz = conj(2 lam_z).
+# ---------------------------------------------------------------------------
+
+
+def stem_4d_vjp(slices, slice_thickness, pot_calib, beam_modes, weights, beam_calib, voltage_kv,
+                scan_positions_px, real_space_calib_ang, g, dtype=np.complex128):
+    """Gradient of L with dL/d data = g (P,H,W) through stem_4d.
+
+    Returns (dV (H,W,S) float64, dbeam (H,W,M) complex in JAX's convention
+    conj(2 dL/dconj(beam))). Weights are treated as constants.
+    """
+    slices = np.atleast_3d(np.asarray(slices, dtype=np.float64))
+    h, w, num_slices = slices.shape
+    positions = np.atleast_2d(np.asarray(scan_positions_px, dtype=np.float64))
+    beam = np.atleast_3d(np.asarray(beam_modes)).astype(dtype)
+    n_modes = beam.shape[2]
+    weights = np.asarray(weights, np.float64)
+    calib = min(float(pot_calib), float(beam_calib))
+    sigma = interaction_sigma(voltage_kv)
+    prop = propagation_func(h, w, slice_thickness, voltage_kv, calib, dtype)
+    trans = [transmission_func(slices[:, :, s], voltage_kv, dtype) for s in range(num_slices)]
+    shifted = shift_beam_fourier(beam, positions, real_space_calib_ang, dtype)
+    dv = np.zeros((h, w, num_slices), np.float64)
+    # adjoint of the shift: psi_p = ifft2(fft2(beam) ramp_p)
+    qy = np.fft.fftfreq(h, d=float(real_space_calib_ang))
+    qx = np.fft.fftfreq(w, d=float(real_space_calib_ang))
+    qya, qxa = np.meshgrid(qy, qx, indexing="ij")
+    lam_beam_k = np.zeros((h, w, n_modes), np.complex128)
+    for i in range(positions.shape[0]):
+        phis = []
+        wave = shifted[i].copy()
+        for s in range(num_slices):
+            phi = wave * trans[s][..., None]
+            phis.append(phi)
+            if s != num_slices - 1:
+                wave = np.fft.ifft2(np.fft.fft2(phi, axes=(0, 1)) * prop[..., None],
+                                    axes=(0, 1)).astype(dtype)
+        amp = np.fft.fftshift(np.fft.fft2(phis[-1], axes=(0, 1)), axes=(0, 1))
+        lam_a = weights[None, None, :] * g[i][..., None] * amp
+        lam = (h * w) * np.fft.ifft2(np.fft.ifftshift(lam_a, axes=(0, 1)), axes=(0, 1))
+        for s in range(num_slices - 1, -1, -1):
+            dv[:, :, s] += 2.0 * sigma * np.sum(np.imag(np.conj(phis[s]) * lam), axis=2)
+            lam = np.conj(trans[s])[..., None] * lam
+            if s > 0:
+                lam = np.fft.ifft2(np.conj(prop)[..., None] * np.fft.fft2(lam, axes=(0, 1)),
+                                   axes=(0, 1))
+        # psi = ifft2(B ramp) -> lam_B = conj(ramp) * fft2(lam)/(HW)
+        phase = -2.0 * np.pi * ((qya * positions[i, 0]) + (qxa * positions[i, 1]))
+        ramp = np.exp(1j * phase)
+        lam_beam_k += np.conj(ramp)[..., None] * np.fft.fft2(lam, axes=(0, 1)) / (h * w)
+    # B = fft2(beam) -> lam_beam = (HW) ifft2(lam_B)
+    lam_beam = (h * w) * np.fft.ifft2(lam_beam_k, axes=(0, 1))
+    return dv, np.conj(2.0 * lam_beam)
+
+
+def aperture_count(voltage_kv, aperture_mrad, probe_shape, probe_calibration_pm) -> int:
+    """Number of pixels inside the hard aperture; sum of every stem_4d pattern."""
+    lam = relativistic_wavelength_ang(voltage_kv)
+    q = probe_fourier_radius(probe_shape, probe_calibration_pm)
+    return int(np.count_nonzero(q <= (aperture_mrad / 1000.0) / lam))

@@ -1,0 +1,33 @@
+"""B200-native multislice 4D-STEM forward model and ptychographic gradient.
+
+A drop-in for the hot path of ptyrodactyl (``ptyrodactyl.multislice``):
+``stem_4d``, ``cbed_image`` and ``make_probe`` keep the reference's signatures
+and run hand-written sm_100a CUDA through the C-ABI in ``include/ptyro_b200.h``.
+"""
+
+from .types import (  # noqa: F401
+    STEM4D,
+    CalibratedArray,
+    DetectorConfig,
+    EnsembleAxes,
+    MicroscopeConfig,
+    PotentialSlices,
+    ProbeModes,
+    create_calibrated_array,
+    create_detector_config,
+    create_microscope_config,
+    create_potential_slices,
+    create_probe_modes,
+    create_stem4d,
+)
+from .simulations import (  # noqa: F401
+    cbed_image,
+    fft2,
+    interaction_sigma,
+    make_probe,
+    relativistic_wavelength_ang,
+    run_forward,
+    stem_4d,
+)
+
+__version__ = "0.1.0"

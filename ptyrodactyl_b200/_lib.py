@@ -1,0 +1,114 @@
+"""ctypes binding of ``libptyro_b200.so`` (the C-ABI in ``include/ptyro_b200.h``).
+
+The product path has no CPU fallback: if the library is missing or cannot be
+loaded this module raises, and every public entry point fails loudly.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+import threading
+
+_PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_PKG, "libptyro_b200.so")
+
+PTYRO_OK = 0
+PTYRO_ERR_INVALID = 1
+PTYRO_ERR_WORKSPACE = 2
+PTYRO_ERR_CUDA = 3
+PTYRO_ERR_UNSUPPORTED = 4
+
+# every symbol include/ptyro_b200.h declares
+EXPORTED_SYMBOLS = (
+    "ptyro_version",
+    "ptyro_last_error",
+    "ptyro_ms_workspace_bytes",
+    "ptyro_ms_forward",
+    "ptyro_ms_forward_plain",
+    "ptyro_make_probe",
+    "ptyro_fft_workspace_bytes",
+    "ptyro_fft2",
+)
+
+
+class MsParams(ctypes.Structure):
+    """Mirror of ``ptyro_ms_params``."""
+
+    _fields_ = [
+        ("n", ctypes.c_int32),
+        ("num_slices", ctypes.c_int32),
+        ("num_modes", ctypes.c_int32),
+        ("num_probes", ctypes.c_int32),
+        ("batch", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
+        ("voltage_kv", ctypes.c_double),
+        ("slice_thickness_ang", ctypes.c_double),
+        ("calib_ang", ctypes.c_double),
+        ("shift_calib_ang", ctypes.c_double),
+        ("pot_stride_y", ctypes.c_int64),
+        ("pot_stride_x", ctypes.c_int64),
+        ("pot_stride_s", ctypes.c_int64),
+        ("mode_stride_y", ctypes.c_int64),
+        ("mode_stride_x", ctypes.c_int64),
+        ("mode_stride_m", ctypes.c_int64),
+    ]
+
+
+class PtyroError(RuntimeError):
+    """A C-ABI call returned an error code."""
+
+    def __init__(self, code: int, message: str):
+        super().__init__(f"ptyro_b200 error {code}: {message}")
+        self.code = code
+
+
+_lock = threading.Lock()
+_lib = None
+
+
+def _declare(lib) -> None:
+    vp, sz, i32, dbl = ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int32, ctypes.c_double
+    pp = ctypes.POINTER(MsParams)
+    lib.ptyro_version.restype = ctypes.c_int
+    lib.ptyro_version.argtypes = []
+    lib.ptyro_last_error.restype = ctypes.c_char_p
+    lib.ptyro_last_error.argtypes = []
+    lib.ptyro_ms_workspace_bytes.restype = sz
+    lib.ptyro_ms_workspace_bytes.argtypes = [pp]
+    for name in ("ptyro_ms_forward", "ptyro_ms_forward_plain"):
+        f = getattr(lib, name)
+        f.restype = ctypes.c_int
+        f.argtypes = [pp, vp, vp, vp, vp, vp, vp, sz, vp]
+    lib.ptyro_make_probe.restype = ctypes.c_int
+    lib.ptyro_make_probe.argtypes = [i32, dbl, dbl, dbl, dbl, dbl, dbl, vp, vp, sz, vp]
+    lib.ptyro_fft_workspace_bytes.restype = sz
+    lib.ptyro_fft_workspace_bytes.argtypes = [i32]
+    lib.ptyro_fft2.restype = ctypes.c_int
+    lib.ptyro_fft2.argtypes = [i32, i32, i32, vp, vp, sz, vp]
+
+
+def load(path: str | None = None):
+    """Load (once) and return the engine library; raise if it is unavailable."""
+    global _lib
+    with _lock:
+        if _lib is not None:
+            return _lib
+        p = path or LIB_PATH
+        if not os.path.exists(p):
+            raise RuntimeError(
+                f"{p} is missing: build the sm_100a engine with "
+                "`python -m ptyrodactyl_b200.build` (there is no CPU fallback)")
+        lib = ctypes.CDLL(p)
+        _declare(lib)
+        _lib = lib
+        return lib
+
+
+def check(code: int) -> None:
+    """Raise :class:`PtyroError` for a non-zero return code."""
+    if code != PTYRO_OK:
+        msg = load().ptyro_last_error().decode("utf-8", "replace")
+        if code == PTYRO_ERR_INVALID or code == PTYRO_ERR_UNSUPPORTED:
+            raise ValueError(msg)
+        raise PtyroError(code, msg)

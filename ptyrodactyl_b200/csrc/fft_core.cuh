@@ -1,0 +1,201 @@
+// Register-resident FFT building blocks for the multislice pass kernels (sm_100a).
+//
+// A line of N = N1 * N2 complex points is owned by N1 threads of one warp.
+// "Natural" distribution: thread t holds x[t + N1*j], j in [0, N2).
+// "K-order" distribution: thread t holds X[k2 + N2*k1] for k2 = t + N1*g,
+//   g in [0, N2/N1), k1 in [0, N1), at register index g*N1 + k1.
+// A forward transform maps natural -> k-order with one warp-local exchange
+// through shared memory (four-step factorisation: N2-point DFTs, twiddles
+// W_N^{t k2}, N1-point DFTs). The inverse maps k-order -> natural by running the
+// same steps backwards, so a forward/inverse pair (a Fresnel convolution along
+// one axis) returns every value to the thread that loaded it.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace ptyro {
+
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+  return make_float2(fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x));
+}
+// a * conj(b)
+__device__ __forceinline__ float2 cmulc(float2 a, float2 b) {
+  return make_float2(fmaf(a.x, b.x, a.y * b.y), fmaf(a.y, b.x, -a.x * b.y));
+}
+__device__ __forceinline__ float2 cscale(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
+__device__ __forceinline__ float2 cconj(float2 a) { return make_float2(a.x, -a.y); }
+
+// cos(2 pi i / 64) for i = 0..16, rounded from the decimal expansion.
+__device__ __forceinline__ float cos64_q(int i) {
+  switch (i) {
+    case 0: return 1.0f;
+    case 1: return (float)0.99518472667219688624;
+    case 2: return (float)0.98078528040323044913;
+    case 3: return (float)0.95694033573220886494;
+    case 4: return (float)0.92387953251128675613;
+    case 5: return (float)0.88192126434835502971;
+    case 6: return (float)0.83146961230254523708;
+    case 7: return (float)0.77301045336273696081;
+    case 8: return (float)0.70710678118654752440;
+    case 9: return (float)0.63439328416364549822;
+    case 10: return (float)0.55557023301960222474;
+    case 11: return (float)0.47139673682599764856;
+    case 12: return (float)0.38268343236508977173;
+    case 13: return (float)0.29028467725446236764;
+    case 14: return (float)0.19509032201612826785;
+    case 15: return (float)0.098017140329560601994;
+    default: return 0.0f;
+  }
+}
+
+// exp(DIR * 2 pi i k / 64) for k in [0, 64); DIR = -1 forward, +1 inverse.
+template <int DIR>
+__device__ __forceinline__ float2 w64(int k) {
+  k &= 63;
+  float c, s;  // cos and sin of 2 pi k / 64
+  if (k <= 16) { c = cos64_q(k); s = cos64_q(16 - k); }
+  else if (k <= 32) { c = -cos64_q(32 - k); s = cos64_q(k - 16); }
+  else if (k <= 48) { c = -cos64_q(k - 32); s = -cos64_q(48 - k); }
+  else { c = cos64_q(64 - k); s = -cos64_q(k - 48); }
+  return make_float2(c, DIR < 0 ? -s : s);
+}
+
+// b * W_64^k (W = exp(DIR 2 pi i / 64)) with the exact cases folded at compile time.
+template <int DIR>
+__device__ __forceinline__ float2 twmul64(float2 b, int k) {
+  k &= 63;
+  if (k == 0) return b;
+  if (k == 32) return make_float2(-b.x, -b.y);
+  if (k == 16) return DIR < 0 ? make_float2(b.y, -b.x) : make_float2(-b.y, b.x);
+  if (k == 48) return DIR < 0 ? make_float2(-b.y, b.x) : make_float2(b.y, -b.x);
+  return cmul(b, w64<DIR>(k));
+}
+
+__host__ __device__ constexpr int ilog2(int n) { return n <= 1 ? 0 : 1 + ilog2(n >> 1); }
+__host__ __device__ constexpr int bitrev(int i, int bits) {
+  return bits == 0 ? 0 : (((i & 1) << (bits - 1)) | bitrev(i >> 1, bits - 1));
+}
+
+// One radix-2 stage (butterfly span HALF) of an R-point decimation-in-time DFT.
+template <int R, int DIR, int HALF>
+__device__ __forceinline__ void dit_stage(float2 (&t)[R]) {
+  constexpr int LEN = 2 * HALF;
+  constexpr int TW = 64 / LEN;
+#pragma unroll
+  for (int i = 0; i < R; i += LEN) {
+#pragma unroll
+    for (int j = 0; j < HALF; ++j) {
+      const float2 u = t[i + j];
+      const float2 w = twmul64<DIR>(t[i + j + HALF], j * TW);
+      t[i + j] = cadd(u, w);
+      t[i + j + HALF] = csub(u, w);
+    }
+  }
+  if constexpr (LEN < R) dit_stage<R, DIR, LEN>(t);
+}
+
+template <int R>
+struct BitRev {
+  int v[R];
+  constexpr BitRev() : v() {
+    for (int i = 0; i < R; ++i) v[i] = bitrev(i, ilog2(R));
+  }
+};
+
+// In-register DFT of size R (power of two, R <= 64) over a[O + S*i], i in [0,R),
+// natural order in and out, unnormalised. Radix-2 decimation in time with every
+// index and twiddle resolved at compile time.
+template <int R, int DIR, int S, int O, int L>
+__device__ __forceinline__ void dft(float2 (&a)[L]) {
+  static_assert(R >= 1 && R <= 64 && (R & (R - 1)) == 0, "radix must be a power of two <= 64");
+  static_assert(O + S * (R - 1) < L, "dft range exceeds register array");
+  if constexpr (R == 1) {
+    return;
+  } else {
+    constexpr BitRev<R> br;
+    float2 t[R];
+#pragma unroll
+    for (int i = 0; i < R; ++i) t[i] = a[O + S * br.v[i]];
+    dit_stage<R, DIR, 1>(t);
+#pragma unroll
+    for (int i = 0; i < R; ++i) a[O + S * i] = t[i];
+  }
+}
+
+// The N1-point DFTs over each contiguous group g*N1 .. g*N1+N1-1.
+template <int N1, int N2, int DIR, int G = 0>
+__device__ __forceinline__ void dft_groups(float2 (&v)[N2]) {
+  if constexpr (G < N2 / N1) {
+    dft<N1, DIR, 1, G * N1, N2>(v);
+    dft_groups<N1, N2, DIR, G + 1>(v);
+  }
+}
+
+// Shared-memory exchange buffer of one line: entry (k2, n1) sits at
+// k2 * (N1 + 1) + n1 so the strided k-order reads fall in distinct banks; the
+// per-line footprint is padded so neighbouring lines start 8 float2 apart mod 16.
+template <int N1, int N2>
+struct LineBuf {
+  static constexpr int kRow = N1 + 1;
+  static constexpr int kRaw = N2 * kRow;
+  static constexpr int kSize = ((kRaw + 15) / 16) * 16 + 8;
+  __device__ static __forceinline__ int at(int k2, int n1) { return k2 * kRow + n1; }
+};
+
+// natural -> k-order transform of one line, unnormalised. DIR = -1 forward.
+// tw[j] = exp(-2 pi i j / N) for j in [0, N) (shared memory).
+template <int N1, int N2, int DIR>
+__device__ __forceinline__ void line_nat_to_k(float2 (&v)[N2], int t, float2* buf, const float2* tw) {
+  using LB = LineBuf<N1, N2>;
+  dft<N2, DIR, 1, 0, N2>(v);
+  if (t != 0) {
+#pragma unroll
+    for (int k2 = 1; k2 < N2; ++k2) {
+      const float2 w = tw[t * k2];
+      v[k2] = DIR < 0 ? cmul(v[k2], w) : cmulc(v[k2], w);
+    }
+  }
+  __syncwarp();
+#pragma unroll
+  for (int k2 = 0; k2 < N2; ++k2) buf[LB::at(k2, t)] = v[k2];
+  __syncwarp();
+#pragma unroll
+  for (int g = 0; g < N2 / N1; ++g)
+#pragma unroll
+    for (int n1 = 0; n1 < N1; ++n1) v[g * N1 + n1] = buf[LB::at(t + N1 * g, n1)];
+  dft_groups<N1, N2, DIR>(v);
+}
+
+// k-order -> natural transform of one line, unnormalised. DIR = +1 inverse.
+template <int N1, int N2, int DIR>
+__device__ __forceinline__ void line_k_to_nat(float2 (&v)[N2], int t, float2* buf, const float2* tw) {
+  using LB = LineBuf<N1, N2>;
+  dft_groups<N1, N2, DIR>(v);
+  __syncwarp();
+#pragma unroll
+  for (int g = 0; g < N2 / N1; ++g)
+#pragma unroll
+    for (int n1 = 0; n1 < N1; ++n1) buf[LB::at(t + N1 * g, n1)] = v[g * N1 + n1];
+  __syncwarp();
+#pragma unroll
+  for (int k2 = 0; k2 < N2; ++k2) v[k2] = buf[LB::at(k2, t)];
+  if (t != 0) {
+#pragma unroll
+    for (int k2 = 1; k2 < N2; ++k2) {
+      const float2 w = tw[t * k2];
+      v[k2] = DIR < 0 ? cmul(v[k2], w) : cmulc(v[k2], w);
+    }
+  }
+  dft<N2, DIR, 1, 0, N2>(v);
+}
+
+// k-order register index r -> frequency index along the line.
+template <int N1, int N2>
+__device__ __forceinline__ int korder_index(int t, int r) {
+  const int g = r / N1, k1 = r % N1;
+  return (t + N1 * g) + N2 * k1;
+}
+
+}  // namespace ptyro

@@ -1,0 +1,217 @@
+"""Public multislice API, call-compatible with ``ptyrodactyl.multislice``.
+
+Each function keeps the signature and argument meaning of the reference
+function it is named after (``src/ptyrodactyl/multislice/simulations.py``) and
+runs on the GPU through the C-ABI of ``libptyro_b200.so``. There is no CPU
+fallback: without CUDA or without the library every entry point raises.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import math
+from typing import Optional
+
+import torch
+
+from . import _lib
+from .types import (
+    CalibratedArray,
+    DetectorConfig,
+    MicroscopeConfig,
+    PotentialSlices,
+    ProbeModes,
+    STEM4D,
+    as_tensor,
+    create_calibrated_array,
+    create_stem4d,
+)
+
+# CODATA 2018 (types/constants.py:60-96)
+H_PLANCK = 6.62607015e-34
+M_E = 9.1093837015e-31
+E_CHARGE = 1.602176634e-19
+C_LIGHT = 2.99792458e8
+
+SUPPORTED_EDGES = (16, 32, 64, 128, 256, 512, 1024)
+
+
+def relativistic_wavelength_ang(voltage_kv: float) -> float:
+    """Electron wavelength in Angstrom (types/constants.py:291-340)."""
+    ev = float(voltage_kv) * 1000.0 * E_CHARGE
+    return 1e10 * math.sqrt((H_PLANCK * H_PLANCK) * (C_LIGHT * C_LIGHT) /
+                            (ev * (2.0 * M_E * (C_LIGHT * C_LIGHT) + ev)))
+
+
+def interaction_sigma(voltage_kv: float) -> float:
+    """sigma of transmission_func (simulations.py:150-157), rad / (V Angstrom)."""
+    volt = float(voltage_kv) * 1000.0
+    ev = E_CHARGE * volt
+    einstein = M_E * (C_LIGHT * C_LIGHT)
+    lam = relativistic_wavelength_ang(voltage_kv)
+    return ((2 * math.pi / (lam * volt)) * (einstein + ev)) / ((2 * einstein) + ev)
+
+
+def _device(device=None) -> torch.device:
+    if not torch.cuda.is_available():
+        raise RuntimeError("ptyrodactyl_b200 needs a CUDA device (there is no CPU fallback)")
+    if device is None:
+        return torch.device("cuda", torch.cuda.current_device())
+    d = torch.device(device)
+    if d.type != "cuda":
+        raise RuntimeError("ptyrodactyl_b200 runs on CUDA devices only")
+    return d
+
+
+def _stream_ptr(device: torch.device) -> int:
+    return torch.cuda.current_stream(device).cuda_stream
+
+
+def _ptr(t: Optional[torch.Tensor]) -> Optional[int]:
+    return None if t is None else t.data_ptr()
+
+
+def _check_edge(h: int, w: int) -> int:
+    if h != w:
+        raise ValueError(f"grid must be square, got ({h}, {w})")
+    if h not in SUPPORTED_EDGES:
+        raise ValueError(f"grid edge must be one of {SUPPORTED_EDGES}, got {h}")
+    return h
+
+
+def _workspace(nbytes: int, device: torch.device) -> torch.Tensor:
+    # torch's caching allocator hands out 512-byte aligned blocks
+    return torch.empty(max(int(nbytes), 256), dtype=torch.uint8, device=device)
+
+
+def ms_params(n: int, num_slices: int, num_modes: int, num_probes: int, voltage_kv: float,
+              slice_thickness: float, calib_ang: float, shift_calib_ang: float,
+              pot_strides=(0, 0, 0), mode_strides=(0, 0, 0), batch: int = 0) -> _lib.MsParams:
+    p = _lib.MsParams()
+    p.n, p.num_slices, p.num_modes, p.num_probes, p.batch = n, num_slices, num_modes, num_probes, batch
+    p.voltage_kv = float(voltage_kv)
+    p.slice_thickness_ang = float(slice_thickness)
+    p.calib_ang = float(calib_ang)
+    p.shift_calib_ang = float(shift_calib_ang)
+    p.pot_stride_y, p.pot_stride_x, p.pot_stride_s = (int(s) for s in pot_strides)
+    p.mode_stride_y, p.mode_stride_x, p.mode_stride_m = (int(s) for s in mode_strides)
+    return p
+
+
+def run_forward(slices: torch.Tensor, slice_thickness: float, modes: torch.Tensor, weights: torch.Tensor,
+                positions: torch.Tensor, voltage_kv: float, calib_ang: float, shift_calib_ang: float,
+                out: Optional[torch.Tensor] = None, batch: int = 0, plain: bool = False) -> torch.Tensor:
+    """Device-level forward: all tensors already on one CUDA device.
+
+    slices (H, W, S) float32 (any strides), modes (H, W, M) complex64 (any strides),
+    weights (M,) float32, positions (P, 2) float64 contiguous. Returns patterns
+    (P, H, W) float32.
+    """
+    lib = _lib.load()
+    dev = slices.device
+    n = _check_edge(slices.shape[0], slices.shape[1])
+    if tuple(modes.shape[:2]) != (n, n):
+        raise ValueError("beam modes and potential slices must share the grid shape")
+    num_probes = positions.shape[0]
+    prm = ms_params(n, slices.shape[2], modes.shape[2], num_probes, voltage_kv, slice_thickness,
+                    calib_ang, shift_calib_ang, slices.stride(), modes.stride(), batch)
+    if out is None:
+        out = torch.empty((num_probes, n, n), dtype=torch.float32, device=dev)
+    if num_probes == 0:
+        return out
+    ws_bytes = lib.ptyro_ms_workspace_bytes(ctypes.byref(prm))
+    if ws_bytes == 0:
+        _lib.check(_lib.PTYRO_ERR_INVALID)
+    ws = _workspace(ws_bytes, dev)
+    fn = lib.ptyro_ms_forward_plain if plain else lib.ptyro_ms_forward
+    rc = fn(ctypes.byref(prm), slices.data_ptr(), modes.data_ptr(), weights.data_ptr(),
+            positions.data_ptr(), out.data_ptr(), ws.data_ptr(), ws_bytes, _stream_ptr(dev))
+    _lib.check(rc)
+    return out
+
+
+def _beam_on(beam: ProbeModes, dev) -> tuple:
+    modes = beam.modes if beam.modes.ndim == 3 else beam.modes[..., None]
+    modes = as_tensor(modes, torch.complex64, dev)
+    weights = as_tensor(beam.weights, torch.float32, dev).contiguous()
+    return modes, weights
+
+
+def stem_4d(pot_slice: PotentialSlices, beam: ProbeModes, microscope: MicroscopeConfig,
+            detector: DetectorConfig) -> STEM4D:
+    """4D-STEM patterns at every scan position (simulations.py:1330-1443).
+
+    ``detector.scan_positions_px`` is used exactly as the reference uses it: passed
+    unchanged as the shift of ``shift_beam_fourier``, whose frequency grid is in
+    1/Angstrom, so each value acts as Angstrom; the returned ``scan_positions``
+    field is ``positions * real_space_calib_ang`` as in the reference. ``data`` is a
+    float32 CUDA tensor (P, H, W).
+    """
+    if detector.scan_positions_px is None:
+        raise ValueError("detector.scan_positions_px is required")
+    if not microscope.ensemble.is_empty():
+        raise NotImplementedError("ensemble axes are not supported by the B200 engine")
+    dev = _device(pot_slice.slices.device if pot_slice.slices.is_cuda else None)
+    slices = as_tensor(pot_slice.slices, torch.float32, dev)
+    if slices.ndim == 2:
+        slices = slices[..., None]
+    modes, weights = _beam_on(beam, dev)
+    positions = as_tensor(detector.scan_positions_px, torch.float64, dev).reshape(-1, 2).contiguous()
+    calib = min(float(pot_slice.calib), float(beam.calib))
+    data = run_forward(slices, pot_slice.slice_thickness, modes, weights, positions,
+                       microscope.voltage_kv, calib, detector.real_space_calib_ang)
+    fourier_calib = 1.0 / (modes.shape[0] * calib)
+    scan_positions = detector.scan_positions_px.to(torch.float64) * detector.real_space_calib_ang
+    return create_stem4d(data, detector.real_space_calib_ang, fourier_calib, scan_positions,
+                         microscope.voltage_kv)
+
+
+def cbed_image(pot_slices: PotentialSlices, beam: ProbeModes, microscope: MicroscopeConfig) -> CalibratedArray:
+    """Single-position CBED intensity (plain branch, simulations.py:1130-1233): the
+    unshifted beam through the slices, sum_m w_m |fftshift(fft2(exit wave))|^2."""
+    if not microscope.ensemble.is_empty():
+        raise NotImplementedError("ensemble axes are not supported by the B200 engine")
+    dev = _device(pot_slices.slices.device if pot_slices.slices.is_cuda else None)
+    slices = as_tensor(pot_slices.slices, torch.float32, dev)
+    if slices.ndim == 2:
+        slices = slices[..., None]
+    modes, weights = _beam_on(beam, dev)
+    calib = min(float(pot_slices.calib), float(beam.calib))
+    zero = torch.zeros((1, 2), dtype=torch.float64, device=dev)
+    data = run_forward(slices, pot_slices.slice_thickness, modes, weights, zero,
+                       microscope.voltage_kv, calib, calib)[0]
+    inv = 1.0 / (modes.shape[0] * calib)
+    return create_calibrated_array(data, inv, inv, False)
+
+
+def make_probe(microscope: MicroscopeConfig, detector: DetectorConfig) -> torch.Tensor:
+    """Real-space probe from aperture and aberrations (simulations.py:334-431):
+    complex64 (H, W) CUDA tensor, centred at (H/2, W/2), unnormalised."""
+    if microscope.probe_shape is None:
+        raise ValueError("microscope.probe_shape is required")
+    h, w = microscope.probe_shape
+    n = _check_edge(h, w)
+    lib = _lib.load()
+    dev = _device()
+    probe = torch.empty((n, n), dtype=torch.complex64, device=dev)
+    ws_bytes = lib.ptyro_fft_workspace_bytes(n)
+    ws = _workspace(ws_bytes, dev)
+    rc = lib.ptyro_make_probe(n, microscope.voltage_kv, microscope.aperture_mrad,
+                              detector.probe_calibration_pm, microscope.defocus_ang, microscope.c3_ang,
+                              microscope.c5_ang, probe.data_ptr(), ws.data_ptr(), ws_bytes, _stream_ptr(dev))
+    _lib.check(rc)
+    return probe
+
+
+def fft2(x: torch.Tensor, inverse: bool = False) -> torch.Tensor:
+    """numpy-convention fft2/ifft2 over the last two axes of a complex64 CUDA tensor."""
+    lib = _lib.load()
+    dev = _device(x.device if x.is_cuda else None)
+    y = as_tensor(x, torch.complex64, dev).contiguous().clone()
+    n = _check_edge(y.shape[-2], y.shape[-1])
+    count = y.numel() // (n * n)
+    ws_bytes = lib.ptyro_fft_workspace_bytes(n)
+    ws = _workspace(ws_bytes, dev)
+    _lib.check(lib.ptyro_fft2(n, count, 1 if inverse else 0, y.data_ptr(), ws.data_ptr(), ws_bytes,
+                              _stream_ptr(dev)))
+    return y

@@ -1,0 +1,267 @@
+"""Carriers and factories of the multislice path, mirroring ptyrodactyl's.
+
+Field names, factory signatures and error messages follow
+``src/ptyrodactyl/types/electron_types.py`` (carriers :103-375, factories
+:529-1527). Differences, all deliberate:
+
+* arrays are ``torch.Tensor`` (CPU or CUDA) instead of JAX arrays, and keep
+  float32/complex64 (the reference's factories force float64/complex128,
+  ``electron_types.py:1275, :1364, :1443``; this engine computes in float32);
+* traced-value checks (``eqx.error_if``) become eager ``ValueError``s with the
+  reference's messages;
+* scalar fields are Python floats.
+"""
+
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+from typing import Optional, Tuple
+
+import numpy as np
+import torch
+
+Array = torch.Tensor
+
+
+def as_tensor(x, dtype: torch.dtype, device=None) -> torch.Tensor:
+    """numpy / torch / sequence -> tensor of ``dtype`` (device kept unless given)."""
+    if isinstance(x, torch.Tensor):
+        t = x
+    else:
+        arr = np.asarray(x)
+        if arr.dtype == np.complex128 and dtype == torch.complex64:
+            arr = arr.astype(np.complex64)
+        elif arr.dtype == np.float64 and dtype == torch.float32:
+            arr = arr.astype(np.float32)
+        t = torch.from_numpy(np.ascontiguousarray(arr))
+    if t.dtype != dtype:
+        if dtype.is_complex and not t.dtype.is_complex:
+            t = t.to(torch.float32 if dtype == torch.complex64 else torch.float64)
+        t = t.to(dtype)
+    if device is not None:
+        t = t.to(device)
+    return t
+
+
+def _scalar(value, name: str) -> float:
+    if isinstance(value, torch.Tensor):
+        if value.numel() != 1:
+            raise ValueError(f"{name} must be a scalar")
+        return float(value.detach().cpu().reshape(()).item())
+    arr = np.asarray(value)
+    if arr.shape != ():
+        raise ValueError(f"{name} must be a scalar")
+    return float(arr)
+
+
+def _positive(value: float, name: str) -> float:
+    if not math.isfinite(value):
+        raise ValueError(f"{name} must be finite")
+    if value <= 0:
+        raise ValueError(f"{name} must be positive")
+    return value
+
+
+def _finite(value: float, name: str) -> float:
+    if not math.isfinite(value):
+        raise ValueError(f"{name} must be finite")
+    return value
+
+
+def _shape_tuple(shape, name: str) -> Optional[Tuple[int, int]]:
+    if shape is None:
+        return None
+    vals = np.asarray(shape.detach().cpu() if isinstance(shape, torch.Tensor) else shape).reshape(-1)
+    if vals.shape != (2,):
+        raise ValueError(f"{name} must have two entries")
+    return (int(vals[0]), int(vals[1]))
+
+
+@dataclass(frozen=True)
+class EnsembleAxes:
+    """Optional ensemble distributions (electron_types.py:74-100). Only the empty
+    carrier is supported by this engine."""
+
+    probe_modes: object = None
+    position_jitter: object = None
+    coherence: object = None
+
+    def is_empty(self) -> bool:
+        return self.probe_modes is None and self.position_jitter is None and self.coherence is None
+
+
+@dataclass(frozen=True)
+class MicroscopeConfig:
+    """Microscope voltage and probe aberrations (electron_types.py:103-144)."""
+
+    voltage_kv: float
+    aperture_mrad: float
+    defocus_ang: float
+    c3_ang: float
+    c5_ang: float
+    ensemble: EnsembleAxes = field(default_factory=EnsembleAxes)
+    probe_shape: Optional[Tuple[int, int]] = None
+
+
+@dataclass(frozen=True)
+class DetectorConfig:
+    """Detector, scan and calibration (electron_types.py:147-189)."""
+
+    real_space_calib_ang: float
+    probe_calibration_pm: float
+    collection_inner_mrad: float
+    collection_outer_mrad: float
+    scan_positions_px: Optional[Array] = None
+    scan_positions_ang: Optional[Array] = None
+    scan_shape: Optional[Tuple[int, int]] = None
+
+
+@dataclass(frozen=True)
+class CalibratedArray:
+    """2-D array with calibrations (electron_types.py:264-292)."""
+
+    data_array: Array
+    calib_y: float
+    calib_x: float
+    real_space: bool
+
+
+@dataclass(frozen=True)
+class ProbeModes:
+    """Probe modes (H, W, M) and normalised weights (electron_types.py:295-317)."""
+
+    modes: Array
+    weights: Array
+    calib: float
+
+
+@dataclass(frozen=True)
+class PotentialSlices:
+    """Potential slices (H, W, S) in volt-Angstrom (electron_types.py:320-342)."""
+
+    slices: Array
+    slice_thickness: float
+    calib: float
+
+
+@dataclass(frozen=True)
+class STEM4D:
+    """4D-STEM dataset, data (P, H, W) (electron_types.py:345-373)."""
+
+    data: Array
+    real_space_calib: float
+    fourier_space_calib: float
+    scan_positions: Array
+    voltage_kv: float
+
+
+def create_microscope_config(voltage_kv, aperture_mrad, defocus_ang=0.0, c3_ang=0.0, c5_ang=0.0,
+                             ensemble: Optional[EnsembleAxes] = None,
+                             probe_shape=None) -> MicroscopeConfig:
+    """electron_types.py:529-612."""
+    voltage = _positive(_scalar(voltage_kv, "voltage_kv"), "voltage_kv")
+    aperture = _positive(_scalar(aperture_mrad, "aperture_mrad"), "aperture_mrad")
+    defocus = _finite(_scalar(defocus_ang, "defocus_ang"), "defocus_ang")
+    c3 = _finite(_scalar(c3_ang, "c3_ang"), "c3_ang")
+    c5 = _finite(_scalar(c5_ang, "c5_ang"), "c5_ang")
+    return MicroscopeConfig(voltage, aperture, defocus, c3, c5,
+                            EnsembleAxes() if ensemble is None else ensemble,
+                            _shape_tuple(probe_shape, "probe_shape"))
+
+
+def _positions(value, name: str) -> Optional[Array]:
+    if value is None:
+        return None
+    t = as_tensor(value, torch.float64)
+    if t.ndim == 1 and t.shape[0] == 2:
+        t = t.reshape(1, 2)
+    if t.ndim != 2 or t.shape[1] != 2:
+        raise ValueError(f"{name} must have shape (P, 2)")
+    if not bool(torch.isfinite(t).all()):
+        raise ValueError(f"{name} contain non-finite values")
+    return t
+
+
+def create_detector_config(real_space_calib_ang, probe_calibration_pm=None, collection_inner_mrad=0.0,
+                           collection_outer_mrad=0.0, scan_positions_px=None, scan_positions_ang=None,
+                           scan_shape=None) -> DetectorConfig:
+    """electron_types.py:616-731."""
+    real = _positive(_scalar(real_space_calib_ang, "real_space_calib_ang"), "real_space_calib_ang")
+    probe_pm = real * 100.0 if probe_calibration_pm is None else _scalar(probe_calibration_pm,
+                                                                          "probe_calibration_pm")
+    _positive(probe_pm, "probe_calibration_pm")
+    inner = _scalar(collection_inner_mrad, "collection_inner_mrad")
+    outer = _scalar(collection_outer_mrad, "collection_outer_mrad")
+    if not (math.isfinite(inner) and inner >= 0):
+        raise ValueError("collection_inner_mrad must be non-negative")
+    if not (math.isfinite(outer) and outer >= 0):
+        raise ValueError("collection_outer_mrad must be non-negative")
+    if outer < inner:
+        raise ValueError("collection_outer_mrad must be >= collection_inner_mrad")
+    return DetectorConfig(real, probe_pm, inner, outer,
+                          _positions(scan_positions_px, "scan_positions_px"),
+                          _positions(scan_positions_ang, "scan_positions_ang"),
+                          _shape_tuple(scan_shape, "scan_shape"))
+
+
+def create_probe_modes(modes, weights, calib) -> ProbeModes:
+    """electron_types.py:1238-1324: modes (H, W, M), weights (M,) normalised to sum 1."""
+    m = as_tensor(modes, torch.complex64)
+    w = as_tensor(weights, torch.float64)
+    c = _scalar(calib, "calib")
+    if m.ndim != 3:
+        raise ValueError("modes must be 3D")
+    if w.ndim != 1:
+        raise ValueError("weights must be 1D")
+    if tuple(w.shape) != (m.shape[2],):
+        raise ValueError("weights must have shape (M,)")
+    if not bool(torch.isfinite(torch.view_as_real(m)).all()):
+        raise ValueError("modes contain non-finite values")
+    if not bool(torch.isfinite(w).all()):
+        raise ValueError("weights contain non-finite values")
+    if bool((w < 0).any()):
+        raise ValueError("weights must be non-negative")
+    total = float(w.sum())
+    if total <= np.finfo(np.float64).eps:
+        raise ValueError("weights must sum to a positive value")
+    _positive(c, "calib")
+    return ProbeModes(m, (w / total).to(torch.float32), c)
+
+
+def create_potential_slices(slices, slice_thickness, calib) -> PotentialSlices:
+    """electron_types.py:1328-1397: slices (H, W, S) volt-Angstrom."""
+    s = as_tensor(slices, torch.float32)
+    if s.ndim != 3:
+        raise ValueError("slices must be 3D")
+    th = _scalar(slice_thickness, "slice_thickness")
+    c = _scalar(calib, "calib")
+    if not bool(torch.isfinite(s).all()):
+        raise ValueError("slices contain non-finite values")
+    _positive(th, "slice_thickness")
+    _positive(c, "calib")
+    return PotentialSlices(s, th, c)
+
+
+def create_calibrated_array(data_array, calib_y, calib_x, real_space) -> CalibratedArray:
+    """electron_types.py:853-930."""
+    d = data_array if isinstance(data_array, torch.Tensor) else torch.as_tensor(np.asarray(data_array))
+    if d.ndim != 2:
+        raise ValueError("data_array must be 2D")
+    cy = _positive(_scalar(calib_y, "calib_y"), "calib_y")
+    cx = _positive(_scalar(calib_x, "calib_x"), "calib_x")
+    return CalibratedArray(d, cy, cx, bool(real_space))
+
+
+def create_stem4d(data, real_space_calib, fourier_space_calib, scan_positions, voltage_kv) -> STEM4D:
+    """electron_types.py:1401-1527: data (P, H, W), scan_positions (P, 2)."""
+    d = data if isinstance(data, torch.Tensor) else as_tensor(data, torch.float32)
+    pos = as_tensor(scan_positions, torch.float64)
+    if d.ndim != 3:
+        raise ValueError("data must be 3D")
+    if pos.ndim != 2 or pos.shape[1] != 2 or pos.shape[0] != d.shape[0]:
+        raise ValueError("scan_positions must have shape (P, 2)")
+    rc = _positive(_scalar(real_space_calib, "real_space_calib"), "real_space_calib")
+    fc = _positive(_scalar(fourier_space_calib, "fourier_space_calib"), "fourier_space_calib")
+    v = _positive(_scalar(voltage_kv, "voltage_kv"), "voltage_kv")
+    return STEM4D(d, rc, fc, pos, v)

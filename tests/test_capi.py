@@ -1,0 +1,97 @@
+"""C-ABI library: loads, exports every declared symbol, validates before touching a GPU."""
+
+import ctypes
+import os
+import re
+
+import pytest
+
+from ptyrodactyl_b200 import _lib
+from ptyrodactyl_b200.build import build
+from ptyrodactyl_b200.simulations import ms_params
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+@pytest.fixture(scope="module")
+def lib():
+    build()
+    return _lib.load()
+
+
+def _declared_functions():
+    names = []
+    for fname in os.listdir(os.path.join(ROOT, "include")):
+        if not fname.endswith(".h"):
+            continue
+        text = open(os.path.join(ROOT, "include", fname)).read()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        names += re.findall(r"\b(ptyro_\w+)\s*\(", text)
+    return sorted(set(names))
+
+
+def test_exports_every_declared_symbol(lib):
+    declared = _declared_functions()
+    assert declared, "no declarations found"
+    for name in declared:
+        assert hasattr(lib, name), f"{name} declared in include/ but not exported"
+    assert set(declared) <= set(_lib.EXPORTED_SYMBOLS) | set(declared)
+    for name in _lib.EXPORTED_SYMBOLS:
+        assert name in declared, f"{name} bound in _lib but not declared in include/"
+
+
+def test_version(lib):
+    assert lib.ptyro_version() >= 100
+
+
+def _p(**kw):
+    base = dict(n=128, num_slices=20, num_modes=1, num_probes=256, voltage_kv=300.0, slice_thickness=1.95,
+                calib_ang=0.244, shift_calib_ang=0.244)
+    base.update(kw)
+    return ms_params(**base)
+
+
+def test_workspace_bytes_scale(lib):
+    small = lib.ptyro_ms_workspace_bytes(ctypes.byref(_p(batch=1)))
+    big = lib.ptyro_ms_workspace_bytes(ctypes.byref(_p(batch=16)))
+    assert small > 0 and big > small
+    assert (big - small) >= 15 * 128 * 128 * 8
+    assert lib.ptyro_ms_workspace_bytes(ctypes.byref(_p(n=100))) == 0
+
+
+@pytest.mark.parametrize("kw,msg", [
+    (dict(n=100), "power of two"),
+    (dict(n=2048), "power of two"),
+    (dict(num_slices=0), "num_slices"),
+    (dict(num_modes=0), "num_modes"),
+    (dict(voltage_kv=-1.0), "voltage_kv"),
+    (dict(slice_thickness=0.0), "slice_thickness"),
+    (dict(calib_ang=float("nan")), "calib"),
+])
+def test_invalid_params_rejected_before_launch(lib, kw, msg):
+    p = _p(**kw)
+    rc = lib.ptyro_ms_forward(ctypes.byref(p), None, None, None, None, None, None, 0, None)
+    assert rc in (_lib.PTYRO_ERR_INVALID, _lib.PTYRO_ERR_UNSUPPORTED)
+    assert msg in lib.ptyro_last_error().decode()
+
+
+def test_workspace_checks(lib):
+    p = _p(batch=1)
+    buf = ctypes.create_string_buffer(64)
+    # null arrays are reported before the workspace
+    rc = lib.ptyro_ms_forward(ctypes.byref(p), None, None, None, None, None, None, 0, None)
+    assert rc == _lib.PTYRO_ERR_INVALID
+    fake = ctypes.addressof(buf)
+    rc = lib.ptyro_ms_forward(ctypes.byref(p), fake, fake, fake, fake, fake, None, 0, None)
+    assert rc == _lib.PTYRO_ERR_WORKSPACE
+    assert "workspace" in lib.ptyro_last_error().decode()
+
+
+def test_zero_probes_is_a_no_op(lib):
+    p = _p(num_probes=0)
+    assert lib.ptyro_ms_forward(ctypes.byref(p), None, None, None, None, None, None, 0, None) == 0
+
+
+def test_fft2_rejects_bad_edge(lib):
+    assert lib.ptyro_fft2(100, 1, 0, None, None, 0, None) == _lib.PTYRO_ERR_UNSUPPORTED
+    assert lib.ptyro_fft2(64, -1, 0, None, None, 0, None) == _lib.PTYRO_ERR_INVALID

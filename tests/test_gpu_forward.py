@@ -1,0 +1,167 @@
+"""GPU parity of the forward model against the oracle and the reference's golden vectors.
+
+Tolerances (relative L2 over all pattern values): <= 1e-5 against the float32
+(complex64) restatement of the reference; <= 1e-4 against the float64 oracle
+and the reference's own float64 golden arrays.
+"""
+
+import ctypes
+
+import numpy as np
+import pytest
+import torch
+
+import ptyrodactyl_b200 as pb
+from oracle import multislice_ref as R
+from ptyrodactyl_b200 import synth
+from tests.conftest import rel_l2
+
+pytestmark = pytest.mark.gpu
+
+TOL_F32 = 1e-5
+TOL_F64 = 1e-4
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _need_cuda():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    pb._lib.load()
+
+
+def _run(pot, dz, probe_modes, weights, pos, kv, calib, shift_calib=None, batch=0, plain=False):
+    dev = torch.device("cuda")
+    slices = torch.as_tensor(np.asarray(pot, np.float32), device=dev)
+    modes = torch.as_tensor(np.asarray(probe_modes, np.complex64), device=dev)
+    w = torch.as_tensor(np.asarray(weights, np.float32), device=dev)
+    p = torch.as_tensor(np.asarray(pos, np.float64), device=dev).reshape(-1, 2).contiguous()
+    out = pb.run_forward(slices, dz, modes, w, p, kv, calib, shift_calib or calib, batch=batch, plain=plain)
+    torch.cuda.synchronize()
+    return out.cpu().numpy()
+
+
+@pytest.mark.parametrize("n", [16, 32, 64, 128, 256, 512, 1024])
+def test_fft2_matches_numpy(n):
+    rng = np.random.default_rng(n)
+    x = (rng.normal(size=(3, n, n)) + 1j * rng.normal(size=(3, n, n))).astype(np.complex64)
+    xf = pb.fft2(torch.as_tensor(x, device="cuda")).cpu().numpy()
+    assert rel_l2(xf, np.fft.fft2(x.astype(np.complex128))) < 2e-6
+    xi = pb.fft2(torch.as_tensor(x, device="cuda"), inverse=True).cpu().numpy()
+    assert rel_l2(xi, np.fft.ifft2(x.astype(np.complex128))) < 2e-6
+
+
+@pytest.mark.parametrize("w", [synth.CONFIG1, synth.CONFIG2])
+def test_make_probe_matches_oracle(w):
+    mic = pb.create_microscope_config(w.voltage_kv, w.aperture_mrad, w.defocus_ang, w.c3_ang,
+                                      probe_shape=(w.n, w.n))
+    det = pb.create_detector_config(w.calib)
+    got = pb.make_probe(mic, det).cpu().numpy()
+    want = R.make_probe(w.voltage_kv, w.aperture_mrad, (w.n, w.n), w.calib * 100.0, w.defocus_ang, w.c3_ang)
+    assert rel_l2(got, want) < 1e-6
+
+
+def test_reference_golden_plan01(golden):
+    g = golden
+    probe = R.make_probe(100.0, 20.0, (32, 32), 20.0)
+    got = _run(g["pot"], 2.0, probe[..., None], [1.0], g["positions_px"], 100.0, 0.2)
+    assert rel_l2(got, g["stem4d"]) < TOL_F64
+    # the public API end to end
+    slices = pb.create_potential_slices(g["pot"], 2.0, 0.2)
+    mic = pb.create_microscope_config(100.0, 20.0, probe_shape=(32, 32))
+    det = pb.create_detector_config(0.2, 20.0, scan_positions_px=g["positions_px"])
+    beam = pb.create_probe_modes(pb.make_probe(mic, det).cpu().numpy()[..., None], [1.0], 0.2)
+    s4 = pb.stem_4d(slices, beam, mic, det)
+    assert rel_l2(s4.data.cpu().numpy(), g["stem4d"]) < TOL_F64
+    assert np.allclose(s4.scan_positions.cpu().numpy(), g["positions_px"] * 0.2)
+    assert abs(s4.fourier_space_calib - 1.0 / (32 * 0.2)) < 1e-12
+    cb = pb.cbed_image(slices, beam, mic)
+    assert rel_l2(cb.data_array.cpu().numpy(), g["cbed"]) < TOL_F64
+
+
+def _workload_case(w, n_probes, num_slices=None, seed=0):
+    pot = synth.potential_slices(w, num_slices=num_slices)
+    probe = R.make_probe(w.voltage_kv, w.aperture_mrad, (w.n, w.n), w.calib * 100.0, w.defocus_ang, w.c3_ang)
+    pos = synth.raster_positions(w)
+    rng = np.random.default_rng(seed)
+    pos = pos[rng.choice(pos.shape[0], n_probes, replace=False)]
+    return pot, probe, pos
+
+
+@pytest.mark.parametrize("w,n_probes,num_slices", [(synth.CONFIG1, 6, None), (synth.CONFIG2, 3, 12),
+                                                   (synth.CONFIG3, 1, 6)])
+def test_forward_matches_oracle(w, n_probes, num_slices):
+    pot, probe, pos = _workload_case(w, n_probes, num_slices)
+    s = pot.shape[2]
+    got = _run(pot, synth.SLICE_DZ, probe[..., None], [1.0], pos, w.voltage_kv, w.calib)
+    args = (pot, synth.SLICE_DZ, w.calib, probe[..., None], [1.0], w.calib, w.voltage_kv, pos, w.calib)
+    want32 = R.stem_4d(*args, dtype=np.complex64)["data"]
+    want64 = R.stem_4d(*args, dtype=np.complex128)["data"]
+    assert rel_l2(got, want32) < TOL_F32, (s, rel_l2(got, want32))
+    assert rel_l2(got, want64) < TOL_F64
+    n_ap = R.aperture_count(w.voltage_kv, w.aperture_mrad, (w.n, w.n), w.calib * 100.0)
+    assert np.allclose(got.sum(axis=(1, 2)), n_ap, rtol=1e-4)
+
+
+def test_modes_weights_and_single_slice():
+    rng = np.random.default_rng(3)
+    n = 64
+    pot = rng.uniform(0, 40, (n, n, 1))
+    p1 = R.make_probe(120.0, 22.0, (n, n), 30.0, defocus_ang=30.0)
+    modes = np.stack([p1, np.roll(p1, 3, axis=0) * (0.6 + 0.2j)], axis=-1)
+    w = np.array([0.7, 0.3])
+    pos = np.array([[0.0, 0.0], [1.3, -2.1], [-4.0, 5.5]])
+    got = _run(pot, 2.0, modes, w, pos, 120.0, 0.3)
+    want = R.stem_4d(pot, 2.0, 0.3, modes, w, 0.3, 120.0, pos, 0.3, dtype=np.complex128)["data"]
+    assert rel_l2(got, want) < TOL_F64
+
+
+def test_batching_is_exact_and_ragged():
+    w = synth.CONFIG1
+    pot, probe, pos = _workload_case(w, 7, 5)
+    a = _run(pot, synth.SLICE_DZ, probe[..., None], [1.0], pos, w.voltage_kv, w.calib, batch=0)
+    b = _run(pot, synth.SLICE_DZ, probe[..., None], [1.0], pos, w.voltage_kv, w.calib, batch=3)
+    c = _run(pot, synth.SLICE_DZ, probe[..., None], [1.0], pos[2:3], w.voltage_kv, w.calib, batch=1)
+    assert np.array_equal(a, b)
+    assert np.array_equal(a[2], c[0])
+
+
+def test_plain_path_matches_fused():
+    w = synth.CONFIG1
+    pot, probe, pos = _workload_case(w, 3, 6)
+    fused = _run(pot, synth.SLICE_DZ, probe[..., None], [1.0], pos, w.voltage_kv, w.calib)
+    plain = _run(pot, synth.SLICE_DZ, probe[..., None], [1.0], pos, w.voltage_kv, w.calib, plain=True)
+    assert rel_l2(plain, fused) < TOL_F32
+
+
+def test_strided_potential_layouts_agree():
+    w = synth.CONFIG1
+    pot, probe, pos = _workload_case(w, 2, 4)
+    dev = torch.device("cuda")
+    a = _run(pot, synth.SLICE_DZ, probe[..., None], [1.0], pos, w.voltage_kv, w.calib)
+    # (S, H, W) storage viewed as (H, W, S)
+    shw = torch.as_tensor(np.ascontiguousarray(np.moveaxis(pot, 2, 0)), device=dev, dtype=torch.float32)
+    view = shw.permute(1, 2, 0)
+    modes = torch.as_tensor(probe[..., None].astype(np.complex64), device=dev)
+    wts = torch.ones(1, device=dev)
+    p = torch.as_tensor(pos, device=dev)
+    b = pb.run_forward(view, synth.SLICE_DZ, modes, wts, p, w.voltage_kv, w.calib, w.calib).cpu().numpy()
+    assert np.array_equal(a, b)
+
+
+def test_zero_positions_returns_empty():
+    w = synth.CONFIG1
+    pot, probe, _ = _workload_case(w, 1, 2)
+    out = _run(pot, synth.SLICE_DZ, probe[..., None], [1.0], np.zeros((0, 2)), w.voltage_kv, w.calib)
+    assert out.shape == (0, w.n, w.n)
+
+
+def test_errors_raise_value_error():
+    slices = pb.create_potential_slices(np.zeros((48, 48, 2)), 1.0, 0.2)
+    mic = pb.create_microscope_config(100.0, 20.0, probe_shape=(48, 48))
+    det = pb.create_detector_config(0.2, scan_positions_px=np.zeros((1, 2)))
+    beam = pb.create_probe_modes(np.ones((48, 48, 1), np.complex64), [1.0], 0.2)
+    with pytest.raises(ValueError):
+        pb.stem_4d(slices, beam, mic, det)
+    det2 = pb.create_detector_config(0.2)
+    with pytest.raises(ValueError, match="scan_positions_px is required"):
+        pb.stem_4d(slices, beam, mic, det2)

@@ -1,0 +1,100 @@
+"""The oracle itself: pinned to the reference's golden vectors and known answers."""
+
+import numpy as np
+import pytest
+
+from oracle import jax_prng
+from oracle import multislice_ref as R
+from tests.conftest import rel_l2
+
+
+def test_threefry_known_answers():
+    # Random123 known-answer vectors for Threefry-2x32-20
+    cases = [((0, 0), (0, 0), (0x6B200159, 0x99BA4EFE)),
+             ((0xFFFFFFFF, 0xFFFFFFFF), (0xFFFFFFFF, 0xFFFFFFFF), (0x1CB996FC, 0xBB002BE7)),
+             ((0x13198A2E, 0x03707344), (0x243F6A88, 0x85A308D3), (0xC4923A9C, 0x483DF7A0))]
+    for key, ctr, want in cases:
+        a, b = jax_prng.threefry2x32(key, np.array([ctr[0]], np.uint32), np.array([ctr[1]], np.uint32))
+        assert (int(a[0]), int(b[0])) == want
+
+
+def test_golden_input_regenerates(golden):
+    pot = jax_prng.uniform_f64(jax_prng.prng_key(42), (32, 32, 2)) * 10.0
+    assert np.array_equal(pot, golden["pot"])
+
+
+def _golden_stem(golden, dtype=np.complex128):
+    g = golden
+    probe = R.make_probe(float(g["voltage_kv"]), float(g["aperture_mrad"]), (32, 32),
+                         float(g["calib_ang"]) * 100.0)
+    return R.stem_4d(g["pot"], float(g["slice_thickness_ang"]), float(g["calib_ang"]), probe[..., None],
+                     [1.0], float(g["calib_ang"]), float(g["voltage_kv"]), g["positions_px"],
+                     float(g["calib_ang"]), dtype=dtype)
+
+
+def test_oracle_matches_reference_golden(golden):
+    """plan01_ug_reference.npz (reference capture, float64)."""
+    g = golden
+    probe = R.make_probe(100.0, 20.0, (32, 32), 20.0)
+    cbed = R.cbed_image(g["pot"], 2.0, 0.2, probe[..., None], [1.0], 0.2, 100.0)
+    assert np.max(np.abs(cbed - g["cbed"])) < 1e-13
+    s4 = _golden_stem(g)
+    assert np.max(np.abs(s4["data"] - g["stem4d"])) < 1e-13
+    assert s4["scan_positions"].shape == (4, 2)
+
+
+def test_oracle_c64_close_to_c128(golden):
+    s64 = _golden_stem(golden, np.complex64)["data"]
+    assert rel_l2(s64, golden["stem4d"]) < 1e-5
+
+
+def test_pattern_sum_is_aperture_count(golden):
+    n_ap = R.aperture_count(100.0, 20.0, (32, 32), 20.0)
+    assert n_ap == 37
+    assert abs(golden["cbed"].sum() - 37.0) < 1e-9
+    assert np.allclose(golden["stem4d"].sum(axis=(1, 2)), 37.0)
+
+
+def test_wavelength_and_sigma_values():
+    # values quoted for the reference's constants (types/constants.py:291-340)
+    for kv, lam in ((60, 0.048661), (100, 0.037014), (200, 0.025079), (300, 0.019687)):
+        assert abs(R.relativistic_wavelength_ang(kv) - lam) < 5e-7
+    for kv, sig in ((100, 9.2440e-4), (200, 7.2884e-4), (300, 6.5262e-4)):
+        assert abs(R.interaction_sigma(kv) - sig) / sig < 1e-4
+
+
+def test_vjp_matches_finite_differences():
+    rng = np.random.default_rng(5)
+    n, s = 16, 3
+    pot = rng.uniform(0, 30, (n, n, s))
+    probe = R.make_probe(200.0, 25.0, (n, n), 40.0, defocus_ang=-20.0)
+    pos = np.array([[0.3, -0.4], [1.2, 0.7]])
+    g = rng.normal(size=(2, n, n))
+
+    def loss(v, beam):
+        d = R.stem_4d(v, 1.5, 0.4, beam[..., None], [1.0], 0.4, 200.0, pos, 0.4)["data"]
+        return float(np.sum(g * d))
+
+    dv, dbeam = R.stem_4d_vjp(pot, 1.5, 0.4, probe[..., None], [1.0], 0.4, 200.0, pos, 0.4, g)
+    for (y, x, k) in [(3, 4, 0), (8, 8, 1), (12, 2, 2)]:
+        e = np.zeros_like(pot)
+        e[y, x, k] = 1e-4
+        fd = (loss(pot + e, probe) - loss(pot - e, probe)) / 2e-4
+        assert abs(fd - dv[y, x, k]) <= 1e-6 * max(1.0, abs(fd))
+    # complex beam gradient, JAX convention grad = dL/dRe - i dL/dIm
+    for (y, x) in [(8, 8), (7, 9)]:
+        e = np.zeros_like(probe)
+        e[y, x] = 1e-5
+        fre = (loss(pot, probe + e) - loss(pot, probe - e)) / 2e-5
+        fim = (loss(pot, probe + 1j * e) - loss(pot, probe - 1j * e)) / 2e-5
+        assert abs(dbeam[y, x, 0] - (fre - 1j * fim)) <= 1e-6 * max(1.0, abs(fre) + abs(fim))
+
+
+def test_golden_gradient_is_null(golden):
+    """grad of sum(cbed) w.r.t. V vanishes (the sum is the aperture count for any V)."""
+    g = golden
+    probe = R.make_probe(100.0, 20.0, (32, 32), 20.0)
+    dv, _ = R.stem_4d_vjp(g["pot"], 2.0, 0.2, probe[..., None], [1.0], 0.2, 100.0, np.zeros((1, 2)), 0.2,
+                          np.ones((1, 32, 32)))
+    assert np.max(np.abs(dv)) < 1e-12
+    assert np.max(np.abs(g["grad_pot"])) < 1e-12
