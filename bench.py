@@ -1,0 +1,443 @@
+#!/usr/bin/env python
+"""Benchmark of the batched fused multislice forward model (probe-slice updates/s).
+
+Workload: the 256x256 perovskite configuration — 16x16 ABO3 supercell, 50 slices of
+1.95 A, 64x64 raster scan (4096 probes), 200 kV, 25 mrad, C1 = -50 A, Cs = 1 um —
+with seeded synthetic inputs (``ptyrodactyl_b200.synth``). One step = one full
+``stem_4d`` forward over the 4096 probes (4096 * 50 probe-slice updates).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+For N > 1 launch under torchrun: every rank runs its own 4096-probe shard of a
+larger scan (weak scaling, no collective on the data path); timings are taken
+on the device with CUDA events and reduced as the max over ranks.
+Rank 0 prints one JSON line.
+"""
+
+from __future__ import annotations
+
+import argparse
+import ctypes
+import datetime
+import json
+import multiprocessing as mp
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+from ptyrodactyl_b200 import synth  # noqa: E402
+
+METRIC = "probe-slice updates/s at 256^2 (batched fused multislice forward, 4096 probes x 50 slices)"
+UNIT = "probe-slice updates/s"
+WORKLOAD = synth.CONFIG2
+L2_FLUSH_BYTES = 256 << 20
+
+
+# ----------------------------------------------------------------------------- CPU leg
+_CPU_STATE = {}
+
+
+def _cpu_worker(task):
+    """Oracle (NumPy complex128 restatement of the reference's x64 path) for some probes."""
+    os.environ.setdefault("OMP_NUM_THREADS", "1")
+    from oracle import multislice_ref as R
+    name, idx = task
+    w = WORKLOAD
+    if "pot" not in _CPU_STATE:
+        _CPU_STATE["pot"] = synth.potential_slices(w).astype(np.float64)
+        _CPU_STATE["probe"] = R.make_probe(w.voltage_kv, w.aperture_mrad, (w.n, w.n), w.calib * 100.0,
+                                           w.defocus_ang, w.c3_ang)
+        _CPU_STATE["pos"] = synth.raster_positions(w)
+    pos = _CPU_STATE["pos"][np.asarray(idx)]
+    t0 = time.perf_counter()
+    R.stem_4d(_CPU_STATE["pot"], synth.SLICE_DZ, w.calib, _CPU_STATE["probe"][..., None], [1.0], w.calib,
+              w.voltage_kv, pos, w.calib, dtype=np.complex128)
+    return time.perf_counter() - t0
+
+
+def _host_cores() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+class CpuOracle:
+    """A spawn pool (safe next to CUDA) running the oracle on bounded probe samples."""
+
+    def __init__(self, procs: int):
+        self.procs = procs
+        self.pool = mp.get_context("spawn").Pool(procs)
+        # warm every worker (imports, potential generation) outside any timing
+        self.pool.map(_cpu_worker, [("warm", [i]) for i in range(procs)])
+        self.next = 0
+
+    def step(self, probes_per_proc: int) -> tuple:
+        """Run procs * probes_per_proc probes; return (updates, wall seconds)."""
+        tasks = []
+        for _ in range(self.procs):
+            idx = [(self.next + k) % WORKLOAD.num_probes for k in range(probes_per_proc)]
+            self.next += probes_per_proc
+            tasks.append(("run", idx))
+        t0 = time.perf_counter()
+        self.pool.map(_cpu_worker, tasks)
+        wall = time.perf_counter() - t0
+        return self.procs * probes_per_proc * WORKLOAD.num_slices, wall
+
+    def close(self):
+        self.pool.close()
+        self.pool.join()
+
+
+# ----------------------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        reasons = set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for r in rows:
+            for name, val in zip(names, r[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(rows)}
+
+
+# ----------------------------------------------------------------------------- GPU leg
+def _events(torch, n):
+    return [torch.cuda.Event(enable_timing=True) for _ in range(n)]
+
+
+def fp32_peak_tflops(torch, lib, dev) -> float:
+    """Measured FP32 FMA ceiling of this device (TFLOP/s), best of 3."""
+    blocks = torch.cuda.get_device_properties(dev).multi_processor_count * 8
+    iters = 4096
+    out = torch.empty(blocks * 256, dtype=torch.float32, device=dev)
+    st = torch.cuda.current_stream(dev).cuda_stream
+    lib.ptyro_fp32_fma_probe(out.data_ptr(), blocks, 64, st)
+    best = 0.0
+    for _ in range(3):
+        s, e = _events(torch, 2)
+        s.record()
+        rc = lib.ptyro_fp32_fma_probe(out.data_ptr(), blocks, iters, st)
+        e.record()
+        torch.cuda.synchronize()
+        assert rc == 0
+        flops = blocks * 256.0 * iters * 128 * 2
+        best = max(best, flops / (s.elapsed_time(e) * 1e-3) / 1e12)
+    return best
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    import torch.distributed as dist
+    import ptyrodactyl_b200 as pb
+    from ptyrodactyl_b200 import _lib
+    from ptyrodactyl_b200.simulations import ms_params
+
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    lib = _lib.load()
+    w = WORKLOAD
+    n, S, P = w.n, w.num_slices, w.num_probes
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = CpuOracle(min(_host_cores(), 64))
+
+    # ---- inputs (this rank's shard: the raster offset by a sub-pixel amount per rank)
+    pot = synth.potential_slices(w)
+    pos = synth.raster_positions(w) + 0.37 * rank
+    mic = pb.create_microscope_config(w.voltage_kv, w.aperture_mrad, w.defocus_ang, w.c3_ang,
+                                      probe_shape=(n, n))
+    det = pb.create_detector_config(w.calib, scan_positions_px=pos)
+    probe = pb.make_probe(mic, det)
+    slices_d = torch.as_tensor(pot, device=dev)
+    modes_d = probe[..., None].contiguous()
+    weights_d = torch.ones(1, dtype=torch.float32, device=dev)
+    pos_d = torch.as_tensor(pos, dtype=torch.float64, device=dev)
+    out_d = torch.empty((P, n, n), dtype=torch.float32, device=dev)
+    prm = ms_params(n, S, 1, P, w.voltage_kv, synth.SLICE_DZ, w.calib, w.calib, slices_d.stride(),
+                    modes_d.stride(), args.batch)
+    ws_bytes = lib.ptyro_ms_workspace_bytes(ctypes.byref(prm))
+    ws = torch.empty(ws_bytes, dtype=torch.uint8, device=dev)
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def step():
+        rc = lib.ptyro_ms_forward(ctypes.byref(prm), slices_d.data_ptr(), modes_d.data_ptr(),
+                                  weights_d.data_ptr(), pos_d.data_ptr(), out_d.data_ptr(), ws.data_ptr(),
+                                  ws_bytes, stream.cuda_stream)
+        _lib.check(rc)
+
+    def barrier():
+        if world > 1:
+            dist.barrier(device_ids=[local_rank])
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+
+    clocks = ClockSampler(_physical_gpu(local_rank))
+    starts, ends = _events(torch, args.steps), _events(torch, args.steps)
+    barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    launches0 = lib.ptyro_launch_count()
+    for k in range(args.steps):
+        flush.zero_()  # evict L2 between steps (256 MB > 126 MB L2)
+        starts[k].record(stream)
+        step()
+        ends[k].record(stream)
+    launches = lib.ptyro_launch_count() - launches0
+    torch.cuda.synchronize()
+    barrier()
+    clk = clocks.stop()
+    step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    total_ms = float(sum(step_ms))
+    if world > 1:
+        t = torch.tensor([total_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    updates = float(P) * S * args.steps * world
+    value = updates / (total_ms * 1e-3)
+
+    # sanity: every pattern sums to the aperture pixel count
+    n_ap = float(((_aperture_mask(w)).sum()))
+    sums = out_d.sum(dim=(1, 2))
+    max_sum_err = float(((sums - n_ap).abs().max() / n_ap).item())
+
+    # ---- dominant kernel alone: the steady-state pass over one batch
+    reps = 20
+    pass_ms = []
+    for axis in (0, 1):
+        s, e = _events(torch, 2)
+        flush.zero_()
+        s.record(stream)
+        _lib.check(lib.ptyro_ms_steady_pass(ctypes.byref(prm), axis, reps, ws.data_ptr(), ws_bytes,
+                                            stream.cuda_stream))
+        e.record(stream)
+        torch.cuda.synchronize()
+        pass_ms.append(s.elapsed_time(e) / reps)
+    batch = _batch_of(lib, prm, n)
+    avg_pass_s = statistics.mean(pass_ms) * 1e-3
+    flops_per_launch = batch * synth.algorithmic_flops_per_update(n)
+    achieved_tflops = flops_per_launch / avg_pass_s / 1e12
+    peak = fp32_peak_tflops(torch, lib, dev)
+    bytes_per_launch = batch * (2.0 * 8 * n * n) + 8.0 * n * n  # wave read+write, T read
+    traffic = _ncu_traffic()
+
+    # ---- end to end through the public API with host buffers
+    e2e = None
+    if not args.no_e2e:
+        pot_h = torch.as_tensor(pot).pin_memory()
+        modes_h = probe.cpu()[..., None].contiguous().pin_memory()
+        pos_h = torch.as_tensor(pos, dtype=torch.float64).pin_memory()
+        out_h = torch.empty((P, n, n), dtype=torch.float32).pin_memory()
+        slices_obj = pb.PotentialSlices(pot_h, synth.SLICE_DZ, w.calib)
+        beam_obj = pb.ProbeModes(modes_h, torch.ones(1, dtype=torch.float32).pin_memory(), w.calib)
+        det_obj = pb.DetectorConfig(w.calib, w.calib * 100, 0.0, 0.0, pos_h, None, None)
+
+        def e2e_step():
+            s4 = pb.stem_4d(slices_obj, beam_obj, mic, det_obj)
+            out_h.copy_(s4.data, non_blocking=True)
+
+        e2e_step()
+        torch.cuda.synchronize()
+        k2 = max(1, min(args.steps, 5))
+        barrier()
+        torch.cuda.synchronize()
+        s, e = _events(torch, 2)
+        s.record(stream)
+        for _ in range(k2):
+            e2e_step()
+        e.record(stream)
+        torch.cuda.synchronize()
+        e2e_ms = s.elapsed_time(e)
+        if world > 1:
+            t = torch.tensor([e2e_ms], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e_ms = float(t.item())
+        h2d = pot_h.numel() * 4 + modes_h.numel() * 8 + pos_h.numel() * 8 + 4
+        e2e = {"value": float(P) * S * k2 * world / (e2e_ms * 1e-3), "unit": UNIT,
+               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(P * n * n * 4), "steps": k2}
+
+    cpu_baseline = None
+    if cpu is not None:
+        upd, wall = 0, 0.0
+        while wall < args.cpu_seconds:
+            u, t = cpu.step(1)
+            upd += u
+            wall += t
+        cpu.close()
+        cpu_baseline = {"value": upd / wall, "unit": UNIT, "cores": cpu.procs, "kind": "port",
+                        "sample": f"{upd // S} probes of this workload (all 50 slices each), NumPy complex128 "
+                                  f"oracle, one process per core"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": w.name, "grid": n, "slices": S, "probes_per_gpu": P, "modes": 1,
+                       "batch": batch, "voltage_kv": w.voltage_kv, "aperture_mrad": w.aperture_mrad,
+                       "defocus_ang": w.defocus_ang, "c3_ang": w.c3_ang,
+                       "l2": "flushed (256 MB write) before every timed step",
+                       "parallelism": f"dp{world} (probe shards, no collective)"},
+            "roofline": {"bound": "fp32", "achieved": achieved_tflops, "peak": peak, "unit": "TFLOP/s",
+                         "frac": achieved_tflops / peak, "traffic": traffic,
+                         "kernel": "ms_pass_kernel<16,16> steady-state pass (conv, x T, conv)",
+                         "flops_per_launch": flops_per_launch, "launch_ms": [round(x, 4) for x in pass_ms],
+                         "peak_source": "measured FP32 FMA stream (ptyro_fp32_fma_probe) in this run",
+                         "hbm_achieved_gbs": bytes_per_launch / avg_pass_s / 1e9,
+                         "hbm_algorithmic_bytes_per_launch": bytes_per_launch},
+            "e2e": e2e,
+            "gpu_launches": int(launches),
+            "clocks": clk,
+            "cpu_baseline": cpu_baseline,
+            "checks": {"pattern_sum_max_rel_err": max_sum_err},
+        }
+        print(json.dumps(line), flush=True)
+
+
+def _physical_gpu(local_rank: int) -> str:
+    """nvidia-smi id of this rank's GPU (CUDA_VISIBLE_DEVICES entry if set)."""
+    vis = [v.strip() for v in os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",") if v.strip()]
+    return vis[local_rank] if local_rank < len(vis) else str(local_rank)
+
+
+def _aperture_mask(w):
+    from ptyrodactyl_b200.simulations import relativistic_wavelength_ang
+    lam = relativistic_wavelength_ang(w.voltage_kv)
+    fov = w.n * 0.01 * (w.calib * 100.0)
+    f = np.fft.fftfreq(w.n) * w.n / fov
+    q = np.sqrt(f[:, None] ** 2 + f[None, :] ** 2)
+    return q <= (w.aperture_mrad / 1000.0) / lam
+
+
+def _batch_of(lib, prm, n) -> int:
+    if prm.batch > 0:
+        return min(prm.batch, prm.num_probes)
+    return max(1, min(prm.num_probes, (64 << 20) // (8 * n * n * prm.num_modes)))
+
+
+def _ncu_traffic():
+    """DRAM bytes per launch of the pass kernel from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", "pass_256_traffic.json")
+    try:
+        with open(path) as f:
+            return json.load(f).get("dram_bytes_per_launch")
+    except (OSError, ValueError):
+        return None
+
+
+# ----------------------------------------------------------------------------- reference arm
+def run_reference(args, rank):
+    if rank != 0:
+        return
+    procs = min(_host_cores(), 64)
+    cpu = CpuOracle(procs)
+    for _ in range(args.warmup):
+        cpu.step(1)
+    upd, wall = 0, 0.0
+    for _ in range(args.steps):
+        u, t = cpu.step(1)
+        upd += u
+        wall += t
+    cpu.close()
+    value = upd / wall
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 0, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": wall / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+        "config": {"workload": WORKLOAD.name, "grid": WORKLOAD.n, "slices": WORKLOAD.num_slices,
+                   "probes": WORKLOAD.num_probes, "sample_probes_per_step": procs},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": procs, "kind": "port",
+                         "sample": f"{procs} probes (all 50 slices) per step, NumPy complex128 restatement of "
+                                   "the reference's x64 stem_4d (JAX is not installed), one process per core"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--batch", type=int, default=0)
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3) if args.impl == "ours" else max(args.warmup, 1)
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local_rank))
+    try:
+        run_ours(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -101,6 +101,23 @@ size_t ptyro_fft_workspace_bytes(int32_t n);
 int ptyro_fft2(int32_t n, int32_t count, int32_t inverse, float* data, void* workspace,
                size_t workspace_bytes, void* stream);
 
+/* Engine kernels enqueued by this process so far (all threads and devices).
+ * Lets a caller count the launches of a timed region. */
+unsigned long long ptyro_launch_count(void);
+
+/* `reps` launches of the steady-state pass (finish slice s-1's convolution along
+ * `axis`, multiply T_1, start slice s's convolution) over the batch of wave slots
+ * held in `workspace` by a preceding ptyro_ms_forward with the same `p`. The
+ * workspace must hold finite values. Used to time the dominant kernel alone; the
+ * reference has no counterpart (its slice step is _scan_fn, simulations.py:544-597). */
+int ptyro_ms_steady_pass(const ptyro_ms_params* p, int32_t axis, int32_t reps, void* workspace,
+                         size_t workspace_bytes, void* stream);
+
+/* Diagnostic: `blocks` x 256 threads each run iters*128 dependent-free FP32 FMAs
+ * and write one float to out[blocks*256]. FLOPs = blocks*256*iters*256. Measures
+ * the FP32 ceiling used as the roofline denominator; no reference counterpart. */
+int ptyro_fp32_fma_probe(float* out, int32_t blocks, int32_t iters, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -29,6 +29,9 @@ EXPORTED_SYMBOLS = (
     "ptyro_make_probe",
     "ptyro_fft_workspace_bytes",
     "ptyro_fft2",
+    "ptyro_launch_count",
+    "ptyro_ms_steady_pass",
+    "ptyro_fp32_fma_probe",
 )
 
 
@@ -86,6 +89,12 @@ def _declare(lib) -> None:
     lib.ptyro_fft_workspace_bytes.argtypes = [i32]
     lib.ptyro_fft2.restype = ctypes.c_int
     lib.ptyro_fft2.argtypes = [i32, i32, i32, vp, vp, sz, vp]
+    lib.ptyro_launch_count.restype = ctypes.c_ulonglong
+    lib.ptyro_launch_count.argtypes = []
+    lib.ptyro_ms_steady_pass.restype = ctypes.c_int
+    lib.ptyro_ms_steady_pass.argtypes = [pp, i32, i32, vp, sz, vp]
+    lib.ptyro_fp32_fma_probe.restype = ctypes.c_int
+    lib.ptyro_fp32_fma_probe.argtypes = [vp, i32, i32, vp]
 
 
 def load(path: str | None = None):

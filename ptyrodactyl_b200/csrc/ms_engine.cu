@@ -5,6 +5,7 @@
 #include <stdint.h>
 #include <stdio.h>
 
+#include <atomic>
 #include <string>
 
 #include "../../include/ptyro_b200.h"
@@ -21,7 +22,11 @@ static int fail(int code, const std::string& msg) {
   return code;
 }
 
-static int check_launch(const char* what) {
+std::atomic<unsigned long long> g_launches{0};
+
+// Every launch site outside the pass launchers reports through here.
+static int check_launch(const char* what, int launches = 1) {
+  g_launches.fetch_add((unsigned long long)launches, std::memory_order_relaxed);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return fail(PTYRO_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
   return PTYRO_OK;
@@ -335,7 +340,7 @@ static int forward_setup(const ptyro_ms_params* p, const Layout& L, char* ws, co
       interaction_sigma(p->voltage_kv), T);
   k_gather_modes<<<blocks_for(nn * p->num_modes, 256), 256, 0, st>>>(
       (const float2*)modes, p->mode_stride_y, p->mode_stride_x, p->mode_stride_m, n, p->num_modes, pk);
-  int rc = check_launch("forward setup");
+  int rc = check_launch("forward setup", 4);
   if (rc) return rc;
   return fft2_planes(n, p->num_modes, false, pk, tw, st);
 }
@@ -430,6 +435,7 @@ int ptyro_ms_forward_plain(const ptyro_ms_params* p, const float* potential, con
   const double lam = wavelength_ang(p->voltage_kv);
   float2* p2 = (float2*)(ws + L.p2);
   k_propagator2d<<<(unsigned)((nn + 255) / 256), 256, 0, st>>>(n, p->calib_ang, lam * p->slice_thickness_ang, p2);
+  if ((rc = check_launch("plain propagator table"))) return rc;
   const float2* tw = (const float2*)(ws + L.tw);
   const float2* T = (const float2*)(ws + L.trans);
   const float2* pk = (const float2*)(ws + L.probe_k);
@@ -440,7 +446,7 @@ int ptyro_ms_forward_plain(const ptyro_ms_params* p, const float* potential, con
   for (int i = 0; i < p->num_probes; ++i) {
     k_ramps<<<(n + 255) / 256, 256, 0, st>>>(positions + 2 * (size_t)i, 1, n, p->shift_calib_ang, ry, rx);
     k_plain_shift<<<eb, 256, 0, st>>>(pk, ry, rx, n, M, w);
-    if ((rc = check_launch("plain shift"))) return rc;
+    if ((rc = check_launch("plain shift", 2))) return rc;
     if ((rc = fft2_planes(n, M, true, w, tw, st))) return rc;
     for (int s = 0; s < S; ++s) {
       k_plain_mul_plane<<<eb, 256, 0, st>>>(w, T + (size_t)s * nn, n, M);
@@ -455,6 +461,35 @@ int ptyro_ms_forward_plain(const ptyro_ms_params* p, const float* potential, con
     k_plain_intensity<<<(unsigned)((nn + 255) / 256), 256, 0, st>>>(w, weights, n, M, patterns + (size_t)i * nn);
     if ((rc = check_launch("plain intensity"))) return rc;
   }
+  return PTYRO_OK;
+}
+
+unsigned long long ptyro_launch_count(void) { return g_launches.load(std::memory_order_relaxed); }
+
+int ptyro_ms_steady_pass(const ptyro_ms_params* p, int32_t axis, int32_t reps, void* workspace,
+                         size_t workspace_bytes, void* stream) {
+  int rc = validate(p);
+  if (rc) return rc;
+  if (axis != 0 && axis != 1) return fail(PTYRO_ERR_INVALID, "axis must be 0 or 1");
+  if (reps < 0) return fail(PTYRO_ERR_INVALID, "reps must be >= 0");
+  if (p->num_slices < 2) return fail(PTYRO_ERR_INVALID, "steady pass needs num_slices >= 2");
+  const Layout L = layout_for(p);
+  if ((rc = check_workspace(L, workspace, workspace_bytes))) return rc;
+  char* ws = (char*)workspace;
+  PassArgs a = {};
+  a.wave = (float2*)(ws + L.waves);
+  a.trans = (const float2*)(ws + L.trans);
+  a.pf = (const float2*)(ws + L.pf);
+  a.tw = (const float2*)(ws + L.tw);
+  a.n_modes = p->num_modes;
+  a.scale = 1.0f / (float)p->n;
+  a.src = SRC_WAVE;
+  a.op1 = OP_CONV;
+  a.t_slice = 1;
+  a.op2 = OP_CONV;
+  a.dst = DST_WAVE;
+  for (int r = 0; r < reps; ++r)
+    if ((rc = launch_pass(p->n, axis, a, L.batch * p->num_modes, (cudaStream_t)stream))) return rc;
   return PTYRO_OK;
 }
 
@@ -499,7 +534,7 @@ int ptyro_make_probe(int32_t n, double voltage_kv, double aperture_mrad, double 
                                                                  (float2*)probe);
   float2* tw = (float2*)workspace;
   k_twiddle<<<(n + 255) / 256, 256, 0, st>>>(n, tw);
-  int rc = check_launch("make_probe setup");
+  int rc = check_launch("make_probe setup", 2);
   if (rc) return rc;
   if ((rc = fft2_planes(n, 1, true, (float2*)probe, tw, st))) return rc;
   k_swap_quadrants<<<(unsigned)((nn / 2 + 255) / 256), 256, 0, st>>>(n, 1, (float2*)probe);

@@ -1,9 +1,14 @@
 // Launchers of the pass kernel, one translation unit per grid edge (pass_<n>.cu).
 // Each returns the cudaError_t of its launch as int (0 = success).
 #pragma once
+#include <atomic>
+
 #include "ms_pass.cuh"
 
 namespace ptyro {
+
+// Number of engine kernels enqueued by this process (all devices, all threads).
+extern std::atomic<unsigned long long> g_launches;
 
 template <int N1, int N2, int AXIS>
 int launch_pass_t(const PassArgs& a, int grid_y, cudaStream_t st) {
@@ -21,6 +26,7 @@ int launch_pass_t(const PassArgs& a, int grid_y, cudaStream_t st) {
   const int lines = warps * G;
   dim3 grid((N + lines - 1) / lines, grid_y);
   ms_pass_kernel<N1, N2, AXIS, kMaxWarps><<<grid, warps * 32, smem, st>>>(a);
+  g_launches.fetch_add(1, std::memory_order_relaxed);
   return (int)cudaGetLastError();
 }
 
