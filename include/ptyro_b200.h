@@ -118,6 +118,24 @@ int ptyro_ms_steady_pass(const ptyro_ms_params* p, int32_t axis, int32_t reps, v
  * the FP32 ceiling used as the roofline denominator; no reference counterpart. */
 int ptyro_fp32_fma_probe(float* out, int32_t blocks, int32_t iters, void* stream);
 
+/* Bytes of the fixed device scratch array behind ptyro_ms_forward_noalloc. */
+#define PTYRO_STATIC_SCRATCH_BYTES (64u * 1024u * 1024u)
+
+/* Forward model that allocates nothing and takes no workspace, for callers that
+ * cannot allocate device memory: a host that owns all of it (an XLA FFI handler
+ * without a workspace operand, a fixed-budget plugin host) or code running during
+ * CUDA stream capture, where cudaMalloc is not allowed. No counterpart in the
+ * reference (JAX allocates for its own path).
+ * Same arguments and results as ptyro_ms_forward minus the workspace; the scratch
+ * is a PTYRO_STATIC_SCRATCH_BYTES array in the library's device image, held on
+ * every GPU that loads the library until exit. The first call on a device looks
+ * up that array's address; make it before any stream capture. Calls on a device
+ * share the array, so calls that overlap on the GPU race: serialise them on one
+ * stream. Jobs whose scratch does not fit (e.g. a 1024^2 grid with many slices)
+ * are rejected with PTYRO_ERR_WORKSPACE before anything is launched. */
+int ptyro_ms_forward_noalloc(const ptyro_ms_params* p, const float* potential, const float* modes,
+                             const float* weights, const double* positions, float* patterns, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

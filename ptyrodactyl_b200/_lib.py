@@ -18,6 +18,7 @@ PTYRO_ERR_INVALID = 1
 PTYRO_ERR_WORKSPACE = 2
 PTYRO_ERR_CUDA = 3
 PTYRO_ERR_UNSUPPORTED = 4
+STATIC_SCRATCH_BYTES = 64 << 20  # PTYRO_STATIC_SCRATCH_BYTES
 
 # every symbol include/ptyro_b200.h declares
 EXPORTED_SYMBOLS = (
@@ -32,6 +33,7 @@ EXPORTED_SYMBOLS = (
     "ptyro_launch_count",
     "ptyro_ms_steady_pass",
     "ptyro_fp32_fma_probe",
+    "ptyro_ms_forward_noalloc",
 )
 
 
@@ -95,6 +97,8 @@ def _declare(lib) -> None:
     lib.ptyro_ms_steady_pass.argtypes = [pp, i32, i32, vp, sz, vp]
     lib.ptyro_fp32_fma_probe.restype = ctypes.c_int
     lib.ptyro_fp32_fma_probe.argtypes = [vp, i32, i32, vp]
+    lib.ptyro_ms_forward_noalloc.restype = ctypes.c_int
+    lib.ptyro_ms_forward_noalloc.argtypes = [pp, vp, vp, vp, vp, vp, vp]
 
 
 def load(path: str | None = None):

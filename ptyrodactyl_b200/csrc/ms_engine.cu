@@ -17,6 +17,8 @@ namespace ptyro {
 // ---------------------------------------------------------------- errors
 static thread_local std::string g_err;
 
+void set_error_message(const std::string& msg) { g_err = msg; }
+
 static int fail(int code, const std::string& msg) {
   g_err = msg;
   return code;
