@@ -205,7 +205,7 @@ def run_ours(args, rank, world, local_rank):
     pos_d = torch.as_tensor(pos, dtype=torch.float64, device=dev)
     out_d = torch.empty((P, n, n), dtype=torch.float32, device=dev)
     prm = ms_params(n, S, 1, P, w.voltage_kv, synth.SLICE_DZ, w.calib, w.calib, slices_d.stride(),
-                    modes_d.stride(), args.batch)
+                    modes_d.stride(), args.batch, args.tune)
     ws_bytes = lib.ptyro_ms_workspace_bytes(ctypes.byref(prm))
     ws = torch.empty(ws_bytes, dtype=torch.uint8, device=dev)
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
@@ -327,7 +327,7 @@ def run_ours(args, rank, world, local_rank):
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": w.name, "grid": n, "slices": S, "probes_per_gpu": P, "modes": 1,
-                       "batch": batch, "voltage_kv": w.voltage_kv, "aperture_mrad": w.aperture_mrad,
+                       "batch": batch, "tune": args.tune, "voltage_kv": w.voltage_kv, "aperture_mrad": w.aperture_mrad,
                        "defocus_ang": w.defocus_ang, "c3_ang": w.c3_ang,
                        "l2": "flushed (256 MB write) before every timed step",
                        "parallelism": f"dp{world} (probe shards, no collective)"},
@@ -414,6 +414,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--batch", type=int, default=0)
+    ap.add_argument("--tune", type=int, default=3, help="pass-kernel occupancy variant bits")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")

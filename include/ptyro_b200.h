@@ -41,7 +41,8 @@ typedef struct ptyro_ms_params {
   int32_t num_modes;           /* M >= 1 */
   int32_t num_probes;          /* P >= 0 scan positions */
   int32_t batch;               /* probes in flight per batch; 0 = automatic */
-  int32_t reserved;
+  int32_t tune;                /* kernel variant bits (0 = default): bit a selects the
+                                  3-CTAs-per-SM register budget for passes along axis a */
   double voltage_kv;           /* MicroscopeConfig.voltage_kv */
   double slice_thickness_ang;  /* PotentialSlices.slice_thickness */
   double calib_ang;            /* min(PotentialSlices.calib, ProbeModes.calib): propagator grid */

@@ -46,7 +46,7 @@ class MsParams(ctypes.Structure):
         ("num_modes", ctypes.c_int32),
         ("num_probes", ctypes.c_int32),
         ("batch", ctypes.c_int32),
-        ("reserved", ctypes.c_int32),
+        ("tune", ctypes.c_int32),
         ("voltage_kv", ctypes.c_double),
         ("slice_thickness_ang", ctypes.c_double),
         ("calib_ang", ctypes.c_double),

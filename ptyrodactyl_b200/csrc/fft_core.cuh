@@ -145,7 +145,8 @@ struct LineBuf {
 };
 
 // natural -> k-order transform of one line, unnormalised. DIR = -1 forward.
-// tw[j] = exp(-2 pi i j / N) for j in [0, N) (shared memory).
+// tw[k2 * N1 + t] = exp(-2 pi i t k2 / N) (shared memory; lanes of one k2 read
+// consecutive entries, so the table is read without bank conflicts).
 template <int N1, int N2, int DIR>
 __device__ __forceinline__ void line_nat_to_k(float2 (&v)[N2], int t, float2* buf, const float2* tw) {
   using LB = LineBuf<N1, N2>;
@@ -153,7 +154,7 @@ __device__ __forceinline__ void line_nat_to_k(float2 (&v)[N2], int t, float2* bu
   if (t != 0) {
 #pragma unroll
     for (int k2 = 1; k2 < N2; ++k2) {
-      const float2 w = tw[t * k2];
+      const float2 w = tw[k2 * N1 + t];
       v[k2] = DIR < 0 ? cmul(v[k2], w) : cmulc(v[k2], w);
     }
   }
@@ -184,7 +185,7 @@ __device__ __forceinline__ void line_k_to_nat(float2 (&v)[N2], int t, float2* bu
   if (t != 0) {
 #pragma unroll
     for (int k2 = 1; k2 < N2; ++k2) {
-      const float2 w = tw[t * k2];
+      const float2 w = tw[k2 * N1 + t];
       v[k2] = DIR < 0 ? cmul(v[k2], w) : cmulc(v[k2], w);
     }
   }

@@ -93,9 +93,9 @@ __global__ void k_propagator2d(int n, double calib, double lam_dz, float2* p2) {
 }
 
 // transmission_func (simulations.py:105-159): T_s = exp(i sigma V_s), evaluated in
-// double and rounded once; output (S, N, N) row-major.
+// double and rounded once; written row-major (S, N, N) and transposed (S, N^T).
 __global__ void k_transmission(const float* __restrict__ V, long long sy, long long sx, long long ss,
-                               int n, int S, double sigma, float2* __restrict__ T) {
+                               int n, int S, double sigma, float2* __restrict__ T, float2* __restrict__ TT) {
   const size_t total = (size_t)S * n * n;
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
        i += (size_t)gridDim.x * blockDim.x) {
@@ -105,7 +105,9 @@ __global__ void k_transmission(const float* __restrict__ V, long long sy, long l
     const double ph = sigma * (double)V[(long long)y * sy + (long long)x * sx + (long long)s * ss];
     double sn, cs;
     sincos(ph, &sn, &cs);
-    T[i] = make_float2((float)cs, (float)sn);
+    const float2 v = make_float2((float)cs, (float)sn);
+    T[i] = v;
+    TT[(size_t)s * n * n + (size_t)x * n + y] = v;
   }
 }
 
@@ -219,17 +221,17 @@ static bool shape_for(int n, Shape* s) {
   }
 }
 
-static int launch_pass(int n, int axis, const PassArgs& a, int grid_y, cudaStream_t st) {
+static int launch_pass(int n, int axis, const PassArgs& a, int grid_y, cudaStream_t st, int variant = 0) {
   if (grid_y <= 0) return PTYRO_OK;
   int rc;
   switch (n) {
-    case 16: rc = launch_pass_16(axis, a, grid_y, st); break;
-    case 32: rc = launch_pass_32(axis, a, grid_y, st); break;
-    case 64: rc = launch_pass_64(axis, a, grid_y, st); break;
-    case 128: rc = launch_pass_128(axis, a, grid_y, st); break;
-    case 256: rc = launch_pass_256(axis, a, grid_y, st); break;
-    case 512: rc = launch_pass_512(axis, a, grid_y, st); break;
-    case 1024: rc = launch_pass_1024(axis, a, grid_y, st); break;
+    case 16: rc = launch_pass_16(axis, a, grid_y, st, variant); break;
+    case 32: rc = launch_pass_32(axis, a, grid_y, st, variant); break;
+    case 64: rc = launch_pass_64(axis, a, grid_y, st, variant); break;
+    case 128: rc = launch_pass_128(axis, a, grid_y, st, variant); break;
+    case 256: rc = launch_pass_256(axis, a, grid_y, st, variant); break;
+    case 512: rc = launch_pass_512(axis, a, grid_y, st, variant); break;
+    case 1024: rc = launch_pass_1024(axis, a, grid_y, st, variant); break;
     default: return fail(PTYRO_ERR_UNSUPPORTED, "grid edge not compiled");
   }
   if (rc != 0) return fail(PTYRO_ERR_CUDA, std::string("ms_pass_kernel: ") + cudaGetErrorString((cudaError_t)rc));
@@ -257,7 +259,7 @@ static int fft2_planes(int n, int count, bool inverse, float2* data, const float
 static size_t align_up(size_t v) { return (v + 255) & ~(size_t)255; }
 
 struct Layout {
-  size_t tw, pf, trans, probe_k, ramp_y, ramp_x, waves, p2, total;
+  size_t tw, pf, trans, trans_t, probe_k, ramp_y, ramp_x, waves, p2, total;
   int batch;
 };
 
@@ -279,6 +281,7 @@ static Layout layout_for(const ptyro_ms_params* p) {
   L.tw = o; o = align_up(o + 8 * (size_t)p->n);
   L.pf = o; o = align_up(o + 8 * (size_t)p->n);
   L.trans = o; o = align_up(o + 8 * nn * p->num_slices);
+  L.trans_t = o; o = align_up(o + 8 * nn * p->num_slices);
   L.probe_k = o; o = align_up(o + 8 * nn * p->num_modes);
   L.ramp_y = o; o = align_up(o + 8 * (size_t)p->n * L.batch);
   L.ramp_x = o; o = align_up(o + 8 * (size_t)p->n * L.batch);
@@ -339,7 +342,7 @@ static int forward_setup(const ptyro_ms_params* p, const Layout& L, char* ws, co
   k_propagator<<<(n + 255) / 256, 256, 0, st>>>(n, p->calib_ang, lam * p->slice_thickness_ang, 1.0 / n, pf);
   k_transmission<<<blocks_for(nn * p->num_slices, 256), 256, 0, st>>>(
       potential, p->pot_stride_y, p->pot_stride_x, p->pot_stride_s, n, p->num_slices,
-      interaction_sigma(p->voltage_kv), T);
+      interaction_sigma(p->voltage_kv), T, (float2*)(ws + L.trans_t));
   k_gather_modes<<<blocks_for(nn * p->num_modes, 256), 256, 0, st>>>(
       (const float2*)modes, p->mode_stride_y, p->mode_stride_x, p->mode_stride_m, n, p->num_modes, pk);
   int rc = check_launch("forward setup", 4);
@@ -387,6 +390,7 @@ int ptyro_ms_forward(const ptyro_ms_params* p, const float* potential, const flo
   a.ramp_y = ry;
   a.ramp_x = rx;
   a.trans = (const float2*)(ws + L.trans);
+  a.trans_t = (const float2*)(ws + L.trans_t);
   a.pf = (const float2*)(ws + L.pf);
   a.tw = (const float2*)(ws + L.tw);
   a.weights = weights;
@@ -399,7 +403,7 @@ int ptyro_ms_forward(const ptyro_ms_params* p, const float* potential, const flo
     // pass 0: x part of the IFFT2 of the shifted probe spectrum
     PassArgs q = a;
     q.src = SRC_PROBE; q.op1 = OP_IFFT; q.t_slice = -1; q.op2 = OP_NONE; q.dst = DST_WAVE;
-    if ((rc = launch_pass(n, 0, q, nb * M, st))) return rc;
+    if ((rc = launch_pass(n, 0, q, nb * M, st, p->tune))) return rc;
     for (int k = 1; k <= S; ++k) {
       q = a;
       q.src = SRC_WAVE;
@@ -407,12 +411,12 @@ int ptyro_ms_forward(const ptyro_ms_params* p, const float* potential, const flo
       q.t_slice = k - 1;
       q.op2 = k == S ? OP_FFT : OP_CONV;
       q.dst = DST_WAVE;
-      if ((rc = launch_pass(n, k % 2, q, nb * M, st))) return rc;
+      if ((rc = launch_pass(n, k % 2, q, nb * M, st, p->tune))) return rc;
     }
     q = a;
     q.src = SRC_WAVE; q.op1 = OP_FFT; q.t_slice = -1; q.op2 = OP_NONE; q.dst = DST_PATTERN;
     q.pattern = patterns + (size_t)b0 * nn;
-    if ((rc = launch_pass(n, (S + 1) % 2, q, nb, st))) return rc;
+    if ((rc = launch_pass(n, (S + 1) % 2, q, nb, st, p->tune))) return rc;
   }
   return PTYRO_OK;
 }
@@ -481,6 +485,7 @@ int ptyro_ms_steady_pass(const ptyro_ms_params* p, int32_t axis, int32_t reps, v
   PassArgs a = {};
   a.wave = (float2*)(ws + L.waves);
   a.trans = (const float2*)(ws + L.trans);
+  a.trans_t = (const float2*)(ws + L.trans_t);
   a.pf = (const float2*)(ws + L.pf);
   a.tw = (const float2*)(ws + L.tw);
   a.n_modes = p->num_modes;
@@ -491,7 +496,7 @@ int ptyro_ms_steady_pass(const ptyro_ms_params* p, int32_t axis, int32_t reps, v
   a.op2 = OP_CONV;
   a.dst = DST_WAVE;
   for (int r = 0; r < reps; ++r)
-    if ((rc = launch_pass(p->n, axis, a, L.batch * p->num_modes, (cudaStream_t)stream))) return rc;
+    if ((rc = launch_pass(p->n, axis, a, L.batch * p->num_modes, (cudaStream_t)stream, p->tune))) return rc;
   return PTYRO_OK;
 }
 

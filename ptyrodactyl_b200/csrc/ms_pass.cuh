@@ -9,6 +9,12 @@
 // same axis, touching the wave in memory once per slice:
 //   pass k (k >= 1):  [axis part of op_{k-1}]  x T_{k-1}  [axis part of op_k]
 // with op_0 = IFFT2 of the shifted probe spectrum, op_j = Conv_{j-1}, op_S = FFT2.
+//
+// Row passes (AXIS 0) read and write each line directly: the N1 lanes of a line
+// touch consecutive addresses. Column passes (AXIS 1) stage the CTA's block of
+// columns through a shared-memory tile so that global traffic moves whole
+// row segments (lines-per-CTA x 8 bytes, 128 B at 256^2) in both directions; they
+// read the transmission from a transposed copy for the same reason.
 #pragma once
 #include "fft_core.cuh"
 
@@ -23,7 +29,8 @@ struct PassArgs {
   const float2* probe_k;   // (M, N, N) spectrum of the beam modes (SRC_PROBE)
   const float2* ramp_y;    // (B, N) shift ramp along y per probe of the batch (SRC_PROBE)
   const float2* ramp_x;    // (B, N) shift ramp along x
-  const float2* trans;     // (S, N, N) transmission exp(i sigma V), row-major
+  const float2* trans;     // (S, N, N) transmission exp(i sigma V), row-major [y][x]
+  const float2* trans_t;   // (S, N, N) the same, transposed [x][y]
   const float2* pf;        // (N) 1-D propagator factor along this axis, already divided by N
   const float2* tw;        // (N) forward twiddles exp(-2 pi i j / N)
   float* pattern;          // (B, N, N) fftshifted intensity (DST_PATTERN)
@@ -40,15 +47,22 @@ struct PassGeom {
   static constexpr int G = 32 / N1;  // lines per warp
   static_assert(N2 % N1 == 0, "N2 must be a multiple of N1");
   static_assert(32 % N1 == 0, "N1 must divide the warp");
+  static constexpr int kWarps = N / G < 8 ? N / G : 8;  // lines per CTA = kWarps * G divides N
+  static constexpr int kLines = kWarps * G;
+  static int warps_for() { return kWarps; }
+  // twiddle table + max(exchange buffers, column tile)
   static size_t smem_bytes(int warps) {
-    return sizeof(float2) * ((size_t)N + (size_t)warps * G * LineBuf<N1, N2>::kSize);
+    const size_t lines = (size_t)warps * G;
+    const size_t xbuf = lines * LineBuf<N1, N2>::kSize;
+    const size_t tile = (size_t)N * (lines + G);
+    return sizeof(float2) * ((size_t)N + (xbuf > tile ? xbuf : tile));
   }
 };
 
 // op on registers in natural distribution; returns true if the result is k-order.
 template <int N1, int N2>
 __device__ __forceinline__ bool apply_op(int op, float2 (&v)[N2], int t, float2* buf, const float2* tw,
-                                         const float2* __restrict__ pf, float scale) {
+                                         const float2* __restrict__ pf) {
   if (op == OP_FFT) {
     line_nat_to_k<N1, N2, -1>(v, t, buf, tw);
     return true;
@@ -66,26 +80,33 @@ __device__ __forceinline__ bool apply_op(int op, float2 (&v)[N2], int t, float2*
   return false;
 }
 
-template <int N1, int N2, int AXIS, int WARPS>
-__global__ void __launch_bounds__(WARPS * 32) ms_pass_kernel(PassArgs a) {
+// MINB: resident CTAs per SM the register allocation must allow (occupancy variant).
+template <int N1, int N2, int AXIS, int WARPS, int MINB>
+__global__ void __launch_bounds__(WARPS * 32, MINB) ms_pass_kernel(PassArgs a) {
   using Geo = PassGeom<N1, N2>;
   using LB = LineBuf<N1, N2>;
   constexpr int N = Geo::N;
   constexpr int G = Geo::G;
   extern __shared__ float2 smem[];
-  float2* tw = smem;
-  for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = a.tw[i];
+  float2* tw = smem;        // tw[k2 * N1 + t] = W_N^{t k2}
+  float2* work = smem + N;  // exchange buffers; column passes alias the staging tile here
+  for (int i = threadIdx.x; i < N; i += blockDim.x) {
+    const int k2 = i / N1, tt = i % N1;
+    tw[i] = a.tw[(tt * k2) % N];
+  }
   __syncthreads();
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  // Row passes put consecutive lanes along x inside a line; column passes put them
-  // across neighbouring columns, so both load full 32-byte sectors.
   const int t = AXIS == 0 ? (lane % N1) : (lane / G);
   const int gl = AXIS == 0 ? (lane / N1) : (lane % G);
-  const int warps = blockDim.x >> 5;
-  const int line = blockIdx.x * (warps * G) + warp * G + gl;
-  if (blockIdx.x * (warps * G) + warp * G >= N) return;  // whole warp idle (N < lines per CTA)
-  float2* buf = smem + N + (warp * G + gl) * LB::kSize;
+  constexpr int lines = WARPS * G;          // lines per CTA (blockDim.x == WARPS * 32); divides N
+  static_assert(N % lines == 0, "lines per CTA must divide N");
+  constexpr int pitch = lines + G;          // staging-tile row pitch (float2): t*pitch + gl spreads banks
+  constexpr int kTileIters = N * lines / (WARPS * 32);
+  const int lc = warp * G + gl;             // line within the CTA
+  const int line0 = blockIdx.x * lines;
+  const int line = line0 + lc;
+  float2* buf = work + lc * LB::kSize;
   const size_t NN = (size_t)N * N;
   auto off = [&](int e) -> size_t { return AXIS == 0 ? (size_t)line * N + e : (size_t)e * N + line; };
 
@@ -94,12 +115,13 @@ __global__ void __launch_bounds__(WARPS * 32) ms_pass_kernel(PassArgs a) {
   float acc[N2];
 #pragma unroll
   for (int r = 0; r < N2; ++r) acc[r] = 0.f;
+  bool korder = false;
 
   for (int m = 0; m < mcount; ++m) {
     const int slot = to_pattern ? blockIdx.y * a.n_modes + m : blockIdx.y;
     float2* w = a.wave + (size_t)slot * NN;
     float2 v[N2];
-    bool korder;
+    const bool load_k = a.src == SRC_PROBE || a.op1 == OP_IFFT;
     // ---- load
     if (a.src == SRC_PROBE) {
       const int b = blockIdx.y / a.n_modes;
@@ -112,16 +134,42 @@ __global__ void __launch_bounds__(WARPS * 32) ms_pass_kernel(PassArgs a) {
         const int k = korder_index<N1, N2>(t, r);
         v[r] = cmul(cmul(pk[off(k)], ra[k]), rl);
       }
-      korder = true;
-    } else if (a.op1 == OP_IFFT) {
+    } else if (AXIS == 0) {
+      if (load_k) {
 #pragma unroll
-      for (int r = 0; r < N2; ++r) v[r] = w[off(korder_index<N1, N2>(t, r))];
-      korder = true;
+        for (int r = 0; r < N2; ++r) v[r] = w[off(korder_index<N1, N2>(t, r))];
+      } else {
+#pragma unroll
+        for (int j = 0; j < N2; ++j) v[j] = w[off(t + N1 * j)];
+      }
     } else {
+      __syncthreads();  // the tile aliases other warps' exchange buffers
+      constexpr int kChunk = kTileIters < 8 ? kTileIters : 8;  // loads in flight per thread
+#pragma unroll 1
+      for (int c0 = 0; c0 < kTileIters; c0 += kChunk) {
+        float2 stage[kChunk];
 #pragma unroll
-      for (int j = 0; j < N2; ++j) v[j] = w[off(t + N1 * j)];
-      korder = false;
+        for (int u = 0; u < kChunk; ++u) {
+          const int i = threadIdx.x + (c0 + u) * WARPS * 32;
+          stage[u] = w[(size_t)(i / lines) * N + line0 + i % lines];
+        }
+#pragma unroll
+        for (int u = 0; u < kChunk; ++u) {
+          const int i = threadIdx.x + (c0 + u) * WARPS * 32;
+          work[(i / lines) * pitch + i % lines] = stage[u];
+        }
+      }
+      __syncthreads();
+      if (load_k) {
+#pragma unroll
+        for (int r = 0; r < N2; ++r) v[r] = work[korder_index<N1, N2>(t, r) * pitch + lc];
+      } else {
+#pragma unroll
+        for (int j = 0; j < N2; ++j) v[j] = work[(t + N1 * j) * pitch + lc];
+      }
+      __syncthreads();
     }
+    korder = load_k;
     // ---- op1
     if (a.op1 == OP_IFFT) {
       line_k_to_nat<N1, N2, +1>(v, t, buf, tw);
@@ -129,41 +177,71 @@ __global__ void __launch_bounds__(WARPS * 32) ms_pass_kernel(PassArgs a) {
       for (int j = 0; j < N2; ++j) v[j] = cscale(v[j], a.scale);
       korder = false;
     } else if (a.op1 != OP_NONE) {
-      korder = apply_op<N1, N2>(a.op1, v, t, buf, tw, a.pf, a.scale);
+      korder = apply_op<N1, N2>(a.op1, v, t, buf, tw, a.pf);
     }
-    // ---- transmission
+    // ---- transmission (natural distribution; row-major table for rows, transposed for columns)
     if (a.t_slice >= 0) {
-      const float2* T = a.trans + (size_t)a.t_slice * NN;
+      const float2* T = (AXIS == 0 ? a.trans : a.trans_t) + (size_t)a.t_slice * NN + (size_t)line * N;
 #pragma unroll
       for (int j = 0; j < N2; ++j) {
-        const float2 tv = __ldg(T + off(t + N1 * j));
+        const float2 tv = __ldg(T + t + N1 * j);
         v[j] = a.t_conj ? cmulc(v[j], tv) : cmul(v[j], tv);
       }
     }
     // ---- op2
-    if (a.op2 != OP_NONE) korder = apply_op<N1, N2>(a.op2, v, t, buf, tw, a.pf, a.scale);
+    if (a.op2 != OP_NONE) korder = apply_op<N1, N2>(a.op2, v, t, buf, tw, a.pf);
     // ---- store
     if (to_pattern) {
       const float wm = a.weights[m];
 #pragma unroll
       for (int r = 0; r < N2; ++r) acc[r] = fmaf(wm, fmaf(v[r].x, v[r].x, v[r].y * v[r].y), acc[r]);
-    } else if (korder) {
+    } else if (AXIS == 0) {
+      if (korder) {
 #pragma unroll
-      for (int r = 0; r < N2; ++r) w[off(korder_index<N1, N2>(t, r))] = v[r];
+        for (int r = 0; r < N2; ++r) w[off(korder_index<N1, N2>(t, r))] = v[r];
+      } else {
+#pragma unroll
+        for (int j = 0; j < N2; ++j) w[off(t + N1 * j)] = v[j];
+      }
     } else {
+      __syncthreads();  // every warp is done with its exchange buffer
+      if (korder) {
 #pragma unroll
-      for (int j = 0; j < N2; ++j) w[off(t + N1 * j)] = v[j];
+        for (int r = 0; r < N2; ++r) work[korder_index<N1, N2>(t, r) * pitch + lc] = v[r];
+      } else {
+#pragma unroll
+        for (int j = 0; j < N2; ++j) work[(t + N1 * j) * pitch + lc] = v[j];
+      }
+      __syncthreads();
+#pragma unroll 8
+      for (int it = 0; it < kTileIters; ++it) {
+        const int i = threadIdx.x + it * WARPS * 32;
+        w[(size_t)(i / lines) * N + line0 + i % lines] = work[(i / lines) * pitch + i % lines];
+      }
     }
   }
   if (to_pattern) {
     // fftshift on store: frequency index k lands at (k + N/2) mod N on both axes.
     float* out = a.pattern + (size_t)blockIdx.y * NN;
-    const int ls = (line + N / 2) % N;
+    if (AXIS == 0) {
+      const int ls = (line + N / 2) % N;
 #pragma unroll
-    for (int r = 0; r < N2; ++r) {
-      const int ks = (korder_index<N1, N2>(t, r) + N / 2) % N;
-      const size_t o = AXIS == 0 ? (size_t)ls * N + ks : (size_t)ks * N + ls;
-      out[o] = acc[r];
+      for (int r = 0; r < N2; ++r) {
+        const int ks = (korder_index<N1, N2>(t, r) + N / 2) % N;
+        out[(size_t)ls * N + ks] = acc[r];
+      }
+    } else {
+      float* tile = reinterpret_cast<float*>(work);
+      __syncthreads();
+#pragma unroll
+      for (int r = 0; r < N2; ++r) tile[korder_index<N1, N2>(t, r) * pitch + lc] = acc[r];
+      __syncthreads();
+#pragma unroll 8
+      for (int it = 0; it < kTileIters; ++it) {
+        const int i = threadIdx.x + it * WARPS * 32;
+        const int rr = i / lines, c = i % lines;
+        out[(size_t)((rr + N / 2) % N) * N + (line0 + c + N / 2) % N] = tile[rr * pitch + c];
+      }
     }
   }
 }

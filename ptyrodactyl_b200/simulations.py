@@ -86,9 +86,10 @@ def _workspace(nbytes: int, device: torch.device) -> torch.Tensor:
 
 def ms_params(n: int, num_slices: int, num_modes: int, num_probes: int, voltage_kv: float,
               slice_thickness: float, calib_ang: float, shift_calib_ang: float,
-              pot_strides=(0, 0, 0), mode_strides=(0, 0, 0), batch: int = 0) -> _lib.MsParams:
+              pot_strides=(0, 0, 0), mode_strides=(0, 0, 0), batch: int = 0, tune: int = 0) -> _lib.MsParams:
     p = _lib.MsParams()
     p.n, p.num_slices, p.num_modes, p.num_probes, p.batch = n, num_slices, num_modes, num_probes, batch
+    p.tune = tune
     p.voltage_kv = float(voltage_kv)
     p.slice_thickness_ang = float(slice_thickness)
     p.calib_ang = float(calib_ang)
@@ -100,7 +101,8 @@ def ms_params(n: int, num_slices: int, num_modes: int, num_probes: int, voltage_
 
 def run_forward(slices: torch.Tensor, slice_thickness: float, modes: torch.Tensor, weights: torch.Tensor,
                 positions: torch.Tensor, voltage_kv: float, calib_ang: float, shift_calib_ang: float,
-                out: Optional[torch.Tensor] = None, batch: int = 0, plain: bool = False) -> torch.Tensor:
+                out: Optional[torch.Tensor] = None, batch: int = 0, plain: bool = False,
+                tune: int = 0) -> torch.Tensor:
     """Device-level forward: all tensors already on one CUDA device.
 
     slices (H, W, S) float32 (any strides), modes (H, W, M) complex64 (any strides),
@@ -114,7 +116,7 @@ def run_forward(slices: torch.Tensor, slice_thickness: float, modes: torch.Tenso
         raise ValueError("beam modes and potential slices must share the grid shape")
     num_probes = positions.shape[0]
     prm = ms_params(n, slices.shape[2], modes.shape[2], num_probes, voltage_kv, slice_thickness,
-                    calib_ang, shift_calib_ang, slices.stride(), modes.stride(), batch)
+                    calib_ang, shift_calib_ang, slices.stride(), modes.stride(), batch, tune)
     if out is None:
         out = torch.empty((num_probes, n, n), dtype=torch.float32, device=dev)
     if num_probes == 0:
