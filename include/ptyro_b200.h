@@ -76,6 +76,40 @@ int ptyro_ms_forward(const ptyro_ms_params* p, const float* potential, const flo
                      const float* weights, const double* positions, float* patterns,
                      void* workspace, size_t workspace_bytes, void* stream);
 
+/* Residual bytes ptyro_ms_forward_ckpt writes for `p`: per (probe, mode) one
+ * complex64 N x N plane per checkpoint (slices 0, K, 2K, ... for K = ckpt_every)
+ * plus one plane for the far-field amplitude. */
+size_t ptyro_ms_residual_bytes(const ptyro_ms_params* p, int32_t ckpt_every);
+
+/* ptyro_ms_forward that also records the residuals the gradient needs: the wave
+ * after every K-th transmission multiply and the complex far-field amplitude, as
+ * `residuals` (P, M, ceil(S/K) + 1, N, N) complex64. The reverse pass of
+ * jax.value_and_grad through stem_4d (src/ptyrodactyl/multislice/multislice_recon.py:1940,
+ * :1915-1966) would instead keep every slice's wave of the lax.scan.
+ * Workspace: ptyro_ms_workspace_bytes(p). */
+int ptyro_ms_forward_ckpt(const ptyro_ms_params* p, int32_t ckpt_every, const float* potential,
+                          const float* modes, const float* weights, const double* positions,
+                          float* patterns, float* residuals, void* workspace, size_t workspace_bytes,
+                          void* stream);
+
+/* Workspace bytes ptyro_ms_backward needs for `p` (p->batch probes per batch, 0 = automatic). */
+size_t ptyro_ms_backward_workspace_bytes(const ptyro_ms_params* p);
+
+/* Vector-Jacobian product of stem_4d: given dL/d(patterns) (P, N, N) float32 in the
+ * patterns' fftshifted layout and the residuals of ptyro_ms_forward_ckpt (same p,
+ * same ckpt_every), write
+ *   grad_potential  float32 dL/dV with the potential's strides (p->pot_stride_*),
+ *   grad_modes      complex64 gradient of the beam modes with the modes' strides, in
+ *                   JAX's convention for a real loss: conj(2 dL/dconj(z)) = dL/dRe - i dL/dIm.
+ * Matches jax.vjp / jax.grad through stem_4d in the reference (the gradient that
+ * multislice_recon.py:1940 takes w.r.t. the potential and the beam). Mode weights and
+ * positions are treated as constants. Sums over probes are in a fixed order.
+ * Workspace: ptyro_ms_backward_workspace_bytes(p). */
+int ptyro_ms_backward(const ptyro_ms_params* p, int32_t ckpt_every, const float* potential,
+                      const float* weights, const double* positions, const float* residuals,
+                      const float* grad_patterns, float* grad_potential, float* grad_modes,
+                      void* workspace, size_t workspace_bytes, void* stream);
+
 /* The same model run the plain way: one scan position at a time, one kernel per
  * stage (shift, and per slice transmission multiply, FFT2, propagator multiply,
  * IFFT2, then FFT2 and |.|^2), the way the reference's vmap body reads

@@ -30,4 +30,6 @@ from .simulations import (  # noqa: F401
     stem_4d,
 )
 
+from .autodiff import Stem4dFunction, make_probe_differentiable, stem_4d_patterns, vjp  # noqa: F401
+
 __version__ = "0.1.0"

@@ -34,6 +34,10 @@ EXPORTED_SYMBOLS = (
     "ptyro_ms_steady_pass",
     "ptyro_fp32_fma_probe",
     "ptyro_ms_forward_noalloc",
+    "ptyro_ms_residual_bytes",
+    "ptyro_ms_forward_ckpt",
+    "ptyro_ms_backward_workspace_bytes",
+    "ptyro_ms_backward",
 )
 
 
@@ -97,6 +101,14 @@ def _declare(lib) -> None:
     lib.ptyro_ms_steady_pass.argtypes = [pp, i32, i32, vp, sz, vp]
     lib.ptyro_fp32_fma_probe.restype = ctypes.c_int
     lib.ptyro_fp32_fma_probe.argtypes = [vp, i32, i32, vp]
+    lib.ptyro_ms_residual_bytes.restype = sz
+    lib.ptyro_ms_residual_bytes.argtypes = [pp, i32]
+    lib.ptyro_ms_forward_ckpt.restype = ctypes.c_int
+    lib.ptyro_ms_forward_ckpt.argtypes = [pp, i32, vp, vp, vp, vp, vp, vp, vp, sz, vp]
+    lib.ptyro_ms_backward_workspace_bytes.restype = sz
+    lib.ptyro_ms_backward_workspace_bytes.argtypes = [pp]
+    lib.ptyro_ms_backward.restype = ctypes.c_int
+    lib.ptyro_ms_backward.argtypes = [pp, i32, vp, vp, vp, vp, vp, vp, vp, vp, sz, vp]
     lib.ptyro_ms_forward_noalloc.restype = ctypes.c_int
     lib.ptyro_ms_forward_noalloc.argtypes = [pp, vp, vp, vp, vp, vp, vp]
 

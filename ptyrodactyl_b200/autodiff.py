@@ -1,0 +1,188 @@
+"""Reverse-mode differentiation of the multislice forward model.
+
+The reference differentiates ``stem_4d`` with ``jax.value_and_grad``
+(``src/ptyrodactyl/multislice/multislice_recon.py:1940``); reverse mode through
+its ``lax.scan`` keeps every slice's wave of every probe. Here the forward
+records only checkpoints (every ``ckpt_every`` slices) and the complex far-field
+amplitude, and the hand-written adjoint kernel (``ptyro_ms_backward``) runs the
+slice operator backwards for the forward wave and the adjoint together. This is
+the analogue of a ``jax.custom_vjp`` rule: :class:`Stem4dFunction` is a
+``torch.autograd.Function`` whose backward calls the adjoint kernel.
+
+Gradient conventions: torch returns ``2 dL/dconj(z)`` for a complex input of a
+real loss; the C-ABI returns JAX's convention ``conj(2 dL/dconj(z))``; this module
+converts between them.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import math
+from typing import Optional
+
+import torch
+
+from . import _lib
+from .simulations import _check_edge, _stream_ptr, _workspace, ms_params, relativistic_wavelength_ang
+
+DEFAULT_CKPT = 0  # 0: ceil(sqrt(S))
+
+
+def _ckpt_for(num_slices: int, ckpt_every: int) -> int:
+    if ckpt_every and ckpt_every > 0:
+        return int(ckpt_every)
+    return max(1, int(math.ceil(math.sqrt(num_slices))))
+
+
+class Stem4dFunction(torch.autograd.Function):
+    """patterns = stem_4d(slices, modes) with a checkpointed adjoint backward.
+
+    slices (H, W, S) float32 CUDA (any strides); modes (H, W, M) complex64 CUDA (any
+    strides); weights (M,) float32; positions (P, 2) float64. Weights and positions
+    are constants (no gradient).
+    """
+
+    @staticmethod
+    def forward(ctx, slices, modes, weights, positions, slice_thickness: float, voltage_kv: float,
+                calib_ang: float, shift_calib_ang: float, ckpt_every: int = 0, batch: int = 0, tune: int = 0):
+        lib = _lib.load()
+        dev = slices.device
+        n = _check_edge(slices.shape[0], slices.shape[1])
+        if tuple(modes.shape[:2]) != (n, n):
+            raise ValueError("beam modes and potential slices must share the grid shape")
+        S, M, P = slices.shape[2], modes.shape[2], positions.shape[0]
+        k = _ckpt_for(S, ckpt_every)
+        prm = ms_params(n, S, M, P, voltage_kv, slice_thickness, calib_ang, shift_calib_ang, slices.stride(),
+                        modes.stride(), batch, tune)
+        out = torch.empty((P, n, n), dtype=torch.float32, device=dev)
+        res = torch.empty(lib.ptyro_ms_residual_bytes(ctypes.byref(prm), k) // 4 if P else 1,
+                          dtype=torch.float32, device=dev)
+        if P:
+            ws_bytes = lib.ptyro_ms_workspace_bytes(ctypes.byref(prm))
+            ws = _workspace(ws_bytes, dev)
+            _lib.check(lib.ptyro_ms_forward_ckpt(ctypes.byref(prm), k, slices.data_ptr(), modes.data_ptr(),
+                                                 weights.data_ptr(), positions.data_ptr(), out.data_ptr(),
+                                                 res.data_ptr(), ws.data_ptr(), ws_bytes, _stream_ptr(dev)))
+        ctx.save_for_backward(slices, modes, weights, positions, res)
+        ctx.cfg = (slice_thickness, voltage_kv, calib_ang, shift_calib_ang, k, batch, tune)
+        return out
+
+    @staticmethod
+    def backward(ctx, grad_out):
+        slices, modes, weights, positions, res = ctx.saved_tensors
+        slice_thickness, voltage_kv, calib_ang, shift_calib_ang, k, batch, tune = ctx.cfg
+        lib = _lib.load()
+        dev = slices.device
+        n, S, M, P = slices.shape[0], slices.shape[2], modes.shape[2], positions.shape[0]
+        g_slices = torch.empty_strided(slices.shape, slices.stride(), dtype=torch.float32, device=dev)
+        g_modes = torch.empty_strided(modes.shape, modes.stride(), dtype=torch.complex64, device=dev)
+        if P == 0:
+            g_slices.zero_()
+            g_modes.zero_()
+        else:
+            g = grad_out.to(torch.float32).contiguous()
+            prm = ms_params(n, S, M, P, voltage_kv, slice_thickness, calib_ang, shift_calib_ang, slices.stride(),
+                            modes.stride(), batch, tune)
+            ws_bytes = lib.ptyro_ms_backward_workspace_bytes(ctypes.byref(prm))
+            ws = _workspace(ws_bytes, dev)
+            _lib.check(lib.ptyro_ms_backward(ctypes.byref(prm), k, slices.data_ptr(), weights.data_ptr(),
+                                             positions.data_ptr(), res.data_ptr(), g.data_ptr(),
+                                             g_slices.data_ptr(), g_modes.data_ptr(), ws.data_ptr(), ws_bytes,
+                                             _stream_ptr(dev)))
+        # the C-ABI gives JAX's convention conj(2 dL/dconj); torch wants 2 dL/dconj
+        return (g_slices if ctx.needs_input_grad[0] else None,
+                g_modes.conj().resolve_conj() if ctx.needs_input_grad[1] else None,
+                None, None, None, None, None, None, None, None, None)
+
+
+def stem_4d_patterns(slices: torch.Tensor, modes: torch.Tensor, weights: torch.Tensor, positions: torch.Tensor,
+                     slice_thickness: float, voltage_kv: float, calib_ang: float,
+                     shift_calib_ang: Optional[float] = None, ckpt_every: int = DEFAULT_CKPT,
+                     batch: int = 0, tune: int = 0) -> torch.Tensor:
+    """Differentiable patterns (P, H, W) of the forward model (device tensors)."""
+    return Stem4dFunction.apply(slices, modes, weights, positions, float(slice_thickness), float(voltage_kv),
+                                float(calib_ang), float(calib_ang if shift_calib_ang is None else shift_calib_ang),
+                                int(ckpt_every), int(batch), int(tune))
+
+
+def vjp(slices, modes, weights, positions, grad_patterns, slice_thickness, voltage_kv, calib_ang,
+        shift_calib_ang=None, ckpt_every: int = DEFAULT_CKPT, batch: int = 0):
+    """(patterns, dL/dV, dL/dmodes in JAX's convention) for dL/dpatterns = grad_patterns."""
+    lib = _lib.load()
+    dev = slices.device
+    n = _check_edge(slices.shape[0], slices.shape[1])
+    S, M, P = slices.shape[2], modes.shape[2], positions.shape[0]
+    k = _ckpt_for(S, ckpt_every)
+    sc = float(calib_ang if shift_calib_ang is None else shift_calib_ang)
+    prm = ms_params(n, S, M, P, voltage_kv, slice_thickness, calib_ang, sc, slices.stride(), modes.stride(), batch)
+    out = torch.empty((P, n, n), dtype=torch.float32, device=dev)
+    res = torch.empty(max(1, lib.ptyro_ms_residual_bytes(ctypes.byref(prm), k) // 4), dtype=torch.float32,
+                      device=dev)
+    ws_bytes = lib.ptyro_ms_workspace_bytes(ctypes.byref(prm))
+    ws = _workspace(ws_bytes, dev)
+    st = _stream_ptr(dev)
+    _lib.check(lib.ptyro_ms_forward_ckpt(ctypes.byref(prm), k, slices.data_ptr(), modes.data_ptr(),
+                                         weights.data_ptr(), positions.data_ptr(), out.data_ptr(), res.data_ptr(),
+                                         ws.data_ptr(), ws_bytes, st))
+    g_slices = torch.empty_strided(slices.shape, slices.stride(), dtype=torch.float32, device=dev)
+    g_modes = torch.empty_strided(modes.shape, modes.stride(), dtype=torch.complex64, device=dev)
+    bws = lib.ptyro_ms_backward_workspace_bytes(ctypes.byref(prm))
+    bw = _workspace(bws, dev)
+    g = grad_patterns.to(torch.float32).contiguous()
+    _lib.check(lib.ptyro_ms_backward(ctypes.byref(prm), k, slices.data_ptr(), weights.data_ptr(),
+                                     positions.data_ptr(), res.data_ptr(), g.data_ptr(), g_slices.data_ptr(),
+                                     g_modes.data_ptr(), bw.data_ptr(), bws, st))
+    return out, g_slices, g_modes
+
+
+# ----------------------------------------------------------------------------- probe
+class _Fft2Fn(torch.autograd.Function):
+    """fft2 / ifft2 on the engine's kernels with their adjoints."""
+
+    @staticmethod
+    def forward(ctx, x, inverse: bool):
+        from .simulations import fft2
+        ctx.inverse = inverse
+        return fft2(x, inverse=inverse)
+
+    @staticmethod
+    def backward(ctx, g):
+        from .simulations import fft2
+        n2 = g.shape[-1] * g.shape[-2]
+        if ctx.inverse:  # y = F^H x / n2  ->  x_bar = F y_bar / n2
+            return fft2(g, inverse=False) / n2, None
+        return fft2(g, inverse=True) * n2, None  # y = F x -> x_bar = F^H y_bar
+
+
+def make_probe_differentiable(voltage_kv: float, aperture_mrad: float, probe_shape, probe_calibration_pm: float,
+                              defocus_ang, c3_ang, c5_ang=0.0, a1x_ang=0.0, a1y_ang=0.0,
+                              device=None) -> torch.Tensor:
+    """make_probe (multislice/simulations.py:334-431) with torch-differentiable
+    aberration coefficients (tensors or floats).
+
+    chi = 2 pi / lambda (C1 p^2/2 + 1e7 C3 p^4/4 + 1e7 C5 p^6/6) as the reference
+    (:491-497), plus a two-fold astigmatism term (extension; the reference has
+    none): 2 pi / lambda * p^2/2 * (A1x cos 2 phi + A1y sin 2 phi), phi the azimuth
+    of q. The IFFT2 runs on the engine's kernels.
+    """
+    dev = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+    h, w = int(probe_shape[0]), int(probe_shape[1])
+    n = _check_edge(h, w)
+    lam = relativistic_wavelength_ang(voltage_kv)
+    fov = n * 0.01 * float(probe_calibration_pm)
+    f = torch.fft.fftfreq(n, d=1.0 / n, dtype=torch.float64, device=dev) / fov
+    ly, lx = torch.meshgrid(f, f, indexing="ij")
+    q = torch.sqrt(lx * lx + ly * ly)
+    mask = (q <= (aperture_mrad / 1000.0) / lam).to(torch.float64)
+    p = lam * q
+
+    def t(v):
+        return v.to(torch.float64) if isinstance(v, torch.Tensor) else torch.tensor(float(v), dtype=torch.float64,
+                                                                                     device=dev)
+    chi = (t(defocus_ang) * p ** 2 / 2 + t(c3_ang) * 1e7 * p ** 4 / 4 + t(c5_ang) * 1e7 * p ** 6 / 6)
+    phi = torch.atan2(ly, lx)
+    chi = chi + p ** 2 / 2 * (t(a1x_ang) * torch.cos(2 * phi) + t(a1y_ang) * torch.sin(2 * phi))
+    chi = 2 * math.pi * chi / lam
+    a = torch.polar(mask, -chi).to(torch.complex64)
+    probe = _Fft2Fn.apply(a, True)
+    return torch.roll(probe, shifts=(n // 2, n // 2), dims=(0, 1))

@@ -16,7 +16,7 @@ ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 LIB = os.path.join(PKG, "libptyro_b200.so")
 SOURCES = ["ms_engine.cu", "diag.cu", "ms_static.cu"] + [f"pass_{n}.cu" for n in (16, 32, 64, 128, 256, 512, 1024)]
-HEADERS = ["fft_core.cuh", "ms_pass.cuh", "pass_launch.cuh"]
+HEADERS = ["fft_core.cuh", "ms_pass.cuh", "ms_bwd.cuh", "pass_launch.cuh"]
 
 NVCC_FLAGS = [
     "-O3", "-std=c++17", "-lineinfo",

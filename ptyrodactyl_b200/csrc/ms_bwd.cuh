@@ -1,0 +1,235 @@
+// Adjoint pass of the multislice engine (reverse-mode gradient).
+//
+// Forward, per probe and mode: phi_s = psi_s T_s, psi_{s+1} = U phi_s with
+// U = ifft2 diag(P) fft2 (unitary), A = fft2(phi_{S-1}), I = sum_m w_m |A_m|^2
+// (stored fftshifted). With g = dL/dI and lam = dL/dconj(.):
+//   lam_A          = N^2 w_m ifftshift(g) A          (so lam_phi_{S-1} = ifft2(lam_A))
+//   dL/dV_s        = 2 sigma Im(conj(phi_s) lam_phi_s)
+//   lam_phi_{s-1}  = U^H (conj(T_s) lam_phi_s)
+//   phi_{s-1}      = U^H (conj(T_s) phi_s)            (the forward run backwards)
+// The adjoint and the reconstructed forward wave obey the same operator, so one
+// pass carries both waves of a line through it in lockstep; at each slice point
+// the pair is in registers and the pass emits the per-pixel dV contribution. The
+// reconstructed wave is replaced by the checkpoint stored in the forward where one
+// exists, which bounds the rounding drift of running U backwards. Passes follow
+// the forward's schedule: op'_0 = IFFT2, op'_j = U^H, op'_S = FFT2 (adjoint only).
+#pragma once
+#include "ms_pass.cuh"
+
+namespace ptyro {
+
+struct BwdArgs {
+  float2* psi;             // reconstructed forward wave slots (B*M planes)
+  float2* lam;             // adjoint slots
+  const float2* amp;       // init: far-field amplitude residual of slot w at amp + w * res_stride
+  const float* gpat;       // init: upstream dL/dI (B, N, N), fftshifted like the patterns
+  const float* weights;    // (M)
+  const float2* ckpt;      // checkpoint plane of this pass's slice point (slot stride res_stride), or null
+  size_t res_stride;
+  const float2* trans;     // (S, N, N) T, row-major
+  const float2* trans_t;   // transposed
+  const float2* pf;        // (N) propagator factor / N (conjugated in use)
+  const float2* tw;        // (N) forward twiddles
+  const float2* ramp_y;    // (B, N) shift ramps (beam-gradient epilogue)
+  const float2* ramp_x;
+  float* contrib;          // (B*M, N, N) row-major dV contribution of this pass's slice point, or null
+  int n_modes;
+  int init;                // 1: psi <- amp, lam <- N^2 w g amp (k-order loads), op1 must be OP_IFFT
+  int op1, t_slice, op2;   // op1 on both waves; T point (conj T) ; op2 on lam (and psi unless psi_done)
+  int psi_done;            // the forward wave is not needed after this pass's slice point
+  int beam_epi;            // op2 / op1 ends in k-order: multiply lam by conj(ramp along this axis)
+  float sigma2;            // 2 sigma
+  float scale;             // 1/N after OP_IFFT
+};
+
+template <int N1, int N2, int AXIS>
+__device__ __forceinline__ void bwd_load(const BwdArgs& a, const float2* w, float2 (&v)[N2], bool korder, int t,
+                                         int line, int lc, float2* work, int line0, int pitch) {
+  constexpr int N = N1 * N2;
+  if (AXIS == 0) {
+    if (korder) {
+#pragma unroll
+      for (int r = 0; r < N2; ++r) v[r] = w[(size_t)line * N + korder_index<N1, N2>(t, r)];
+    } else {
+#pragma unroll
+      for (int j = 0; j < N2; ++j) v[j] = w[(size_t)line * N + t + N1 * j];
+    }
+  } else {
+    (void)line;
+    if (korder) {
+#pragma unroll
+      for (int r = 0; r < N2; ++r) v[r] = work[korder_index<N1, N2>(t, r) * pitch + lc];
+    } else {
+#pragma unroll
+      for (int j = 0; j < N2; ++j) v[j] = work[(t + N1 * j) * pitch + lc];
+    }
+  }
+}
+
+template <int N1, int N2, int AXIS, int WARPS, int MINB>
+__global__ void __launch_bounds__(WARPS * 32, MINB) ms_bwd_pass_kernel(BwdArgs a) {
+  using Geo = PassGeom<N1, N2>;
+  using LB = LineBuf<N1, N2>;
+  constexpr int N = Geo::N;
+  constexpr int G = Geo::G;
+  constexpr int lines = WARPS * G;
+  static_assert(N % lines == 0, "lines per CTA must divide N");
+  constexpr int pitch = lines + G;
+  extern __shared__ float2 smem[];
+  float2* tw = smem;
+  float2* work = smem + N;
+  for (int i = threadIdx.x; i < N; i += blockDim.x) {
+    const int k2 = i / N1, tt = i % N1;
+    tw[i] = a.tw[(tt * k2) % N];
+  }
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int t = AXIS == 0 ? (lane % N1) : (lane / G);
+  const int gl = AXIS == 0 ? (lane / N1) : (lane % G);
+  const int lc = warp * G + gl;
+  const int line0 = blockIdx.x * lines;
+  const int line = line0 + lc;
+  float2* buf = work + lc * LB::kSize;
+  const size_t NN = (size_t)N * N;
+  const int slot = blockIdx.y;
+  const int b = slot / a.n_modes, m = slot % a.n_modes;
+  auto off = [&](int e) -> size_t { return AXIS == 0 ? (size_t)line * N + e : (size_t)e * N + line; };
+
+  float2* Wp = a.psi + (size_t)slot * NN;
+  float2* Wl = a.lam + (size_t)slot * NN;
+  const bool korder_in = a.init || a.op1 == OP_IFFT;
+  float2 p[N2], l[N2];
+
+  // ---- load both waves (column passes stage each through the tile in turn)
+  if (a.init) {
+    // row pass over k-space: psi = A, lam = N^2 w_m g(shifted) A
+    const float2* A = a.amp + (size_t)slot * a.res_stride;
+    const float* g = a.gpat + (size_t)b * NN;
+    const float s = (float)N * (float)N * a.weights[m];
+    const int ks_line = (line + N / 2) % N;
+#pragma unroll
+    for (int r = 0; r < N2; ++r) {
+      const int k = korder_index<N1, N2>(t, r);
+      const float2 av = A[off(k)];
+      const float gv = AXIS == 0 ? g[(size_t)ks_line * N + (k + N / 2) % N] : g[(size_t)((k + N / 2) % N) * N + ks_line];
+      p[r] = av;
+      l[r] = cscale(av, s * gv);
+    }
+  } else if (AXIS == 0) {
+    if (a.op1 != OP_FFT) bwd_load<N1, N2, AXIS>(a, Wp, p, korder_in, t, line, lc, work, line0, pitch);
+    bwd_load<N1, N2, AXIS>(a, Wl, l, korder_in, t, line, lc, work, line0, pitch);
+  } else {
+    for (int wv = a.op1 == OP_FFT ? 1 : 0; wv < 2; ++wv) {
+      const float2* W = wv == 0 ? Wp : Wl;
+      __syncthreads();
+      tile_load<N, lines, pitch, WARPS * 32>(W, work, line0);
+      __syncthreads();
+      if (wv == 0) bwd_load<N1, N2, AXIS>(a, W, p, korder_in, t, line, lc, work, line0, pitch);
+      else bwd_load<N1, N2, AXIS>(a, W, l, korder_in, t, line, lc, work, line0, pitch);
+    }
+    __syncthreads();
+  }
+
+  // ---- op1 on both
+  if (a.op1 == OP_IFFT) {
+    line_k_to_nat<N1, N2, +1>(p, t, buf, tw);
+    line_k_to_nat<N1, N2, +1>(l, t, buf, tw);
+#pragma unroll
+    for (int j = 0; j < N2; ++j) {
+      p[j] = cscale(p[j], a.scale);
+      l[j] = cscale(l[j], a.scale);
+    }
+  } else if (a.op1 == OP_CONV_CONJ) {
+    apply_op<N1, N2>(OP_CONV_CONJ, p, t, buf, tw, a.pf);
+    apply_op<N1, N2>(OP_CONV_CONJ, l, t, buf, tw, a.pf);
+  } else if (a.op1 == OP_FFT) {
+    apply_op<N1, N2>(OP_FFT, l, t, buf, tw, a.pf);
+  }
+
+  // ---- slice point: checkpoint refresh, dV contribution, conj(T)
+  float cv[N2];
+  if (a.t_slice >= 0) {
+    if (a.ckpt) {
+      const float2* ck = a.ckpt + (size_t)slot * a.res_stride;
+#pragma unroll
+      for (int j = 0; j < N2; ++j) p[j] = ck[off(t + N1 * j)];
+    }
+#pragma unroll
+    for (int j = 0; j < N2; ++j) cv[j] = a.sigma2 * (p[j].x * l[j].y - p[j].y * l[j].x);
+    const float2* T = (AXIS == 0 ? a.trans : a.trans_t) + (size_t)a.t_slice * NN + (size_t)line * N;
+#pragma unroll
+    for (int j = 0; j < N2; ++j) {
+      const float2 tv = __ldg(T + t + N1 * j);
+      p[j] = cmulc(p[j], tv);
+      l[j] = cmulc(l[j], tv);
+    }
+  }
+
+  // ---- op2
+  bool lam_k = a.op1 == OP_FFT;
+  if (a.op2 == OP_CONV_CONJ) {
+    if (!a.psi_done) apply_op<N1, N2>(OP_CONV_CONJ, p, t, buf, tw, a.pf);
+    apply_op<N1, N2>(OP_CONV_CONJ, l, t, buf, tw, a.pf);
+  } else if (a.op2 == OP_FFT) {
+    apply_op<N1, N2>(OP_FFT, l, t, buf, tw, a.pf);
+    lam_k = true;
+  }
+  if (a.beam_epi) {
+    // lam is k-order along this axis: multiply conj(ramp(k)) of this axis
+    const float2* ra = (AXIS == 0 ? a.ramp_x : a.ramp_y) + (size_t)b * N;
+#pragma unroll
+    for (int r = 0; r < N2; ++r) l[r] = cmulc(l[r], ra[korder_index<N1, N2>(t, r)]);
+  }
+
+  // ---- store
+  const bool store_psi = !a.psi_done && a.op1 != OP_FFT;
+  if (AXIS == 0) {
+    if (store_psi) {
+#pragma unroll
+      for (int j = 0; j < N2; ++j) Wp[off(t + N1 * j)] = p[j];
+    }
+    if (lam_k) {
+#pragma unroll
+      for (int r = 0; r < N2; ++r) Wl[off(korder_index<N1, N2>(t, r))] = l[r];
+    } else {
+#pragma unroll
+      for (int j = 0; j < N2; ++j) Wl[off(t + N1 * j)] = l[j];
+    }
+    if (a.t_slice >= 0 && a.contrib) {
+      float* C = a.contrib + (size_t)slot * NN;
+#pragma unroll
+      for (int j = 0; j < N2; ++j) C[off(t + N1 * j)] = cv[j];
+    }
+  } else {
+    for (int wv = 0; wv < 3; ++wv) {
+      if (wv == 0 && !store_psi) continue;
+      if (wv == 2 && !(a.t_slice >= 0 && a.contrib)) continue;
+      __syncthreads();
+      if (wv == 0) {
+#pragma unroll
+        for (int j = 0; j < N2; ++j) work[(t + N1 * j) * pitch + lc] = p[j];
+      } else if (wv == 1) {
+        if (lam_k) {
+#pragma unroll
+          for (int r = 0; r < N2; ++r) work[korder_index<N1, N2>(t, r) * pitch + lc] = l[r];
+        } else {
+#pragma unroll
+          for (int j = 0; j < N2; ++j) work[(t + N1 * j) * pitch + lc] = l[j];
+        }
+      } else {
+        float* tile = reinterpret_cast<float*>(work);
+#pragma unroll
+        for (int j = 0; j < N2; ++j) tile[(t + N1 * j) * pitch + lc] = cv[j];
+      }
+      __syncthreads();
+      if (wv < 2) {
+        tile_store<N, lines, pitch, WARPS * 32>(wv == 0 ? Wp : Wl, work, line0);
+      } else {
+        tile_store<N, lines, pitch, WARPS * 32>(a.contrib + (size_t)slot * NN,
+                                                reinterpret_cast<const float*>(work), line0);
+      }
+    }
+  }
+}
+
+}  // namespace ptyro

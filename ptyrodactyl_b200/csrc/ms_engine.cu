@@ -350,6 +350,260 @@ static int forward_setup(const ptyro_ms_params* p, const Layout& L, char* ws, co
   return fft2_planes(n, p->num_modes, false, pk, tw, st);
 }
 
+// Batched forward over all probes. With residuals != null (gradient mode) every
+// pass whose slice point s has s % ckpt_every == 0 also stores the wave after the
+// T multiply, and the pattern pass stores the complex far-field amplitude:
+// residual planes per (probe, mode) slot = ceil(S / ckpt_every) checkpoints + 1.
+static int forward_impl(const ptyro_ms_params* p, int ckpt_every, const float* potential, const float* modes,
+                        const float* weights, const double* positions, float* patterns, float2* residuals,
+                        void* workspace, size_t workspace_bytes, void* stream) {
+  int rc = validate(p);
+  if (rc) return rc;
+  if (p->num_probes == 0) return PTYRO_OK;
+  if (!potential || !modes || !weights || !positions || !patterns)
+    return fail(PTYRO_ERR_INVALID, "NULL array argument");
+  const Layout L = layout_for(p);
+  rc = check_workspace(L, workspace, workspace_bytes);
+  if (rc) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  char* ws = (char*)workspace;
+  rc = forward_setup(p, L, ws, potential, modes, st);
+  if (rc) return rc;
+  const int n = p->n, S = p->num_slices, M = p->num_modes;
+  const size_t nn = (size_t)n * n;
+  const int C = residuals ? (S + ckpt_every - 1) / ckpt_every : 0;
+  const size_t res_stride = (size_t)(C + 1) * nn;
+  float2* ry = (float2*)(ws + L.ramp_y);
+  float2* rx = (float2*)(ws + L.ramp_x);
+  PassArgs a = {};
+  a.wave = (float2*)(ws + L.waves);
+  a.probe_k = (const float2*)(ws + L.probe_k);
+  a.ramp_y = ry;
+  a.ramp_x = rx;
+  a.trans = (const float2*)(ws + L.trans);
+  a.trans_t = (const float2*)(ws + L.trans_t);
+  a.pf = (const float2*)(ws + L.pf);
+  a.tw = (const float2*)(ws + L.tw);
+  a.weights = weights;
+  a.n_modes = M;
+  a.scale = 1.0f / (float)n;
+  a.res_stride = res_stride;
+  for (int b0 = 0; b0 < p->num_probes; b0 += L.batch) {
+    const int nb = p->num_probes - b0 < L.batch ? p->num_probes - b0 : L.batch;
+    float2* res_base = residuals ? residuals + (size_t)b0 * M * res_stride : nullptr;
+    k_ramps<<<(nb * n + 255) / 256, 256, 0, st>>>(positions + 2 * (size_t)b0, nb, n, p->shift_calib_ang, ry, rx);
+    if ((rc = check_launch("k_ramps"))) return rc;
+    // pass 0: x part of the IFFT2 of the shifted probe spectrum
+    PassArgs q = a;
+    q.src = SRC_PROBE; q.op1 = OP_IFFT; q.t_slice = -1; q.op2 = OP_NONE; q.dst = DST_WAVE;
+    if ((rc = launch_pass(n, 0, q, nb * M, st, p->tune))) return rc;
+    for (int k = 1; k <= S; ++k) {
+      q = a;
+      q.src = SRC_WAVE;
+      q.op1 = k == 1 ? OP_IFFT : OP_CONV;
+      q.t_slice = k - 1;
+      q.op2 = k == S ? OP_FFT : OP_CONV;
+      q.dst = DST_WAVE;
+      if (res_base && (k - 1) % ckpt_every == 0) q.ckpt_store = res_base + (size_t)((k - 1) / ckpt_every) * nn;
+      if ((rc = launch_pass(n, k % 2, q, nb * M, st, p->tune))) return rc;
+    }
+    q = a;
+    q.src = SRC_WAVE; q.op1 = OP_FFT; q.t_slice = -1; q.op2 = OP_NONE; q.dst = DST_PATTERN;
+    q.pattern = patterns + (size_t)b0 * nn;
+    if (res_base) q.amp_store = res_base + (size_t)C * nn;
+    if ((rc = launch_pass(n, (S + 1) % 2, q, nb, st, p->tune))) return rc;
+  }
+  return PTYRO_OK;
+}
+
+// ---------------------------------------------------------------- gradient
+__global__ void k_zero_pot(float* dv, long long sy, long long sx, long long ss, int n, int S) {
+  const size_t total = (size_t)S * n * n;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+    const int s = (int)(i / ((size_t)n * n)), y = (int)((i / n) % n), x = (int)(i % n);
+    dv[(long long)y * sy + (long long)x * sx + (long long)s * ss] = 0.f;
+  }
+}
+
+__global__ void k_zero2(float2* d, size_t count) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += (size_t)gridDim.x * blockDim.x)
+    d[i] = make_float2(0.f, 0.f);
+}
+
+// dV_s += sum over slots of the per-slot contributions, in slot order (deterministic).
+__global__ void k_reduce_dv(const float* __restrict__ contrib, int nslots, int n, float* dv, long long sy,
+                            long long sx, long long ss, int s) {
+  const size_t nn = (size_t)n * n;
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nn) return;
+  float acc = 0.f;
+  for (int w = 0; w < nslots; ++w) acc += contrib[(size_t)w * nn + i];
+  const int y = (int)(i / n), x = (int)(i % n);
+  dv[(long long)y * sy + (long long)x * sx + (long long)s * ss] += acc;
+}
+
+// beam spectrum gradient: acc[m] += sum_b lam[b*M + m], in probe order.
+__global__ void k_reduce_beam(const float2* __restrict__ lam, int nb, int M, int n, float2* acc) {
+  const size_t nn = (size_t)n * n;
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nn * M) return;
+  const int m = (int)(i / nn);
+  const size_t px = i % nn;
+  float2 s = acc[i];
+  for (int b = 0; b < nb; ++b) s = cadd(s, lam[((size_t)b * M + m) * nn + px]);
+  acc[i] = s;
+}
+
+// JAX's gradient convention for a complex input of a real loss: conj(2 dL/dconj(z)).
+__global__ void k_write_grad_modes(const float2* __restrict__ lam_beam, int n, int M, float2* out, long long sy,
+                                   long long sx, long long sm) {
+  const size_t nn = (size_t)n * n;
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nn * M) return;
+  const int m = (int)(i / nn), y = (int)((i % nn) / n), x = (int)(i % n);
+  const float2 v = lam_beam[i];
+  out[(long long)y * sy + (long long)x * sx + (long long)m * sm] = make_float2(2.f * v.x, -2.f * v.y);
+}
+
+struct BwdLayout {
+  size_t tw, pf, trans, trans_t, ramp_y, ramp_x, psi, lam, contrib, beam, total;
+  int batch;
+};
+
+static BwdLayout bwd_layout_for(const ptyro_ms_params* p) {
+  BwdLayout L = {};
+  const size_t nn = (size_t)p->n * p->n;
+  if (p->batch > 0) {
+    L.batch = p->batch < p->num_probes ? p->batch : (p->num_probes > 0 ? p->num_probes : 1);
+  } else {
+    // the two wave sets of a batch (forward + adjoint) near 64 MB: L2-resident
+    int b = (int)(32.0 * 1024 * 1024 / (8.0 * nn * p->num_modes));
+    if (b < 1) b = 1;
+    L.batch = b > p->num_probes ? (p->num_probes > 0 ? p->num_probes : 1) : b;
+  }
+  const size_t slots = (size_t)L.batch * p->num_modes;
+  size_t o = 0;
+  L.tw = o; o = align_up(o + 8 * (size_t)p->n);
+  L.pf = o; o = align_up(o + 8 * (size_t)p->n);
+  L.trans = o; o = align_up(o + 8 * nn * p->num_slices);
+  L.trans_t = o; o = align_up(o + 8 * nn * p->num_slices);
+  L.ramp_y = o; o = align_up(o + 8 * (size_t)p->n * L.batch);
+  L.ramp_x = o; o = align_up(o + 8 * (size_t)p->n * L.batch);
+  L.psi = o; o = align_up(o + 8 * nn * slots);
+  L.lam = o; o = align_up(o + 8 * nn * slots);
+  L.contrib = o; o = align_up(o + 4 * nn * slots);
+  L.beam = o; o = align_up(o + 8 * nn * p->num_modes);
+  L.total = o;
+  return L;
+}
+
+static int launch_bwd(int n, int axis, const BwdArgs& a, int grid_y, cudaStream_t st) {
+  if (grid_y <= 0) return PTYRO_OK;
+  int rc;
+  switch (n) {
+    case 16: rc = launch_bwd_16(axis, a, grid_y, st); break;
+    case 32: rc = launch_bwd_32(axis, a, grid_y, st); break;
+    case 64: rc = launch_bwd_64(axis, a, grid_y, st); break;
+    case 128: rc = launch_bwd_128(axis, a, grid_y, st); break;
+    case 256: rc = launch_bwd_256(axis, a, grid_y, st); break;
+    case 512: rc = launch_bwd_512(axis, a, grid_y, st); break;
+    case 1024: rc = launch_bwd_1024(axis, a, grid_y, st); break;
+    default: return fail(PTYRO_ERR_UNSUPPORTED, "grid edge not compiled");
+  }
+  if (rc != 0) return fail(PTYRO_ERR_CUDA, std::string("ms_bwd_pass_kernel: ") + cudaGetErrorString((cudaError_t)rc));
+  return PTYRO_OK;
+}
+
+static int backward_impl(const ptyro_ms_params* p, int ckpt_every, const float* potential, const float* weights,
+                         const double* positions, const float2* residuals, const float* grad_patterns,
+                         float* grad_potential, float* grad_modes, void* workspace, size_t workspace_bytes,
+                         void* stream) {
+  int rc = validate(p);
+  if (rc) return rc;
+  if (ckpt_every < 1) return fail(PTYRO_ERR_INVALID, "ckpt_every must be >= 1");
+  if (!potential || !weights || !positions || !residuals || !grad_patterns || !grad_potential || !grad_modes)
+    return fail(PTYRO_ERR_INVALID, "NULL array argument");
+  const BwdLayout L = bwd_layout_for(p);
+  if (!workspace) return fail(PTYRO_ERR_WORKSPACE, "workspace is NULL");
+  if (((uintptr_t)workspace & 255) != 0) return fail(PTYRO_ERR_WORKSPACE, "workspace must be 256-byte aligned");
+  if (workspace_bytes < L.total)
+    return fail(PTYRO_ERR_WORKSPACE, "workspace too small: need " + std::to_string(L.total) + " bytes, got " +
+                                         std::to_string(workspace_bytes));
+  cudaStream_t st = (cudaStream_t)stream;
+  char* ws = (char*)workspace;
+  const int n = p->n, S = p->num_slices, M = p->num_modes;
+  const size_t nn = (size_t)n * n;
+  const int C = (S + ckpt_every - 1) / ckpt_every;
+  const size_t res_stride = (size_t)(C + 1) * nn;
+  const double lam = wavelength_ang(p->voltage_kv);
+  float2* tw = (float2*)(ws + L.tw);
+  float2* beam = (float2*)(ws + L.beam);
+  k_twiddle<<<(n + 255) / 256, 256, 0, st>>>(n, tw);
+  k_propagator<<<(n + 255) / 256, 256, 0, st>>>(n, p->calib_ang, lam * p->slice_thickness_ang, 1.0 / n,
+                                                (float2*)(ws + L.pf));
+  k_transmission<<<blocks_for(nn * S, 256), 256, 0, st>>>(potential, p->pot_stride_y, p->pot_stride_x,
+                                                          p->pot_stride_s, n, S, interaction_sigma(p->voltage_kv),
+                                                          (float2*)(ws + L.trans), (float2*)(ws + L.trans_t));
+  k_zero_pot<<<blocks_for(nn * S, 256), 256, 0, st>>>(grad_potential, p->pot_stride_y, p->pot_stride_x,
+                                                      p->pot_stride_s, n, S);
+  k_zero2<<<blocks_for(nn * M, 256), 256, 0, st>>>(beam, nn * M);
+  if ((rc = check_launch("backward setup", 5))) return rc;
+  BwdArgs a = {};
+  a.psi = (float2*)(ws + L.psi);
+  a.lam = (float2*)(ws + L.lam);
+  a.weights = weights;
+  a.res_stride = res_stride;
+  a.trans = (const float2*)(ws + L.trans);
+  a.trans_t = (const float2*)(ws + L.trans_t);
+  a.pf = (const float2*)(ws + L.pf);
+  a.tw = tw;
+  a.ramp_y = (const float2*)(ws + L.ramp_y);
+  a.ramp_x = (const float2*)(ws + L.ramp_x);
+  a.n_modes = M;
+  a.sigma2 = (float)(2.0 * interaction_sigma(p->voltage_kv));
+  a.scale = 1.0f / (float)n;
+  float* contrib = (float*)(ws + L.contrib);
+  for (int b0 = 0; b0 < p->num_probes; b0 += L.batch) {
+    const int nb = p->num_probes - b0 < L.batch ? p->num_probes - b0 : L.batch;
+    const float2* res_base = residuals + (size_t)b0 * M * res_stride;
+    k_ramps<<<(nb * n + 255) / 256, 256, 0, st>>>(positions + 2 * (size_t)b0, nb, n, p->shift_calib_ang,
+                                                  (float2*)(ws + L.ramp_y), (float2*)(ws + L.ramp_x));
+    if ((rc = check_launch("k_ramps"))) return rc;
+    BwdArgs q = a;
+    q.init = 1;
+    q.amp = res_base + (size_t)C * nn;
+    q.gpat = grad_patterns + (size_t)b0 * nn;
+    q.op1 = OP_IFFT; q.t_slice = -1; q.op2 = OP_NONE;
+    if ((rc = launch_bwd(n, 0, q, nb * M, st))) return rc;
+    for (int k = 1; k <= S; ++k) {
+      const int s = S - k;
+      q = a;
+      q.op1 = k == 1 ? OP_IFFT : OP_CONV_CONJ;
+      q.t_slice = s;
+      q.ckpt = (s % ckpt_every == 0) ? res_base + (size_t)(s / ckpt_every) * nn : nullptr;
+      q.contrib = contrib;
+      q.op2 = k == S ? OP_FFT : OP_CONV_CONJ;
+      q.psi_done = k == S;
+      q.beam_epi = k == S;
+      if ((rc = launch_bwd(n, k % 2, q, nb * M, st))) return rc;
+      k_reduce_dv<<<(unsigned)((nn + 255) / 256), 256, 0, st>>>(contrib, nb * M, n, grad_potential, p->pot_stride_y,
+                                                                 p->pot_stride_x, p->pot_stride_s, s);
+      if ((rc = check_launch("k_reduce_dv"))) return rc;
+    }
+    q = a;
+    q.op1 = OP_FFT; q.t_slice = -1; q.op2 = OP_NONE; q.psi_done = 1; q.beam_epi = 1;
+    if ((rc = launch_bwd(n, (S + 1) % 2, q, nb * M, st))) return rc;
+    k_reduce_beam<<<(unsigned)((nn * M + 255) / 256), 256, 0, st>>>(a.lam, nb, M, n, beam);
+    if ((rc = check_launch("k_reduce_beam"))) return rc;
+  }
+  // beam = ifft2(sum_p conj(R_p) fft2(lam_psi0_p)); gradient = conj(2 beam)
+  if ((rc = fft2_planes(n, M, true, beam, tw, st))) return rc;
+  k_write_grad_modes<<<(unsigned)((nn * M + 255) / 256), 256, 0, st>>>(beam, n, M, (float2*)grad_modes,
+                                                                       p->mode_stride_y, p->mode_stride_x,
+                                                                       p->mode_stride_m);
+  return check_launch("k_write_grad_modes");
+}
+
 }  // namespace ptyro
 
 using namespace ptyro;
@@ -368,57 +622,36 @@ size_t ptyro_ms_workspace_bytes(const ptyro_ms_params* p) {
 int ptyro_ms_forward(const ptyro_ms_params* p, const float* potential, const float* modes,
                      const float* weights, const double* positions, float* patterns, void* workspace,
                      size_t workspace_bytes, void* stream) {
-  int rc = validate(p);
-  if (rc) return rc;
-  if (p->num_probes == 0) return PTYRO_OK;
-  if (!potential || !modes || !weights || !positions || !patterns)
-    return fail(PTYRO_ERR_INVALID, "NULL array argument");
-  const Layout L = layout_for(p);
-  rc = check_workspace(L, workspace, workspace_bytes);
-  if (rc) return rc;
-  cudaStream_t st = (cudaStream_t)stream;
-  char* ws = (char*)workspace;
-  rc = forward_setup(p, L, ws, potential, modes, st);
-  if (rc) return rc;
-  const int n = p->n, S = p->num_slices, M = p->num_modes;
-  const size_t nn = (size_t)n * n;
-  float2* ry = (float2*)(ws + L.ramp_y);
-  float2* rx = (float2*)(ws + L.ramp_x);
-  PassArgs a = {};
-  a.wave = (float2*)(ws + L.waves);
-  a.probe_k = (const float2*)(ws + L.probe_k);
-  a.ramp_y = ry;
-  a.ramp_x = rx;
-  a.trans = (const float2*)(ws + L.trans);
-  a.trans_t = (const float2*)(ws + L.trans_t);
-  a.pf = (const float2*)(ws + L.pf);
-  a.tw = (const float2*)(ws + L.tw);
-  a.weights = weights;
-  a.n_modes = M;
-  a.scale = 1.0f / (float)n;
-  for (int b0 = 0; b0 < p->num_probes; b0 += L.batch) {
-    const int nb = p->num_probes - b0 < L.batch ? p->num_probes - b0 : L.batch;
-    k_ramps<<<(nb * n + 255) / 256, 256, 0, st>>>(positions + 2 * (size_t)b0, nb, n, p->shift_calib_ang, ry, rx);
-    if ((rc = check_launch("k_ramps"))) return rc;
-    // pass 0: x part of the IFFT2 of the shifted probe spectrum
-    PassArgs q = a;
-    q.src = SRC_PROBE; q.op1 = OP_IFFT; q.t_slice = -1; q.op2 = OP_NONE; q.dst = DST_WAVE;
-    if ((rc = launch_pass(n, 0, q, nb * M, st, p->tune))) return rc;
-    for (int k = 1; k <= S; ++k) {
-      q = a;
-      q.src = SRC_WAVE;
-      q.op1 = k == 1 ? OP_IFFT : OP_CONV;
-      q.t_slice = k - 1;
-      q.op2 = k == S ? OP_FFT : OP_CONV;
-      q.dst = DST_WAVE;
-      if ((rc = launch_pass(n, k % 2, q, nb * M, st, p->tune))) return rc;
-    }
-    q = a;
-    q.src = SRC_WAVE; q.op1 = OP_FFT; q.t_slice = -1; q.op2 = OP_NONE; q.dst = DST_PATTERN;
-    q.pattern = patterns + (size_t)b0 * nn;
-    if ((rc = launch_pass(n, (S + 1) % 2, q, nb, st, p->tune))) return rc;
-  }
-  return PTYRO_OK;
+  return forward_impl(p, 0, potential, modes, weights, positions, patterns, nullptr, workspace, workspace_bytes,
+                      stream);
+}
+
+size_t ptyro_ms_residual_bytes(const ptyro_ms_params* p, int32_t ckpt_every) {
+  if (validate(p) || ckpt_every < 1) return 0;
+  const int C = (p->num_slices + ckpt_every - 1) / ckpt_every;
+  return 8 * (size_t)p->n * p->n * (size_t)(C + 1) * p->num_modes * (size_t)p->num_probes;
+}
+
+size_t ptyro_ms_backward_workspace_bytes(const ptyro_ms_params* p) {
+  if (validate(p)) return 0;
+  return bwd_layout_for(p).total;
+}
+
+int ptyro_ms_forward_ckpt(const ptyro_ms_params* p, int32_t ckpt_every, const float* potential, const float* modes,
+                          const float* weights, const double* positions, float* patterns, float* residuals,
+                          void* workspace, size_t workspace_bytes, void* stream) {
+  if (ckpt_every < 1) return fail(PTYRO_ERR_INVALID, "ckpt_every must be >= 1");
+  if (!residuals && p && p->num_probes > 0) return fail(PTYRO_ERR_INVALID, "residuals is NULL");
+  return forward_impl(p, ckpt_every, potential, modes, weights, positions, patterns, (float2*)residuals, workspace,
+                      workspace_bytes, stream);
+}
+
+int ptyro_ms_backward(const ptyro_ms_params* p, int32_t ckpt_every, const float* potential, const float* weights,
+                      const double* positions, const float* residuals, const float* grad_patterns,
+                      float* grad_potential, float* grad_modes, void* workspace, size_t workspace_bytes,
+                      void* stream) {
+  return backward_impl(p, ckpt_every, potential, weights, positions, (const float2*)residuals, grad_patterns,
+                       grad_potential, grad_modes, workspace, workspace_bytes, stream);
 }
 
 int ptyro_ms_forward_plain(const ptyro_ms_params* p, const float* potential, const float* modes,

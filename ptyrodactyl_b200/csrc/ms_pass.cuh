@@ -39,6 +39,13 @@ struct PassArgs {
   int src, op1, t_slice, op2, dst;
   int t_conj;              // multiply by conj(T) instead of T
   float scale;             // factor applied after op1 == OP_IFFT
+  // gradient-mode residuals (null when not recording): the wave right after the
+  // T multiply is stored to ckpt_store (checkpoint plane), and a pattern pass stores
+  // the complex far-field amplitude (unshifted, both axes transformed) to amp_store.
+  // Plane of slot w: base + w * res_stride.
+  float2* ckpt_store;
+  float2* amp_store;
+  size_t res_stride;
 };
 
 template <int N1, int N2>
@@ -58,6 +65,40 @@ struct PassGeom {
     return sizeof(float2) * ((size_t)N + (xbuf > tile ? xbuf : tile));
   }
 };
+
+// Column passes: copy the CTA's block of LINES columns (all N rows) between a plane
+// in global memory and the shared staging tile (row pitch PITCH float2). Global
+// accesses move LINES consecutive elements per row; loads keep up to 8 per thread
+// in flight.
+template <int N, int LINES, int PITCH, int THREADS, typename T2>
+__device__ __forceinline__ void tile_load(const T2* __restrict__ W, T2* work, int line0) {
+  constexpr int kIters = N * LINES / THREADS;
+  constexpr int kChunk = kIters < 8 ? kIters : 8;
+#pragma unroll 1
+  for (int c0 = 0; c0 < kIters; c0 += kChunk) {
+    T2 stage[kChunk];
+#pragma unroll
+    for (int u = 0; u < kChunk; ++u) {
+      const int i = threadIdx.x + (c0 + u) * THREADS;
+      stage[u] = W[(size_t)(i / LINES) * N + line0 + i % LINES];
+    }
+#pragma unroll
+    for (int u = 0; u < kChunk; ++u) {
+      const int i = threadIdx.x + (c0 + u) * THREADS;
+      work[(i / LINES) * PITCH + i % LINES] = stage[u];
+    }
+  }
+}
+
+template <int N, int LINES, int PITCH, int THREADS, typename T2>
+__device__ __forceinline__ void tile_store(T2* __restrict__ W, const T2* work, int line0) {
+  constexpr int kIters = N * LINES / THREADS;
+#pragma unroll 8
+  for (int it = 0; it < kIters; ++it) {
+    const int i = threadIdx.x + it * THREADS;
+    W[(size_t)(i / LINES) * N + line0 + i % LINES] = work[(i / LINES) * PITCH + i % LINES];
+  }
+}
 
 // op on registers in natural distribution; returns true if the result is k-order.
 template <int N1, int N2>
@@ -144,21 +185,7 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) ms_pass_kernel(PassArgs a) {
       }
     } else {
       __syncthreads();  // the tile aliases other warps' exchange buffers
-      constexpr int kChunk = kTileIters < 8 ? kTileIters : 8;  // loads in flight per thread
-#pragma unroll 1
-      for (int c0 = 0; c0 < kTileIters; c0 += kChunk) {
-        float2 stage[kChunk];
-#pragma unroll
-        for (int u = 0; u < kChunk; ++u) {
-          const int i = threadIdx.x + (c0 + u) * WARPS * 32;
-          stage[u] = w[(size_t)(i / lines) * N + line0 + i % lines];
-        }
-#pragma unroll
-        for (int u = 0; u < kChunk; ++u) {
-          const int i = threadIdx.x + (c0 + u) * WARPS * 32;
-          work[(i / lines) * pitch + i % lines] = stage[u];
-        }
-      }
+      tile_load<N, lines, pitch, WARPS * 32>(w, work, line0);
       __syncthreads();
       if (load_k) {
 #pragma unroll
@@ -187,6 +214,11 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) ms_pass_kernel(PassArgs a) {
         const float2 tv = __ldg(T + t + N1 * j);
         v[j] = a.t_conj ? cmulc(v[j], tv) : cmul(v[j], tv);
       }
+      if (a.ckpt_store) {
+        float2* ck = a.ckpt_store + (size_t)slot * a.res_stride;
+#pragma unroll
+        for (int j = 0; j < N2; ++j) ck[off(t + N1 * j)] = v[j];
+      }
     }
     // ---- op2
     if (a.op2 != OP_NONE) korder = apply_op<N1, N2>(a.op2, v, t, buf, tw, a.pf);
@@ -195,6 +227,11 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) ms_pass_kernel(PassArgs a) {
       const float wm = a.weights[m];
 #pragma unroll
       for (int r = 0; r < N2; ++r) acc[r] = fmaf(wm, fmaf(v[r].x, v[r].x, v[r].y * v[r].y), acc[r]);
+      if (a.amp_store) {
+        float2* am = a.amp_store + (size_t)slot * a.res_stride;
+#pragma unroll
+        for (int r = 0; r < N2; ++r) am[off(korder_index<N1, N2>(t, r))] = v[r];
+      }
     } else if (AXIS == 0) {
       if (korder) {
 #pragma unroll
@@ -213,11 +250,7 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) ms_pass_kernel(PassArgs a) {
         for (int j = 0; j < N2; ++j) work[(t + N1 * j) * pitch + lc] = v[j];
       }
       __syncthreads();
-#pragma unroll 8
-      for (int it = 0; it < kTileIters; ++it) {
-        const int i = threadIdx.x + it * WARPS * 32;
-        w[(size_t)(i / lines) * N + line0 + i % lines] = work[(i / lines) * pitch + i % lines];
-      }
+      tile_store<N, lines, pitch, WARPS * 32>(w, work, line0);
     }
   }
   if (to_pattern) {

@@ -3,7 +3,7 @@
 #pragma once
 #include <atomic>
 
-#include "ms_pass.cuh"
+#include "ms_bwd.cuh"
 
 namespace ptyro {
 
@@ -28,6 +28,24 @@ int launch_pass_t(const PassArgs& a, int grid_y, cudaStream_t st) {
   return (int)cudaGetLastError();
 }
 
+template <int N1, int N2, int AXIS>
+int launch_bwd_t(const BwdArgs& a, int grid_y, cudaStream_t st) {
+  using Geo = PassGeom<N1, N2>;
+  constexpr int N = Geo::N;
+  constexpr int W = Geo::kWarps;
+  const size_t smem = Geo::smem_bytes(W);
+  static bool attr_done = false;
+  if (!attr_done) {
+    cudaFuncSetAttribute(ms_bwd_pass_kernel<N1, N2, AXIS, W, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)smem);
+    attr_done = true;
+  }
+  dim3 grid(N / Geo::kLines, grid_y);
+  ms_bwd_pass_kernel<N1, N2, AXIS, W, 1><<<grid, W * 32, smem, st>>>(a);
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  return (int)cudaGetLastError();
+}
+
 // variant bit (1 << axis) selects the 3-CTAs-per-SM register budget where the
 // shape allows it (N2 <= 16); otherwise 2 (N2 <= 16) or 1 (N2 = 32) CTAs per SM.
 #define PTYRO_DEFINE_PASS_LAUNCHER(NN, N1, N2)                                                   \
@@ -37,8 +55,18 @@ int launch_pass_t(const PassArgs& a, int grid_y, cudaStream_t st) {
     if (axis == 0)                                                                               \
       return occ ? launch_pass_t<N1, N2, 0, hi>(a, grid_y, st) : launch_pass_t<N1, N2, 0, lo>(a, grid_y, st); \
     return occ ? launch_pass_t<N1, N2, 1, hi>(a, grid_y, st) : launch_pass_t<N1, N2, 1, lo>(a, grid_y, st);   \
+  }                                                                                              \
+  int launch_bwd_##NN(int axis, const BwdArgs& a, int grid_y, cudaStream_t st) {                \
+    return axis == 0 ? launch_bwd_t<N1, N2, 0>(a, grid_y, st) : launch_bwd_t<N1, N2, 1>(a, grid_y, st); \
   }
 
+int launch_bwd_16(int axis, const BwdArgs& a, int grid_y, cudaStream_t st);
+int launch_bwd_32(int axis, const BwdArgs& a, int grid_y, cudaStream_t st);
+int launch_bwd_64(int axis, const BwdArgs& a, int grid_y, cudaStream_t st);
+int launch_bwd_128(int axis, const BwdArgs& a, int grid_y, cudaStream_t st);
+int launch_bwd_256(int axis, const BwdArgs& a, int grid_y, cudaStream_t st);
+int launch_bwd_512(int axis, const BwdArgs& a, int grid_y, cudaStream_t st);
+int launch_bwd_1024(int axis, const BwdArgs& a, int grid_y, cudaStream_t st);
 int launch_pass_16(int axis, const PassArgs& a, int grid_y, cudaStream_t st, int variant);
 int launch_pass_32(int axis, const PassArgs& a, int grid_y, cudaStream_t st, int variant);
 int launch_pass_64(int axis, const PassArgs& a, int grid_y, cudaStream_t st, int variant);

@@ -160,8 +160,14 @@ def stem_4d(pot_slice: PotentialSlices, beam: ProbeModes, microscope: Microscope
     modes, weights = _beam_on(beam, dev)
     positions = as_tensor(detector.scan_positions_px, torch.float64, dev).reshape(-1, 2).contiguous()
     calib = min(float(pot_slice.calib), float(beam.calib))
-    data = run_forward(slices, pot_slice.slice_thickness, modes, weights, positions,
-                       microscope.voltage_kv, calib, detector.real_space_calib_ang)
+    if torch.is_grad_enabled() and (slices.requires_grad or modes.requires_grad):
+        # differentiable path: checkpointed forward + hand-written adjoint kernel
+        from .autodiff import stem_4d_patterns
+        data = stem_4d_patterns(slices, modes, weights, positions, pot_slice.slice_thickness,
+                                microscope.voltage_kv, calib, detector.real_space_calib_ang)
+    else:
+        data = run_forward(slices, pot_slice.slice_thickness, modes, weights, positions,
+                           microscope.voltage_kv, calib, detector.real_space_calib_ang)
     fourier_calib = 1.0 / (modes.shape[0] * calib)
     scan_positions = detector.scan_positions_px.to(torch.float64) * detector.real_space_calib_ang
     return create_stem4d(data, detector.real_space_calib_ang, fourier_calib, scan_positions,
