@@ -378,6 +378,106 @@ def _ncu_traffic():
         return None
 
 
+# ----------------------------------------------------------------------------- gradient leg
+def run_grad(args, rank, world, local_rank):
+    """Ptychographic gradient at the 256^2-window / 512^2-field workload: time the plain
+    forward, the residual-recording forward and the adjoint; one JSON line."""
+    import torch
+    import ptyrodactyl_b200 as pb
+    from ptyrodactyl_b200 import _lib
+    from ptyrodactyl_b200.simulations import ms_params
+    from ptyrodactyl_b200.recon import amplitude_loss
+
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    lib = _lib.load()
+    w = synth.CONFIG4
+    n, S, P, F = w.n, w.num_slices, w.num_probes, w.field_n
+    win = torch.as_tensor(w.windows(), device=dev)
+    pos = torch.zeros((P, 2), dtype=torch.float64, device=dev)
+    mic = pb.create_microscope_config(w.voltage_kv, w.aperture_mrad, w.defocus_ang, w.c3_ang, probe_shape=(n, n))
+    probe = pb.make_probe(mic, pb.create_detector_config(w.calib))[..., None].contiguous()
+    wts = torch.ones(1, dtype=torch.float32, device=dev)
+    truth = torch.as_tensor(w.field(0), device=dev)
+    model = torch.as_tensor(w.field(1), device=dev)  # another frozen-phonon draw: the current estimate
+    clean = pb.run_forward(truth, synth.SLICE_DZ, probe, wts, pos, w.voltage_kv, w.calib, w.calib, windows=win)
+    rng = np.random.default_rng(w.seed)
+    targets = torch.as_tensor(synth.poisson_targets(clean.cpu().numpy().astype(np.float64), w.dose, rng),
+                              dtype=torch.float32, device=dev)
+    k = args.ckpt if args.ckpt > 0 else int(np.ceil(np.sqrt(S)))
+    prm = ms_params(n, S, 1, P, w.voltage_kv, synth.SLICE_DZ, w.calib, w.calib, model.stride(), probe.stride(),
+                    0, args.tune, F, win)
+    bprm = ms_params(n, S, 1, P, w.voltage_kv, synth.SLICE_DZ, w.calib, w.calib, model.stride(), probe.stride(),
+                     args.bwd_batch, 0, F, win)
+    ws_b = lib.ptyro_ms_workspace_bytes(ctypes.byref(prm))
+    ws = torch.empty(ws_b, dtype=torch.uint8, device=dev)
+    bws_b = lib.ptyro_ms_backward_workspace_bytes(ctypes.byref(bprm))
+    bws = torch.empty(bws_b, dtype=torch.uint8, device=dev)
+    res = torch.empty(lib.ptyro_ms_residual_bytes(ctypes.byref(prm), k) // 4, dtype=torch.float32, device=dev)
+    out = torch.empty((P, n, n), dtype=torch.float32, device=dev)
+    g_field = torch.empty_like(model)
+    g_modes = torch.empty_like(probe)
+    st = torch.cuda.current_stream(dev).cuda_stream
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
+
+    def fwd():
+        _lib.check(lib.ptyro_ms_forward(ctypes.byref(prm), model.data_ptr(), probe.data_ptr(), wts.data_ptr(),
+                                        pos.data_ptr(), out.data_ptr(), ws.data_ptr(), ws_b, st))
+
+    def fwd_ckpt():
+        _lib.check(lib.ptyro_ms_forward_ckpt(ctypes.byref(prm), k, model.data_ptr(), probe.data_ptr(),
+                                             wts.data_ptr(), pos.data_ptr(), out.data_ptr(), res.data_ptr(),
+                                             ws.data_ptr(), ws_b, st))
+
+    gbuf = {}
+
+    def loss_grad():
+        o = out.detach().requires_grad_(True)
+        loss = amplitude_loss(o, targets)
+        loss.backward()
+        gbuf["g"] = o.grad.contiguous()
+        gbuf["loss"] = loss.detach()
+
+    def bwd():
+        _lib.check(lib.ptyro_ms_backward(ctypes.byref(bprm), k, model.data_ptr(), wts.data_ptr(), pos.data_ptr(),
+                                         res.data_ptr(), gbuf["g"].data_ptr(), g_field.data_ptr(),
+                                         g_modes.data_ptr(), bws.data_ptr(), bws_b, st))
+
+    def timed(fn, reps):
+        ts = []
+        for _ in range(reps):
+            flush.zero_()
+            s, e = _events(torch, 2)
+            s.record()
+            fn()
+            e.record()
+            torch.cuda.synchronize()
+            ts.append(s.elapsed_time(e))
+        return statistics.median(ts)
+
+    for _ in range(args.warmup):
+        fwd(); fwd_ckpt(); loss_grad(); bwd()
+    torch.cuda.synchronize()
+    reps = max(3, args.steps // 4)
+    t_f = timed(fwd, reps)
+    t_fc = timed(fwd_ckpt, reps)
+    loss_grad()
+    t_b = timed(bwd, reps)
+    updates = float(P) * S
+    line = {
+        "metric": "ptychographic gradient: value+grad probe-slice updates/s (256^2 windows, 512^2 field)",
+        "value": updates / ((t_fc + t_b) * 1e-3), "unit": UNIT, "n_gpus": world, "mode": "grad",
+        "forward_ms": t_f, "forward_with_residuals_ms": t_fc, "adjoint_ms": t_b,
+        "adjoint_over_forward": t_b / t_f, "value_and_grad_over_forward": (t_fc + t_b) / t_f,
+        "loss": float(gbuf["loss"]), "dtype": "f32", "data": "synthetic",
+        "config": {"workload": w.name, "grid": n, "field": F, "slices": S, "probes": P, "ckpt_every": k,
+                   "residual_bytes": int(res.numel() * 4), "backward_batch": bprm.batch,
+                   "targets": f"Poisson noise at {w.dose:g} e- per pattern", "loss": "amplitude"},
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 # ----------------------------------------------------------------------------- reference arm
 def run_reference(args, rank):
     if rank != 0:
@@ -418,6 +518,9 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--mode", choices=("forward", "grad"), default="forward")
+    ap.add_argument("--ckpt", type=int, default=0, help="gradient mode: checkpoint spacing (0 = sqrt(S))")
+    ap.add_argument("--bwd-batch", type=int, default=0, help="gradient mode: probes per adjoint batch")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else max(args.warmup, 1)
     rank = int(os.environ.get("RANK", "0"))
@@ -433,7 +536,10 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                 device_id=torch.device("cuda", local_rank))
     try:
-        run_ours(args, rank, world, local_rank)
+        if args.mode == "grad":
+            run_grad(args, rank, world, local_rank)
+        else:
+            run_ours(args, rank, world, local_rank)
     finally:
         if world > 1:
             import torch.distributed as dist

@@ -43,12 +43,21 @@ typedef struct ptyro_ms_params {
   int32_t batch;               /* probes in flight per batch; 0 = automatic */
   int32_t tune;                /* kernel variant bits (0 = default): bit a selects the
                                   3-CTAs-per-SM register budget for passes along axis a */
+  int32_t field_n;             /* 0, or edge F of a larger periodic potential field (power of
+                                  two, n <= F <= 8192) from which every probe reads an n x n
+                                  window; the potential (and its gradient) is then F x F x S */
+  int32_t reserved;
   double voltage_kv;           /* MicroscopeConfig.voltage_kv */
   double slice_thickness_ang;  /* PotentialSlices.slice_thickness */
   double calib_ang;            /* min(PotentialSlices.calib, ProbeModes.calib): propagator grid */
   double shift_calib_ang;      /* DetectorConfig.real_space_calib_ang: shift-ramp grid */
   int64_t pot_stride_y, pot_stride_x, pot_stride_s;
   int64_t mode_stride_y, mode_stride_x, mode_stride_m;
+  const int32_t* windows;      /* DEVICE (P, 2) int32 (y, x) window origins in the field, or
+                                  NULL (all windows at 0); taken modulo F. The windowed run
+                                  stands in for the reference's tiled workflow, which crops a
+                                  tile of the sample around each position
+                                  (src/ptyrodactyl/workflows/stem_4d.py:553) */
 } ptyro_ms_params;
 
 /* Library version, major*10000 + minor*100 + patch. */

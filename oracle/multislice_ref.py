@@ -257,3 +257,37 @@ def aperture_count(voltage_kv, aperture_mrad, probe_shape, probe_calibration_pm)
     lam = relativistic_wavelength_ang(voltage_kv)
     q = probe_fourier_radius(probe_shape, probe_calibration_pm)
     return int(np.count_nonzero(q <= (aperture_mrad / 1000.0) / lam))
+
+
+def stem_4d_windowed(field, slice_thickness, pot_calib, beam_modes, weights, beam_calib, voltage_kv,
+                     scan_positions_px, real_space_calib_ang, windows, dtype=np.complex128):
+    """Probe p sees the n x n window of the periodic field (F, F, S) starting at
+    windows[p]; otherwise stem_4d. (The reference crops a tile per position in
+    workflows/stem_4d.py:553; here the crop is periodic.)"""
+    n = np.atleast_3d(beam_modes).shape[0]
+    pos = np.atleast_2d(np.asarray(scan_positions_px, np.float64))
+    out = np.empty((pos.shape[0], n, n), np.float64)
+    for i, (wy, wx) in enumerate(np.asarray(windows)):
+        win = np.roll(field, (-int(wy), -int(wx)), axis=(0, 1))[:n, :n]
+        out[i] = stem_4d(win, slice_thickness, pot_calib, beam_modes, weights, beam_calib, voltage_kv, pos[i:i + 1],
+                         real_space_calib_ang, dtype)["data"][0]
+    return out
+
+
+def stem_4d_windowed_vjp(field, slice_thickness, pot_calib, beam_modes, weights, beam_calib, voltage_kv,
+                         scan_positions_px, real_space_calib_ang, windows, g, dtype=np.complex128):
+    """(dL/dfield, dL/dbeam JAX convention) of stem_4d_windowed for dL/ddata = g."""
+    beam = np.atleast_3d(beam_modes)
+    n = beam.shape[0]
+    pos = np.atleast_2d(np.asarray(scan_positions_px, np.float64))
+    dfield = np.zeros(field.shape, np.float64)
+    dbeam = np.zeros(beam.shape, np.complex128)
+    for i, (wy, wx) in enumerate(np.asarray(windows)):
+        rolled = np.roll(field, (-int(wy), -int(wx)), axis=(0, 1))
+        dv, db = stem_4d_vjp(rolled[:n, :n], slice_thickness, pot_calib, beam, weights, beam_calib, voltage_kv,
+                             pos[i:i + 1], real_space_calib_ang, g[i:i + 1], dtype)
+        acc = np.zeros(field.shape, np.float64)
+        acc[:n, :n] = dv
+        dfield += np.roll(acc, (int(wy), int(wx)), axis=(0, 1))
+        dbeam += db
+    return dfield, dbeam

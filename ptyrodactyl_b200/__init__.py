@@ -28,6 +28,7 @@ from .simulations import (  # noqa: F401
     relativistic_wavelength_ang,
     run_forward,
     stem_4d,
+    stem_4d_windowed,
 )
 
 from .autodiff import Stem4dFunction, make_probe_differentiable, stem_4d_patterns, vjp  # noqa: F401

@@ -51,6 +51,8 @@ class MsParams(ctypes.Structure):
         ("num_probes", ctypes.c_int32),
         ("batch", ctypes.c_int32),
         ("tune", ctypes.c_int32),
+        ("field_n", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
         ("voltage_kv", ctypes.c_double),
         ("slice_thickness_ang", ctypes.c_double),
         ("calib_ang", ctypes.c_double),
@@ -61,6 +63,7 @@ class MsParams(ctypes.Structure):
         ("mode_stride_y", ctypes.c_int64),
         ("mode_stride_x", ctypes.c_int64),
         ("mode_stride_m", ctypes.c_int64),
+        ("windows", ctypes.c_void_p),
     ]
 
 

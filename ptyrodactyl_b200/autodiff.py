@@ -23,7 +23,7 @@ from typing import Optional
 import torch
 
 from . import _lib
-from .simulations import _check_edge, _stream_ptr, _workspace, ms_params, relativistic_wavelength_ang
+from .simulations import _check_edge, _stream_ptr, _workspace, check_windows, ms_params, relativistic_wavelength_ang
 
 DEFAULT_CKPT = 0  # 0: ceil(sqrt(S))
 
@@ -44,16 +44,15 @@ class Stem4dFunction(torch.autograd.Function):
 
     @staticmethod
     def forward(ctx, slices, modes, weights, positions, slice_thickness: float, voltage_kv: float,
-                calib_ang: float, shift_calib_ang: float, ckpt_every: int = 0, batch: int = 0, tune: int = 0):
+                calib_ang: float, shift_calib_ang: float, ckpt_every: int = 0, batch: int = 0, tune: int = 0,
+                windows=None):
         lib = _lib.load()
         dev = slices.device
-        n = _check_edge(slices.shape[0], slices.shape[1])
-        if tuple(modes.shape[:2]) != (n, n):
-            raise ValueError("beam modes and potential slices must share the grid shape")
         S, M, P = slices.shape[2], modes.shape[2], positions.shape[0]
+        n, f = check_windows(slices, modes, windows, P)
         k = _ckpt_for(S, ckpt_every)
         prm = ms_params(n, S, M, P, voltage_kv, slice_thickness, calib_ang, shift_calib_ang, slices.stride(),
-                        modes.stride(), batch, tune)
+                        modes.stride(), batch, tune, f, windows)
         out = torch.empty((P, n, n), dtype=torch.float32, device=dev)
         res = torch.empty(lib.ptyro_ms_residual_bytes(ctypes.byref(prm), k) // 4 if P else 1,
                           dtype=torch.float32, device=dev)
@@ -63,17 +62,17 @@ class Stem4dFunction(torch.autograd.Function):
             _lib.check(lib.ptyro_ms_forward_ckpt(ctypes.byref(prm), k, slices.data_ptr(), modes.data_ptr(),
                                                  weights.data_ptr(), positions.data_ptr(), out.data_ptr(),
                                                  res.data_ptr(), ws.data_ptr(), ws_bytes, _stream_ptr(dev)))
-        ctx.save_for_backward(slices, modes, weights, positions, res)
-        ctx.cfg = (slice_thickness, voltage_kv, calib_ang, shift_calib_ang, k, batch, tune)
+        ctx.save_for_backward(slices, modes, weights, positions, res, windows)
+        ctx.cfg = (slice_thickness, voltage_kv, calib_ang, shift_calib_ang, k, batch, tune, n, f)
         return out
 
     @staticmethod
     def backward(ctx, grad_out):
-        slices, modes, weights, positions, res = ctx.saved_tensors
-        slice_thickness, voltage_kv, calib_ang, shift_calib_ang, k, batch, tune = ctx.cfg
+        slices, modes, weights, positions, res, windows = ctx.saved_tensors
+        slice_thickness, voltage_kv, calib_ang, shift_calib_ang, k, batch, tune, n, f = ctx.cfg
         lib = _lib.load()
         dev = slices.device
-        n, S, M, P = slices.shape[0], slices.shape[2], modes.shape[2], positions.shape[0]
+        S, M, P = slices.shape[2], modes.shape[2], positions.shape[0]
         g_slices = torch.empty_strided(slices.shape, slices.stride(), dtype=torch.float32, device=dev)
         g_modes = torch.empty_strided(modes.shape, modes.stride(), dtype=torch.complex64, device=dev)
         if P == 0:
@@ -82,7 +81,7 @@ class Stem4dFunction(torch.autograd.Function):
         else:
             g = grad_out.to(torch.float32).contiguous()
             prm = ms_params(n, S, M, P, voltage_kv, slice_thickness, calib_ang, shift_calib_ang, slices.stride(),
-                            modes.stride(), batch, tune)
+                            modes.stride(), batch, tune, f, windows)
             ws_bytes = lib.ptyro_ms_backward_workspace_bytes(ctypes.byref(prm))
             ws = _workspace(ws_bytes, dev)
             _lib.check(lib.ptyro_ms_backward(ctypes.byref(prm), k, slices.data_ptr(), weights.data_ptr(),
@@ -92,29 +91,31 @@ class Stem4dFunction(torch.autograd.Function):
         # the C-ABI gives JAX's convention conj(2 dL/dconj); torch wants 2 dL/dconj
         return (g_slices if ctx.needs_input_grad[0] else None,
                 g_modes.conj().resolve_conj() if ctx.needs_input_grad[1] else None,
-                None, None, None, None, None, None, None, None, None)
+                None, None, None, None, None, None, None, None, None, None)
 
 
 def stem_4d_patterns(slices: torch.Tensor, modes: torch.Tensor, weights: torch.Tensor, positions: torch.Tensor,
                      slice_thickness: float, voltage_kv: float, calib_ang: float,
                      shift_calib_ang: Optional[float] = None, ckpt_every: int = DEFAULT_CKPT,
-                     batch: int = 0, tune: int = 0) -> torch.Tensor:
-    """Differentiable patterns (P, H, W) of the forward model (device tensors)."""
+                     batch: int = 0, tune: int = 0, windows: Optional[torch.Tensor] = None) -> torch.Tensor:
+    """Differentiable patterns (P, n, n) of the forward model (device tensors); with
+    ``windows`` the potential is a larger periodic field (see ``run_forward``)."""
     return Stem4dFunction.apply(slices, modes, weights, positions, float(slice_thickness), float(voltage_kv),
                                 float(calib_ang), float(calib_ang if shift_calib_ang is None else shift_calib_ang),
-                                int(ckpt_every), int(batch), int(tune))
+                                int(ckpt_every), int(batch), int(tune), windows)
 
 
 def vjp(slices, modes, weights, positions, grad_patterns, slice_thickness, voltage_kv, calib_ang,
-        shift_calib_ang=None, ckpt_every: int = DEFAULT_CKPT, batch: int = 0):
+        shift_calib_ang=None, ckpt_every: int = DEFAULT_CKPT, batch: int = 0, windows=None):
     """(patterns, dL/dV, dL/dmodes in JAX's convention) for dL/dpatterns = grad_patterns."""
     lib = _lib.load()
     dev = slices.device
-    n = _check_edge(slices.shape[0], slices.shape[1])
     S, M, P = slices.shape[2], modes.shape[2], positions.shape[0]
+    n, f = check_windows(slices, modes, windows, P)
     k = _ckpt_for(S, ckpt_every)
     sc = float(calib_ang if shift_calib_ang is None else shift_calib_ang)
-    prm = ms_params(n, S, M, P, voltage_kv, slice_thickness, calib_ang, sc, slices.stride(), modes.stride(), batch)
+    prm = ms_params(n, S, M, P, voltage_kv, slice_thickness, calib_ang, sc, slices.stride(), modes.stride(), batch,
+                    0, f, windows)
     out = torch.empty((P, n, n), dtype=torch.float32, device=dev)
     res = torch.empty(max(1, lib.ptyro_ms_residual_bytes(ctypes.byref(prm), k) // 4), dtype=torch.float32,
                       device=dev)

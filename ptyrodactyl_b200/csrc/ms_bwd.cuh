@@ -26,8 +26,10 @@ struct BwdArgs {
   const float* weights;    // (M)
   const float2* ckpt;      // checkpoint plane of this pass's slice point (slot stride res_stride), or null
   size_t res_stride;
-  const float2* trans;     // (S, N, N) T, row-major
+  const float2* trans;     // (S, F, F) T, row-major
   const float2* trans_t;   // transposed
+  const int* win;          // (B, 2) window origins in the field, or null
+  int field_n;             // F (== N without windows)
   const float2* pf;        // (N) propagator factor / N (conjugated in use)
   const float2* tw;        // (N) forward twiddles
   const float2* ramp_y;    // (B, N) shift ramps (beam-gradient epilogue)
@@ -156,10 +158,12 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) ms_bwd_pass_kernel(BwdArgs a
     }
 #pragma unroll
     for (int j = 0; j < N2; ++j) cv[j] = a.sigma2 * (p[j].x * l[j].y - p[j].y * l[j].x);
-    const float2* T = (AXIS == 0 ? a.trans : a.trans_t) + (size_t)a.t_slice * NN + (size_t)line * N;
+    int eoff;
+    const float2* T = trans_row<AXIS>(a.trans, a.trans_t, a.field_n, a.t_slice, a.win, b, line, &eoff);
+    const int fm = a.field_n - 1;
 #pragma unroll
     for (int j = 0; j < N2; ++j) {
-      const float2 tv = __ldg(T + t + N1 * j);
+      const float2 tv = __ldg(T + ((t + N1 * j + eoff) & fm));
       p[j] = cmulc(p[j], tv);
       l[j] = cmulc(l[j], tv);
     }

@@ -258,6 +258,10 @@ static int fft2_planes(int n, int count, bool inverse, float2* data, const float
 // ---------------------------------------------------------------- workspace layout
 static size_t align_up(size_t v) { return (v + 255) & ~(size_t)255; }
 
+static bool is_pow2(int n) { return n > 0 && (n & (n - 1)) == 0; }
+
+static int field_of(const ptyro_ms_params* p) { return p->field_n > 0 ? p->field_n : p->n; }
+
 struct Layout {
   size_t tw, pf, trans, trans_t, probe_k, ramp_y, ramp_x, waves, p2, total;
   int batch;
@@ -280,8 +284,9 @@ static Layout layout_for(const ptyro_ms_params* p) {
   size_t o = 0;
   L.tw = o; o = align_up(o + 8 * (size_t)p->n);
   L.pf = o; o = align_up(o + 8 * (size_t)p->n);
-  L.trans = o; o = align_up(o + 8 * nn * p->num_slices);
-  L.trans_t = o; o = align_up(o + 8 * nn * p->num_slices);
+  const size_t ff = (size_t)field_of(p) * field_of(p);
+  L.trans = o; o = align_up(o + 8 * ff * p->num_slices);
+  L.trans_t = o; o = align_up(o + 8 * ff * p->num_slices);
   L.probe_k = o; o = align_up(o + 8 * nn * p->num_modes);
   L.ramp_y = o; o = align_up(o + 8 * (size_t)p->n * L.batch);
   L.ramp_x = o; o = align_up(o + 8 * (size_t)p->n * L.batch);
@@ -291,10 +296,11 @@ static Layout layout_for(const ptyro_ms_params* p) {
   return L;
 }
 
-static bool is_pow2(int n) { return n > 0 && (n & (n - 1)) == 0; }
 
 static int validate(const ptyro_ms_params* p) {
   if (!p) return fail(PTYRO_ERR_INVALID, "params is NULL");
+  if (p->field_n != 0 && (!is_pow2(p->field_n) || p->field_n < p->n || p->field_n > 8192))
+    return fail(PTYRO_ERR_INVALID, "field_n must be 0 or a power of two in [n, 8192]");
   if (!is_pow2(p->n) || p->n < 16 || p->n > 1024)
     return fail(PTYRO_ERR_UNSUPPORTED, "grid edge n must be a power of two in [16, 1024], got " +
                                            std::to_string(p->n));
@@ -340,8 +346,9 @@ static int forward_setup(const ptyro_ms_params* p, const Layout& L, char* ws, co
   const double lam = wavelength_ang(p->voltage_kv);
   k_twiddle<<<(n + 255) / 256, 256, 0, st>>>(n, tw);
   k_propagator<<<(n + 255) / 256, 256, 0, st>>>(n, p->calib_ang, lam * p->slice_thickness_ang, 1.0 / n, pf);
-  k_transmission<<<blocks_for(nn * p->num_slices, 256), 256, 0, st>>>(
-      potential, p->pot_stride_y, p->pot_stride_x, p->pot_stride_s, n, p->num_slices,
+  const int F = field_of(p);
+  k_transmission<<<blocks_for((size_t)F * F * p->num_slices, 256), 256, 0, st>>>(
+      potential, p->pot_stride_y, p->pot_stride_x, p->pot_stride_s, F, p->num_slices,
       interaction_sigma(p->voltage_kv), T, (float2*)(ws + L.trans_t));
   k_gather_modes<<<blocks_for(nn * p->num_modes, 256), 256, 0, st>>>(
       (const float2*)modes, p->mode_stride_y, p->mode_stride_x, p->mode_stride_m, n, p->num_modes, pk);
@@ -388,9 +395,11 @@ static int forward_impl(const ptyro_ms_params* p, int ckpt_every, const float* p
   a.n_modes = M;
   a.scale = 1.0f / (float)n;
   a.res_stride = res_stride;
+  a.field_n = field_of(p);
   for (int b0 = 0; b0 < p->num_probes; b0 += L.batch) {
     const int nb = p->num_probes - b0 < L.batch ? p->num_probes - b0 : L.batch;
     float2* res_base = residuals ? residuals + (size_t)b0 * M * res_stride : nullptr;
+    a.win = p->windows ? (const int*)p->windows + 2 * (size_t)b0 : nullptr;
     k_ramps<<<(nb * n + 255) / 256, 256, 0, st>>>(positions + 2 * (size_t)b0, nb, n, p->shift_calib_ang, ry, rx);
     if ((rc = check_launch("k_ramps"))) return rc;
     // pass 0: x part of the IFFT2 of the shifted probe spectrum
@@ -442,6 +451,60 @@ __global__ void k_reduce_dv(const float* __restrict__ contrib, int nslots, int n
   dv[(long long)y * sy + (long long)x * sx + (long long)s * ss] += acc;
 }
 
+// Windowed runs: field pixel (fy, fx) of dV_s collects the contribution of every
+// slot whose n x n window (origin modulo F) covers it, added in slot order (no
+// atomics). Loads of 8 slots are issued together before they are summed, so a
+// thread keeps several reads in flight; neighbouring threads read neighbouring
+// pixels of the same slot plane.
+constexpr int kReduceWinStaged = 4096;
+
+__global__ void __launch_bounds__(256) k_reduce_dv_win(const float* __restrict__ contrib, int nb, int M, int n,
+                                                       int F, const int* __restrict__ win, float* dv, long long sy,
+                                                       long long sx, long long ss, int s) {
+  extern __shared__ int swin[];
+  const bool staged = nb <= kReduceWinStaged;  // window origins in shared memory when they fit
+  if (staged)
+    for (int i = threadIdx.x; i < 2 * nb; i += blockDim.x) swin[i] = win ? win[i] : 0;
+  __syncthreads();
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (size_t)F * F) return;
+  const int fy = (int)(i / F), fx = (int)(i % F);
+  const int fm = F - 1;
+  const size_t nn = (size_t)n * n;
+  float acc = 0.f;
+  for (int b0 = 0; b0 < nb; b0 += 8) {
+    float v[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int bb = b0 + u;
+      v[u] = 0.f;
+      if (bb < nb) {
+        const int wy = staged ? swin[2 * bb] : (win ? win[2 * bb] : 0);
+        const int wx = staged ? swin[2 * bb + 1] : (win ? win[2 * bb + 1] : 0);
+        const int ly = (fy - wy) & fm, lx = (fx - wx) & fm;
+        if (ly < n && lx < n) {
+          const float* cp = contrib + (size_t)bb * M * nn + (size_t)ly * n + lx;
+          float t = cp[0];
+          for (int m = 1; m < M; ++m) t += cp[(size_t)m * nn];
+          v[u] = t;
+        }
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < 8; ++u) acc += v[u];
+  }
+  dv[(long long)fy * sy + (long long)fx * sx + (long long)s * ss] += acc;
+}
+
+static int launch_reduce_dv_win(const float* contrib, int nb, int M, int n, int F, const int* win, float* dv,
+                                long long sy, long long sx, long long ss, int s, cudaStream_t st) {
+  const size_t ff = (size_t)F * F;
+  const size_t smem = nb <= kReduceWinStaged ? 2 * sizeof(int) * (size_t)nb : 0;
+  k_reduce_dv_win<<<(unsigned)((ff + 255) / 256), 256, smem, st>>>(
+      contrib, nb, M, n, F, win, dv, sy, sx, ss, s);
+  return check_launch("k_reduce_dv_win");
+}
+
 // beam spectrum gradient: acc[m] += sum_b lam[b*M + m], in probe order.
 __global__ void k_reduce_beam(const float2* __restrict__ lam, int nb, int M, int n, float2* acc) {
   const size_t nn = (size_t)n * n;
@@ -476,8 +539,9 @@ static BwdLayout bwd_layout_for(const ptyro_ms_params* p) {
   if (p->batch > 0) {
     L.batch = p->batch < p->num_probes ? p->batch : (p->num_probes > 0 ? p->num_probes : 1);
   } else {
-    // the two wave sets of a batch (forward + adjoint) near 64 MB: L2-resident
-    int b = (int)(32.0 * 1024 * 1024 / (8.0 * nn * p->num_modes));
+    // 64 MiB per wave set (forward + adjoint = 128 MiB): measured faster than an
+    // L2-resident 32 MiB set at 256^2 (fewer, fuller launches and reductions)
+    int b = (int)(64.0 * 1024 * 1024 / (8.0 * nn * p->num_modes));
     if (b < 1) b = 1;
     L.batch = b > p->num_probes ? (p->num_probes > 0 ? p->num_probes : 1) : b;
   }
@@ -485,8 +549,9 @@ static BwdLayout bwd_layout_for(const ptyro_ms_params* p) {
   size_t o = 0;
   L.tw = o; o = align_up(o + 8 * (size_t)p->n);
   L.pf = o; o = align_up(o + 8 * (size_t)p->n);
-  L.trans = o; o = align_up(o + 8 * nn * p->num_slices);
-  L.trans_t = o; o = align_up(o + 8 * nn * p->num_slices);
+  const size_t ff = (size_t)field_of(p) * field_of(p);
+  L.trans = o; o = align_up(o + 8 * ff * p->num_slices);
+  L.trans_t = o; o = align_up(o + 8 * ff * p->num_slices);
   L.ramp_y = o; o = align_up(o + 8 * (size_t)p->n * L.batch);
   L.ramp_x = o; o = align_up(o + 8 * (size_t)p->n * L.batch);
   L.psi = o; o = align_up(o + 8 * nn * slots);
@@ -541,11 +606,14 @@ static int backward_impl(const ptyro_ms_params* p, int ckpt_every, const float* 
   k_twiddle<<<(n + 255) / 256, 256, 0, st>>>(n, tw);
   k_propagator<<<(n + 255) / 256, 256, 0, st>>>(n, p->calib_ang, lam * p->slice_thickness_ang, 1.0 / n,
                                                 (float2*)(ws + L.pf));
-  k_transmission<<<blocks_for(nn * S, 256), 256, 0, st>>>(potential, p->pot_stride_y, p->pot_stride_x,
-                                                          p->pot_stride_s, n, S, interaction_sigma(p->voltage_kv),
-                                                          (float2*)(ws + L.trans), (float2*)(ws + L.trans_t));
-  k_zero_pot<<<blocks_for(nn * S, 256), 256, 0, st>>>(grad_potential, p->pot_stride_y, p->pot_stride_x,
-                                                      p->pot_stride_s, n, S);
+  const int F = field_of(p);
+  const bool windowed = p->windows != nullptr || F != n;
+  k_transmission<<<blocks_for((size_t)F * F * S, 256), 256, 0, st>>>(potential, p->pot_stride_y, p->pot_stride_x,
+                                                                     p->pot_stride_s, F, S,
+                                                                     interaction_sigma(p->voltage_kv),
+                                                                     (float2*)(ws + L.trans), (float2*)(ws + L.trans_t));
+  k_zero_pot<<<blocks_for((size_t)F * F * S, 256), 256, 0, st>>>(grad_potential, p->pot_stride_y, p->pot_stride_x,
+                                                                 p->pot_stride_s, F, S);
   k_zero2<<<blocks_for(nn * M, 256), 256, 0, st>>>(beam, nn * M);
   if ((rc = check_launch("backward setup", 5))) return rc;
   BwdArgs a = {};
@@ -561,11 +629,14 @@ static int backward_impl(const ptyro_ms_params* p, int ckpt_every, const float* 
   a.ramp_x = (const float2*)(ws + L.ramp_x);
   a.n_modes = M;
   a.sigma2 = (float)(2.0 * interaction_sigma(p->voltage_kv));
+  a.field_n = F;
   a.scale = 1.0f / (float)n;
   float* contrib = (float*)(ws + L.contrib);
   for (int b0 = 0; b0 < p->num_probes; b0 += L.batch) {
     const int nb = p->num_probes - b0 < L.batch ? p->num_probes - b0 : L.batch;
     const float2* res_base = residuals + (size_t)b0 * M * res_stride;
+    const int* win = p->windows ? (const int*)p->windows + 2 * (size_t)b0 : nullptr;
+    a.win = win;
     k_ramps<<<(nb * n + 255) / 256, 256, 0, st>>>(positions + 2 * (size_t)b0, nb, n, p->shift_calib_ang,
                                                   (float2*)(ws + L.ramp_y), (float2*)(ws + L.ramp_x));
     if ((rc = check_launch("k_ramps"))) return rc;
@@ -586,9 +657,15 @@ static int backward_impl(const ptyro_ms_params* p, int ckpt_every, const float* 
       q.psi_done = k == S;
       q.beam_epi = k == S;
       if ((rc = launch_bwd(n, k % 2, q, nb * M, st))) return rc;
-      k_reduce_dv<<<(unsigned)((nn + 255) / 256), 256, 0, st>>>(contrib, nb * M, n, grad_potential, p->pot_stride_y,
-                                                                 p->pot_stride_x, p->pot_stride_s, s);
-      if ((rc = check_launch("k_reduce_dv"))) return rc;
+      if (windowed) {
+        if ((rc = launch_reduce_dv_win(contrib, nb, M, n, F, win, grad_potential, p->pot_stride_y,
+                                       p->pot_stride_x, p->pot_stride_s, s, st)))
+          return rc;
+      } else {
+        k_reduce_dv<<<(unsigned)((nn + 255) / 256), 256, 0, st>>>(contrib, nb * M, n, grad_potential,
+                                                                   p->pot_stride_y, p->pot_stride_x, p->pot_stride_s, s);
+        if ((rc = check_launch("k_reduce_dv"))) return rc;
+      }
     }
     q = a;
     q.op1 = OP_FFT; q.t_slice = -1; q.op2 = OP_NONE; q.psi_done = 1; q.beam_epi = 1;
@@ -662,6 +739,8 @@ int ptyro_ms_forward_plain(const ptyro_ms_params* p, const float* potential, con
   if (p->num_probes == 0) return PTYRO_OK;
   if (!potential || !modes || !weights || !positions || !patterns)
     return fail(PTYRO_ERR_INVALID, "NULL array argument");
+  if (p->windows || field_of(p) != p->n)
+    return fail(PTYRO_ERR_UNSUPPORTED, "the plain per-position path has no windowed mode");
   const Layout L = layout_for(p);
   rc = check_workspace(L, workspace, workspace_bytes);
   if (rc) return rc;
@@ -728,6 +807,7 @@ int ptyro_ms_steady_pass(const ptyro_ms_params* p, int32_t axis, int32_t reps, v
   a.t_slice = 1;
   a.op2 = OP_CONV;
   a.dst = DST_WAVE;
+  a.field_n = field_of(p);
   for (int r = 0; r < reps; ++r)
     if ((rc = launch_pass(p->n, axis, a, L.batch * p->num_modes, (cudaStream_t)stream, p->tune))) return rc;
   return PTYRO_OK;

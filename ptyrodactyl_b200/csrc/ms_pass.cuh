@@ -29,8 +29,11 @@ struct PassArgs {
   const float2* probe_k;   // (M, N, N) spectrum of the beam modes (SRC_PROBE)
   const float2* ramp_y;    // (B, N) shift ramp along y per probe of the batch (SRC_PROBE)
   const float2* ramp_x;    // (B, N) shift ramp along x
-  const float2* trans;     // (S, N, N) transmission exp(i sigma V), row-major [y][x]
-  const float2* trans_t;   // (S, N, N) the same, transposed [x][y]
+  const float2* trans;     // (S, F, F) transmission exp(i sigma V), row-major [y][x]
+  const float2* trans_t;   // (S, F, F) the same, transposed [x][y]
+  const int* win;          // (B, 2) window origins (y, x) in the field for this batch, or null
+  int field_n;             // F (== N without windows); power of two
+
   const float2* pf;        // (N) 1-D propagator factor along this axis, already divided by N
   const float2* tw;        // (N) forward twiddles exp(-2 pi i j / N)
   float* pattern;          // (B, N, N) fftshifted intensity (DST_PATTERN)
@@ -98,6 +101,22 @@ __device__ __forceinline__ void tile_store(T2* __restrict__ W, const T2* work, i
     const int i = threadIdx.x + it * THREADS;
     W[(size_t)(i / LINES) * N + line0 + i % LINES] = work[(i / LINES) * PITCH + i % LINES];
   }
+}
+
+// Transmission row of `line` for a probe whose window starts at (wy, wx) in the
+// periodic F x F field; element e of the line is at index (e + off) & (F - 1).
+template <int AXIS>
+__device__ __forceinline__ const float2* trans_row(const float2* trans, const float2* trans_t, int field_n,
+                                                   int t_slice, const int* win, int b, int line, int* off) {
+  int wy = 0, wx = 0;
+  if (win) {
+    wy = win[2 * b];
+    wx = win[2 * b + 1];
+  }
+  const int fm = field_n - 1;
+  *off = AXIS == 0 ? wx : wy;
+  const float2* T = (AXIS == 0 ? trans : trans_t) + (size_t)t_slice * field_n * field_n;
+  return T + (size_t)((line + (AXIS == 0 ? wy : wx)) & fm) * field_n;
 }
 
 // op on registers in natural distribution; returns true if the result is k-order.
@@ -208,10 +227,13 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) ms_pass_kernel(PassArgs a) {
     }
     // ---- transmission (natural distribution; row-major table for rows, transposed for columns)
     if (a.t_slice >= 0) {
-      const float2* T = (AXIS == 0 ? a.trans : a.trans_t) + (size_t)a.t_slice * NN + (size_t)line * N;
+      int eoff;
+      const float2* T = trans_row<AXIS>(a.trans, a.trans_t, a.field_n, a.t_slice, a.win, blockIdx.y / a.n_modes,
+                                        line, &eoff);
+      const int fm = a.field_n - 1;
 #pragma unroll
       for (int j = 0; j < N2; ++j) {
-        const float2 tv = __ldg(T + t + N1 * j);
+        const float2 tv = __ldg(T + ((t + N1 * j + eoff) & fm));
         v[j] = a.t_conj ? cmulc(v[j], tv) : cmul(v[j], tv);
       }
       if (a.ckpt_store) {

@@ -33,15 +33,16 @@ int launch_bwd_t(const BwdArgs& a, int grid_y, cudaStream_t st) {
   using Geo = PassGeom<N1, N2>;
   constexpr int N = Geo::N;
   constexpr int W = Geo::kWarps;
+  constexpr int MINB = N2 <= 16 ? 2 : 1;  // two resident CTAs where the register budget allows
   const size_t smem = Geo::smem_bytes(W);
   static bool attr_done = false;
   if (!attr_done) {
-    cudaFuncSetAttribute(ms_bwd_pass_kernel<N1, N2, AXIS, W, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaFuncSetAttribute(ms_bwd_pass_kernel<N1, N2, AXIS, W, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)smem);
     attr_done = true;
   }
   dim3 grid(N / Geo::kLines, grid_y);
-  ms_bwd_pass_kernel<N1, N2, AXIS, W, 1><<<grid, W * 32, smem, st>>>(a);
+  ms_bwd_pass_kernel<N1, N2, AXIS, W, MINB><<<grid, W * 32, smem, st>>>(a);
   g_launches.fetch_add(1, std::memory_order_relaxed);
   return (int)cudaGetLastError();
 }

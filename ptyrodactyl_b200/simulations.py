@@ -86,10 +86,13 @@ def _workspace(nbytes: int, device: torch.device) -> torch.Tensor:
 
 def ms_params(n: int, num_slices: int, num_modes: int, num_probes: int, voltage_kv: float,
               slice_thickness: float, calib_ang: float, shift_calib_ang: float,
-              pot_strides=(0, 0, 0), mode_strides=(0, 0, 0), batch: int = 0, tune: int = 0) -> _lib.MsParams:
+              pot_strides=(0, 0, 0), mode_strides=(0, 0, 0), batch: int = 0, tune: int = 0,
+              field_n: int = 0, windows: Optional[torch.Tensor] = None) -> _lib.MsParams:
     p = _lib.MsParams()
     p.n, p.num_slices, p.num_modes, p.num_probes, p.batch = n, num_slices, num_modes, num_probes, batch
     p.tune = tune
+    p.field_n = 0 if field_n == n else int(field_n)
+    p.windows = None if windows is None else windows.data_ptr()
     p.voltage_kv = float(voltage_kv)
     p.slice_thickness_ang = float(slice_thickness)
     p.calib_ang = float(calib_ang)
@@ -99,24 +102,42 @@ def ms_params(n: int, num_slices: int, num_modes: int, num_probes: int, voltage_
     return p
 
 
+def check_windows(slices: torch.Tensor, modes: torch.Tensor, windows: Optional[torch.Tensor], num_probes: int):
+    """Grid edge n (from the beam) and field edge F (from the potential)."""
+    n = _check_edge(modes.shape[0], modes.shape[1])
+    f = slices.shape[0]
+    if slices.shape[0] != slices.shape[1]:
+        raise ValueError(f"potential field must be square, got {tuple(slices.shape[:2])}")
+    if f != n:
+        if f < n or f & (f - 1) or f > 8192:
+            raise ValueError(f"potential field edge must be a power of two in [{n}, 8192], got {f}")
+    elif windows is None:
+        return n, f
+    if windows is not None:
+        if windows.dtype != torch.int32 or tuple(windows.shape) != (num_probes, 2) or not windows.is_contiguous():
+            raise ValueError("windows must be a contiguous (P, 2) int32 tensor")
+        if windows.device != slices.device:
+            raise ValueError("windows must be on the potential's device")
+    return n, f
+
+
 def run_forward(slices: torch.Tensor, slice_thickness: float, modes: torch.Tensor, weights: torch.Tensor,
                 positions: torch.Tensor, voltage_kv: float, calib_ang: float, shift_calib_ang: float,
                 out: Optional[torch.Tensor] = None, batch: int = 0, plain: bool = False,
-                tune: int = 0) -> torch.Tensor:
+                tune: int = 0, windows: Optional[torch.Tensor] = None) -> torch.Tensor:
     """Device-level forward: all tensors already on one CUDA device.
 
-    slices (H, W, S) float32 (any strides), modes (H, W, M) complex64 (any strides),
-    weights (M,) float32, positions (P, 2) float64 contiguous. Returns patterns
-    (P, H, W) float32.
+    slices (F, F, S) float32 (any strides), modes (n, n, M) complex64 (any strides),
+    weights (M,) float32, positions (P, 2) float64 contiguous. F == n, or F > n with
+    ``windows`` (P, 2) int32: probe p then reads the n x n window of the periodic
+    field starting at windows[p]. Returns patterns (P, n, n) float32.
     """
     lib = _lib.load()
     dev = slices.device
-    n = _check_edge(slices.shape[0], slices.shape[1])
-    if tuple(modes.shape[:2]) != (n, n):
-        raise ValueError("beam modes and potential slices must share the grid shape")
     num_probes = positions.shape[0]
+    n, f = check_windows(slices, modes, windows, num_probes)
     prm = ms_params(n, slices.shape[2], modes.shape[2], num_probes, voltage_kv, slice_thickness,
-                    calib_ang, shift_calib_ang, slices.stride(), modes.stride(), batch, tune)
+                    calib_ang, shift_calib_ang, slices.stride(), modes.stride(), batch, tune, f, windows)
     if out is None:
         out = torch.empty((num_probes, n, n), dtype=torch.float32, device=dev)
     if num_probes == 0:
@@ -172,6 +193,33 @@ def stem_4d(pot_slice: PotentialSlices, beam: ProbeModes, microscope: Microscope
     scan_positions = detector.scan_positions_px.to(torch.float64) * detector.real_space_calib_ang
     return create_stem4d(data, detector.real_space_calib_ang, fourier_calib, scan_positions,
                          microscope.voltage_kv)
+
+
+def stem_4d_windowed(pot_slice: PotentialSlices, beam: ProbeModes, microscope: MicroscopeConfig,
+                     detector: DetectorConfig, windows) -> STEM4D:
+    """stem_4d where probe p sees the (n x n) window of a larger periodic potential
+    field that starts at pixel ``windows[p] = (y, x)``; positions shift the probe
+    inside its window as in ``stem_4d``. The tiled counterpart of the reference's
+    ``crystal2stem4d_tiled`` (src/ptyrodactyl/workflows/stem_4d.py:553), which crops
+    a tile of the sample around each position."""
+    if detector.scan_positions_px is None:
+        raise ValueError("detector.scan_positions_px is required")
+    dev = _device(pot_slice.slices.device if pot_slice.slices.is_cuda else None)
+    slices = as_tensor(pot_slice.slices, torch.float32, dev)
+    modes, weights = _beam_on(beam, dev)
+    positions = as_tensor(detector.scan_positions_px, torch.float64, dev).reshape(-1, 2).contiguous()
+    win = as_tensor(windows, torch.int32, dev).reshape(-1, 2).contiguous()
+    calib = min(float(pot_slice.calib), float(beam.calib))
+    if torch.is_grad_enabled() and (slices.requires_grad or modes.requires_grad):
+        from .autodiff import stem_4d_patterns
+        data = stem_4d_patterns(slices, modes, weights, positions, pot_slice.slice_thickness,
+                                microscope.voltage_kv, calib, detector.real_space_calib_ang, windows=win)
+    else:
+        data = run_forward(slices, pot_slice.slice_thickness, modes, weights, positions, microscope.voltage_kv,
+                           calib, detector.real_space_calib_ang, windows=win)
+    fourier_calib = 1.0 / (modes.shape[0] * calib)
+    scan_positions = detector.scan_positions_px.to(torch.float64) * detector.real_space_calib_ang
+    return create_stem4d(data, detector.real_space_calib_ang, fourier_calib, scan_positions, microscope.voltage_kv)
 
 
 def cbed_image(pot_slices: PotentialSlices, beam: ProbeModes, microscope: MicroscopeConfig) -> CalibratedArray:

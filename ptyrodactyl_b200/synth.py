@@ -135,3 +135,54 @@ def raster_positions(w: Workload, scan=None) -> np.ndarray:
 def algorithmic_flops_per_update(n: int) -> float:
     """Two complex 2-D FFTs (5 N^2 log2 N^2 each) and two complex multiplies (6 N^2)."""
     return 20.0 * n * n * np.log2(n) + 12.0 * n * n
+
+
+@dataclass(frozen=True)
+class GradWorkload:
+    """Ptychographic gradient configuration: n x n probe windows over an F x F field."""
+
+    name: str
+    n: int
+    field_n: int
+    cells: int
+    num_slices: int
+    scan: tuple
+    step_px: int
+    voltage_kv: float
+    aperture_mrad: float
+    defocus_ang: float
+    c3_ang: float
+    dose: float
+    seed: int
+
+    @property
+    def calib(self) -> float:
+        return self.cells * LATTICE_A / self.field_n
+
+    @property
+    def num_probes(self) -> int:
+        return int(self.scan[0] * self.scan[1])
+
+    def windows(self) -> np.ndarray:
+        """(P, 2) int32 window origins: a raster with step_px that keeps windows inside the field."""
+        iy, ix = np.meshgrid(np.arange(self.scan[0]), np.arange(self.scan[1]), indexing="ij")
+        return np.stack([iy.ravel() * self.step_px, ix.ravel() * self.step_px], axis=1).astype(np.int32)
+
+    def field(self, phonon: int = 0) -> np.ndarray:
+        w = Workload(self.name, self.field_n, self.cells, self.num_slices, self.scan, self.voltage_kv,
+                     self.aperture_mrad, seed=self.seed)
+        return potential_slices(w, phonon)
+
+
+# 256^2 windows over a 512^2 field (32x32 cells), 10 slices, 32x32 scan with an 8 px step,
+# targets Poisson-noised at 1e4 electrons per pattern.
+CONFIG4 = GradWorkload("ptycho-512px-field-256px-window-10sl-32x32scan", 256, 512, 32, 10, (32, 32), 8,
+                       200.0, 25.0, -50.0, 1e-3, 1e4, seed=4)
+
+
+def poisson_targets(patterns: np.ndarray, dose: float, rng: np.random.Generator) -> np.ndarray:
+    """Patterns (P, n, n) with Poisson counting noise at ``dose`` electrons per pattern,
+    scaled back to the patterns' units."""
+    total = patterns.sum(axis=(1, 2), keepdims=True)
+    lam = np.clip(patterns, 0, None) / total * dose
+    return rng.poisson(lam).astype(np.float64) * total / dose
