@@ -1,0 +1,60 @@
+"""CUDA-graph replay and the autotuner (GPU)."""
+
+import numpy as np
+import pytest
+import torch
+
+import ptyrodactyl_b200 as pb
+from oracle import multislice_ref as R
+from ptyrodactyl_b200 import synth
+from ptyrodactyl_b200.autotune import tune_forward
+from ptyrodactyl_b200.graphs import GraphedForward
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def case():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    w = synth.CONFIG1
+    dev = torch.device("cuda")
+    pot = torch.as_tensor(synth.potential_slices(w, num_slices=6), device=dev)
+    probe = R.make_probe(w.voltage_kv, w.aperture_mrad, (w.n, w.n), w.calib * 100.0)
+    modes = torch.as_tensor(probe[..., None].astype(np.complex64), device=dev)
+    wts = torch.ones(1, device=dev)
+    pos = torch.as_tensor(synth.raster_positions(w)[:40], device=dev).contiguous()
+    return w, pot, modes, wts, pos
+
+
+def test_graph_replay_matches_direct_and_follows_inputs(case):
+    w, pot, modes, wts, pos = case
+    g = GraphedForward(pot, modes, wts, pos.clone(), synth.SLICE_DZ, w.voltage_kv, w.calib, batch=16)
+    assert g.launches_per_replay > 0
+    direct = pb.run_forward(pot, synth.SLICE_DZ, modes, wts, pos, w.voltage_kv, w.calib, w.calib, batch=16)
+    out = g.replay().clone()
+    torch.cuda.synchronize()
+    assert torch.equal(out, direct)
+    moved = (pos + 0.75).contiguous()
+    g.positions.copy_(moved)
+    out2 = g.replay().clone()
+    direct2 = pb.run_forward(pot, synth.SLICE_DZ, modes, wts, moved, w.voltage_kv, w.calib, w.calib, batch=16)
+    torch.cuda.synchronize()
+    assert torch.equal(out2, direct2)
+    assert not torch.equal(out2, out)
+
+
+def test_autotune_picks_and_caches(case, tmp_path, monkeypatch):
+    monkeypatch.setenv("PTYRO_B200_TUNE_CACHE", str(tmp_path / "tune.json"))
+    import ptyrodactyl_b200.autotune as at
+    at._memo.clear()
+    w, pot, modes, wts, pos = case
+    batch, tune = tune_forward(pot, modes, wts, pos, synth.SLICE_DZ, w.voltage_kv, w.calib)
+    assert 1 <= batch <= pos.shape[0] and 0 <= tune <= 3
+    assert (tmp_path / "tune.json").exists()
+    at._memo.clear()
+    assert tune_forward(pot, modes, wts, pos, synth.SLICE_DZ, w.voltage_kv, w.calib) == (batch, tune)
+    ref = pb.run_forward(pot, synth.SLICE_DZ, modes, wts, pos, w.voltage_kv, w.calib, w.calib)
+    got = pb.run_forward(pot, synth.SLICE_DZ, modes, wts, pos, w.voltage_kv, w.calib, w.calib, batch=batch,
+                         tune=tune)
+    assert torch.equal(ref, got)
