@@ -492,6 +492,79 @@ def run_grad(args, rank, world, local_rank):
         print(json.dumps(line), flush=True)
 
 
+# ----------------------------------------------------------------------------- serving leg
+def run_serve(args, rank, world, local_rank):
+    """Poisson-arrival mix of simulations and gradient solves through the server;
+    p50/p99 latency and aggregate probe-slice updates/s (one JSON line)."""
+    import torch
+    from ptyrodactyl_b200.serving import Request, Server, serving_mix
+
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    srv = Server(arena_bytes=int(args.arena_gb * (1 << 30)), max_slots=args.max_slots, device=dev)
+    smax = 100
+    for n in (64, 128, 256, 512):
+        w = synth.Workload(f"serve-{n}", n, n * 4 // 64 if n >= 64 else 1, smax, (1, 1), 200.0, 20.0, seed=5)
+        srv.add_potential(f"p{n}", synth.potential_slices(w))
+    calib = 4 * synth.LATTICE_A / 64  # 4 cells per 64 px at every edge
+
+    def build(spec, arrival_abs):
+        n, p = spec["n"], spec["num_probes"]
+        side = int(np.ceil(np.sqrt(p)))
+        fov = n * calib
+        g = (np.arange(side) - (side - 1) / 2.0) * (fov / side)
+        yy, xx = np.meshgrid(g, g, indexing="ij")
+        pos = np.stack([yy.ravel(), xx.ravel()], axis=1)[:p]
+        req = Request(n=n, num_slices=spec["num_slices"], positions=pos, voltage_kv=spec["voltage_kv"],
+                      aperture_mrad=spec["aperture_mrad"], defocus_ang=spec["defocus_ang"], kind=spec["kind"],
+                      potential_key=f"p{n}", calib_ang=calib, arrival_s=arrival_abs)
+        if spec["kind"] == "grad":
+            gen = torch.Generator(device=dev)
+            gen.manual_seed(spec["seed"])
+            req.targets = torch.rand((p, n, n), generator=gen, device=dev) * (2.0 / (n * n))
+        return req
+
+    # warm-up: one request of every grid edge and kind (module loading, first launches)
+    for n in (64, 128, 256, 512):
+        for kind in ("forward", "grad"):
+            srv.submit(build(dict(n=n, num_probes=4, num_slices=5, voltage_kv=200.0, aperture_mrad=20.0,
+                                  defocus_ang=0.0, kind=kind, seed=1), time.perf_counter()))
+    srv.drain()
+    srv.finished.clear()
+    mix = serving_mix(args.requests, args.seed, args.rate)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    i = 0
+    while i < len(mix) or srv.active:
+        now = time.perf_counter() - t0
+        while i < len(mix) and mix[i]["arrival_s"] <= now:
+            srv.submit(build(mix[i], t0 + mix[i]["arrival_s"]))
+            i += 1
+        if srv.active:
+            srv.poll()
+        elif i < len(mix):
+            time.sleep(max(0.0, min(0.001, mix[i]["arrival_s"] - now)))
+    torch.cuda.synchronize()
+    t_end = time.perf_counter()
+    lat = np.array([r.latency_s for r in srv.finished]) * 1e3
+    upd = sum(r.request.updates for r in srv.finished)
+    ok = sum(1 for r in srv.finished if r.state == 2)
+    srv.close()
+    line = {
+        "metric": "serving mix: p50/p99 latency and aggregate probe-slice updates/s", "mode": "serve",
+        "value": upd / (t_end - t0), "unit": UNIT, "p50_ms": float(np.percentile(lat, 50)),
+        "p99_ms": float(np.percentile(lat, 99)), "mean_ms": float(lat.mean()), "requests": len(mix),
+        "completed": ok, "makespan_s": t_end - t0, "n_gpus": world, "dtype": "f32", "data": "synthetic",
+        "config": {"grids": [64, 128, 256, 512], "slices": "5-100 log-uniform", "probes": "1-4096 log-uniform",
+                   "kv": "60-300", "aperture_mrad": "10-30", "grad_fraction": 0.3, "rate_hz": args.rate,
+                   "seed": args.seed, "arena_gb": args.arena_gb, "max_slots": args.max_slots,
+                   "admission": "HBM footprint (arena) + wave-slot budget",
+                   "targets": "uniform random patterns (gradient cost does not depend on them)"},
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 # ----------------------------------------------------------------------------- reference arm
 def run_reference(args, rank):
     if rank != 0:
@@ -533,7 +606,12 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--mode", choices=("forward", "grad"), default="forward")
+    ap.add_argument("--mode", choices=("forward", "grad", "serve"), default="forward")
+    ap.add_argument("--requests", type=int, default=64, help="serve mode: requests in the mix")
+    ap.add_argument("--rate", type=float, default=20.0, help="serve mode: Poisson arrival rate (1/s)")
+    ap.add_argument("--seed", type=int, default=5, help="serve mode: mix seed")
+    ap.add_argument("--arena-gb", type=float, default=48.0, help="serve mode: scheduler arena")
+    ap.add_argument("--max-slots", type=int, default=1024, help="serve mode: wave slots in flight")
     ap.add_argument("--ckpt", type=int, default=0, help="gradient mode: checkpoint spacing (0 = sqrt(S))")
     ap.add_argument("--bwd-batch", type=int, default=0, help="gradient mode: probes per adjoint batch")
     args = ap.parse_args()
@@ -553,6 +631,8 @@ def main():
     try:
         if args.mode == "grad":
             run_grad(args, rank, world, local_rank)
+        elif args.mode == "serve":
+            run_serve(args, rank, world, local_rank)
         else:
             run_ours(args, rank, world, local_rank)
     finally:

@@ -162,6 +162,71 @@ int ptyro_ms_steady_pass(const ptyro_ms_params* p, int32_t axis, int32_t reps, v
  * the FP32 ceiling used as the roofline denominator; no reference counterpart. */
 int ptyro_fp32_fma_probe(float* out, int32_t blocks, int32_t iters, void* stream);
 
+/* ---------------------------------------------------------------- scheduler
+ * Continuous batching of forward and gradient jobs of any grid edge, slice count
+ * and scan size (the batching and serving patterns; no reference counterpart:
+ * the reference runs one jitted stem_4d call at a time). Jobs wait until their
+ * scratch fits in the caller-provided arena and their probes in flight fit the slot
+ * budget; each ptyro_sched_step advances every running job by one pass, the
+ * passes of all running jobs with the same grid edge going out as one multi-job
+ * launch per (forward/adjoint, axis). Inputs and outputs are the caller's device
+ * buffers; they must stay valid until the job is DONE, FAILED or CANCELLED. */
+#define PTYRO_JOB_FORWARD 0
+#define PTYRO_JOB_GRADIENT 1
+
+#define PTYRO_JOB_QUEUED 0
+#define PTYRO_JOB_RUNNING 1
+#define PTYRO_JOB_DONE 2
+#define PTYRO_JOB_FAILED 3
+#define PTYRO_JOB_CANCELLED 4
+
+typedef struct ptyro_sched ptyro_sched;
+
+typedef struct ptyro_job_desc {
+  ptyro_ms_params p;          /* geometry; p.batch = probes in flight (0 = automatic) */
+  int32_t kind;               /* PTYRO_JOB_FORWARD or PTYRO_JOB_GRADIENT */
+  int32_t ckpt_every;         /* gradient jobs: checkpoint spacing (0 = ceil(sqrt(S))) */
+  const float* potential;     /* as ptyro_ms_forward */
+  const float* modes;
+  const float* weights;
+  const double* positions;
+  float* patterns;            /* out (P, n, n) */
+  const float* targets;       /* gradient jobs: measured patterns (P, n, n), fftshifted */
+  float* grad_potential;      /* gradient jobs, out: d(loss)/dV with the potential's strides */
+  float* grad_modes;          /* gradient jobs, out: JAX-convention gradient of the modes */
+  float* loss;                /* gradient jobs, out: amplitude loss sum (sqrt(I) - sqrt(target))^2 */
+  void* ready_event;          /* optional cudaEvent_t: the job's inputs are ready once it completes */
+} ptyro_job_desc;
+
+/* Device scratch bytes a job takes from the arena while it runs (0 if invalid). */
+size_t ptyro_sched_job_bytes(const ptyro_job_desc* d);
+
+/* New scheduler on `device` (must be current) with `arena` (DEVICE, 256-byte
+ * aligned) as its only device memory and at most `max_slots` wave slots in flight. */
+int ptyro_sched_create(int32_t device, void* arena, size_t arena_bytes, int32_t max_slots, ptyro_sched** out);
+
+/* Waits for all issued work and frees the scheduler's host resources. */
+int ptyro_sched_destroy(ptyro_sched* s);
+
+/* Queue a job (copied); `*id` identifies it. Invalid jobs, and jobs larger than
+ * the arena, are rejected here. Thread-safe. */
+int ptyro_sched_submit(ptyro_sched* s, const ptyro_job_desc* d, int64_t* id);
+
+/* Cancel a queued or running job (running: no further passes are issued). */
+int ptyro_sched_cancel(ptyro_sched* s, int64_t id);
+
+/* Retire finished jobs, admit queued ones, issue one pass of every running job. */
+int ptyro_sched_step(ptyro_sched* s, int32_t* running, int32_t* queued);
+
+/* PTYRO_JOB_* state of a job. Thread-safe. */
+int ptyro_sched_job_state(ptyro_sched* s, int64_t id, int32_t* state);
+
+/* Forget a finished job. */
+int ptyro_sched_release(ptyro_sched* s, int64_t id);
+
+/* Free arena bytes and free wave slots. */
+int ptyro_sched_memory(ptyro_sched* s, size_t* free_bytes, int32_t* free_slots);
+
 /* Bytes of the fixed device scratch array behind ptyro_ms_forward_noalloc. */
 #define PTYRO_STATIC_SCRATCH_BYTES (64u * 1024u * 1024u)
 

@@ -38,7 +38,20 @@ EXPORTED_SYMBOLS = (
     "ptyro_ms_forward_ckpt",
     "ptyro_ms_backward_workspace_bytes",
     "ptyro_ms_backward",
+    "ptyro_sched_job_bytes",
+    "ptyro_sched_create",
+    "ptyro_sched_destroy",
+    "ptyro_sched_submit",
+    "ptyro_sched_cancel",
+    "ptyro_sched_step",
+    "ptyro_sched_job_state",
+    "ptyro_sched_release",
+    "ptyro_sched_memory",
 )
+
+PTYRO_JOB_FORWARD = 0
+PTYRO_JOB_GRADIENT = 1
+JOB_QUEUED, JOB_RUNNING, JOB_DONE, JOB_FAILED, JOB_CANCELLED = 0, 1, 2, 3, 4
 
 
 class MsParams(ctypes.Structure):
@@ -64,6 +77,26 @@ class MsParams(ctypes.Structure):
         ("mode_stride_x", ctypes.c_int64),
         ("mode_stride_m", ctypes.c_int64),
         ("windows", ctypes.c_void_p),
+    ]
+
+
+class JobDesc(ctypes.Structure):
+    """Mirror of ``ptyro_job_desc``."""
+
+    _fields_ = [
+        ("p", MsParams),
+        ("kind", ctypes.c_int32),
+        ("ckpt_every", ctypes.c_int32),
+        ("potential", ctypes.c_void_p),
+        ("modes", ctypes.c_void_p),
+        ("weights", ctypes.c_void_p),
+        ("positions", ctypes.c_void_p),
+        ("patterns", ctypes.c_void_p),
+        ("targets", ctypes.c_void_p),
+        ("grad_potential", ctypes.c_void_p),
+        ("grad_modes", ctypes.c_void_p),
+        ("loss", ctypes.c_void_p),
+        ("ready_event", ctypes.c_void_p),
     ]
 
 
@@ -112,6 +145,25 @@ def _declare(lib) -> None:
     lib.ptyro_ms_backward_workspace_bytes.argtypes = [pp]
     lib.ptyro_ms_backward.restype = ctypes.c_int
     lib.ptyro_ms_backward.argtypes = [pp, i32, vp, vp, vp, vp, vp, vp, vp, vp, sz, vp]
+    jd = ctypes.POINTER(JobDesc)
+    lib.ptyro_sched_job_bytes.restype = sz
+    lib.ptyro_sched_job_bytes.argtypes = [jd]
+    lib.ptyro_sched_create.restype = ctypes.c_int
+    lib.ptyro_sched_create.argtypes = [i32, vp, sz, i32, ctypes.POINTER(vp)]
+    lib.ptyro_sched_destroy.restype = ctypes.c_int
+    lib.ptyro_sched_destroy.argtypes = [vp]
+    lib.ptyro_sched_submit.restype = ctypes.c_int
+    lib.ptyro_sched_submit.argtypes = [vp, jd, ctypes.POINTER(ctypes.c_int64)]
+    lib.ptyro_sched_cancel.restype = ctypes.c_int
+    lib.ptyro_sched_cancel.argtypes = [vp, ctypes.c_int64]
+    lib.ptyro_sched_step.restype = ctypes.c_int
+    lib.ptyro_sched_step.argtypes = [vp, ctypes.POINTER(i32), ctypes.POINTER(i32)]
+    lib.ptyro_sched_job_state.restype = ctypes.c_int
+    lib.ptyro_sched_job_state.argtypes = [vp, ctypes.c_int64, ctypes.POINTER(i32)]
+    lib.ptyro_sched_release.restype = ctypes.c_int
+    lib.ptyro_sched_release.argtypes = [vp, ctypes.c_int64]
+    lib.ptyro_sched_memory.restype = ctypes.c_int
+    lib.ptyro_sched_memory.argtypes = [vp, ctypes.POINTER(sz), ctypes.POINTER(i32)]
     lib.ptyro_ms_forward_noalloc.restype = ctypes.c_int
     lib.ptyro_ms_forward_noalloc.argtypes = [pp, vp, vp, vp, vp, vp, vp]
 

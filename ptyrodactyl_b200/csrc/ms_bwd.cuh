@@ -68,8 +68,8 @@ __device__ __forceinline__ void bwd_load(const BwdArgs& a, const float2* w, floa
   }
 }
 
-template <int N1, int N2, int AXIS, int WARPS, int MINB>
-__global__ void __launch_bounds__(WARPS * 32, MINB) ms_bwd_pass_kernel(BwdArgs a) {
+template <int N1, int N2, int AXIS, int WARPS>
+__device__ __forceinline__ void bwd_body(const BwdArgs& a, const int slot) {
   using Geo = PassGeom<N1, N2>;
   using LB = LineBuf<N1, N2>;
   constexpr int N = Geo::N;
@@ -93,7 +93,6 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) ms_bwd_pass_kernel(BwdArgs a
   const int line = line0 + lc;
   float2* buf = work + lc * LB::kSize;
   const size_t NN = (size_t)N * N;
-  const int slot = blockIdx.y;
   const int b = slot / a.n_modes, m = slot % a.n_modes;
   auto off = [&](int e) -> size_t { return AXIS == 0 ? (size_t)line * N + e : (size_t)e * N + line; };
 
@@ -234,6 +233,20 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) ms_bwd_pass_kernel(BwdArgs a
       }
     }
   }
+}
+
+
+template <int N1, int N2, int AXIS, int WARPS, int MINB>
+__global__ void __launch_bounds__(WARPS * 32, MINB) ms_bwd_pass_kernel(BwdArgs a) {
+  bwd_body<N1, N2, AXIS, WARPS>(a, blockIdx.y);
+}
+
+// Adjoint passes of several jobs in one launch (see ms_pass_multi_kernel).
+template <int N1, int N2, int AXIS, int WARPS, int MINB>
+__global__ void __launch_bounds__(WARPS * 32, MINB) ms_bwd_multi_kernel(const BwdArgs* __restrict__ descs,
+                                                                        const int2* __restrict__ rows) {
+  const int2 r = rows[blockIdx.y];
+  bwd_body<N1, N2, AXIS, WARPS>(descs[r.x], r.y);
 }
 
 }  // namespace ptyro

@@ -140,9 +140,10 @@ __device__ __forceinline__ bool apply_op(int op, float2 (&v)[N2], int t, float2*
   return false;
 }
 
-// MINB: resident CTAs per SM the register allocation must allow (occupancy variant).
-template <int N1, int N2, int AXIS, int WARPS, int MINB>
-__global__ void __launch_bounds__(WARPS * 32, MINB) ms_pass_kernel(PassArgs a) {
+// The pass on wave slot `yslot` of the job described by `a` (one CTA per
+// (line tile, slot); for pattern passes the slot index is the probe index).
+template <int N1, int N2, int AXIS, int WARPS>
+__device__ __forceinline__ void pass_body(const PassArgs& a, const int yslot) {
   using Geo = PassGeom<N1, N2>;
   using LB = LineBuf<N1, N2>;
   constexpr int N = Geo::N;
@@ -178,14 +179,14 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) ms_pass_kernel(PassArgs a) {
   bool korder = false;
 
   for (int m = 0; m < mcount; ++m) {
-    const int slot = to_pattern ? blockIdx.y * a.n_modes + m : blockIdx.y;
+    const int slot = to_pattern ? yslot * a.n_modes + m : yslot;
     float2* w = a.wave + (size_t)slot * NN;
     float2 v[N2];
     const bool load_k = a.src == SRC_PROBE || a.op1 == OP_IFFT;
     // ---- load
     if (a.src == SRC_PROBE) {
-      const int b = blockIdx.y / a.n_modes;
-      const int mode = blockIdx.y % a.n_modes;
+      const int b = yslot / a.n_modes;
+      const int mode = yslot % a.n_modes;
       const float2* pk = a.probe_k + (size_t)mode * NN;
       const float2 rl = AXIS == 0 ? a.ramp_y[(size_t)b * N + line] : a.ramp_x[(size_t)b * N + line];
       const float2* ra = (AXIS == 0 ? a.ramp_x : a.ramp_y) + (size_t)b * N;
@@ -228,7 +229,7 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) ms_pass_kernel(PassArgs a) {
     // ---- transmission (natural distribution; row-major table for rows, transposed for columns)
     if (a.t_slice >= 0) {
       int eoff;
-      const float2* T = trans_row<AXIS>(a.trans, a.trans_t, a.field_n, a.t_slice, a.win, blockIdx.y / a.n_modes,
+      const float2* T = trans_row<AXIS>(a.trans, a.trans_t, a.field_n, a.t_slice, a.win, yslot / a.n_modes,
                                         line, &eoff);
       const int fm = a.field_n - 1;
 #pragma unroll
@@ -277,7 +278,7 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) ms_pass_kernel(PassArgs a) {
   }
   if (to_pattern) {
     // fftshift on store: frequency index k lands at (k + N/2) mod N on both axes.
-    float* out = a.pattern + (size_t)blockIdx.y * NN;
+    float* out = a.pattern + (size_t)yslot * NN;
     if (AXIS == 0) {
       const int ls = (line + N / 2) % N;
 #pragma unroll
@@ -299,6 +300,23 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) ms_pass_kernel(PassArgs a) {
       }
     }
   }
+}
+
+
+// MINB: resident CTAs per SM the register allocation must allow (occupancy variant).
+template <int N1, int N2, int AXIS, int WARPS, int MINB>
+__global__ void __launch_bounds__(WARPS * 32, MINB) ms_pass_kernel(PassArgs a) {
+  pass_body<N1, N2, AXIS, WARPS>(a, blockIdx.y);
+}
+
+// Passes of several jobs in one launch: CTA row y works on slot rows[y].y of the
+// job whose arguments are descs[rows[y].x]. Jobs may differ in potential, probe,
+// slice count and progress; they share the grid edge and the axis.
+template <int N1, int N2, int AXIS, int WARPS, int MINB>
+__global__ void __launch_bounds__(WARPS * 32, MINB) ms_pass_multi_kernel(const PassArgs* __restrict__ descs,
+                                                                         const int2* __restrict__ rows) {
+  const int2 r = rows[blockIdx.y];
+  pass_body<N1, N2, AXIS, WARPS>(descs[r.x], r.y);
 }
 
 }  // namespace ptyro

@@ -13,7 +13,7 @@ extern std::atomic<unsigned long long> g_launches;
 template <int N1, int N2, int AXIS, int MINB>
 int launch_pass_t(const PassArgs& a, int grid_y, cudaStream_t st) {
   using Geo = PassGeom<N1, N2>;
-  constexpr int N = Geo::N, G = Geo::G;
+  constexpr int N = Geo::N;
   constexpr int W = Geo::kWarps;
   const size_t smem = Geo::smem_bytes(W);
   static bool attr_done = false;  // once per template instance
@@ -47,6 +47,41 @@ int launch_bwd_t(const BwdArgs& a, int grid_y, cudaStream_t st) {
   return (int)cudaGetLastError();
 }
 
+template <int N1, int N2, int AXIS, int MINB>
+int launch_pass_multi_t(const PassArgs* descs, const int2* rows, int nrows, cudaStream_t st) {
+  using Geo = PassGeom<N1, N2>;
+  constexpr int W = Geo::kWarps;
+  const size_t smem = Geo::smem_bytes(W);
+  static bool attr_done = false;
+  if (!attr_done) {
+    cudaFuncSetAttribute(ms_pass_multi_kernel<N1, N2, AXIS, W, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)smem);
+    attr_done = true;
+  }
+  dim3 grid(Geo::N / Geo::kLines, nrows);
+  ms_pass_multi_kernel<N1, N2, AXIS, W, MINB><<<grid, W * 32, smem, st>>>(descs, rows);
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  return (int)cudaGetLastError();
+}
+
+template <int N1, int N2, int AXIS>
+int launch_bwd_multi_t(const BwdArgs* descs, const int2* rows, int nrows, cudaStream_t st) {
+  using Geo = PassGeom<N1, N2>;
+  constexpr int W = Geo::kWarps;
+  constexpr int MINB = N2 <= 16 ? 2 : 1;
+  const size_t smem = Geo::smem_bytes(W);
+  static bool attr_done = false;
+  if (!attr_done) {
+    cudaFuncSetAttribute(ms_bwd_multi_kernel<N1, N2, AXIS, W, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)smem);
+    attr_done = true;
+  }
+  dim3 grid(Geo::N / Geo::kLines, nrows);
+  ms_bwd_multi_kernel<N1, N2, AXIS, W, MINB><<<grid, W * 32, smem, st>>>(descs, rows);
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  return (int)cudaGetLastError();
+}
+
 // variant bit (1 << axis) selects the 3-CTAs-per-SM register budget where the
 // shape allows it (N2 <= 16); otherwise 2 (N2 <= 16) or 1 (N2 = 32) CTAs per SM.
 #define PTYRO_DEFINE_PASS_LAUNCHER(NN, N1, N2)                                                   \
@@ -59,8 +94,33 @@ int launch_bwd_t(const BwdArgs& a, int grid_y, cudaStream_t st) {
   }                                                                                              \
   int launch_bwd_##NN(int axis, const BwdArgs& a, int grid_y, cudaStream_t st) {                \
     return axis == 0 ? launch_bwd_t<N1, N2, 0>(a, grid_y, st) : launch_bwd_t<N1, N2, 1>(a, grid_y, st); \
+  }                                                                                              \
+  int launch_pass_multi_##NN(int axis, const PassArgs* d, const int2* r, int nr, cudaStream_t st,  \
+                             int variant) {                                                      \
+    constexpr int lo = (N2) <= 16 ? 2 : 1, hi = (N2) <= 16 ? 3 : 1;                              \
+    const bool occ = (variant >> axis) & 1;                                                      \
+    if (axis == 0)                                                                               \
+      return occ ? launch_pass_multi_t<N1, N2, 0, hi>(d, r, nr, st) : launch_pass_multi_t<N1, N2, 0, lo>(d, r, nr, st); \
+    return occ ? launch_pass_multi_t<N1, N2, 1, hi>(d, r, nr, st) : launch_pass_multi_t<N1, N2, 1, lo>(d, r, nr, st);   \
+  }                                                                                              \
+  int launch_bwd_multi_##NN(int axis, const BwdArgs* d, const int2* r, int nr, cudaStream_t st) {  \
+    return axis == 0 ? launch_bwd_multi_t<N1, N2, 0>(d, r, nr, st) : launch_bwd_multi_t<N1, N2, 1>(d, r, nr, st); \
   }
 
+int launch_pass_multi_16(int axis, const PassArgs* d, const int2* r, int nr, cudaStream_t st, int variant);
+int launch_bwd_multi_16(int axis, const BwdArgs* d, const int2* r, int nr, cudaStream_t st);
+int launch_pass_multi_32(int axis, const PassArgs* d, const int2* r, int nr, cudaStream_t st, int variant);
+int launch_bwd_multi_32(int axis, const BwdArgs* d, const int2* r, int nr, cudaStream_t st);
+int launch_pass_multi_64(int axis, const PassArgs* d, const int2* r, int nr, cudaStream_t st, int variant);
+int launch_bwd_multi_64(int axis, const BwdArgs* d, const int2* r, int nr, cudaStream_t st);
+int launch_pass_multi_128(int axis, const PassArgs* d, const int2* r, int nr, cudaStream_t st, int variant);
+int launch_bwd_multi_128(int axis, const BwdArgs* d, const int2* r, int nr, cudaStream_t st);
+int launch_pass_multi_256(int axis, const PassArgs* d, const int2* r, int nr, cudaStream_t st, int variant);
+int launch_bwd_multi_256(int axis, const BwdArgs* d, const int2* r, int nr, cudaStream_t st);
+int launch_pass_multi_512(int axis, const PassArgs* d, const int2* r, int nr, cudaStream_t st, int variant);
+int launch_bwd_multi_512(int axis, const BwdArgs* d, const int2* r, int nr, cudaStream_t st);
+int launch_pass_multi_1024(int axis, const PassArgs* d, const int2* r, int nr, cudaStream_t st, int variant);
+int launch_bwd_multi_1024(int axis, const BwdArgs* d, const int2* r, int nr, cudaStream_t st);
 int launch_bwd_16(int axis, const BwdArgs& a, int grid_y, cudaStream_t st);
 int launch_bwd_32(int axis, const BwdArgs& a, int grid_y, cudaStream_t st);
 int launch_bwd_64(int axis, const BwdArgs& a, int grid_y, cudaStream_t st);
