@@ -323,6 +323,30 @@ def run_ours(args, rank, world, local_rank):
         e2e = {"value": float(P) * S * k2 * world / (e2e_ms * 1e-3), "unit": UNIT,
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(P * n * n * 4), "steps": k2}
 
+    # the plain per-position path (one kernel per stage, one probe at a time) on a sample
+    plain_probes = 8
+    out_p = torch.empty((plain_probes, n, n), dtype=torch.float32, device=dev)
+    pp = ms_params(n, S, 1, plain_probes, w.voltage_kv, synth.SLICE_DZ, w.calib, w.calib, slices_d.stride(),
+                   modes_d.stride())
+    pws_b = lib.ptyro_ms_workspace_bytes(ctypes.byref(pp))
+    pws = torch.empty(pws_b, dtype=torch.uint8, device=dev)
+
+    def plain_step():
+        _lib.check(lib.ptyro_ms_forward_plain(ctypes.byref(pp), slices_d.data_ptr(), modes_d.data_ptr(),
+                                              weights_d.data_ptr(), pos_d.data_ptr(), out_p.data_ptr(),
+                                              pws.data_ptr(), pws_b, stream.cuda_stream))
+
+    plain_step()
+    torch.cuda.synchronize()
+    s, e = _events(torch, 2)
+    s.record(stream)
+    for _ in range(3):
+        plain_step()
+    e.record(stream)
+    torch.cuda.synchronize()
+    plain_value = 3.0 * plain_probes * S / (s.elapsed_time(e) * 1e-3)
+    del pws
+
     cpu_baseline = None
     if cpu is not None:
         upd, wall = 0, 0.0
@@ -353,6 +377,8 @@ def run_ours(args, rank, world, local_rank):
                          "hbm_achieved_gbs": bytes_per_launch / avg_pass_s / 1e9,
                          "hbm_algorithmic_bytes_per_launch": bytes_per_launch},
             "e2e": e2e,
+            "plain_per_position": {"value": plain_value, "unit": UNIT, "probes_sampled": plain_probes,
+                                   "fused_over_plain": value / plain_value},
             "gpu_launches": int(launches),
             "clocks": clk,
             "cpu_baseline": cpu_baseline,
@@ -492,6 +518,57 @@ def run_grad(args, rank, world, local_rank):
         print(json.dumps(line), flush=True)
 
 
+# ----------------------------------------------------------------------------- 512^2 leg
+def run_config3(args, rank, world, local_rank):
+    """512^2 grid, 32x32 cell, 100 slices, frozen-phonon average of 4 configurations,
+    on a sample of the 128x128 scan (``--probes``); one JSON line."""
+    import torch
+    import ptyrodactyl_b200 as pb
+
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    w = synth.CONFIG3
+    n, S = w.n, w.num_slices
+    pos_all = synth.raster_positions(w)
+    idx = np.linspace(0, pos_all.shape[0] - 1, args.probes).astype(np.int64)
+    pos = torch.as_tensor(pos_all[idx], device=dev).contiguous()
+    pots = [torch.as_tensor(synth.potential_slices(w, phonon=k), device=dev) for k in range(w.phonon_configs)]
+    mic = pb.create_microscope_config(w.voltage_kv, w.aperture_mrad, probe_shape=(n, n))
+    modes = pb.make_probe(mic, pb.create_detector_config(w.calib))[..., None].contiguous()
+    wq = torch.full((1,), 1.0 / len(pots), dtype=torch.float32, device=dev)
+    out = torch.zeros((args.probes, n, n), dtype=torch.float32, device=dev)
+
+    def step():
+        out.zero_()
+        for v in pots:
+            pb.run_forward(v, synth.SLICE_DZ, modes, wq, pos, w.voltage_kv, w.calib, w.calib, out=out,
+                           accumulate=True, batch=args.batch)
+
+    for _ in range(max(1, args.warmup // 3)):
+        step()
+    torch.cuda.synchronize()
+    s, e = _events(torch, 2)
+    reps = max(1, args.steps // 10)
+    s.record()
+    for _ in range(reps):
+        step()
+    e.record()
+    torch.cuda.synchronize()
+    ms = s.elapsed_time(e) / reps
+    updates = float(args.probes) * S * len(pots)
+    sums = out.sum(dim=(1, 2))
+    n_ap = float(_aperture_mask(w).sum())
+    line = {"metric": "probe-slice updates/s at 512^2 (100 slices, 4 frozen-phonon configurations averaged)",
+            "mode": "config3", "value": updates / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms,
+            "tflops_algorithmic": updates / (ms * 1e-3) * synth.algorithmic_flops_per_update(n) / 1e12,
+            "n_gpus": world, "dtype": "f32", "data": "synthetic",
+            "checks": {"pattern_sum_max_rel_err": float(((sums - n_ap).abs().max() / n_ap).item())},
+            "config": {"workload": w.name, "grid": n, "slices": S, "probes_sampled": args.probes,
+                       "probes_full_scan": w.num_probes, "phonon_configs": len(pots), "batch": args.batch}}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 # ----------------------------------------------------------------------------- serving leg
 def run_serve(args, rank, world, local_rank):
     """Poisson-arrival mix of simulations and gradient solves through the server;
@@ -606,7 +683,8 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--mode", choices=("forward", "grad", "serve"), default="forward")
+    ap.add_argument("--mode", choices=("forward", "grad", "serve", "config3"), default="forward")
+    ap.add_argument("--probes", type=int, default=2048, help="config3 mode: scan positions sampled")
     ap.add_argument("--requests", type=int, default=64, help="serve mode: requests in the mix")
     ap.add_argument("--rate", type=float, default=20.0, help="serve mode: Poisson arrival rate (1/s)")
     ap.add_argument("--seed", type=int, default=5, help="serve mode: mix seed")
@@ -633,6 +711,8 @@ def main():
             run_grad(args, rank, world, local_rank)
         elif args.mode == "serve":
             run_serve(args, rank, world, local_rank)
+        elif args.mode == "config3":
+            run_config3(args, rank, world, local_rank)
         else:
             run_ours(args, rank, world, local_rank)
     finally:

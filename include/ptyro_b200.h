@@ -30,6 +30,11 @@ extern "C" {
 #define PTYRO_ERR_CUDA 3        /* a launch failed */
 #define PTYRO_ERR_UNSUPPORTED 4 /* grid size outside the compiled set */
 
+/* ptyro_ms_params.flags: add sum_m w_m |A_m|^2 into `patterns` instead of
+ * overwriting them (frozen-phonon averaging: one forward per configuration with
+ * weights scaled by 1/configurations; the plain and gradient paths ignore it). */
+#define PTYRO_FLAG_ACCUMULATE 1
+
 /* Geometry and physics scalars of one multislice job.
  * The potential is V[y][x][s] with element strides pot_stride_{y,x,s} (the
  * reference stores slices last, PotentialSlices.slices (H, W, S)); the beam is
@@ -46,7 +51,7 @@ typedef struct ptyro_ms_params {
   int32_t field_n;             /* 0, or edge F of a larger periodic potential field (power of
                                   two, n <= F <= 8192) from which every probe reads an n x n
                                   window; the potential (and its gradient) is then F x F x S */
-  int32_t reserved;
+  int32_t flags;               /* PTYRO_FLAG_* bits */
   double voltage_kv;           /* MicroscopeConfig.voltage_kv */
   double slice_thickness_ang;  /* PotentialSlices.slice_thickness */
   double calib_ang;            /* min(PotentialSlices.calib, ProbeModes.calib): propagator grid */

@@ -28,6 +28,7 @@ from .simulations import (  # noqa: F401
     relativistic_wavelength_ang,
     run_forward,
     stem_4d,
+    stem_4d_frozen_phonon,
     stem_4d_windowed,
 )
 

@@ -19,6 +19,7 @@ PTYRO_ERR_WORKSPACE = 2
 PTYRO_ERR_CUDA = 3
 PTYRO_ERR_UNSUPPORTED = 4
 STATIC_SCRATCH_BYTES = 64 << 20  # PTYRO_STATIC_SCRATCH_BYTES
+PTYRO_FLAG_ACCUMULATE = 1
 
 # every symbol include/ptyro_b200.h declares
 EXPORTED_SYMBOLS = (
@@ -65,7 +66,7 @@ class MsParams(ctypes.Structure):
         ("batch", ctypes.c_int32),
         ("tune", ctypes.c_int32),
         ("field_n", ctypes.c_int32),
-        ("reserved", ctypes.c_int32),
+        ("flags", ctypes.c_int32),
         ("voltage_kv", ctypes.c_double),
         ("slice_thickness_ang", ctypes.c_double),
         ("calib_ang", ctypes.c_double),

@@ -423,6 +423,7 @@ static FwdPlan fwd_pass_plan(const ptyro_ms_params* p, const FwdBuffers& B, cons
   } else {  // last axis of the FFT2, |.|^2, fftshifted store
     a.src = SRC_WAVE; a.op1 = OP_FFT; a.t_slice = -1; a.op2 = OP_NONE; a.dst = DST_PATTERN;
     a.pattern = patterns + (size_t)b0 * nn;
+    a.accumulate = (p->flags & PTYRO_FLAG_ACCUMULATE) != 0;
     if (res_base) a.amp_store = res_base + (size_t)C * nn;
     r.axis = (S + 1) % 2;
     r.rows = nb;

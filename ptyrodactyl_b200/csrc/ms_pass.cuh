@@ -49,6 +49,7 @@ struct PassArgs {
   float2* ckpt_store;
   float2* amp_store;
   size_t res_stride;
+  int accumulate;          // pattern pass adds into the output instead of overwriting it
 };
 
 template <int N1, int N2>
@@ -284,7 +285,8 @@ __device__ __forceinline__ void pass_body(const PassArgs& a, const int yslot) {
 #pragma unroll
       for (int r = 0; r < N2; ++r) {
         const int ks = (korder_index<N1, N2>(t, r) + N / 2) % N;
-        out[(size_t)ls * N + ks] = acc[r];
+        const size_t o = (size_t)ls * N + ks;
+        out[o] = a.accumulate ? out[o] + acc[r] : acc[r];
       }
     } else {
       float* tile = reinterpret_cast<float*>(work);
@@ -296,7 +298,8 @@ __device__ __forceinline__ void pass_body(const PassArgs& a, const int yslot) {
       for (int it = 0; it < kTileIters; ++it) {
         const int i = threadIdx.x + it * WARPS * 32;
         const int rr = i / lines, c = i % lines;
-        out[(size_t)((rr + N / 2) % N) * N + (line0 + c + N / 2) % N] = tile[rr * pitch + c];
+        const size_t o = (size_t)((rr + N / 2) % N) * N + (line0 + c + N / 2) % N;
+        out[o] = a.accumulate ? out[o] + tile[rr * pitch + c] : tile[rr * pitch + c];
       }
     }
   }

@@ -87,8 +87,9 @@ def _workspace(nbytes: int, device: torch.device) -> torch.Tensor:
 def ms_params(n: int, num_slices: int, num_modes: int, num_probes: int, voltage_kv: float,
               slice_thickness: float, calib_ang: float, shift_calib_ang: float,
               pot_strides=(0, 0, 0), mode_strides=(0, 0, 0), batch: int = 0, tune: int = 0,
-              field_n: int = 0, windows: Optional[torch.Tensor] = None) -> _lib.MsParams:
+              field_n: int = 0, windows: Optional[torch.Tensor] = None, flags: int = 0) -> _lib.MsParams:
     p = _lib.MsParams()
+    p.flags = int(flags)
     p.n, p.num_slices, p.num_modes, p.num_probes, p.batch = n, num_slices, num_modes, num_probes, batch
     p.tune = tune
     p.field_n = 0 if field_n == n else int(field_n)
@@ -124,22 +125,24 @@ def check_windows(slices: torch.Tensor, modes: torch.Tensor, windows: Optional[t
 def run_forward(slices: torch.Tensor, slice_thickness: float, modes: torch.Tensor, weights: torch.Tensor,
                 positions: torch.Tensor, voltage_kv: float, calib_ang: float, shift_calib_ang: float,
                 out: Optional[torch.Tensor] = None, batch: int = 0, plain: bool = False,
-                tune: int = 0, windows: Optional[torch.Tensor] = None) -> torch.Tensor:
+                tune: int = 0, windows: Optional[torch.Tensor] = None, accumulate: bool = False) -> torch.Tensor:
     """Device-level forward: all tensors already on one CUDA device.
 
     slices (F, F, S) float32 (any strides), modes (n, n, M) complex64 (any strides),
     weights (M,) float32, positions (P, 2) float64 contiguous. F == n, or F > n with
     ``windows`` (P, 2) int32: probe p then reads the n x n window of the periodic
-    field starting at windows[p]. Returns patterns (P, n, n) float32.
+    field starting at windows[p]. Returns patterns (P, n, n) float32; with
+    ``accumulate`` the intensities are added into ``out`` instead.
     """
     lib = _lib.load()
     dev = slices.device
     num_probes = positions.shape[0]
     n, f = check_windows(slices, modes, windows, num_probes)
     prm = ms_params(n, slices.shape[2], modes.shape[2], num_probes, voltage_kv, slice_thickness,
-                    calib_ang, shift_calib_ang, slices.stride(), modes.stride(), batch, tune, f, windows)
+                    calib_ang, shift_calib_ang, slices.stride(), modes.stride(), batch, tune, f, windows,
+                    _lib.PTYRO_FLAG_ACCUMULATE if accumulate else 0)
     if out is None:
-        out = torch.empty((num_probes, n, n), dtype=torch.float32, device=dev)
+        out = (torch.zeros if accumulate else torch.empty)((num_probes, n, n), dtype=torch.float32, device=dev)
     if num_probes == 0:
         return out
     ws_bytes = lib.ptyro_ms_workspace_bytes(ctypes.byref(prm))
@@ -220,6 +223,31 @@ def stem_4d_windowed(pot_slice: PotentialSlices, beam: ProbeModes, microscope: M
     fourier_calib = 1.0 / (modes.shape[0] * calib)
     scan_positions = detector.scan_positions_px.to(torch.float64) * detector.real_space_calib_ang
     return create_stem4d(data, detector.real_space_calib_ang, fourier_calib, scan_positions, microscope.voltage_kv)
+
+
+def stem_4d_frozen_phonon(pot_slices: list, beam: ProbeModes, microscope: MicroscopeConfig,
+                          detector: DetectorConfig) -> STEM4D:
+    """Mean of ``stem_4d`` over frozen-phonon configurations (one PotentialSlices per
+    configuration, same geometry). Each configuration's intensities are added into
+    the output by the pattern pass with the mode weights scaled by 1/configurations."""
+    if not pot_slices:
+        raise ValueError("at least one potential configuration is required")
+    if detector.scan_positions_px is None:
+        raise ValueError("detector.scan_positions_px is required")
+    dev = _device(pot_slices[0].slices.device if pot_slices[0].slices.is_cuda else None)
+    modes, weights = _beam_on(beam, dev)
+    wscaled = (weights / len(pot_slices)).contiguous()
+    positions = as_tensor(detector.scan_positions_px, torch.float64, dev).reshape(-1, 2).contiguous()
+    n = modes.shape[0]
+    out = torch.zeros((positions.shape[0], n, n), dtype=torch.float32, device=dev)
+    calib = min(float(pot_slices[0].calib), float(beam.calib))
+    for ps in pot_slices:
+        slices = as_tensor(ps.slices, torch.float32, dev)
+        run_forward(slices, ps.slice_thickness, modes, wscaled, positions, microscope.voltage_kv, calib,
+                    detector.real_space_calib_ang, out=out, accumulate=True)
+    fourier_calib = 1.0 / (n * calib)
+    scan_positions = detector.scan_positions_px.to(torch.float64) * detector.real_space_calib_ang
+    return create_stem4d(out, detector.real_space_calib_ang, fourier_calib, scan_positions, microscope.voltage_kv)
 
 
 def cbed_image(pot_slices: PotentialSlices, beam: ProbeModes, microscope: MicroscopeConfig) -> CalibratedArray:

@@ -165,3 +165,18 @@ def test_errors_raise_value_error():
     det2 = pb.create_detector_config(0.2)
     with pytest.raises(ValueError, match="scan_positions_px is required"):
         pb.stem_4d(slices, beam, mic, det2)
+
+
+def test_frozen_phonon_average_matches_oracle_mean():
+    w = synth.CONFIG1
+    pots = [synth.potential_slices(w, phonon=k, num_slices=4) for k in range(3)]
+    probe = R.make_probe(w.voltage_kv, w.aperture_mrad, (w.n, w.n), w.calib * 100.0)
+    pos = synth.raster_positions(w)[:5]
+    mic = pb.create_microscope_config(w.voltage_kv, w.aperture_mrad, probe_shape=(w.n, w.n))
+    det = pb.create_detector_config(w.calib, scan_positions_px=pos)
+    beam = pb.create_probe_modes(probe[..., None], [1.0], w.calib)
+    got = pb.stem_4d_frozen_phonon([pb.create_potential_slices(p, synth.SLICE_DZ, w.calib) for p in pots], beam,
+                                   mic, det).data.cpu().numpy()
+    want = np.mean([R.stem_4d(p, synth.SLICE_DZ, w.calib, probe[..., None], [1.0], w.calib, w.voltage_kv, pos,
+                              w.calib)["data"] for p in pots], axis=0)
+    assert rel_l2(got, want) < TOL_F64
