@@ -143,8 +143,15 @@ __device__ __forceinline__ bool apply_op(int op, float2 (&v)[N2], int t, float2*
 
 // The pass on wave slot `yslot` of the job described by `a` (one CTA per
 // (line tile, slot); for pattern passes the slot index is the probe index).
-template <int N1, int N2, int AXIS, int WARPS>
+// STEADY compiles the program of the middle slices (wave -> conv, x T, conv ->
+// wave) in as constants, so the branches of the other programs disappear.
+template <int N1, int N2, int AXIS, int WARPS, bool STEADY = false>
 __device__ __forceinline__ void pass_body(const PassArgs& a, const int yslot) {
+  const int src = STEADY ? (int)SRC_WAVE : a.src;
+  const int op1 = STEADY ? (int)OP_CONV : a.op1;
+  const int op2 = STEADY ? (int)OP_CONV : a.op2;
+  const int dst = STEADY ? (int)DST_WAVE : a.dst;
+  const bool has_t = STEADY ? true : a.t_slice >= 0;
   using Geo = PassGeom<N1, N2>;
   using LB = LineBuf<N1, N2>;
   constexpr int N = Geo::N;
@@ -172,7 +179,7 @@ __device__ __forceinline__ void pass_body(const PassArgs& a, const int yslot) {
   const size_t NN = (size_t)N * N;
   auto off = [&](int e) -> size_t { return AXIS == 0 ? (size_t)line * N + e : (size_t)e * N + line; };
 
-  const bool to_pattern = a.dst == DST_PATTERN;
+  const bool to_pattern = dst == DST_PATTERN;
   const int mcount = to_pattern ? a.n_modes : 1;
   float acc[N2];
 #pragma unroll
@@ -183,9 +190,9 @@ __device__ __forceinline__ void pass_body(const PassArgs& a, const int yslot) {
     const int slot = to_pattern ? yslot * a.n_modes + m : yslot;
     float2* w = a.wave + (size_t)slot * NN;
     float2 v[N2];
-    const bool load_k = a.src == SRC_PROBE || a.op1 == OP_IFFT;
+    const bool load_k = src == SRC_PROBE || op1 == OP_IFFT;
     // ---- load
-    if (a.src == SRC_PROBE) {
+    if (src == SRC_PROBE) {
       const int b = yslot / a.n_modes;
       const int mode = yslot % a.n_modes;
       const float2* pk = a.probe_k + (size_t)mode * NN;
@@ -219,16 +226,16 @@ __device__ __forceinline__ void pass_body(const PassArgs& a, const int yslot) {
     }
     korder = load_k;
     // ---- op1
-    if (a.op1 == OP_IFFT) {
+    if (op1 == OP_IFFT) {
       line_k_to_nat<N1, N2, +1>(v, t, buf, tw);
 #pragma unroll
       for (int j = 0; j < N2; ++j) v[j] = cscale(v[j], a.scale);
       korder = false;
-    } else if (a.op1 != OP_NONE) {
-      korder = apply_op<N1, N2>(a.op1, v, t, buf, tw, a.pf);
+    } else if (op1 != OP_NONE) {
+      korder = apply_op<N1, N2>(op1, v, t, buf, tw, a.pf);
     }
     // ---- transmission (natural distribution; row-major table for rows, transposed for columns)
-    if (a.t_slice >= 0) {
+    if (has_t) {
       int eoff;
       const float2* T = trans_row<AXIS>(a.trans, a.trans_t, a.field_n, a.t_slice, a.win, yslot / a.n_modes,
                                         line, &eoff);
@@ -245,7 +252,7 @@ __device__ __forceinline__ void pass_body(const PassArgs& a, const int yslot) {
       }
     }
     // ---- op2
-    if (a.op2 != OP_NONE) korder = apply_op<N1, N2>(a.op2, v, t, buf, tw, a.pf);
+    if (op2 != OP_NONE) korder = apply_op<N1, N2>(op2, v, t, buf, tw, a.pf);
     // ---- store
     if (to_pattern) {
       const float wm = a.weights[m];
@@ -307,9 +314,15 @@ __device__ __forceinline__ void pass_body(const PassArgs& a, const int yslot) {
 
 
 // MINB: resident CTAs per SM the register allocation must allow (occupancy variant).
-template <int N1, int N2, int AXIS, int WARPS, int MINB>
+template <int N1, int N2, int AXIS, int WARPS, int MINB, bool STEADY = false>
 __global__ void __launch_bounds__(WARPS * 32, MINB) ms_pass_kernel(PassArgs a) {
-  pass_body<N1, N2, AXIS, WARPS>(a, blockIdx.y);
+  pass_body<N1, N2, AXIS, WARPS, STEADY>(a, blockIdx.y);
+}
+
+// a pass running the middle-slice program (see pass_body's STEADY)
+inline bool is_steady_pass(const PassArgs& a) {
+  return a.src == SRC_WAVE && a.op1 == OP_CONV && a.op2 == OP_CONV && a.dst == DST_WAVE && a.t_slice >= 0 &&
+         !a.t_conj;
 }
 
 // Passes of several jobs in one launch: CTA row y works on slot rows[y].y of the

@@ -10,20 +10,20 @@ namespace ptyro {
 // Number of engine kernels enqueued by this process (all devices, all threads).
 extern std::atomic<unsigned long long> g_launches;
 
-template <int N1, int N2, int AXIS, int MINB>
-int launch_pass_t(const PassArgs& a, int grid_y, cudaStream_t st) {
+template <int N1, int N2, int AXIS, int MINB, bool STEADY>
+int launch_pass_s(const PassArgs& a, int grid_y, cudaStream_t st) {
   using Geo = PassGeom<N1, N2>;
   constexpr int N = Geo::N;
   constexpr int W = Geo::kWarps;
   const size_t smem = Geo::smem_bytes(W);
   static bool attr_done = false;  // once per template instance
   if (!attr_done) {
-    cudaFuncSetAttribute(ms_pass_kernel<N1, N2, AXIS, W, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaFuncSetAttribute(ms_pass_kernel<N1, N2, AXIS, W, MINB, STEADY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)smem);
     attr_done = true;
   }
   dim3 grid(N / Geo::kLines, grid_y);
-  ms_pass_kernel<N1, N2, AXIS, W, MINB><<<grid, W * 32, smem, st>>>(a);
+  ms_pass_kernel<N1, N2, AXIS, W, MINB, STEADY><<<grid, W * 32, smem, st>>>(a);
   g_launches.fetch_add(1, std::memory_order_relaxed);
   return (int)cudaGetLastError();
 }
@@ -45,6 +45,12 @@ int launch_bwd_t(const BwdArgs& a, int grid_y, cudaStream_t st) {
   ms_bwd_pass_kernel<N1, N2, AXIS, W, MINB><<<grid, W * 32, smem, st>>>(a);
   g_launches.fetch_add(1, std::memory_order_relaxed);
   return (int)cudaGetLastError();
+}
+
+template <int N1, int N2, int AXIS, int MINB>
+int launch_pass_t(const PassArgs& a, int grid_y, cudaStream_t st) {
+  return is_steady_pass(a) ? launch_pass_s<N1, N2, AXIS, MINB, true>(a, grid_y, st)
+                           : launch_pass_s<N1, N2, AXIS, MINB, false>(a, grid_y, st);
 }
 
 template <int N1, int N2, int AXIS, int MINB>
