@@ -46,8 +46,9 @@ typedef struct ptyro_ms_params {
   int32_t num_modes;           /* M >= 1 */
   int32_t num_probes;          /* P >= 0 scan positions */
   int32_t batch;               /* probes in flight per batch; 0 = automatic */
-  int32_t tune;                /* kernel variant bits (0 = default): bit a selects the
-                                  3-CTAs-per-SM register budget for passes along axis a */
+  int32_t tune;                /* kernel variant bits (0 = default): bit a (a = 0, 1) selects
+                                  the 3-CTAs-per-SM register budget for passes along axis a;
+                                  bit 2 the persistent double-buffered steady-pass kernel */
   int32_t field_n;             /* 0, or edge F of a larger periodic potential field (power of
                                   two, n <= F <= 8192) from which every probe reads an n x n
                                   window; the potential (and its gradient) is then F x F x S */

@@ -74,6 +74,16 @@ static __global__ void k_twiddle(int n, float2* tw) {
   tw[j] = make_float2((float)c, (float)s);
 }
 
+// twiddles in line-transform order: tw2[k2 * n1 + t] = exp(-2 pi i t k2 / n)
+static __global__ void k_twiddle2(int n, int n1, float2* tw2) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int k2 = i / n1, t = i % n1;
+  double s, c;
+  sincospi(-2.0 * (double)((t * k2) % n) / (double)n, &s, &c);
+  tw2[i] = make_float2((float)c, (float)s);
+}
+
 // 1-D factor of propagation_func (simulations.py:213-224): exp(-i pi lambda dz q^2) * scale
 static __global__ void k_propagator(int n, double calib, double lam_dz, double scale, float2* pf) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -266,7 +276,7 @@ static bool is_pow2(int n) { return n > 0 && (n & (n - 1)) == 0; }
 static int field_of(const ptyro_ms_params* p) { return p->field_n > 0 ? p->field_n : p->n; }
 
 struct Layout {
-  size_t tw, pf, trans, trans_t, probe_k, ramp_y, ramp_x, waves, p2, total;
+  size_t tw, tw2, pf, trans, trans_t, probe_k, ramp_y, ramp_x, waves, p2, total;
   int batch;
 };
 
@@ -286,6 +296,7 @@ static Layout layout_for(const ptyro_ms_params* p) {
                          : auto_batch(p);
   size_t o = 0;
   L.tw = o; o = align_up(o + 8 * (size_t)p->n);
+  L.tw2 = o; o = align_up(o + 8 * (size_t)p->n);
   L.pf = o; o = align_up(o + 8 * (size_t)p->n);
   const size_t ff = (size_t)field_of(p) * field_of(p);
   L.trans = o; o = align_up(o + 8 * ff * p->num_slices);
@@ -347,7 +358,10 @@ static int forward_setup(const ptyro_ms_params* p, const Layout& L, char* ws, co
   float2* T = (float2*)(ws + L.trans);
   float2* pk = (float2*)(ws + L.probe_k);
   const double lam = wavelength_ang(p->voltage_kv);
+  Shape sh;
+  shape_for(n, &sh);
   k_twiddle<<<(n + 255) / 256, 256, 0, st>>>(n, tw);
+  k_twiddle2<<<(n + 255) / 256, 256, 0, st>>>(n, sh.n1, (float2*)(ws + L.tw2));
   k_propagator<<<(n + 255) / 256, 256, 0, st>>>(n, p->calib_ang, lam * p->slice_thickness_ang, 1.0 / n, pf);
   const int F = field_of(p);
   k_transmission<<<blocks_for((size_t)F * F * p->num_slices, 256), 256, 0, st>>>(
@@ -355,7 +369,7 @@ static int forward_setup(const ptyro_ms_params* p, const Layout& L, char* ws, co
       interaction_sigma(p->voltage_kv), T, (float2*)(ws + L.trans_t));
   k_gather_modes<<<blocks_for(nn * p->num_modes, 256), 256, 0, st>>>(
       (const float2*)modes, p->mode_stride_y, p->mode_stride_x, p->mode_stride_m, n, p->num_modes, pk);
-  int rc = check_launch("forward setup", 4);
+  int rc = check_launch("forward setup", 5);
   if (rc) return rc;
   return fft2_planes(n, p->num_modes, false, pk, tw, st);
 }
@@ -370,7 +384,7 @@ struct FwdPlan {
 struct FwdBuffers {
   float2* waves;
   const float2* probe_k;
-  const float2 *ramp_y, *ramp_x, *trans, *trans_t, *pf, *tw;
+  const float2 *ramp_y, *ramp_x, *trans, *trans_t, *pf, *tw, *tw2;
 };
 
 static FwdBuffers fwd_buffers(const Layout& L, char* ws) {
@@ -383,6 +397,7 @@ static FwdBuffers fwd_buffers(const Layout& L, char* ws) {
   b.trans_t = (const float2*)(ws + L.trans_t);
   b.pf = (const float2*)(ws + L.pf);
   b.tw = (const float2*)(ws + L.tw);
+  b.tw2 = (const float2*)(ws + L.tw2);
   return b;
 }
 
@@ -401,6 +416,7 @@ static FwdPlan fwd_pass_plan(const ptyro_ms_params* p, const FwdBuffers& B, cons
   a.trans_t = B.trans_t;
   a.pf = B.pf;
   a.tw = B.tw;
+  a.tw2 = B.tw2;
   a.weights = weights;
   a.n_modes = M;
   a.scale = 1.0f / (float)n;

@@ -20,6 +20,21 @@
 
 namespace ptyro {
 
+// asynchronous global -> shared copies (completion tracked per thread by groups)
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem_src) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void* smem_dst, const void* gmem_src) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem_src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int PENDING>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(PENDING) : "memory");
+}
+
 enum SrcKind : int { SRC_WAVE = 0, SRC_PROBE = 1 };
 enum OpKind : int { OP_NONE = 0, OP_FFT = 1, OP_IFFT = 2, OP_CONV = 3, OP_CONV_CONJ = 4 };
 enum DstKind : int { DST_WAVE = 0, DST_PATTERN = 1 };
@@ -36,6 +51,7 @@ struct PassArgs {
 
   const float2* pf;        // (N) 1-D propagator factor along this axis, already divided by N
   const float2* tw;        // (N) forward twiddles exp(-2 pi i j / N)
+  const float2* tw2;       // (N) the same in the (k2, t) order the line transforms read: [k2 * N1 + t]
   float* pattern;          // (B, N, N) fftshifted intensity (DST_PATTERN)
   const float* weights;    // (M) incoherent mode weights (DST_PATTERN)
   int n_modes;
@@ -68,6 +84,8 @@ struct PassGeom {
     const size_t tile = (size_t)N * (lines + G);
     return sizeof(float2) * ((size_t)N + (xbuf > tile ? xbuf : tile));
   }
+  // steady passes also keep the transmission rows of their lines (prefetched)
+  static size_t smem_bytes_steady(int warps) { return smem_bytes(warps) + sizeof(float2) * (size_t)warps * G * N; }
 };
 
 // Column passes: copy the CTA's block of LINES columns (all N rows) between a plane
@@ -179,6 +197,19 @@ __device__ __forceinline__ void pass_body(const PassArgs& a, const int yslot) {
   const size_t NN = (size_t)N * N;
   auto off = [&](int e) -> size_t { return AXIS == 0 ? (size_t)line * N + e : (size_t)e * N + line; };
 
+  // steady passes without windows prefetch their transmission row into shared
+  // memory at the start; each thread copies exactly the elements it multiplies, so
+  // waiting for its own copies is enough (no barrier)
+  constexpr int kWork = (WARPS * G * LB::kSize > N * (WARPS * G + G)) ? WARPS * G * LB::kSize
+                                                                     : N * (WARPS * G + G);
+  float2* tpre = work + kWork + lc * N;
+  const bool pre = STEADY && a.win == nullptr && a.field_n == N;
+  if (pre) {
+    const float2* Trow = (AXIS == 0 ? a.trans : a.trans_t) + (size_t)a.t_slice * NN + (size_t)line * N;
+#pragma unroll
+    for (int j = 0; j < N2; ++j) cp_async8(tpre + t + N1 * j, Trow + t + N1 * j);
+    cp_async_commit();
+  }
   const bool to_pattern = dst == DST_PATTERN;
   const int mcount = to_pattern ? a.n_modes : 1;
   float acc[N2];
@@ -236,14 +267,20 @@ __device__ __forceinline__ void pass_body(const PassArgs& a, const int yslot) {
     }
     // ---- transmission (natural distribution; row-major table for rows, transposed for columns)
     if (has_t) {
-      int eoff;
-      const float2* T = trans_row<AXIS>(a.trans, a.trans_t, a.field_n, a.t_slice, a.win, yslot / a.n_modes,
-                                        line, &eoff);
-      const int fm = a.field_n - 1;
+      if (pre) {
+        cp_async_wait<0>();
 #pragma unroll
-      for (int j = 0; j < N2; ++j) {
-        const float2 tv = __ldg(T + ((t + N1 * j + eoff) & fm));
-        v[j] = a.t_conj ? cmulc(v[j], tv) : cmul(v[j], tv);
+        for (int j = 0; j < N2; ++j) v[j] = cmul(v[j], tpre[t + N1 * j]);
+      } else {
+        int eoff;
+        const float2* T = trans_row<AXIS>(a.trans, a.trans_t, a.field_n, a.t_slice, a.win, yslot / a.n_modes,
+                                          line, &eoff);
+        const int fm = a.field_n - 1;
+#pragma unroll
+        for (int j = 0; j < N2; ++j) {
+          const float2 tv = __ldg(T + ((t + N1 * j + eoff) & fm));
+          v[j] = a.t_conj ? cmulc(v[j], tv) : cmul(v[j], tv);
+        }
       }
       if (a.ckpt_store) {
         float2* ck = a.ckpt_store + (size_t)slot * a.res_stride;

@@ -4,6 +4,7 @@
 #include <atomic>
 
 #include "ms_bwd.cuh"
+#include "ms_pipe.cuh"
 
 namespace ptyro {
 
@@ -15,7 +16,7 @@ int launch_pass_s(const PassArgs& a, int grid_y, cudaStream_t st) {
   using Geo = PassGeom<N1, N2>;
   constexpr int N = Geo::N;
   constexpr int W = Geo::kWarps;
-  const size_t smem = Geo::smem_bytes(W);
+  const size_t smem = STEADY ? Geo::smem_bytes_steady(W) : Geo::smem_bytes(W);
   static bool attr_done = false;  // once per template instance
   if (!attr_done) {
     cudaFuncSetAttribute(ms_pass_kernel<N1, N2, AXIS, W, MINB, STEADY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -47,8 +48,40 @@ int launch_bwd_t(const BwdArgs& a, int grid_y, cudaStream_t st) {
   return (int)cudaGetLastError();
 }
 
+// Steady passes: persistent, prefetching CTAs; the grid holds exactly the CTAs that
+// can be resident at once (line tiles x rows), each walking several slots.
 template <int N1, int N2, int AXIS, int MINB>
-int launch_pass_t(const PassArgs& a, int grid_y, cudaStream_t st) {
+int launch_pipe_t(const PassArgs& a, int nslots, cudaStream_t st) {
+  using Geo = PassGeom<N1, N2>;
+  constexpr int W = Geo::kWarps;
+  using PG = PipeGeom<N1, N2, AXIS, W>;
+  const size_t smem = PG::smem_bytes();
+  static int resident = 0;  // CTAs of this kernel per SM x SMs
+  if (!resident) {
+    cudaFuncSetAttribute(ms_pass_pipe_kernel<N1, N2, AXIS, W, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)smem);
+    int per_sm = 0, dev = 0, sms = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ms_pass_pipe_kernel<N1, N2, AXIS, W, MINB>, W * 32,
+                                                  smem);
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    resident = (per_sm > 0 ? per_sm : 1) * (sms > 0 ? sms : 1);
+  }
+  const int tiles = Geo::N / Geo::kLines;
+  int rows = resident / tiles;
+  if (rows < 1) rows = 1;
+  if (rows > nslots) rows = nslots;
+  dim3 grid(tiles, rows);
+  ms_pass_pipe_kernel<N1, N2, AXIS, W, MINB><<<grid, W * 32, smem, st>>>(a, nslots);
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  return (int)cudaGetLastError();
+}
+
+// tune bit 2 (value 4) selects the persistent double-buffered kernel for steady
+// passes (measured slower than the one-slot-per-CTA kernel on B200 at 128-512^2)
+template <int N1, int N2, int AXIS, int MINB>
+int launch_pass_t(const PassArgs& a, int grid_y, cudaStream_t st, int variant) {
+  if (is_steady_pass(a) && a.tw2 != nullptr && (variant & 4)) return launch_pipe_t<N1, N2, AXIS, MINB>(a, grid_y, st);
   return is_steady_pass(a) ? launch_pass_s<N1, N2, AXIS, MINB, true>(a, grid_y, st)
                            : launch_pass_s<N1, N2, AXIS, MINB, false>(a, grid_y, st);
 }
@@ -95,8 +128,10 @@ int launch_bwd_multi_t(const BwdArgs* descs, const int2* rows, int nrows, cudaSt
     constexpr int lo = (N2) <= 16 ? 2 : 1, hi = (N2) <= 16 ? 3 : 1;                              \
     const bool occ = (variant >> axis) & 1;                                                      \
     if (axis == 0)                                                                               \
-      return occ ? launch_pass_t<N1, N2, 0, hi>(a, grid_y, st) : launch_pass_t<N1, N2, 0, lo>(a, grid_y, st); \
-    return occ ? launch_pass_t<N1, N2, 1, hi>(a, grid_y, st) : launch_pass_t<N1, N2, 1, lo>(a, grid_y, st);   \
+      return occ ? launch_pass_t<N1, N2, 0, hi>(a, grid_y, st, variant)                          \
+                 : launch_pass_t<N1, N2, 0, lo>(a, grid_y, st, variant);                         \
+    return occ ? launch_pass_t<N1, N2, 1, hi>(a, grid_y, st, variant)                            \
+               : launch_pass_t<N1, N2, 1, lo>(a, grid_y, st, variant);                           \
   }                                                                                              \
   int launch_bwd_##NN(int axis, const BwdArgs& a, int grid_y, cudaStream_t st) {                \
     return axis == 0 ? launch_bwd_t<N1, N2, 0>(a, grid_y, st) : launch_bwd_t<N1, N2, 1>(a, grid_y, st); \
