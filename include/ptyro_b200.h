@@ -168,6 +168,25 @@ int ptyro_ms_steady_pass(const ptyro_ms_params* p, int32_t axis, int32_t reps, v
  * the FP32 ceiling used as the roofline denominator; no reference counterpart. */
 int ptyro_fp32_fma_probe(float* out, int32_t blocks, int32_t iters, void* stream);
 
+/* Workspace bytes of ptyro_atom_slices for edge n and num_types atom types. */
+size_t ptyro_atom_slices_workspace_bytes(int32_t n, int32_t num_types);
+
+/* Potential slices built on the device from atoms, the slice builder of the
+ * reference's atom-backed path (_compute_slice_potential,
+ * src/ptyrodactyl/multislice/parallelized.py:54-169; used by stem4d_sharded :348).
+ *   atom_coords     DEVICE float64 (N, 3) x, y, z in Angstrom
+ *   atom_types      DEVICE int32 (N) indices into atom_potentials
+ *   slice_z_bounds  HOST float64 (S, 2) [z_min, z_max) per slice
+ *   atom_potentials DEVICE float32 (T, n, n) per-type projected potentials (V A)
+ *   atom_mask       DEVICE float32 (N) inclusion weights, or NULL
+ *   slices          DEVICE float32 out, V[y][x][s] at strides (sy, sx, ss)
+ * Atoms land on floor(coord / calib) mod n; each type's delta grid is circularly
+ * convolved with its kernel (FFT), and the types are summed. */
+int ptyro_atom_slices(int32_t n, int32_t num_atoms, int32_t num_types, int32_t num_slices, const double* atom_coords,
+                      const int32_t* atom_types, const double* slice_z_bounds, const float* atom_potentials,
+                      const float* atom_mask, double calib_ang, float* slices, int64_t sy, int64_t sx, int64_t ss,
+                      void* workspace, size_t workspace_bytes, void* stream);
+
 /* ---------------------------------------------------------------- scheduler
  * Continuous batching of forward and gradient jobs of any grid edge, slice count
  * and scan size (the batching and serving patterns; no reference counterpart:

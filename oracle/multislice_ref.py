@@ -291,3 +291,43 @@ def stem_4d_windowed_vjp(field, slice_thickness, pot_calib, beam_modes, weights,
         dfield += np.roll(acc, (int(wy), int(wx)), axis=(0, 1))
         dbeam += db
     return dfield, dbeam
+
+
+def slice_potential_from_atoms(atom_coords, atom_types, z_min, z_max, atom_potentials, grid_shape, calib_ang,
+                               atom_mask=None) -> np.ndarray:
+    """_compute_slice_potential (multislice/parallelized.py:54-169): atoms with
+    z_min <= z < z_max scattered to floor(coord / calib) mod grid per type, each type's
+    delta grid circularly convolved with its kernel by FFT, summed over types."""
+    h, w = int(grid_shape[0]), int(grid_shape[1])
+    coords = np.asarray(atom_coords, np.float64)
+    types = np.asarray(atom_types)
+    in_slice = ((coords[:, 2] >= z_min) & (coords[:, 2] < z_max)).astype(np.float64)
+    if atom_mask is not None:
+        in_slice = in_slice * np.asarray(atom_mask, np.float64)
+    x_idx = np.mod(np.floor(coords[:, 0] / calib_ang).astype(np.int64), w)
+    y_idx = np.mod(np.floor(coords[:, 1] / calib_ang).astype(np.int64), h)
+    out = np.zeros((h, w), np.float64)
+    pots = np.asarray(atom_potentials, np.float64)
+    for t in range(pots.shape[0]):
+        grid = np.zeros((h, w), np.float64)
+        np.add.at(grid, (y_idx, x_idx), (types == t) * in_slice)
+        out += np.real(np.fft.ifft2(np.fft.fft2(grid) * np.fft.fft2(pots[t])))
+    return out
+
+
+def stem4d_sharded(beam_modes, weights, atom_coords, atom_types, slice_z_bounds, atom_potentials, voltage_kv,
+                   real_space_calib_ang, scan_positions_ang, atom_mask=None, dtype=np.complex128) -> dict:
+    """stem4d_sharded (multislice/parallelized.py:348-536) without a mesh: slices built
+    from atoms (thickness = first slice's z extent), positions in Angstrom, every
+    calibration = detector.real_space_calib_ang."""
+    beam = np.atleast_3d(np.asarray(beam_modes))
+    h, w = beam.shape[0], beam.shape[1]
+    bounds = np.asarray(slice_z_bounds, np.float64)
+    slices = np.stack([slice_potential_from_atoms(atom_coords, atom_types, b[0], b[1], atom_potentials, (h, w),
+                                                  real_space_calib_ang, atom_mask) for b in bounds], axis=-1)
+    thickness = bounds[0, 1] - bounds[0, 0]
+    out = stem_4d(slices, thickness, real_space_calib_ang, beam, weights, real_space_calib_ang, voltage_kv,
+                  scan_positions_ang, real_space_calib_ang, dtype)
+    out["scan_positions"] = np.atleast_2d(np.asarray(scan_positions_ang, np.float64))
+    out["slices"] = slices
+    return out

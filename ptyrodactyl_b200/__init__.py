@@ -7,12 +7,14 @@ and run hand-written sm_100a CUDA through the C-ABI in ``include/ptyro_b200.h``.
 
 from .types import (  # noqa: F401
     STEM4D,
+    AtomicSliceData,
     CalibratedArray,
     DetectorConfig,
     EnsembleAxes,
     MicroscopeConfig,
     PotentialSlices,
     ProbeModes,
+    create_atomic_slice_data,
     create_calibrated_array,
     create_detector_config,
     create_microscope_config,
@@ -27,6 +29,8 @@ from .simulations import (  # noqa: F401
     make_probe,
     relativistic_wavelength_ang,
     run_forward,
+    slices_from_atoms,
+    stem4d_sharded,
     stem_4d,
     stem_4d_frozen_phonon,
     stem_4d_windowed,

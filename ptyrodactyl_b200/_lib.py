@@ -48,6 +48,8 @@ EXPORTED_SYMBOLS = (
     "ptyro_sched_job_state",
     "ptyro_sched_release",
     "ptyro_sched_memory",
+    "ptyro_atom_slices_workspace_bytes",
+    "ptyro_atom_slices",
 )
 
 PTYRO_JOB_FORWARD = 0
@@ -165,6 +167,11 @@ def _declare(lib) -> None:
     lib.ptyro_sched_release.argtypes = [vp, ctypes.c_int64]
     lib.ptyro_sched_memory.restype = ctypes.c_int
     lib.ptyro_sched_memory.argtypes = [vp, ctypes.POINTER(sz), ctypes.POINTER(i32)]
+    lib.ptyro_atom_slices_workspace_bytes.restype = sz
+    lib.ptyro_atom_slices_workspace_bytes.argtypes = [i32, i32]
+    lib.ptyro_atom_slices.restype = ctypes.c_int
+    i64 = ctypes.c_int64
+    lib.ptyro_atom_slices.argtypes = [i32, i32, i32, i32, vp, vp, vp, vp, vp, dbl, vp, i64, i64, i64, vp, sz, vp]
     lib.ptyro_ms_forward_noalloc.restype = ctypes.c_int
     lib.ptyro_ms_forward_noalloc.argtypes = [pp, vp, vp, vp, vp, vp, vp]
 

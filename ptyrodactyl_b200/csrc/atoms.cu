@@ -1,0 +1,106 @@
+// On-device potential slices from atoms: the slice builder of the reference's
+// atom-backed path (_compute_slice_potential, src/ptyrodactyl/multislice/parallelized.py:54-169).
+// Per slice: scatter the atoms with z_min <= z < z_max to floor(coord / calib) mod n
+// per type, FFT2 the type planes, multiply by each type's kernel spectrum and sum,
+// IFFT2, keep the real part.
+#include "engine.cuh"
+
+namespace ptyro {
+
+static __global__ void k_real_to_complex(const float* __restrict__ src, size_t count, float2* __restrict__ dst) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += (size_t)gridDim.x * blockDim.x)
+    dst[i] = make_float2(src[i], 0.f);
+}
+
+// atoms of the slice add their weight at their pixel; weights are 1 unless a mask is
+// given, so the sums are exact whatever the order of the additions
+static __global__ void k_scatter_atoms(const double* __restrict__ coords, const int* __restrict__ types,
+                                       const float* __restrict__ mask, int num_atoms, int num_types, double z_min,
+                                       double z_max, double calib, int n, float2* __restrict__ delta) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= num_atoms) return;
+  const double z = coords[3 * i + 2];
+  if (!(z >= z_min && z < z_max)) return;
+  const int t = types[i];
+  if (t < 0 || t >= num_types) return;
+  const float wgt = mask ? mask[i] : 1.0f;
+  long long xi = (long long)floor(coords[3 * i + 0] / calib) % n;
+  long long yi = (long long)floor(coords[3 * i + 1] / calib) % n;
+  if (xi < 0) xi += n;
+  if (yi < 0) yi += n;
+  atomicAdd(&delta[((size_t)t * n + yi) * n + xi].x, wgt);
+}
+
+static __global__ void k_combine_types(const float2* __restrict__ delta_k, const float2* __restrict__ kern_k,
+                                       int num_types, size_t nn, float2* __restrict__ out) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < nn; i += (size_t)gridDim.x * blockDim.x) {
+    float2 acc = make_float2(0.f, 0.f);
+    for (int t = 0; t < num_types; ++t) acc = cadd(acc, cmul(delta_k[t * nn + i], kern_k[t * nn + i]));
+    out[i] = acc;
+  }
+}
+
+static __global__ void k_store_slice(const float2* __restrict__ c, int n, float* __restrict__ slices, long long sy,
+                                     long long sx, long long ss, int s) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (size_t)n * n) return;
+  const int y = (int)(i / n), x = (int)(i % n);
+  slices[(long long)y * sy + (long long)x * sx + (long long)s * ss] = c[i].x;
+}
+
+}  // namespace ptyro
+
+using namespace ptyro;
+
+extern "C" {
+
+size_t ptyro_atom_slices_workspace_bytes(int32_t n, int32_t num_types) {
+  if (n <= 0 || num_types <= 0) return 0;
+  const size_t nn = (size_t)n * n;
+  return align_up(8 * (size_t)n) + 2 * align_up(8 * nn * num_types) + align_up(8 * nn);
+}
+
+int ptyro_atom_slices(int32_t n, int32_t num_atoms, int32_t num_types, int32_t num_slices, const double* atom_coords,
+                      const int32_t* atom_types, const double* slice_z_bounds_host, const float* atom_potentials,
+                      const float* atom_mask, double calib_ang, float* slices, int64_t sy, int64_t sx, int64_t ss,
+                      void* workspace, size_t workspace_bytes, void* stream) {
+  Shape sh;
+  if (!shape_for(n, &sh)) return fail(PTYRO_ERR_UNSUPPORTED, "atom slices: n must be a power of two in [16, 1024]");
+  if (num_atoms < 0 || num_types < 1 || num_slices < 1)
+    return fail(PTYRO_ERR_INVALID, "atom slices: need num_atoms >= 0, num_types >= 1, num_slices >= 1");
+  if (!(calib_ang > 0)) return fail(PTYRO_ERR_INVALID, "calib must be > 0");
+  if ((num_atoms && (!atom_coords || !atom_types)) || !slice_z_bounds_host || !atom_potentials || !slices)
+    return fail(PTYRO_ERR_INVALID, "NULL array argument");
+  const size_t need = ptyro_atom_slices_workspace_bytes(n, num_types);
+  if (!workspace || workspace_bytes < need || ((uintptr_t)workspace & 255))
+    return fail(PTYRO_ERR_WORKSPACE, "atom slices: workspace too small or misaligned: need " + std::to_string(need));
+  cudaStream_t st = (cudaStream_t)stream;
+  const size_t nn = (size_t)n * n;
+  char* ws = (char*)workspace;
+  float2* tw = (float2*)ws;
+  float2* kern = (float2*)(ws + align_up(8 * (size_t)n));
+  float2* delta = (float2*)((char*)kern + align_up(8 * nn * num_types));
+  float2* acc = (float2*)((char*)delta + align_up(8 * nn * num_types));
+  k_twiddle<<<(n + 255) / 256, 256, 0, st>>>(n, tw);
+  k_real_to_complex<<<blocks_for(nn * num_types, 256), 256, 0, st>>>(atom_potentials, nn * num_types, kern);
+  int rc = check_launch("atom slices setup", 2);
+  if (rc) return rc;
+  if ((rc = fft2_planes(n, num_types, false, kern, tw, st))) return rc;
+  for (int s = 0; s < num_slices; ++s) {
+    k_zero2<<<blocks_for(nn * num_types, 256), 256, 0, st>>>(delta, nn * num_types);
+    if (num_atoms > 0)
+      k_scatter_atoms<<<(num_atoms + 255) / 256, 256, 0, st>>>(atom_coords, atom_types, atom_mask, num_atoms,
+                                                               num_types, slice_z_bounds_host[2 * s],
+                                                               slice_z_bounds_host[2 * s + 1], calib_ang, n, delta);
+    if ((rc = check_launch("k_scatter_atoms", num_atoms > 0 ? 2 : 1))) return rc;
+    if ((rc = fft2_planes(n, num_types, false, delta, tw, st))) return rc;
+    k_combine_types<<<blocks_for(nn, 256), 256, 0, st>>>(delta, kern, num_types, nn, acc);
+    if ((rc = check_launch("k_combine_types"))) return rc;
+    if ((rc = fft2_planes(n, 1, true, acc, tw, st))) return rc;
+    k_store_slice<<<(unsigned)((nn + 255) / 256), 256, 0, st>>>(acc, n, slices, sy, sx, ss, s);
+    if ((rc = check_launch("k_store_slice"))) return rc;
+  }
+  return PTYRO_OK;
+}
+
+}  // extern "C"

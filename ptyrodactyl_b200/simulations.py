@@ -16,6 +16,7 @@ import torch
 
 from . import _lib
 from .types import (
+    AtomicSliceData,
     CalibratedArray,
     DetectorConfig,
     MicroscopeConfig,
@@ -248,6 +249,54 @@ def stem_4d_frozen_phonon(pot_slices: list, beam: ProbeModes, microscope: Micros
     fourier_calib = 1.0 / (n * calib)
     scan_positions = detector.scan_positions_px.to(torch.float64) * detector.real_space_calib_ang
     return create_stem4d(out, detector.real_space_calib_ang, fourier_calib, scan_positions, microscope.voltage_kv)
+
+
+def slices_from_atoms(sample: AtomicSliceData, grid_shape, calib_ang: float, device=None) -> torch.Tensor:
+    """Potential slices (H, W, S) float32 built on the device from atoms
+    (_compute_slice_potential, multislice/parallelized.py:54-169)."""
+    lib = _lib.load()
+    dev = _device(device)
+    h, w = int(grid_shape[0]), int(grid_shape[1])
+    n = _check_edge(h, w)
+    pots = as_tensor(sample.atom_potentials, torch.float32, dev).contiguous()
+    if tuple(pots.shape[1:]) != (n, n):
+        raise ValueError("atom_potentials must match the grid shape")
+    coords = as_tensor(sample.atom_coords, torch.float64, dev).contiguous()
+    types = sample.atom_types.to(dev, torch.int32).contiguous()
+    bounds = as_tensor(sample.slice_z_bounds, torch.float64).cpu().contiguous()
+    mask = None if sample.atom_mask is None else as_tensor(sample.atom_mask, torch.float32, dev).contiguous()
+    S = bounds.shape[0]
+    out = torch.empty((n, n, S), dtype=torch.float32, device=dev)
+    nbytes = lib.ptyro_atom_slices_workspace_bytes(n, pots.shape[0])
+    ws = _workspace(nbytes, dev)
+    _lib.check(lib.ptyro_atom_slices(n, coords.shape[0], pots.shape[0], S, coords.data_ptr(), types.data_ptr(),
+                                     bounds.data_ptr(), pots.data_ptr(), None if mask is None else mask.data_ptr(),
+                                     float(calib_ang), out.data_ptr(), *out.stride(), ws.data_ptr(), nbytes,
+                                     _stream_ptr(dev)))
+    return out
+
+
+def stem4d_sharded(probe_modes: ProbeModes, sample: AtomicSliceData, microscope: MicroscopeConfig,
+                   detector: DetectorConfig, mesh=None) -> STEM4D:
+    """Atom-backed 4D-STEM (multislice/parallelized.py:348-536): slices built on the
+    device from atoms, positions in Angstrom (``detector.scan_positions_ang``), every
+    calibration = ``detector.real_space_calib_ang``. ``mesh`` must be None: this engine
+    runs on one GPU per process (shard scan positions across processes instead)."""
+    if detector.scan_positions_ang is None:
+        raise ValueError("detector.scan_positions_ang is required")
+    if mesh is not None:
+        raise NotImplementedError("device meshes are not supported; shard positions across processes")
+    dev = _device()
+    modes, weights = _beam_on(probe_modes, dev)
+    n = modes.shape[0]
+    calib = float(detector.real_space_calib_ang)
+    slices = slices_from_atoms(sample, (n, n), calib, dev)
+    bounds = as_tensor(sample.slice_z_bounds, torch.float64)
+    thickness = float(bounds[0, 1] - bounds[0, 0])
+    positions = as_tensor(detector.scan_positions_ang, torch.float64, dev).reshape(-1, 2).contiguous()
+    data = run_forward(slices, thickness, modes, weights, positions, microscope.voltage_kv, calib, calib)
+    return create_stem4d(data, calib, 1.0 / (n * calib), detector.scan_positions_ang.to(torch.float64),
+                         microscope.voltage_kv)
 
 
 def cbed_image(pot_slices: PotentialSlices, beam: ProbeModes, microscope: MicroscopeConfig) -> CalibratedArray:

@@ -118,6 +118,18 @@ class DetectorConfig:
 
 
 @dataclass(frozen=True)
+class AtomicSliceData:
+    """Atoms, slice z bounds and per-type kernels for the atom-backed path
+    (electron_types.py:192-224)."""
+
+    atom_coords: Array
+    atom_types: Array
+    slice_z_bounds: Array
+    atom_potentials: Array
+    atom_mask: Optional[Array] = None
+
+
+@dataclass(frozen=True)
 class CalibratedArray:
     """2-D array with calibrations (electron_types.py:264-292)."""
 
@@ -241,6 +253,43 @@ def create_potential_slices(slices, slice_thickness, calib) -> PotentialSlices:
     _positive(th, "slice_thickness")
     _positive(c, "calib")
     return PotentialSlices(s, th, c)
+
+
+def create_atomic_slice_data(atom_coords, atom_types, slice_z_bounds, atom_potentials,
+                             atom_mask=None) -> AtomicSliceData:
+    """electron_types.py:735-850: coords (N, 3) x, y, z Angstrom; types (N,);
+    bounds (S, 2); kernels (T, H, W) volt-Angstrom; optional mask (N,)."""
+    coords = as_tensor(atom_coords, torch.float64)
+    types = as_tensor(atom_types, torch.int32) if not isinstance(atom_types, torch.Tensor) else atom_types.to(
+        torch.int32)
+    bounds = as_tensor(slice_z_bounds, torch.float64)
+    pots = as_tensor(atom_potentials, torch.float32)
+    mask = None if atom_mask is None else as_tensor(atom_mask, torch.float32)
+    if coords.ndim != 2 or coords.shape[1] != 3:
+        raise ValueError("atom_coords must have shape (N, 3)")
+    if types.ndim != 1 or types.shape[0] != coords.shape[0]:
+        raise ValueError("atom_types must have shape (N,)")
+    if bounds.ndim != 2 or bounds.shape[1] != 2:
+        raise ValueError("slice_z_bounds must have shape (S, 2)")
+    if pots.ndim != 3:
+        raise ValueError("atom_potentials must have shape (T, H, W)")
+    if mask is not None and tuple(mask.shape) != (coords.shape[0],):
+        raise ValueError("atom_mask must have shape (N,)")
+    if not bool(torch.isfinite(coords).all()):
+        raise ValueError("atom_coords contain non-finite values")
+    if types.numel() and bool((types < 0).any()):
+        raise ValueError("atom_types must be non-negative")
+    if types.numel() and int(types.max()) >= pots.shape[0]:
+        raise ValueError("atom_types must index atom_potentials")
+    if not bool(torch.isfinite(bounds).all()):
+        raise ValueError("slice_z_bounds contain non-finite values")
+    if bounds.numel() and bool((bounds[:, 1] <= bounds[:, 0]).any()):
+        raise ValueError("slice_z_bounds thicknesses must be positive")
+    if not bool(torch.isfinite(pots).all()):
+        raise ValueError("atom_potentials contain non-finite values")
+    if mask is not None and not bool(torch.isfinite(mask).all()):
+        raise ValueError("atom_mask contains non-finite values")
+    return AtomicSliceData(coords, types, bounds, pots, mask)
 
 
 def create_calibrated_array(data_array, calib_y, calib_x, real_space) -> CalibratedArray:

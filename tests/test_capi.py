@@ -95,3 +95,46 @@ def test_zero_probes_is_a_no_op(lib):
 def test_fft2_rejects_bad_edge(lib):
     assert lib.ptyro_fft2(100, 1, 0, None, None, 0, None) == _lib.PTYRO_ERR_UNSUPPORTED
     assert lib.ptyro_fft2(64, -1, 0, None, None, 0, None) == _lib.PTYRO_ERR_INVALID
+
+
+def test_atom_slices_validate_before_launch(lib):
+    ws = lib.ptyro_atom_slices_workspace_bytes(64, 2)
+    assert ws > 0
+    args = dict(n=64, na=3, nt=2, ns=2, calib=0.2)
+
+    def call(**kw):
+        a = {**args, **kw}
+        z = ctypes.c_void_p(16)
+        return lib.ptyro_atom_slices(a["n"], a["na"], a["nt"], a["ns"], z, z, z, z, None, a["calib"], z,
+                                     64 * 2, 2, 1, z, kw.get("wsb", ws), None)
+
+    assert call(n=100) == _lib.PTYRO_ERR_UNSUPPORTED
+    assert call(nt=0) == _lib.PTYRO_ERR_INVALID
+    assert call(ns=0) == _lib.PTYRO_ERR_INVALID
+    assert call(calib=0.0) == _lib.PTYRO_ERR_INVALID
+    assert call(wsb=ws - 1) == _lib.PTYRO_ERR_WORKSPACE
+
+
+def test_atomic_slice_data_validation():
+    import numpy as np
+    import ptyrodactyl_b200 as pb
+    coords = np.zeros((4, 3))
+    pots = np.zeros((2, 16, 16))
+    ok = pb.create_atomic_slice_data(coords, [0, 1, 0, 1], [[0, 1], [1, 2]], pots)
+    assert ok.atom_types.dtype.is_floating_point is False and ok.atom_mask is None
+    bad = [
+        (dict(atom_coords=np.zeros((4, 2))), "atom_coords must have shape"),
+        (dict(atom_types=[0, 1, 0]), "atom_types must have shape"),
+        (dict(slice_z_bounds=[0, 1]), "slice_z_bounds must have shape"),
+        (dict(atom_potentials=np.zeros((16, 16))), "atom_potentials must have shape"),
+        (dict(atom_types=[0, 1, 0, 2]), "atom_types must index atom_potentials"),
+        (dict(atom_types=[0, -1, 0, 1]), "atom_types must be non-negative"),
+        (dict(slice_z_bounds=[[0, 1], [2, 2]]), "thicknesses must be positive"),
+        (dict(atom_coords=np.full((4, 3), np.nan)), "atom_coords contain non-finite"),
+        (dict(atom_mask=[1, 1, 0]), "atom_mask must have shape"),
+        (dict(atom_mask=[1, np.inf, 0, 1]), "atom_mask contains non-finite"),
+    ]
+    base = dict(atom_coords=coords, atom_types=[0, 1, 0, 1], slice_z_bounds=[[0, 1], [1, 2]], atom_potentials=pots)
+    for kw, msg in bad:
+        with pytest.raises(ValueError, match=msg):
+            pb.create_atomic_slice_data(**{**base, **kw})

@@ -180,3 +180,31 @@ def test_frozen_phonon_average_matches_oracle_mean():
     want = np.mean([R.stem_4d(p, synth.SLICE_DZ, w.calib, probe[..., None], [1.0], w.calib, w.voltage_kv, pos,
                               w.calib)["data"] for p in pots], axis=0)
     assert rel_l2(got, want) < TOL_F64
+
+
+def test_atom_backed_stem4d_sharded_matches_reference_golden(golden):
+    g = golden
+    atoms = np.array([[2.0, 2.5, 0.25], [4.5, 5.0, 2.25], [3.0, 4.0, 1.25]])
+    sample = pb.create_atomic_slice_data(atoms, [0, 0, 0], [[0.0, 2.0], [2.0, 4.0]], g["pot"][..., 0][None])
+    mic = pb.create_microscope_config(100.0, 20.0, probe_shape=(32, 32))
+    det = pb.create_detector_config(0.2, 20.0, scan_positions_ang=g["positions_px"] * 0.2)
+    beam = pb.create_probe_modes(R.make_probe(100.0, 20.0, (32, 32), 20.0)[..., None], [1.0], 0.2)
+    s4 = pb.stem4d_sharded(beam, sample, mic, det)
+    assert rel_l2(s4.data.cpu().numpy(), g["stem4d_sharded"]) < TOL_F64
+    assert np.allclose(s4.scan_positions.cpu().numpy(), g["positions_px"] * 0.2)
+
+
+def test_slices_from_atoms_match_oracle():
+    rng = np.random.default_rng(12)
+    n, calib = 128, 0.25
+    atoms = np.column_stack([rng.uniform(-5, 40, 300), rng.uniform(-5, 40, 300), rng.uniform(0, 6, 300)])
+    types = rng.integers(0, 3, 300)
+    kern = rng.uniform(0, 1, (3, n, n)) * np.exp(-np.hypot(*np.meshgrid(np.fft.fftfreq(n) * n, np.fft.fftfreq(n) * n,
+                                                                         indexing="ij")) / 3.0)
+    bounds = [[0.0, 2.0], [2.0, 4.0], [4.0, 6.0]]
+    mask = (rng.uniform(size=300) > 0.2).astype(np.float32)
+    sample = pb.create_atomic_slice_data(atoms, types, bounds, kern, mask)
+    got = pb.slices_from_atoms(sample, (n, n), calib).cpu().numpy()
+    want = np.stack([R.slice_potential_from_atoms(atoms, types, b[0], b[1], kern, (n, n), calib, mask)
+                     for b in bounds], axis=-1)
+    assert rel_l2(got, want) < 1e-5

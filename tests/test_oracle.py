@@ -98,3 +98,13 @@ def test_golden_gradient_is_null(golden):
                           np.ones((1, 32, 32)))
     assert np.max(np.abs(dv)) < 1e-12
     assert np.max(np.abs(g["grad_pot"])) < 1e-12
+
+
+def test_oracle_atom_backed_matches_reference_golden(golden):
+    """stem4d_sharded of the golden capture (atom-backed slices, plan01_ug_capture.py:74-97)."""
+    g = golden
+    probe = R.make_probe(100.0, 20.0, (32, 32), 20.0)
+    atoms = np.array([[2.0, 2.5, 0.25], [4.5, 5.0, 2.25], [3.0, 4.0, 1.25]])
+    out = R.stem4d_sharded(probe[..., None], [1.0], atoms, [0, 0, 0], [[0.0, 2.0], [2.0, 4.0]],
+                           g["pot"][..., 0][None], 100.0, 0.2, g["positions_px"] * 0.2)
+    assert np.max(np.abs(out["data"] - g["stem4d_sharded"])) < 1e-13
