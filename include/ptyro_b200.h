@@ -133,6 +133,35 @@ int ptyro_ms_forward_plain(const ptyro_ms_params* p, const float* potential, con
                            const float* weights, const double* positions, float* patterns,
                            void* workspace, size_t workspace_bytes, void* stream);
 
+/* Most virtual detectors one forward or one ptyro_detect_patterns call evaluates. */
+#define PTYRO_MAX_DETECTORS 32
+
+/* Workspace bytes ptyro_ms_forward_detect needs for `p` and `num_det` detectors
+ * (0 when invalid). */
+size_t ptyro_ms_detect_workspace_bytes(const ptyro_ms_params* p, int32_t num_det);
+
+/* ptyro_ms_forward with virtual detectors fused into the pattern pass: the
+ * integration step of annular_detector (src/ptyrodactyl/multislice/simulations.py:
+ * 1539-1656) runs on each far-field intensity while it is in registers.
+ *   det_mask  uint32 (n, n) in UNSHIFTED frequency order [ky][kx]: bit d set puts
+ *             the pixel in detector d (the reference's annular mask is built on the
+ *             fftshifted grid; pixel (i, j) there is frequency (i - n/2, j - n/2))
+ *   num_det   1 .. PTYRO_MAX_DETECTORS
+ *   det_out   float64 (P, num_det) masked intensity sums
+ *   patterns  float32 (P, n, n) fftshifted intensities, or NULL to store none
+ * PTYRO_FLAG_ACCUMULATE adds into det_out (and patterns). */
+int ptyro_ms_forward_detect(const ptyro_ms_params* p, const float* potential, const float* modes,
+                            const float* weights, const double* positions, const uint32_t* det_mask,
+                            int32_t num_det, double* det_out, float* patterns, void* workspace,
+                            size_t workspace_bytes, void* stream);
+
+/* Masked sums of stored fftshifted patterns (P, n, n) float32: det_out[p][d] = sum of
+ * the pixels of pattern p whose frequency has bit d set in det_mask (unshifted
+ * order, as above). The vmap'd integration of annular_detector
+ * (simulations.py:1620-1636). n a power of two in [2, 8192]. No workspace. */
+int ptyro_detect_patterns(const float* patterns, int64_t num_patterns, int32_t n, const uint32_t* det_mask,
+                          int32_t num_det, double* det_out, void* stream);
+
 /* Probe formation. Replaces make_probe (src/ptyrodactyl/multislice/simulations.py:334-431)
  * with aberration (:434-498): aperture |q| <= alpha/lambda times exp(-i chi),
  * ifftshift(ifft2(.)). Writes a complex64 (n, n) probe to `probe`.

@@ -331,3 +331,22 @@ def stem4d_sharded(beam_modes, weights, atom_coords, atom_types, slice_z_bounds,
     out["scan_positions"] = np.atleast_2d(np.asarray(scan_positions_ang, np.float64))
     out["slices"] = slices
     return out
+
+
+def annular_mask(shape, fourier_calib, voltage_kv, inner_mrad, outer_mrad):
+    """Annulus on the fftshifted grid (simulations.py:1590-1618)."""
+    wavelength = relativistic_wavelength_ang(voltage_kv)
+    inner_k = (inner_mrad / 1000.0) / wavelength
+    outer_k = (outer_mrad / 1000.0) / wavelength
+    hh, ww = shape
+    qya, qxa = np.meshgrid(np.arange(hh) - hh // 2, np.arange(ww) - ww // 2, indexing="ij")
+    q_radius = np.sqrt(qya ** 2 + qxa ** 2) * fourier_calib
+    return (q_radius >= inner_k) & (q_radius <= outer_k)
+
+
+def annular_detector(data, fourier_calib, voltage_kv, inner_mrad, outer_mrad, scan_shape):
+    """simulations.py:1539-1656: sum of each (fftshifted) pattern inside the
+    annulus, reshaped to the scan raster."""
+    data = np.asarray(data, dtype=np.float64)
+    mask = annular_mask(data.shape[1:], fourier_calib, voltage_kv, inner_mrad, outer_mrad)
+    return np.sum(data * mask, axis=(1, 2)).reshape(scan_shape)

@@ -36,6 +36,13 @@ from .simulations import (  # noqa: F401
     stem_4d_windowed,
 )
 
+from .detectors import (  # noqa: F401
+    annular_detector,
+    annular_mask,
+    stem_4d_annular,
+    stem_4d_detectors,
+    virtual_detectors,
+)
 from .autodiff import Stem4dFunction, make_probe_differentiable, stem_4d_patterns, vjp  # noqa: F401
 
 __version__ = "0.1.0"

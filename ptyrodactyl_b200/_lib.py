@@ -20,6 +20,7 @@ PTYRO_ERR_CUDA = 3
 PTYRO_ERR_UNSUPPORTED = 4
 STATIC_SCRATCH_BYTES = 64 << 20  # PTYRO_STATIC_SCRATCH_BYTES
 PTYRO_FLAG_ACCUMULATE = 1
+MAX_DETECTORS = 32
 
 # every symbol include/ptyro_b200.h declares
 EXPORTED_SYMBOLS = (
@@ -35,6 +36,9 @@ EXPORTED_SYMBOLS = (
     "ptyro_ms_steady_pass",
     "ptyro_fp32_fma_probe",
     "ptyro_ms_forward_noalloc",
+    "ptyro_ms_detect_workspace_bytes",
+    "ptyro_ms_forward_detect",
+    "ptyro_detect_patterns",
     "ptyro_ms_residual_bytes",
     "ptyro_ms_forward_ckpt",
     "ptyro_ms_backward_workspace_bytes",
@@ -167,10 +171,16 @@ def _declare(lib) -> None:
     lib.ptyro_sched_release.argtypes = [vp, ctypes.c_int64]
     lib.ptyro_sched_memory.restype = ctypes.c_int
     lib.ptyro_sched_memory.argtypes = [vp, ctypes.POINTER(sz), ctypes.POINTER(i32)]
+    i64 = ctypes.c_int64
+    lib.ptyro_ms_detect_workspace_bytes.restype = sz
+    lib.ptyro_ms_detect_workspace_bytes.argtypes = [pp, i32]
+    lib.ptyro_ms_forward_detect.restype = ctypes.c_int
+    lib.ptyro_ms_forward_detect.argtypes = [pp, vp, vp, vp, vp, vp, i32, vp, vp, vp, sz, vp]
+    lib.ptyro_detect_patterns.restype = ctypes.c_int
+    lib.ptyro_detect_patterns.argtypes = [vp, i64, i32, vp, i32, vp, vp]
     lib.ptyro_atom_slices_workspace_bytes.restype = sz
     lib.ptyro_atom_slices_workspace_bytes.argtypes = [i32, i32]
     lib.ptyro_atom_slices.restype = ctypes.c_int
-    i64 = ctypes.c_int64
     lib.ptyro_atom_slices.argtypes = [i32, i32, i32, i32, vp, vp, vp, vp, vp, dbl, vp, i64, i64, i64, vp, sz, vp]
     lib.ptyro_ms_forward_noalloc.restype = ctypes.c_int
     lib.ptyro_ms_forward_noalloc.argtypes = [pp, vp, vp, vp, vp, vp, vp]

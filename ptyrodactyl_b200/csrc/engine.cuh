@@ -401,8 +401,18 @@ static FwdBuffers fwd_buffers(const Layout& L, char* ws) {
   return b;
 }
 
+// Virtual detectors of a forward: the mask (n, n), the detector count and the
+// per-line partial sums (batch, n, n_det) the pattern pass writes.
+struct DetOut {
+  const uint32_t* mask;
+  int n_det;
+  float* part;
+  double* out;  // (P, n_det)
+};
+
 static FwdPlan fwd_pass_plan(const ptyro_ms_params* p, const FwdBuffers& B, const float* weights, float* patterns,
-                             float2* res_base, int ckpt_every, int C, int b0, int nb, int k) {
+                             float2* res_base, int ckpt_every, int C, int b0, int nb, int k,
+                             const DetOut* det = nullptr) {
   const int n = p->n, S = p->num_slices, M = p->num_modes;
   const size_t nn = (size_t)n * n;
   FwdPlan r;
@@ -438,8 +448,13 @@ static FwdPlan fwd_pass_plan(const ptyro_ms_params* p, const FwdBuffers& B, cons
     r.rows = nb * M;
   } else {  // last axis of the FFT2, |.|^2, fftshifted store
     a.src = SRC_WAVE; a.op1 = OP_FFT; a.t_slice = -1; a.op2 = OP_NONE; a.dst = DST_PATTERN;
-    a.pattern = patterns + (size_t)b0 * nn;
+    a.pattern = patterns ? patterns + (size_t)b0 * nn : nullptr;
     a.accumulate = (p->flags & PTYRO_FLAG_ACCUMULATE) != 0;
+    if (det && det->n_det > 0) {
+      a.det_mask = det->mask;
+      a.det_part = det->part;
+      a.n_det = det->n_det;
+    }
     if (res_base) a.amp_store = res_base + (size_t)C * nn;
     r.axis = (S + 1) % 2;
     r.rows = nb;
@@ -451,17 +466,92 @@ static FwdPlan fwd_pass_plan(const ptyro_ms_params* p, const FwdBuffers& B, cons
 // pass whose slice point s has s % ckpt_every == 0 also stores the wave after the
 // T multiply, and the pattern pass stores the complex far-field amplitude:
 // residual planes per (probe, mode) slot = ceil(S / ckpt_every) checkpoints + 1.
+// Detector sums of `nb` probes: out[b][d] (+)= sum over the n line partials, in
+// line order (deterministic).
+static __global__ void k_det_reduce(const float* __restrict__ part, int nb, int n, int n_det, double* out,
+                                    int accumulate) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nb * n_det) return;
+  const int b = i / n_det, d = i % n_det;
+  double s = 0.0;
+  for (int l = 0; l < n; ++l) s += (double)part[((size_t)b * n + l) * n_det + d];
+  out[i] = accumulate ? out[i] + s : s;
+}
+
+// Bytes of the per-line detector partials behind the forward layout.
+static size_t det_part_bytes(const Layout& L, int n, int n_det) {
+  return n_det > 0 ? align_up(4 * (size_t)L.batch * n * n_det) : 0;
+}
+
+// Masked sums of stored (fftshifted) patterns: one CTA per pattern, float64
+// accumulation, the warps' sums added in warp order (deterministic). Pixel (y, x)
+// of a stored pattern holds frequency ((y + n/2) mod n, (x + n/2) mod n).
+constexpr int kDetThreads = 256;
+static __global__ void __launch_bounds__(kDetThreads) k_detect_patterns(const float* __restrict__ pat, int n,
+                                                                        const uint32_t* __restrict__ mask,
+                                                                        int n_det, double* out) {
+  __shared__ double red[kDetThreads / 32][PTYRO_MAX_DETECTORS];
+  const size_t nn = (size_t)n * n;
+  const float* p = pat + (size_t)blockIdx.x * nn;
+  double acc[PTYRO_MAX_DETECTORS];
+#pragma unroll
+  for (int d = 0; d < PTYRO_MAX_DETECTORS; ++d) acc[d] = 0.0;
+  const int h = n / 2, m = n - 1;
+  for (size_t i = threadIdx.x; i < nn; i += kDetThreads) {
+    const int y = (int)(i / n), x = (int)(i % n);
+    const float v = p[i];
+    const uint32_t b = __ldg(mask + (size_t)((y + h) & m) * n + ((x + h) & m));
+#pragma unroll
+    for (int d = 0; d < PTYRO_MAX_DETECTORS; ++d)
+      if (d < n_det && ((b >> d) & 1u)) acc[d] += (double)v;
+  }
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+#pragma unroll
+  for (int d = 0; d < PTYRO_MAX_DETECTORS; ++d) {
+    if (d >= n_det) break;
+    double s = acc[d];
+#pragma unroll
+    for (int o = 16; o >= 1; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) red[warp][d] = s;
+  }
+  __syncthreads();
+  if (threadIdx.x < n_det) {
+    double s = 0.0;
+    for (int w = 0; w < kDetThreads / 32; ++w) s += red[w][threadIdx.x];
+    out[(size_t)blockIdx.x * n_det + threadIdx.x] = s;
+  }
+}
+
+static int detect_patterns(const float* patterns, int count, int n, const uint32_t* mask, int n_det, double* out,
+                           cudaStream_t st) {
+  k_detect_patterns<<<count, kDetThreads, 0, st>>>(patterns, n, mask, n_det, out);
+  return check_launch("k_detect_patterns");
+}
+
 static int forward_impl(const ptyro_ms_params* p, int ckpt_every, const float* potential, const float* modes,
                         const float* weights, const double* positions, float* patterns, float2* residuals,
-                        void* workspace, size_t workspace_bytes, void* stream) {
+                        void* workspace, size_t workspace_bytes, void* stream, const DetOut* det_in = nullptr) {
   int rc = validate(p);
   if (rc) return rc;
   if (p->num_probes == 0) return PTYRO_OK;
-  if (!potential || !modes || !weights || !positions || !patterns)
+  const bool has_det = det_in && det_in->n_det > 0;
+  if (!potential || !modes || !weights || !positions || (!patterns && !has_det))
     return fail(PTYRO_ERR_INVALID, "NULL array argument");
+  if (has_det && (!det_in->mask || !det_in->out)) return fail(PTYRO_ERR_INVALID, "NULL detector argument");
   const Layout L = layout_for(p);
+  if (has_det) {
+    if (workspace_bytes < L.total + det_part_bytes(L, p->n, det_in->n_det))
+      return fail(PTYRO_ERR_WORKSPACE, "workspace too small for the detector partials: need " +
+                                           std::to_string(L.total + det_part_bytes(L, p->n, det_in->n_det)));
+    workspace_bytes = L.total;
+  }
   rc = check_workspace(L, workspace, workspace_bytes);
   if (rc) return rc;
+  DetOut det = {};
+  if (has_det) {
+    det = *det_in;
+    det.part = (float*)((char*)workspace + L.total);
+  }
   cudaStream_t st = (cudaStream_t)stream;
   char* ws = (char*)workspace;
   rc = forward_setup(p, L, ws, potential, modes, st);
@@ -478,8 +568,15 @@ static int forward_impl(const ptyro_ms_params* p, int ckpt_every, const float* p
                                                   (float2*)B.ramp_y, (float2*)B.ramp_x);
     if ((rc = check_launch("k_ramps"))) return rc;
     for (int k = 0; k <= S + 1; ++k) {
-      const FwdPlan f = fwd_pass_plan(p, B, weights, patterns, res_base, ckpt_every, C, b0, nb, k);
+      const FwdPlan f = fwd_pass_plan(p, B, weights, patterns, res_base, ckpt_every, C, b0, nb, k,
+                                      has_det ? &det : nullptr);
       if ((rc = launch_pass(n, f.axis, f.a, f.rows, st, p->tune))) return rc;
+    }
+    if (has_det) {
+      k_det_reduce<<<(nb * det.n_det + 127) / 128, 128, 0, st>>>(det.part, nb, n, det.n_det,
+                                                                  det.out + (size_t)b0 * det.n_det,
+                                                                  (p->flags & PTYRO_FLAG_ACCUMULATE) != 0);
+      if ((rc = check_launch("k_det_reduce"))) return rc;
     }
   }
   return PTYRO_OK;

@@ -27,6 +27,35 @@ int ptyro_ms_forward(const ptyro_ms_params* p, const float* potential, const flo
                       stream);
 }
 
+size_t ptyro_ms_detect_workspace_bytes(const ptyro_ms_params* p, int32_t num_det) {
+  if (validate(p) || num_det < 1 || num_det > PTYRO_MAX_DETECTORS) return 0;
+  const Layout L = layout_for(p);
+  return L.total + det_part_bytes(L, p->n, num_det);
+}
+
+int ptyro_ms_forward_detect(const ptyro_ms_params* p, const float* potential, const float* modes,
+                            const float* weights, const double* positions, const uint32_t* det_mask,
+                            int32_t num_det, double* det_out, float* patterns, void* workspace,
+                            size_t workspace_bytes, void* stream) {
+  if (num_det < 1 || num_det > PTYRO_MAX_DETECTORS)
+    return fail(PTYRO_ERR_INVALID, "num_det must be in [1, " + std::to_string(PTYRO_MAX_DETECTORS) + "]");
+  const DetOut det = {det_mask, num_det, nullptr, det_out};
+  return forward_impl(p, 0, potential, modes, weights, positions, patterns, nullptr, workspace, workspace_bytes,
+                      stream, &det);
+}
+
+int ptyro_detect_patterns(const float* patterns, int64_t num_patterns, int32_t n, const uint32_t* det_mask,
+                          int32_t num_det, double* det_out, void* stream) {
+  if (n < 2 || n > 8192 || (n & (n - 1)) != 0)
+    return fail(PTYRO_ERR_UNSUPPORTED, "pattern edge must be a power of two in [2, 8192]");
+  if (num_patterns < 0 || num_patterns > 0x7fffffffLL) return fail(PTYRO_ERR_INVALID, "num_patterns out of range");
+  if (num_det < 1 || num_det > PTYRO_MAX_DETECTORS)
+    return fail(PTYRO_ERR_INVALID, "num_det must be in [1, " + std::to_string(PTYRO_MAX_DETECTORS) + "]");
+  if (num_patterns == 0) return PTYRO_OK;
+  if (!patterns || !det_mask || !det_out) return fail(PTYRO_ERR_INVALID, "NULL array argument");
+  return detect_patterns(patterns, (int)num_patterns, n, det_mask, num_det, det_out, (cudaStream_t)stream);
+}
+
 size_t ptyro_ms_residual_bytes(const ptyro_ms_params* p, int32_t ckpt_every) {
   if (validate(p) || ckpt_every < 1) return 0;
   const int C = (p->num_slices + ckpt_every - 1) / ckpt_every;

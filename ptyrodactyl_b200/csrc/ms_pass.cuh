@@ -66,6 +66,13 @@ struct PassArgs {
   float2* amp_store;
   size_t res_stride;
   int accumulate;          // pattern pass adds into the output instead of overwriting it
+  // virtual detectors fused into the pattern pass: bit d of det_mask[ky * N + kx]
+  // (unshifted frequency order) puts that pixel in detector d; each line's masked
+  // intensity sum goes to det_part[(slot * N + line) * n_det + d]. pattern may then
+  // be null (no pattern is stored).
+  const uint32_t* det_mask;
+  float* det_part;
+  int n_det;
 };
 
 template <int N1, int N2>
@@ -321,7 +328,30 @@ __device__ __forceinline__ void pass_body(const PassArgs& a, const int yslot) {
       tile_store<N, lines, pitch, WARPS * 32>(w, work, line0);
     }
   }
-  if (to_pattern) {
+  if (to_pattern && a.n_det > 0) {
+    uint32_t mb[N2];
+#pragma unroll
+    for (int r = 0; r < N2; ++r) {
+      const int k = korder_index<N1, N2>(t, r);
+      mb[r] = __ldg(a.det_mask + (AXIS == 0 ? (size_t)line * N + k : (size_t)k * N + line));
+    }
+    float* part = a.det_part + ((size_t)yslot * N + line) * a.n_det;
+    for (int d = 0; d < a.n_det; ++d) {
+      float s = 0.f;
+#pragma unroll
+      for (int r = 0; r < N2; ++r) s += ((mb[r] >> d) & 1u) ? acc[r] : 0.f;
+      // the lanes of one line differ in t: lane % N1 for rows, lane / G for columns
+      if (AXIS == 0) {
+#pragma unroll
+        for (int o = N1 / 2; o >= 1; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+      } else {
+#pragma unroll
+        for (int o = 16; o >= G; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+      }
+      if (t == 0) part[d] = s;
+    }
+  }
+  if (to_pattern && a.pattern) {
     // fftshift on store: frequency index k lands at (k + N/2) mod N on both axes.
     float* out = a.pattern + (size_t)yslot * NN;
     if (AXIS == 0) {

@@ -108,3 +108,27 @@ def test_oracle_atom_backed_matches_reference_golden(golden):
     out = R.stem4d_sharded(probe[..., None], [1.0], atoms, [0, 0, 0], [[0.0, 2.0], [2.0, 4.0]],
                            g["pot"][..., 0][None], 100.0, 0.2, g["positions_px"] * 0.2)
     assert np.max(np.abs(out["data"] - g["stem4d_sharded"])) < 1e-13
+
+
+def test_oracle_annular_detector_known_answer():
+    """test_simulations.py:84-122: 0-1000 mrad covers every pixel of a 4x4 pattern."""
+    data = np.arange(6 * 4 * 4, dtype=np.float64).reshape(6, 4, 4)
+    img = R.annular_detector(data, 0.25, 80.0, 0.0, 1000.0, (2, 3))
+    assert np.array_equal(img, np.array([[120.0, 376.0, 632.0], [888.0, 1144.0, 1400.0]]))
+
+
+def test_oracle_annular_detector_golden_invariant(golden):
+    """A detector covering the whole pattern collects the aperture count (37 per probe)."""
+    g = golden
+    fc = 1.0 / (32 * 0.2)
+    full = R.annular_detector(g["stem4d"], fc, 100.0, 0.0, 1e6, (2, 2))
+    assert np.allclose(full, 37.0, rtol=1e-12)
+    bf = R.annular_detector(g["stem4d"], fc, 100.0, 0.0, 20.0, (2, 2))
+    df = R.annular_detector(g["stem4d"], fc, 100.0, 20.0 + 1e-9, 1e6, (2, 2))
+    assert np.allclose(bf + df, full, rtol=1e-12)
+
+
+def test_product_mask_matches_oracle_mask():
+    from ptyrodactyl_b200.detectors import annular_mask
+    for n, fc, kv, a, b in [(64, 0.05, 200.0, 10.0, 40.0), (128, 0.03, 300.0, 0.0, 25.0), (16, 0.2, 80.0, 5.0, 5.0)]:
+        assert np.array_equal(annular_mask((n, n), fc, kv, a, b), R.annular_mask((n, n), fc, kv, a, b))
