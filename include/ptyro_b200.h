@@ -133,6 +133,22 @@ int ptyro_ms_forward_plain(const ptyro_ms_params* p, const float* potential, con
                            const float* weights, const double* positions, float* patterns,
                            void* workspace, size_t workspace_bytes, void* stream);
 
+/* Workspace bytes ptyro_ms_jvp needs for `p` (0 when invalid). */
+size_t ptyro_ms_jvp_workspace_bytes(const ptyro_ms_params* p);
+
+/* Forward-mode product of the forward model: the patterns and their directional
+ * derivative along (tangent_potential, tangent_modes). This is the jax.jvp that
+ * jvp_operator / jtj_operator (src/ptyrodactyl/jacobian/operators.py:30-186) take
+ * through stem_4d (src/ptyrodactyl/multislice/simulations.py:1330-1443):
+ *   tangent_potential  float32 dV with the potential's strides, or NULL (zero)
+ *   tangent_modes      complex64 dmodes with the modes' strides, or NULL (zero)
+ *   patterns           float32 (P, n, n) intensities, or NULL to skip them
+ *   tangent_patterns   float32 (P, n, n) dI, fftshifted like the patterns
+ * Windows (ptyro_ms_params.windows) apply to the tangent potential as to V. */
+int ptyro_ms_jvp(const ptyro_ms_params* p, const float* potential, const float* tangent_potential,
+                 const float* modes, const float* tangent_modes, const float* weights, const double* positions,
+                 float* patterns, float* tangent_patterns, void* workspace, size_t workspace_bytes, void* stream);
+
 /* Most virtual detectors one forward or one ptyro_detect_patterns call evaluates. */
 #define PTYRO_MAX_DETECTORS 32
 

@@ -350,3 +350,45 @@ def annular_detector(data, fourier_calib, voltage_kv, inner_mrad, outer_mrad, sc
     data = np.asarray(data, dtype=np.float64)
     mask = annular_mask(data.shape[1:], fourier_calib, voltage_kv, inner_mrad, outer_mrad)
     return np.sum(data * mask, axis=(1, 2)).reshape(scan_shape)
+
+
+# ---------------------------------------------------------------------------
+# Tangent (forward-mode) restatement, the checker for the JVP kernels: what
+# jax.jvp computes through stem_4d (jacobian/operators.py:30-80 takes it).
+#   dpsi_0 = shift(dbeam);  dphi_s = T_s (dpsi_s + i sigma dV_s psi_s)
+#   dpsi_{s+1} = U dphi_s;  dI = sum_m w_m 2 Re(conj(A_m) dA_m)
+# ---------------------------------------------------------------------------
+
+
+def stem_4d_jvp(slices, slice_thickness, pot_calib, beam_modes, weights, beam_calib, voltage_kv,
+                scan_positions_px, real_space_calib_ang, dslices=None, dbeam=None, dtype=np.complex128):
+    """(data, ddata): patterns and their directional derivative along
+    (dslices, dbeam) (either may be None = zero); shapes as stem_4d's."""
+    slices = np.atleast_3d(np.asarray(slices, dtype=np.float64))
+    beam = np.atleast_3d(np.asarray(beam_modes)).astype(dtype)
+    dsl = np.zeros_like(slices) if dslices is None else np.atleast_3d(np.asarray(dslices, dtype=np.float64))
+    db = np.zeros_like(beam) if dbeam is None else np.atleast_3d(np.asarray(dbeam)).astype(dtype)
+    positions = np.atleast_2d(np.asarray(scan_positions_px, dtype=np.float64))
+    w = np.asarray(weights, np.float64)
+    calib = min(float(pot_calib), float(beam_calib))
+    sigma = interaction_sigma(voltage_kv)
+    psi0 = shift_beam_fourier(beam, positions, real_space_calib_ang, dtype)
+    dpsi0 = shift_beam_fourier(db, positions, real_space_calib_ang, dtype)
+    prop = propagation_func(beam.shape[0], beam.shape[1], slice_thickness, voltage_kv, calib, dtype)
+    num = slices.shape[2]
+    data = np.empty((positions.shape[0],) + beam.shape[:2], np.float64)
+    ddata = np.empty_like(data)
+    for i in range(positions.shape[0]):
+        wave, dwave = psi0[i], dpsi0[i]
+        for s in range(num):
+            trans = transmission_func(slices[:, :, s], voltage_kv, dtype)[..., None]
+            dwave = trans * (dwave + 1j * sigma * dsl[:, :, s][..., None] * wave)
+            wave = wave * trans
+            if s != num - 1:
+                wave = np.fft.ifft2(np.fft.fft2(wave, axes=(0, 1)) * prop[..., None], axes=(0, 1))
+                dwave = np.fft.ifft2(np.fft.fft2(dwave, axes=(0, 1)) * prop[..., None], axes=(0, 1))
+        amp = np.fft.fftshift(np.fft.fft2(wave, axes=(0, 1)), axes=(0, 1))
+        damp = np.fft.fftshift(np.fft.fft2(dwave, axes=(0, 1)), axes=(0, 1))
+        data[i] = np.einsum("m,hwm->hw", w, np.abs(amp) ** 2)
+        ddata[i] = np.einsum("m,hwm->hw", w, 2.0 * np.real(np.conj(amp) * damp))
+    return data, ddata

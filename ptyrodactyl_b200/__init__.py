@@ -43,6 +43,7 @@ from .detectors import (  # noqa: F401
     stem_4d_detectors,
     virtual_detectors,
 )
-from .autodiff import Stem4dFunction, make_probe_differentiable, stem_4d_patterns, vjp  # noqa: F401
+from .autodiff import Stem4dFunction, jvp, make_probe_differentiable, stem_4d_patterns, vjp  # noqa: F401
+from . import jacobian  # noqa: F401
 
 __version__ = "0.1.0"

@@ -39,6 +39,8 @@ EXPORTED_SYMBOLS = (
     "ptyro_ms_detect_workspace_bytes",
     "ptyro_ms_forward_detect",
     "ptyro_detect_patterns",
+    "ptyro_ms_jvp_workspace_bytes",
+    "ptyro_ms_jvp",
     "ptyro_ms_residual_bytes",
     "ptyro_ms_forward_ckpt",
     "ptyro_ms_backward_workspace_bytes",
@@ -178,6 +180,10 @@ def _declare(lib) -> None:
     lib.ptyro_ms_forward_detect.argtypes = [pp, vp, vp, vp, vp, vp, i32, vp, vp, vp, sz, vp]
     lib.ptyro_detect_patterns.restype = ctypes.c_int
     lib.ptyro_detect_patterns.argtypes = [vp, i64, i32, vp, i32, vp, vp]
+    lib.ptyro_ms_jvp_workspace_bytes.restype = sz
+    lib.ptyro_ms_jvp_workspace_bytes.argtypes = [pp]
+    lib.ptyro_ms_jvp.restype = ctypes.c_int
+    lib.ptyro_ms_jvp.argtypes = [pp, vp, vp, vp, vp, vp, vp, vp, vp, vp, sz, vp]
     lib.ptyro_atom_slices_workspace_bytes.restype = sz
     lib.ptyro_atom_slices_workspace_bytes.argtypes = [i32, i32]
     lib.ptyro_atom_slices.restype = ctypes.c_int

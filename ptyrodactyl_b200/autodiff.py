@@ -34,18 +34,29 @@ def _ckpt_for(num_slices: int, ckpt_every: int) -> int:
     return max(1, int(math.ceil(math.sqrt(num_slices))))
 
 
+def _plain(t: Optional[torch.Tensor]) -> Optional[torch.Tensor]:
+    """The tensor under any functorch wrappers (None stays None)."""
+    while t is not None and torch._C._functorch.is_functorch_wrapped_tensor(t):
+        t = torch._C._functorch.get_unwrapped(t)
+    return t
+
+
 class Stem4dFunction(torch.autograd.Function):
-    """patterns = stem_4d(slices, modes) with a checkpointed adjoint backward.
+    """(patterns, residuals) = stem_4d(slices, modes) with a checkpointed adjoint
+    backward and a tangent-kernel forward-mode rule.
 
     slices (H, W, S) float32 CUDA (any strides); modes (H, W, M) complex64 CUDA (any
     strides); weights (M,) float32; positions (P, 2) float64. Weights and positions
-    are constants (no gradient).
+    are constants (no derivative). ``record`` makes the forward keep the slice
+    checkpoints and far-field amplitudes the backward needs; a forward-mode-only
+    evaluation (``torch.func.jvp``, dual tensors) skips them. The residuals are the
+    second, non-differentiable output.
     """
 
     @staticmethod
-    def forward(ctx, slices, modes, weights, positions, slice_thickness: float, voltage_kv: float,
-                calib_ang: float, shift_calib_ang: float, ckpt_every: int = 0, batch: int = 0, tune: int = 0,
-                windows=None):
+    def forward(slices, modes, weights, positions, slice_thickness: float, voltage_kv: float, calib_ang: float,
+                shift_calib_ang: float, ckpt_every: int = 0, batch: int = 0, tune: int = 0, windows=None,
+                record: bool = True):
         lib = _lib.load()
         dev = slices.device
         S, M, P = slices.shape[2], modes.shape[2], positions.shape[0]
@@ -54,22 +65,49 @@ class Stem4dFunction(torch.autograd.Function):
         prm = ms_params(n, S, M, P, voltage_kv, slice_thickness, calib_ang, shift_calib_ang, slices.stride(),
                         modes.stride(), batch, tune, f, windows)
         out = torch.empty((P, n, n), dtype=torch.float32, device=dev)
-        res = torch.empty(lib.ptyro_ms_residual_bytes(ctypes.byref(prm), k) // 4 if P else 1,
-                          dtype=torch.float32, device=dev)
+        nres = lib.ptyro_ms_residual_bytes(ctypes.byref(prm), k) // 4 if (P and record) else 0
+        res = torch.empty(nres, dtype=torch.float32, device=dev)
         if P:
             ws_bytes = lib.ptyro_ms_workspace_bytes(ctypes.byref(prm))
             ws = _workspace(ws_bytes, dev)
-            _lib.check(lib.ptyro_ms_forward_ckpt(ctypes.byref(prm), k, slices.data_ptr(), modes.data_ptr(),
-                                                 weights.data_ptr(), positions.data_ptr(), out.data_ptr(),
-                                                 res.data_ptr(), ws.data_ptr(), ws_bytes, _stream_ptr(dev)))
-        ctx.save_for_backward(slices, modes, weights, positions, res, windows)
-        ctx.cfg = (slice_thickness, voltage_kv, calib_ang, shift_calib_ang, k, batch, tune, n, f)
-        return out
+            if record:
+                rc = lib.ptyro_ms_forward_ckpt(ctypes.byref(prm), k, slices.data_ptr(), modes.data_ptr(),
+                                               weights.data_ptr(), positions.data_ptr(), out.data_ptr(),
+                                               res.data_ptr(), ws.data_ptr(), ws_bytes, _stream_ptr(dev))
+            else:
+                rc = lib.ptyro_ms_forward(ctypes.byref(prm), slices.data_ptr(), modes.data_ptr(),
+                                          weights.data_ptr(), positions.data_ptr(), out.data_ptr(), ws.data_ptr(),
+                                          ws_bytes, _stream_ptr(dev))
+            _lib.check(rc)
+        return out, res
 
     @staticmethod
-    def backward(ctx, grad_out):
-        slices, modes, weights, positions, res, windows = ctx.saved_tensors
-        slice_thickness, voltage_kv, calib_ang, shift_calib_ang, k, batch, tune, n, f = ctx.cfg
+    def setup_context(ctx, inputs, output):
+        (slices, modes, weights, positions, slice_thickness, voltage_kv, calib_ang, shift_calib_ang, ckpt_every,
+         batch, tune, windows, record) = inputs
+        _, res = output
+        ctx.mark_non_differentiable(res)
+        ctx.save_for_backward(slices, modes, weights, positions, res, windows)
+        ctx.save_for_forward(slices, modes, weights, positions, windows)
+        n = modes.shape[0]
+        ctx.cfg = (slice_thickness, voltage_kv, calib_ang, shift_calib_ang, _ckpt_for(slices.shape[2], ckpt_every),
+                   batch, tune, n, slices.shape[0], record)
+
+    @staticmethod
+    def backward(ctx, grad_out, grad_res):
+        if not ctx.cfg[-1]:
+            raise RuntimeError("stem_4d was evaluated without residuals (record=False); no backward")
+        # under torch.func the rule sees functorch wrappers; the kernels need storage
+        saved = [_plain(t) for t in ctx.saved_tensors]
+        with torch._C._DisableFuncTorch():
+            g_slices, g_modes = Stem4dFunction._adjoint(ctx, saved, _plain(grad_out))
+        return (g_slices if ctx.needs_input_grad[0] else None, g_modes if ctx.needs_input_grad[1] else None,
+                None, None, None, None, None, None, None, None, None, None, None)
+
+    @staticmethod
+    def _adjoint(ctx, saved, grad_out):
+        slices, modes, weights, positions, res, windows = saved
+        slice_thickness, voltage_kv, calib_ang, shift_calib_ang, k, batch, tune, n, f, record = ctx.cfg
         lib = _lib.load()
         dev = slices.device
         S, M, P = slices.shape[2], modes.shape[2], positions.shape[0]
@@ -89,9 +127,21 @@ class Stem4dFunction(torch.autograd.Function):
                                              g_slices.data_ptr(), g_modes.data_ptr(), ws.data_ptr(), ws_bytes,
                                              _stream_ptr(dev)))
         # the C-ABI gives JAX's convention conj(2 dL/dconj); torch wants 2 dL/dconj
-        return (g_slices if ctx.needs_input_grad[0] else None,
-                g_modes.conj().resolve_conj() if ctx.needs_input_grad[1] else None,
-                None, None, None, None, None, None, None, None, None, None)
+        return g_slices, g_modes.conj().resolve_conj()
+
+    @staticmethod
+    def jvp(ctx, t_slices, t_modes, t_weights, t_positions, *rest):
+        # under torch.func the rule sees functorch wrappers; the kernels need storage
+        slices, modes, weights, positions, windows = (_plain(t) for t in ctx.saved_tensors)
+        t_slices, t_modes, t_weights, t_positions = (_plain(t) for t in (t_slices, t_modes, t_weights, t_positions))
+        slice_thickness, voltage_kv, calib_ang, shift_calib_ang, k, batch, tune, n, f, record = ctx.cfg
+        # torch.func.jvp hands zero tangents to the inputs it does not differentiate
+        if any(t is not None and bool(t.any()) for t in (t_weights, t_positions)):
+            raise NotImplementedError("stem_4d has no derivative with respect to weights or positions")
+        with torch._C._DisableFuncTorch():  # buffers made here must be plain tensors
+            _, tangent = jvp(slices, modes, weights, positions, t_slices, t_modes, slice_thickness, voltage_kv,
+                             calib_ang, shift_calib_ang, batch=batch, windows=windows, want_patterns=False)
+        return tangent, None
 
 
 def stem_4d_patterns(slices: torch.Tensor, modes: torch.Tensor, weights: torch.Tensor, positions: torch.Tensor,
@@ -99,10 +149,51 @@ def stem_4d_patterns(slices: torch.Tensor, modes: torch.Tensor, weights: torch.T
                      shift_calib_ang: Optional[float] = None, ckpt_every: int = DEFAULT_CKPT,
                      batch: int = 0, tune: int = 0, windows: Optional[torch.Tensor] = None) -> torch.Tensor:
     """Differentiable patterns (P, n, n) of the forward model (device tensors); with
-    ``windows`` the potential is a larger periodic field (see ``run_forward``)."""
+    ``windows`` the potential is a larger periodic field (see ``run_forward``).
+    Reverse mode (``backward``, ``torch.func.grad/vjp``) and forward mode
+    (``torch.func.jvp``, dual tensors) both run hand-written kernels."""
+    record = bool(slices.requires_grad or modes.requires_grad) and torch.is_grad_enabled()
     return Stem4dFunction.apply(slices, modes, weights, positions, float(slice_thickness), float(voltage_kv),
                                 float(calib_ang), float(calib_ang if shift_calib_ang is None else shift_calib_ang),
-                                int(ckpt_every), int(batch), int(tune), windows)
+                                int(ckpt_every), int(batch), int(tune), windows, record)[0]
+
+
+def _like(t: Optional[torch.Tensor], primal: torch.Tensor, dtype) -> Optional[torch.Tensor]:
+    """The tangent with the primal's strides (the kernels read both with one set)."""
+    if t is None:
+        return None
+    t = t.to(device=primal.device, dtype=dtype)
+    if t.shape != primal.shape:
+        raise ValueError(f"tangent shape {tuple(t.shape)} does not match {tuple(primal.shape)}")
+    if t.stride() == primal.stride():
+        return t
+    return torch.empty_strided(primal.shape, primal.stride(), dtype=dtype, device=primal.device).copy_(t)
+
+
+def jvp(slices, modes, weights, positions, tangent_slices, tangent_modes, slice_thickness, voltage_kv, calib_ang,
+        shift_calib_ang=None, batch: int = 0, windows=None, want_patterns: bool = True):
+    """(patterns or None, dI) for the tangent (tangent_slices, tangent_modes), either
+    of which may be None (zero). Runs ``ptyro_ms_jvp``: the wave and its tangent go
+    through the forward's passes together."""
+    lib = _lib.load()
+    dev = slices.device
+    S, M, P = slices.shape[2], modes.shape[2], positions.shape[0]
+    n, f = check_windows(slices, modes, windows, P)
+    sc = float(calib_ang if shift_calib_ang is None else shift_calib_ang)
+    prm = ms_params(n, S, M, P, voltage_kv, slice_thickness, calib_ang, sc, slices.stride(), modes.stride(), batch,
+                    0, f, windows)
+    ts = _like(tangent_slices, slices, torch.float32)
+    tm = _like(tangent_modes, modes, torch.complex64)
+    out = torch.empty((P, n, n), dtype=torch.float32, device=dev) if want_patterns else None
+    tan = torch.empty((P, n, n), dtype=torch.float32, device=dev)
+    if P:
+        ws_bytes = lib.ptyro_ms_jvp_workspace_bytes(ctypes.byref(prm))
+        ws = _workspace(ws_bytes, dev)
+        _lib.check(lib.ptyro_ms_jvp(ctypes.byref(prm), slices.data_ptr(), None if ts is None else ts.data_ptr(),
+                                    modes.data_ptr(), None if tm is None else tm.data_ptr(), weights.data_ptr(),
+                                    positions.data_ptr(), None if out is None else out.data_ptr(), tan.data_ptr(),
+                                    ws.data_ptr(), ws_bytes, _stream_ptr(dev)))
+    return out, tan
 
 
 def vjp(slices, modes, weights, positions, grad_patterns, slice_thickness, voltage_kv, calib_ang,

@@ -15,7 +15,7 @@ PKG = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 LIB = os.path.join(PKG, "libptyro_b200.so")
-SOURCES = ["ms_engine.cu", "diag.cu", "ms_static.cu", "ms_sched.cu", "atoms.cu"] + [f"pass_{n}.cu" for n in (16, 32, 64, 128, 256, 512, 1024)]
+SOURCES = ["ms_engine.cu", "diag.cu", "ms_static.cu", "ms_sched.cu", "atoms.cu", "ms_jvp.cu"] + [f"pass_{n}.cu" for n in (16, 32, 64, 128, 256, 512, 1024)]
 HEADERS = ["fft_core.cuh", "ms_pass.cuh", "ms_bwd.cuh", "pass_launch.cuh", "engine.cuh"]
 
 NVCC_FLAGS = [

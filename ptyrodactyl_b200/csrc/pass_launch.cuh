@@ -4,6 +4,7 @@
 #include <atomic>
 
 #include "ms_bwd.cuh"
+#include "ms_jvp.cuh"
 #include "ms_pipe.cuh"
 
 namespace ptyro {
@@ -44,6 +45,25 @@ int launch_bwd_t(const BwdArgs& a, int grid_y, cudaStream_t st) {
   }
   dim3 grid(N / Geo::kLines, grid_y);
   ms_bwd_pass_kernel<N1, N2, AXIS, W, MINB><<<grid, W * 32, smem, st>>>(a);
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  return (int)cudaGetLastError();
+}
+
+template <int N1, int N2, int AXIS>
+int launch_jvp_t(const JvpArgs& a, int grid_y, cudaStream_t st) {
+  using Geo = PassGeom<N1, N2>;
+  constexpr int N = Geo::N;
+  constexpr int W = Geo::kWarps;
+  constexpr int MINB = N2 <= 16 ? 2 : 1;
+  const size_t smem = Geo::smem_bytes(W);
+  static bool attr_done = false;
+  if (!attr_done) {
+    cudaFuncSetAttribute(ms_jvp_pass_kernel<N1, N2, AXIS, W, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)smem);
+    attr_done = true;
+  }
+  dim3 grid(N / Geo::kLines, grid_y);
+  ms_jvp_pass_kernel<N1, N2, AXIS, W, MINB><<<grid, W * 32, smem, st>>>(a);
   g_launches.fetch_add(1, std::memory_order_relaxed);
   return (int)cudaGetLastError();
 }
@@ -136,6 +156,9 @@ int launch_bwd_multi_t(const BwdArgs* descs, const int2* rows, int nrows, cudaSt
   int launch_bwd_##NN(int axis, const BwdArgs& a, int grid_y, cudaStream_t st) {                \
     return axis == 0 ? launch_bwd_t<N1, N2, 0>(a, grid_y, st) : launch_bwd_t<N1, N2, 1>(a, grid_y, st); \
   }                                                                                              \
+  int launch_jvp_##NN(int axis, const JvpArgs& a, int grid_y, cudaStream_t st) {                \
+    return axis == 0 ? launch_jvp_t<N1, N2, 0>(a, grid_y, st) : launch_jvp_t<N1, N2, 1>(a, grid_y, st); \
+  }                                                                                              \
   int launch_pass_multi_##NN(int axis, const PassArgs* d, const int2* r, int nr, cudaStream_t st,  \
                              int variant) {                                                      \
     constexpr int lo = (N2) <= 16 ? 2 : 1, hi = (N2) <= 16 ? 3 : 1;                              \
@@ -162,6 +185,13 @@ int launch_pass_multi_512(int axis, const PassArgs* d, const int2* r, int nr, cu
 int launch_bwd_multi_512(int axis, const BwdArgs* d, const int2* r, int nr, cudaStream_t st);
 int launch_pass_multi_1024(int axis, const PassArgs* d, const int2* r, int nr, cudaStream_t st, int variant);
 int launch_bwd_multi_1024(int axis, const BwdArgs* d, const int2* r, int nr, cudaStream_t st);
+int launch_jvp_16(int axis, const JvpArgs& a, int grid_y, cudaStream_t st);
+int launch_jvp_32(int axis, const JvpArgs& a, int grid_y, cudaStream_t st);
+int launch_jvp_64(int axis, const JvpArgs& a, int grid_y, cudaStream_t st);
+int launch_jvp_128(int axis, const JvpArgs& a, int grid_y, cudaStream_t st);
+int launch_jvp_256(int axis, const JvpArgs& a, int grid_y, cudaStream_t st);
+int launch_jvp_512(int axis, const JvpArgs& a, int grid_y, cudaStream_t st);
+int launch_jvp_1024(int axis, const JvpArgs& a, int grid_y, cudaStream_t st);
 int launch_bwd_16(int axis, const BwdArgs& a, int grid_y, cudaStream_t st);
 int launch_bwd_32(int axis, const BwdArgs& a, int grid_y, cudaStream_t st);
 int launch_bwd_64(int axis, const BwdArgs& a, int grid_y, cudaStream_t st);

@@ -157,6 +157,18 @@ def run_forward(slices: torch.Tensor, slice_thickness: float, modes: torch.Tenso
     return out
 
 
+def _needs_autodiff(*tensors) -> bool:
+    """True when a reverse- or forward-mode derivative will be taken through the
+    forward (requires_grad, a torch.func transform's wrapper, or a dual tensor)."""
+    from torch.autograd import forward_ad
+    for t in tensors:
+        if t.requires_grad and torch.is_grad_enabled():
+            return True
+        if torch._C._functorch.is_functorch_wrapped_tensor(t) or forward_ad.unpack_dual(t).tangent is not None:
+            return True
+    return False
+
+
 def _beam_on(beam: ProbeModes, dev) -> tuple:
     modes = beam.modes if beam.modes.ndim == 3 else beam.modes[..., None]
     modes = as_tensor(modes, torch.complex64, dev)
@@ -185,7 +197,7 @@ def stem_4d(pot_slice: PotentialSlices, beam: ProbeModes, microscope: Microscope
     modes, weights = _beam_on(beam, dev)
     positions = as_tensor(detector.scan_positions_px, torch.float64, dev).reshape(-1, 2).contiguous()
     calib = min(float(pot_slice.calib), float(beam.calib))
-    if torch.is_grad_enabled() and (slices.requires_grad or modes.requires_grad):
+    if _needs_autodiff(slices, modes):
         # differentiable path: checkpointed forward + hand-written adjoint kernel
         from .autodiff import stem_4d_patterns
         data = stem_4d_patterns(slices, modes, weights, positions, pot_slice.slice_thickness,
@@ -214,7 +226,7 @@ def stem_4d_windowed(pot_slice: PotentialSlices, beam: ProbeModes, microscope: M
     positions = as_tensor(detector.scan_positions_px, torch.float64, dev).reshape(-1, 2).contiguous()
     win = as_tensor(windows, torch.int32, dev).reshape(-1, 2).contiguous()
     calib = min(float(pot_slice.calib), float(beam.calib))
-    if torch.is_grad_enabled() and (slices.requires_grad or modes.requires_grad):
+    if _needs_autodiff(slices, modes):
         from .autodiff import stem_4d_patterns
         data = stem_4d_patterns(slices, modes, weights, positions, pot_slice.slice_thickness,
                                 microscope.voltage_kv, calib, detector.real_space_calib_ang, windows=win)

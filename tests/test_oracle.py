@@ -132,3 +132,41 @@ def test_product_mask_matches_oracle_mask():
     from ptyrodactyl_b200.detectors import annular_mask
     for n, fc, kv, a, b in [(64, 0.05, 200.0, 10.0, 40.0), (128, 0.03, 300.0, 0.0, 25.0), (16, 0.2, 80.0, 5.0, 5.0)]:
         assert np.array_equal(annular_mask((n, n), fc, kv, a, b), R.annular_mask((n, n), fc, kv, a, b))
+
+
+def _jvp_case(seed=9, n=16, s=3, m=2):
+    rng = np.random.default_rng(seed)
+    pot = rng.uniform(0, 30, (n, n, s))
+    probe = R.make_probe(200.0, 25.0, (n, n), 40.0, defocus_ang=-20.0)
+    beam = np.stack([probe * np.exp(0.3j * k) * (1.0 - 0.3 * k) for k in range(m)], axis=-1)
+    w = np.linspace(1.0, 0.5, m)
+    w = w / w.sum()
+    pos = np.array([[0.3, -0.4], [1.2, 0.7]])
+    dv = rng.normal(size=pot.shape)
+    db = (rng.normal(size=beam.shape) + 1j * rng.normal(size=beam.shape)) * 0.01
+    return pot, beam, w, pos, dv, db
+
+
+def test_oracle_jvp_matches_finite_differences():
+    pot, beam, w, pos, dv, db = _jvp_case()
+    args = (1.5, 0.4)
+
+    def f(v, b):
+        return R.stem_4d(v, 1.5, 0.4, b, w, 0.4, 200.0, pos, 0.4)["data"]
+
+    data, dd = R.stem_4d_jvp(pot, *args, beam, w, 0.4, 200.0, pos, 0.4, dslices=dv, dbeam=db)
+    assert np.allclose(data, f(pot, beam), rtol=1e-12, atol=1e-14)
+    eps = 1e-5
+    fd = (f(pot + eps * dv, beam + eps * db) - f(pot - eps * dv, beam - eps * db)) / (2 * eps)
+    assert np.max(np.abs(fd - dd)) <= 1e-6 * np.max(np.abs(dd))
+
+
+def test_oracle_jvp_is_the_transpose_of_the_vjp():
+    """<J v, g> = <dV, vV> + Re sum(dbeam_jax * vbeam) (dot-product test)."""
+    pot, beam, w, pos, dv, db = _jvp_case(seed=4)
+    g = np.random.default_rng(1).normal(size=(2, 16, 16))
+    _, dd = R.stem_4d_jvp(pot, 1.5, 0.4, beam, w, 0.4, 200.0, pos, 0.4, dslices=dv, dbeam=db)
+    gv, gb = R.stem_4d_vjp(pot, 1.5, 0.4, beam, w, 0.4, 200.0, pos, 0.4, g)
+    lhs = np.sum(dd * g)
+    rhs = np.sum(gv * dv) + np.real(np.sum(gb * db))
+    assert abs(lhs - rhs) <= 1e-10 * abs(lhs)
