@@ -84,12 +84,12 @@ struct PassGeom {
   static constexpr int kWarps = N / G < 8 ? N / G : 8;  // lines per CTA = kWarps * G divides N
   static constexpr int kLines = kWarps * G;
   static int warps_for() { return kWarps; }
-  // twiddle table + max(exchange buffers, column tile)
+  // twiddle table + propagator factor + max(exchange buffers, column tile)
   static size_t smem_bytes(int warps) {
     const size_t lines = (size_t)warps * G;
     const size_t xbuf = lines * LineBuf<N1, N2>::kSize;
     const size_t tile = (size_t)N * (lines + G);
-    return sizeof(float2) * ((size_t)N + (xbuf > tile ? xbuf : tile));
+    return sizeof(float2) * ((size_t)2 * N + (xbuf > tile ? xbuf : tile));
   }
   // steady passes also keep the transmission rows of their lines (prefetched)
   static size_t smem_bytes_steady(int warps) { return smem_bytes(warps) + sizeof(float2) * (size_t)warps * G * N; }
@@ -148,7 +148,7 @@ __device__ __forceinline__ const float2* trans_row(const float2* trans, const fl
 // op on registers in natural distribution; returns true if the result is k-order.
 template <int N1, int N2>
 __device__ __forceinline__ bool apply_op(int op, float2 (&v)[N2], int t, float2* buf, const float2* tw,
-                                         const float2* __restrict__ pf) {
+                                         const float2* pf) {
   if (op == OP_FFT) {
     line_nat_to_k<N1, N2, -1>(v, t, buf, tw);
     return true;
@@ -157,7 +157,7 @@ __device__ __forceinline__ bool apply_op(int op, float2 (&v)[N2], int t, float2*
     line_nat_to_k<N1, N2, -1>(v, t, buf, tw);
 #pragma unroll
     for (int r = 0; r < N2; ++r) {
-      const float2 p = __ldg(pf + korder_index<N1, N2>(t, r));
+      const float2 p = pf[korder_index<N1, N2>(t, r)];
       v[r] = op == OP_CONV ? cmul(v[r], p) : cmulc(v[r], p);
     }
     line_k_to_nat<N1, N2, +1>(v, t, buf, tw);
@@ -182,11 +182,13 @@ __device__ __forceinline__ void pass_body(const PassArgs& a, const int yslot) {
   constexpr int N = Geo::N;
   constexpr int G = Geo::G;
   extern __shared__ float2 smem[];
-  float2* tw = smem;        // tw[k2 * N1 + t] = W_N^{t k2}
-  float2* work = smem + N;  // exchange buffers; column passes alias the staging tile here
+  float2* tw = smem;            // tw[k2 * N1 + t] = W_N^{t k2}
+  float2* pfs = smem + N;       // propagator factor along this axis
+  float2* work = smem + 2 * N;  // exchange buffers; column passes alias the staging tile here
   for (int i = threadIdx.x; i < N; i += blockDim.x) {
     const int k2 = i / N1, tt = i % N1;
     tw[i] = a.tw[(tt * k2) % N];
+    if (a.pf) pfs[i] = a.pf[i];
   }
   __syncthreads();
 
@@ -270,7 +272,7 @@ __device__ __forceinline__ void pass_body(const PassArgs& a, const int yslot) {
       for (int j = 0; j < N2; ++j) v[j] = cscale(v[j], a.scale);
       korder = false;
     } else if (op1 != OP_NONE) {
-      korder = apply_op<N1, N2>(op1, v, t, buf, tw, a.pf);
+      korder = apply_op<N1, N2>(op1, v, t, buf, tw, pfs);
     }
     // ---- transmission (natural distribution; row-major table for rows, transposed for columns)
     if (has_t) {
@@ -296,7 +298,7 @@ __device__ __forceinline__ void pass_body(const PassArgs& a, const int yslot) {
       }
     }
     // ---- op2
-    if (op2 != OP_NONE) korder = apply_op<N1, N2>(op2, v, t, buf, tw, a.pf);
+    if (op2 != OP_NONE) korder = apply_op<N1, N2>(op2, v, t, buf, tw, pfs);
     // ---- store
     if (to_pattern) {
       const float wm = a.weights[m];
