@@ -222,7 +222,7 @@ def run_ours(args, rank, world, local_rank):
         # the same forward captured once as a CUDA graph; a step is one replay
         from ptyrodactyl_b200.graphs import GraphedForward
         graphed = GraphedForward(slices_d, modes_d, weights_d, pos_d, synth.SLICE_DZ, w.voltage_kv, w.calib,
-                                 batch=args.batch, tune=args.tune)
+                                 batch=args.batch, tune=args.tune, lanes=args.lanes)
         out_d = graphed.out
         ws, ws_bytes, prm = graphed.ws, graphed.ws_bytes, graphed.prm  # the steady-pass timing reuses them
 
@@ -365,7 +365,7 @@ def run_ours(args, rank, world, local_rank):
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": w.name, "grid": n, "slices": S, "probes_per_gpu": P, "modes": 1,
-                       "batch": batch, "tune": args.tune, "cuda_graph": bool(args.graph), "voltage_kv": w.voltage_kv, "aperture_mrad": w.aperture_mrad,
+                       "batch": batch, "tune": args.tune, "cuda_graph": bool(args.graph), "lanes": args.lanes if args.graph else 1, "voltage_kv": w.voltage_kv, "aperture_mrad": w.aperture_mrad,
                        "defocus_ang": w.defocus_ang, "c3_ang": w.c3_ang,
                        "l2": "flushed (256 MB write) before every timed step",
                        "parallelism": f"dp{world} (probe shards, no collective)"},
@@ -680,6 +680,7 @@ def main():
     ap.add_argument("--batch", type=int, default=0)
     ap.add_argument("--tune", type=int, default=3, help="pass-kernel occupancy variant bits")
     ap.add_argument("--graph", type=int, default=1, help="1: time CUDA-graph replays of the captured forward")
+    ap.add_argument("--lanes", type=int, default=2, help="concurrent probe ranges (streams) in the captured forward")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")

@@ -73,6 +73,7 @@ struct PassArgs {
   const uint32_t* det_mask;
   float* det_part;
   int n_det;
+  int direct;              // column passes: read and write the columns straight from global memory
 };
 
 template <int N1, int N2>
@@ -243,7 +244,7 @@ __device__ __forceinline__ void pass_body(const PassArgs& a, const int yslot) {
         const int k = korder_index<N1, N2>(t, r);
         v[r] = cmul(cmul(pk[off(k)], ra[k]), rl);
       }
-    } else if (AXIS == 0) {
+    } else if (AXIS == 0 || a.direct) {
       if (load_k) {
 #pragma unroll
         for (int r = 0; r < N2; ++r) v[r] = w[off(korder_index<N1, N2>(t, r))];
@@ -309,7 +310,7 @@ __device__ __forceinline__ void pass_body(const PassArgs& a, const int yslot) {
 #pragma unroll
         for (int r = 0; r < N2; ++r) am[off(korder_index<N1, N2>(t, r))] = v[r];
       }
-    } else if (AXIS == 0) {
+    } else if (AXIS == 0 || a.direct) {
       if (korder) {
 #pragma unroll
         for (int r = 0; r < N2; ++r) w[off(korder_index<N1, N2>(t, r))] = v[r];

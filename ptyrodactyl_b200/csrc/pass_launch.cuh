@@ -100,7 +100,10 @@ int launch_pipe_t(const PassArgs& a, int nslots, cudaStream_t st) {
 // tune bit 2 (value 4) selects the persistent double-buffered kernel for steady
 // passes (measured slower than the one-slot-per-CTA kernel on B200 at 128-512^2)
 template <int N1, int N2, int AXIS, int MINB>
-int launch_pass_t(const PassArgs& a, int grid_y, cudaStream_t st, int variant) {
+int launch_pass_t(const PassArgs& a0, int grid_y, cudaStream_t st, int variant) {
+  // tune bit 3 (value 8): column passes access global memory directly (no staging tile)
+  PassArgs a = a0;
+  if (AXIS == 1 && (variant & 8)) a.direct = 1;
   if (is_steady_pass(a) && a.tw2 != nullptr && (variant & 4)) return launch_pipe_t<N1, N2, AXIS, MINB>(a, grid_y, st);
   return is_steady_pass(a) ? launch_pass_s<N1, N2, AXIS, MINB, true>(a, grid_y, st)
                            : launch_pass_s<N1, N2, AXIS, MINB, false>(a, grid_y, st);

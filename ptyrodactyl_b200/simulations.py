@@ -123,22 +123,55 @@ def check_windows(slices: torch.Tensor, modes: torch.Tensor, windows: Optional[t
     return n, f
 
 
+_LANE_MIN_WAVE_BYTES = 256 << 20  # two lanes once the probes' waves span about four batches
+
+
+def _side_streams(dev: torch.device, count: int) -> list:
+    key = (dev.index, count)
+    if key not in _STREAMS:
+        _STREAMS[key] = [torch.cuda.Stream(device=dev) for _ in range(count)]
+    return _STREAMS[key]
+
+
+_STREAMS: dict = {}
+
+
 def run_forward(slices: torch.Tensor, slice_thickness: float, modes: torch.Tensor, weights: torch.Tensor,
                 positions: torch.Tensor, voltage_kv: float, calib_ang: float, shift_calib_ang: float,
                 out: Optional[torch.Tensor] = None, batch: int = 0, plain: bool = False,
-                tune: int = 0, windows: Optional[torch.Tensor] = None, accumulate: bool = False) -> torch.Tensor:
+                tune: int = 0, windows: Optional[torch.Tensor] = None, accumulate: bool = False,
+                lanes: int = 0) -> torch.Tensor:
     """Device-level forward: all tensors already on one CUDA device.
 
     slices (F, F, S) float32 (any strides), modes (n, n, M) complex64 (any strides),
     weights (M,) float32, positions (P, 2) float64 contiguous. F == n, or F > n with
     ``windows`` (P, 2) int32: probe p then reads the n x n window of the periodic
     field starting at windows[p]. Returns patterns (P, n, n) float32; with
-    ``accumulate`` the intensities are added into ``out`` instead.
+    ``accumulate`` the intensities are added into ``out`` instead. ``lanes`` > 1
+    runs contiguous probe ranges as concurrent forwards on side streams (0: two
+    lanes when the probes' waves exceed 256 MiB); results do not depend on it.
     """
     lib = _lib.load()
     dev = slices.device
     num_probes = positions.shape[0]
     n, f = check_windows(slices, modes, windows, num_probes)
+    if lanes == 0:
+        lanes = 2 if (not plain and num_probes * n * n * modes.shape[2] * 8 >= _LANE_MIN_WAVE_BYTES) else 1
+    if lanes > 1 and num_probes >= lanes:
+        if out is None:
+            out = (torch.zeros if accumulate else torch.empty)((num_probes, n, n), dtype=torch.float32, device=dev)
+        main = torch.cuda.current_stream(dev)
+        bounds = [num_probes * i // lanes for i in range(lanes + 1)]
+        streams = _side_streams(dev, lanes)
+        for (lo, hi), st in zip(zip(bounds[:-1], bounds[1:]), streams):
+            st.wait_stream(main)
+            with torch.cuda.stream(st):
+                run_forward(slices, slice_thickness, modes, weights, positions[lo:hi], voltage_kv, calib_ang,
+                            shift_calib_ang, out=out[lo:hi], batch=batch, plain=plain, tune=tune,
+                            windows=None if windows is None else windows[lo:hi], accumulate=accumulate, lanes=1)
+        for st in streams:
+            main.wait_stream(st)
+        return out
     prm = ms_params(n, slices.shape[2], modes.shape[2], num_probes, voltage_kv, slice_thickness,
                     calib_ang, shift_calib_ang, slices.stride(), modes.stride(), batch, tune, f, windows,
                     _lib.PTYRO_FLAG_ACCUMULATE if accumulate else 0)

@@ -58,3 +58,25 @@ def test_autotune_picks_and_caches(case, tmp_path, monkeypatch):
     got = pb.run_forward(pot, synth.SLICE_DZ, modes, wts, pos, w.voltage_kv, w.calib, w.calib, batch=batch,
                          tune=tune)
     assert torch.equal(ref, got)
+
+
+def test_lanes_do_not_change_results():
+    import numpy as np
+    from oracle import multislice_ref as R
+    from ptyrodactyl_b200.graphs import GraphedForward
+    from ptyrodactyl_b200.simulations import run_forward
+    rng = np.random.default_rng(21)
+    n, s, p = 64, 5, 37
+    dev = torch.device("cuda")
+    slices = torch.as_tensor(rng.uniform(0, 40, (n, n, s)), dtype=torch.float32, device=dev)
+    probe = R.make_probe(200.0, 25.0, (n, n), 30.0, defocus_ang=-20.0)
+    modes = torch.as_tensor(probe[..., None].astype(np.complex64), device=dev)
+    wt = torch.ones(1, device=dev)
+    pos = torch.as_tensor(rng.uniform(-2, 2, (p, 2)), dtype=torch.float64, device=dev)
+    one = run_forward(slices, 1.7, modes, wt, pos, 200.0, 0.3, 0.3, batch=4, lanes=1)
+    three = run_forward(slices, 1.7, modes, wt, pos, 200.0, 0.3, 0.3, batch=4, lanes=3)
+    assert torch.equal(one, three)
+    g = GraphedForward(slices, modes, wt, pos, 1.7, 200.0, 0.3, batch=4, lanes=2)
+    g.replay()
+    torch.cuda.synchronize()
+    assert torch.equal(g.out, one)
