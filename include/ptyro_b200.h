@@ -133,6 +133,25 @@ int ptyro_ms_forward_plain(const ptyro_ms_params* p, const float* potential, con
                            const float* weights, const double* positions, float* patterns,
                            void* workspace, size_t workspace_bytes, void* stream);
 
+/* ptyro_ms_forward with a beam tilt per mode: tilts is complex64 (M, 2, n), row
+ * [m][0] the factors along y and [m][1] along x, multiplied into mode m's wave in real
+ * space after the scan shift, before the first slice. This is the tilt phase ramp
+ * that cbed_image's ensemble branch applies per coherence sample
+ * (_apply_tilt_phase_ramp, src/ptyrodactyl/multislice/simulations.py:891-946), after
+ * stem_4d's scan shift. Workspace: ptyro_ms_workspace_bytes(p). */
+int ptyro_ms_forward_tilted(const ptyro_ms_params* p, const float* potential, const float* modes,
+                            const float* weights, const double* positions, const float* tilts, float* patterns,
+                            void* workspace, size_t workspace_bytes, void* stream);
+
+/* Complex far-field amplitudes of every (probe, mode): complex64 (P, M, n, n),
+ * fftshifted. Replaces cbed_amplitude (src/ptyrodactyl/multislice/simulations.py:
+ * 606-679) at the probe's own place (positions zero) or shifted per position as in
+ * stem_4d. tilts as in ptyro_ms_forward_tilted, or NULL. No weights: nothing is
+ * summed. PTYRO_FLAG_ACCUMULATE is rejected. Workspace: ptyro_ms_workspace_bytes(p). */
+int ptyro_ms_amplitudes(const ptyro_ms_params* p, const float* potential, const float* modes,
+                        const double* positions, const float* tilts, float* amplitudes, void* workspace,
+                        size_t workspace_bytes, void* stream);
+
 /* Workspace bytes ptyro_ms_jvp needs for `p` (0 when invalid). */
 size_t ptyro_ms_jvp_workspace_bytes(const ptyro_ms_params* p);
 

@@ -392,3 +392,92 @@ def stem_4d_jvp(slices, slice_thickness, pot_calib, beam_modes, weights, beam_ca
         data[i] = np.einsum("m,hwm->hw", w, np.abs(amp) ** 2)
         ddata[i] = np.einsum("m,hwm->hw", w, 2.0 * np.real(np.conj(amp) * damp))
     return data, ddata
+
+
+# ---------------------------------------------------------------------------
+# Ensemble axes: cbed_image's ensemble branch (simulations.py:1163-1193) with
+# bind_cbed_axes (:769-888), _apply_tilt_phase_ramp (:891-946) and
+# apply_distributions (multislice/reduce.py:92-201); the Gauss-Hermite producers
+# of multislice/producers.py:46-290. An axis is (samples (N, D), weights (N,),
+# reduction "coherent" | "incoherent", axis_id).
+# ---------------------------------------------------------------------------
+
+
+def gauss_hermite_normal(n_quad):
+    x, w = np.polynomial.hermite.hermgauss(int(n_quad))
+    return np.sqrt(2.0) * x, w / np.sqrt(np.pi)
+
+
+def jitter_axis(sigma_ang, n_quad):
+    nodes, weights = gauss_hermite_normal(n_quad)
+    d = sigma_ang * nodes if sigma_ang > 0 else np.zeros_like(nodes)
+    dy, dx = np.meshgrid(d, d, indexing="ij")
+    wy, wx = np.meshgrid(weights, weights, indexing="ij")
+    w = (wy * wx).reshape(-1)
+    return np.stack((dy.reshape(-1), dx.reshape(-1)), axis=1), w / w.sum(), "incoherent", "position_jitter"
+
+
+def coherence_axis(energy_spread_ev, divergence_mrad, n_quad):
+    nodes, weights = gauss_hermite_normal(n_quad)
+    e = energy_spread_ev * nodes if energy_spread_ev > 0 else np.zeros_like(nodes)
+    t = divergence_mrad * nodes if divergence_mrad > 0 else np.zeros_like(nodes)
+    eg, txg, tyg = np.meshgrid(e, t, t, indexing="ij")
+    we, wx, wy = np.meshgrid(weights, weights, weights, indexing="ij")
+    w = (we * wx * wy).reshape(-1)
+    samples = np.stack((eg.reshape(-1), txg.reshape(-1), tyg.reshape(-1)), axis=1)
+    return samples, w / w.sum(), "incoherent", "coherence"
+
+
+def tilt_phase_ramp(modes, tilt_mrad, voltage_kv, calib_ang):
+    h, w = modes.shape[0], modes.shape[1]
+    y = (np.arange(h, dtype=np.float64) - (h - 1) / 2.0) * calib_ang
+    x = (np.arange(w, dtype=np.float64) - (w - 1) / 2.0) * calib_ang
+    yy, xx = np.meshgrid(y, x, indexing="ij")
+    phase = (2.0 * np.pi / relativistic_wavelength_ang(voltage_kv)) * (
+        tilt_mrad[0] / 1000.0 * xx + tilt_mrad[1] / 1000.0 * yy)
+    return modes * np.exp(1j * phase)[..., None]
+
+
+def ensemble_cbed(slices, slice_thickness, pot_calib, beam_modes, beam_calib, voltage_kv, axes):
+    """CBED intensity of an ensemble: beam_modes (H, W, M) already at its place."""
+    beam_modes = np.atleast_3d(np.asarray(beam_modes)).astype(np.complex128)
+    calib = min(float(pot_calib), float(beam_calib))
+    counts = [a[0].shape[0] for a in axes]
+    amps = np.empty(tuple(counts) + beam_modes.shape[:2], np.complex128)
+    for idx in np.ndindex(*counts):
+        mode, delta, de, tilt = 0, np.zeros(2), 0.0, np.zeros(2)
+        for (samples, _, _, axis_id), k in zip(axes, idx):
+            row = samples[k]
+            if axis_id == "probe_modes":
+                mode = int(row[0])
+            elif axis_id == "position_jitter":
+                delta = delta + row
+            else:
+                de, tilt = de + row[0], tilt + row[1:3]
+        volt = voltage_kv + de / 1000.0
+        sel = beam_modes[:, :, mode:mode + 1]
+        shifted = shift_beam_fourier(sel, delta[None, :], calib)[0]
+        tilted = tilt_phase_ramp(shifted, tilt, volt, calib)
+        amps[idx] = cbed_amplitude(slices, slice_thickness, volt, calib, tilted)[..., 0]
+    field = amps
+    labels = list(range(len(axes)))
+    for ax in sorted([i for i, a in enumerate(axes) if a[2] == "coherent"], reverse=True):
+        cur = labels.index(ax)
+        field = np.sum(np.moveaxis(field, cur, -1) * axes[ax][1], axis=-1)
+        labels.pop(cur)
+    inten = np.abs(field) ** 2
+    for ax in sorted([i for i, a in enumerate(axes) if a[2] == "incoherent"], reverse=True):
+        cur = labels.index(ax)
+        inten = np.sum(np.moveaxis(inten, cur, -1) * axes[ax][1], axis=-1)
+        labels.pop(cur)
+    return inten
+
+
+def stem_4d_ensemble(slices, slice_thickness, pot_calib, beam_modes, beam_calib, voltage_kv, scan_positions_px,
+                     real_space_calib_ang, axes):
+    """stem_4d whose microscope carries ensemble axes: per position the scan-shifted
+    beam through ensemble_cbed (simulations.py:1386-1427)."""
+    positions = np.atleast_2d(np.asarray(scan_positions_px, dtype=np.float64))
+    shifted = shift_beam_fourier(beam_modes, positions, real_space_calib_ang)
+    return np.stack([ensemble_cbed(slices, slice_thickness, pot_calib, shifted[i], beam_calib, voltage_kv, axes)
+                     for i in range(positions.shape[0])])

@@ -8,6 +8,10 @@ and run hand-written sm_100a CUDA through the C-ABI in ``include/ptyro_b200.h``.
 from .types import (  # noqa: F401
     STEM4D,
     AtomicSliceData,
+    Distribution,
+    ReductionMode,
+    create_distribution,
+    create_ensemble_axes,
     CalibratedArray,
     DetectorConfig,
     EnsembleAxes,
@@ -23,6 +27,7 @@ from .types import (  # noqa: F401
     create_stem4d,
 )
 from .simulations import (  # noqa: F401
+    cbed_amplitude,
     cbed_image,
     fft2,
     interaction_sigma,
@@ -45,5 +50,11 @@ from .detectors import (  # noqa: F401
 )
 from .autodiff import Stem4dFunction, jvp, make_probe_differentiable, stem_4d_patterns, vjp  # noqa: F401
 from . import jacobian  # noqa: F401
+from .ensemble import (  # noqa: F401
+    coherence_to_distribution,
+    ensemble_axes_for_cbed,
+    position_jitter_to_distribution,
+    probe_modes_to_distribution,
+)
 
 __version__ = "0.1.0"

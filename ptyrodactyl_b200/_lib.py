@@ -41,6 +41,8 @@ EXPORTED_SYMBOLS = (
     "ptyro_detect_patterns",
     "ptyro_ms_jvp_workspace_bytes",
     "ptyro_ms_jvp",
+    "ptyro_ms_forward_tilted",
+    "ptyro_ms_amplitudes",
     "ptyro_ms_residual_bytes",
     "ptyro_ms_forward_ckpt",
     "ptyro_ms_backward_workspace_bytes",
@@ -184,6 +186,10 @@ def _declare(lib) -> None:
     lib.ptyro_ms_jvp_workspace_bytes.argtypes = [pp]
     lib.ptyro_ms_jvp.restype = ctypes.c_int
     lib.ptyro_ms_jvp.argtypes = [pp, vp, vp, vp, vp, vp, vp, vp, vp, vp, sz, vp]
+    lib.ptyro_ms_forward_tilted.restype = ctypes.c_int
+    lib.ptyro_ms_forward_tilted.argtypes = [pp, vp, vp, vp, vp, vp, vp, vp, sz, vp]
+    lib.ptyro_ms_amplitudes.restype = ctypes.c_int
+    lib.ptyro_ms_amplitudes.argtypes = [pp, vp, vp, vp, vp, vp, vp, sz, vp]
     lib.ptyro_atom_slices_workspace_bytes.restype = sz
     lib.ptyro_atom_slices_workspace_bytes.argtypes = [i32, i32]
     lib.ptyro_atom_slices.restype = ctypes.c_int

@@ -410,9 +410,16 @@ struct DetOut {
   double* out;  // (P, n_det)
 };
 
+// Optional extras of a forward: beam tilts (M, 2, n) applied after the probe's
+// inverse transform, and fftshifted amplitudes (P, M, n, n) stored by the pattern pass.
+struct FwdExtras {
+  const float2* tilt;
+  float2* amplitudes;
+};
+
 static FwdPlan fwd_pass_plan(const ptyro_ms_params* p, const FwdBuffers& B, const float* weights, float* patterns,
                              float2* res_base, int ckpt_every, int C, int b0, int nb, int k,
-                             const DetOut* det = nullptr) {
+                             const DetOut* det = nullptr, const FwdExtras* ex = nullptr) {
   const int n = p->n, S = p->num_slices, M = p->num_modes;
   const size_t nn = (size_t)n * n;
   FwdPlan r;
@@ -444,6 +451,7 @@ static FwdPlan fwd_pass_plan(const ptyro_ms_params* p, const FwdBuffers& B, cons
     a.op2 = k == S ? OP_FFT : OP_CONV;
     a.dst = DST_WAVE;
     if (res_base && (k - 1) % ckpt_every == 0) a.ckpt_store = res_base + (size_t)((k - 1) / ckpt_every) * nn;
+    if (ex && k == 1) a.tilt = ex->tilt;
     r.axis = k % 2;
     r.rows = nb * M;
   } else {  // last axis of the FFT2, |.|^2, fftshifted store
@@ -456,6 +464,11 @@ static FwdPlan fwd_pass_plan(const ptyro_ms_params* p, const FwdBuffers& B, cons
       a.n_det = det->n_det;
     }
     if (res_base) a.amp_store = res_base + (size_t)C * nn;
+    if (ex && ex->amplitudes) {
+      a.amp_store = ex->amplitudes + (size_t)b0 * M * nn;
+      a.res_stride = nn;
+      a.amp_shift = 1;
+    }
     r.axis = (S + 1) % 2;
     r.rows = nb;
   }
@@ -530,12 +543,15 @@ static int detect_patterns(const float* patterns, int count, int n, const uint32
 
 static int forward_impl(const ptyro_ms_params* p, int ckpt_every, const float* potential, const float* modes,
                         const float* weights, const double* positions, float* patterns, float2* residuals,
-                        void* workspace, size_t workspace_bytes, void* stream, const DetOut* det_in = nullptr) {
+                        void* workspace, size_t workspace_bytes, void* stream, const DetOut* det_in = nullptr,
+                        const FwdExtras* ex = nullptr) {
   int rc = validate(p);
   if (rc) return rc;
   if (p->num_probes == 0) return PTYRO_OK;
   const bool has_det = det_in && det_in->n_det > 0;
-  if (!potential || !modes || !weights || !positions || (!patterns && !has_det))
+  const bool has_amp = ex && ex->amplitudes;
+  if (!potential || !modes || !positions || (!patterns && !has_det && !has_amp) ||
+      (!weights && (patterns || has_det)))
     return fail(PTYRO_ERR_INVALID, "NULL array argument");
   if (has_det && (!det_in->mask || !det_in->out)) return fail(PTYRO_ERR_INVALID, "NULL detector argument");
   const Layout L = layout_for(p);
@@ -569,7 +585,7 @@ static int forward_impl(const ptyro_ms_params* p, int ckpt_every, const float* p
     if ((rc = check_launch("k_ramps"))) return rc;
     for (int k = 0; k <= S + 1; ++k) {
       const FwdPlan f = fwd_pass_plan(p, B, weights, patterns, res_base, ckpt_every, C, b0, nb, k,
-                                      has_det ? &det : nullptr);
+                                      has_det ? &det : nullptr, ex);
       if ((rc = launch_pass(n, f.axis, f.a, f.rows, st, p->tune))) return rc;
     }
     if (has_det) {

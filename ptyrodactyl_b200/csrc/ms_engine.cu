@@ -56,6 +56,26 @@ int ptyro_detect_patterns(const float* patterns, int64_t num_patterns, int32_t n
   return detect_patterns(patterns, (int)num_patterns, n, det_mask, num_det, det_out, (cudaStream_t)stream);
 }
 
+int ptyro_ms_forward_tilted(const ptyro_ms_params* p, const float* potential, const float* modes,
+                            const float* weights, const double* positions, const float* tilts, float* patterns,
+                            void* workspace, size_t workspace_bytes, void* stream) {
+  if (!tilts && p && p->num_probes > 0) return fail(PTYRO_ERR_INVALID, "tilts is NULL");
+  const FwdExtras ex = {(const float2*)tilts, nullptr};
+  return forward_impl(p, 0, potential, modes, weights, positions, patterns, nullptr, workspace, workspace_bytes,
+                      stream, nullptr, &ex);
+}
+
+int ptyro_ms_amplitudes(const ptyro_ms_params* p, const float* potential, const float* modes,
+                        const double* positions, const float* tilts, float* amplitudes, void* workspace,
+                        size_t workspace_bytes, void* stream) {
+  if (!amplitudes && p && p->num_probes > 0) return fail(PTYRO_ERR_INVALID, "amplitudes is NULL");
+  if (p && (p->flags & PTYRO_FLAG_ACCUMULATE))
+    return fail(PTYRO_ERR_INVALID, "amplitudes cannot be accumulated");
+  const FwdExtras ex = {(const float2*)tilts, (float2*)amplitudes};
+  return forward_impl(p, 0, potential, modes, nullptr, positions, nullptr, nullptr, workspace, workspace_bytes,
+                      stream, nullptr, &ex);
+}
+
 size_t ptyro_ms_residual_bytes(const ptyro_ms_params* p, int32_t ckpt_every) {
   if (validate(p) || ckpt_every < 1) return 0;
   const int C = (p->num_slices + ckpt_every - 1) / ckpt_every;

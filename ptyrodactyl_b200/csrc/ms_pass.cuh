@@ -74,6 +74,11 @@ struct PassArgs {
   float* det_part;
   int n_det;
   int direct;              // column passes: read and write the columns straight from global memory
+  // beam tilt per mode: (M, 2, N) complex factors, [m][0][y] and [m][1][x], applied
+  // in real space right after the probe's inverse transform completes (the pass with
+  // src == SRC_WAVE and op1 == OP_IFFT), or null
+  const float2* tilt;
+  int amp_shift;           // amp_store receives the fftshifted amplitude with plane stride res_stride
 };
 
 template <int N1, int N2>
@@ -275,6 +280,15 @@ __device__ __forceinline__ void pass_body(const PassArgs& a, const int yslot) {
     } else if (op1 != OP_NONE) {
       korder = apply_op<N1, N2>(op1, v, t, buf, tw, pfs);
     }
+    // ---- beam tilt (real space, natural distribution)
+    if (!STEADY && a.tilt && src == SRC_WAVE && op1 == OP_IFFT) {
+      const float2* ty = a.tilt + (size_t)(slot % a.n_modes) * 2 * N;
+      const float2* tx = ty + N;
+      const float2 tl = AXIS == 0 ? ty[line] : tx[line];
+      const float2* te = AXIS == 0 ? tx : ty;
+#pragma unroll
+      for (int j = 0; j < N2; ++j) v[j] = cmul(v[j], cmul(te[t + N1 * j], tl));
+    }
     // ---- transmission (natural distribution; row-major table for rows, transposed for columns)
     if (has_t) {
       if (pre) {
@@ -302,13 +316,24 @@ __device__ __forceinline__ void pass_body(const PassArgs& a, const int yslot) {
     if (op2 != OP_NONE) korder = apply_op<N1, N2>(op2, v, t, buf, tw, pfs);
     // ---- store
     if (to_pattern) {
-      const float wm = a.weights[m];
+      if (a.pattern || a.n_det > 0) {
+        const float wm = a.weights[m];
 #pragma unroll
-      for (int r = 0; r < N2; ++r) acc[r] = fmaf(wm, fmaf(v[r].x, v[r].x, v[r].y * v[r].y), acc[r]);
+        for (int r = 0; r < N2; ++r) acc[r] = fmaf(wm, fmaf(v[r].x, v[r].x, v[r].y * v[r].y), acc[r]);
+      }
       if (a.amp_store) {
         float2* am = a.amp_store + (size_t)slot * a.res_stride;
+        if (a.amp_shift) {
+          const int ls = (line + N / 2) % N;
 #pragma unroll
-        for (int r = 0; r < N2; ++r) am[off(korder_index<N1, N2>(t, r))] = v[r];
+          for (int r = 0; r < N2; ++r) {
+            const int ks = (korder_index<N1, N2>(t, r) + N / 2) % N;
+            am[AXIS == 0 ? (size_t)ls * N + ks : (size_t)ks * N + ls] = v[r];
+          }
+        } else {
+#pragma unroll
+          for (int r = 0; r < N2; ++r) am[off(korder_index<N1, N2>(t, r))] = v[r];
+        }
       }
     } else if (AXIS == 0 || a.direct) {
       if (korder) {

@@ -1,0 +1,281 @@
+"""Ensemble axes of the forward model: probe modes, position jitter and partial
+coherence, reduced the way the reference's cbed_image ensemble branch reduces them
+(multislice/simulations.py:1163-1193, bind_cbed_axes :769-888,
+multislice/reduce.py:92-201).
+
+Per Cartesian sample of the axes the reference selects a probe mode, shifts it by
+the jitter, applies the coherence sample's beam tilt (a real-space phase ramp, after
+stem_4d's scan shift) at the energy-shifted voltage, runs the slice loop, sums the
+COHERENT axes' weighted amplitudes and the INCOHERENT axes' weighted intensities.
+
+Here the samples become *virtual modes* of the batched engine. The slice loop is
+linear in its input wave for a fixed voltage, so every incoherent combination of
+samples is one virtual mode: the coherent samples' jitter-shifted modes summed with
+their weights (they must share one energy and tilt), with the combination's
+product weight as the mode weight and its tilt applied by the engine after the scan
+shift (``ptyro_ms_forward_tilted``). Virtual modes are grouped by energy; each group
+is one engine call at its voltage, accumulating into the same patterns.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import itertools
+import math
+from typing import List, Optional, Tuple
+
+import numpy as np
+import torch
+
+from . import _lib
+from .simulations import (
+    _device,
+    _stream_ptr,
+    _workspace,
+    check_windows,
+    fft2,
+    ms_params,
+    relativistic_wavelength_ang,
+)
+from .types import (
+    Distribution,
+    EnsembleAxes,
+    ProbeModes,
+    ReductionMode,
+    as_tensor,
+    create_distribution,
+)
+
+AXIS_PROBE_MODES = "probe_modes"
+AXIS_POSITION_JITTER = "position_jitter"
+AXIS_COHERENCE = "coherence"
+_AXIS_DIM = {AXIS_PROBE_MODES: 1, AXIS_POSITION_JITTER: 2, AXIS_COHERENCE: 3}
+
+
+# ----------------------------------------------------------------------------- producers
+def _normal_gauss_hermite_rule(n_quad) -> Tuple[np.ndarray, np.ndarray]:
+    """Nodes and weights of the probabilists' Gauss-Hermite rule for a standard
+    normal (multislice/producers.py:250-290)."""
+    q = int(n_quad)
+    if q <= 0:
+        raise ValueError("n_quad must be positive")
+    x, w = np.polynomial.hermite.hermgauss(q)
+    return np.sqrt(2.0) * x, w / np.sqrt(np.pi)
+
+
+def _collapse_width(width, nodes: np.ndarray, name: str) -> np.ndarray:
+    arr = np.asarray(width, dtype=np.float64)
+    if arr.shape != ():
+        raise ValueError(f"{name} must be a scalar")
+    v = float(arr)
+    if not math.isfinite(v):
+        raise ValueError(f"{name} must be finite")
+    if v < 0.0:
+        raise ValueError(f"{name} must be non-negative")
+    return v * nodes if v > 0.0 else np.zeros_like(nodes)
+
+
+def coherence_to_distribution(energy_spread_ev, angular_divergence_mrad, n_quad) -> Distribution:
+    """Gauss-Hermite grid over (dE, tilt x, tilt y) (producers.py:46-128)."""
+    nodes, weights = _normal_gauss_hermite_rule(n_quad)
+    e = _collapse_width(energy_spread_ev, nodes, "energy_spread_ev")
+    t = _collapse_width(angular_divergence_mrad, nodes, "angular_divergence_mrad")
+    eg, txg, tyg = np.meshgrid(e, t, t, indexing="ij")
+    we, wx, wy = np.meshgrid(weights, weights, weights, indexing="ij")
+    samples = np.stack((eg.reshape(-1), txg.reshape(-1), tyg.reshape(-1)), axis=1)
+    return create_distribution(samples, (we * wx * wy).reshape(-1), ReductionMode.INCOHERENT, AXIS_COHERENCE)
+
+
+def position_jitter_to_distribution(sigma_ang, n_quad) -> Distribution:
+    """Gauss-Hermite grid over (dy, dx) in Angstrom (producers.py:131-198)."""
+    nodes, weights = _normal_gauss_hermite_rule(n_quad)
+    d = _collapse_width(sigma_ang, nodes, "sigma_ang")
+    dy, dx = np.meshgrid(d, d, indexing="ij")
+    wy, wx = np.meshgrid(weights, weights, indexing="ij")
+    samples = np.stack((dy.reshape(-1), dx.reshape(-1)), axis=1)
+    return create_distribution(samples, (wy * wx).reshape(-1), ReductionMode.INCOHERENT, AXIS_POSITION_JITTER)
+
+
+def probe_modes_to_distribution(probe: ProbeModes) -> Distribution:
+    """The incoherent mode axis with the beam's weights (simulations.py:682-711)."""
+    m = probe.modes.shape[2] if probe.modes.ndim == 3 else 1
+    samples = np.arange(m, dtype=np.float64)[:, None]
+    return create_distribution(samples, as_tensor(probe.weights, torch.float64).cpu(), ReductionMode.INCOHERENT,
+                               AXIS_PROBE_MODES)
+
+
+# ----------------------------------------------------------------------------- axes
+def has_extra_ensemble_axes(ensemble: EnsembleAxes) -> bool:
+    """simulations.py:714-732."""
+    return ensemble.probe_modes is not None or ensemble.position_jitter is not None or ensemble.coherence is not None
+
+
+def ensemble_axes_for_cbed(ensemble: EnsembleAxes, beam: ProbeModes) -> Tuple[Distribution, ...]:
+    """The axes cbed_image reduces over, in order (simulations.py:735-766)."""
+    axes: List[Distribution] = []
+    mode_count = beam.modes.shape[2] if beam.modes.ndim == 3 else 1
+    if ensemble.probe_modes is not None:
+        axes.append(ensemble.probe_modes)
+    elif mode_count > 1:
+        axes.append(probe_modes_to_distribution(beam))
+    if ensemble.position_jitter is not None:
+        axes.append(ensemble.position_jitter)
+    if ensemble.coherence is not None:
+        axes.append(ensemble.coherence)
+    if not axes:
+        axes.append(probe_modes_to_distribution(beam))
+    return tuple(axes)
+
+
+def _axis_maps(axes, mode_count: int) -> Tuple[str, ...]:
+    """simulations.py:1032-1127: axis ids, sample widths, probe-mode axis first."""
+    maps = []
+    for i, axis in enumerate(axes):
+        if axis.axis_id is None:
+            raise ValueError("distribution axis_id is required")
+        if axis.axis_id not in _AXIS_DIM:
+            raise ValueError(f"unknown axis_id {axis.axis_id!r}")
+        if axis.samples.shape[1] != _AXIS_DIM[axis.axis_id]:
+            raise ValueError(f"{axis.axis_id!r} axis must have sample width {_AXIS_DIM[axis.axis_id]}")
+        if axis.axis_id == AXIS_PROBE_MODES and i != 0:
+            raise ValueError("probe_modes axis must be first")
+        maps.append(axis.axis_id)
+    if AXIS_PROBE_MODES not in maps and mode_count != 1:
+        raise ValueError("multimode probes require a first probe_modes axis")
+    return tuple(maps)
+
+
+class VirtualModes:
+    """Virtual modes of one energy: (n, n, K) complex64 input waves, (K,) weights,
+    (K, 2, n) tilt factors (or None when no sample is tilted), and the voltage."""
+
+    def __init__(self, modes: torch.Tensor, weights: torch.Tensor, tilts: Optional[torch.Tensor], voltage_kv: float):
+        self.modes, self.weights, self.tilts, self.voltage_kv = modes, weights, tilts, voltage_kv
+
+
+def _jitter_shift(spectra: torch.Tensor, delta, calib: float) -> torch.Tensor:
+    """ifft2(fft2(mode) exp(-2 pi i (qy dy + qx dx))) of (M, n, n) spectra
+    (shift_beam_fourier, simulations.py:1236-1327)."""
+    n = spectra.shape[-1]
+    q = np.fft.fftfreq(n, d=calib)
+    ry = np.exp(-2j * np.pi * q * float(delta[0]))
+    rx = np.exp(-2j * np.pi * q * float(delta[1]))
+    ramp = torch.as_tensor(np.outer(ry, rx).astype(np.complex64), device=spectra.device)
+    return fft2(spectra * ramp, inverse=True)
+
+
+def _tilt_factors(tilt_mrad, voltage_kv: float, calib: float, n: int) -> np.ndarray:
+    """(2, n) factors along y and x of _apply_tilt_phase_ramp (simulations.py:891-946)."""
+    lam = relativistic_wavelength_ang(voltage_kv)
+    c = (np.arange(n, dtype=np.float64) - (n - 1) / 2.0) * calib
+    k = 2.0 * np.pi / lam
+    ty = np.exp(1j * k * (float(tilt_mrad[1]) / 1000.0) * c)
+    tx = np.exp(1j * k * (float(tilt_mrad[0]) / 1000.0) * c)
+    return np.stack([ty, tx])
+
+
+def virtual_modes(ensemble: EnsembleAxes, beam_modes: torch.Tensor, beam: ProbeModes, voltage_kv: float,
+                  calib: float) -> List[VirtualModes]:
+    """Expand the ensemble of ``beam`` into engine calls (one per energy)."""
+    axes = ensemble_axes_for_cbed(ensemble, beam)
+    n = beam_modes.shape[0]
+    mode_count = beam_modes.shape[2]
+    maps = _axis_maps(axes, mode_count)
+    coherent = [i for i, a in enumerate(axes) if a.reduction is ReductionMode.COHERENT]
+    incoherent = [i for i, a in enumerate(axes) if a.reduction is ReductionMode.INCOHERENT]
+    samples = [a.samples.numpy() for a in axes]
+    weights = [a.weights.numpy() for a in axes]
+    dev = beam_modes.device
+    spectra = fft2(beam_modes.permute(2, 0, 1).contiguous())  # (M, n, n)
+
+    def update(choice):
+        mode, delta, de, tilt = 0, np.zeros(2), 0.0, np.zeros(2)
+        for ax, k in choice.items():
+            row = samples[ax][k]
+            if maps[ax] == AXIS_PROBE_MODES:
+                mode = int(row[0])
+            elif maps[ax] == AXIS_POSITION_JITTER:
+                delta = delta + row
+            else:
+                de, tilt = de + float(row[0]), tilt + row[1:3]
+        if not 0 <= mode < mode_count:
+            raise ValueError(f"probe mode index {mode} out of range")
+        return mode, delta, de, tilt
+
+    groups = {}  # energy -> list of (wave, weight, tilt)
+    for inc in itertools.product(*[range(samples[i].shape[0]) for i in incoherent]):
+        w_inc = float(np.prod([weights[i][k] for i, k in zip(incoherent, inc)])) if incoherent else 1.0
+        wave = None
+        shared = None
+        for coh in itertools.product(*[range(samples[i].shape[0]) for i in coherent]):
+            choice = dict(zip(incoherent, inc))
+            choice.update(zip(coherent, coh))
+            mode, delta, de, tilt = update(choice)
+            if shared is None:
+                shared = (de, tuple(tilt))
+            elif shared != (de, tuple(tilt)):
+                raise NotImplementedError("coherent sums over energy or tilt samples are not supported")
+            w_coh = float(np.prod([weights[i][k] for i, k in zip(coherent, coh)])) if coherent else 1.0
+            if np.any(delta != 0.0):
+                part = _jitter_shift(spectra[mode], delta, calib)
+            else:
+                part = beam_modes[:, :, mode]
+            wave = part * w_coh if wave is None else wave + part * w_coh
+        de, tilt = shared
+        groups.setdefault(de, []).append((wave, w_inc, tilt))
+
+    out = []
+    for de, members in groups.items():
+        volt = voltage_kv + de / 1000.0
+        modes = torch.stack([m[0] for m in members], dim=2).to(torch.complex64)
+        wts = torch.tensor([m[1] for m in members], dtype=torch.float32, device=dev)
+        tilted = any(any(t != 0.0 for t in m[2]) for m in members)
+        tilts = None
+        if tilted:
+            tf = np.stack([_tilt_factors(m[2], volt, calib, n) for m in members]).astype(np.complex64)
+            tilts = torch.as_tensor(tf, device=dev).contiguous()
+        out.append(VirtualModes(modes, wts, tilts, volt))
+    return out
+
+
+def run_forward_ensemble(slices: torch.Tensor, slice_thickness: float, groups: List[VirtualModes],
+                         positions: torch.Tensor, calib_ang: float, shift_calib_ang: float) -> torch.Tensor:
+    """Patterns (P, n, n) float32: one engine call per energy group, accumulated."""
+    lib = _lib.load()
+    dev = slices.device
+    num_probes = positions.shape[0]
+    n = groups[0].modes.shape[0]
+    out = torch.zeros((num_probes, n, n), dtype=torch.float32, device=dev)
+    if num_probes == 0:
+        return out
+    for g in groups:
+        _, f = check_windows(slices, g.modes, None, num_probes)
+        prm = ms_params(n, slices.shape[2], g.modes.shape[2], num_probes, g.voltage_kv, slice_thickness, calib_ang,
+                        shift_calib_ang, slices.stride(), g.modes.stride(), 0, 0, f, None,
+                        _lib.PTYRO_FLAG_ACCUMULATE)
+        nbytes = lib.ptyro_ms_workspace_bytes(ctypes.byref(prm))
+        if nbytes == 0:
+            _lib.check(_lib.PTYRO_ERR_INVALID)
+        ws = _workspace(nbytes, dev)
+        if g.tilts is None:
+            rc = lib.ptyro_ms_forward(ctypes.byref(prm), slices.data_ptr(), g.modes.data_ptr(), g.weights.data_ptr(),
+                                      positions.data_ptr(), out.data_ptr(), ws.data_ptr(), nbytes, _stream_ptr(dev))
+        else:
+            rc = lib.ptyro_ms_forward_tilted(ctypes.byref(prm), slices.data_ptr(), g.modes.data_ptr(),
+                                             g.weights.data_ptr(), positions.data_ptr(), g.tilts.data_ptr(),
+                                             out.data_ptr(), ws.data_ptr(), nbytes, _stream_ptr(dev))
+        _lib.check(rc)
+    return out
+
+
+def ensemble_patterns(slices: torch.Tensor, slice_thickness: float, beam: ProbeModes, ensemble: EnsembleAxes,
+                      voltage_kv: float, calib_ang: float, positions: torch.Tensor,
+                      shift_calib_ang: float) -> torch.Tensor:
+    """Patterns with the ensemble reduced; ``calib_ang`` = min(potential, beam)
+    calibration (the jitter shift and tilt ramps use it), ``shift_calib_ang`` the
+    scan shift's."""
+    dev = _device(slices.device)
+    modes = beam.modes if beam.modes.ndim == 3 else beam.modes[..., None]
+    modes = as_tensor(modes, torch.complex64, dev).contiguous()
+    groups = virtual_modes(ensemble, modes, beam, voltage_kv, calib_ang)
+    return run_forward_ensemble(slices, slice_thickness, groups, positions, calib_ang, shift_calib_ang)

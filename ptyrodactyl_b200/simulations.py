@@ -221,8 +221,6 @@ def stem_4d(pot_slice: PotentialSlices, beam: ProbeModes, microscope: Microscope
     """
     if detector.scan_positions_px is None:
         raise ValueError("detector.scan_positions_px is required")
-    if not microscope.ensemble.is_empty():
-        raise NotImplementedError("ensemble axes are not supported by the B200 engine")
     dev = _device(pot_slice.slices.device if pot_slice.slices.is_cuda else None)
     slices = as_tensor(pot_slice.slices, torch.float32, dev)
     if slices.ndim == 2:
@@ -230,7 +228,14 @@ def stem_4d(pot_slice: PotentialSlices, beam: ProbeModes, microscope: Microscope
     modes, weights = _beam_on(beam, dev)
     positions = as_tensor(detector.scan_positions_px, torch.float64, dev).reshape(-1, 2).contiguous()
     calib = min(float(pot_slice.calib), float(beam.calib))
-    if _needs_autodiff(slices, modes):
+    if not microscope.ensemble.is_empty():
+        # per position, cbed_image's ensemble branch (simulations.py:1163-1193)
+        if _needs_autodiff(slices, modes):
+            raise NotImplementedError("derivatives through ensemble axes are not supported by the B200 engine")
+        from .ensemble import ensemble_patterns
+        data = ensemble_patterns(slices, pot_slice.slice_thickness, beam, microscope.ensemble,
+                                 microscope.voltage_kv, calib, positions, detector.real_space_calib_ang)
+    elif _needs_autodiff(slices, modes):
         # differentiable path: checkpointed forward + hand-written adjoint kernel
         from .autodiff import stem_4d_patterns
         data = stem_4d_patterns(slices, modes, weights, positions, pot_slice.slice_thickness,
@@ -345,10 +350,9 @@ def stem4d_sharded(probe_modes: ProbeModes, sample: AtomicSliceData, microscope:
 
 
 def cbed_image(pot_slices: PotentialSlices, beam: ProbeModes, microscope: MicroscopeConfig) -> CalibratedArray:
-    """Single-position CBED intensity (plain branch, simulations.py:1130-1233): the
-    unshifted beam through the slices, sum_m w_m |fftshift(fft2(exit wave))|^2."""
-    if not microscope.ensemble.is_empty():
-        raise NotImplementedError("ensemble axes are not supported by the B200 engine")
+    """Single-position CBED intensity (simulations.py:1130-1233): the unshifted beam
+    through the slices, sum_m w_m |fftshift(fft2(exit wave))|^2, or, when the
+    microscope carries ensemble axes, the ensemble branch (:1163-1193)."""
     dev = _device(pot_slices.slices.device if pot_slices.slices.is_cuda else None)
     slices = as_tensor(pot_slices.slices, torch.float32, dev)
     if slices.ndim == 2:
@@ -356,10 +360,37 @@ def cbed_image(pot_slices: PotentialSlices, beam: ProbeModes, microscope: Micros
     modes, weights = _beam_on(beam, dev)
     calib = min(float(pot_slices.calib), float(beam.calib))
     zero = torch.zeros((1, 2), dtype=torch.float64, device=dev)
-    data = run_forward(slices, pot_slices.slice_thickness, modes, weights, zero,
-                       microscope.voltage_kv, calib, calib)[0]
+    if not microscope.ensemble.is_empty():
+        from .ensemble import ensemble_patterns
+        data = ensemble_patterns(slices, pot_slices.slice_thickness, beam, microscope.ensemble,
+                                 microscope.voltage_kv, calib, zero, calib)[0]
+    else:
+        data = run_forward(slices, pot_slices.slice_thickness, modes, weights, zero,
+                           microscope.voltage_kv, calib, calib)[0]
     inv = 1.0 / (modes.shape[0] * calib)
     return create_calibrated_array(data, inv, inv, False)
+
+
+def cbed_amplitude(pot_slices: PotentialSlices, beam: ProbeModes, microscope: MicroscopeConfig) -> torch.Tensor:
+    """Complex detector-plane amplitudes (H, W, M) of every beam mode at the probe's
+    own place: fftshift(fft2(exit wave)) (simulations.py:606-679), complex64 CUDA."""
+    lib = _lib.load()
+    dev = _device(pot_slices.slices.device if pot_slices.slices.is_cuda else None)
+    slices = as_tensor(pot_slices.slices, torch.float32, dev)
+    if slices.ndim == 2:
+        slices = slices[..., None]
+    modes, _ = _beam_on(beam, dev)
+    calib = min(float(pot_slices.calib), float(beam.calib))
+    n, f = check_windows(slices, modes, None, 1)
+    zero = torch.zeros((1, 2), dtype=torch.float64, device=dev)
+    prm = ms_params(n, slices.shape[2], modes.shape[2], 1, microscope.voltage_kv, pot_slices.slice_thickness, calib,
+                    calib, slices.stride(), modes.stride(), 0, 0, f)
+    amps = torch.empty((1, modes.shape[2], n, n), dtype=torch.complex64, device=dev)
+    nbytes = lib.ptyro_ms_workspace_bytes(ctypes.byref(prm))
+    ws = _workspace(nbytes, dev)
+    _lib.check(lib.ptyro_ms_amplitudes(ctypes.byref(prm), slices.data_ptr(), modes.data_ptr(), zero.data_ptr(),
+                                       None, amps.data_ptr(), ws.data_ptr(), nbytes, _stream_ptr(dev)))
+    return amps[0].permute(1, 2, 0)
 
 
 def make_probe(microscope: MicroscopeConfig, detector: DetectorConfig) -> torch.Tensor:

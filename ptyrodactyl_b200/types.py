@@ -16,6 +16,7 @@ from __future__ import annotations
 
 import math
 from dataclasses import dataclass, field
+from enum import Enum
 from typing import Optional, Tuple
 
 import numpy as np
@@ -78,14 +79,62 @@ def _shape_tuple(shape, name: str) -> Optional[Tuple[int, int]]:
     return (int(vals[0]), int(vals[1]))
 
 
+class ReductionMode(str, Enum):
+    """How an ensemble axis is reduced (types/distributions.py:38-52): COHERENT sums
+    weighted amplitudes before |.|^2, INCOHERENT sums weighted intensities."""
+
+    COHERENT = "coherent"
+    INCOHERENT = "incoherent"
+
+
+@dataclass(frozen=True)
+class Distribution:
+    """Weighted samples of one ensemble axis (types/distributions.py:55-102):
+    samples (N, D) float64, weights (N,) float64 summing to one."""
+
+    samples: Array
+    weights: Array
+    reduction: ReductionMode = ReductionMode.INCOHERENT
+    axis_id: Optional[str] = None
+
+
+def create_distribution(samples, weights, reduction=ReductionMode.INCOHERENT, axis_id=None) -> Distribution:
+    """types/distributions.py:105-188: validated, weights clipped at zero and
+    normalised to unit sum."""
+    smp = as_tensor(samples, torch.float64).cpu()
+    wts = as_tensor(weights, torch.float64).cpu()
+    if smp.ndim != 2:
+        raise ValueError("samples must have shape (N, D)")
+    if wts.ndim != 1:
+        raise ValueError("weights must have shape (N,)")
+    if smp.shape[0] <= 0:
+        raise ValueError("samples must contain at least one row")
+    if smp.shape[0] != wts.shape[0]:
+        raise ValueError("samples and weights must share leading dimension")
+    mode = ReductionMode(reduction)
+    if not bool(torch.isfinite(smp).all()):
+        raise ValueError("samples must be finite")
+    if not bool(torch.isfinite(wts).all()):
+        raise ValueError("weights must be finite")
+    if bool((wts < 0).any()):
+        raise ValueError("weights must be non-negative")
+    if float(wts.sum()) <= 0.0:
+        raise ValueError("weights must have positive total probability")
+    clipped = wts.clamp(min=0.0)
+    total = float(clipped.sum())
+    norm = clipped / total if total > 0 else torch.full_like(clipped, 1.0 / clipped.shape[0])
+    return Distribution(smp, norm, mode, axis_id)
+
+
 @dataclass(frozen=True)
 class EnsembleAxes:
-    """Optional ensemble distributions (electron_types.py:74-100). Only the empty
-    carrier is supported by this engine."""
+    """Optional ensemble distributions (electron_types.py:74-100): a probe-mode axis
+    (sample width 1: the mode index), position jitter (width 2: dy, dx in Angstrom)
+    and partial coherence (width 3: dE in eV, tilt x and y in mrad)."""
 
-    probe_modes: object = None
-    position_jitter: object = None
-    coherence: object = None
+    probe_modes: Optional[Distribution] = None
+    position_jitter: Optional[Distribution] = None
+    coherence: Optional[Distribution] = None
 
     def is_empty(self) -> bool:
         return self.probe_modes is None and self.position_jitter is None and self.coherence is None
@@ -166,6 +215,28 @@ class STEM4D:
     fourier_space_calib: float
     scan_positions: Array
     voltage_kv: float
+
+
+def _validate_distribution_axis(axis: Optional[Distribution], expected_axis_id: str, expected_dim: int) -> None:
+    if axis is None:
+        return
+    if axis.samples.ndim != 2:
+        raise ValueError(f"{expected_axis_id}.samples must be 2D")
+    if axis.samples.shape[1] != expected_dim:
+        raise ValueError(f"{expected_axis_id}.samples must have width {expected_dim}")
+    if axis.weights.ndim != 1 or tuple(axis.weights.shape) != (axis.samples.shape[0],):
+        raise ValueError(f"{expected_axis_id}.weights must have shape (N,)")
+    if axis.axis_id not in (None, expected_axis_id):
+        raise ValueError(f"{expected_axis_id}.axis_id must be {expected_axis_id!r}")
+
+
+def create_ensemble_axes(probe_modes: Optional[Distribution] = None, position_jitter: Optional[Distribution] = None,
+                         coherence: Optional[Distribution] = None) -> EnsembleAxes:
+    """electron_types.py:488-526."""
+    _validate_distribution_axis(probe_modes, "probe_modes", 1)
+    _validate_distribution_axis(position_jitter, "position_jitter", 2)
+    _validate_distribution_axis(coherence, "coherence", 3)
+    return EnsembleAxes(probe_modes, position_jitter, coherence)
 
 
 def create_microscope_config(voltage_kv, aperture_mrad, defocus_ang=0.0, c3_ang=0.0, c5_ang=0.0,

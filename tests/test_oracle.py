@@ -170,3 +170,58 @@ def test_oracle_jvp_is_the_transpose_of_the_vjp():
     lhs = np.sum(dd * g)
     rhs = np.sum(gv * dv) + np.real(np.sum(gb * db))
     assert abs(lhs - rhs) <= 1e-10 * abs(lhs)
+
+
+def test_oracle_ensemble_reduces_to_plain_and_explicit_composition():
+    """Zero-width ensembles give the plain CBED; a jitter axis equals the weighted
+    sum of CBEDs of explicitly shifted beams (test_simulations.py:243-285)."""
+    rng = np.random.default_rng(0)
+    n = 16
+    pot = rng.uniform(0, 20, (n, n, 2))
+    probe = R.make_probe(200.0, 25.0, (n, n), 20.0)
+    modes = np.stack([probe, np.roll(probe, 1, 0)], -1)
+    w = np.array([0.7, 0.3])
+    axes = [(np.arange(2.0)[:, None], w, "incoherent", "probe_modes"), R.jitter_axis(0.0, 2),
+            R.coherence_axis(0.0, 0.0, 2)]
+    plain = R.cbed_image(pot, 1.5, 0.2, modes, w, 0.2, 200.0)
+    assert np.max(np.abs(R.ensemble_cbed(pot, 1.5, 0.2, modes, 0.2, 200.0, axes) - plain)) < 1e-13
+    jit = R.jitter_axis(0.15, 2)
+    e = R.ensemble_cbed(pot, 1.5, 0.2, probe[..., None], 0.2, 200.0, [jit])
+    explicit = sum(wk * R.cbed_image(pot, 1.5, 0.2, R.shift_beam_fourier(probe[..., None], d[None], 0.2)[0], [1.0],
+                                     0.2, 200.0) for d, wk in zip(jit[0], jit[1]))
+    assert np.max(np.abs(e - explicit)) < 1e-13
+    # Gauss-Hermite(2) nodes are +-sigma with weight 1/4 per (dy, dx) pair
+    assert np.allclose(np.abs(jit[0]), 0.15) and np.allclose(jit[1], 0.25)
+
+
+def test_product_producers_match_oracle():
+    from ptyrodactyl_b200 import ensemble as E
+    for q in (1, 2, 3):
+        d = E.position_jitter_to_distribution(0.2, q)
+        s, w, _, _ = R.jitter_axis(0.2, q)
+        assert np.allclose(d.samples.numpy(), s) and np.allclose(d.weights.numpy(), w)
+        c = E.coherence_to_distribution(0.7, 0.05, q)
+        s, w, _, _ = R.coherence_axis(0.7, 0.05, q)
+        assert np.allclose(c.samples.numpy(), s) and np.allclose(c.weights.numpy(), w)
+    with pytest.raises(ValueError, match="n_quad must be positive"):
+        E.position_jitter_to_distribution(0.2, 0)
+    with pytest.raises(ValueError, match="sigma_ang must be non-negative"):
+        E.position_jitter_to_distribution(-0.2, 2)
+
+
+def test_ensemble_axis_validation():
+    import ptyrodactyl_b200 as pb
+    jit = pb.position_jitter_to_distribution(0.1, 2)
+    with pytest.raises(ValueError, match="coherence.samples must have width 3"):
+        pb.create_ensemble_axes(coherence=jit)
+    with pytest.raises(ValueError, match="samples and weights must share leading dimension"):
+        pb.create_distribution(np.zeros((3, 1)), np.ones(2))
+    with pytest.raises(ValueError, match="weights must be non-negative"):
+        pb.create_distribution(np.zeros((2, 1)), [1.0, -1.0])
+    ax = pb.create_ensemble_axes(position_jitter=jit)
+    beam = pb.create_probe_modes(np.ones((16, 16, 2), np.complex64), [0.5, 0.5], 0.2)
+    from ptyrodactyl_b200.ensemble import _axis_maps, ensemble_axes_for_cbed
+    axes = ensemble_axes_for_cbed(ax, beam)
+    assert [a.axis_id for a in axes] == ["probe_modes", "position_jitter"]
+    with pytest.raises(ValueError, match="multimode probes require a first probe_modes axis"):
+        _axis_maps((jit,), 2)
