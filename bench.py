@@ -35,6 +35,7 @@ if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
 from ptyrodactyl_b200 import synth  # noqa: E402
+from ptyrodactyl_b200.simulations import default_tune  # noqa: E402
 
 METRIC = "probe-slice updates/s at 256^2 (batched fused multislice forward, 4096 probes x 50 slices)"
 UNIT = "probe-slice updates/s"
@@ -187,6 +188,7 @@ def run_ours(args, rank, world, local_rank):
     lib = _lib.load()
     w = WORKLOAD
     n, S, P = w.n, w.num_slices, w.num_probes
+    tune = default_tune(n) if args.tune < 0 else args.tune
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -205,7 +207,7 @@ def run_ours(args, rank, world, local_rank):
     pos_d = torch.as_tensor(pos, dtype=torch.float64, device=dev)
     out_d = torch.empty((P, n, n), dtype=torch.float32, device=dev)
     prm = ms_params(n, S, 1, P, w.voltage_kv, synth.SLICE_DZ, w.calib, w.calib, slices_d.stride(),
-                    modes_d.stride(), args.batch, args.tune)
+                    modes_d.stride(), args.batch, tune)
     ws_bytes = lib.ptyro_ms_workspace_bytes(ctypes.byref(prm))
     ws = torch.empty(ws_bytes, dtype=torch.uint8, device=dev)
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
@@ -222,7 +224,7 @@ def run_ours(args, rank, world, local_rank):
         # the same forward captured once as a CUDA graph; a step is one replay
         from ptyrodactyl_b200.graphs import GraphedForward
         graphed = GraphedForward(slices_d, modes_d, weights_d, pos_d, synth.SLICE_DZ, w.voltage_kv, w.calib,
-                                 batch=args.batch, tune=args.tune, lanes=args.lanes)
+                                 batch=args.batch, tune=tune, lanes=args.lanes)
         out_d = graphed.out
         ws, ws_bytes, prm = graphed.ws, graphed.ws_bytes, graphed.prm  # the steady-pass timing reuses them
 
@@ -365,13 +367,13 @@ def run_ours(args, rank, world, local_rank):
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": w.name, "grid": n, "slices": S, "probes_per_gpu": P, "modes": 1,
-                       "batch": batch, "tune": args.tune, "cuda_graph": bool(args.graph), "lanes": args.lanes if args.graph else 1, "voltage_kv": w.voltage_kv, "aperture_mrad": w.aperture_mrad,
+                       "batch": batch, "tune": tune, "cuda_graph": bool(args.graph), "lanes": args.lanes if args.graph else 1, "voltage_kv": w.voltage_kv, "aperture_mrad": w.aperture_mrad,
                        "defocus_ang": w.defocus_ang, "c3_ang": w.c3_ang,
                        "l2": "flushed (256 MB write) before every timed step",
                        "parallelism": f"dp{world} (probe shards, no collective)"},
             "roofline": {"bound": "fp32", "achieved": achieved_tflops, "peak": peak, "unit": "TFLOP/s",
                          "frac": achieved_tflops / peak, "traffic": traffic,
-                         "kernel": "ms_pass_kernel<16,16> steady-state pass (conv, x T, conv)",
+                         "kernel": ("ms_pass_pair_kernel<16,16> steady-state pass (two lines per thread, f32x2; conv, x T, conv)" if tune & 16 else "ms_pass_kernel<16,16> steady-state pass (conv, x T, conv)"),
                          "flops_per_launch": flops_per_launch, "launch_ms": [round(x, 4) for x in pass_ms],
                          "peak_source": "measured FP32 FMA stream (ptyro_fp32_fma_probe) in this run",
                          "hbm_achieved_gbs": bytes_per_launch / avg_pass_s / 1e9,
@@ -446,7 +448,7 @@ def run_grad(args, rank, world, local_rank):
                               dtype=torch.float32, device=dev)
     k = args.ckpt if args.ckpt > 0 else int(np.ceil(np.sqrt(S)))
     prm = ms_params(n, S, 1, P, w.voltage_kv, synth.SLICE_DZ, w.calib, w.calib, model.stride(), probe.stride(),
-                    0, args.tune, F, win)
+                    0, default_tune(n) if args.tune < 0 else args.tune, F, win)
     bprm = ms_params(n, S, 1, P, w.voltage_kv, synth.SLICE_DZ, w.calib, w.calib, model.stride(), probe.stride(),
                      args.bwd_batch, 0, F, win)
     ws_b = lib.ptyro_ms_workspace_bytes(ctypes.byref(prm))
@@ -678,7 +680,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--batch", type=int, default=0)
-    ap.add_argument("--tune", type=int, default=3, help="pass-kernel occupancy variant bits")
+    ap.add_argument("--tune", type=int, default=-1,
+                    help="pass-kernel variant bits; -1: the measured default for the grid edge")
     ap.add_argument("--graph", type=int, default=1, help="1: time CUDA-graph replays of the captured forward")
     ap.add_argument("--lanes", type=int, default=2, help="concurrent probe ranges (streams) in the captured forward")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)

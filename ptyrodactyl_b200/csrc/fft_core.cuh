@@ -27,6 +27,40 @@ __device__ __forceinline__ float2 cmulc(float2 a, float2 b) {
 __device__ __forceinline__ float2 cscale(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
 __device__ __forceinline__ float2 cconj(float2 a) { return make_float2(a.x, -a.y); }
 
+// Two complex values of two different lines that go through identical arithmetic,
+// kept as (real parts, imaginary parts) so that every operation is one paired FP32
+// instruction (add / mul / fma .f32x2 on sm_100): the pair costs one issue slot
+// where two scalar instructions would cost two. Each paired operation rounds
+// exactly like the scalar float2 operation it replaces.
+struct alignas(16) Pair {
+  float2 re;  // (line A, line B)
+  float2 im;
+};
+__device__ __forceinline__ float2 dup2(float v) { return make_float2(v, v); }
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __ffma2_rn(b, dup2(-1.f), a); }
+__device__ __forceinline__ Pair cadd(Pair a, Pair b) { return {__fadd2_rn(a.re, b.re), __fadd2_rn(a.im, b.im)}; }
+__device__ __forceinline__ Pair csub(Pair a, Pair b) { return {sub2(a.re, b.re), sub2(a.im, b.im)}; }
+// a * w with the same w for both lines: (a.x w.x - a.y w.y, a.x w.y + a.y w.x)
+__device__ __forceinline__ Pair cmul(Pair a, float2 w) {
+  return {__ffma2_rn(a.re, dup2(w.x), __fmul2_rn(a.im, dup2(-w.y))),
+          __ffma2_rn(a.re, dup2(w.y), __fmul2_rn(a.im, dup2(w.x)))};
+}
+// a * conj(w)
+__device__ __forceinline__ Pair cmulc(Pair a, float2 w) {
+  return {__ffma2_rn(a.re, dup2(w.x), __fmul2_rn(a.im, dup2(w.y))),
+          __ffma2_rn(a.im, dup2(w.x), __fmul2_rn(a.re, dup2(-w.y)))};
+}
+// a * w with a different w per line: (wA, wB)
+__device__ __forceinline__ Pair cmul(Pair a, float2 wa, float2 wb) {
+  const float2 wx = make_float2(wa.x, wb.x), wy = make_float2(wa.y, wb.y);
+  return {__ffma2_rn(a.re, wx, __fmul2_rn(a.im, make_float2(-wa.y, -wb.y))),
+          __ffma2_rn(a.re, wy, __fmul2_rn(a.im, wx))};
+}
+__device__ __forceinline__ Pair cscale(Pair a, float s) { return {__fmul2_rn(a.re, dup2(s)), __fmul2_rn(a.im, dup2(s))}; }
+__device__ __forceinline__ Pair make_pair(float2 a, float2 b) { return {make_float2(a.x, b.x), make_float2(a.y, b.y)}; }
+__device__ __forceinline__ float2 pair_a(Pair p) { return make_float2(p.re.x, p.im.x); }
+__device__ __forceinline__ float2 pair_b(Pair p) { return make_float2(p.re.y, p.im.y); }
+
 // cos(2 pi i / 64) for i = 0..16, rounded from the decimal expansion.
 __device__ __forceinline__ float cos64_q(int i) {
   switch (i) {
@@ -78,20 +112,46 @@ __host__ __device__ constexpr int bitrev(int i, int bits) {
   return bits == 0 ? 0 : (((i & 1) << (bits - 1)) | bitrev(i >> 1, bits - 1));
 }
 
+// u +- b W_64^k for paired values; the exact twiddles become additions of the
+// swapped parts, as the scalar path's twmul64 + cadd/csub round them.
+template <int DIR>
+__device__ __forceinline__ void bfly(Pair& u, Pair& b, int k) {
+  k &= 63;
+  Pair o1, o2;
+  if (k == 0) {
+    o1 = cadd(u, b); o2 = csub(u, b);
+  } else if (k == 32) {
+    o1 = csub(u, b); o2 = cadd(u, b);
+  } else if ((k == 16 && DIR < 0) || (k == 48 && DIR > 0)) {  // w = (b.y, -b.x)
+    o1 = {__fadd2_rn(u.re, b.im), sub2(u.im, b.re)};
+    o2 = {sub2(u.re, b.im), __fadd2_rn(u.im, b.re)};
+  } else if (k == 16 || k == 48) {  // w = (-b.y, b.x)
+    o1 = {sub2(u.re, b.im), __fadd2_rn(u.im, b.re)};
+    o2 = {__fadd2_rn(u.re, b.im), sub2(u.im, b.re)};
+  } else {
+    const Pair w = cmul(b, w64<DIR>(k));
+    o1 = cadd(u, w); o2 = csub(u, w);
+  }
+  u = o1;
+  b = o2;
+}
+template <int DIR>
+__device__ __forceinline__ void bfly(float2& u, float2& b, int k) {
+  const float2 w = twmul64<DIR>(b, k);
+  const float2 o1 = cadd(u, w), o2 = csub(u, w);
+  u = o1;
+  b = o2;
+}
+
 // One radix-2 stage (butterfly span HALF) of an R-point decimation-in-time DFT.
-template <int R, int DIR, int HALF>
-__device__ __forceinline__ void dit_stage(float2 (&t)[R]) {
+template <int R, int DIR, int HALF, typename T>
+__device__ __forceinline__ void dit_stage(T (&t)[R]) {
   constexpr int LEN = 2 * HALF;
   constexpr int TW = 64 / LEN;
 #pragma unroll
   for (int i = 0; i < R; i += LEN) {
 #pragma unroll
-    for (int j = 0; j < HALF; ++j) {
-      const float2 u = t[i + j];
-      const float2 w = twmul64<DIR>(t[i + j + HALF], j * TW);
-      t[i + j] = cadd(u, w);
-      t[i + j + HALF] = csub(u, w);
-    }
+    for (int j = 0; j < HALF; ++j) bfly<DIR>(t[i + j], t[i + j + HALF], j * TW);
   }
   if constexpr (LEN < R) dit_stage<R, DIR, LEN>(t);
 }
@@ -107,15 +167,15 @@ struct BitRev {
 // In-register DFT of size R (power of two, R <= 64) over a[O + S*i], i in [0,R),
 // natural order in and out, unnormalised. Radix-2 decimation in time with every
 // index and twiddle resolved at compile time.
-template <int R, int DIR, int S, int O, int L>
-__device__ __forceinline__ void dft(float2 (&a)[L]) {
+template <int R, int DIR, int S, int O, int L, typename T>
+__device__ __forceinline__ void dft(T (&a)[L]) {
   static_assert(R >= 1 && R <= 64 && (R & (R - 1)) == 0, "radix must be a power of two <= 64");
   static_assert(O + S * (R - 1) < L, "dft range exceeds register array");
   if constexpr (R == 1) {
     return;
   } else {
     constexpr BitRev<R> br;
-    float2 t[R];
+    T t[R];
 #pragma unroll
     for (int i = 0; i < R; ++i) t[i] = a[O + S * br.v[i]];
     dit_stage<R, DIR, 1>(t);
@@ -125,8 +185,8 @@ __device__ __forceinline__ void dft(float2 (&a)[L]) {
 }
 
 // The N1-point DFTs over each contiguous group g*N1 .. g*N1+N1-1.
-template <int N1, int N2, int DIR, int G = 0>
-__device__ __forceinline__ void dft_groups(float2 (&v)[N2]) {
+template <int N1, int N2, int DIR, int G = 0, typename T>
+__device__ __forceinline__ void dft_groups(T (&v)[N2]) {
   if constexpr (G < N2 / N1) {
     dft<N1, DIR, 1, G * N1, N2>(v);
     dft_groups<N1, N2, DIR, G + 1>(v);
@@ -147,8 +207,8 @@ struct LineBuf {
 // natural -> k-order transform of one line, unnormalised. DIR = -1 forward.
 // tw[k2 * N1 + t] = exp(-2 pi i t k2 / N) (shared memory; lanes of one k2 read
 // consecutive entries, so the table is read without bank conflicts).
-template <int N1, int N2, int DIR>
-__device__ __forceinline__ void line_nat_to_k(float2 (&v)[N2], int t, float2* buf, const float2* tw) {
+template <int N1, int N2, int DIR, typename T>
+__device__ __forceinline__ void line_nat_to_k(T (&v)[N2], int t, T* buf, const float2* tw) {
   using LB = LineBuf<N1, N2>;
   dft<N2, DIR, 1, 0, N2>(v);
   if (t != 0) {
@@ -170,8 +230,8 @@ __device__ __forceinline__ void line_nat_to_k(float2 (&v)[N2], int t, float2* bu
 }
 
 // k-order -> natural transform of one line, unnormalised. DIR = +1 inverse.
-template <int N1, int N2, int DIR>
-__device__ __forceinline__ void line_k_to_nat(float2 (&v)[N2], int t, float2* buf, const float2* tw) {
+template <int N1, int N2, int DIR, typename T>
+__device__ __forceinline__ void line_k_to_nat(T (&v)[N2], int t, T* buf, const float2* tw) {
   using LB = LineBuf<N1, N2>;
   dft_groups<N1, N2, DIR>(v);
   __syncwarp();

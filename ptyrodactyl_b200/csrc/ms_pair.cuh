@@ -1,0 +1,164 @@
+// Steady-state pass with two lines per thread in paired FP32 arithmetic.
+//
+// The middle slices' program (wave -> conv, x T, conv -> wave) is identical for
+// every line, so each thread carries the same element positions of two neighbouring
+// lines (A, B) as Pair values: real parts (A, B) and imaginary parts (A, B) in
+// register pairs. Every add, multiply and fma of the line transforms is then one
+// add/mul/fma.f32x2 instruction for both lines (sm_100), halving the issue slots of
+// the FP32 work, and twiddles and propagator factors are read once for two lines.
+// Results are bit-identical to the one-line kernel (each paired operation rounds
+// as the scalar one it replaces).
+//
+// Per CTA: WARPS warps, 32 / N1 line pairs per warp. Row passes read and write the
+// lines directly; column passes stage the CTA's block of 2 * pairs columns through a
+// shared tile (row pitch lines + 4 float2, so 16-byte column-pair reads of eight
+// lanes fall in distinct banks).
+#pragma once
+#include "ms_pass.cuh"
+
+namespace ptyro {
+
+// Exchange buffer of one line pair (Pair elements): same (k2, n1) index layout as
+// LineBuf, padded to 4 mod 8 Pairs so the two line pairs of a warp start 64 bytes
+// apart modulo the 128-byte bank window.
+template <int N1, int N2>
+struct PairBuf {
+  static constexpr int kRaw = N2 * (N1 + 1);
+  static constexpr int kSize = ((kRaw + 7) / 8) * 8 + 4;
+};
+
+template <int N1, int N2, int WARPS, bool PRE = false>
+struct PairGeom {
+  static constexpr int N = N1 * N2;
+  static constexpr int G = 32 / N1;          // line pairs per warp
+  static constexpr int kPairs = WARPS * G;   // line pairs per CTA
+  static constexpr int kLines = 2 * kPairs;  // lines per CTA
+  static constexpr int kPitch = kLines + 4;  // column tile row pitch (float2)
+  static_assert(N % kLines == 0, "lines per CTA must divide N");
+  static constexpr size_t kXbuf = sizeof(Pair) * (size_t)kPairs * PairBuf<N1, N2>::kSize;
+  static constexpr size_t kTile = sizeof(float2) * (size_t)N * kPitch;
+  static constexpr size_t kWork = kXbuf > kTile ? kXbuf : kTile;
+  // twiddles + propagator factor + max(exchange buffers, column tile)
+  // [+ the transmission rows of the CTA's lines, prefetched]
+  static size_t smem_bytes() {
+    return sizeof(float2) * 2 * (size_t)N + kWork + (PRE ? sizeof(float2) * (size_t)kLines * N : 0);
+  }
+};
+
+// PRE: the transmission rows of the thread's two lines are copied into shared
+// memory with cp.async at the start (each thread copies exactly the elements it
+// multiplies, so waiting for its own copies suffices); windows need PRE = false.
+// DIRECT (column passes): each lane pair reads and writes its two neighbouring
+// columns straight from global memory as 16-byte pieces (32 contiguous bytes per row
+// and lane pair), with no staging tile and no barriers.
+template <int N1, int N2, int AXIS, int WARPS, int MINB, bool PRE, bool DIRECT = false>
+__global__ void __launch_bounds__(WARPS * 32, MINB) ms_pass_pair_kernel(PassArgs a) {
+  using PG = PairGeom<N1, N2, WARPS, PRE>;
+  using PB = PairBuf<N1, N2>;
+  constexpr int N = PG::N, G = PG::G, lines = PG::kLines, pitch = PG::kPitch;
+  extern __shared__ float4 smem4[];
+  float2* tw = reinterpret_cast<float2*>(smem4);  // tw[k2 * N1 + t] = W_N^{t k2}
+  float2* pfs = tw + N;                           // propagator factor along this axis
+  float2* work = pfs + N;                         // column tile; aliases the exchange buffers
+  Pair* xbuf = reinterpret_cast<Pair*>(work);
+  for (int i = threadIdx.x; i < N; i += blockDim.x) {
+    const int k2 = i / N1, tt = i % N1;
+    tw[i] = a.tw[(tt * k2) % N];
+    pfs[i] = a.pf[i];
+  }
+  __syncthreads();
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int t = AXIS == 0 ? (lane % N1) : (lane / G);
+  const int gl = AXIS == 0 ? (lane / N1) : (lane % G);
+  const int lp = warp * G + gl;  // line pair within the CTA
+  const int line0 = blockIdx.x * lines;
+  const int la = line0 + 2 * lp, lb = la + 1;
+  const int slot = blockIdx.y;
+  Pair* buf = xbuf + lp * PB::kSize;
+  float2* w = a.wave + (size_t)slot * N * N;
+  float2* tpre = reinterpret_cast<float2*>(reinterpret_cast<char*>(work) + PG::kWork) + (size_t)(2 * lp) * N;
+  if (PRE) {
+    const float2* T = (AXIS == 0 ? a.trans : a.trans_t) + (size_t)a.t_slice * N * N;
+#pragma unroll
+    for (int j = 0; j < N2; ++j) {
+      cp_async8(tpre + t + N1 * j, T + (size_t)la * N + t + N1 * j);
+      cp_async8(tpre + N + t + N1 * j, T + (size_t)lb * N + t + N1 * j);
+    }
+    cp_async_commit();
+  }
+  Pair v[N2];
+
+  // ---- load (natural distribution: element t + N1 j of lines A and B)
+  if (AXIS == 0) {
+#pragma unroll
+    for (int j = 0; j < N2; ++j)
+      v[j] = make_pair(w[(size_t)la * N + t + N1 * j], w[(size_t)lb * N + t + N1 * j]);
+  } else if (DIRECT) {
+#pragma unroll
+    for (int j = 0; j < N2; ++j) {
+      const float4 q = *reinterpret_cast<const float4*>(w + (size_t)(t + N1 * j) * N + la);
+      v[j] = {make_float2(q.x, q.z), make_float2(q.y, q.w)};
+    }
+  } else {
+    tile_load<N, lines, pitch, WARPS * 32>(w, work, line0);
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < N2; ++j) {
+      const float4 q = *reinterpret_cast<const float4*>(work + (t + N1 * j) * pitch + 2 * lp);
+      v[j] = {make_float2(q.x, q.z), make_float2(q.y, q.w)};
+    }
+    __syncthreads();  // the tile becomes the exchange buffers
+  }
+
+  // ---- finish slice s-1's convolution along this axis
+  line_nat_to_k<N1, N2, -1>(v, t, buf, tw);
+#pragma unroll
+  for (int r = 0; r < N2; ++r) v[r] = cmul(v[r], pfs[korder_index<N1, N2>(t, r)]);
+  line_k_to_nat<N1, N2, +1>(v, t, buf, tw);
+
+  // ---- transmission T_s (row-major table for rows, transposed for columns)
+  if (PRE) {
+    cp_async_wait<0>();
+#pragma unroll
+    for (int j = 0; j < N2; ++j) v[j] = cmul(v[j], tpre[t + N1 * j], tpre[N + t + N1 * j]);
+  } else {
+    int oa, ob;
+    const float2* Ta = trans_row<AXIS>(a.trans, a.trans_t, a.field_n, a.t_slice, a.win, slot / a.n_modes, la, &oa);
+    const float2* Tb = trans_row<AXIS>(a.trans, a.trans_t, a.field_n, a.t_slice, a.win, slot / a.n_modes, lb, &ob);
+    const int fm = a.field_n - 1;
+#pragma unroll
+    for (int j = 0; j < N2; ++j)
+      v[j] = cmul(v[j], __ldg(Ta + ((t + N1 * j + oa) & fm)), __ldg(Tb + ((t + N1 * j + ob) & fm)));
+  }
+
+  // ---- start slice s's convolution along this axis
+  line_nat_to_k<N1, N2, -1>(v, t, buf, tw);
+#pragma unroll
+  for (int r = 0; r < N2; ++r) v[r] = cmul(v[r], pfs[korder_index<N1, N2>(t, r)]);
+  line_k_to_nat<N1, N2, +1>(v, t, buf, tw);
+
+  // ---- store
+  if (AXIS == 0) {
+#pragma unroll
+    for (int j = 0; j < N2; ++j) {
+      w[(size_t)la * N + t + N1 * j] = pair_a(v[j]);
+      w[(size_t)lb * N + t + N1 * j] = pair_b(v[j]);
+    }
+  } else if (DIRECT) {
+#pragma unroll
+    for (int j = 0; j < N2; ++j)
+      *reinterpret_cast<float4*>(w + (size_t)(t + N1 * j) * N + la) =
+          make_float4(v[j].re.x, v[j].im.x, v[j].re.y, v[j].im.y);
+  } else {
+    __syncthreads();  // every warp is done with its exchange buffer
+#pragma unroll
+    for (int j = 0; j < N2; ++j)
+      *reinterpret_cast<float4*>(work + (t + N1 * j) * pitch + 2 * lp) =
+          make_float4(v[j].re.x, v[j].im.x, v[j].re.y, v[j].im.y);
+    __syncthreads();
+    tile_store<N, lines, pitch, WARPS * 32>(w, work, line0);
+  }
+}
+
+}  // namespace ptyro

@@ -5,6 +5,7 @@
 
 #include "ms_bwd.cuh"
 #include "ms_jvp.cuh"
+#include "ms_pair.cuh"
 #include "ms_pipe.cuh"
 
 namespace ptyro {
@@ -97,6 +98,44 @@ int launch_pipe_t(const PassArgs& a, int nslots, cudaStream_t st) {
   return (int)cudaGetLastError();
 }
 
+// Steady passes with two lines per thread in paired FP32 arithmetic (ms_pair.cuh).
+template <int N1, int N2, int AXIS, int W, int MINB, bool PRE, bool DIRECT = false>
+int launch_pair_w(const PassArgs& a, int grid_y, cudaStream_t st) {
+  using PG = PairGeom<N1, N2, W, PRE>;
+  const size_t smem = PG::smem_bytes();
+  static bool attr_done = false;
+  if (!attr_done) {
+    cudaFuncSetAttribute(ms_pass_pair_kernel<N1, N2, AXIS, W, MINB, PRE, DIRECT>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    attr_done = true;
+  }
+  dim3 grid(PG::N / PG::kLines, grid_y);
+  ms_pass_pair_kernel<N1, N2, AXIS, W, MINB, PRE, DIRECT><<<grid, W * 32, smem, st>>>(a);
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  return (int)cudaGetLastError();
+}
+
+// variant bit 5 (32): transmission rows prefetched into shared memory, 3 CTAs/SM
+// variant bit 6 (64): 8 warps per CTA, 2 CTAs/SM
+// variant bit 7 (128): column passes access their column pairs in global memory directly
+template <int N1, int N2, int AXIS>
+int launch_pair_t(const PassArgs& a, int grid_y, cudaStream_t st, int variant) {
+  constexpr int G = 32 / N1;
+  constexpr int N = N1 * N2;
+  constexpr int W4 = N / (2 * G) < 4 ? N / (2 * G) : 4;
+  constexpr int W8 = N / (2 * G) < 8 ? N / (2 * G) : 8;
+  const bool pre = (variant & 32) && a.win == nullptr && a.field_n == N;
+  if (AXIS == 1 && (variant & 128)) {
+    if (variant & 64) return launch_pair_w<N1, N2, AXIS, W8, 16 / W8, false, true>(a, grid_y, st);
+    return launch_pair_w<N1, N2, AXIS, W4, 16 / W4, false, true>(a, grid_y, st);
+  }
+  if (variant & 64) return launch_pair_w<N1, N2, AXIS, W8, 16 / W8, false>(a, grid_y, st);
+  if (pre) return launch_pair_w<N1, N2, AXIS, W4, 3, true>(a, grid_y, st);
+  return launch_pair_w<N1, N2, AXIS, W4, 16 / W4, false>(a, grid_y, st);
+}
+
+// tune bit 4 (value 16): steady passes run the paired two-lines-per-thread kernel
+// (not for passes that store checkpoints).
 // tune bit 2 (value 4) selects the persistent double-buffered kernel for steady
 // passes (measured slower than the one-slot-per-CTA kernel on B200 at 128-512^2)
 template <int N1, int N2, int AXIS, int MINB>
@@ -104,6 +143,8 @@ int launch_pass_t(const PassArgs& a0, int grid_y, cudaStream_t st, int variant) 
   // tune bit 3 (value 8): column passes access global memory directly (no staging tile)
   PassArgs a = a0;
   if (AXIS == 1 && (variant & 8)) a.direct = 1;
+  if (is_steady_pass(a) && (variant & 16) && a.ckpt_store == nullptr && a.pf != nullptr)
+    return launch_pair_t<N1, N2, AXIS>(a, grid_y, st, variant);
   if (is_steady_pass(a) && a.tw2 != nullptr && (variant & 4)) return launch_pipe_t<N1, N2, AXIS, MINB>(a, grid_y, st);
   return is_steady_pass(a) ? launch_pass_s<N1, N2, AXIS, MINB, true>(a, grid_y, st)
                            : launch_pass_s<N1, N2, AXIS, MINB, false>(a, grid_y, st);

@@ -1,6 +1,6 @@
 """A small, self-checking case of the forward engine for profilers.
 
-    python -m ptyrodactyl_b200.profile_case [n] [probes] [reps]
+    python -m ptyrodactyl_b200.profile_case [n] [probes] [reps] [tune]
 
 Runs one batched forward over ``probes`` scan positions of the perovskite workload
 (n x n grid, 2 slices, one batch), then ``reps`` steady-state passes per axis
@@ -26,6 +26,7 @@ def main(argv=None) -> int:
     n = int(argv[0]) if len(argv) > 0 else 256
     probes = int(argv[1]) if len(argv) > 1 else 256
     reps = int(argv[2]) if len(argv) > 2 else 1
+    tune = int(argv[3]) if len(argv) > 3 else 3
     w = synth.CONFIG2
     dev = torch.device("cuda")
     lib = _lib.load()
@@ -40,7 +41,7 @@ def main(argv=None) -> int:
     probes = pos.shape[0]
     wt = torch.ones(1, device=dev)
     prm = ms_params(n, 2, 1, probes, w.voltage_kv, synth.SLICE_DZ, w.calib, w.calib, pot.stride(), probe.stride(),
-                    probes, 3)
+                    probes, tune)
     nb = lib.ptyro_ms_workspace_bytes(ctypes.byref(prm))
     ws = torch.empty(nb, dtype=torch.uint8, device=dev)
     out = torch.empty((probes, n, n), device=dev)
@@ -51,7 +52,7 @@ def main(argv=None) -> int:
         _lib.check(lib.ptyro_ms_steady_pass(ctypes.byref(prm), axis, reps, ws.data_ptr(), nb, st))
     torch.cuda.synchronize()
     total = float(out.sum())
-    print(f"profile case n={n} probes={probes} reps={reps}: pattern sum {total:.6g}")
+    print(f"profile case n={n} probes={probes} reps={reps} tune={tune}: pattern sum {total:.6g}")
     return 0 if total == total and abs(total) != float("inf") else 1
 
 

@@ -123,6 +123,16 @@ def check_windows(slices: torch.Tensor, modes: torch.Tensor, windows: Optional[t
     return n, f
 
 
+# Launch variant per grid edge measured fastest on B200 (ptyro_ms_params.tune bits:
+# 1/2 three CTAs per SM per axis, 16 paired two-lines-per-thread steady passes,
+# 64 eight warps per CTA, 128 direct column access); the autotuner refines it.
+DEFAULT_TUNE = {16: 147, 32: 147, 64: 147, 128: 147, 256: 211, 512: 3, 1024: 0}
+
+
+def default_tune(n: int) -> int:
+    return DEFAULT_TUNE.get(int(n), 0)
+
+
 _LANE_MIN_WAVE_BYTES = 256 << 20  # two lanes once the probes' waves span about four batches
 
 
@@ -139,7 +149,7 @@ _STREAMS: dict = {}
 def run_forward(slices: torch.Tensor, slice_thickness: float, modes: torch.Tensor, weights: torch.Tensor,
                 positions: torch.Tensor, voltage_kv: float, calib_ang: float, shift_calib_ang: float,
                 out: Optional[torch.Tensor] = None, batch: int = 0, plain: bool = False,
-                tune: int = 0, windows: Optional[torch.Tensor] = None, accumulate: bool = False,
+                tune: Optional[int] = None, windows: Optional[torch.Tensor] = None, accumulate: bool = False,
                 lanes: int = 0) -> torch.Tensor:
     """Device-level forward: all tensors already on one CUDA device.
 
@@ -155,6 +165,8 @@ def run_forward(slices: torch.Tensor, slice_thickness: float, modes: torch.Tenso
     dev = slices.device
     num_probes = positions.shape[0]
     n, f = check_windows(slices, modes, windows, num_probes)
+    if tune is None:
+        tune = default_tune(n)
     if lanes == 0:
         lanes = 2 if (not plain and num_probes * n * n * modes.shape[2] * 8 >= _LANE_MIN_WAVE_BYTES) else 1
     if lanes > 1 and num_probes >= lanes:

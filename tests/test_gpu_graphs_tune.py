@@ -50,7 +50,8 @@ def test_autotune_picks_and_caches(case, tmp_path, monkeypatch):
     at._memo.clear()
     w, pot, modes, wts, pos = case
     batch, tune = tune_forward(pot, modes, wts, pos, synth.SLICE_DZ, w.voltage_kv, w.calib)
-    assert 1 <= batch <= pos.shape[0] and 0 <= tune <= 3
+    from ptyrodactyl_b200.autotune import candidates
+    assert (batch, tune) in candidates(pot.shape[0], pos.shape[0], modes.shape[2])
     assert (tmp_path / "tune.json").exists()
     at._memo.clear()
     assert tune_forward(pot, modes, wts, pos, synth.SLICE_DZ, w.voltage_kv, w.calib) == (batch, tune)
@@ -80,3 +81,31 @@ def test_lanes_do_not_change_results():
     g.replay()
     torch.cuda.synchronize()
     assert torch.equal(g.out, one)
+
+
+@pytest.mark.parametrize("n", [16, 32, 64, 128, 256, 512])
+def test_paired_steady_kernels_are_bit_identical(n):
+    """Two-lines-per-thread f32x2 steady passes (tune bits 16, 32, 64, 128) give
+    exactly the one-line kernel's patterns, also with windows."""
+    import numpy as np
+    from oracle import multislice_ref as R
+    from ptyrodactyl_b200.simulations import run_forward
+    rng = np.random.default_rng(n)
+    s, p = 5, 6
+    dev = torch.device("cuda")
+    slices = torch.as_tensor(rng.uniform(0, 40, (n, n, s)), dtype=torch.float32, device=dev)
+    probe = R.make_probe(200.0, 25.0, (n, n), 30.0, defocus_ang=-20.0)
+    modes = torch.as_tensor(np.stack([probe, np.roll(probe, 1, 0)], -1).astype(np.complex64), device=dev)
+    wt = torch.tensor([0.6, 0.4], device=dev)
+    pos = torch.as_tensor(rng.uniform(-2, 2, (p, 2)), dtype=torch.float64, device=dev)
+    ref = run_forward(slices, 1.7, modes, wt, pos, 200.0, 0.3, 0.3, tune=3, lanes=1)
+    for tune in (19, 51, 83, 147, 211):
+        got = run_forward(slices, 1.7, modes, wt, pos, 200.0, 0.3, 0.3, tune=tune, lanes=1)
+        assert torch.equal(got, ref), tune
+    if n <= 256:
+        field = torch.as_tensor(rng.uniform(0, 40, (2 * n, 2 * n, s)), dtype=torch.float32, device=dev)
+        win = torch.as_tensor(rng.integers(0, 2 * n, (p, 2)), dtype=torch.int32, device=dev)
+        ref = run_forward(field, 1.7, modes, wt, pos, 200.0, 0.3, 0.3, tune=3, windows=win, lanes=1)
+        for tune in (19, 51, 211):
+            got = run_forward(field, 1.7, modes, wt, pos, 200.0, 0.3, 0.3, tune=tune, windows=win, lanes=1)
+            assert torch.equal(got, ref), tune
