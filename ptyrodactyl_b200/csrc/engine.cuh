@@ -626,36 +626,62 @@ static __global__ void k_reduce_dv(const float* __restrict__ contrib, int nslots
 
 // Windowed runs: field pixel (fy, fx) of dV_s collects the contribution of every
 // slot whose n x n window (origin modulo F) covers it, added in slot order (no
-// atomics). Loads of 8 slots are issued together before they are summed, so a
-// thread keeps several reads in flight; neighbouring threads read neighbouring
-// pixels of the same slot plane.
-constexpr int kReduceWinStaged = 4096;
+// atomics). Slots whose window rows miss the CTA's field row are culled once per
+// CTA; loads of 8 listed slots are issued together before they are summed, and
+// neighbouring threads read neighbouring pixels of the same slot plane.
 
 static __global__ void __launch_bounds__(256) k_reduce_dv_win(const float* __restrict__ contrib, int nb, int M, int n,
                                                        int F, const int* __restrict__ win, float* dv, long long sy,
                                                        long long sx, long long ss, int s) {
-  extern __shared__ int swin[];
-  const bool staged = nb <= kReduceWinStaged;  // window origins in shared memory when they fit
-  if (staged)
-    for (int i = threadIdx.x; i < 2 * nb; i += blockDim.x) swin[i] = win ? win[i] : 0;
-  __syncthreads();
-  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= (size_t)F * F) return;
-  const int fy = (int)(i / F), fx = (int)(i % F);
+  // a CTA covers blockDim.x (<= F) pixels of one field row fy: first the slots whose
+  // window rows contain fy are listed in slot order (warp 0, ballots), then every
+  // pixel adds the listed slots whose window columns contain it, in list order
+  extern __shared__ int sh[];
+  int* swx = sh;           // window column origin of each listed slot
+  int* sslot = sh + nb;    // listed slots, ascending
+  __shared__ int count;
+  const size_t i0 = (size_t)blockIdx.x * blockDim.x;
+  const int fy = (int)(i0 / F);
   const int fm = F - 1;
+  if (threadIdx.x < 32) {
+    int c = 0;
+    for (int b0 = 0; b0 < nb; b0 += 32) {
+      const int bb = b0 + (int)threadIdx.x;
+      int wy = 0, wx = 0;
+      if (bb < nb && win) {
+        wy = win[2 * bb];
+        wx = win[2 * bb + 1];
+      }
+      const bool in = bb < nb && ((fy - wy) & fm) < n;
+      const unsigned mask = __ballot_sync(0xffffffffu, in);
+      if (in) {
+        const int pos = c + __popc(mask & ((1u << threadIdx.x) - 1u));
+        sslot[pos] = bb;
+        swx[pos] = wx;
+      }
+      c += __popc(mask);
+    }
+    if (threadIdx.x == 0) count = c;
+  }
+  __syncthreads();
+  const size_t i = i0 + threadIdx.x;
+  if (i >= (size_t)F * F) return;
+  const int fx = (int)(i % F);
+  const int ly_base = fy;
   const size_t nn = (size_t)n * n;
+  const int cnt = count;
   float acc = 0.f;
-  for (int b0 = 0; b0 < nb; b0 += 8) {
+  for (int k0 = 0; k0 < cnt; k0 += 8) {
     float v[8];
 #pragma unroll
     for (int u = 0; u < 8; ++u) {
-      const int bb = b0 + u;
+      const int k = k0 + u;
       v[u] = 0.f;
-      if (bb < nb) {
-        const int wy = staged ? swin[2 * bb] : (win ? win[2 * bb] : 0);
-        const int wx = staged ? swin[2 * bb + 1] : (win ? win[2 * bb + 1] : 0);
-        const int ly = (fy - wy) & fm, lx = (fx - wx) & fm;
-        if (ly < n && lx < n) {
+      if (k < cnt) {
+        const int bb = sslot[k];
+        const int wy = win ? win[2 * bb] : 0;
+        const int ly = (ly_base - wy) & fm, lx = (fx - swx[k]) & fm;
+        if (lx < n) {
           const float* cp = contrib + (size_t)bb * M * nn + (size_t)ly * n + lx;
           float t = cp[0];
           for (int m = 1; m < M; ++m) t += cp[(size_t)m * nn];
@@ -672,10 +698,16 @@ static __global__ void __launch_bounds__(256) k_reduce_dv_win(const float* __res
 static int launch_reduce_dv_win(const float* contrib, int nb, int M, int n, int F, const int* win, float* dv,
                                 long long sy, long long sx, long long ss, int s, cudaStream_t st) {
   const size_t ff = (size_t)F * F;
-  const size_t smem = nb <= kReduceWinStaged ? 2 * sizeof(int) * (size_t)nb : 0;
-  k_reduce_dv_win<<<(unsigned)((ff + 255) / 256), 256, smem, st>>>(
-      contrib, nb, M, n, F, win, dv, sy, sx, ss, s);
-  return check_launch("k_reduce_dv_win");
+  const int threads = F < 256 ? F : 256;  // a CTA never spans two field rows
+  constexpr int kChunk = 4096;            // probes listed per launch (32 KB of shared memory)
+  for (int c0 = 0; c0 < nb; c0 += kChunk) {  // chunks add into dv in probe order
+    const int cn = nb - c0 < kChunk ? nb - c0 : kChunk;
+    k_reduce_dv_win<<<(unsigned)((ff + threads - 1) / threads), threads, 2 * sizeof(int) * (size_t)cn, st>>>(
+        contrib + (size_t)c0 * M * n * n, cn, M, n, F, win ? win + 2 * (size_t)c0 : nullptr, dv, sy, sx, ss, s);
+    int rc = check_launch("k_reduce_dv_win");
+    if (rc) return rc;
+  }
+  return PTYRO_OK;
 }
 
 // beam spectrum gradient: acc[m] += sum_b lam[b*M + m], in probe order.

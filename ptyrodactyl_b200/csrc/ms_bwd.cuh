@@ -14,7 +14,7 @@
 // exists, which bounds the rounding drift of running U backwards. Passes follow
 // the forward's schedule: op'_0 = IFFT2, op'_j = U^H, op'_S = FFT2 (adjoint only).
 #pragma once
-#include "ms_pass.cuh"
+#include "ms_pair.cuh"
 
 namespace ptyro {
 
@@ -44,30 +44,39 @@ struct BwdArgs {
   float scale;             // 1/N after OP_IFFT
 };
 
-template <int N1, int N2, int AXIS>
-__device__ __forceinline__ void bwd_load(const BwdArgs& a, const float2* w, float2 (&v)[N2], bool korder, int t,
-                                         int line, int lc, float2* work, int line0, int pitch) {
+// Shared memory of an adjoint pass: twiddles + max(paired exchange buffers, tile).
+template <int N1, int N2>
+size_t bwd_smem_bytes(int warps) {
+  constexpr int N = N1 * N2, G = 32 / N1;
+  const size_t lines = (size_t)warps * G;
+  const size_t xbuf = sizeof(Pair) * lines * PairBuf<N1, N2>::kSize;
+  const size_t tile = sizeof(float2) * (size_t)N * (lines + G);
+  return sizeof(float2) * (size_t)N + (xbuf > tile ? xbuf : tile);
+}
+
+// Read one wave of a line from global memory (rows) or the staged tile (columns)
+// into half H (0: the forward wave, 1: the adjoint) of the paired registers.
+template <int N1, int N2, int AXIS, int H>
+__device__ __forceinline__ void bwd_load_half(const float2* w, Pair (&v)[N2], bool korder, int t, int line, int lc,
+                                              const float2* work, int pitch) {
   constexpr int N = N1 * N2;
-  if (AXIS == 0) {
-    if (korder) {
 #pragma unroll
-      for (int r = 0; r < N2; ++r) v[r] = w[(size_t)line * N + korder_index<N1, N2>(t, r)];
+  for (int r = 0; r < N2; ++r) {
+    const int e = korder ? korder_index<N1, N2>(t, r) : t + N1 * r;
+    const float2 x = AXIS == 0 ? w[(size_t)line * N + e] : work[e * pitch + lc];
+    if (H == 0) {
+      v[r].re.x = x.x;
+      v[r].im.x = x.y;
     } else {
-#pragma unroll
-      for (int j = 0; j < N2; ++j) v[j] = w[(size_t)line * N + t + N1 * j];
-    }
-  } else {
-    (void)line;
-    if (korder) {
-#pragma unroll
-      for (int r = 0; r < N2; ++r) v[r] = work[korder_index<N1, N2>(t, r) * pitch + lc];
-    } else {
-#pragma unroll
-      for (int j = 0; j < N2; ++j) v[j] = work[(t + N1 * j) * pitch + lc];
+      v[r].re.y = x.x;
+      v[r].im.y = x.y;
     }
   }
 }
 
+// The forward wave psi and the adjoint lambda of a line go through identical
+// operators, so they are carried as one Pair per element (half 0 = psi, half 1 =
+// lambda) and every transform step is one paired f32x2 operation for both.
 template <int N1, int N2, int AXIS, int WARPS>
 __device__ __forceinline__ void bwd_body(const BwdArgs& a, const int slot) {
   using Geo = PassGeom<N1, N2>;
@@ -91,7 +100,8 @@ __device__ __forceinline__ void bwd_body(const BwdArgs& a, const int slot) {
   const int lc = warp * G + gl;
   const int line0 = blockIdx.x * lines;
   const int line = line0 + lc;
-  float2* buf = work + lc * LB::kSize;
+  // exchange buffer of the line (Pair elements)
+  Pair* buf = reinterpret_cast<Pair*>(work) + lc * PairBuf<N1, N2>::kSize;
   const size_t NN = (size_t)N * N;
   const int b = slot / a.n_modes, m = slot % a.n_modes;
   auto off = [&](int e) -> size_t { return AXIS == 0 ? (size_t)line * N + e : (size_t)e * N + line; };
@@ -99,7 +109,7 @@ __device__ __forceinline__ void bwd_body(const BwdArgs& a, const int slot) {
   float2* Wp = a.psi + (size_t)slot * NN;
   float2* Wl = a.lam + (size_t)slot * NN;
   const bool korder_in = a.init || a.op1 == OP_IFFT;
-  float2 p[N2], l[N2];
+  Pair v[N2];
 
   // ---- load both waves (column passes stage each through the tile in turn)
   if (a.init) {
@@ -113,38 +123,39 @@ __device__ __forceinline__ void bwd_body(const BwdArgs& a, const int slot) {
       const int k = korder_index<N1, N2>(t, r);
       const float2 av = A[off(k)];
       const float gv = AXIS == 0 ? g[(size_t)ks_line * N + (k + N / 2) % N] : g[(size_t)((k + N / 2) % N) * N + ks_line];
-      p[r] = av;
-      l[r] = cscale(av, s * gv);
+      v[r] = make_pair(av, cscale(av, s * gv));
     }
   } else if (AXIS == 0) {
-    if (a.op1 != OP_FFT) bwd_load<N1, N2, AXIS>(a, Wp, p, korder_in, t, line, lc, work, line0, pitch);
-    bwd_load<N1, N2, AXIS>(a, Wl, l, korder_in, t, line, lc, work, line0, pitch);
+    if (a.op1 != OP_FFT) {
+      bwd_load_half<N1, N2, AXIS, 0>(Wp, v, korder_in, t, line, lc, work, pitch);
+    } else {
+#pragma unroll
+      for (int r = 0; r < N2; ++r) v[r].re.x = v[r].im.x = 0.f;  // psi is not carried
+    }
+    bwd_load_half<N1, N2, AXIS, 1>(Wl, v, korder_in, t, line, lc, work, pitch);
   } else {
+    if (a.op1 == OP_FFT) {
+#pragma unroll
+      for (int r = 0; r < N2; ++r) v[r].re.x = v[r].im.x = 0.f;
+    }
     for (int wv = a.op1 == OP_FFT ? 1 : 0; wv < 2; ++wv) {
       const float2* W = wv == 0 ? Wp : Wl;
       __syncthreads();
       tile_load<N, lines, pitch, WARPS * 32>(W, work, line0);
       __syncthreads();
-      if (wv == 0) bwd_load<N1, N2, AXIS>(a, W, p, korder_in, t, line, lc, work, line0, pitch);
-      else bwd_load<N1, N2, AXIS>(a, W, l, korder_in, t, line, lc, work, line0, pitch);
+      if (wv == 0) bwd_load_half<N1, N2, AXIS, 0>(W, v, korder_in, t, line, lc, work, pitch);
+      else bwd_load_half<N1, N2, AXIS, 1>(W, v, korder_in, t, line, lc, work, pitch);
     }
     __syncthreads();
   }
 
   // ---- op1 on both
   if (a.op1 == OP_IFFT) {
-    line_k_to_nat<N1, N2, +1>(p, t, buf, tw);
-    line_k_to_nat<N1, N2, +1>(l, t, buf, tw);
+    line_k_to_nat<N1, N2, +1>(v, t, buf, tw);
 #pragma unroll
-    for (int j = 0; j < N2; ++j) {
-      p[j] = cscale(p[j], a.scale);
-      l[j] = cscale(l[j], a.scale);
-    }
-  } else if (a.op1 == OP_CONV_CONJ) {
-    apply_op<N1, N2>(OP_CONV_CONJ, p, t, buf, tw, a.pf);
-    apply_op<N1, N2>(OP_CONV_CONJ, l, t, buf, tw, a.pf);
-  } else if (a.op1 == OP_FFT) {
-    apply_op<N1, N2>(OP_FFT, l, t, buf, tw, a.pf);
+    for (int j = 0; j < N2; ++j) v[j] = cscale(v[j], a.scale);
+  } else if (a.op1 == OP_CONV_CONJ || a.op1 == OP_FFT) {
+    apply_op<N1, N2>(a.op1, v, t, buf, tw, a.pf);
   }
 
   // ---- slice point: checkpoint refresh, dV contribution, conj(T)
@@ -153,35 +164,38 @@ __device__ __forceinline__ void bwd_body(const BwdArgs& a, const int slot) {
     if (a.ckpt) {
       const float2* ck = a.ckpt + (size_t)slot * a.res_stride;
 #pragma unroll
-      for (int j = 0; j < N2; ++j) p[j] = ck[off(t + N1 * j)];
+      for (int j = 0; j < N2; ++j) {
+        const float2 c = ck[off(t + N1 * j)];
+        v[j].re.x = c.x;
+        v[j].im.x = c.y;
+      }
     }
 #pragma unroll
-    for (int j = 0; j < N2; ++j) cv[j] = a.sigma2 * (p[j].x * l[j].y - p[j].y * l[j].x);
+    for (int j = 0; j < N2; ++j) cv[j] = a.sigma2 * (v[j].re.x * v[j].im.y - v[j].im.x * v[j].re.y);
     int eoff;
     const float2* T = trans_row<AXIS>(a.trans, a.trans_t, a.field_n, a.t_slice, a.win, b, line, &eoff);
     const int fm = a.field_n - 1;
 #pragma unroll
-    for (int j = 0; j < N2; ++j) {
-      const float2 tv = __ldg(T + ((t + N1 * j + eoff) & fm));
-      p[j] = cmulc(p[j], tv);
-      l[j] = cmulc(l[j], tv);
-    }
+    for (int j = 0; j < N2; ++j) v[j] = cmulc(v[j], __ldg(T + ((t + N1 * j + eoff) & fm)));
   }
 
-  // ---- op2
+  // ---- op2 (psi too, even where it is no longer needed: it rides in the same instructions)
   bool lam_k = a.op1 == OP_FFT;
   if (a.op2 == OP_CONV_CONJ) {
-    if (!a.psi_done) apply_op<N1, N2>(OP_CONV_CONJ, p, t, buf, tw, a.pf);
-    apply_op<N1, N2>(OP_CONV_CONJ, l, t, buf, tw, a.pf);
+    apply_op<N1, N2>(OP_CONV_CONJ, v, t, buf, tw, a.pf);
   } else if (a.op2 == OP_FFT) {
-    apply_op<N1, N2>(OP_FFT, l, t, buf, tw, a.pf);
+    apply_op<N1, N2>(OP_FFT, v, t, buf, tw, a.pf);
     lam_k = true;
   }
   if (a.beam_epi) {
     // lam is k-order along this axis: multiply conj(ramp(k)) of this axis
     const float2* ra = (AXIS == 0 ? a.ramp_x : a.ramp_y) + (size_t)b * N;
 #pragma unroll
-    for (int r = 0; r < N2; ++r) l[r] = cmulc(l[r], ra[korder_index<N1, N2>(t, r)]);
+    for (int r = 0; r < N2; ++r) {
+      const float2 l = cmulc(pair_b(v[r]), ra[korder_index<N1, N2>(t, r)]);
+      v[r].re.y = l.x;
+      v[r].im.y = l.y;
+    }
   }
 
   // ---- store
@@ -189,15 +203,10 @@ __device__ __forceinline__ void bwd_body(const BwdArgs& a, const int slot) {
   if (AXIS == 0) {
     if (store_psi) {
 #pragma unroll
-      for (int j = 0; j < N2; ++j) Wp[off(t + N1 * j)] = p[j];
+      for (int j = 0; j < N2; ++j) Wp[off(t + N1 * j)] = pair_a(v[j]);
     }
-    if (lam_k) {
 #pragma unroll
-      for (int r = 0; r < N2; ++r) Wl[off(korder_index<N1, N2>(t, r))] = l[r];
-    } else {
-#pragma unroll
-      for (int j = 0; j < N2; ++j) Wl[off(t + N1 * j)] = l[j];
-    }
+    for (int r = 0; r < N2; ++r) Wl[off(lam_k ? korder_index<N1, N2>(t, r) : t + N1 * r)] = pair_b(v[r]);
     if (a.t_slice >= 0 && a.contrib) {
       float* C = a.contrib + (size_t)slot * NN;
 #pragma unroll
@@ -210,15 +219,11 @@ __device__ __forceinline__ void bwd_body(const BwdArgs& a, const int slot) {
       __syncthreads();
       if (wv == 0) {
 #pragma unroll
-        for (int j = 0; j < N2; ++j) work[(t + N1 * j) * pitch + lc] = p[j];
+        for (int j = 0; j < N2; ++j) work[(t + N1 * j) * pitch + lc] = pair_a(v[j]);
       } else if (wv == 1) {
-        if (lam_k) {
 #pragma unroll
-          for (int r = 0; r < N2; ++r) work[korder_index<N1, N2>(t, r) * pitch + lc] = l[r];
-        } else {
-#pragma unroll
-          for (int j = 0; j < N2; ++j) work[(t + N1 * j) * pitch + lc] = l[j];
-        }
+        for (int r = 0; r < N2; ++r)
+          work[(lam_k ? korder_index<N1, N2>(t, r) : t + N1 * r) * pitch + lc] = pair_b(v[r]);
       } else {
         float* tile = reinterpret_cast<float*>(work);
 #pragma unroll

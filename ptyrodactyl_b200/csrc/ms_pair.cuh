@@ -132,6 +132,21 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) ms_pass_pair_kernel(PassArgs
       v[j] = cmul(v[j], __ldg(Ta + ((t + N1 * j + oa) & fm)), __ldg(Tb + ((t + N1 * j + ob) & fm)));
   }
 
+  // gradient-mode checkpoint: the wave right after the T multiply
+  if (a.ckpt_store) {
+    float2* ck = a.ckpt_store + (size_t)slot * a.res_stride;
+#pragma unroll
+    for (int j = 0; j < N2; ++j) {
+      if (AXIS == 0) {
+        ck[(size_t)la * N + t + N1 * j] = pair_a(v[j]);
+        ck[(size_t)lb * N + t + N1 * j] = pair_b(v[j]);
+      } else {
+        *reinterpret_cast<float4*>(ck + (size_t)(t + N1 * j) * N + la) =
+            make_float4(v[j].re.x, v[j].im.x, v[j].re.y, v[j].im.y);
+      }
+    }
+  }
+
   // ---- start slice s's convolution along this axis
   line_nat_to_k<N1, N2, -1>(v, t, buf, tw);
 #pragma unroll

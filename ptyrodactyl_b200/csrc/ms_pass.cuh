@@ -152,9 +152,8 @@ __device__ __forceinline__ const float2* trans_row(const float2* trans, const fl
 }
 
 // op on registers in natural distribution; returns true if the result is k-order.
-template <int N1, int N2>
-__device__ __forceinline__ bool apply_op(int op, float2 (&v)[N2], int t, float2* buf, const float2* tw,
-                                         const float2* pf) {
+template <int N1, int N2, typename T>
+__device__ __forceinline__ bool apply_op(int op, T (&v)[N2], int t, T* buf, const float2* tw, const float2* pf) {
   if (op == OP_FFT) {
     line_nat_to_k<N1, N2, -1>(v, t, buf, tw);
     return true;

@@ -37,7 +37,7 @@ int launch_bwd_t(const BwdArgs& a, int grid_y, cudaStream_t st) {
   constexpr int N = Geo::N;
   constexpr int W = Geo::kWarps;
   constexpr int MINB = N2 <= 16 ? 2 : 1;  // two resident CTAs where the register budget allows
-  const size_t smem = Geo::smem_bytes(W);
+  const size_t smem = bwd_smem_bytes<N1, N2>(W);
   static bool attr_done = false;
   if (!attr_done) {
     cudaFuncSetAttribute(ms_bwd_pass_kernel<N1, N2, AXIS, W, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -134,8 +134,7 @@ int launch_pair_t(const PassArgs& a, int grid_y, cudaStream_t st, int variant) {
   return launch_pair_w<N1, N2, AXIS, W4, 16 / W4, false>(a, grid_y, st);
 }
 
-// tune bit 4 (value 16): steady passes run the paired two-lines-per-thread kernel
-// (not for passes that store checkpoints).
+// tune bit 4 (value 16): steady passes run the paired two-lines-per-thread kernel.
 // tune bit 2 (value 4) selects the persistent double-buffered kernel for steady
 // passes (measured slower than the one-slot-per-CTA kernel on B200 at 128-512^2)
 template <int N1, int N2, int AXIS, int MINB>
@@ -143,7 +142,7 @@ int launch_pass_t(const PassArgs& a0, int grid_y, cudaStream_t st, int variant) 
   // tune bit 3 (value 8): column passes access global memory directly (no staging tile)
   PassArgs a = a0;
   if (AXIS == 1 && (variant & 8)) a.direct = 1;
-  if (is_steady_pass(a) && (variant & 16) && a.ckpt_store == nullptr && a.pf != nullptr)
+  if (is_steady_pass(a) && (variant & 16) && a.pf != nullptr)
     return launch_pair_t<N1, N2, AXIS>(a, grid_y, st, variant);
   if (is_steady_pass(a) && a.tw2 != nullptr && (variant & 4)) return launch_pipe_t<N1, N2, AXIS, MINB>(a, grid_y, st);
   return is_steady_pass(a) ? launch_pass_s<N1, N2, AXIS, MINB, true>(a, grid_y, st)
@@ -172,7 +171,7 @@ int launch_bwd_multi_t(const BwdArgs* descs, const int2* rows, int nrows, cudaSt
   using Geo = PassGeom<N1, N2>;
   constexpr int W = Geo::kWarps;
   constexpr int MINB = N2 <= 16 ? 2 : 1;
-  const size_t smem = Geo::smem_bytes(W);
+  const size_t smem = bwd_smem_bytes<N1, N2>(W);
   static bool attr_done = false;
   if (!attr_done) {
     cudaFuncSetAttribute(ms_bwd_multi_kernel<N1, N2, AXIS, W, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
