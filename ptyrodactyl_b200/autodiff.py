@@ -23,7 +23,15 @@ from typing import Optional
 import torch
 
 from . import _lib
-from .simulations import _check_edge, _stream_ptr, _workspace, check_windows, ms_params, relativistic_wavelength_ang
+from .simulations import (
+    _check_edge,
+    _stream_ptr,
+    _workspace,
+    check_windows,
+    default_tune,
+    ms_params,
+    relativistic_wavelength_ang,
+)
 
 DEFAULT_CKPT = 0  # 0: ceil(sqrt(S))
 
@@ -147,7 +155,8 @@ class Stem4dFunction(torch.autograd.Function):
 def stem_4d_patterns(slices: torch.Tensor, modes: torch.Tensor, weights: torch.Tensor, positions: torch.Tensor,
                      slice_thickness: float, voltage_kv: float, calib_ang: float,
                      shift_calib_ang: Optional[float] = None, ckpt_every: int = DEFAULT_CKPT,
-                     batch: int = 0, tune: int = 0, windows: Optional[torch.Tensor] = None) -> torch.Tensor:
+                     batch: int = 0, tune: Optional[int] = None,
+                     windows: Optional[torch.Tensor] = None) -> torch.Tensor:
     """Differentiable patterns (P, n, n) of the forward model (device tensors); with
     ``windows`` the potential is a larger periodic field (see ``run_forward``).
     Reverse mode (``backward``, ``torch.func.grad/vjp``) and forward mode
@@ -155,7 +164,8 @@ def stem_4d_patterns(slices: torch.Tensor, modes: torch.Tensor, weights: torch.T
     record = bool(slices.requires_grad or modes.requires_grad) and torch.is_grad_enabled()
     return Stem4dFunction.apply(slices, modes, weights, positions, float(slice_thickness), float(voltage_kv),
                                 float(calib_ang), float(calib_ang if shift_calib_ang is None else shift_calib_ang),
-                                int(ckpt_every), int(batch), int(tune), windows, record)[0]
+                                int(ckpt_every), int(batch), int(default_tune(modes.shape[0]) if tune is None else tune),
+                                windows, record)[0]
 
 
 def _like(t: Optional[torch.Tensor], primal: torch.Tensor, dtype) -> Optional[torch.Tensor]:
@@ -197,7 +207,7 @@ def jvp(slices, modes, weights, positions, tangent_slices, tangent_modes, slice_
 
 
 def vjp(slices, modes, weights, positions, grad_patterns, slice_thickness, voltage_kv, calib_ang,
-        shift_calib_ang=None, ckpt_every: int = DEFAULT_CKPT, batch: int = 0, windows=None):
+        shift_calib_ang=None, ckpt_every: int = DEFAULT_CKPT, batch: int = 0, windows=None, tune=None):
     """(patterns, dL/dV, dL/dmodes in JAX's convention) for dL/dpatterns = grad_patterns."""
     lib = _lib.load()
     dev = slices.device
@@ -206,7 +216,7 @@ def vjp(slices, modes, weights, positions, grad_patterns, slice_thickness, volta
     k = _ckpt_for(S, ckpt_every)
     sc = float(calib_ang if shift_calib_ang is None else shift_calib_ang)
     prm = ms_params(n, S, M, P, voltage_kv, slice_thickness, calib_ang, sc, slices.stride(), modes.stride(), batch,
-                    0, f, windows)
+                    default_tune(n) if tune is None else int(tune), f, windows)
     out = torch.empty((P, n, n), dtype=torch.float32, device=dev)
     res = torch.empty(max(1, lib.ptyro_ms_residual_bytes(ctypes.byref(prm), k) // 4), dtype=torch.float32,
                       device=dev)

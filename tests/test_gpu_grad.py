@@ -167,3 +167,18 @@ def test_windowed_forward_and_vjp_match_oracle():
     beam = pb.create_probe_modes(probe[..., None], [1.0], 0.3)
     s4 = pb.stem_4d_windowed(slices, beam, mic, det, windows)
     assert rel_l2(s4.data.cpu().numpy(), want) < TOL
+
+
+def test_gradient_identical_across_launch_variants():
+    """Checkpointing forward passes in the paired kernel give the scalar kernel's
+    residuals, hence identical gradients."""
+    pot, modes, w, pos, g = _case(128, 6, 2, 4, seed=9)
+    dev = torch.device("cuda")
+    args = [torch.as_tensor(pot, dtype=torch.float32, device=dev), torch.as_tensor(modes.astype(np.complex64), device=dev),
+            torch.as_tensor(w, dtype=torch.float32, device=dev), torch.as_tensor(pos, dtype=torch.float64, device=dev),
+            torch.as_tensor(g, dtype=torch.float32, device=dev), 1.7, 200.0, 0.3]
+    ref = pb.vjp(*args, ckpt_every=2, tune=3)
+    for tune in (19, 147, 211):
+        got = pb.vjp(*args, ckpt_every=2, tune=tune)
+        for a, b in zip(ref, got):
+            assert torch.equal(a, b), tune
