@@ -251,6 +251,24 @@ int ptyro_atom_slices(int32_t n, int32_t num_atoms, int32_t num_types, int32_t n
                       const float* atom_mask, double calib_ang, float* slices, int64_t sy, int64_t sx, int64_t ss,
                       void* workspace, size_t workspace_bytes, void* stream);
 
+/* Workspace bytes of ptyro_place_atoms (0 when invalid). */
+size_t ptyro_place_atoms_workspace_bytes(int32_t n, int32_t num_types, int32_t num_atoms);
+
+/* Sub-pixel placement of crystal_potential_slices (src/ptyrodactyl/multislice/
+ * atom_potentials.py:826-994): slice s = real(ifft2(sum over its atoms of
+ * fft2(P_type) exp(2 pi i (kx shift_x + ky shift_y)))), k = fftfreq(n) per pixel.
+ *   shift_y, shift_x   float64 device (num_atoms): the atom's offset from the grid
+ *                      centre in pixels ((coord - min) / pixel_size - n / 2)
+ *   group_offsets_host int32 HOST (num_slices * num_types + 1): the atoms are sorted
+ *                      by (slice, type); group g = s * num_types + t holds atoms
+ *                      [offsets[g], offsets[g+1])
+ *   atom_potentials    float32 device (num_types, n, n) per-type lookup potentials
+ *   slices             float32 (n, n, num_slices) written with strides (sy, sx, ss) */
+int ptyro_place_atoms(int32_t n, int32_t num_atoms, int32_t num_types, int32_t num_slices, const double* shift_y,
+                      const double* shift_x, const int32_t* group_offsets_host, const float* atom_potentials,
+                      float* slices, int64_t sy, int64_t sx, int64_t ss, void* workspace, size_t workspace_bytes,
+                      void* stream);
+
 /* ---------------------------------------------------------------- scheduler
  * Continuous batching of forward and gradient jobs of any grid edge, slice count
  * and scan size (the batching and serving patterns; no reference counterpart:

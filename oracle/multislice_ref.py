@@ -481,3 +481,45 @@ def stem_4d_ensemble(slices, slice_thickness, pot_calib, beam_modes, beam_calib,
     shifted = shift_beam_fourier(beam_modes, positions, real_space_calib_ang)
     return np.stack([ensemble_cbed(slices, slice_thickness, pot_calib, shifted[i], beam_calib, voltage_kv, axes)
                      for i in range(positions.shape[0])])
+
+
+def crystal_potential_slices(positions, atomic_numbers, lattice, atom_potentials, pixel_size, slice_thickness=1.0,
+                             repeats=(1, 1, 1), padding=4.0, grid_shape=None):
+    """crystal_potential_slices (multislice/atom_potentials.py:1364-1510) given the
+    per-element lookup potentials (atomic number -> (H, W), atom at the centre):
+    lattice repeats (:1126-1241), z slicing (:684-745), padded grid (:748-823), every
+    atom's Fourier sub-pixel shift of its lookup added to its slice (:826-994), crop.
+    Returns (h, w, S) float64."""
+    positions = np.asarray(positions, np.float64)
+    numbers = np.asarray(atomic_numbers)
+    reps = list(repeats)
+    if any(r > 1 for r in reps):
+        ix, iy, iz = np.meshgrid(np.arange(reps[0]), np.arange(reps[1]), np.arange(reps[2]), indexing="ij")
+        shifts = np.stack([ix.ravel(), iy.ravel(), iz.ravel()], -1).astype(np.float64) @ np.asarray(lattice)
+        positions = (positions[None] + shifts[:, None]).reshape(-1, 3)
+        numbers = np.tile(numbers, shifts.shape[0])
+    z = positions[:, 2]
+    sidx = np.floor((z - z.min()) / slice_thickness).astype(int)
+    x, y = positions[:, 0], positions[:, 1]
+    x_min, y_min = x.min() - padding, y.min() - padding
+    if grid_shape is not None:
+        height, width, num_slices = grid_shape
+    else:
+        width = int(np.ceil((x.max() + padding - x_min) / pixel_size))
+        height = int(np.ceil((y.max() + padding - y_min) / pixel_size))
+        crop = int(round(padding / pixel_size))
+        width, height = max(width, 2 * crop + 1), max(height, 2 * crop + 1)
+        num_slices = int(sidx.max()) + 1
+    ky = np.fft.fftfreq(height, d=1.0).reshape(-1, 1)
+    kx = np.fft.fftfreq(width, d=1.0).reshape(1, -1)
+    out = np.zeros((height, width, num_slices))
+    spectra = {int(e): np.fft.fft2(np.asarray(p, np.float64)) for e, p in atom_potentials.items()}
+    for a in range(positions.shape[0]):
+        if not 0 <= sidx[a] < num_slices:
+            continue
+        sx = (x[a] - x_min) / pixel_size - width / 2.0
+        sy = (y[a] - y_min) / pixel_size - height / 2.0
+        phase = np.exp(2j * np.pi * (kx * sx + ky * sy))
+        out[:, :, sidx[a]] += np.real(np.fft.ifft2(spectra[int(numbers[a])] * phase))
+    crop = int(round(padding / pixel_size))
+    return out[crop:height - crop, crop:width - crop, :]

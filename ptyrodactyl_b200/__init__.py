@@ -50,6 +50,7 @@ from .detectors import (  # noqa: F401
 )
 from .autodiff import Stem4dFunction, jvp, make_probe_differentiable, stem_4d_patterns, vjp  # noqa: F401
 from . import jacobian  # noqa: F401
+from .crystal import CrystalData, create_crystal_data, crystal_potential_slices  # noqa: F401
 from .ensemble import (  # noqa: F401
     coherence_to_distribution,
     ensemble_axes_for_cbed,
