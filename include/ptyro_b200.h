@@ -269,6 +269,18 @@ int ptyro_place_atoms(int32_t n, int32_t num_atoms, int32_t num_types, int32_t n
                       float* slices, int64_t sy, int64_t sx, int64_t ss, void* workspace, size_t workspace_bytes,
                       void* stream);
 
+/* Scratch bytes of ptyro_clip_resize: a (P, hc, wo) float32 intermediate. */
+size_t ptyro_clip_resize_workspace_bytes(int64_t num_patterns, int32_t hc, int32_t wo);
+
+/* clip_cbed (src/ptyrodactyl/plots/figuring.py:37-117) over P stored float32 patterns
+ * (P, h, w): the crop rows [y0, y0 + hc) and columns [x0, x0 + wc), resized by the
+ * separable weight matrices wy (ho, hc) and wx (wo, wc) (row-major float32: output
+ * index major) into out (P, ho, wo). The caller builds the weights of the resize
+ * method (jax.image.resize "linear" for the reference). */
+int ptyro_clip_resize(const float* patterns, int64_t num_patterns, int32_t h, int32_t w, int32_t y0, int32_t x0,
+                      int32_t hc, int32_t wc, const float* wy, int32_t ho, const float* wx, int32_t wo, float* out,
+                      void* workspace, size_t workspace_bytes, void* stream);
+
 /* ---------------------------------------------------------------- scheduler
  * Continuous batching of forward and gradient jobs of any grid edge, slice count
  * and scan size (the batching and serving patterns; no reference counterpart:

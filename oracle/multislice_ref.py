@@ -523,3 +523,34 @@ def crystal_potential_slices(positions, atomic_numbers, lattice, atom_potentials
         out[:, :, sidx[a]] += np.real(np.fft.ifft2(spectra[int(numbers[a])] * phase))
     crop = int(round(padding / pixel_size))
     return out[crop:height - crop, crop:width - crop, :]
+
+
+def resize_linear_weights(input_size, output_size, antialias=True):
+    """jax.image.resize(method="linear") weights along one axis (jax 0.9.2,
+    jax/_src/image/scale.py compute_weight_mat): triangle kernel at half-pixel
+    centres, widened by the downscale factor, normalised, zero outside the input.
+    Returns (input_size, output_size)."""
+    inv_scale = input_size / output_size
+    kernel_scale = max(inv_scale, 1.0) if antialias else 1.0
+    sample_f = (np.arange(output_size) + 0.5) * inv_scale - 0.5
+    x = np.abs(sample_f[None, :] - np.arange(input_size, dtype=np.float64)[:, None]) / kernel_scale
+    w = np.maximum(0.0, 1.0 - x)
+    tot = w.sum(axis=0, keepdims=True)
+    w = np.where(np.abs(tot) > 1000.0 * float(np.finfo(np.float32).eps), w / np.where(tot != 0, tot, 1), 0.0)
+    return np.where(((sample_f >= -0.5) & (sample_f <= input_size - 0.5))[None, :], w, 0.0)
+
+
+def clip_cbed(cbed, fourier_calib_inv_ang, voltage_kv, extent_mrad, output_shape):
+    """plots/figuring.py:37-117: crop around (h//2, w//2) to ceil(extent / calib) pixels
+    each side (clamped), then a linear resize of the axes whose size changes."""
+    cbed = np.asarray(cbed, np.float64)
+    h, w = cbed.shape
+    px = int(np.ceil((extent_mrad / (relativistic_wavelength_ang(voltage_kv) * 1000.0)) / fourier_calib_inv_ang))
+    y0, y1 = max(0, h // 2 - px), min(h, h // 2 + px)
+    x0, x1 = max(0, w // 2 - px), min(w, w // 2 + px)
+    c = cbed[y0:y1, x0:x1]
+    if output_shape[0] != c.shape[0]:
+        c = resize_linear_weights(c.shape[0], output_shape[0]).T @ c
+    if output_shape[1] != c.shape[1]:
+        c = c @ resize_linear_weights(c.shape[1], output_shape[1])
+    return c

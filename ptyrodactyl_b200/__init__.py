@@ -44,6 +44,8 @@ from .simulations import (  # noqa: F401
 from .detectors import (  # noqa: F401
     annular_detector,
     annular_mask,
+    clip_cbed,
+    stem_4d_clipped,
     stem_4d_annular,
     stem_4d_detectors,
     virtual_detectors,

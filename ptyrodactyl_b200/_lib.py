@@ -45,6 +45,8 @@ EXPORTED_SYMBOLS = (
     "ptyro_ms_amplitudes",
     "ptyro_place_atoms_workspace_bytes",
     "ptyro_place_atoms",
+    "ptyro_clip_resize_workspace_bytes",
+    "ptyro_clip_resize",
     "ptyro_ms_residual_bytes",
     "ptyro_ms_forward_ckpt",
     "ptyro_ms_backward_workspace_bytes",
@@ -196,6 +198,10 @@ def _declare(lib) -> None:
     lib.ptyro_place_atoms_workspace_bytes.argtypes = [i32, i32, i32]
     lib.ptyro_place_atoms.restype = ctypes.c_int
     lib.ptyro_place_atoms.argtypes = [i32, i32, i32, i32, vp, vp, vp, vp, vp, i64, i64, i64, vp, sz, vp]
+    lib.ptyro_clip_resize_workspace_bytes.restype = sz
+    lib.ptyro_clip_resize_workspace_bytes.argtypes = [i64, i32, i32]
+    lib.ptyro_clip_resize.restype = ctypes.c_int
+    lib.ptyro_clip_resize.argtypes = [vp, i64, i32, i32, i32, i32, i32, i32, vp, i32, vp, i32, vp, vp, sz, vp]
     lib.ptyro_atom_slices_workspace_bytes.restype = sz
     lib.ptyro_atom_slices_workspace_bytes.argtypes = [i32, i32]
     lib.ptyro_atom_slices.restype = ctypes.c_int

@@ -218,3 +218,69 @@ int ptyro_place_atoms(int32_t n, int32_t num_atoms, int32_t num_types, int32_t n
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------- CBED clip + resize
+// clip_cbed (src/ptyrodactyl/plots/figuring.py:37-117) over a batch of stored
+// patterns: the central crop [y0, y0 + hc) x [x0, x0 + wc), then a separable linear
+// resize given as dense weight matrices wy (ho x hc) and wx (wo x wc), applied along
+// x into a (P, hc, wo) scratch and then along y.
+namespace ptyro {
+
+static __global__ void k_resize_x(const float* __restrict__ pat, int h, int w, int y0, int x0, int hc, int wc,
+                                  const float* __restrict__ wx, int wo, size_t count, float* __restrict__ tmp) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += (size_t)gridDim.x * blockDim.x) {
+    const int ox = (int)(i % wo);
+    const int iy = (int)((i / wo) % hc);
+    const size_t p = i / ((size_t)wo * hc);
+    const float* row = pat + (p * h + (size_t)(y0 + iy)) * w + x0;
+    const float* wr = wx + (size_t)ox * wc;
+    float acc = 0.f;
+    for (int ix = 0; ix < wc; ++ix) acc = fmaf(wr[ix], row[ix], acc);
+    tmp[i] = acc;
+  }
+}
+
+static __global__ void k_resize_y(const float* __restrict__ tmp, int hc, int wo, const float* __restrict__ wy, int ho,
+                                  size_t count, float* __restrict__ out) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += (size_t)gridDim.x * blockDim.x) {
+    const int ox = (int)(i % wo);
+    const int oy = (int)((i / wo) % ho);
+    const size_t p = i / ((size_t)wo * ho);
+    const float* col = tmp + p * hc * wo + ox;
+    const float* wr = wy + (size_t)oy * hc;
+    float acc = 0.f;
+    for (int iy = 0; iy < hc; ++iy) acc = fmaf(wr[iy], col[(size_t)iy * wo], acc);
+    out[i] = acc;
+  }
+}
+
+}  // namespace ptyro
+
+extern "C" {
+
+size_t ptyro_clip_resize_workspace_bytes(int64_t num_patterns, int32_t hc, int32_t wo) {
+  if (num_patterns < 0 || hc <= 0 || wo <= 0) return 0;
+  return align_up(4 * (size_t)(num_patterns > 0 ? num_patterns : 1) * hc * wo);
+}
+
+int ptyro_clip_resize(const float* patterns, int64_t num_patterns, int32_t h, int32_t w, int32_t y0, int32_t x0,
+                      int32_t hc, int32_t wc, const float* wy, int32_t ho, const float* wx, int32_t wo, float* out,
+                      void* workspace, size_t workspace_bytes, void* stream) {
+  if (num_patterns < 0 || h <= 0 || w <= 0 || hc <= 0 || wc <= 0 || ho <= 0 || wo <= 0)
+    return fail(PTYRO_ERR_INVALID, "clip resize: sizes must be positive");
+  if (y0 < 0 || x0 < 0 || y0 + hc > h || x0 + wc > w)
+    return fail(PTYRO_ERR_INVALID, "clip resize: the crop must lie inside the pattern");
+  if (num_patterns == 0) return PTYRO_OK;
+  if (!patterns || !wy || !wx || !out) return fail(PTYRO_ERR_INVALID, "NULL array argument");
+  const size_t need = ptyro_clip_resize_workspace_bytes(num_patterns, hc, wo);
+  if (!workspace || workspace_bytes < need)
+    return fail(PTYRO_ERR_WORKSPACE, "clip resize: workspace too small: need " + std::to_string(need));
+  cudaStream_t st = (cudaStream_t)stream;
+  float* tmp = (float*)workspace;
+  const size_t c1 = (size_t)num_patterns * hc * wo, c2 = (size_t)num_patterns * ho * wo;
+  k_resize_x<<<blocks_for(c1, 256), 256, 0, st>>>(patterns, h, w, y0, x0, hc, wc, wx, wo, c1, tmp);
+  k_resize_y<<<blocks_for(c2, 256), 256, 0, st>>>(tmp, hc, wo, wy, ho, c2, out);
+  return check_launch("clip resize", 2);
+}
+
+}  // extern "C"

@@ -173,3 +173,92 @@ def stem_4d_annular(pot_slice: PotentialSlices, beam: ProbeModes, microscope: Mi
         raise ValueError("detector.scan_shape is required")
     vals = stem_4d_detectors(pot_slice, beam, microscope, detector)
     return _image(vals[:, 0], detector, detector.real_space_calib_ang)
+
+
+# ----------------------------------------------------------------------------- CBED clip + resize
+def linear_resize_weights(input_size: int, output_size: int, antialias: bool = True) -> np.ndarray:
+    """(output_size, input_size) weights of a linear (triangle-kernel) resize with
+    half-pixel centres, widened by the downscale factor when antialiasing, each
+    output row normalised to unit sum and zero where the sample falls outside the
+    input: the scale-and-translate weights of jax.image.resize(method="linear")
+    (jax 0.9.2, jax/_src/image/scale.py), restated."""
+    scale = output_size / input_size
+    inv_scale = 1.0 / scale
+    kernel_scale = max(inv_scale, 1.0) if antialias else 1.0
+    sample_f = (np.arange(output_size) + 0.5) * inv_scale - 0.5
+    x = np.abs(sample_f[None, :] - np.arange(input_size, dtype=np.float64)[:, None]) / kernel_scale
+    weights = np.maximum(0.0, 1.0 - x)
+    total = np.sum(weights, axis=0, keepdims=True)
+    weights = np.where(np.abs(total) > 1000.0 * float(np.finfo(np.float32).eps),
+                       weights / np.where(total != 0, total, 1), 0.0)
+    inside = (sample_f >= -0.5) & (sample_f <= input_size - 0.5)
+    return np.where(inside[None, :], weights, 0.0).T
+
+
+def _crop_bounds(h: int, w: int, fourier_calib_inv_ang: float, voltage_kv: float, extent_mrad: float) -> tuple:
+    mrad_per_inv_ang = relativistic_wavelength_ang(voltage_kv) * 1000.0
+    extent_pixels = int(np.ceil((float(extent_mrad) / mrad_per_inv_ang) / float(fourier_calib_inv_ang)))
+    cy, cx = h // 2, w // 2
+    y0, y1 = max(0, cy - extent_pixels), min(h, cy + extent_pixels)
+    x0, x1 = max(0, cx - extent_pixels), min(w, cx + extent_pixels)
+    return y0, y1, x0, x1
+
+
+def clip_cbed(cbed: torch.Tensor, fourier_calib_inv_ang: float, voltage_kv: float, extent_mrad: float,
+              output_shape: Tuple[int, int]) -> torch.Tensor:
+    """Central crop of ``extent_mrad`` (half angle) and linear resize to
+    ``output_shape`` (plots/figuring.py:37-117) of one (H, W) pattern or a (P, H, W)
+    stack, float32 on the device."""
+    dev = _device(cbed.device if cbed.is_cuda else None)
+    pats = as_tensor(cbed, torch.float32, dev)
+    single = pats.ndim == 2
+    if single:
+        pats = pats[None]
+    if pats.ndim != 3:
+        raise ValueError("cbed must be (H, W) or (P, H, W)")
+    pats = pats.contiguous()
+    p, h, w = pats.shape
+    ho, wo = (int(v) for v in output_shape)
+    y0, y1, x0, x1 = _crop_bounds(h, w, fourier_calib_inv_ang, voltage_kv, extent_mrad)
+    hc, wc = y1 - y0, x1 - x0
+    if hc <= 0 or wc <= 0:
+        raise ValueError("extent_mrad selects no pixels")
+    wy = linear_resize_weights(hc, ho) if ho != hc else np.eye(hc)
+    wx = linear_resize_weights(wc, wo) if wo != wc else np.eye(wc)
+    wy_d = torch.as_tensor(wy.astype(np.float32), device=dev).contiguous()
+    wx_d = torch.as_tensor(wx.astype(np.float32), device=dev).contiguous()
+    out = torch.empty((p, ho, wo), dtype=torch.float32, device=dev)
+    lib = _lib.load()
+    nbytes = lib.ptyro_clip_resize_workspace_bytes(p, hc, wo)
+    ws = _workspace(nbytes, dev)
+    _lib.check(lib.ptyro_clip_resize(pats.data_ptr(), p, h, w, y0, x0, hc, wc, wy_d.data_ptr(), ho, wx_d.data_ptr(),
+                                     wo, out.data_ptr(), ws.data_ptr(), nbytes, _stream_ptr(dev)))
+    return out[0] if single else out
+
+
+def stem_4d_clipped(pot_slice: PotentialSlices, beam: ProbeModes, microscope: MicroscopeConfig,
+                    detector: DetectorConfig, cbed_extent_mrad: float, cbed_shape: Tuple[int, int],
+                    chunk: int = 1024) -> STEM4D:
+    """4D-STEM with every pattern clipped to ``cbed_extent_mrad`` and resized to
+    ``cbed_shape``, as the reference's 4D-STEM workflow stores them
+    (workflows/stem_4d.py:488-540): the forward runs ``chunk`` probes at a time so the
+    full-size patterns of only one chunk exist in device memory. The output Fourier
+    calibration is ``2 extent / cbed_shape[0]`` mrad per pixel, in 1/Angstrom."""
+    from .simulations import stem_4d
+    from .types import create_detector_config, create_stem4d
+    if detector.scan_positions_px is None:
+        raise ValueError("detector.scan_positions_px is required")
+    pos = detector.scan_positions_px
+    parts = []
+    s4 = None
+    for c0 in range(0, pos.shape[0], int(chunk)):
+        sub = create_detector_config(detector.real_space_calib_ang, detector.probe_calibration_pm,
+                                     detector.collection_inner_mrad, detector.collection_outer_mrad,
+                                     scan_positions_px=pos[c0:c0 + int(chunk)])
+        s4 = stem_4d(pot_slice, beam, microscope, sub)
+        parts.append(clip_cbed(s4.data, s4.fourier_space_calib, microscope.voltage_kv, cbed_extent_mrad, cbed_shape))
+    data = torch.cat(parts, dim=0)
+    mrad_per_inv_ang = relativistic_wavelength_ang(microscope.voltage_kv) * 1000.0
+    fourier = (2.0 * float(cbed_extent_mrad) / int(cbed_shape[0])) / mrad_per_inv_ang
+    return create_stem4d(data, detector.real_space_calib_ang, fourier,
+                         pos.to(torch.float64) * detector.real_space_calib_ang, microscope.voltage_kv)

@@ -105,3 +105,32 @@ def test_detector_argument_errors():
         pb.virtual_detectors(s4, [(0.0, 1.0)] * 33)
     with pytest.raises(ValueError, match="inner <= outer"):
         pb.virtual_detectors(s4, [(2.0, 1.0)])
+
+
+@pytest.mark.parametrize("shape,extent,out", [((128, 128), 30.0, (64, 64)), ((256, 256), 45.0, (100, 80)),
+                                              ((64, 64), 10.0, (48, 48)), ((128, 128), 500.0, (128, 128))])
+def test_clip_cbed_matches_oracle(shape, extent, out):
+    rng = np.random.default_rng(shape[0] + int(extent))
+    pats = rng.uniform(0, 1, (5,) + shape)
+    fc = 1.0 / (shape[0] * 0.2)
+    got = pb.clip_cbed(torch.as_tensor(pats, dtype=torch.float32, device="cuda"), fc, 200.0, extent, out)
+    want = np.stack([R.clip_cbed(p, fc, 200.0, extent, out) for p in pats])
+    assert got.shape == want.shape
+    assert rel_l2(got.cpu().numpy(), want) < 1e-6
+    one = pb.clip_cbed(torch.as_tensor(pats[0], dtype=torch.float32, device="cuda"), fc, 200.0, extent, out)
+    assert torch.allclose(one, got[0])
+
+
+def test_stem_4d_clipped_matches_clipped_stem_4d():
+    n, S, P, calib, kv = 128, 3, 9, 0.2, 200.0
+    pot, modes, w, pos = _case(n, S, 1, P, 5)
+    pots = pb.create_potential_slices(pot, 1.5, calib)
+    beam = pb.create_probe_modes(modes, w, calib)
+    mic = pb.create_microscope_config(kv, 25.0, probe_shape=(n, n))
+    det = pb.create_detector_config(calib, scan_positions_px=pos)
+    full = pb.stem_4d(pots, beam, mic, det)
+    clipped = pb.stem_4d_clipped(pots, beam, mic, det, 40.0, (64, 64), chunk=4)
+    want = pb.clip_cbed(full.data, full.fourier_space_calib, kv, 40.0, (64, 64))
+    assert torch.equal(clipped.data, want)
+    lam = R.relativistic_wavelength_ang(kv)
+    assert abs(clipped.fourier_space_calib - (80.0 / 64) / (lam * 1000.0)) < 1e-15

@@ -225,3 +225,19 @@ def test_ensemble_axis_validation():
     assert [a.axis_id for a in axes] == ["probe_modes", "position_jitter"]
     with pytest.raises(ValueError, match="multimode probes require a first probe_modes axis"):
         _axis_maps((jit,), 2)
+
+
+def test_oracle_resize_weights_properties():
+    """Upscaling by 2 interpolates at quarter offsets; downscaling by 2 widens the
+    triangle to four taps (antialias), renormalised at the edges; rows sum to one."""
+    w = R.resize_linear_weights(4, 8)
+    assert np.allclose(w.sum(axis=0), 1.0)
+    x = np.arange(4.0)
+    assert np.allclose((w.T @ x)[1:-1], [0.25, 0.75, 1.25, 1.75, 2.25, 2.75])
+    d = R.resize_linear_weights(8, 4)
+    assert np.allclose(d.sum(axis=0), 1.0)
+    assert np.allclose(d[:, 1], [0.0, 0.125, 0.375, 0.375, 0.125, 0.0, 0.0, 0.0])  # interior taps
+    assert np.allclose(d.T @ np.arange(8.0), [5 / 7, 2.5, 4.5, 44 / 7])  # edges renormalised
+    from ptyrodactyl_b200.detectors import linear_resize_weights
+    for a, b in [(4, 8), (8, 4), (100, 37), (37, 64), (64, 64)]:
+        assert np.allclose(linear_resize_weights(a, b), R.resize_linear_weights(a, b).T)
