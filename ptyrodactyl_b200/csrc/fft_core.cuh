@@ -112,8 +112,12 @@ __host__ __device__ constexpr int bitrev(int i, int bits) {
   return bits == 0 ? 0 : (((i & 1) << (bits - 1)) | bitrev(i >> 1, bits - 1));
 }
 
-// u +- b W_64^k for paired values; the exact twiddles become additions of the
-// swapped parts, as the scalar path's twmul64 + cadd/csub round them.
+// Butterflies u +- b W_64^k. The exact twiddles (k = 0, 16, 32, 48) become additions
+// of the swapped parts. Every other twiddle w = (c, s) is factored as
+// c (1 + i s/c) when |c| >= |s| and s (c/s + i) otherwise, so b w costs two fmas
+// and the two outputs u +- (scale) q two more each: six fused operations instead of
+// a complex multiply and two complex additions (eight). The scalar and the paired
+// versions perform the same operations, so they round identically.
 template <int DIR>
 __device__ __forceinline__ void bfly(Pair& u, Pair& b, int k) {
   k &= 63;
@@ -129,16 +133,45 @@ __device__ __forceinline__ void bfly(Pair& u, Pair& b, int k) {
     o1 = {sub2(u.re, b.im), __fadd2_rn(u.im, b.re)};
     o2 = {__fadd2_rn(u.re, b.im), sub2(u.im, b.re)};
   } else {
-    const Pair w = cmul(b, w64<DIR>(k));
-    o1 = cadd(u, w); o2 = csub(u, w);
+    const float2 w = w64<DIR>(k);
+    if (fabsf(w.x) >= fabsf(w.y)) {  // b w = c (b.re - t b.im, b.im + t b.re)
+      const float t = w.y / w.x, c = w.x;
+      const Pair q = {__ffma2_rn(dup2(-t), b.im, b.re), __ffma2_rn(dup2(t), b.re, b.im)};
+      o1 = {__ffma2_rn(dup2(c), q.re, u.re), __ffma2_rn(dup2(c), q.im, u.im)};
+      o2 = {__ffma2_rn(dup2(-c), q.re, u.re), __ffma2_rn(dup2(-c), q.im, u.im)};
+    } else {  // b w = s (t b.re - b.im, t b.im + b.re), real part kept negated
+      const float t = w.x / w.y, sn = w.y;
+      const Pair q = {__ffma2_rn(dup2(-t), b.re, b.im), __ffma2_rn(dup2(t), b.im, b.re)};
+      o1 = {__ffma2_rn(dup2(-sn), q.re, u.re), __ffma2_rn(dup2(sn), q.im, u.im)};
+      o2 = {__ffma2_rn(dup2(sn), q.re, u.re), __ffma2_rn(dup2(-sn), q.im, u.im)};
+    }
   }
   u = o1;
   b = o2;
 }
 template <int DIR>
 __device__ __forceinline__ void bfly(float2& u, float2& b, int k) {
-  const float2 w = twmul64<DIR>(b, k);
-  const float2 o1 = cadd(u, w), o2 = csub(u, w);
+  k &= 63;
+  if (k == 0 || k == 16 || k == 32 || k == 48) {
+    const float2 w = twmul64<DIR>(b, k);
+    const float2 o1 = cadd(u, w), o2 = csub(u, w);
+    u = o1;
+    b = o2;
+    return;
+  }
+  const float2 w = w64<DIR>(k);
+  float2 o1, o2;
+  if (fabsf(w.x) >= fabsf(w.y)) {
+    const float t = w.y / w.x, c = w.x;
+    const float2 q = make_float2(fmaf(-t, b.y, b.x), fmaf(t, b.x, b.y));
+    o1 = make_float2(fmaf(c, q.x, u.x), fmaf(c, q.y, u.y));
+    o2 = make_float2(fmaf(-c, q.x, u.x), fmaf(-c, q.y, u.y));
+  } else {
+    const float t = w.x / w.y, sn = w.y;
+    const float2 q = make_float2(fmaf(-t, b.x, b.y), fmaf(t, b.y, b.x));
+    o1 = make_float2(fmaf(-sn, q.x, u.x), fmaf(sn, q.y, u.y));
+    o2 = make_float2(fmaf(sn, q.x, u.x), fmaf(-sn, q.y, u.y));
+  }
   u = o1;
   b = o2;
 }
