@@ -1,0 +1,190 @@
+// Steady-state pass for lines of N = N1 * 2 N1 points (512 = 16 x 32) with the two
+// halves of each thread's work paired in f32x2 arithmetic.
+//
+// A thread owns 2 N1 points of one line. Two lines per thread (ms_pair.cuh) would
+// not fit in registers here, so the pairing is inside the line:
+//   natural order:   Pair j = (x[t + N1 j], x[t + N1 (j + N1)]),  j < N1
+//   in-thread DFT:   decimation in frequency, a_j = x_j + x_{j+N1},
+//                    b_j = (x_j - x_{j+N1}) W_{2 N1}^j, then one paired N1-point DFT
+//                    gives (X[2k], X[2k+1]) in Pair k
+//   exchange:        as the one-line kernel; the k-order groups g = 0, 1 of the
+//                    second stage form the Pairs, so the N1-point group DFTs pair too
+//   inverse:         the mirror image (paired group DFTs, exchange, paired N1-point
+//                    DFT of (even, odd) inputs, decimation-in-time final stage), which
+//                    returns each value to the thread and the pairing it came from.
+// Every step that treats the pair halves alike runs as paired instructions; only
+// the two radix-2 stages that join the halves run scalar.
+#pragma once
+#include "ms_pass.cuh"
+
+namespace ptyro {
+
+template <int N1, int N2>
+struct HalfLine {
+  static_assert(N2 == 2 * N1, "the half-paired line needs N2 == 2 N1");
+  static constexpr int N = N1 * N2;
+  static constexpr int H = N1;  // Pairs per thread
+};
+
+// forward, natural (j, j + H) pairs -> k-order Pairs (g = 0, g = 1 of k1); DIR = -1
+template <int N1, int N2, int DIR>
+__device__ __forceinline__ void half_nat_to_k(Pair (&p)[N1], int t, float2* buf, const float2* tw) {
+  using LB = LineBuf<N1, N2>;
+  constexpr int H = N1;
+  // decimation in frequency: a_j = x_j + x_{j+H}, b_j = (x_j - x_{j+H}) W_{2H}^j
+#pragma unroll
+  for (int j = 0; j < H; ++j) {
+    const float2 xa = pair_a(p[j]), xb = pair_b(p[j]);
+    const float2 a = cadd(xa, xb);
+    const float2 b = twmul64<DIR>(csub(xa, xb), j * (64 / (2 * H)));
+    p[j] = make_pair(a, b);
+  }
+  dft<H, DIR, 1, 0, H>(p);  // Pair k = (X[2k], X[2k+1])
+  // twiddles W_N^{t k2}, k2 = 2k and 2k + 1
+  if (t != 0) {
+#pragma unroll
+    for (int k = 0; k < H; ++k) {
+      const float2 wa = tw[(2 * k) * N1 + t], wb = tw[(2 * k + 1) * N1 + t];
+      p[k] = DIR < 0 ? cmul(p[k], wa, wb) : cmul(p[k], cconj(wa), cconj(wb));
+    }
+  }
+  __syncwarp();
+#pragma unroll
+  for (int k = 0; k < H; ++k) {
+    buf[LB::at(2 * k, t)] = pair_a(p[k]);
+    buf[LB::at(2 * k + 1, t)] = pair_b(p[k]);
+  }
+  __syncwarp();
+#pragma unroll
+  for (int n1 = 0; n1 < N1; ++n1) p[n1] = make_pair(buf[LB::at(t, n1)], buf[LB::at(t + N1, n1)]);
+  dft<N1, DIR, 1, 0, N1>(p);  // Pair k1 = (r = k1, r = N1 + k1) of the k-order layout
+}
+
+// inverse, k-order Pairs -> natural (j, j + H) pairs; DIR = +1
+template <int N1, int N2, int DIR>
+__device__ __forceinline__ void half_k_to_nat(Pair (&p)[N1], int t, float2* buf, const float2* tw) {
+  using LB = LineBuf<N1, N2>;
+  constexpr int H = N1;
+  dft<N1, DIR, 1, 0, N1>(p);
+  __syncwarp();
+#pragma unroll
+  for (int n1 = 0; n1 < N1; ++n1) {
+    buf[LB::at(t, n1)] = pair_a(p[n1]);
+    buf[LB::at(t + N1, n1)] = pair_b(p[n1]);
+  }
+  __syncwarp();
+#pragma unroll
+  for (int m = 0; m < H; ++m) p[m] = make_pair(buf[LB::at(2 * m, t)], buf[LB::at(2 * m + 1, t)]);
+  if (t != 0) {
+#pragma unroll
+    for (int m = 0; m < H; ++m) {
+      const float2 wa = tw[(2 * m) * N1 + t], wb = tw[(2 * m + 1) * N1 + t];
+      p[m] = DIR < 0 ? cmul(p[m], wa, wb) : cmul(p[m], cconj(wa), cconj(wb));
+    }
+  }
+  dft<H, DIR, 1, 0, H>(p);  // Pair j = (E_j, O_j): transforms of the even and odd inputs
+  // decimation in time: x_j = E_j + W_{2H}^j O_j, x_{j+H} = E_j - W_{2H}^j O_j
+#pragma unroll
+  for (int j = 0; j < H; ++j) {
+    float2 e = pair_a(p[j]), o = pair_b(p[j]);
+    bfly<DIR>(e, o, j * (64 / (2 * H)));
+    p[j] = make_pair(e, o);
+  }
+}
+
+template <int N1, int N2, int AXIS, int WARPS, int MINB>
+__global__ void __launch_bounds__(WARPS * 32, MINB) ms_pass_half_kernel(PassArgs a) {
+  using Geo = PassGeom<N1, N2>;
+  using LB = LineBuf<N1, N2>;
+  constexpr int N = Geo::N, G = Geo::G, H = N1;
+  constexpr int lines = WARPS * G;
+  static_assert(N % lines == 0, "lines per CTA must divide N");
+  constexpr int pitch = lines + G;
+  extern __shared__ float2 smem[];
+  float2* tw = smem;
+  float2* pfs = smem + N;
+  float2* work = smem + 2 * N;
+  for (int i = threadIdx.x; i < N; i += blockDim.x) {
+    const int k2 = i / N1, tt = i % N1;
+    tw[i] = a.tw[(tt * k2) % N];
+    pfs[i] = a.pf[i];
+  }
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int t = AXIS == 0 ? (lane % N1) : (lane / G);
+  const int gl = AXIS == 0 ? (lane / N1) : (lane % G);
+  const int lc = warp * G + gl;
+  const int line0 = blockIdx.x * lines;
+  const int line = line0 + lc;
+  const int slot = blockIdx.y;
+  float2* buf = work + lc * LB::kSize;
+  float2* w = a.wave + (size_t)slot * N * N;
+  auto off = [&](int e) -> size_t { return AXIS == 0 ? (size_t)line * N + e : (size_t)e * N + line; };
+  Pair p[H];
+
+  // ---- load: Pair j = elements t + N1 j and t + N1 (j + H)
+  if (AXIS == 0) {
+#pragma unroll
+    for (int j = 0; j < H; ++j) p[j] = make_pair(w[off(t + N1 * j)], w[off(t + N1 * (j + H))]);
+  } else {
+    tile_load<N, lines, pitch, WARPS * 32>(w, work, line0);
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < H; ++j)
+      p[j] = make_pair(work[(t + N1 * j) * pitch + lc], work[(t + N1 * (j + H)) * pitch + lc]);
+    __syncthreads();
+  }
+
+  // ---- finish slice s-1's convolution along this axis
+  half_nat_to_k<N1, N2, -1>(p, t, buf, tw);
+#pragma unroll
+  for (int k1 = 0; k1 < N1; ++k1)
+    p[k1] = cmul(p[k1], pfs[korder_index<N1, N2>(t, k1)], pfs[korder_index<N1, N2>(t, N1 + k1)]);
+  half_k_to_nat<N1, N2, +1>(p, t, buf, tw);
+
+  // ---- transmission (and the gradient-mode checkpoint)
+  {
+    int eoff;
+    const float2* T = trans_row<AXIS>(a.trans, a.trans_t, a.field_n, a.t_slice, a.win, slot / a.n_modes, line,
+                                      &eoff);
+    const int fm = a.field_n - 1;
+#pragma unroll
+    for (int j = 0; j < H; ++j)
+      p[j] = cmul(p[j], __ldg(T + ((t + N1 * j + eoff) & fm)), __ldg(T + ((t + N1 * (j + H) + eoff) & fm)));
+    if (a.ckpt_store) {
+      float2* ck = a.ckpt_store + (size_t)slot * a.res_stride;
+#pragma unroll
+      for (int j = 0; j < H; ++j) {
+        ck[off(t + N1 * j)] = pair_a(p[j]);
+        ck[off(t + N1 * (j + H))] = pair_b(p[j]);
+      }
+    }
+  }
+
+  // ---- start slice s's convolution along this axis
+  half_nat_to_k<N1, N2, -1>(p, t, buf, tw);
+#pragma unroll
+  for (int k1 = 0; k1 < N1; ++k1)
+    p[k1] = cmul(p[k1], pfs[korder_index<N1, N2>(t, k1)], pfs[korder_index<N1, N2>(t, N1 + k1)]);
+  half_k_to_nat<N1, N2, +1>(p, t, buf, tw);
+
+  // ---- store
+  if (AXIS == 0) {
+#pragma unroll
+    for (int j = 0; j < H; ++j) {
+      w[off(t + N1 * j)] = pair_a(p[j]);
+      w[off(t + N1 * (j + H))] = pair_b(p[j]);
+    }
+  } else {
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < H; ++j) {
+      work[(t + N1 * j) * pitch + lc] = pair_a(p[j]);
+      work[(t + N1 * (j + H)) * pitch + lc] = pair_b(p[j]);
+    }
+    __syncthreads();
+    tile_store<N, lines, pitch, WARPS * 32>(w, work, line0);
+  }
+}
+
+}  // namespace ptyro

@@ -5,6 +5,7 @@
 
 #include "ms_bwd.cuh"
 #include "ms_jvp.cuh"
+#include "ms_half.cuh"
 #include "ms_pair.cuh"
 #include "ms_pipe.cuh"
 
@@ -134,6 +135,26 @@ int launch_pair_t(const PassArgs& a, int grid_y, cudaStream_t st, int variant) {
   return launch_pair_w<N1, N2, AXIS, W4, 16 / W4, false>(a, grid_y, st);
 }
 
+// Steady passes with the halves of each line paired (ms_half.cuh), N2 == 2 N1.
+template <int N1, int N2, int AXIS, int MINB>
+int launch_half_t(const PassArgs& a, int grid_y, cudaStream_t st) {
+  using Geo = PassGeom<N1, N2>;
+  constexpr int W = Geo::kWarps;
+  const size_t smem = Geo::smem_bytes(W);
+  static bool attr_done = false;
+  if (!attr_done) {
+    cudaFuncSetAttribute(ms_pass_half_kernel<N1, N2, AXIS, W, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)smem);
+    attr_done = true;
+  }
+  dim3 grid(Geo::N / Geo::kLines, grid_y);
+  ms_pass_half_kernel<N1, N2, AXIS, W, MINB><<<grid, W * 32, smem, st>>>(a);
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  return (int)cudaGetLastError();
+}
+
+// tune bit 8 (value 256): steady passes of N2 == 2 N1 shapes run the half-paired kernel
+// (bit 9, value 512: with one CTA per SM and up to 255 registers).
 // tune bit 4 (value 16): steady passes run the paired two-lines-per-thread kernel.
 // tune bit 2 (value 4) selects the persistent double-buffered kernel for steady
 // passes (measured slower than the one-slot-per-CTA kernel on B200 at 128-512^2)
@@ -142,6 +163,11 @@ int launch_pass_t(const PassArgs& a0, int grid_y, cudaStream_t st, int variant) 
   // tune bit 3 (value 8): column passes access global memory directly (no staging tile)
   PassArgs a = a0;
   if (AXIS == 1 && (variant & 8)) a.direct = 1;
+  if constexpr (N2 == 2 * N1) {
+    if (is_steady_pass(a) && (variant & 256) && a.pf != nullptr)
+      return (variant & 512) ? launch_half_t<N1, N2, AXIS, 1>(a, grid_y, st)
+                             : launch_half_t<N1, N2, AXIS, 2>(a, grid_y, st);
+  }
   if (is_steady_pass(a) && (variant & 16) && a.pf != nullptr)
     return launch_pair_t<N1, N2, AXIS>(a, grid_y, st, variant);
   if (is_steady_pass(a) && a.tw2 != nullptr && (variant & 4)) return launch_pipe_t<N1, N2, AXIS, MINB>(a, grid_y, st);

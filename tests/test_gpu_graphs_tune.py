@@ -109,3 +109,29 @@ def test_paired_steady_kernels_are_bit_identical(n):
         for tune in (19, 51, 211):
             got = run_forward(field, 1.7, modes, wt, pos, 200.0, 0.3, 0.3, tune=tune, windows=win, lanes=1)
             assert torch.equal(got, ref), tune
+
+
+@pytest.mark.parametrize("n", [32, 512])
+def test_half_paired_steady_kernel_matches_oracle(n):
+    """The half-paired steady pass (tune bit 256; decimation in frequency inside the
+    thread) agrees with the oracle and the one-line kernel to float32 rounding."""
+    import numpy as np
+    from oracle import multislice_ref as R
+    from tests.conftest import rel_l2
+    from ptyrodactyl_b200.simulations import run_forward
+    rng = np.random.default_rng(n + 1)
+    s, p = 6, 3
+    pot = rng.uniform(0, 40, (n, n, s))
+    probe = R.make_probe(200.0, 25.0, (n, n), 30.0, defocus_ang=-20.0)
+    dev = torch.device("cuda")
+    slices = torch.as_tensor(pot, dtype=torch.float32, device=dev)
+    modes = torch.as_tensor(probe[..., None].astype(np.complex64), device=dev)
+    wt = torch.ones(1, device=dev)
+    pos = rng.uniform(-2, 2, (p, 2))
+    pos_d = torch.as_tensor(pos, dtype=torch.float64, device=dev)
+    ref = run_forward(slices, 1.7, modes, wt, pos_d, 200.0, 0.3, 0.3, tune=3, lanes=1).cpu().numpy()
+    want = R.stem_4d(pot, 1.7, 0.3, probe[..., None], [1.0], 0.3, 200.0, pos, 0.3, dtype=np.complex128)["data"]
+    for tune in (259, 771):
+        got = run_forward(slices, 1.7, modes, wt, pos_d, 200.0, 0.3, 0.3, tune=tune, lanes=1).cpu().numpy()
+        assert rel_l2(got, want) < 1e-4
+        assert rel_l2(got, ref) < 2e-6
