@@ -203,6 +203,45 @@ def run_forward(slices: torch.Tensor, slice_thickness: float, modes: torch.Tenso
     return out
 
 
+def run_forward_to_host(slices: torch.Tensor, slice_thickness: float, modes: torch.Tensor, weights: torch.Tensor,
+                        positions: torch.Tensor, voltage_kv: float, calib_ang: float, shift_calib_ang: float,
+                        host_out: torch.Tensor, chunks: int = 8, lanes: int = 2, tune: Optional[int] = None,
+                        windows: Optional[torch.Tensor] = None) -> torch.Tensor:
+    """``run_forward`` whose patterns land in a host tensor (pinned for overlap): the
+    probes run as ``chunks`` consecutive ranges on ``lanes`` compute streams, and
+    each range's patterns are copied to the host on a copy stream as soon as the
+    range is done, so the device-to-host transfer overlaps the remaining compute."""
+    dev = slices.device
+    num_probes = positions.shape[0]
+    n, _ = check_windows(slices, modes, windows, num_probes)
+    if tuple(host_out.shape) != (num_probes, n, n) or host_out.dtype != torch.float32:
+        raise ValueError(f"host_out must be a float32 tensor of shape {(num_probes, n, n)}")
+    if num_probes == 0:
+        return host_out
+    dev_out = torch.empty((num_probes, n, n), dtype=torch.float32, device=dev)
+    main = torch.cuda.current_stream(dev)
+    streams = _side_streams(dev, max(1, lanes))
+    copy = _side_streams(dev, 1 + max(1, lanes))[-1]
+    chunks = max(1, min(int(chunks), num_probes))
+    bounds = [num_probes * i // chunks for i in range(chunks + 1)]
+    for st in streams + [copy]:
+        st.wait_stream(main)
+    for i, (lo, hi) in enumerate(zip(bounds[:-1], bounds[1:])):
+        st = streams[i % len(streams)]
+        with torch.cuda.stream(st):
+            run_forward(slices, slice_thickness, modes, weights, positions[lo:hi], voltage_kv, calib_ang,
+                        shift_calib_ang, out=dev_out[lo:hi], tune=tune,
+                        windows=None if windows is None else windows[lo:hi], lanes=1)
+        done = torch.cuda.Event()
+        done.record(st)
+        copy.wait_event(done)
+        with torch.cuda.stream(copy):
+            host_out[lo:hi].copy_(dev_out[lo:hi], non_blocking=True)
+    for st in streams + [copy]:
+        main.wait_stream(st)
+    return host_out
+
+
 def _needs_autodiff(*tensors) -> bool:
     """True when a reverse- or forward-mode derivative will be taken through the
     forward (requires_grad, a torch.func transform's wrapper, or a dual tensor)."""
@@ -223,14 +262,16 @@ def _beam_on(beam: ProbeModes, dev) -> tuple:
 
 
 def stem_4d(pot_slice: PotentialSlices, beam: ProbeModes, microscope: MicroscopeConfig,
-            detector: DetectorConfig) -> STEM4D:
+            detector: DetectorConfig, *, out: Optional[torch.Tensor] = None) -> STEM4D:
     """4D-STEM patterns at every scan position (simulations.py:1330-1443).
 
     ``detector.scan_positions_px`` is used exactly as the reference uses it: passed
     unchanged as the shift of ``shift_beam_fourier``, whose frequency grid is in
     1/Angstrom, so each value acts as Angstrom; the returned ``scan_positions``
     field is ``positions * real_space_calib_ang`` as in the reference. ``data`` is a
-    float32 CUDA tensor (P, H, W).
+    float32 CUDA tensor (P, H, W), or ``out`` when given: a CUDA tensor is written in
+    place; a host tensor (pinned) receives the patterns chunk by chunk while the
+    remaining probes compute.
     """
     if detector.scan_positions_px is None:
         raise ValueError("detector.scan_positions_px is required")
@@ -253,9 +294,15 @@ def stem_4d(pot_slice: PotentialSlices, beam: ProbeModes, microscope: Microscope
         from .autodiff import stem_4d_patterns
         data = stem_4d_patterns(slices, modes, weights, positions, pot_slice.slice_thickness,
                                 microscope.voltage_kv, calib, detector.real_space_calib_ang)
+    elif out is not None and not out.is_cuda:
+        data = run_forward_to_host(slices, pot_slice.slice_thickness, modes, weights, positions,
+                                   microscope.voltage_kv, calib, detector.real_space_calib_ang, out)
     else:
         data = run_forward(slices, pot_slice.slice_thickness, modes, weights, positions,
-                           microscope.voltage_kv, calib, detector.real_space_calib_ang)
+                           microscope.voltage_kv, calib, detector.real_space_calib_ang, out=out)
+    if out is not None and data is not out:
+        out.copy_(data)
+        data = out
     fourier_calib = 1.0 / (modes.shape[0] * calib)
     scan_positions = detector.scan_positions_px.to(torch.float64) * detector.real_space_calib_ang
     return create_stem4d(data, detector.real_space_calib_ang, fourier_calib, scan_positions,

@@ -208,3 +208,23 @@ def test_slices_from_atoms_match_oracle():
     want = np.stack([R.slice_potential_from_atoms(atoms, types, b[0], b[1], kern, (n, n), calib, mask)
                      for b in bounds], axis=-1)
     assert rel_l2(got, want) < 1e-5
+
+
+def test_stem_4d_streams_patterns_to_host():
+    """out= a pinned host tensor: chunked compute with overlapped copies gives the
+    device result exactly."""
+    rng = np.random.default_rng(4)
+    n, s, p = 64, 4, 37
+    pot = rng.uniform(0, 30, (n, n, s))
+    probe = R.make_probe(200.0, 25.0, (n, n), 20.0)
+    pots = pb.create_potential_slices(torch.as_tensor(pot, dtype=torch.float32), 1.5, 0.2)
+    beam = pb.create_probe_modes(probe[..., None], [1.0], 0.2)
+    mic = pb.create_microscope_config(200.0, 25.0, probe_shape=(n, n))
+    det = pb.create_detector_config(0.2, scan_positions_px=rng.uniform(-2, 2, (p, 2)))
+    ref = pb.stem_4d(pots, beam, mic, det).data.cpu()
+    host = torch.empty((p, n, n), dtype=torch.float32).pin_memory()
+    s4 = pb.stem_4d(pots, beam, mic, det, out=host)
+    torch.cuda.synchronize()
+    assert s4.data is host and torch.equal(host, ref)
+    dev_out = torch.empty((p, n, n), dtype=torch.float32, device="cuda")
+    assert torch.equal(pb.stem_4d(pots, beam, mic, det, out=dev_out).data.cpu(), ref)
