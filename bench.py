@@ -483,6 +483,9 @@ def run_grad(args, rank, world, local_rank):
         _lib.check(lib.ptyro_ms_backward(ctypes.byref(bprm), k, model.data_ptr(), wts.data_ptr(), pos.data_ptr(),
                                          res.data_ptr(), gbuf["g"].data_ptr(), g_field.data_ptr(),
                                          g_modes.data_ptr(), bws.data_ptr(), bws_b, st))
+        if world > 1:  # each rank holds its probes' share of dL/dV: one NCCL all-reduce sums them
+            import torch.distributed as dist
+            dist.all_reduce(g_field)
 
     def timed(fn, reps):
         ts = []
@@ -504,7 +507,12 @@ def run_grad(args, rank, world, local_rank):
     t_fc = timed(fwd_ckpt, reps)
     loss_grad()
     t_b = timed(bwd, reps)
-    updates = float(P) * S
+    if world > 1:  # whole-job times: the slowest rank
+        import torch.distributed as dist
+        tt = torch.tensor([t_f, t_fc, t_b], dtype=torch.float64, device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_f, t_fc, t_b = (float(v) for v in tt.tolist())
+    updates = float(P) * S * world
     line = {
         "metric": "ptychographic gradient: value+grad probe-slice updates/s (256^2 windows, 512^2 field)",
         "value": updates / ((t_fc + t_b) * 1e-3), "unit": UNIT, "n_gpus": world, "mode": "grad",

@@ -59,3 +59,55 @@ def value_and_grad(field: torch.Tensor, aberrations: Dict[str, torch.Tensor], ta
     value.backward()
     grads = {k: v.grad.detach() for k, v in ab.items()}
     return value.detach(), field.grad.detach(), grads
+
+
+def sharded_value_and_grad(field: torch.Tensor, aberrations: Dict[str, torch.Tensor], targets: torch.Tensor,
+                           windows: Optional[torch.Tensor], positions: torch.Tensor, *, group=None,
+                           local_fn=None, **kwargs):
+    """value_and_grad over scan positions sharded across the ranks of a
+    torch.distributed process group (one process per GPU, NCCL over NVLink): each
+    rank passes its own probes (positions, targets, windows), runs the forward and
+    the adjoint kernels on them, and one all-reduce per quantity sums the loss, the
+    potential gradient and the aberration gradients — the only exchange of the
+    sharded path (the reference shards positions the same way,
+    multislice/parallelized.py:512-521). Mean-type losses are weighted by each
+    rank's share of the patterns before the sum. ``local_fn`` replaces the local
+    computation (tests)."""
+    import torch.distributed as dist
+    fn = value_and_grad if local_fn is None else local_fn
+    value, g_field, g_ab = fn(field, aberrations, targets, windows, positions, **kwargs)
+    if not dist.is_available() or not dist.is_initialized():
+        return value, g_field, g_ab
+    world = dist.get_world_size(group)
+    loss = kwargs.get("loss", "amplitude")
+    if loss in ("mae", "mse", "rmse") and world > 1:
+        count = torch.tensor([float(targets.numel())], dtype=torch.float64, device=g_field.device)
+        total = count.clone()
+        dist.all_reduce(total, group=group)
+        share = float(count.item() / total.item())
+        if loss == "rmse":  # combine mean squares, then the root: d sqrt(m)/dm = 1 / (2 sqrt(m))
+            ms = value.to(torch.float64) ** 2 * share
+            g_scale = share * value.to(torch.float64)  # dL_r/dx = dms_r/dx / (2 L_r); rescaled below
+            buf = ms.reshape(1).to(g_field.device)
+            dist.all_reduce(buf, group=group)
+            root = torch.sqrt(buf)[0]
+            scale = (g_scale / root).to(g_field.dtype)
+            value = root.to(value.dtype)
+            g_field = g_field * scale
+            g_ab = {k: v * scale.to(v.dtype) for k, v in g_ab.items()}
+        else:
+            value = value * share
+            g_field = g_field * share
+            g_ab = {k: v * share for k, v in g_ab.items()}
+    if loss != "rmse" or world == 1:
+        v = value.reshape(1).to(g_field.device).clone()
+        dist.all_reduce(v, group=group)
+        value = v[0]
+    g_field = g_field.contiguous()
+    dist.all_reduce(g_field, group=group)
+    names = sorted(g_ab)
+    if names:
+        flat = torch.stack([g_ab[k].reshape(()).to(torch.float64) for k in names]).to(g_field.device)
+        dist.all_reduce(flat, group=group)
+        g_ab = {k: flat[i] for i, k in enumerate(names)}
+    return value, g_field, g_ab
