@@ -12,7 +12,7 @@
 // of a line through the forward's schedule in lockstep (the same passes, the same
 // transforms) and couples them only at the slice point.
 #pragma once
-#include "ms_pass.cuh"
+#include "ms_bwd.cuh"
 
 namespace ptyro {
 
@@ -54,32 +54,9 @@ __device__ __forceinline__ const T* field_row(const T* rowmaj, const T* colmaj, 
   return P + (size_t)((line + (AXIS == 0 ? wy : wx)) & (field_n - 1)) * field_n;
 }
 
-template <int N1, int N2, int AXIS>
-__device__ __forceinline__ void jvp_read(const float2* w, float2 (&v)[N2], bool korder, int t, int line, int lc,
-                                         const float2* work, int pitch) {
-  constexpr int N = N1 * N2;
-  if (AXIS == 0) {
-    if (korder) {
-#pragma unroll
-      for (int r = 0; r < N2; ++r) v[r] = w[(size_t)line * N + korder_index<N1, N2>(t, r)];
-    } else {
-#pragma unroll
-      for (int j = 0; j < N2; ++j) v[j] = w[(size_t)line * N + t + N1 * j];
-    }
-  } else {
-    if (korder) {
-#pragma unroll
-      for (int r = 0; r < N2; ++r) v[r] = work[korder_index<N1, N2>(t, r) * pitch + lc];
-    } else {
-#pragma unroll
-      for (int j = 0; j < N2; ++j) v[j] = work[(t + N1 * j) * pitch + lc];
-    }
-  }
-}
-
-template <int N1, int N2>
-__device__ __forceinline__ bool jvp_op(int op, float2 (&v)[N2], int t, float2* buf, const float2* tw,
-                                       const float2* pf, float scale) {
+template <int N1, int N2, typename T>
+__device__ __forceinline__ bool jvp_op(int op, T (&v)[N2], int t, T* buf, const float2* tw, const float2* pf,
+                                       float scale) {
   if (op == OP_IFFT) {
     line_k_to_nat<N1, N2, +1>(v, t, buf, tw);
 #pragma unroll
@@ -92,7 +69,6 @@ __device__ __forceinline__ bool jvp_op(int op, float2 (&v)[N2], int t, float2* b
 template <int N1, int N2, int AXIS, int WARPS>
 __device__ __forceinline__ void jvp_body(const JvpArgs& a, const int yslot) {
   using Geo = PassGeom<N1, N2>;
-  using LB = LineBuf<N1, N2>;
   constexpr int N = Geo::N;
   constexpr int G = Geo::G;
   constexpr int lines = WARPS * G;
@@ -113,7 +89,8 @@ __device__ __forceinline__ void jvp_body(const JvpArgs& a, const int yslot) {
   const int lc = warp * G + gl;
   const int line0 = blockIdx.x * lines;
   const int line = line0 + lc;
-  float2* buf = work + lc * LB::kSize;
+  // the wave and its tangent ride as one Pair per element (half 0, half 1)
+  Pair* buf = reinterpret_cast<Pair*>(work) + lc * PairBuf<N1, N2>::kSize;
   const size_t NN = (size_t)N * N;
   auto off = [&](int e) -> size_t { return AXIS == 0 ? (size_t)line * N + e : (size_t)e * N + line; };
   const bool to_pattern = a.dst == DST_PATTERN;
@@ -127,7 +104,7 @@ __device__ __forceinline__ void jvp_body(const JvpArgs& a, const int yslot) {
     const int b = slot / a.n_modes;
     float2* Wp = a.psi + (size_t)slot * NN;
     float2* Wd = a.dpsi + (size_t)slot * NN;
-    float2 v[N2], u[N2];
+    Pair q[N2];
     const bool korder_in = a.src == SRC_PROBE || a.op1 == OP_IFFT;
     // ---- load both waves
     if (a.src == SRC_PROBE) {
@@ -140,29 +117,25 @@ __device__ __forceinline__ void jvp_body(const JvpArgs& a, const int yslot) {
       for (int r = 0; r < N2; ++r) {
         const int k = korder_index<N1, N2>(t, r);
         const float2 f = cmul(ra[k], rl);
-        v[r] = cmul(pk[off(k)], f);
-        u[r] = dk ? cmul(dk[off(k)], f) : make_float2(0.f, 0.f);
+        q[r] = make_pair(cmul(pk[off(k)], f), dk ? cmul(dk[off(k)], f) : make_float2(0.f, 0.f));
       }
     } else if (AXIS == 0) {
-      jvp_read<N1, N2, AXIS>(Wp, v, korder_in, t, line, lc, work, pitch);
-      jvp_read<N1, N2, AXIS>(Wd, u, korder_in, t, line, lc, work, pitch);
+      bwd_load_half<N1, N2, AXIS, 0>(Wp, q, korder_in, t, line, lc, work, pitch);
+      bwd_load_half<N1, N2, AXIS, 1>(Wd, q, korder_in, t, line, lc, work, pitch);
     } else {
       __syncthreads();
       tile_load<N, lines, pitch, WARPS * 32>(Wp, work, line0);
       __syncthreads();
-      jvp_read<N1, N2, AXIS>(Wp, v, korder_in, t, line, lc, work, pitch);
+      bwd_load_half<N1, N2, AXIS, 0>(Wp, q, korder_in, t, line, lc, work, pitch);
       __syncthreads();
       tile_load<N, lines, pitch, WARPS * 32>(Wd, work, line0);
       __syncthreads();
-      jvp_read<N1, N2, AXIS>(Wd, u, korder_in, t, line, lc, work, pitch);
+      bwd_load_half<N1, N2, AXIS, 1>(Wd, q, korder_in, t, line, lc, work, pitch);
       __syncthreads();
     }
     bool korder = korder_in;
     // ---- op1 on both
-    if (a.op1 != OP_NONE) {
-      korder = jvp_op<N1, N2>(a.op1, v, t, buf, tw, a.pf, a.scale);
-      jvp_op<N1, N2>(a.op1, u, t, buf, tw, a.pf, a.scale);
-    }
+    if (a.op1 != OP_NONE) korder = jvp_op<N1, N2>(a.op1, q, t, buf, tw, a.pf, a.scale);
     // ---- slice point: dphi = T (dpsi + i sigma dV psi), phi = T psi
     if (a.t_slice >= 0) {
       int eoff;
@@ -174,42 +147,37 @@ __device__ __forceinline__ void jvp_body(const JvpArgs& a, const int yslot) {
 #pragma unroll
         for (int j = 0; j < N2; ++j) {
           const float e = __ldg(D + ((t + N1 * j + doff) & fm));
-          u[j] = make_float2(fmaf(-e, v[j].y, u[j].x), fmaf(e, v[j].x, u[j].y));
+          q[j].re.y = fmaf(-e, q[j].im.x, q[j].re.y);
+          q[j].im.y = fmaf(e, q[j].re.x, q[j].im.y);
         }
       }
 #pragma unroll
-      for (int j = 0; j < N2; ++j) {
-        const float2 tv = __ldg(T + ((t + N1 * j + eoff) & fm));
-        v[j] = cmul(v[j], tv);
-        u[j] = cmul(u[j], tv);
-      }
+      for (int j = 0; j < N2; ++j) q[j] = cmul(q[j], __ldg(T + ((t + N1 * j + eoff) & fm)));
     }
     // ---- op2 on both
-    if (a.op2 != OP_NONE) {
-      korder = jvp_op<N1, N2>(a.op2, v, t, buf, tw, a.pf, a.scale);
-      jvp_op<N1, N2>(a.op2, u, t, buf, tw, a.pf, a.scale);
-    }
+    if (a.op2 != OP_NONE) korder = jvp_op<N1, N2>(a.op2, q, t, buf, tw, a.pf, a.scale);
     // ---- store
     if (to_pattern) {
       const float wm = a.weights[m];
 #pragma unroll
       for (int r = 0; r < N2; ++r) {
-        acc[r] = fmaf(wm, fmaf(v[r].x, v[r].x, v[r].y * v[r].y), acc[r]);
-        dacc[r] = fmaf(2.f * wm, fmaf(v[r].x, u[r].x, v[r].y * u[r].y), dacc[r]);
+        const float2 v = pair_a(q[r]), u = pair_b(q[r]);
+        acc[r] = fmaf(wm, fmaf(v.x, v.x, v.y * v.y), acc[r]);
+        dacc[r] = fmaf(2.f * wm, fmaf(v.x, u.x, v.y * u.y), dacc[r]);
       }
     } else if (AXIS == 0) {
 #pragma unroll
       for (int r = 0; r < N2; ++r) {
         const size_t o = off(korder ? korder_index<N1, N2>(t, r) : t + N1 * r);
-        Wp[o] = v[r];
-        Wd[o] = u[r];
+        Wp[o] = pair_a(q[r]);
+        Wd[o] = pair_b(q[r]);
       }
     } else {
       for (int wv = 0; wv < 2; ++wv) {
         __syncthreads();
 #pragma unroll
         for (int r = 0; r < N2; ++r)
-          work[(korder ? korder_index<N1, N2>(t, r) : t + N1 * r) * pitch + lc] = wv == 0 ? v[r] : u[r];
+          work[(korder ? korder_index<N1, N2>(t, r) : t + N1 * r) * pitch + lc] = wv == 0 ? pair_a(q[r]) : pair_b(q[r]);
         __syncthreads();
         tile_store<N, lines, pitch, WARPS * 32>(wv == 0 ? Wp : Wd, work, line0);
       }

@@ -57,7 +57,7 @@ int launch_jvp_t(const JvpArgs& a, int grid_y, cudaStream_t st) {
   constexpr int N = Geo::N;
   constexpr int W = Geo::kWarps;
   constexpr int MINB = N2 <= 16 ? 2 : 1;
-  const size_t smem = Geo::smem_bytes(W);
+  const size_t smem = bwd_smem_bytes<N1, N2>(W);
   static bool attr_done = false;
   if (!attr_done) {
     cudaFuncSetAttribute(ms_jvp_pass_kernel<N1, N2, AXIS, W, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
