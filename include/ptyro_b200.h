@@ -125,6 +125,19 @@ int ptyro_ms_backward(const ptyro_ms_params* p, int32_t ckpt_every, const float*
                       const float* grad_patterns, float* grad_potential, float* grad_modes,
                       void* workspace, size_t workspace_bytes, void* stream);
 
+/* ptyro_ms_backward plus the gradient of L with respect to every scan position:
+ * grad_positions float64 (P, 2) (y, x), in the units of `positions`. The
+ * reconstruction loops that refine positions (single_slice_poscorrected,
+ * single_slice_multi_modal, multi_slice_multi_modal,
+ * src/ptyrodactyl/multislice/multislice_recon.py:671-2227) differentiate stem_4d
+ * with respect to scan_positions_px; this is that derivative. `modes` as in
+ * ptyro_ms_forward. Workspace: ptyro_ms_backward_workspace_bytes(p). */
+int ptyro_ms_backward_positions(const ptyro_ms_params* p, int32_t ckpt_every, const float* potential,
+                                const float* modes, const float* weights, const double* positions,
+                                const float* residuals, const float* grad_patterns, float* grad_potential,
+                                float* grad_modes, double* grad_positions, void* workspace, size_t workspace_bytes,
+                                void* stream);
+
 /* The same model run the plain way: one scan position at a time, one kernel per
  * stage (shift, and per slice transmission multiply, FFT2, propagator multiply,
  * IFFT2, then FFT2 and |.|^2), the way the reference's vmap body reads

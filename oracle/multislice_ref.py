@@ -202,11 +202,13 @@ def stem_4d(slices, slice_thickness, pot_calib, beam_modes, weights, beam_calib,
 
 
 def stem_4d_vjp(slices, slice_thickness, pot_calib, beam_modes, weights, beam_calib, voltage_kv,
-                scan_positions_px, real_space_calib_ang, g, dtype=np.complex128):
+                scan_positions_px, real_space_calib_ang, g, dtype=np.complex128, with_positions=False):
     """Gradient of L with dL/d data = g (P,H,W) through stem_4d.
 
     Returns (dV (H,W,S) float64, dbeam (H,W,M) complex in JAX's convention
-    conj(2 dL/dconj(beam))). Weights are treated as constants.
+    conj(2 dL/dconj(beam))), and with ``with_positions`` also dL/d(positions) (P, 2):
+    psi0_p = ifft2(fft2(beam) R_p) and dL/dy_p = 2 Re sum conj(lam_psi0) d psi0/dy_p.
+    Weights are treated as constants.
     """
     slices = np.atleast_3d(np.asarray(slices, dtype=np.float64))
     h, w, num_slices = slices.shape
@@ -225,6 +227,8 @@ def stem_4d_vjp(slices, slice_thickness, pot_calib, beam_modes, weights, beam_ca
     qx = np.fft.fftfreq(w, d=float(real_space_calib_ang))
     qya, qxa = np.meshgrid(qy, qx, indexing="ij")
     lam_beam_k = np.zeros((h, w, n_modes), np.complex128)
+    dpos = np.zeros((positions.shape[0], 2))
+    beam_k = np.fft.fft2(beam, axes=(0, 1))
     for i in range(positions.shape[0]):
         phis = []
         wave = shifted[i].copy()
@@ -246,9 +250,15 @@ def stem_4d_vjp(slices, slice_thickness, pot_calib, beam_modes, weights, beam_ca
         # psi = ifft2(B ramp) -> lam_B = conj(ramp) * fft2(lam)/(HW)
         phase = -2.0 * np.pi * ((qya * positions[i, 0]) + (qxa * positions[i, 1]))
         ramp = np.exp(1j * phase)
+        if with_positions:
+            for c, q in enumerate((qya, qxa)):
+                dpsi = np.fft.ifft2(beam_k * (ramp * (-2j * np.pi * q))[..., None], axes=(0, 1))
+                dpos[i, c] = 2.0 * np.real(np.sum(np.conj(lam) * dpsi))
         lam_beam_k += np.conj(ramp)[..., None] * np.fft.fft2(lam, axes=(0, 1)) / (h * w)
     # B = fft2(beam) -> lam_beam = (HW) ifft2(lam_B)
     lam_beam = (h * w) * np.fft.ifft2(lam_beam_k, axes=(0, 1))
+    if with_positions:
+        return dv, np.conj(2.0 * lam_beam), dpos
     return dv, np.conj(2.0 * lam_beam)
 
 

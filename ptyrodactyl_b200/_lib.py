@@ -51,6 +51,7 @@ EXPORTED_SYMBOLS = (
     "ptyro_ms_forward_ckpt",
     "ptyro_ms_backward_workspace_bytes",
     "ptyro_ms_backward",
+    "ptyro_ms_backward_positions",
     "ptyro_sched_job_bytes",
     "ptyro_sched_create",
     "ptyro_sched_destroy",
@@ -160,6 +161,8 @@ def _declare(lib) -> None:
     lib.ptyro_ms_backward_workspace_bytes.argtypes = [pp]
     lib.ptyro_ms_backward.restype = ctypes.c_int
     lib.ptyro_ms_backward.argtypes = [pp, i32, vp, vp, vp, vp, vp, vp, vp, vp, sz, vp]
+    lib.ptyro_ms_backward_positions.restype = ctypes.c_int
+    lib.ptyro_ms_backward_positions.argtypes = [pp, i32, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, sz, vp]
     jd = ctypes.POINTER(JobDesc)
     lib.ptyro_sched_job_bytes.restype = sz
     lib.ptyro_sched_job_bytes.argtypes = [jd]

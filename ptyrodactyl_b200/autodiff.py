@@ -108,9 +108,9 @@ class Stem4dFunction(torch.autograd.Function):
         # under torch.func the rule sees functorch wrappers; the kernels need storage
         saved = [_plain(t) for t in ctx.saved_tensors]
         with torch._C._DisableFuncTorch():
-            g_slices, g_modes = Stem4dFunction._adjoint(ctx, saved, _plain(grad_out))
+            g_slices, g_modes, g_pos = Stem4dFunction._adjoint(ctx, saved, _plain(grad_out))
         return (g_slices if ctx.needs_input_grad[0] else None, g_modes if ctx.needs_input_grad[1] else None,
-                None, None, None, None, None, None, None, None, None, None, None)
+                None, g_pos, None, None, None, None, None, None, None, None, None)
 
     @staticmethod
     def _adjoint(ctx, saved, grad_out):
@@ -121,6 +121,7 @@ class Stem4dFunction(torch.autograd.Function):
         S, M, P = slices.shape[2], modes.shape[2], positions.shape[0]
         g_slices = torch.empty_strided(slices.shape, slices.stride(), dtype=torch.float32, device=dev)
         g_modes = torch.empty_strided(modes.shape, modes.stride(), dtype=torch.complex64, device=dev)
+        g_pos = torch.zeros((P, 2), dtype=torch.float64, device=dev) if ctx.needs_input_grad[3] else None
         if P == 0:
             g_slices.zero_()
             g_modes.zero_()
@@ -130,12 +131,19 @@ class Stem4dFunction(torch.autograd.Function):
                             modes.stride(), batch, tune, f, windows)
             ws_bytes = lib.ptyro_ms_backward_workspace_bytes(ctypes.byref(prm))
             ws = _workspace(ws_bytes, dev)
-            _lib.check(lib.ptyro_ms_backward(ctypes.byref(prm), k, slices.data_ptr(), weights.data_ptr(),
-                                             positions.data_ptr(), res.data_ptr(), g.data_ptr(),
-                                             g_slices.data_ptr(), g_modes.data_ptr(), ws.data_ptr(), ws_bytes,
-                                             _stream_ptr(dev)))
+            if g_pos is None:
+                _lib.check(lib.ptyro_ms_backward(ctypes.byref(prm), k, slices.data_ptr(), weights.data_ptr(),
+                                                 positions.data_ptr(), res.data_ptr(), g.data_ptr(),
+                                                 g_slices.data_ptr(), g_modes.data_ptr(), ws.data_ptr(), ws_bytes,
+                                                 _stream_ptr(dev)))
+            else:
+                _lib.check(lib.ptyro_ms_backward_positions(ctypes.byref(prm), k, slices.data_ptr(), modes.data_ptr(),
+                                                           weights.data_ptr(), positions.data_ptr(), res.data_ptr(),
+                                                           g.data_ptr(), g_slices.data_ptr(), g_modes.data_ptr(),
+                                                           g_pos.data_ptr(), ws.data_ptr(), ws_bytes,
+                                                           _stream_ptr(dev)))
         # the C-ABI gives JAX's convention conj(2 dL/dconj); torch wants 2 dL/dconj
-        return g_slices, g_modes.conj().resolve_conj()
+        return g_slices, g_modes.conj().resolve_conj(), g_pos
 
     @staticmethod
     def jvp(ctx, t_slices, t_modes, t_weights, t_positions, *rest):
@@ -161,7 +169,7 @@ def stem_4d_patterns(slices: torch.Tensor, modes: torch.Tensor, weights: torch.T
     ``windows`` the potential is a larger periodic field (see ``run_forward``).
     Reverse mode (``backward``, ``torch.func.grad/vjp``) and forward mode
     (``torch.func.jvp``, dual tensors) both run hand-written kernels."""
-    record = bool(slices.requires_grad or modes.requires_grad) and torch.is_grad_enabled()
+    record = bool(slices.requires_grad or modes.requires_grad or positions.requires_grad) and torch.is_grad_enabled()
     return Stem4dFunction.apply(slices, modes, weights, positions, float(slice_thickness), float(voltage_kv),
                                 float(calib_ang), float(calib_ang if shift_calib_ang is None else shift_calib_ang),
                                 int(ckpt_every), int(batch), int(default_tune(modes.shape[0]) if tune is None else tune),

@@ -734,7 +734,7 @@ static __global__ void k_write_grad_modes(const float2* __restrict__ lam_beam, i
 }
 
 struct BwdLayout {
-  size_t tw, pf, trans, trans_t, ramp_y, ramp_x, psi, lam, contrib, beam, total;
+  size_t tw, pf, trans, trans_t, ramp_y, ramp_x, psi, lam, contrib, beam, probe_k, total;
   int batch;
 };
 
@@ -763,8 +763,51 @@ static BwdLayout bwd_layout_for(const ptyro_ms_params* p) {
   L.lam = o; o = align_up(o + 8 * nn * slots);
   L.contrib = o; o = align_up(o + 4 * nn * slots);
   L.beam = o; o = align_up(o + 8 * nn * p->num_modes);
+  L.probe_k = o; o = align_up(o + 8 * nn * p->num_modes);  // position gradients only
   L.total = o;
   return L;
+}
+
+// dL/d(position) of every probe of a batch from the adjoint left in k-space by the
+// last passes, G_p = fft2(lam_psi0_p) conj(R_p), and the probe spectra B_m:
+// psi0_p = ifft2(B R_p), R_p = exp(-2 pi i (qy y_p + qx x_p)), so
+// dL/dy_p = 2 Re sum_r conj(lam) d psi0/dy = (4 pi / N^2) sum_{m,k} qy Im(conj(G) B)
+// (Parseval), likewise x. One CTA per probe, float64 accumulation, warps added in
+// order (deterministic).
+static __global__ void __launch_bounds__(256) k_position_grad(const float2* __restrict__ G, const float2* __restrict__ B,
+                                                              int n, int M, double shift_calib, double* out) {
+  __shared__ double red[8][2];
+  const size_t nn = (size_t)n * n;
+  const int b = blockIdx.x;
+  double sy = 0.0, sx = 0.0;
+  for (int m = 0; m < M; ++m) {
+    const float2* g = G + ((size_t)b * M + m) * nn;
+    const float2* bk = B + (size_t)m * nn;
+    for (size_t i = threadIdx.x; i < nn; i += blockDim.x) {
+      const int ky = (int)(i / n), kx = (int)(i % n);
+      const double qy = (double)(ky < n / 2 ? ky : ky - n) / (n * shift_calib);
+      const double qx = (double)(kx < n / 2 ? kx : kx - n) / (n * shift_calib);
+      const float2 gv = g[i], bv = bk[i];
+      const double im = (double)gv.x * bv.y - (double)gv.y * bv.x;  // Im(conj(G) B)
+      sy += qy * im;
+      sx += qx * im;
+    }
+  }
+  for (int o = 16; o >= 1; o >>= 1) {
+    sy += __shfl_xor_sync(0xffffffffu, sy, o);
+    sx += __shfl_xor_sync(0xffffffffu, sx, o);
+  }
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (lane == 0) {
+    red[warp][0] = sy;
+    red[warp][1] = sx;
+  }
+  __syncthreads();
+  if (threadIdx.x < 2) {
+    double s = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += red[w][threadIdx.x];
+    out[2 * (size_t)b + threadIdx.x] = 4.0 * 3.14159265358979323846 / ((double)n * n) * s;
+  }
 }
 
 static int launch_bwd(int n, int axis, const BwdArgs& a, int grid_y, cudaStream_t st) {
@@ -864,7 +907,7 @@ static int launch_reduce_dv_any(const ptyro_ms_params* p, const float* contrib, 
 static int backward_impl(const ptyro_ms_params* p, int ckpt_every, const float* potential, const float* weights,
                          const double* positions, const float2* residuals, const float* grad_patterns,
                          float* grad_potential, float* grad_modes, void* workspace, size_t workspace_bytes,
-                         void* stream) {
+                         void* stream, const float* modes = nullptr, double* grad_positions = nullptr) {
   int rc = validate(p);
   if (rc) return rc;
   if (ckpt_every < 1) return fail(PTYRO_ERR_INVALID, "ckpt_every must be >= 1");
@@ -897,6 +940,14 @@ static int backward_impl(const ptyro_ms_params* p, int ckpt_every, const float* 
                                                                  p->pot_stride_s, F, S);
   k_zero2<<<blocks_for(nn * M, 256), 256, 0, st>>>(beam, nn * M);
   if ((rc = check_launch("backward setup", 5))) return rc;
+  if (grad_positions) {
+    if (!modes) return fail(PTYRO_ERR_INVALID, "position gradients need the beam modes");
+    float2* pk = (float2*)(ws + L.probe_k);
+    k_gather_modes<<<blocks_for(nn * M, 256), 256, 0, st>>>((const float2*)modes, p->mode_stride_y,
+                                                            p->mode_stride_x, p->mode_stride_m, n, M, pk);
+    if ((rc = check_launch("k_gather_modes"))) return rc;
+    if ((rc = fft2_planes(n, M, false, pk, tw, st))) return rc;
+  }
   BwdBuffers B;
   B.psi = (float2*)(ws + L.psi);
   B.lam = (float2*)(ws + L.lam);
@@ -918,6 +969,11 @@ static int backward_impl(const ptyro_ms_params* p, int ckpt_every, const float* 
                                       nb, k);
       if ((rc = launch_bwd(n, b.axis, b.a, b.rows, st))) return rc;
       if (b.slice >= 0 && (rc = launch_reduce_dv_any(p, B.contrib, nb, b0, grad_potential, b.slice, st))) return rc;
+    }
+    if (grad_positions) {
+      k_position_grad<<<nb, 256, 0, st>>>(B.lam, (const float2*)(ws + L.probe_k), n, M, p->shift_calib_ang,
+                                          grad_positions + 2 * (size_t)b0);
+      if ((rc = check_launch("k_position_grad"))) return rc;
     }
     k_reduce_beam<<<(unsigned)((nn * M + 255) / 256), 256, 0, st>>>(B.lam, nb, M, n, beam);
     if ((rc = check_launch("k_reduce_beam"))) return rc;

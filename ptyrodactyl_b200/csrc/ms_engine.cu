@@ -104,6 +104,16 @@ int ptyro_ms_backward(const ptyro_ms_params* p, int32_t ckpt_every, const float*
                        grad_potential, grad_modes, workspace, workspace_bytes, stream);
 }
 
+int ptyro_ms_backward_positions(const ptyro_ms_params* p, int32_t ckpt_every, const float* potential,
+                                const float* modes, const float* weights, const double* positions,
+                                const float* residuals, const float* grad_patterns, float* grad_potential,
+                                float* grad_modes, double* grad_positions, void* workspace, size_t workspace_bytes,
+                                void* stream) {
+  if (!grad_positions && p && p->num_probes > 0) return fail(PTYRO_ERR_INVALID, "grad_positions is NULL");
+  return backward_impl(p, ckpt_every, potential, weights, positions, (const float2*)residuals, grad_patterns,
+                       grad_potential, grad_modes, workspace, workspace_bytes, stream, modes, grad_positions);
+}
+
 int ptyro_ms_forward_plain(const ptyro_ms_params* p, const float* potential, const float* modes,
                            const float* weights, const double* positions, float* patterns, void* workspace,
                            size_t workspace_bytes, void* stream) {

@@ -284,12 +284,12 @@ def stem_4d(pot_slice: PotentialSlices, beam: ProbeModes, microscope: Microscope
     calib = min(float(pot_slice.calib), float(beam.calib))
     if not microscope.ensemble.is_empty():
         # per position, cbed_image's ensemble branch (simulations.py:1163-1193)
-        if _needs_autodiff(slices, modes):
+        if _needs_autodiff(slices, modes, positions):
             raise NotImplementedError("derivatives through ensemble axes are not supported by the B200 engine")
         from .ensemble import ensemble_patterns
         data = ensemble_patterns(slices, pot_slice.slice_thickness, beam, microscope.ensemble,
                                  microscope.voltage_kv, calib, positions, detector.real_space_calib_ang)
-    elif _needs_autodiff(slices, modes):
+    elif _needs_autodiff(slices, modes, positions):
         # differentiable path: checkpointed forward + hand-written adjoint kernel
         from .autodiff import stem_4d_patterns
         data = stem_4d_patterns(slices, modes, weights, positions, pot_slice.slice_thickness,
@@ -324,7 +324,7 @@ def stem_4d_windowed(pot_slice: PotentialSlices, beam: ProbeModes, microscope: M
     positions = as_tensor(detector.scan_positions_px, torch.float64, dev).reshape(-1, 2).contiguous()
     win = as_tensor(windows, torch.int32, dev).reshape(-1, 2).contiguous()
     calib = min(float(pot_slice.calib), float(beam.calib))
-    if _needs_autodiff(slices, modes):
+    if _needs_autodiff(slices, modes, positions):
         from .autodiff import stem_4d_patterns
         data = stem_4d_patterns(slices, modes, weights, positions, pot_slice.slice_thickness,
                                 microscope.voltage_kv, calib, detector.real_space_calib_ang, windows=win)

@@ -182,3 +182,17 @@ def test_gradient_identical_across_launch_variants():
         got = pb.vjp(*args, ckpt_every=2, tune=tune)
         for a, b in zip(ref, got):
             assert torch.equal(a, b), tune
+
+
+@pytest.mark.parametrize("n,s,m,p", [(64, 4, 2, 5), (128, 3, 1, 3), (256, 2, 1, 2)])
+def test_position_gradient_matches_oracle(n, s, m, p):
+    pot, modes, w, pos, g = _case(n, s, m, p, seed=n)
+    dev = torch.device("cuda")
+    sl = torch.as_tensor(pot, dtype=torch.float32, device=dev)
+    md = torch.as_tensor(modes.astype(np.complex64), device=dev)
+    wt = torch.as_tensor(w, dtype=torch.float32, device=dev)
+    ps = torch.as_tensor(pos, dtype=torch.float64, device=dev).requires_grad_(True)
+    pat = pb.stem_4d_patterns(sl, md, wt, ps, 1.7, 200.0, 0.3)
+    (pat * torch.as_tensor(g, dtype=torch.float32, device=dev)).sum().backward()
+    _, _, dpos = R.stem_4d_vjp(pot, 1.7, 0.3, modes, w, 0.3, 200.0, pos, 0.3, g, with_positions=True)
+    assert rel_l2(ps.grad.cpu().numpy(), dpos) < TOL, rel_l2(ps.grad.cpu().numpy(), dpos)

@@ -241,3 +241,25 @@ def test_oracle_resize_weights_properties():
     from ptyrodactyl_b200.detectors import linear_resize_weights
     for a, b in [(4, 8), (8, 4), (100, 37), (37, 64), (64, 64)]:
         assert np.allclose(linear_resize_weights(a, b), R.resize_linear_weights(a, b).T)
+
+
+def test_oracle_position_gradient_matches_finite_differences():
+    rng = np.random.default_rng(6)
+    n, s = 16, 3
+    pot = rng.uniform(0, 30, (n, n, s))
+    probe = R.make_probe(200.0, 25.0, (n, n), 40.0, defocus_ang=-20.0)
+    modes = np.stack([probe, np.roll(probe, 1, 0) * 0.5j], -1)
+    w = [0.7, 0.3]
+    pos = np.array([[0.3, -0.4], [1.2, 0.7]])
+    g = rng.normal(size=(2, n, n))
+
+    def loss(p):
+        return float(np.sum(g * R.stem_4d(pot, 1.5, 0.4, modes, w, 0.4, 200.0, p, 0.4)["data"]))
+
+    _, _, dpos = R.stem_4d_vjp(pot, 1.5, 0.4, modes, w, 0.4, 200.0, pos, 0.4, g, with_positions=True)
+    for i in range(2):
+        for c in range(2):
+            e = np.zeros_like(pos)
+            e[i, c] = 1e-5
+            fd = (loss(pos + e) - loss(pos - e)) / 2e-5
+            assert abs(fd - dpos[i, c]) <= 1e-6 * max(1.0, abs(fd))
