@@ -564,3 +564,42 @@ def clip_cbed(cbed, fourier_calib_inv_ang, voltage_kv, extent_mrad, output_shape
     if output_shape[1] != c.shape[1]:
         c = c @ resize_linear_weights(c.shape[1], output_shape[1])
     return c
+
+
+# ---------------------------------------------------------------------------
+# Reconstruction loop (multislice/multislice_recon.py:671-1221) with optax 0.2.3's
+# Adam restated, for a few iterations in float64: the checker of the engine's loops.
+# ---------------------------------------------------------------------------
+
+
+def _adam_step(g, state, lr, b1=0.9, b2=0.999, eps=1e-8):
+    mu = b1 * state["mu"] + (1 - b1) * g
+    nu = b2 * state["nu"] + (1 - b2) * np.real(np.conj(g) * g)
+    c = state["count"] + 1
+    step = -lr * (mu / (1 - b1 ** c)) / (np.sqrt(nu / (1 - b2 ** c)) + eps)
+    return step, {"mu": mu, "nu": nu, "count": c}
+
+
+def single_slice_poscorrected(data, positions, voltage_kv, calib_ang, pot0, beam0, slice_thickness, iterations,
+                              lr, lr_pos):
+    """MSE loss, one slice; returns (pot, beam, positions, losses)."""
+    pot, beam, pos = pot0.astype(np.complex128), beam0.astype(np.complex128), np.asarray(positions, np.float64)
+    zero = lambda x: {"mu": np.zeros_like(x), "nu": np.zeros(x.shape), "count": 0}
+    s_pot, s_beam, s_pos = zero(pot), zero(beam), zero(pos)
+    losses = []
+    for _ in range(iterations):
+        model = stem_4d(np.real(pot)[..., None], slice_thickness, calib_ang, beam[..., None], [1.0], calib_ang,
+                        voltage_kv, pos, calib_ang)["data"]
+        diff = model - data
+        losses.append(float(np.mean(diff ** 2)))
+        g = 2.0 * diff / diff.size
+        dv, dbeam, dpos = stem_4d_vjp(np.real(pot)[..., None], slice_thickness, calib_ang, beam[..., None], [1.0],
+                                      calib_ang, voltage_kv, pos, calib_ang, g, with_positions=True)
+        # the reference steps with conj(JAX gradient)
+        step, s_pot = _adam_step(dv[:, :, 0].astype(np.complex128), s_pot, lr)
+        pot = pot + step
+        step, s_beam = _adam_step(np.conj(dbeam[:, :, 0]), s_beam, lr)
+        beam = beam + step
+        step, s_pos = _adam_step(dpos, s_pos, lr_pos)
+        pos = pos + step
+    return pot, beam, pos, losses

@@ -52,6 +52,13 @@ from .detectors import (  # noqa: F401
 )
 from .autodiff import Stem4dFunction, jvp, make_probe_differentiable, stem_4d_patterns, vjp  # noqa: F401
 from . import jacobian  # noqa: F401
+from . import multislice_recon  # noqa: F401
+from .multislice_recon import (  # noqa: F401
+    multi_slice_multi_modal,
+    single_slice_multi_modal,
+    single_slice_poscorrected,
+    single_slice_ptychography,
+)
 from .crystal import CrystalData, create_crystal_data, crystal_potential_slices  # noqa: F401
 from .ensemble import (  # noqa: F401
     coherence_to_distribution,
