@@ -52,6 +52,13 @@ from .detectors import (  # noqa: F401
 )
 from .autodiff import Stem4dFunction, jvp, make_probe_differentiable, stem_4d_patterns, vjp  # noqa: F401
 from . import jacobian  # noqa: F401
+from .checked import (  # noqa: F401
+    CheckedValueError,
+    checked_cbed_image,
+    checked_make_probe,
+    checked_stem4d_sharded,
+    checked_stem_4d,
+)
 from . import multislice_recon  # noqa: F401
 from .multislice_recon import (  # noqa: F401
     multi_slice_multi_modal,
