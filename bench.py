@@ -372,7 +372,8 @@ def run_ours(args, rank, world, local_rank):
                        "parallelism": f"dp{world} (probe shards, no collective)"},
             "roofline": {"bound": "fp32", "achieved": achieved_tflops, "peak": peak, "unit": "TFLOP/s",
                          "frac": achieved_tflops / peak, "traffic": traffic,
-                         "kernel": ("ms_pass_pair_kernel<16,16> steady-state pass (two lines per thread, f32x2; conv, x T, conv)" if tune & 16 else "ms_pass_kernel<16,16> steady-state pass (conv, x T, conv)"),
+                         "kernel": ("ms_pass_pair_kernel<16,16> steady-state pass (two lines per thread, f32x2; conv, x T, conv"
+                                    + ("; column blocks by TMA)" if tune & 2048 else ")") if tune & 16 else "ms_pass_kernel<16,16> steady-state pass (conv, x T, conv)"),
                          "flops_per_launch": flops_per_launch, "launch_ms": [round(x, 4) for x in pass_ms],
                          "peak_source": "measured FP32 FMA stream (ptyro_fp32_fma_probe) in this run",
                          "hbm_achieved_gbs": bytes_per_launch / avg_pass_s / 1e9,

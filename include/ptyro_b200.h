@@ -232,6 +232,12 @@ int ptyro_fft2(int32_t n, int32_t count, int32_t inverse, float* data, void* wor
  * Lets a caller count the launches of a timed region. */
 unsigned long long ptyro_launch_count(void);
 
+/* Device-side waits of the pass kernels (tensor-memory-access copies of the 256^2
+ * column pass, tune bit 2048) that gave up after their poll limit on the current
+ * device; 0 means every copy completed. No counterpart in the reference (a health
+ * check of this engine's bounded waits). */
+unsigned int ptyro_pass_wait_timeouts(void);
+
 /* `reps` launches of the steady-state pass (finish slice s-1's convolution along
  * `axis`, multiply T_1, start slice s's convolution) over the batch of wave slots
  * held in `workspace` by a preceding ptyro_ms_forward with the same `p`. The

@@ -33,6 +33,7 @@ EXPORTED_SYMBOLS = (
     "ptyro_fft_workspace_bytes",
     "ptyro_fft2",
     "ptyro_launch_count",
+    "ptyro_pass_wait_timeouts",
     "ptyro_ms_steady_pass",
     "ptyro_fp32_fma_probe",
     "ptyro_ms_forward_noalloc",
@@ -149,6 +150,8 @@ def _declare(lib) -> None:
     lib.ptyro_fft2.argtypes = [i32, i32, i32, vp, vp, sz, vp]
     lib.ptyro_launch_count.restype = ctypes.c_ulonglong
     lib.ptyro_launch_count.argtypes = []
+    lib.ptyro_pass_wait_timeouts.restype = ctypes.c_uint
+    lib.ptyro_pass_wait_timeouts.argtypes = []
     lib.ptyro_ms_steady_pass.restype = ctypes.c_int
     lib.ptyro_ms_steady_pass.argtypes = [pp, i32, i32, vp, sz, vp]
     lib.ptyro_fp32_fma_probe.restype = ctypes.c_int

@@ -167,6 +167,8 @@ int ptyro_ms_forward_plain(const ptyro_ms_params* p, const float* potential, con
 
 unsigned long long ptyro_launch_count(void) { return g_launches.load(std::memory_order_relaxed); }
 
+unsigned int ptyro_pass_wait_timeouts(void) { return ptyro::pair_wait_timeouts_256(); }
+
 int ptyro_ms_steady_pass(const ptyro_ms_params* p, int32_t axis, int32_t reps, void* workspace,
                          size_t workspace_bytes, void* stream) {
   int rc = validate(p);

@@ -14,9 +14,53 @@
 // shared tile (row pitch lines + 4 float2, so 16-byte column-pair reads of eight
 // lanes fall in distinct banks).
 #pragma once
+#include <cuda.h>
+
 #include "ms_pass.cuh"
 
 namespace ptyro {
+
+// Waits on a TMA completion that gave up after the iteration limit (this
+// translation unit's launches); read on the host by the pass launcher's accessor.
+static __device__ unsigned int g_pair_wait_timeouts = 0;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(uint32_t bar, int count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+// true once the barrier's phase `parity` has completed; false after `limit` polls
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, int limit) {
+  for (int i = 0; i < limit; ++i) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+// plain (non-multicast) 3-D tiled TMA load of box (x, y, z) into this CTA's shared memory
+__device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap* map, int x, int y, int z, uint32_t bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];" ::
+          "r"(dst),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(bar)
+      : "memory");
+}
+__device__ __forceinline__ void tma_store_3d(const CUtensorMap* map, int x, int y, int z, uint32_t src) {
+  asm volatile("cp.async.bulk.tensor.3d.global.shared::cta.bulk_group [%0, {%1, %2, %3}], [%4];" ::"l"(
+                   reinterpret_cast<uint64_t>(map)),
+               "r"(x), "r"(y), "r"(z), "r"(src)
+               : "memory");
+  asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+}
+__device__ __forceinline__ void tma_store_wait_read() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+__device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
 // Exchange buffer of one line pair (Pair elements): same (k2, n1) index layout as
 // LineBuf, padded to 4 mod 8 Pairs so the two line pairs of a warp start 64 bytes
@@ -51,16 +95,43 @@ struct PairGeom {
 // DIRECT (column passes): each lane pair reads and writes its two neighbouring
 // columns straight from global memory as 16-byte pieces (32 contiguous bytes per row
 // and lane pair), with no staging tile and no barriers.
-template <int N1, int N2, int AXIS, int WARPS, int MINB, bool PRE, bool DIRECT = false>
-__global__ void __launch_bounds__(WARPS * 32, MINB) ms_pass_pair_kernel(PassArgs a) {
+// TMA (column passes of 256^2 grids): each warp moves its block of 2 G columns x N
+// rows of the slot with one tiled TMA copy (wmap: the batch's wave slots as a 3-D
+// tensor (x, y, slot) of 8-byte elements, box 2 G x N x 1), into and out of its own
+// exchange buffers, instead of 16-byte loads and stores per row and lane pair; the
+// wait on the copy's mbarrier gives up after a bounded number of polls and counts
+// the failure in g_pair_wait_timeouts.
+template <int N1, int N2, int AXIS, int WARPS, int MINB, bool PRE, bool DIRECT = false, bool TMA = false>
+__global__ void __launch_bounds__(WARPS * 32, MINB)
+    ms_pass_pair_kernel(PassArgs a, const __grid_constant__ CUtensorMap wmap) {
   using PG = PairGeom<N1, N2, WARPS, PRE>;
   using PB = PairBuf<N1, N2>;
   constexpr int N = PG::N, G = PG::G, lines = PG::kLines, pitch = PG::kPitch;
+  static_assert(!TMA || (AXIS == 1 && DIRECT && !PRE && N <= 256), "TMA moves whole columns of a direct column pass");
+  constexpr uint32_t kWarpBytes = sizeof(float2) * 2 * G * N;  // one warp's column block
+  static_assert(!TMA || sizeof(Pair) * G * PB::kSize >= kWarpBytes + 127,
+                "the warp's exchange buffers must hold its column block at 128-byte alignment");
+  __shared__ __align__(8) uint64_t tma_bar[TMA ? WARPS : 1];
   extern __shared__ float4 smem4[];
   float2* tw = reinterpret_cast<float2*>(smem4);  // tw[k2 * N1 + t] = W_N^{t k2}
   float2* pfs = tw + N;                           // propagator factor along this axis
   float2* work = pfs + N;                         // column tile; aliases the exchange buffers
   Pair* xbuf = reinterpret_cast<Pair*>(work);
+  // TMA staging: this warp's exchange buffers, rounded up to 128 bytes; [row][2 G columns]
+  float2* stg = nullptr;
+  uint32_t bar = 0;
+  if (TMA) {
+    const int wp = threadIdx.x >> 5;
+    const uintptr_t base = reinterpret_cast<uintptr_t>(xbuf + (size_t)(wp * G) * PB::kSize);
+    stg = reinterpret_cast<float2*>((base + 127) & ~(uintptr_t)127);
+    bar = smem_u32(&tma_bar[wp]);
+    if ((threadIdx.x & 31) == 0) {
+      mbar_init(bar, 1);
+      asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+      mbar_expect_tx(bar, kWarpBytes);
+      tma_load_3d(smem_u32(stg), &wmap, blockIdx.x * lines + wp * 2 * G, 0, blockIdx.y, bar);
+    }
+  }
   for (int i = threadIdx.x; i < N; i += blockDim.x) {
     const int k2 = i / N1, tt = i % N1;
     tw[i] = a.tw[(tt * k2) % N];
@@ -94,6 +165,13 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) ms_pass_pair_kernel(PassArgs
 #pragma unroll
     for (int j = 0; j < N2; ++j)
       v[j] = make_pair(w[(size_t)la * N + t + N1 * j], w[(size_t)lb * N + t + N1 * j]);
+  } else if (TMA) {
+    if (!mbar_wait(bar, 0, 1 << 20) && lane == 0) atomicAdd(&g_pair_wait_timeouts, 1u);
+#pragma unroll
+    for (int j = 0; j < N2; ++j) {
+      const float4 q = *reinterpret_cast<const float4*>(stg + (t + N1 * j) * (2 * G) + 2 * gl);
+      v[j] = {make_float2(q.x, q.z), make_float2(q.y, q.w)};
+    }
   } else if (DIRECT) {
 #pragma unroll
     for (int j = 0; j < N2; ++j) {
@@ -159,6 +237,18 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) ms_pass_pair_kernel(PassArgs
     for (int j = 0; j < N2; ++j) {
       w[(size_t)la * N + t + N1 * j] = pair_a(v[j]);
       w[(size_t)lb * N + t + N1 * j] = pair_b(v[j]);
+    }
+  } else if (TMA) {
+    __syncwarp();  // every lane has read the last exchange
+#pragma unroll
+    for (int j = 0; j < N2; ++j)
+      *reinterpret_cast<float4*>(stg + (t + N1 * j) * (2 * G) + 2 * gl) =
+          make_float4(v[j].re.x, v[j].im.x, v[j].re.y, v[j].im.y);
+    fence_proxy_async_smem();
+    __syncwarp();
+    if (lane == 0) {
+      tma_store_3d(&wmap, la, 0, slot, smem_u32(stg));
+      tma_store_wait_read();
     }
   } else if (DIRECT) {
 #pragma unroll

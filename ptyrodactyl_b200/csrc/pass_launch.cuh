@@ -1,7 +1,11 @@
 // Launchers of the pass kernel, one translation unit per grid edge (pass_<n>.cu).
 // Each returns the cudaError_t of its launch as int (0 = success).
 #pragma once
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
 #include <atomic>
+#include <mutex>
 
 #include "ms_bwd.cuh"
 #include "ms_jvp.cuh"
@@ -100,20 +104,63 @@ int launch_pipe_t(const PassArgs& a, int nslots, cudaStream_t st) {
 }
 
 // Steady passes with two lines per thread in paired FP32 arithmetic (ms_pair.cuh).
-template <int N1, int N2, int AXIS, int W, int MINB, bool PRE, bool DIRECT = false>
-int launch_pair_w(const PassArgs& a, int grid_y, cudaStream_t st) {
+template <int N1, int N2, int AXIS, int W, int MINB, bool PRE, bool DIRECT = false, bool TMA = false>
+int launch_pair_w(const PassArgs& a, int grid_y, cudaStream_t st, const CUtensorMap* wmap = nullptr) {
   using PG = PairGeom<N1, N2, W, PRE>;
   const size_t smem = PG::smem_bytes();
   static bool attr_done = false;
   if (!attr_done) {
-    cudaFuncSetAttribute(ms_pass_pair_kernel<N1, N2, AXIS, W, MINB, PRE, DIRECT>,
+    cudaFuncSetAttribute(ms_pass_pair_kernel<N1, N2, AXIS, W, MINB, PRE, DIRECT, TMA>,
                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     attr_done = true;
   }
+  static const CUtensorMap kNoMap = {};
   dim3 grid(PG::N / PG::kLines, grid_y);
-  ms_pass_pair_kernel<N1, N2, AXIS, W, MINB, PRE, DIRECT><<<grid, W * 32, smem, st>>>(a);
+  ms_pass_pair_kernel<N1, N2, AXIS, W, MINB, PRE, DIRECT, TMA><<<grid, W * 32, smem, st>>>(a, wmap ? *wmap : kNoMap);
   g_launches.fetch_add(1, std::memory_order_relaxed);
   return (int)cudaGetLastError();
+}
+
+// cuTensorMapEncodeTiled from the driver (no link-time dependency on libcuda), or null.
+inline PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      p = nullptr;
+    return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  }();
+  return fn;
+}
+
+// The batch's wave slots as a 3-D tensor (x, y, slot) of 8-byte elements with box
+// (cols, N, 1), for the TMA column pass. The last encoding is reused. False if the
+// driver offers no encoder or rejects the map (the caller then uses plain loads).
+inline bool wave_tensor_map(float2* wave, int n, int slots, int cols, CUtensorMap* out) {
+  static std::mutex mu;
+  static float2* last_wave = nullptr;
+  static int last_n = 0, last_slots = 0, last_cols = 0;
+  static CUtensorMap last_map;
+  std::lock_guard<std::mutex> lock(mu);
+  if (wave == last_wave && n == last_n && slots == last_slots && cols == last_cols) {
+    *out = last_map;
+    return true;
+  }
+  PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+  if (!enc || (reinterpret_cast<uintptr_t>(wave) & 15) != 0) return false;
+  const cuuint64_t dims[3] = {(cuuint64_t)n, (cuuint64_t)n, (cuuint64_t)slots};
+  const cuuint64_t strides[2] = {(cuuint64_t)n * 8, (cuuint64_t)n * n * 8};
+  const cuuint32_t box[3] = {(cuuint32_t)cols, (cuuint32_t)n, 1};
+  const cuuint32_t estr[3] = {1, 1, 1};
+  CUtensorMap m;
+  if (enc(&m, CU_TENSOR_MAP_DATA_TYPE_UINT64, 3, wave, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+          CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+    return false;
+  last_wave = wave, last_n = n, last_slots = slots, last_cols = cols, last_map = m;
+  *out = m;
+  return true;
 }
 
 // variant bit 5 (32): transmission rows prefetched into shared memory, 3 CTAs/SM
@@ -126,6 +173,13 @@ int launch_pair_t(const PassArgs& a, int grid_y, cudaStream_t st, int variant) {
   constexpr int W4 = N / (2 * G) < 4 ? N / (2 * G) : 4;
   constexpr int W8 = N / (2 * G) < 8 ? N / (2 * G) : 8;
   const bool pre = (variant & 32) && a.win == nullptr && a.field_n == N;
+  if constexpr (AXIS == 1 && N == 256 && W8 == 8) {
+    // variant bit 11 (2048, with bits 6 and 7): column blocks moved by TMA
+    CUtensorMap wmap;
+    if ((variant & 2048) && (variant & 64) && (variant & 128) &&
+        wave_tensor_map(a.wave, N, grid_y, 2 * G, &wmap))
+      return launch_pair_w<N1, N2, AXIS, W8, 16 / W8, false, true, true>(a, grid_y, st, &wmap);
+  }
   if (AXIS == 1 && (variant & 128)) {
     if (variant & 64) return launch_pair_w<N1, N2, AXIS, W8, 16 / W8, false, true>(a, grid_y, st);
     return launch_pair_w<N1, N2, AXIS, W4, 16 / W4, false, true>(a, grid_y, st);
@@ -273,6 +327,7 @@ int launch_pass_32(int axis, const PassArgs& a, int grid_y, cudaStream_t st, int
 int launch_pass_64(int axis, const PassArgs& a, int grid_y, cudaStream_t st, int variant);
 int launch_pass_128(int axis, const PassArgs& a, int grid_y, cudaStream_t st, int variant);
 int launch_pass_256(int axis, const PassArgs& a, int grid_y, cudaStream_t st, int variant);
+unsigned int pair_wait_timeouts_256();
 int launch_pass_512(int axis, const PassArgs& a, int grid_y, cudaStream_t st, int variant);
 int launch_pass_1024(int axis, const PassArgs& a, int grid_y, cudaStream_t st, int variant);
 
