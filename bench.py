@@ -450,7 +450,7 @@ def run_grad(args, rank, world, local_rank):
     prm = ms_params(n, S, 1, P, w.voltage_kv, synth.SLICE_DZ, w.calib, w.calib, model.stride(), probe.stride(),
                     0, default_tune(n) if args.tune < 0 else args.tune, F, win)
     bprm = ms_params(n, S, 1, P, w.voltage_kv, synth.SLICE_DZ, w.calib, w.calib, model.stride(), probe.stride(),
-                     args.bwd_batch, 0, F, win)
+                     args.bwd_batch, prm.tune, F, win)
     ws_b = lib.ptyro_ms_workspace_bytes(ctypes.byref(prm))
     ws = torch.empty(ws_b, dtype=torch.uint8, device=dev)
     bws_b = lib.ptyro_ms_backward_workspace_bytes(ctypes.byref(bprm))

@@ -810,17 +810,17 @@ static __global__ void __launch_bounds__(256) k_position_grad(const float2* __re
   }
 }
 
-static int launch_bwd(int n, int axis, const BwdArgs& a, int grid_y, cudaStream_t st) {
+static int launch_bwd(int n, int axis, const BwdArgs& a, int grid_y, cudaStream_t st, int variant = 0) {
   if (grid_y <= 0) return PTYRO_OK;
   int rc;
   switch (n) {
-    case 16: rc = launch_bwd_16(axis, a, grid_y, st); break;
-    case 32: rc = launch_bwd_32(axis, a, grid_y, st); break;
-    case 64: rc = launch_bwd_64(axis, a, grid_y, st); break;
-    case 128: rc = launch_bwd_128(axis, a, grid_y, st); break;
-    case 256: rc = launch_bwd_256(axis, a, grid_y, st); break;
-    case 512: rc = launch_bwd_512(axis, a, grid_y, st); break;
-    case 1024: rc = launch_bwd_1024(axis, a, grid_y, st); break;
+    case 16: rc = launch_bwd_16(axis, a, grid_y, st, variant); break;
+    case 32: rc = launch_bwd_32(axis, a, grid_y, st, variant); break;
+    case 64: rc = launch_bwd_64(axis, a, grid_y, st, variant); break;
+    case 128: rc = launch_bwd_128(axis, a, grid_y, st, variant); break;
+    case 256: rc = launch_bwd_256(axis, a, grid_y, st, variant); break;
+    case 512: rc = launch_bwd_512(axis, a, grid_y, st, variant); break;
+    case 1024: rc = launch_bwd_1024(axis, a, grid_y, st, variant); break;
     default: return fail(PTYRO_ERR_UNSUPPORTED, "grid edge not compiled");
   }
   if (rc != 0) return fail(PTYRO_ERR_CUDA, std::string("ms_bwd_pass_kernel: ") + cudaGetErrorString((cudaError_t)rc));
@@ -967,7 +967,7 @@ static int backward_impl(const ptyro_ms_params* p, int ckpt_every, const float* 
     for (int k = 0; k <= S + 1; ++k) {
       const BwdPlan b = bwd_pass_plan(p, B, weights, res_base, grad_patterns + (size_t)b0 * nn, ckpt_every, C, b0,
                                       nb, k);
-      if ((rc = launch_bwd(n, b.axis, b.a, b.rows, st))) return rc;
+      if ((rc = launch_bwd(n, b.axis, b.a, b.rows, st, p->tune))) return rc;
       if (b.slice >= 0 && (rc = launch_reduce_dv_any(p, B.contrib, nb, b0, grad_potential, b.slice, st))) return rc;
     }
     if (grad_positions) {

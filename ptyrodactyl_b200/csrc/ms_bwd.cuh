@@ -77,18 +77,47 @@ __device__ __forceinline__ void bwd_load_half(const float2* w, Pair (&v)[N2], bo
 // The forward wave psi and the adjoint lambda of a line go through identical
 // operators, so they are carried as one Pair per element (half 0 = psi, half 1 =
 // lambda) and every transform step is one paired f32x2 operation for both.
-template <int N1, int N2, int AXIS, int WARPS>
-__device__ __forceinline__ void bwd_body(const BwdArgs& a, const int slot) {
+// TMA (column passes without the k-space init): each warp's block of G columns x N
+// rows of psi and of lambda comes in with two tiled TMA copies issued together at the
+// start (pmap / lmap: the slots as 3-D tensors (x, y, slot), box G x N x 1) into its
+// own exchange buffers, and goes back the same way, instead of two rounds through
+// the CTA's column tile with barriers; the dV contribution keeps the tile (a box of
+// G floats is narrower than TMA's 16-byte minimum).
+template <int N1, int N2, int AXIS, int WARPS, bool TMA = false>
+__device__ __forceinline__ void bwd_body(const BwdArgs& a, const int slot, const CUtensorMap* pmap = nullptr,
+                                         const CUtensorMap* lmap = nullptr) {
   using Geo = PassGeom<N1, N2>;
   using LB = LineBuf<N1, N2>;
   constexpr int N = Geo::N;
   constexpr int G = Geo::G;
   constexpr int lines = WARPS * G;
   static_assert(N % lines == 0, "lines per CTA must divide N");
+  static_assert(!TMA || (AXIS == 1 && N <= 256 && G * 8 % 16 == 0), "TMA moves whole column blocks");
   constexpr int pitch = lines + G;
+  constexpr uint32_t kBlock = sizeof(float2) * G * N;  // one wave's column block of a warp
+  static_assert(!TMA || sizeof(Pair) * G * PairBuf<N1, N2>::kSize >= 2 * kBlock + 127,
+                "the warp's exchange buffers must hold both column blocks at 128-byte alignment");
+  __shared__ __align__(8) uint64_t bwd_bar[TMA ? WARPS : 1];
   extern __shared__ float2 smem[];
   float2* tw = smem;
   float2* work = smem + N;
+  float2* stg = nullptr;  // TMA staging: psi block, then lambda block, [row][G]
+  uint32_t bar = 0;
+  if (TMA) {
+    const int wp = threadIdx.x >> 5;
+    const uintptr_t base = reinterpret_cast<uintptr_t>(reinterpret_cast<Pair*>(work) + (size_t)(wp * G) * PairBuf<N1, N2>::kSize);
+    stg = reinterpret_cast<float2*>((base + 127) & ~(uintptr_t)127);
+    bar = smem_u32(&bwd_bar[wp]);
+    if ((threadIdx.x & 31) == 0) {
+      const bool with_psi = a.op1 != OP_FFT;
+      const int x = blockIdx.x * lines + wp * G;
+      mbar_init(bar, 1);
+      asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+      mbar_expect_tx(bar, (with_psi ? 2u : 1u) * kBlock);
+      if (with_psi) tma_load_3d(smem_u32(stg), pmap, x, 0, slot, bar);
+      tma_load_3d(smem_u32(stg + G * N), lmap, x, 0, slot, bar);
+    }
+  }
   for (int i = threadIdx.x; i < N; i += blockDim.x) {
     const int k2 = i / N1, tt = i % N1;
     tw[i] = a.tw[(tt * k2) % N];
@@ -133,6 +162,15 @@ __device__ __forceinline__ void bwd_body(const BwdArgs& a, const int slot) {
       for (int r = 0; r < N2; ++r) v[r].re.x = v[r].im.x = 0.f;  // psi is not carried
     }
     bwd_load_half<N1, N2, AXIS, 1>(Wl, v, korder_in, t, line, lc, work, pitch);
+  } else if (TMA) {
+    if (!mbar_wait(bar, 0, 1 << 20) && lane == 0) atomicAdd(&g_pair_wait_timeouts, 1u);
+    if (a.op1 == OP_FFT) {
+#pragma unroll
+      for (int r = 0; r < N2; ++r) v[r].re.x = v[r].im.x = 0.f;
+    } else {
+      bwd_load_half<N1, N2, AXIS, 0>(Wp, v, korder_in, t, line, gl, stg, G);
+    }
+    bwd_load_half<N1, N2, AXIS, 1>(Wl, v, korder_in, t, line, gl, stg + G * N, G);
   } else {
     if (a.op1 == OP_FFT) {
 #pragma unroll
@@ -212,6 +250,31 @@ __device__ __forceinline__ void bwd_body(const BwdArgs& a, const int slot) {
 #pragma unroll
       for (int j = 0; j < N2; ++j) C[off(t + N1 * j)] = cv[j];
     }
+  } else if (TMA) {
+    __syncwarp();  // every lane has read the last exchange
+    if (store_psi) {
+#pragma unroll
+      for (int j = 0; j < N2; ++j) stg[(t + N1 * j) * G + gl] = pair_a(v[j]);
+    }
+#pragma unroll
+    for (int r = 0; r < N2; ++r) stg[G * N + (lam_k ? korder_index<N1, N2>(t, r) : t + N1 * r) * G + gl] = pair_b(v[r]);
+    fence_proxy_async_smem();
+    __syncwarp();
+    if (lane == 0) {
+      const int x = line0 + warp * G;
+      if (store_psi) tma_store_3d(pmap, x, 0, slot, smem_u32(stg));
+      tma_store_3d(lmap, x, 0, slot, smem_u32(stg + G * N));
+      tma_store_wait_read();
+    }
+    if (a.t_slice >= 0 && a.contrib) {
+      __syncthreads();  // every warp's copies have read its staging before the tile reuses it
+      float* tile = reinterpret_cast<float*>(work);
+#pragma unroll
+      for (int j = 0; j < N2; ++j) tile[(t + N1 * j) * pitch + lc] = cv[j];
+      __syncthreads();
+      tile_store<N, lines, pitch, WARPS * 32>(a.contrib + (size_t)slot * NN, reinterpret_cast<const float*>(work),
+                                              line0);
+    }
   } else {
     for (int wv = 0; wv < 3; ++wv) {
       if (wv == 0 && !store_psi) continue;
@@ -241,9 +304,10 @@ __device__ __forceinline__ void bwd_body(const BwdArgs& a, const int slot) {
 }
 
 
-template <int N1, int N2, int AXIS, int WARPS, int MINB>
-__global__ void __launch_bounds__(WARPS * 32, MINB) ms_bwd_pass_kernel(BwdArgs a) {
-  bwd_body<N1, N2, AXIS, WARPS>(a, blockIdx.y);
+template <int N1, int N2, int AXIS, int WARPS, int MINB, bool TMA = false>
+__global__ void __launch_bounds__(WARPS * 32, MINB)
+    ms_bwd_pass_kernel(BwdArgs a, const __grid_constant__ CUtensorMap pmap, const __grid_constant__ CUtensorMap lmap) {
+  bwd_body<N1, N2, AXIS, WARPS, TMA>(a, blockIdx.y, &pmap, &lmap);
 }
 
 // Adjoint passes of several jobs in one launch (see ms_pass_multi_kernel).

@@ -18,6 +18,56 @@ namespace ptyro {
 // Number of engine kernels enqueued by this process (all devices, all threads).
 extern std::atomic<unsigned long long> g_launches;
 
+// cuTensorMapEncodeTiled from the driver (no link-time dependency on libcuda), or null.
+inline PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      p = nullptr;
+    return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  }();
+  return fn;
+}
+
+// The batch's wave slots as a 3-D tensor (x, y, slot) of 8-byte elements with box
+// (cols, N, 1), for the TMA column passes. The last few encodings are reused. False
+// if the driver offers no encoder or rejects the map (the caller then uses plain loads).
+inline bool wave_tensor_map(float2* wave, int n, int slots, int cols, CUtensorMap* out) {
+  struct Entry {
+    float2* wave;
+    int n, slots, cols;
+    CUtensorMap map;
+  };
+  constexpr int kEntries = 8;
+  static std::mutex mu;
+  static Entry cache[kEntries] = {};
+  static int next = 0;
+  std::lock_guard<std::mutex> lock(mu);
+  for (const Entry& e : cache) {
+    if (e.wave == wave && e.n == n && e.slots == slots && e.cols == cols && wave != nullptr) {
+      *out = e.map;
+      return true;
+    }
+  }
+  PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+  if (!enc || (reinterpret_cast<uintptr_t>(wave) & 15) != 0) return false;
+  const cuuint64_t dims[3] = {(cuuint64_t)n, (cuuint64_t)n, (cuuint64_t)slots};
+  const cuuint64_t strides[2] = {(cuuint64_t)n * 8, (cuuint64_t)n * n * 8};
+  const cuuint32_t box[3] = {(cuuint32_t)cols, (cuuint32_t)n, 1};
+  const cuuint32_t estr[3] = {1, 1, 1};
+  CUtensorMap m;
+  if (enc(&m, CU_TENSOR_MAP_DATA_TYPE_UINT64, 3, wave, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+          CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+    return false;
+  cache[next] = {wave, n, slots, cols, m};
+  next = (next + 1) % kEntries;
+  *out = m;
+  return true;
+}
+
 template <int N1, int N2, int AXIS, int MINB, bool STEADY>
 int launch_pass_s(const PassArgs& a, int grid_y, cudaStream_t st) {
   using Geo = PassGeom<N1, N2>;
@@ -36,8 +86,9 @@ int launch_pass_s(const PassArgs& a, int grid_y, cudaStream_t st) {
   return (int)cudaGetLastError();
 }
 
-template <int N1, int N2, int AXIS>
-int launch_bwd_t(const BwdArgs& a, int grid_y, cudaStream_t st) {
+template <int N1, int N2, int AXIS, bool TMA>
+int launch_bwd_w(const BwdArgs& a, int grid_y, cudaStream_t st, const CUtensorMap* pmap = nullptr,
+                 const CUtensorMap* lmap = nullptr) {
   using Geo = PassGeom<N1, N2>;
   constexpr int N = Geo::N;
   constexpr int W = Geo::kWarps;
@@ -45,14 +96,28 @@ int launch_bwd_t(const BwdArgs& a, int grid_y, cudaStream_t st) {
   const size_t smem = bwd_smem_bytes<N1, N2>(W);
   static bool attr_done = false;
   if (!attr_done) {
-    cudaFuncSetAttribute(ms_bwd_pass_kernel<N1, N2, AXIS, W, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaFuncSetAttribute(ms_bwd_pass_kernel<N1, N2, AXIS, W, MINB, TMA>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)smem);
     attr_done = true;
   }
+  static const CUtensorMap kNoMap = {};
   dim3 grid(N / Geo::kLines, grid_y);
-  ms_bwd_pass_kernel<N1, N2, AXIS, W, MINB><<<grid, W * 32, smem, st>>>(a);
+  ms_bwd_pass_kernel<N1, N2, AXIS, W, MINB, TMA>
+      <<<grid, W * 32, smem, st>>>(a, pmap ? *pmap : kNoMap, lmap ? *lmap : kNoMap);
   g_launches.fetch_add(1, std::memory_order_relaxed);
   return (int)cudaGetLastError();
+}
+
+// variant bit 11 (2048): 256^2 adjoint column passes move their column blocks by TMA
+template <int N1, int N2, int AXIS>
+int launch_bwd_t(const BwdArgs& a, int grid_y, cudaStream_t st, int variant) {
+  if constexpr (AXIS == 1 && N1 * N2 == 256) {
+    CUtensorMap pmap, lmap;
+    if ((variant & 2048) && !a.init && wave_tensor_map(a.psi, N1 * N2, grid_y, 32 / N1, &pmap) &&
+        wave_tensor_map(a.lam, N1 * N2, grid_y, 32 / N1, &lmap))
+      return launch_bwd_w<N1, N2, AXIS, true>(a, grid_y, st, &pmap, &lmap);
+  }
+  return launch_bwd_w<N1, N2, AXIS, false>(a, grid_y, st);
 }
 
 template <int N1, int N2, int AXIS>
@@ -121,47 +186,6 @@ int launch_pair_w(const PassArgs& a, int grid_y, cudaStream_t st, const CUtensor
   return (int)cudaGetLastError();
 }
 
-// cuTensorMapEncodeTiled from the driver (no link-time dependency on libcuda), or null.
-inline PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
-  static PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
-    void* p = nullptr;
-    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
-    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
-        q != cudaDriverEntryPointSuccess)
-      p = nullptr;
-    return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
-  }();
-  return fn;
-}
-
-// The batch's wave slots as a 3-D tensor (x, y, slot) of 8-byte elements with box
-// (cols, N, 1), for the TMA column pass. The last encoding is reused. False if the
-// driver offers no encoder or rejects the map (the caller then uses plain loads).
-inline bool wave_tensor_map(float2* wave, int n, int slots, int cols, CUtensorMap* out) {
-  static std::mutex mu;
-  static float2* last_wave = nullptr;
-  static int last_n = 0, last_slots = 0, last_cols = 0;
-  static CUtensorMap last_map;
-  std::lock_guard<std::mutex> lock(mu);
-  if (wave == last_wave && n == last_n && slots == last_slots && cols == last_cols) {
-    *out = last_map;
-    return true;
-  }
-  PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
-  if (!enc || (reinterpret_cast<uintptr_t>(wave) & 15) != 0) return false;
-  const cuuint64_t dims[3] = {(cuuint64_t)n, (cuuint64_t)n, (cuuint64_t)slots};
-  const cuuint64_t strides[2] = {(cuuint64_t)n * 8, (cuuint64_t)n * n * 8};
-  const cuuint32_t box[3] = {(cuuint32_t)cols, (cuuint32_t)n, 1};
-  const cuuint32_t estr[3] = {1, 1, 1};
-  CUtensorMap m;
-  if (enc(&m, CU_TENSOR_MAP_DATA_TYPE_UINT64, 3, wave, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-          CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
-    return false;
-  last_wave = wave, last_n = n, last_slots = slots, last_cols = cols, last_map = m;
-  *out = m;
-  return true;
-}
 
 // variant bit 5 (32): transmission rows prefetched into shared memory, 3 CTAs/SM
 // variant bit 6 (64): 8 warps per CTA, 2 CTAs/SM
@@ -276,8 +300,9 @@ int launch_bwd_multi_t(const BwdArgs* descs, const int2* rows, int nrows, cudaSt
     return occ ? launch_pass_t<N1, N2, 1, hi>(a, grid_y, st, variant)                            \
                : launch_pass_t<N1, N2, 1, lo>(a, grid_y, st, variant);                           \
   }                                                                                              \
-  int launch_bwd_##NN(int axis, const BwdArgs& a, int grid_y, cudaStream_t st) {                \
-    return axis == 0 ? launch_bwd_t<N1, N2, 0>(a, grid_y, st) : launch_bwd_t<N1, N2, 1>(a, grid_y, st); \
+  int launch_bwd_##NN(int axis, const BwdArgs& a, int grid_y, cudaStream_t st, int variant) {   \
+    return axis == 0 ? launch_bwd_t<N1, N2, 0>(a, grid_y, st, variant)                          \
+                     : launch_bwd_t<N1, N2, 1>(a, grid_y, st, variant);                         \
   }                                                                                              \
   int launch_jvp_##NN(int axis, const JvpArgs& a, int grid_y, cudaStream_t st) {                \
     return axis == 0 ? launch_jvp_t<N1, N2, 0>(a, grid_y, st) : launch_jvp_t<N1, N2, 1>(a, grid_y, st); \
@@ -315,13 +340,13 @@ int launch_jvp_128(int axis, const JvpArgs& a, int grid_y, cudaStream_t st);
 int launch_jvp_256(int axis, const JvpArgs& a, int grid_y, cudaStream_t st);
 int launch_jvp_512(int axis, const JvpArgs& a, int grid_y, cudaStream_t st);
 int launch_jvp_1024(int axis, const JvpArgs& a, int grid_y, cudaStream_t st);
-int launch_bwd_16(int axis, const BwdArgs& a, int grid_y, cudaStream_t st);
-int launch_bwd_32(int axis, const BwdArgs& a, int grid_y, cudaStream_t st);
-int launch_bwd_64(int axis, const BwdArgs& a, int grid_y, cudaStream_t st);
-int launch_bwd_128(int axis, const BwdArgs& a, int grid_y, cudaStream_t st);
-int launch_bwd_256(int axis, const BwdArgs& a, int grid_y, cudaStream_t st);
-int launch_bwd_512(int axis, const BwdArgs& a, int grid_y, cudaStream_t st);
-int launch_bwd_1024(int axis, const BwdArgs& a, int grid_y, cudaStream_t st);
+int launch_bwd_16(int axis, const BwdArgs& a, int grid_y, cudaStream_t st, int variant);
+int launch_bwd_32(int axis, const BwdArgs& a, int grid_y, cudaStream_t st, int variant);
+int launch_bwd_64(int axis, const BwdArgs& a, int grid_y, cudaStream_t st, int variant);
+int launch_bwd_128(int axis, const BwdArgs& a, int grid_y, cudaStream_t st, int variant);
+int launch_bwd_256(int axis, const BwdArgs& a, int grid_y, cudaStream_t st, int variant);
+int launch_bwd_512(int axis, const BwdArgs& a, int grid_y, cudaStream_t st, int variant);
+int launch_bwd_1024(int axis, const BwdArgs& a, int grid_y, cudaStream_t st, int variant);
 int launch_pass_16(int axis, const PassArgs& a, int grid_y, cudaStream_t st, int variant);
 int launch_pass_32(int axis, const PassArgs& a, int grid_y, cudaStream_t st, int variant);
 int launch_pass_64(int axis, const PassArgs& a, int grid_y, cudaStream_t st, int variant);
