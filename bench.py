@@ -552,7 +552,7 @@ def run_config3(args, rank, world, local_rank):
         out.zero_()
         for v in pots:
             pb.run_forward(v, synth.SLICE_DZ, modes, wq, pos, w.voltage_kv, w.calib, w.calib, out=out,
-                           accumulate=True, batch=args.batch)
+                           accumulate=True, batch=args.batch, tune=None if args.tune < 0 else args.tune)
 
     for _ in range(max(1, args.warmup // 3)):
         step()
@@ -574,7 +574,8 @@ def run_config3(args, rank, world, local_rank):
             "n_gpus": world, "dtype": "f32", "data": "synthetic",
             "checks": {"pattern_sum_max_rel_err": float(((sums - n_ap).abs().max() / n_ap).item())},
             "config": {"workload": w.name, "grid": n, "slices": S, "probes_sampled": args.probes,
-                       "probes_full_scan": w.num_probes, "phonon_configs": len(pots), "batch": args.batch}}
+                       "probes_full_scan": w.num_probes, "phonon_configs": len(pots), "batch": args.batch,
+                       "tune": default_tune(w.n) if args.tune < 0 else args.tune}}
     if rank == 0:
         print(json.dumps(line), flush=True)
 

@@ -232,9 +232,9 @@ int ptyro_fft2(int32_t n, int32_t count, int32_t inverse, float* data, void* wor
  * Lets a caller count the launches of a timed region. */
 unsigned long long ptyro_launch_count(void);
 
-/* Device-side waits of the pass kernels (tensor-memory-access copies of the 256^2
- * column pass, tune bit 2048) that gave up after their poll limit on the current
- * device; 0 means every copy completed. No counterpart in the reference (a health
+/* Device-side waits of the pass kernels (the TMA copies of the column passes,
+ * tune bit 2048) that gave up after their poll limit on the current device, summed
+ * over grid edges; 0 means every copy completed. No counterpart in the reference (a health
  * check of this engine's bounded waits). */
 unsigned int ptyro_pass_wait_timeouts(void);
 

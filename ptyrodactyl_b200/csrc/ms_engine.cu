@@ -167,7 +167,14 @@ int ptyro_ms_forward_plain(const ptyro_ms_params* p, const float* potential, con
 
 unsigned long long ptyro_launch_count(void) { return g_launches.load(std::memory_order_relaxed); }
 
-unsigned int ptyro_pass_wait_timeouts(void) { return ptyro::pair_wait_timeouts_256(); }
+unsigned int ptyro_pass_wait_timeouts(void) {
+  unsigned int (*const units[])() = {pair_wait_timeouts_16,  pair_wait_timeouts_32,  pair_wait_timeouts_64,
+                                     pair_wait_timeouts_128, pair_wait_timeouts_256, pair_wait_timeouts_512,
+                                     pair_wait_timeouts_1024};
+  unsigned long long total = 0;
+  for (auto f : units) total += f();
+  return total > 0xffffffffull ? 0xffffffffu : (unsigned int)total;
+}
 
 int ptyro_ms_steady_pass(const ptyro_ms_params* p, int32_t axis, int32_t reps, void* workspace,
                          size_t workspace_bytes, void* stream) {

@@ -15,7 +15,7 @@
 // Every step that treats the pair halves alike runs as paired instructions; only
 // the two radix-2 stages that join the halves run scalar.
 #pragma once
-#include "ms_pass.cuh"
+#include "ms_pair.cuh"
 
 namespace ptyro {
 
@@ -92,18 +92,45 @@ __device__ __forceinline__ void half_k_to_nat(Pair (&p)[N1], int t, float2* buf,
   }
 }
 
-template <int N1, int N2, int AXIS, int WARPS, int MINB>
-__global__ void __launch_bounds__(WARPS * 32, MINB) ms_pass_half_kernel(PassArgs a) {
+// TMA (column passes of 512^2 grids): each warp's block of G columns x N rows comes
+// in and goes back as N / 256 tiled TMA copies of 256 rows (wmap: the slots as a 3-D
+// tensor (x, y, slot), box G x 256 x 1) through its own exchange buffers, instead of
+// the CTA's column tile and its barriers; bounded mbarrier wait as in ms_pair.cuh.
+template <int N1, int N2, int AXIS, int WARPS, int MINB, bool TMA = false>
+__global__ void __launch_bounds__(WARPS * 32, MINB)
+    ms_pass_half_kernel(PassArgs a, const __grid_constant__ CUtensorMap wmap) {
   using Geo = PassGeom<N1, N2>;
   using LB = LineBuf<N1, N2>;
   constexpr int N = Geo::N, G = Geo::G, H = N1;
   constexpr int lines = WARPS * G;
   static_assert(N % lines == 0, "lines per CTA must divide N");
   constexpr int pitch = lines + G;
+  constexpr int kBoxRows = N < 256 ? N : 256;
+  constexpr uint32_t kWarpBytes = sizeof(float2) * G * N;
+  static_assert(!TMA || (AXIS == 1 && N % kBoxRows == 0 && (G * 8) % 16 == 0), "TMA moves whole column blocks");
+  static_assert(!TMA || sizeof(float2) * G * LB::kSize >= kWarpBytes + 127,
+                "the warp's exchange buffers must hold its column block at 128-byte alignment");
+  __shared__ __align__(8) uint64_t half_bar[TMA ? WARPS : 1];
   extern __shared__ float2 smem[];
   float2* tw = smem;
   float2* pfs = smem + N;
   float2* work = smem + 2 * N;
+  float2* stg = nullptr;  // TMA staging: [row][G]
+  uint32_t bar = 0;
+  if (TMA) {
+    const int wp = threadIdx.x >> 5;
+    const uintptr_t base = reinterpret_cast<uintptr_t>(work + (size_t)(wp * G) * LB::kSize);
+    stg = reinterpret_cast<float2*>((base + 127) & ~(uintptr_t)127);
+    bar = smem_u32(&half_bar[wp]);
+    if ((threadIdx.x & 31) == 0) {
+      mbar_init(bar, 1);
+      asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+      mbar_expect_tx(bar, kWarpBytes);
+#pragma unroll
+      for (int y = 0; y < N; y += kBoxRows)
+        tma_load_3d(smem_u32(stg + (size_t)y * G), &wmap, blockIdx.x * lines + wp * G, y, blockIdx.y, bar);
+    }
+  }
   for (int i = threadIdx.x; i < N; i += blockDim.x) {
     const int k2 = i / N1, tt = i % N1;
     tw[i] = a.tw[(tt * k2) % N];
@@ -126,6 +153,10 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) ms_pass_half_kernel(PassArgs
   if (AXIS == 0) {
 #pragma unroll
     for (int j = 0; j < H; ++j) p[j] = make_pair(w[off(t + N1 * j)], w[off(t + N1 * (j + H))]);
+  } else if (TMA) {
+    if (!mbar_wait(bar, 0, 1 << 20) && (threadIdx.x & 31) == 0) atomicAdd(&g_pair_wait_timeouts, 1u);
+#pragma unroll
+    for (int j = 0; j < H; ++j) p[j] = make_pair(stg[(t + N1 * j) * G + gl], stg[(t + N1 * (j + H)) * G + gl]);
   } else {
     tile_load<N, lines, pitch, WARPS * 32>(w, work, line0);
     __syncthreads();
@@ -174,6 +205,21 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) ms_pass_half_kernel(PassArgs
     for (int j = 0; j < H; ++j) {
       w[off(t + N1 * j)] = pair_a(p[j]);
       w[off(t + N1 * (j + H))] = pair_b(p[j]);
+    }
+  } else if (TMA) {
+    __syncwarp();  // every lane has read the last exchange
+#pragma unroll
+    for (int j = 0; j < H; ++j) {
+      stg[(t + N1 * j) * G + gl] = pair_a(p[j]);
+      stg[(t + N1 * (j + H)) * G + gl] = pair_b(p[j]);
+    }
+    fence_proxy_async_smem();
+    __syncwarp();
+    if ((threadIdx.x & 31) == 0) {
+#pragma unroll
+      for (int y = 0; y < N; y += kBoxRows)
+        tma_store_3d(&wmap, line0 + warp * G, y, slot, smem_u32(stg + (size_t)y * G));
+      tma_store_wait_read();
     }
   } else {
     __syncthreads();

@@ -32,12 +32,14 @@ inline PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
 }
 
 // The batch's wave slots as a 3-D tensor (x, y, slot) of 8-byte elements with box
-// (cols, N, 1), for the TMA column passes. The last few encodings are reused. False
+// (cols, rows, 1) (rows = N by default), for the TMA column passes. The last few encodings are reused. False
 // if the driver offers no encoder or rejects the map (the caller then uses plain loads).
-inline bool wave_tensor_map(float2* wave, int n, int slots, int cols, CUtensorMap* out) {
+inline bool wave_tensor_map(float2* wave, int n, int slots, int cols, CUtensorMap* out, int rows = 0) {
+  if (rows <= 0) rows = n;
+  if (rows > 256 || n % rows != 0) return false;  // TMA box dimensions are at most 256
   struct Entry {
     float2* wave;
-    int n, slots, cols;
+    int n, slots, cols, rows;
     CUtensorMap map;
   };
   constexpr int kEntries = 8;
@@ -46,7 +48,7 @@ inline bool wave_tensor_map(float2* wave, int n, int slots, int cols, CUtensorMa
   static int next = 0;
   std::lock_guard<std::mutex> lock(mu);
   for (const Entry& e : cache) {
-    if (e.wave == wave && e.n == n && e.slots == slots && e.cols == cols && wave != nullptr) {
+    if (e.wave == wave && e.n == n && e.slots == slots && e.cols == cols && e.rows == rows && wave != nullptr) {
       *out = e.map;
       return true;
     }
@@ -55,14 +57,14 @@ inline bool wave_tensor_map(float2* wave, int n, int slots, int cols, CUtensorMa
   if (!enc || (reinterpret_cast<uintptr_t>(wave) & 15) != 0) return false;
   const cuuint64_t dims[3] = {(cuuint64_t)n, (cuuint64_t)n, (cuuint64_t)slots};
   const cuuint64_t strides[2] = {(cuuint64_t)n * 8, (cuuint64_t)n * n * 8};
-  const cuuint32_t box[3] = {(cuuint32_t)cols, (cuuint32_t)n, 1};
+  const cuuint32_t box[3] = {(cuuint32_t)cols, (cuuint32_t)rows, 1};
   const cuuint32_t estr[3] = {1, 1, 1};
   CUtensorMap m;
   if (enc(&m, CU_TENSOR_MAP_DATA_TYPE_UINT64, 3, wave, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
           CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
           CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
     return false;
-  cache[next] = {wave, n, slots, cols, m};
+  cache[next] = {wave, n, slots, cols, rows, m};
   next = (next + 1) % kEntries;
   *out = m;
   return true;
@@ -214,21 +216,33 @@ int launch_pair_t(const PassArgs& a, int grid_y, cudaStream_t st, int variant) {
 }
 
 // Steady passes with the halves of each line paired (ms_half.cuh), N2 == 2 N1.
-template <int N1, int N2, int AXIS, int MINB>
-int launch_half_t(const PassArgs& a, int grid_y, cudaStream_t st) {
+template <int N1, int N2, int AXIS, int MINB, bool TMA>
+int launch_half_w(const PassArgs& a, int grid_y, cudaStream_t st, const CUtensorMap* wmap = nullptr) {
   using Geo = PassGeom<N1, N2>;
   constexpr int W = Geo::kWarps;
   const size_t smem = Geo::smem_bytes(W);
   static bool attr_done = false;
   if (!attr_done) {
-    cudaFuncSetAttribute(ms_pass_half_kernel<N1, N2, AXIS, W, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaFuncSetAttribute(ms_pass_half_kernel<N1, N2, AXIS, W, MINB, TMA>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)smem);
     attr_done = true;
   }
+  static const CUtensorMap kNoMap = {};
   dim3 grid(Geo::N / Geo::kLines, grid_y);
-  ms_pass_half_kernel<N1, N2, AXIS, W, MINB><<<grid, W * 32, smem, st>>>(a);
+  ms_pass_half_kernel<N1, N2, AXIS, W, MINB, TMA><<<grid, W * 32, smem, st>>>(a, wmap ? *wmap : kNoMap);
   g_launches.fetch_add(1, std::memory_order_relaxed);
   return (int)cudaGetLastError();
+}
+
+// variant bit 11 (2048): 512^2 column passes move their column blocks by TMA
+template <int N1, int N2, int AXIS, int MINB>
+int launch_half_t(const PassArgs& a, int grid_y, cudaStream_t st, int variant) {
+  if constexpr (AXIS == 1 && N1 * N2 == 512) {
+    CUtensorMap wmap;
+    if ((variant & 2048) && wave_tensor_map(a.wave, N1 * N2, grid_y, 32 / N1, &wmap, 256))
+      return launch_half_w<N1, N2, AXIS, MINB, true>(a, grid_y, st, &wmap);
+  }
+  return launch_half_w<N1, N2, AXIS, MINB, false>(a, grid_y, st);
 }
 
 // tune bit 8 (value 256): steady passes of N2 == 2 N1 shapes run the half-paired kernel
@@ -243,8 +257,8 @@ int launch_pass_t(const PassArgs& a0, int grid_y, cudaStream_t st, int variant) 
   if (AXIS == 1 && (variant & 8)) a.direct = 1;
   if constexpr (N2 == 2 * N1) {
     if (is_steady_pass(a) && (variant & 256) && a.pf != nullptr)
-      return (variant & 512) ? launch_half_t<N1, N2, AXIS, 1>(a, grid_y, st)
-                             : launch_half_t<N1, N2, AXIS, 2>(a, grid_y, st);
+      return (variant & 512) ? launch_half_t<N1, N2, AXIS, 1>(a, grid_y, st, variant)
+                             : launch_half_t<N1, N2, AXIS, 2>(a, grid_y, st, variant);
   }
   if (is_steady_pass(a) && (variant & 16) && a.pf != nullptr)
     return launch_pair_t<N1, N2, AXIS>(a, grid_y, st, variant);
@@ -300,6 +314,12 @@ int launch_bwd_multi_t(const BwdArgs* descs, const int2* rows, int nrows, cudaSt
     return occ ? launch_pass_t<N1, N2, 1, hi>(a, grid_y, st, variant)                            \
                : launch_pass_t<N1, N2, 1, lo>(a, grid_y, st, variant);                           \
   }                                                                                              \
+  /* TMA completion waits of this unit's passes that hit their poll limit (current device) */ \
+  unsigned int pair_wait_timeouts_##NN() {                                                      \
+    unsigned int v = 0;                                                                          \
+    if (cudaMemcpyFromSymbol(&v, g_pair_wait_timeouts, sizeof v) != cudaSuccess) return 0xffffffffu; \
+    return v;                                                                                    \
+  }                                                                                              \
   int launch_bwd_##NN(int axis, const BwdArgs& a, int grid_y, cudaStream_t st, int variant) {   \
     return axis == 0 ? launch_bwd_t<N1, N2, 0>(a, grid_y, st, variant)                          \
                      : launch_bwd_t<N1, N2, 1>(a, grid_y, st, variant);                         \
@@ -352,7 +372,13 @@ int launch_pass_32(int axis, const PassArgs& a, int grid_y, cudaStream_t st, int
 int launch_pass_64(int axis, const PassArgs& a, int grid_y, cudaStream_t st, int variant);
 int launch_pass_128(int axis, const PassArgs& a, int grid_y, cudaStream_t st, int variant);
 int launch_pass_256(int axis, const PassArgs& a, int grid_y, cudaStream_t st, int variant);
+unsigned int pair_wait_timeouts_16();
+unsigned int pair_wait_timeouts_32();
+unsigned int pair_wait_timeouts_64();
+unsigned int pair_wait_timeouts_128();
 unsigned int pair_wait_timeouts_256();
+unsigned int pair_wait_timeouts_512();
+unsigned int pair_wait_timeouts_1024();
 int launch_pass_512(int axis, const PassArgs& a, int grid_y, cudaStream_t st, int variant);
 int launch_pass_1024(int axis, const PassArgs& a, int grid_y, cudaStream_t st, int variant);
 
