@@ -626,22 +626,22 @@ static __global__ void k_reduce_dv(const float* __restrict__ contrib, int nslots
 
 // Windowed runs: field pixel (fy, fx) of dV_s collects the contribution of every
 // slot whose n x n window (origin modulo F) covers it, added in slot order (no
-// atomics). Slots whose window rows miss the CTA's field row are culled once per
-// CTA; loads of 8 listed slots are issued together before they are summed, and
-// neighbouring threads read neighbouring pixels of the same slot plane.
-
+// atomics). A CTA covers a TX x TY tile of the field (TX, TY <= n); warp 0 first
+// lists, in slot order, the slots whose window meets the tile (rows and columns;
+// both lengths are at most n, so a window meets the tile iff it holds one of the
+// tile's corner rows and one of its corner columns), then every pixel adds the
+// listed slots whose window covers it. Loads of 8 listed slots are issued together,
+// and neighbouring threads read neighbouring pixels of the same slot plane.
 static __global__ void __launch_bounds__(256) k_reduce_dv_win(const float* __restrict__ contrib, int nb, int M, int n,
                                                        int F, const int* __restrict__ win, float* dv, long long sy,
-                                                       long long sx, long long ss, int s) {
-  // a CTA covers blockDim.x (<= F) pixels of one field row fy: first the slots whose
-  // window rows contain fy are listed in slot order (warp 0, ballots), then every
-  // pixel adds the listed slots whose window columns contain it, in list order
+                                                       long long sx, long long ss, int s, int tx_log2) {
   extern __shared__ int sh[];
   int* swx = sh;           // window column origin of each listed slot
-  int* sslot = sh + nb;    // listed slots, ascending
+  int* swy = sh + nb;      // window row origin
+  int* sslot = sh + 2 * nb;  // listed slots, ascending
   __shared__ int count;
-  const size_t i0 = (size_t)blockIdx.x * blockDim.x;
-  const int fy = (int)(i0 / F);
+  const int TX = 1 << tx_log2, TY = (int)blockDim.x >> tx_log2;
+  const int fx0 = (int)blockIdx.x * TX, fy0 = (int)blockIdx.y * TY;
   const int fm = F - 1;
   if (threadIdx.x < 32) {
     int c = 0;
@@ -652,22 +652,23 @@ static __global__ void __launch_bounds__(256) k_reduce_dv_win(const float* __res
         wy = win[2 * bb];
         wx = win[2 * bb + 1];
       }
-      const bool in = bb < nb && ((fy - wy) & fm) < n;
+      const bool rows = ((fy0 - wy) & fm) < n || ((fy0 + TY - 1 - wy) & fm) < n;
+      const bool cols = ((fx0 - wx) & fm) < n || ((fx0 + TX - 1 - wx) & fm) < n;
+      const bool in = bb < nb && rows && cols;
       const unsigned mask = __ballot_sync(0xffffffffu, in);
       if (in) {
         const int pos = c + __popc(mask & ((1u << threadIdx.x) - 1u));
         sslot[pos] = bb;
         swx[pos] = wx;
+        swy[pos] = wy;
       }
       c += __popc(mask);
     }
     if (threadIdx.x == 0) count = c;
   }
   __syncthreads();
-  const size_t i = i0 + threadIdx.x;
-  if (i >= (size_t)F * F) return;
-  const int fx = (int)(i % F);
-  const int ly_base = fy;
+  const int fx = fx0 + ((int)threadIdx.x & (TX - 1));
+  const int fy = fy0 + ((int)threadIdx.x >> tx_log2);
   const size_t nn = (size_t)n * n;
   const int cnt = count;
   float acc = 0.f;
@@ -678,11 +679,9 @@ static __global__ void __launch_bounds__(256) k_reduce_dv_win(const float* __res
       const int k = k0 + u;
       v[u] = 0.f;
       if (k < cnt) {
-        const int bb = sslot[k];
-        const int wy = win ? win[2 * bb] : 0;
-        const int ly = (ly_base - wy) & fm, lx = (fx - swx[k]) & fm;
-        if (lx < n) {
-          const float* cp = contrib + (size_t)bb * M * nn + (size_t)ly * n + lx;
+        const int ly = (fy - swy[k]) & fm, lx = (fx - swx[k]) & fm;
+        if (ly < n && lx < n) {
+          const float* cp = contrib + (size_t)sslot[k] * M * nn + (size_t)ly * n + lx;
           float t = cp[0];
           for (int m = 1; m < M; ++m) t += cp[(size_t)m * nn];
           v[u] = t;
@@ -697,13 +696,18 @@ static __global__ void __launch_bounds__(256) k_reduce_dv_win(const float* __res
 
 static int launch_reduce_dv_win(const float* contrib, int nb, int M, int n, int F, const int* win, float* dv,
                                 long long sy, long long sx, long long ss, int s, cudaStream_t st) {
-  const size_t ff = (size_t)F * F;
-  const int threads = F < 256 ? F : 256;  // a CTA never spans two field rows
-  constexpr int kChunk = 4096;            // probes listed per launch (32 KB of shared memory)
+  // tile TX x TY = 256 pixels with TX, TY <= n (n and F are powers of two, n >= 16)
+  const int tx = n < 32 ? n : 32;
+  int tx_log2 = 0;
+  while ((1 << tx_log2) < tx) ++tx_log2;
+  const int ty = 256 / tx;
+  constexpr int kChunk = 2048;  // probes listed per launch (24 KB of shared memory)
+  const dim3 grid((unsigned)(F / tx), (unsigned)(F / ty));
   for (int c0 = 0; c0 < nb; c0 += kChunk) {  // chunks add into dv in probe order
     const int cn = nb - c0 < kChunk ? nb - c0 : kChunk;
-    k_reduce_dv_win<<<(unsigned)((ff + threads - 1) / threads), threads, 2 * sizeof(int) * (size_t)cn, st>>>(
-        contrib + (size_t)c0 * M * n * n, cn, M, n, F, win ? win + 2 * (size_t)c0 : nullptr, dv, sy, sx, ss, s);
+    k_reduce_dv_win<<<grid, 256, 3 * sizeof(int) * (size_t)cn, st>>>(
+        contrib + (size_t)c0 * M * n * n, cn, M, n, F, win ? win + 2 * (size_t)c0 : nullptr, dv, sy, sx, ss, s,
+        tx_log2);
     int rc = check_launch("k_reduce_dv_win");
     if (rc) return rc;
   }
