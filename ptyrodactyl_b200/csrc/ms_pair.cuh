@@ -101,12 +101,20 @@ struct PairGeom {
 // exchange buffers, instead of 16-byte loads and stores per row and lane pair; the
 // wait on the copy's mbarrier gives up after a bounded number of polls and counts
 // the failure in g_pair_wait_timeouts.
-template <int N1, int N2, int AXIS, int WARPS, int MINB, bool PRE, bool DIRECT = false, bool TMA = false>
+// GEN: the first and last slice passes too: op1 may be OP_IFFT (the wave arrives
+// transformed along this axis; inverse transform and a.scale instead of finishing a
+// convolution) and op2 OP_FFT (forward transform instead of starting one). With
+// N1 == N2 a thread's k-order positions are its natural ones (t + N1 r), so loads
+// and stores are unchanged.
+template <int N1, int N2, int AXIS, int WARPS, int MINB, bool PRE, bool DIRECT = false, bool TMA = false,
+          bool GEN = false>
 __global__ void __launch_bounds__(WARPS * 32, MINB)
     ms_pass_pair_kernel(PassArgs a, const __grid_constant__ CUtensorMap wmap) {
   using PG = PairGeom<N1, N2, WARPS, PRE>;
   using PB = PairBuf<N1, N2>;
   constexpr int N = PG::N, G = PG::G, lines = PG::kLines, pitch = PG::kPitch;
+  static_assert(!GEN || N1 == N2, "first / last passes need k-order positions equal to natural ones");
+  const int op1 = GEN ? a.op1 : (int)OP_CONV, op2 = GEN ? a.op2 : (int)OP_CONV;
   static_assert(!TMA || (AXIS == 1 && DIRECT && !PRE && N <= 256), "TMA moves whole columns of a direct column pass");
   constexpr uint32_t kWarpBytes = sizeof(float2) * 2 * G * N;  // one warp's column block
   static_assert(!TMA || sizeof(Pair) * G * PB::kSize >= kWarpBytes + 127,
@@ -189,11 +197,17 @@ __global__ void __launch_bounds__(WARPS * 32, MINB)
     __syncthreads();  // the tile becomes the exchange buffers
   }
 
-  // ---- finish slice s-1's convolution along this axis
-  line_nat_to_k<N1, N2, -1>(v, t, buf, tw);
+  // ---- finish slice s-1's convolution along this axis (or the probe's inverse transform)
+  if (op1 == OP_IFFT) {
+    line_k_to_nat<N1, N2, +1>(v, t, buf, tw);
 #pragma unroll
-  for (int r = 0; r < N2; ++r) v[r] = cmul(v[r], pfs[korder_index<N1, N2>(t, r)]);
-  line_k_to_nat<N1, N2, +1>(v, t, buf, tw);
+    for (int j = 0; j < N2; ++j) v[j] = cscale(v[j], a.scale);
+  } else {
+    line_nat_to_k<N1, N2, -1>(v, t, buf, tw);
+#pragma unroll
+    for (int r = 0; r < N2; ++r) v[r] = cmul(v[r], pfs[korder_index<N1, N2>(t, r)]);
+    line_k_to_nat<N1, N2, +1>(v, t, buf, tw);
+  }
 
   // ---- transmission T_s (row-major table for rows, transposed for columns)
   if (PRE) {
@@ -225,11 +239,15 @@ __global__ void __launch_bounds__(WARPS * 32, MINB)
     }
   }
 
-  // ---- start slice s's convolution along this axis
-  line_nat_to_k<N1, N2, -1>(v, t, buf, tw);
+  // ---- start slice s's convolution along this axis (or the far field's forward transform)
+  if (op2 == OP_FFT) {
+    line_nat_to_k<N1, N2, -1>(v, t, buf, tw);
+  } else {
+    line_nat_to_k<N1, N2, -1>(v, t, buf, tw);
 #pragma unroll
-  for (int r = 0; r < N2; ++r) v[r] = cmul(v[r], pfs[korder_index<N1, N2>(t, r)]);
-  line_k_to_nat<N1, N2, +1>(v, t, buf, tw);
+    for (int r = 0; r < N2; ++r) v[r] = cmul(v[r], pfs[korder_index<N1, N2>(t, r)]);
+    line_k_to_nat<N1, N2, +1>(v, t, buf, tw);
+  }
 
   // ---- store
   if (AXIS == 0) {

@@ -414,6 +414,14 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) ms_pass_kernel(PassArgs a) {
 }
 
 // a pass running the middle-slice program (see pass_body's STEADY)
+// The first (op1 = IFFT) and last (op2 = FFT) slice passes: wave in, one T multiply,
+// wave out, no tilt.
+inline bool is_edge_slice_pass(const PassArgs& a) {
+  return a.src == SRC_WAVE && a.dst == DST_WAVE && a.t_slice >= 0 && !a.t_conj && a.tilt == nullptr &&
+         (a.op1 == OP_IFFT || a.op1 == OP_CONV) && (a.op2 == OP_FFT || a.op2 == OP_CONV) &&
+         !(a.op1 == OP_CONV && a.op2 == OP_CONV);
+}
+
 inline bool is_steady_pass(const PassArgs& a) {
   return a.src == SRC_WAVE && a.op1 == OP_CONV && a.op2 == OP_CONV && a.dst == DST_WAVE && a.t_slice >= 0 &&
          !a.t_conj;

@@ -171,19 +171,21 @@ int launch_pipe_t(const PassArgs& a, int nslots, cudaStream_t st) {
 }
 
 // Steady passes with two lines per thread in paired FP32 arithmetic (ms_pair.cuh).
-template <int N1, int N2, int AXIS, int W, int MINB, bool PRE, bool DIRECT = false, bool TMA = false>
+template <int N1, int N2, int AXIS, int W, int MINB, bool PRE, bool DIRECT = false, bool TMA = false,
+          bool GEN = false>
 int launch_pair_w(const PassArgs& a, int grid_y, cudaStream_t st, const CUtensorMap* wmap = nullptr) {
   using PG = PairGeom<N1, N2, W, PRE>;
   const size_t smem = PG::smem_bytes();
   static bool attr_done = false;
   if (!attr_done) {
-    cudaFuncSetAttribute(ms_pass_pair_kernel<N1, N2, AXIS, W, MINB, PRE, DIRECT, TMA>,
+    cudaFuncSetAttribute(ms_pass_pair_kernel<N1, N2, AXIS, W, MINB, PRE, DIRECT, TMA, GEN>,
                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     attr_done = true;
   }
   static const CUtensorMap kNoMap = {};
   dim3 grid(PG::N / PG::kLines, grid_y);
-  ms_pass_pair_kernel<N1, N2, AXIS, W, MINB, PRE, DIRECT, TMA><<<grid, W * 32, smem, st>>>(a, wmap ? *wmap : kNoMap);
+  ms_pass_pair_kernel<N1, N2, AXIS, W, MINB, PRE, DIRECT, TMA, GEN>
+      <<<grid, W * 32, smem, st>>>(a, wmap ? *wmap : kNoMap);
   g_launches.fetch_add(1, std::memory_order_relaxed);
   return (int)cudaGetLastError();
 }
@@ -262,6 +264,22 @@ int launch_pass_t(const PassArgs& a0, int grid_y, cudaStream_t st, int variant) 
   }
   if (is_steady_pass(a) && (variant & 16) && a.pf != nullptr)
     return launch_pair_t<N1, N2, AXIS>(a, grid_y, st, variant);
+  if constexpr (N1 == N2 && N1 * N2 == 256) {
+    // tune bit 12 (4096, with bits 4, 6 and 7): the first and last slice passes run the
+    // paired kernel too (column passes with TMA blocks when bit 11 is set)
+    if ((variant & 4096) && (variant & 16) && (variant & 64) && (variant & 128) && is_edge_slice_pass(a) &&
+        a.pf != nullptr) {
+      constexpr int G = 32 / N1;
+      if constexpr (AXIS == 1) {
+        CUtensorMap wmap;
+        if ((variant & 2048) && wave_tensor_map(a.wave, N1 * N2, grid_y, 2 * G, &wmap))
+          return launch_pair_w<N1, N2, AXIS, 8, 2, false, true, true, true>(a, grid_y, st, &wmap);
+        return launch_pair_w<N1, N2, AXIS, 8, 2, false, true, false, true>(a, grid_y, st);
+      } else {
+        return launch_pair_w<N1, N2, AXIS, 8, 2, false, false, false, true>(a, grid_y, st);
+      }
+    }
+  }
   if (is_steady_pass(a) && a.tw2 != nullptr && (variant & 4)) return launch_pipe_t<N1, N2, AXIS, MINB>(a, grid_y, st);
   return is_steady_pass(a) ? launch_pass_s<N1, N2, AXIS, MINB, true>(a, grid_y, st)
                            : launch_pass_s<N1, N2, AXIS, MINB, false>(a, grid_y, st);

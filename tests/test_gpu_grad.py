@@ -172,15 +172,15 @@ def test_windowed_forward_and_vjp_match_oracle():
 @pytest.mark.parametrize("n", [128, 256])
 def test_gradient_identical_across_launch_variants(n):
     """Checkpointing forward passes in the paired kernel (at 256 also with TMA column
-    blocks, tune bit 2048) give the scalar kernel's residuals, hence identical
-    gradients."""
+    blocks, tune bit 2048, and paired first / last slice passes, bit 4096) give the
+    scalar kernel's residuals, hence identical gradients."""
     pot, modes, w, pos, g = _case(n, 6, 2, 4, seed=9)
     dev = torch.device("cuda")
     args = [torch.as_tensor(pot, dtype=torch.float32, device=dev), torch.as_tensor(modes.astype(np.complex64), device=dev),
             torch.as_tensor(w, dtype=torch.float32, device=dev), torch.as_tensor(pos, dtype=torch.float64, device=dev),
             torch.as_tensor(g, dtype=torch.float32, device=dev), 1.7, 200.0, 0.3]
     ref = pb.vjp(*args, ckpt_every=2, tune=3)
-    for tune in (19, 147, 211, 2259):
+    for tune in (19, 147, 211, 2259, 6355):
         got = pb.vjp(*args, ckpt_every=2, tune=tune)
         for a, b in zip(ref, got):
             assert torch.equal(a, b), tune
