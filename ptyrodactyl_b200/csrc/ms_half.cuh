@@ -96,9 +96,8 @@ __device__ __forceinline__ void half_k_to_nat(Pair (&p)[N1], int t, float2* buf,
 // in and goes back as N / 256 tiled TMA copies of 256 rows (wmap: the slots as a 3-D
 // tensor (x, y, slot), box G x 256 x 1) through its own exchange buffers, instead of
 // the CTA's column tile and its barriers; bounded mbarrier wait as in ms_pair.cuh.
-template <int N1, int N2, int AXIS, int WARPS, int MINB, bool TMA = false>
-__global__ void __launch_bounds__(WARPS * 32, MINB)
-    ms_pass_half_kernel(PassArgs a, const __grid_constant__ CUtensorMap wmap) {
+template <int N1, int N2, int AXIS, int WARPS, bool TMA>
+__device__ __forceinline__ void half_body(const PassArgs& a, const int slot, const CUtensorMap& wmap) {
   using Geo = PassGeom<N1, N2>;
   using LB = LineBuf<N1, N2>;
   constexpr int N = Geo::N, G = Geo::G, H = N1;
@@ -128,7 +127,7 @@ __global__ void __launch_bounds__(WARPS * 32, MINB)
       mbar_expect_tx(bar, kWarpBytes);
 #pragma unroll
       for (int y = 0; y < N; y += kBoxRows)
-        tma_load_3d(smem_u32(stg + (size_t)y * G), &wmap, blockIdx.x * lines + wp * G, y, blockIdx.y, bar);
+        tma_load_3d(smem_u32(stg + (size_t)y * G), &wmap, blockIdx.x * lines + wp * G, y, slot, bar);
     }
   }
   for (int i = threadIdx.x; i < N; i += blockDim.x) {
@@ -143,7 +142,6 @@ __global__ void __launch_bounds__(WARPS * 32, MINB)
   const int lc = warp * G + gl;
   const int line0 = blockIdx.x * lines;
   const int line = line0 + lc;
-  const int slot = blockIdx.y;
   float2* buf = work + lc * LB::kSize;
   float2* w = a.wave + (size_t)slot * N * N;
   auto off = [&](int e) -> size_t { return AXIS == 0 ? (size_t)line * N + e : (size_t)e * N + line; };
@@ -231,6 +229,28 @@ __global__ void __launch_bounds__(WARPS * 32, MINB)
     __syncthreads();
     tile_store<N, lines, pitch, WARPS * 32>(w, work, line0);
   }
+}
+
+template <int N1, int N2, int AXIS, int WARPS, int MINB, bool TMA = false>
+__global__ void __launch_bounds__(WARPS * 32, MINB)
+    ms_pass_half_kernel(PassArgs a, const __grid_constant__ CUtensorMap wmap) {
+  half_body<N1, N2, AXIS, WARPS, TMA>(a, blockIdx.y, wmap);
+}
+
+// Steady passes of several jobs in one launch (the scheduler's half-paired rows):
+// CTA row y works on slot rows[y].y of the job descs[rows[y].x], copied into shared
+// memory once per CTA; column passes stage through the CTA's column tile.
+template <int N1, int N2, int AXIS, int WARPS, int MINB>
+__global__ void __launch_bounds__(WARPS * 32, MINB)
+    ms_pass_half_multi_kernel(const PassArgs* __restrict__ descs, const int2* __restrict__ rows) {
+  __shared__ __align__(16) PassArgs sa;
+  const int2 r = rows[blockIdx.y];
+  const uint32_t* src = reinterpret_cast<const uint32_t*>(descs + r.x);
+  uint32_t* dst = reinterpret_cast<uint32_t*>(&sa);
+  for (int i = threadIdx.x; i < (int)(sizeof(PassArgs) / 4); i += blockDim.x) dst[i] = src[i];
+  __syncthreads();
+  const CUtensorMap none = {};
+  half_body<N1, N2, AXIS, WARPS, false>(sa, r.y, none);
 }
 
 }  // namespace ptyro

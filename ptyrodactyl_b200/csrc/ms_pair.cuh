@@ -106,10 +106,8 @@ struct PairGeom {
 // convolution) and op2 OP_FFT (forward transform instead of starting one). With
 // N1 == N2 a thread's k-order positions are its natural ones (t + N1 r), so loads
 // and stores are unchanged.
-template <int N1, int N2, int AXIS, int WARPS, int MINB, bool PRE, bool DIRECT = false, bool TMA = false,
-          bool GEN = false>
-__global__ void __launch_bounds__(WARPS * 32, MINB)
-    ms_pass_pair_kernel(PassArgs a, const __grid_constant__ CUtensorMap wmap) {
+template <int N1, int N2, int AXIS, int WARPS, bool PRE, bool DIRECT, bool TMA, bool GEN>
+__device__ __forceinline__ void pair_body(const PassArgs& a, const int slot, const CUtensorMap& wmap) {
   using PG = PairGeom<N1, N2, WARPS, PRE>;
   using PB = PairBuf<N1, N2>;
   constexpr int N = PG::N, G = PG::G, lines = PG::kLines, pitch = PG::kPitch;
@@ -137,7 +135,7 @@ __global__ void __launch_bounds__(WARPS * 32, MINB)
       mbar_init(bar, 1);
       asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
       mbar_expect_tx(bar, kWarpBytes);
-      tma_load_3d(smem_u32(stg), &wmap, blockIdx.x * lines + wp * 2 * G, 0, blockIdx.y, bar);
+      tma_load_3d(smem_u32(stg), &wmap, blockIdx.x * lines + wp * 2 * G, 0, slot, bar);
     }
   }
   for (int i = threadIdx.x; i < N; i += blockDim.x) {
@@ -153,7 +151,6 @@ __global__ void __launch_bounds__(WARPS * 32, MINB)
   const int lp = warp * G + gl;  // line pair within the CTA
   const int line0 = blockIdx.x * lines;
   const int la = line0 + 2 * lp, lb = la + 1;
-  const int slot = blockIdx.y;
   Pair* buf = xbuf + lp * PB::kSize;
   float2* w = a.wave + (size_t)slot * N * N;
   float2* tpre = reinterpret_cast<float2*>(reinterpret_cast<char*>(work) + PG::kWork) + (size_t)(2 * lp) * N;
@@ -282,6 +279,30 @@ __global__ void __launch_bounds__(WARPS * 32, MINB)
     __syncthreads();
     tile_store<N, lines, pitch, WARPS * 32>(w, work, line0);
   }
+}
+
+template <int N1, int N2, int AXIS, int WARPS, int MINB, bool PRE, bool DIRECT = false, bool TMA = false,
+          bool GEN = false>
+__global__ void __launch_bounds__(WARPS * 32, MINB)
+    ms_pass_pair_kernel(PassArgs a, const __grid_constant__ CUtensorMap wmap) {
+  pair_body<N1, N2, AXIS, WARPS, PRE, DIRECT, TMA, GEN>(a, blockIdx.y, wmap);
+}
+
+// Steady passes of several jobs in one launch (the scheduler's paired rows): CTA row
+// y works on slot rows[y].y of the job whose arguments are descs[rows[y].x], copied
+// into shared memory once per CTA. Column passes read their column pairs directly.
+template <int N1, int N2, int AXIS, int WARPS, int MINB>
+__global__ void __launch_bounds__(WARPS * 32, MINB)
+    ms_pass_pair_multi_kernel(const PassArgs* __restrict__ descs, const int2* __restrict__ rows) {
+  __shared__ __align__(16) PassArgs sa;
+  const int2 r = rows[blockIdx.y];
+  static_assert(sizeof(PassArgs) % 4 == 0, "descriptor copy in 32-bit words");
+  const uint32_t* src = reinterpret_cast<const uint32_t*>(descs + r.x);
+  uint32_t* dst = reinterpret_cast<uint32_t*>(&sa);
+  for (int i = threadIdx.x; i < (int)(sizeof(PassArgs) / 4); i += blockDim.x) dst[i] = src[i];
+  __syncthreads();
+  const CUtensorMap none = {};
+  pair_body<N1, N2, AXIS, WARPS, false, AXIS == 1, false, false>(sa, r.y, none);
 }
 
 }  // namespace ptyro

@@ -77,6 +77,23 @@ static int launch_pass_multi(int n, int axis, const PassArgs* d, const int2* r, 
   return rc ? fail(PTYRO_ERR_CUDA, std::string("ms_pass_multi_kernel: ") + cudaGetErrorString((cudaError_t)rc)) : 0;
 }
 
+// paired steady passes of several jobs (grid edges up to 512)
+static int launch_pass_pair_multi(int n, int axis, const PassArgs* d, const int2* r, int nr, cudaStream_t st) {
+  if (nr <= 0) return PTYRO_OK;
+  int rc;
+  switch (n) {
+    case 16: rc = launch_pass_pair_multi_16(axis, d, r, nr, st); break;
+    case 32: rc = launch_pass_pair_multi_32(axis, d, r, nr, st); break;
+    case 64: rc = launch_pass_pair_multi_64(axis, d, r, nr, st); break;
+    case 128: rc = launch_pass_pair_multi_128(axis, d, r, nr, st); break;
+    case 256: rc = launch_pass_pair_multi_256(axis, d, r, nr, st); break;
+    case 512: rc = launch_pass_pair_multi_512(axis, d, r, nr, st); break;
+    default: return fail(PTYRO_ERR_UNSUPPORTED, "paired multi-job pass: grid edge not served");
+  }
+  if (rc != 0) return fail(PTYRO_ERR_CUDA, std::string("ms_pass_pair_multi_kernel: ") + cudaGetErrorString((cudaError_t)rc));
+  return PTYRO_OK;
+}
+
 static int launch_bwd_multi(int n, int axis, const BwdArgs* d, const int2* r, int nr, cudaStream_t st) {
   if (nr <= 0) return PTYRO_OK;
   int rc;
@@ -323,7 +340,9 @@ static int finish_job(Job& j, GridClass& c) {
 struct TickRows {
   std::vector<PassArgs> fdesc;
   std::vector<BwdArgs> bdesc;
-  std::vector<int2> rows[4];  // forward axis 0, forward axis 1, adjoint axis 0, adjoint axis 1
+  // forward axis 0, forward axis 1, adjoint axis 0, adjoint axis 1, paired steady
+  // forward axis 0, paired steady forward axis 1
+  std::vector<int2> rows[6];
 };
 
 // one pass of every running job of grid class c
@@ -353,7 +372,10 @@ static int tick_class(ptyro_sched* s, GridClass& c, std::vector<Job*>& jobs) {
                                       j->plan.grad ? j->plan.C : 0, j->b0, j->nb, j->k);
       const int di = (int)t.fdesc.size();
       t.fdesc.push_back(f.a);
-      for (int r = 0; r < f.rows; ++r) t.rows[f.axis].push_back(make_int2(di, r));
+      // steady passes of grids up to 512 run in paired arithmetic (two lines per thread
+      // up to 256, the two halves of each line at 512)
+      const int table = (p->n <= 512 && is_steady_pass(f.a)) ? 4 + f.axis : f.axis;
+      for (int r = 0; r < f.rows; ++r) t.rows[table].push_back(make_int2(di, r));
       if (j->plan.grad && j->k == S + 1) fl.loss = true;
     } else {
       const BwdBuffers b = job_bwd_buffers(*j);
@@ -370,7 +392,7 @@ static int tick_class(ptyro_sched* s, GridClass& c, std::vector<Job*>& jobs) {
   }
   // upload descriptors and rows through the staging ring
   size_t bytes = align_up(t.fdesc.size() * sizeof(PassArgs)) + align_up(t.bdesc.size() * sizeof(BwdArgs));
-  for (int i = 0; i < 4; ++i) bytes += align_up(t.rows[i].size() * sizeof(int2));
+  for (int i = 0; i < 6; ++i) bytes += align_up(t.rows[i].size() * sizeof(int2));
   if (bytes > s->stage_bytes) return fail(PTYRO_ERR_INVALID, "tick descriptors exceed the staging buffer");
   const int slot = c.next;
   c.next = (c.next + 1) % GridClass::kRing;
@@ -384,8 +406,8 @@ static int tick_class(ptyro_sched* s, GridClass& c, std::vector<Job*>& jobs) {
   const BwdArgs* bd = (const BwdArgs*)(dptr + o);
   memcpy(h + o, t.bdesc.data(), t.bdesc.size() * sizeof(BwdArgs));
   o += align_up(t.bdesc.size() * sizeof(BwdArgs));
-  const int2* rows[4];
-  for (int i = 0; i < 4; ++i) {
+  const int2* rows[6];
+  for (int i = 0; i < 6; ++i) {
     rows[i] = (const int2*)(dptr + o);
     memcpy(h + o, t.rows[i].data(), t.rows[i].size() * sizeof(int2));
     o += align_up(t.rows[i].size() * sizeof(int2));
@@ -396,6 +418,8 @@ static int tick_class(ptyro_sched* s, GridClass& c, std::vector<Job*>& jobs) {
   const int tune = 3;
   if ((rc = launch_pass_multi(c.n, 0, fd, rows[0], (int)t.rows[0].size(), c.stream, tune))) return rc;
   if ((rc = launch_pass_multi(c.n, 1, fd, rows[1], (int)t.rows[1].size(), c.stream, tune))) return rc;
+  if ((rc = launch_pass_pair_multi(c.n, 0, fd, rows[4], (int)t.rows[4].size(), c.stream))) return rc;
+  if ((rc = launch_pass_pair_multi(c.n, 1, fd, rows[5], (int)t.rows[5].size(), c.stream))) return rc;
   if ((rc = launch_bwd_multi(c.n, 0, bd, rows[2], (int)t.rows[2].size(), c.stream))) return rc;
   if ((rc = launch_bwd_multi(c.n, 1, bd, rows[3], (int)t.rows[3].size(), c.stream))) return rc;
   // per-job follow-up kernels, then advance
@@ -461,8 +485,8 @@ int ptyro_sched_create(int32_t device, void* arena, size_t arena_bytes, int32_t 
   s->max_slots = max_slots;
   s->arena.init((char*)arena, arena_bytes);
   s->arena_bytes = arena_bytes;
-  // per tick: up to max_slots rows in each of 4 tables plus one descriptor per job
-  s->stage_bytes = align_up((size_t)4 * max_slots * sizeof(int2) + (size_t)max_slots * (sizeof(PassArgs) +
+  // per tick: up to max_slots rows in each of 6 tables plus one descriptor per job
+  s->stage_bytes = align_up((size_t)6 * max_slots * sizeof(int2) + (size_t)max_slots * (sizeof(PassArgs) +
                                                                                         sizeof(BwdArgs)) + 4096);
   *out = s;
   return PTYRO_OK;

@@ -302,6 +302,47 @@ int launch_pass_multi_t(const PassArgs* descs, const int2* rows, int nrows, cuda
   return (int)cudaGetLastError();
 }
 
+// Steady forward passes of several jobs with two lines per thread (N <= 256) or the
+// two halves of each line paired (512); returns -1 where no paired kernel serves the
+// shape.
+template <int N1, int N2, int AXIS>
+int launch_pass_pair_multi_t(const PassArgs* descs, const int2* rows, int nrows, cudaStream_t st) {
+  if constexpr (N1 * N2 == 512 && N2 == 2 * N1) {  // half-paired lines (ms_half.cuh), 2 CTAs per SM
+    using Geo = PassGeom<N1, N2>;
+    constexpr int W = Geo::kWarps;
+    const size_t smem = Geo::smem_bytes(W);
+    static bool attr_done = false;
+    if (!attr_done) {
+      cudaFuncSetAttribute(ms_pass_half_multi_kernel<N1, N2, AXIS, W, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)smem);
+      attr_done = true;
+    }
+    dim3 grid(Geo::N / Geo::kLines, nrows);
+    ms_pass_half_multi_kernel<N1, N2, AXIS, W, 2><<<grid, W * 32, smem, st>>>(descs, rows);
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    return (int)cudaGetLastError();
+  } else if constexpr (N1 * N2 > 256) {
+    return -1;
+  } else {
+    constexpr int G = 32 / N1;
+    constexpr int N = N1 * N2;
+    constexpr int W = N == 256 ? 8 : (N / (2 * G) < 4 ? N / (2 * G) : 4);
+    constexpr int MINB = 16 / W;
+    using PG = PairGeom<N1, N2, W, false>;
+    const size_t smem = PG::smem_bytes();
+    static bool attr_done = false;
+    if (!attr_done) {
+      cudaFuncSetAttribute(ms_pass_pair_multi_kernel<N1, N2, AXIS, W, MINB>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      attr_done = true;
+    }
+    dim3 grid(N / PG::kLines, nrows);
+    ms_pass_pair_multi_kernel<N1, N2, AXIS, W, MINB><<<grid, W * 32, smem, st>>>(descs, rows);
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    return (int)cudaGetLastError();
+  }
+}
+
 template <int N1, int N2, int AXIS>
 int launch_bwd_multi_t(const BwdArgs* descs, const int2* rows, int nrows, cudaStream_t st) {
   using Geo = PassGeom<N1, N2>;
@@ -353,24 +394,35 @@ int launch_bwd_multi_t(const BwdArgs* descs, const int2* rows, int nrows, cudaSt
       return occ ? launch_pass_multi_t<N1, N2, 0, hi>(d, r, nr, st) : launch_pass_multi_t<N1, N2, 0, lo>(d, r, nr, st); \
     return occ ? launch_pass_multi_t<N1, N2, 1, hi>(d, r, nr, st) : launch_pass_multi_t<N1, N2, 1, lo>(d, r, nr, st);   \
   }                                                                                              \
+  int launch_pass_pair_multi_##NN(int axis, const PassArgs* d, const int2* r, int nr, cudaStream_t st) { \
+    return axis == 0 ? launch_pass_pair_multi_t<N1, N2, 0>(d, r, nr, st)                         \
+                     : launch_pass_pair_multi_t<N1, N2, 1>(d, r, nr, st);                        \
+  }                                                                                              \
   int launch_bwd_multi_##NN(int axis, const BwdArgs* d, const int2* r, int nr, cudaStream_t st) {  \
     return axis == 0 ? launch_bwd_multi_t<N1, N2, 0>(d, r, nr, st) : launch_bwd_multi_t<N1, N2, 1>(d, r, nr, st); \
   }
 
 int launch_pass_multi_16(int axis, const PassArgs* d, const int2* r, int nr, cudaStream_t st, int variant);
 int launch_bwd_multi_16(int axis, const BwdArgs* d, const int2* r, int nr, cudaStream_t st);
+int launch_pass_pair_multi_16(int axis, const PassArgs* d, const int2* r, int nr, cudaStream_t st);
 int launch_pass_multi_32(int axis, const PassArgs* d, const int2* r, int nr, cudaStream_t st, int variant);
 int launch_bwd_multi_32(int axis, const BwdArgs* d, const int2* r, int nr, cudaStream_t st);
+int launch_pass_pair_multi_32(int axis, const PassArgs* d, const int2* r, int nr, cudaStream_t st);
 int launch_pass_multi_64(int axis, const PassArgs* d, const int2* r, int nr, cudaStream_t st, int variant);
 int launch_bwd_multi_64(int axis, const BwdArgs* d, const int2* r, int nr, cudaStream_t st);
+int launch_pass_pair_multi_64(int axis, const PassArgs* d, const int2* r, int nr, cudaStream_t st);
 int launch_pass_multi_128(int axis, const PassArgs* d, const int2* r, int nr, cudaStream_t st, int variant);
 int launch_bwd_multi_128(int axis, const BwdArgs* d, const int2* r, int nr, cudaStream_t st);
+int launch_pass_pair_multi_128(int axis, const PassArgs* d, const int2* r, int nr, cudaStream_t st);
 int launch_pass_multi_256(int axis, const PassArgs* d, const int2* r, int nr, cudaStream_t st, int variant);
 int launch_bwd_multi_256(int axis, const BwdArgs* d, const int2* r, int nr, cudaStream_t st);
+int launch_pass_pair_multi_256(int axis, const PassArgs* d, const int2* r, int nr, cudaStream_t st);
 int launch_pass_multi_512(int axis, const PassArgs* d, const int2* r, int nr, cudaStream_t st, int variant);
 int launch_bwd_multi_512(int axis, const BwdArgs* d, const int2* r, int nr, cudaStream_t st);
+int launch_pass_pair_multi_512(int axis, const PassArgs* d, const int2* r, int nr, cudaStream_t st);
 int launch_pass_multi_1024(int axis, const PassArgs* d, const int2* r, int nr, cudaStream_t st, int variant);
 int launch_bwd_multi_1024(int axis, const BwdArgs* d, const int2* r, int nr, cudaStream_t st);
+int launch_pass_pair_multi_1024(int axis, const PassArgs* d, const int2* r, int nr, cudaStream_t st);
 int launch_jvp_16(int axis, const JvpArgs& a, int grid_y, cudaStream_t st);
 int launch_jvp_32(int axis, const JvpArgs& a, int grid_y, cudaStream_t st);
 int launch_jvp_64(int axis, const JvpArgs& a, int grid_y, cudaStream_t st);

@@ -21,7 +21,7 @@ def server():
         pytest.skip("no CUDA device")
     srv = Server(arena_bytes=4 << 30, max_slots=512)
     rng = np.random.default_rng(0)
-    for n in (64, 128, 256):
+    for n in (64, 128, 256, 512):
         srv.add_potential(f"p{n}", rng.uniform(0.0, 40.0, (n, n, 24)).astype(np.float32))
     yield srv
     srv.close()
@@ -52,7 +52,7 @@ def test_single_job_equals_direct_forward(server):
 
 def test_mixed_jobs_equal_alone(server):
     reqs = [_req(64, 5, 33, seed=2), _req(128, 12, 70, seed=3), _req(256, 3, 9, seed=4), _req(64, 20, 1, seed=5),
-            _req(128, 1, 40, seed=6), _req(256, 9, 65, seed=7)]
+            _req(128, 1, 40, seed=6), _req(256, 9, 65, seed=7), _req(512, 5, 3, seed=10)]
     n0 = len(server.finished)
     # staggered: half submitted, a few ticks, then the rest join the running ones
     for r in reqs[:3]:
