@@ -384,7 +384,8 @@ def run_ours(args, rank, world, local_rank):
             "gpu_launches": int(launches),
             "clocks": clk,
             "cpu_baseline": cpu_baseline,
-            "checks": {"pattern_sum_max_rel_err": max_sum_err},
+            "checks": {"pattern_sum_max_rel_err": max_sum_err,
+                       "tma_wait_timeouts": int(lib.ptyro_pass_wait_timeouts())},
         }
         print(json.dumps(line), flush=True)
 
@@ -534,6 +535,7 @@ def run_config3(args, rank, world, local_rank):
     on a sample of the 128x128 scan (``--probes``); one JSON line."""
     import torch
     import ptyrodactyl_b200 as pb
+    from ptyrodactyl_b200 import _lib
 
     dev = torch.device("cuda", local_rank)
     torch.cuda.set_device(dev)
@@ -572,7 +574,8 @@ def run_config3(args, rank, world, local_rank):
             "mode": "config3", "value": updates / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms,
             "tflops_algorithmic": updates / (ms * 1e-3) * synth.algorithmic_flops_per_update(n) / 1e12,
             "n_gpus": world, "dtype": "f32", "data": "synthetic",
-            "checks": {"pattern_sum_max_rel_err": float(((sums - n_ap).abs().max() / n_ap).item())},
+            "checks": {"pattern_sum_max_rel_err": float(((sums - n_ap).abs().max() / n_ap).item()),
+                       "tma_wait_timeouts": int(_lib.load().ptyro_pass_wait_timeouts())},
             "config": {"workload": w.name, "grid": n, "slices": S, "probes_sampled": args.probes,
                        "probes_full_scan": w.num_probes, "phonon_configs": len(pots), "batch": args.batch,
                        "tune": default_tune(w.n) if args.tune < 0 else args.tune}}
