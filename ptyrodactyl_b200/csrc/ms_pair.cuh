@@ -44,7 +44,7 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, int lim
   }
   return false;
 }
-// plain (non-multicast) 3-D tiled TMA load of box (x, y, z) into this CTA's shared memory
+// plain 3-D tiled TMA load of box (x, y, z) into this CTA's own shared memory only
 __device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap* map, int x, int y, int z, uint32_t bar) {
   asm volatile(
       "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];" ::
