@@ -108,7 +108,8 @@ static __global__ void k_propagator2d(int n, double calib, double lam_dz, float2
 // transmission_func (simulations.py:105-159): T_s = exp(i sigma V_s), evaluated in
 // double and rounded once; written row-major (S, N, N) and transposed (S, N^T).
 static __global__ void k_transmission(const float* __restrict__ V, long long sy, long long sx, long long ss,
-                               int n, int S, double sigma, float2* __restrict__ T, float2* __restrict__ TT) {
+                               int n, int S, double sigma, float2* __restrict__ T, float2* __restrict__ TT,
+                               float* __restrict__ TP = nullptr, float* __restrict__ TPT = nullptr) {
   const size_t total = (size_t)S * n * n;
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
        i += (size_t)gridDim.x * blockDim.x) {
@@ -121,6 +122,14 @@ static __global__ void k_transmission(const float* __restrict__ V, long long sy,
     const float2 v = make_float2((float)cs, (float)sn);
     T[i] = v;
     TT[(size_t)s * n * n + (size_t)x * n + y] = v;
+    if (TP) {  // line-pair interleaved copies: component (line & 1) holds re, 2 + (line & 1) im
+      const size_t pr = (((size_t)s * (n / 2) + (size_t)(y >> 1)) * n + x) * 4 + (y & 1);
+      TP[pr] = v.x;
+      TP[pr + 2] = v.y;
+      const size_t pc = (((size_t)s * (n / 2) + (size_t)(x >> 1)) * n + y) * 4 + (x & 1);
+      TPT[pc] = v.x;
+      TPT[pc + 2] = v.y;
+    }
   }
 }
 
@@ -276,8 +285,9 @@ static bool is_pow2(int n) { return n > 0 && (n & (n - 1)) == 0; }
 static int field_of(const ptyro_ms_params* p) { return p->field_n > 0 ? p->field_n : p->n; }
 
 struct Layout {
-  size_t tw, tw2, pf, trans, trans_t, probe_k, ramp_y, ramp_x, waves, p2, total;
+  size_t tw, tw2, pf, trans, trans_t, trans_p, trans_pt, probe_k, ramp_y, ramp_x, waves, p2, total;
   int batch;
+  bool paired_t;  // line-pair interleaved transmission tables present (tune bit 16384 at 256^2)
 };
 
 static int auto_batch(const ptyro_ms_params* p) {
@@ -301,6 +311,11 @@ static Layout layout_for(const ptyro_ms_params* p) {
   const size_t ff = (size_t)field_of(p) * field_of(p);
   L.trans = o; o = align_up(o + 8 * ff * p->num_slices);
   L.trans_t = o; o = align_up(o + 8 * ff * p->num_slices);
+  L.paired_t = p->n == 256 && (p->tune & 16384) && (p->tune & 16) && (p->tune & 64);
+  if (L.paired_t) {
+    L.trans_p = o; o = align_up(o + 8 * ff * p->num_slices);
+    L.trans_pt = o; o = align_up(o + 8 * ff * p->num_slices);
+  }
   L.probe_k = o; o = align_up(o + 8 * nn * p->num_modes);
   L.ramp_y = o; o = align_up(o + 8 * (size_t)p->n * L.batch);
   L.ramp_x = o; o = align_up(o + 8 * (size_t)p->n * L.batch);
@@ -366,7 +381,8 @@ static int forward_setup(const ptyro_ms_params* p, const Layout& L, char* ws, co
   const int F = field_of(p);
   k_transmission<<<blocks_for((size_t)F * F * p->num_slices, 256), 256, 0, st>>>(
       potential, p->pot_stride_y, p->pot_stride_x, p->pot_stride_s, F, p->num_slices,
-      interaction_sigma(p->voltage_kv), T, (float2*)(ws + L.trans_t));
+      interaction_sigma(p->voltage_kv), T, (float2*)(ws + L.trans_t),
+      L.paired_t ? (float*)(ws + L.trans_p) : nullptr, L.paired_t ? (float*)(ws + L.trans_pt) : nullptr);
   k_gather_modes<<<blocks_for(nn * p->num_modes, 256), 256, 0, st>>>(
       (const float2*)modes, p->mode_stride_y, p->mode_stride_x, p->mode_stride_m, n, p->num_modes, pk);
   int rc = check_launch("forward setup", 5);
@@ -385,6 +401,7 @@ struct FwdBuffers {
   float2* waves;
   const float2* probe_k;
   const float2 *ramp_y, *ramp_x, *trans, *trans_t, *pf, *tw, *tw2;
+  const float4 *trans_p, *trans_pt;  // or null
 };
 
 static FwdBuffers fwd_buffers(const Layout& L, char* ws) {
@@ -398,6 +415,8 @@ static FwdBuffers fwd_buffers(const Layout& L, char* ws) {
   b.pf = (const float2*)(ws + L.pf);
   b.tw = (const float2*)(ws + L.tw);
   b.tw2 = (const float2*)(ws + L.tw2);
+  b.trans_p = L.paired_t ? (const float4*)(ws + L.trans_p) : nullptr;
+  b.trans_pt = L.paired_t ? (const float4*)(ws + L.trans_pt) : nullptr;
   return b;
 }
 
@@ -431,6 +450,8 @@ static FwdPlan fwd_pass_plan(const ptyro_ms_params* p, const FwdBuffers& B, cons
   a.ramp_x = B.ramp_x;
   a.trans = B.trans;
   a.trans_t = B.trans_t;
+  a.trans_p = B.trans_p;
+  a.trans_pt = B.trans_pt;
   a.pf = B.pf;
   a.tw = B.tw;
   a.tw2 = B.tw2;

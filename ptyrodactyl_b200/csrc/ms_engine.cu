@@ -190,6 +190,10 @@ int ptyro_ms_steady_pass(const ptyro_ms_params* p, int32_t axis, int32_t reps, v
   a.wave = (float2*)(ws + L.waves);
   a.trans = (const float2*)(ws + L.trans);
   a.trans_t = (const float2*)(ws + L.trans_t);
+  if (L.paired_t) {  // written by the forward that filled this workspace
+    a.trans_p = (const float4*)(ws + L.trans_p);
+    a.trans_pt = (const float4*)(ws + L.trans_pt);
+  }
   a.pf = (const float2*)(ws + L.pf);
   a.tw = (const float2*)(ws + L.tw);
   a.n_modes = p->num_modes;

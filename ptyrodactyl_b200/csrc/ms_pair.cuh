@@ -89,6 +89,12 @@ struct PairGeom {
   }
 };
 
+// a * w with w = ((wA.x, wB.x), (wA.y, wB.y)): the operations of cmul(Pair, wA, wB)
+__device__ __forceinline__ Pair cmul_pp(Pair a, Pair w) {
+  return {__ffma2_rn(a.re, w.re, __fmul2_rn(a.im, make_float2(-w.im.x, -w.im.y))),
+          __ffma2_rn(a.re, w.im, __fmul2_rn(a.im, w.re))};
+}
+
 // PRE: the transmission rows of the thread's two lines are copied into shared
 // memory with cp.async at the start (each thread copies exactly the elements it
 // multiplies, so waiting for its own copies suffices); windows need PRE = false.
@@ -212,13 +218,32 @@ __device__ __forceinline__ void pair_body(const PassArgs& a, const int slot, con
 #pragma unroll
     for (int j = 0; j < N2; ++j) v[j] = cmul(v[j], tpre[t + N1 * j], tpre[N + t + N1 * j]);
   } else {
-    int oa, ob;
-    const float2* Ta = trans_row<AXIS>(a.trans, a.trans_t, a.field_n, a.t_slice, a.win, slot / a.n_modes, la, &oa);
-    const float2* Tb = trans_row<AXIS>(a.trans, a.trans_t, a.field_n, a.t_slice, a.win, slot / a.n_modes, lb, &ob);
+    // the pair's lines sit at field lines la + lo, la + 1 + lo: one interleaved entry
+    // serves both when lo is even (la is even)
+    const float4* TP = AXIS == 0 ? a.trans_p : a.trans_pt;
+    int lo = 0, eo = 0;
+    if (a.win) {
+      const int b = slot / a.n_modes;
+      lo = AXIS == 0 ? a.win[2 * b] : a.win[2 * b + 1];
+      eo = AXIS == 0 ? a.win[2 * b + 1] : a.win[2 * b];
+    }
     const int fm = a.field_n - 1;
+    if (TP != nullptr && (lo & 1) == 0) {
+      const float4* row =
+          TP + ((size_t)a.t_slice * (a.field_n / 2) + (size_t)(((la + lo) & fm) >> 1)) * a.field_n;
 #pragma unroll
-    for (int j = 0; j < N2; ++j)
-      v[j] = cmul(v[j], __ldg(Ta + ((t + N1 * j + oa) & fm)), __ldg(Tb + ((t + N1 * j + ob) & fm)));
+      for (int j = 0; j < N2; ++j) {
+        const float4 q = __ldg(row + ((t + N1 * j + eo) & fm));
+        v[j] = cmul_pp(v[j], {make_float2(q.x, q.y), make_float2(q.z, q.w)});
+      }
+    } else {
+      int oa, ob;
+      const float2* Ta = trans_row<AXIS>(a.trans, a.trans_t, a.field_n, a.t_slice, a.win, slot / a.n_modes, la, &oa);
+      const float2* Tb = trans_row<AXIS>(a.trans, a.trans_t, a.field_n, a.t_slice, a.win, slot / a.n_modes, lb, &ob);
+#pragma unroll
+      for (int j = 0; j < N2; ++j)
+        v[j] = cmul(v[j], __ldg(Ta + ((t + N1 * j + oa) & fm)), __ldg(Tb + ((t + N1 * j + ob) & fm)));
+    }
   }
 
   // gradient-mode checkpoint: the wave right after the T multiply

@@ -46,6 +46,11 @@ struct PassArgs {
   const float2* ramp_x;    // (B, N) shift ramp along x
   const float2* trans;     // (S, F, F) transmission exp(i sigma V), row-major [y][x]
   const float2* trans_t;   // (S, F, F) the same, transposed [x][y]
+  // the same interleaved by line pairs for paired passes, or null: trans_p[s][y/2][x] =
+  // (T[2p][x].re, T[2p+1][x].re, T[2p][x].im, T[2p+1][x].im) with p = y/2; trans_pt
+  // likewise over column pairs of trans_t
+  const float4* trans_p;
+  const float4* trans_pt;
   const int* win;          // (B, 2) window origins (y, x) in the field for this batch, or null
   int field_n;             // F (== N without windows); power of two
 

@@ -180,7 +180,7 @@ def test_gradient_identical_across_launch_variants(n):
             torch.as_tensor(w, dtype=torch.float32, device=dev), torch.as_tensor(pos, dtype=torch.float64, device=dev),
             torch.as_tensor(g, dtype=torch.float32, device=dev), 1.7, 200.0, 0.3]
     ref = pb.vjp(*args, ckpt_every=2, tune=3)
-    for tune in (19, 147, 211, 2259, 6355):
+    for tune in (19, 147, 211, 2259, 6355, 22739):
         got = pb.vjp(*args, ckpt_every=2, tune=tune)
         for a, b in zip(ref, got):
             assert torch.equal(a, b), tune

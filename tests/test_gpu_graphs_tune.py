@@ -86,9 +86,10 @@ def test_lanes_do_not_change_results():
 @pytest.mark.parametrize("n", [16, 32, 64, 128, 256, 512])
 def test_paired_steady_kernels_are_bit_identical(n):
     """Two-lines-per-thread f32x2 steady passes (tune bits 16, 32, 64, 128; at 256^2
-    also 2048: column blocks moved by TMA, and 4096: the first and last slice passes
-    paired) give exactly the one-line kernel's patterns, also with windows, and no
-    TMA wait gives up."""
+    also 2048: column blocks moved by TMA, 4096: the first and last slice passes
+    paired, 16384: line-pair interleaved transmission tables, used where the window
+    keeps a pair aligned) give exactly the one-line kernel's patterns, also with
+    windows, and no TMA wait gives up."""
     import numpy as np
     from oracle import multislice_ref as R
     from ptyrodactyl_b200.simulations import run_forward
@@ -101,14 +102,14 @@ def test_paired_steady_kernels_are_bit_identical(n):
     wt = torch.tensor([0.6, 0.4], device=dev)
     pos = torch.as_tensor(rng.uniform(-2, 2, (p, 2)), dtype=torch.float64, device=dev)
     ref = run_forward(slices, 1.7, modes, wt, pos, 200.0, 0.3, 0.3, tune=3, lanes=1)
-    for tune in (19, 51, 83, 147, 211, 2259, 6355, 4307):
+    for tune in (19, 51, 83, 147, 211, 2259, 6355, 4307, 22739):
         got = run_forward(slices, 1.7, modes, wt, pos, 200.0, 0.3, 0.3, tune=tune, lanes=1)
         assert torch.equal(got, ref), tune
     if n <= 256:
         field = torch.as_tensor(rng.uniform(0, 40, (2 * n, 2 * n, s)), dtype=torch.float32, device=dev)
         win = torch.as_tensor(rng.integers(0, 2 * n, (p, 2)), dtype=torch.int32, device=dev)
         ref = run_forward(field, 1.7, modes, wt, pos, 200.0, 0.3, 0.3, tune=3, windows=win, lanes=1)
-        for tune in (19, 51, 211, 2259, 6355):
+        for tune in (19, 51, 211, 2259, 6355, 22739):
             got = run_forward(field, 1.7, modes, wt, pos, 200.0, 0.3, 0.3, tune=tune, windows=win, lanes=1)
             assert torch.equal(got, ref), tune
     torch.cuda.synchronize()
