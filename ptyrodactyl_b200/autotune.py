@@ -74,7 +74,7 @@ def candidates(n: int, num_probes: int, num_modes: int) -> list:
     for mib in (16, 32, 64, 128, 256):
         b = max(1, min(num_probes, (mib << 20) // slot))
         batches.add(b)
-    tunes = (0, 3, 19, 83, 147, 211) + ((2259, 6355, 22739) if n == 256 else ()) if n <= 256 else ((3, 259, 771, 2307) if n == 512 else (0, 3))
+    tunes = (0, 3, 19, 83, 147, 211) + ((2259, 6355, 22739) if n == 256 else ()) if n <= 256 else ((3, 259, 771, 2307, 18691) if n == 512 else (0, 3))
     return [(b, t) for b in sorted(batches) for t in tunes]
 
 

@@ -109,7 +109,8 @@ static __global__ void k_propagator2d(int n, double calib, double lam_dz, float2
 // double and rounded once; written row-major (S, N, N) and transposed (S, N^T).
 static __global__ void k_transmission(const float* __restrict__ V, long long sy, long long sx, long long ss,
                                int n, int S, double sigma, float2* __restrict__ T, float2* __restrict__ TT,
-                               float* __restrict__ TP = nullptr, float* __restrict__ TPT = nullptr) {
+                               float* __restrict__ TP = nullptr, float* __restrict__ TPT = nullptr,
+                               float* __restrict__ TH = nullptr, float* __restrict__ THT = nullptr) {
   const size_t total = (size_t)S * n * n;
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
        i += (size_t)gridDim.x * blockDim.x) {
@@ -129,6 +130,15 @@ static __global__ void k_transmission(const float* __restrict__ V, long long sy,
       const size_t pc = (((size_t)s * (n / 2) + (size_t)(x >> 1)) * n + y) * 4 + (x & 1);
       TPT[pc] = v.x;
       TPT[pc + 2] = v.y;
+    }
+    if (TH) {  // half-pair interleaved copies: component (element >= n/2) holds re, 2 + it im
+      const int h = n / 2;
+      const size_t hr = (((size_t)s * n + y) * h + (x % h)) * 4 + (x >= h);
+      TH[hr] = v.x;
+      TH[hr + 2] = v.y;
+      const size_t hc = (((size_t)s * n + x) * h + (y % h)) * 4 + (y >= h);
+      THT[hc] = v.x;
+      THT[hc + 2] = v.y;
     }
   }
 }
@@ -285,9 +295,11 @@ static bool is_pow2(int n) { return n > 0 && (n & (n - 1)) == 0; }
 static int field_of(const ptyro_ms_params* p) { return p->field_n > 0 ? p->field_n : p->n; }
 
 struct Layout {
-  size_t tw, tw2, pf, trans, trans_t, trans_p, trans_pt, probe_k, ramp_y, ramp_x, waves, p2, total;
+  size_t tw, tw2, pf, trans, trans_t, trans_p, trans_pt, trans_h, trans_ht, probe_k, ramp_y, ramp_x, waves, p2,
+      total;
   int batch;
   bool paired_t;  // line-pair interleaved transmission tables present (tune bit 16384 at 256^2)
+  bool half_t;    // half-pair interleaved tables present (tune bit 16384 at 512^2 without a field)
 };
 
 static int auto_batch(const ptyro_ms_params* p) {
@@ -315,6 +327,11 @@ static Layout layout_for(const ptyro_ms_params* p) {
   if (L.paired_t) {
     L.trans_p = o; o = align_up(o + 8 * ff * p->num_slices);
     L.trans_pt = o; o = align_up(o + 8 * ff * p->num_slices);
+  }
+  L.half_t = p->n == 512 && field_of(p) == p->n && (p->tune & 16384) && (p->tune & 256);
+  if (L.half_t) {
+    L.trans_h = o; o = align_up(o + 8 * ff * p->num_slices);
+    L.trans_ht = o; o = align_up(o + 8 * ff * p->num_slices);
   }
   L.probe_k = o; o = align_up(o + 8 * nn * p->num_modes);
   L.ramp_y = o; o = align_up(o + 8 * (size_t)p->n * L.batch);
@@ -382,7 +399,8 @@ static int forward_setup(const ptyro_ms_params* p, const Layout& L, char* ws, co
   k_transmission<<<blocks_for((size_t)F * F * p->num_slices, 256), 256, 0, st>>>(
       potential, p->pot_stride_y, p->pot_stride_x, p->pot_stride_s, F, p->num_slices,
       interaction_sigma(p->voltage_kv), T, (float2*)(ws + L.trans_t),
-      L.paired_t ? (float*)(ws + L.trans_p) : nullptr, L.paired_t ? (float*)(ws + L.trans_pt) : nullptr);
+      L.paired_t ? (float*)(ws + L.trans_p) : nullptr, L.paired_t ? (float*)(ws + L.trans_pt) : nullptr,
+      L.half_t ? (float*)(ws + L.trans_h) : nullptr, L.half_t ? (float*)(ws + L.trans_ht) : nullptr);
   k_gather_modes<<<blocks_for(nn * p->num_modes, 256), 256, 0, st>>>(
       (const float2*)modes, p->mode_stride_y, p->mode_stride_x, p->mode_stride_m, n, p->num_modes, pk);
   int rc = check_launch("forward setup", 5);
@@ -402,6 +420,7 @@ struct FwdBuffers {
   const float2* probe_k;
   const float2 *ramp_y, *ramp_x, *trans, *trans_t, *pf, *tw, *tw2;
   const float4 *trans_p, *trans_pt;  // or null
+  const float4 *trans_h, *trans_ht;  // or null
 };
 
 static FwdBuffers fwd_buffers(const Layout& L, char* ws) {
@@ -417,6 +436,8 @@ static FwdBuffers fwd_buffers(const Layout& L, char* ws) {
   b.tw2 = (const float2*)(ws + L.tw2);
   b.trans_p = L.paired_t ? (const float4*)(ws + L.trans_p) : nullptr;
   b.trans_pt = L.paired_t ? (const float4*)(ws + L.trans_pt) : nullptr;
+  b.trans_h = L.half_t ? (const float4*)(ws + L.trans_h) : nullptr;
+  b.trans_ht = L.half_t ? (const float4*)(ws + L.trans_ht) : nullptr;
   return b;
 }
 
@@ -452,6 +473,8 @@ static FwdPlan fwd_pass_plan(const ptyro_ms_params* p, const FwdBuffers& B, cons
   a.trans_t = B.trans_t;
   a.trans_p = B.trans_p;
   a.trans_pt = B.trans_pt;
+  a.trans_h = B.trans_h;
+  a.trans_ht = B.trans_ht;
   a.pf = B.pf;
   a.tw = B.tw;
   a.tw2 = B.tw2;

@@ -194,6 +194,10 @@ int ptyro_ms_steady_pass(const ptyro_ms_params* p, int32_t axis, int32_t reps, v
     a.trans_p = (const float4*)(ws + L.trans_p);
     a.trans_pt = (const float4*)(ws + L.trans_pt);
   }
+  if (L.half_t) {
+    a.trans_h = (const float4*)(ws + L.trans_h);
+    a.trans_ht = (const float4*)(ws + L.trans_ht);
+  }
   a.pf = (const float2*)(ws + L.pf);
   a.tw = (const float2*)(ws + L.tw);
   a.n_modes = p->num_modes;

@@ -173,13 +173,23 @@ __device__ __forceinline__ void half_body(const PassArgs& a, const int slot, con
 
   // ---- transmission (and the gradient-mode checkpoint)
   {
-    int eoff;
-    const float2* T = trans_row<AXIS>(a.trans, a.trans_t, a.field_n, a.t_slice, a.win, slot / a.n_modes, line,
-                                      &eoff);
-    const int fm = a.field_n - 1;
+    const float4* TH = AXIS == 0 ? a.trans_h : a.trans_ht;
+    if (TH != nullptr && a.win == nullptr) {  // one entry holds the factors of both halves
+      const float4* row = TH + ((size_t)a.t_slice * N + line) * (N / 2);
 #pragma unroll
-    for (int j = 0; j < H; ++j)
-      p[j] = cmul(p[j], __ldg(T + ((t + N1 * j + eoff) & fm)), __ldg(T + ((t + N1 * (j + H) + eoff) & fm)));
+      for (int j = 0; j < H; ++j) {
+        const float4 q = __ldg(row + t + N1 * j);
+        p[j] = cmul_pp(p[j], {make_float2(q.x, q.y), make_float2(q.z, q.w)});
+      }
+    } else {
+      int eoff;
+      const float2* T = trans_row<AXIS>(a.trans, a.trans_t, a.field_n, a.t_slice, a.win, slot / a.n_modes, line,
+                                        &eoff);
+      const int fm = a.field_n - 1;
+#pragma unroll
+      for (int j = 0; j < H; ++j)
+        p[j] = cmul(p[j], __ldg(T + ((t + N1 * j + eoff) & fm)), __ldg(T + ((t + N1 * (j + H) + eoff) & fm)));
+    }
     if (a.ckpt_store) {
       float2* ck = a.ckpt_store + (size_t)slot * a.res_stride;
 #pragma unroll

@@ -51,6 +51,11 @@ struct PassArgs {
   // likewise over column pairs of trans_t
   const float4* trans_p;
   const float4* trans_pt;
+  // for half-paired passes (F == N), or null: trans_h[s][y][x] = (T[y][x].re,
+  // T[y][x+N/2].re, T[y][x].im, T[y][x+N/2].im) for x < N/2; trans_ht likewise over
+  // the transposed table
+  const float4* trans_h;
+  const float4* trans_ht;
   const int* win;          // (B, 2) window origins (y, x) in the field for this batch, or null
   int field_n;             // F (== N without windows); power of two
 

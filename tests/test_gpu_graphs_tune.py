@@ -120,7 +120,8 @@ def test_paired_steady_kernels_are_bit_identical(n):
 def test_half_paired_steady_kernel_matches_oracle(n):
     """The half-paired steady pass (tune bit 256; decimation in frequency inside the
     thread) agrees with the oracle and the one-line kernel to float32 rounding; at
-    512^2 its TMA column variant (bit 2048) gives the same bits as the tiled one."""
+    512^2 its TMA column variant (bit 2048) and its half-pair interleaved
+    transmission tables (bit 16384) give the same bits as the plain variant."""
     import numpy as np
     from oracle import multislice_ref as R
     from tests.conftest import rel_l2
@@ -138,11 +139,12 @@ def test_half_paired_steady_kernel_matches_oracle(n):
     ref = run_forward(slices, 1.7, modes, wt, pos_d, 200.0, 0.3, 0.3, tune=3, lanes=1).cpu().numpy()
     want = R.stem_4d(pot, 1.7, 0.3, probe[..., None], [1.0], 0.3, 200.0, pos, 0.3, dtype=np.complex128)["data"]
     outs = {}
-    for tune in (259, 771, 2307, 2819):
+    for tune in (259, 771, 2307, 2819, 18691, 19203):
         got = run_forward(slices, 1.7, modes, wt, pos_d, 200.0, 0.3, 0.3, tune=tune, lanes=1).cpu().numpy()
         assert rel_l2(got, want) < 1e-4
         assert rel_l2(got, ref) < 2e-6
         outs[tune] = got
     assert np.array_equal(outs[2307], outs[259]) and np.array_equal(outs[2819], outs[771])
+    assert np.array_equal(outs[18691], outs[259]) and np.array_equal(outs[19203], outs[771])
     torch.cuda.synchronize()
     assert pb._lib.load().ptyro_pass_wait_timeouts() == 0
