@@ -23,7 +23,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from .simulations import make_probe, ms_params, relativistic_wavelength_ang
+from .simulations import default_tune, make_probe, ms_params, relativistic_wavelength_ang
 from .types import create_detector_config, create_microscope_config
 
 
@@ -175,8 +175,10 @@ class Server:
         pos = torch.as_tensor(np.asarray(req.positions, np.float64), device=self.device).reshape(P, 2).contiguous()
         out = torch.empty((P, req.n, req.n), dtype=torch.float32, device=self.device)
         d = _lib.JobDesc()
+        # the per-edge launch variant also lays out the interleaved transmission tables
+        # that the paired multi-job passes read
         d.p = ms_params(req.n, req.num_slices, 1, P, req.voltage_kv, req.slice_thickness, req.calib_ang,
-                        req.calib_ang, slices.stride(), modes.stride(), req.batch)
+                        req.calib_ang, slices.stride(), modes.stride(), req.batch, default_tune(req.n))
         d.kind = _lib.PTYRO_JOB_GRADIENT if req.kind == "grad" else _lib.PTYRO_JOB_FORWARD
         d.potential, d.modes, d.weights, d.positions = (slices.data_ptr(), modes.data_ptr(),
                                                         self.weights.data_ptr(), pos.data_ptr())
