@@ -148,3 +148,26 @@ def test_half_paired_steady_kernel_matches_oracle(n):
     assert np.array_equal(outs[18691], outs[259]) and np.array_equal(outs[19203], outs[771])
     torch.cuda.synchronize()
     assert pb._lib.load().ptyro_pass_wait_timeouts() == 0
+
+
+def test_ragged_batches_and_lanes_at_256_match_one_line_kernel():
+    """At 256^2 the default launch variant (TMA column blocks with tensor maps encoded
+    per batch size, paired first/last passes, interleaved transmission tables) gives
+    the one-line kernel's bits with a ragged last batch and several lanes."""
+    import numpy as np
+    from oracle import multislice_ref as R
+    from ptyrodactyl_b200.simulations import default_tune, run_forward
+    rng = np.random.default_rng(256)
+    n, s, p = 256, 6, 37
+    dev = torch.device("cuda")
+    slices = torch.as_tensor(rng.uniform(0, 40, (n, n, s)), dtype=torch.float32, device=dev)
+    probe = R.make_probe(200.0, 25.0, (n, n), 30.0, defocus_ang=-20.0)
+    modes = torch.as_tensor(probe[..., None].astype(np.complex64), device=dev)
+    wt = torch.ones(1, device=dev)
+    pos = torch.as_tensor(rng.uniform(-2, 2, (p, 2)), dtype=torch.float64, device=dev)
+    ref = run_forward(slices, 1.7, modes, wt, pos, 200.0, 0.3, 0.3, tune=3, batch=8, lanes=1)
+    for lanes in (1, 3):
+        got = run_forward(slices, 1.7, modes, wt, pos, 200.0, 0.3, 0.3, tune=default_tune(n), batch=8, lanes=lanes)
+        assert torch.equal(got, ref), lanes
+    torch.cuda.synchronize()
+    assert pb._lib.load().ptyro_pass_wait_timeouts() == 0
