@@ -66,12 +66,20 @@ __device__ __forceinline__ double fftfreq(int k, int n, double d) {
   return (double)(k <= (n - 1) / 2 ? k : k - n) / (n * d);
 }
 
+// exp(-2 pi i j / n) in float32. Entries at multiples of n / 64 are 64th roots of
+// unity and take the energy-balanced constants of the butterflies (w64); every other
+// entry is evaluated in double and rounded to nearest.
+__device__ __forceinline__ float2 unit_root(int j, int n) {
+  if ((j * 64) % n == 0) return w64<-1>((j * 64) / n);
+  double s, c;
+  sincospi(-2.0 * (double)j / (double)n, &s, &c);
+  return make_float2((float)c, (float)s);
+}
+
 static __global__ void k_twiddle(int n, float2* tw) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= n) return;
-  double s, c;
-  sincospi(-2.0 * (double)j / (double)n, &s, &c);
-  tw[j] = make_float2((float)c, (float)s);
+  tw[j] = unit_root(j, n);
 }
 
 // twiddles in line-transform order: tw2[k2 * n1 + t] = exp(-2 pi i t k2 / n)
@@ -79,9 +87,7 @@ static __global__ void k_twiddle2(int n, int n1, float2* tw2) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const int k2 = i / n1, t = i % n1;
-  double s, c;
-  sincospi(-2.0 * (double)((t * k2) % n) / (double)n, &s, &c);
-  tw2[i] = make_float2((float)c, (float)s);
+  tw2[i] = unit_root((t * k2) % n, n);
 }
 
 // 1-D factor of propagation_func (simulations.py:213-224): exp(-i pi lambda dz q^2) * scale

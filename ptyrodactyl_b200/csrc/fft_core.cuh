@@ -13,6 +13,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "unit_consts.cuh"
+
 namespace ptyro {
 
 __device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
@@ -61,39 +63,46 @@ __device__ __forceinline__ Pair make_pair(float2 a, float2 b) { return {make_flo
 __device__ __forceinline__ float2 pair_a(Pair p) { return make_float2(p.re.x, p.im.x); }
 __device__ __forceinline__ float2 pair_b(Pair p) { return make_float2(p.re.y, p.im.y); }
 
-// cos(2 pi i / 64) for i = 0..16, rounded from the decimal expansion.
-__device__ __forceinline__ float cos64_q(int i) {
-  switch (i) {
-    case 0: return 1.0f;
-    case 1: return (float)0.99518472667219688624;
-    case 2: return (float)0.98078528040323044913;
-    case 3: return (float)0.95694033573220886494;
-    case 4: return (float)0.92387953251128675613;
-    case 5: return (float)0.88192126434835502971;
-    case 6: return (float)0.83146961230254523708;
-    case 7: return (float)0.77301045336273696081;
-    case 8: return (float)0.70710678118654752440;
-    case 9: return (float)0.63439328416364549822;
-    case 10: return (float)0.55557023301960222474;
-    case 11: return (float)0.47139673682599764856;
-    case 12: return (float)0.38268343236508977173;
-    case 13: return (float)0.29028467725446236764;
-    case 14: return (float)0.19509032201612826785;
-    case 15: return (float)0.098017140329560601994;
-    default: return 0.0f;
-  }
-}
-
-// exp(DIR * 2 pi i k / 64) for k in [0, 64); DIR = -1 forward, +1 inverse.
+// exp(DIR * 2 pi i k / 64) for k in [0, 64); DIR = -1 forward, +1 inverse. The
+// first-quadrant values come from unit_consts.cuh (float32 roots chosen so that the
+// tables and stages built from them neither gain nor lose energy on average); the
+// other quadrants follow by exact rotations by i.
 template <int DIR>
 __device__ __forceinline__ float2 w64(int k) {
   k &= 63;
-  float c, s;  // cos and sin of 2 pi k / 64
-  if (k <= 16) { c = cos64_q(k); s = cos64_q(16 - k); }
-  else if (k <= 32) { c = -cos64_q(32 - k); s = cos64_q(k - 16); }
-  else if (k <= 48) { c = -cos64_q(k - 32); s = -cos64_q(48 - k); }
-  else { c = cos64_q(64 - k); s = -cos64_q(k - 48); }
+  const int q = k >> 4, r = k & 15;
+  const float c0 = unit_c(r), s0 = unit_s(r);
+  float c, s;
+  if (q == 0) { c = c0; s = s0; }
+  else if (q == 1) { c = -s0; s = c0; }
+  else if (q == 2) { c = -c0; s = -s0; }
+  else { c = s0; s = -c0; }
   return make_float2(c, DIR < 0 ? -s : s);
+}
+
+// Factored form of W_64^k for the butterflies: w = m (1 + i t) when A is true
+// (|cos| >= |sin|), w = m (t + i) otherwise. First-quadrant (m, t) come from
+// bfly_m / bfly_t (r <= 8: m ~ cos, t ~ tan; r > 8 uses r' = 16 - r with the roles of
+// cos and sin swapped); multiplying by i^q and conjugating (DIR = -1) only moves
+// signs between m and t and switches the form.
+struct FactTw {
+  float m, t;
+  bool a;
+};
+template <int DIR>
+__device__ __forceinline__ FactTw fact_tw(int k) {
+  k &= 63;
+  const int q = k >> 4, r = k & 15;
+  FactTw f = r <= 8 ? FactTw{bfly_m(r), bfly_t(r), true} : FactTw{bfly_m(16 - r), bfly_t(16 - r), false};
+  for (int i = 0; i < q; ++i) {  // times i: m (1 + i t) -> m (-t + i); m (t + i) -> (-m) (1 - i t)
+    if (f.a) f = FactTw{f.m, -f.t, false};
+    else f = FactTw{-f.m, -f.t, true};
+  }
+  if (DIR < 0) {  // conjugate: m (1 - i t) -> form A with -t; m (t - i) = (-m) (-t + i)
+    if (f.a) f.t = -f.t;
+    else f = FactTw{-f.m, -f.t, false};
+  }
+  return f;
 }
 
 // b * W_64^k (W = exp(DIR 2 pi i / 64)) with the exact cases folded at compile time.
@@ -113,8 +122,8 @@ __host__ __device__ constexpr int bitrev(int i, int bits) {
 }
 
 // Butterflies u +- b W_64^k. The exact twiddles (k = 0, 16, 32, 48) become additions
-// of the swapped parts. Every other twiddle w = (c, s) is factored as
-// c (1 + i s/c) when |c| >= |s| and s (c/s + i) otherwise, so b w costs two fmas
+// of the swapped parts. Every other twiddle is held factored (fact_tw) as
+// c (1 + i t) when |c| >= |s| and s (t + i) otherwise, so b w costs two fmas
 // and the two outputs u +- (scale) q two more each: six fused operations instead of
 // a complex multiply and two complex additions (eight). The scalar and the paired
 // versions perform the same operations, so they round identically.
@@ -133,14 +142,14 @@ __device__ __forceinline__ void bfly(Pair& u, Pair& b, int k) {
     o1 = {sub2(u.re, b.im), __fadd2_rn(u.im, b.re)};
     o2 = {__fadd2_rn(u.re, b.im), sub2(u.im, b.re)};
   } else {
-    const float2 w = w64<DIR>(k);
-    if (fabsf(w.x) >= fabsf(w.y)) {  // b w = c (b.re - t b.im, b.im + t b.re)
-      const float t = w.y / w.x, c = w.x;
+    const FactTw f = fact_tw<DIR>(k);
+    if (f.a) {  // b w = c (b.re - t b.im, b.im + t b.re)
+      const float t = f.t, c = f.m;
       const Pair q = {__ffma2_rn(dup2(-t), b.im, b.re), __ffma2_rn(dup2(t), b.re, b.im)};
       o1 = {__ffma2_rn(dup2(c), q.re, u.re), __ffma2_rn(dup2(c), q.im, u.im)};
       o2 = {__ffma2_rn(dup2(-c), q.re, u.re), __ffma2_rn(dup2(-c), q.im, u.im)};
     } else {  // b w = s (t b.re - b.im, t b.im + b.re), real part kept negated
-      const float t = w.x / w.y, sn = w.y;
+      const float t = f.t, sn = f.m;
       const Pair q = {__ffma2_rn(dup2(-t), b.re, b.im), __ffma2_rn(dup2(t), b.im, b.re)};
       o1 = {__ffma2_rn(dup2(-sn), q.re, u.re), __ffma2_rn(dup2(sn), q.im, u.im)};
       o2 = {__ffma2_rn(dup2(sn), q.re, u.re), __ffma2_rn(dup2(-sn), q.im, u.im)};
@@ -159,15 +168,15 @@ __device__ __forceinline__ void bfly(float2& u, float2& b, int k) {
     b = o2;
     return;
   }
-  const float2 w = w64<DIR>(k);
+  const FactTw f = fact_tw<DIR>(k);
   float2 o1, o2;
-  if (fabsf(w.x) >= fabsf(w.y)) {
-    const float t = w.y / w.x, c = w.x;
+  if (f.a) {
+    const float t = f.t, c = f.m;
     const float2 q = make_float2(fmaf(-t, b.y, b.x), fmaf(t, b.x, b.y));
     o1 = make_float2(fmaf(c, q.x, u.x), fmaf(c, q.y, u.y));
     o2 = make_float2(fmaf(-c, q.x, u.x), fmaf(-c, q.y, u.y));
   } else {
-    const float t = w.x / w.y, sn = w.y;
+    const float t = f.t, sn = f.m;
     const float2 q = make_float2(fmaf(-t, b.x, b.y), fmaf(t, b.y, b.x));
     o1 = make_float2(fmaf(-sn, q.x, u.x), fmaf(sn, q.y, u.y));
     o2 = make_float2(fmaf(sn, q.x, u.x), fmaf(-sn, q.y, u.y));

@@ -2,7 +2,9 @@
 
 Tolerances (relative L2 over all pattern values): <= 1e-5 against the float32
 (complex64) restatement of the reference; <= 1e-4 against the float64 oracle
-and the reference's own float64 golden arrays.
+and the reference's own float64 golden arrays. The full-depth 512^2 / 100-slice
+case is held to 1.5e-5 against the float32 restatement, whose own distance from
+float64 is 1e-5 there, and to a smaller float64 error than that restatement.
 """
 
 import ctypes
@@ -100,6 +102,68 @@ def test_forward_matches_oracle(w, n_probes, num_slices):
     assert rel_l2(got, want64) < TOL_F64
     n_ap = R.aperture_count(w.voltage_kv, w.aperture_mrad, (w.n, w.n), w.calib * 100.0)
     assert np.allclose(got.sum(axis=(1, 2)), n_ap, rtol=1e-4)
+
+
+def _spread_positions(w, count):
+    """``count`` raster positions spread over the whole scan (first, last and evenly between)."""
+    pos = synth.raster_positions(w)
+    return pos[np.linspace(0, pos.shape[0] - 1, count).round().astype(int)]
+
+
+# At 512^2 and 100 slices the float32 restatement of the reference is itself
+# 0.99e-5 - 1.01e-5 (relative L2) away from the float64 oracle, most of it a coherent
+# loss of intensity (-8.4e-6) in its own float32 FFTs, so no implementation can be
+# within 1e-5 of it without sharing its rounding. There the kernels are held to being
+# closer to float64 than that float32 path is, and within 1.5e-5 of it.
+TOL_F32_512_100 = 1.5e-5
+
+
+def _check_full_depth(w, got, pot, probe, pos, tol32=TOL_F32):
+    args = (pot, synth.SLICE_DZ, w.calib, probe[..., None], [1.0], w.calib, w.voltage_kv, pos, w.calib)
+    want32 = R.stem_4d(*args, dtype=np.complex64)["data"]
+    want64 = R.stem_4d(*args, dtype=np.complex128)["data"]
+    e32, e64, ref32 = rel_l2(got, want32), rel_l2(got, want64), rel_l2(want32, want64)
+    # the kernels against the float32 restatement of the reference, and both against float64
+    assert e32 < tol32, (pot.shape[2], e32, e64, ref32)
+    assert e64 < TOL_F64, (e64, ref32)
+    # the kernels are at least as accurate as the reference's own float32 path
+    assert e64 < ref32, (e64, ref32)
+    # no coherent loss of intensity: every exact pattern sums to the aperture pixel count
+    n_ap = R.aperture_count(w.voltage_kv, w.aperture_mrad, (w.n, w.n), w.calib * 100.0)
+    assert np.allclose(got.sum(axis=(1, 2)), n_ap, rtol=5e-6), got.sum(axis=(1, 2)) / n_ap - 1
+    return want64
+
+
+def test_forward_full_depth_256_50_slices():
+    """The 256^2 workload at all 50 slices: 6 probes from corner to corner of the 64 x 64 scan."""
+    w = synth.CONFIG2
+    pot = synth.potential_slices(w)
+    assert pot.shape[2] == 50
+    probe = R.make_probe(w.voltage_kv, w.aperture_mrad, (w.n, w.n), w.calib * 100.0, w.defocus_ang, w.c3_ang)
+    pos = _spread_positions(w, 6)
+    got = _run(pot, synth.SLICE_DZ, probe[..., None], [1.0], pos, w.voltage_kv, w.calib)
+    _check_full_depth(w, got, pot, probe, pos)
+
+
+def test_forward_full_depth_512_100_slices_frozen_phonons():
+    """The 512^2 workload at all 100 slices: each of the 4 frozen-phonon configurations
+    for 2 probes, and the 4-configuration mean through the public API."""
+    w = synth.CONFIG3
+    probe = R.make_probe(w.voltage_kv, w.aperture_mrad, (w.n, w.n), w.calib * 100.0, w.defocus_ang, w.c3_ang)
+    pos = _spread_positions(w, 2)
+    pots, wants = [], []
+    for k in range(w.phonon_configs):
+        pot = synth.potential_slices(w, phonon=k)
+        assert pot.shape[2] == 100
+        got = _run(pot, synth.SLICE_DZ, probe[..., None], [1.0], pos, w.voltage_kv, w.calib)
+        wants.append(_check_full_depth(w, got, pot, probe, pos, tol32=TOL_F32_512_100))
+        pots.append(pot)
+    mic = pb.create_microscope_config(w.voltage_kv, w.aperture_mrad, probe_shape=(w.n, w.n))
+    det = pb.create_detector_config(w.calib, scan_positions_px=pos)
+    beam = pb.create_probe_modes(probe[..., None], [1.0], w.calib)
+    mean = pb.stem_4d_frozen_phonon([pb.create_potential_slices(p, synth.SLICE_DZ, w.calib) for p in pots], beam,
+                                    mic, det).data.cpu().numpy()
+    assert rel_l2(mean, np.mean(wants, axis=0)) < TOL_F64
 
 
 def test_modes_weights_and_single_slice():
