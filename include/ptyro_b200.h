@@ -13,6 +13,15 @@
  *
  * Return value: PTYRO_OK or an error code; ptyro_last_error() gives the message
  * of the last failure on the calling host thread.
+ *
+ * Device status: the first PTYRO_WS_STATUS_BYTES of every engine workspace
+ * (ptyro_ms_forward and its variants, ptyro_ms_backward*, ptyro_ms_jvp) hold the
+ * call's device status word, a uint32 at offset 0. Each call zeroes it on its
+ * stream before its first kernel and its kernels OR PTYRO_STATUS_* bits into it.
+ * Since the call does not synchronise, its return value cannot report these: the
+ * caller reads the word once the stream has run the call (for an XLA FFI handler:
+ * copy it into an output flag buffer and raise on the host, like eqx.error_if)
+ * and treats any set bit as a failed call whose outputs are unusable.
  */
 #ifndef PTYRO_B200_H
 #define PTYRO_B200_H
@@ -29,6 +38,11 @@ extern "C" {
 #define PTYRO_ERR_WORKSPACE 2   /* workspace too small or misaligned */
 #define PTYRO_ERR_CUDA 3        /* a launch failed */
 #define PTYRO_ERR_UNSUPPORTED 4 /* grid size outside the compiled set */
+
+#define PTYRO_WS_STATUS_BYTES 256 /* the status block at the start of each workspace */
+/* Status bit: a bounded wait for a tile copy (TMA) gave up; the warps that gave up
+ * left their lines of the wave unwritten, so the call's results are wrong. */
+#define PTYRO_STATUS_WAIT_TIMEOUT 1u
 
 /* ptyro_ms_params.flags: add sum_m w_m |A_m|^2 into `patterns` instead of
  * overwriting them (frozen-phonon averaging: one forward per configuration with
@@ -251,6 +265,15 @@ int ptyro_ms_steady_pass(const ptyro_ms_params* p, int32_t axis, int32_t reps, v
  * the FP32 ceiling used as the roofline denominator; no reference counterpart. */
 int ptyro_fp32_fma_probe(float* out, int32_t blocks, int32_t iters, void* stream);
 
+/* Self-test of the bounded tile wait the TMA column passes use: one CTA of `warps`
+ * warps (1..32) arms an mbarrier for a copy that is never issued, so every warp's
+ * wait gives up after `polls` polls (1..2^20) and takes the pass kernels' give-up
+ * path: the warp skips its work, *skipped_warps (DEVICE int32) counts it and
+ * PTYRO_STATUS_WAIT_TIMEOUT is ORed into *status (DEVICE uint32). Nothing is in
+ * flight when the CTA exits. No counterpart in the reference. */
+int ptyro_test_wait_timeout(int32_t warps, int32_t polls, uint32_t* status, int32_t* skipped_warps,
+                            void* stream);
+
 /* Workspace bytes of ptyro_atom_slices for edge n and num_types atom types. */
 size_t ptyro_atom_slices_workspace_bytes(int32_t n, int32_t num_types);
 
@@ -375,11 +398,16 @@ int ptyro_sched_memory(ptyro_sched* s, size_t* free_bytes, int32_t* free_slots);
  * reference (JAX allocates for its own path).
  * Same arguments and results as ptyro_ms_forward minus the workspace; the scratch
  * is a PTYRO_STATIC_SCRATCH_BYTES array in the library's device image, held on
- * every GPU that loads the library until exit. The first call on a device looks
- * up that array's address; make it before any stream capture. Calls on a device
+ * every GPU that loads the library until exit. Every call made outside stream
+ * capture looks up that array's address on the current device; captured calls reuse
+ * it, so make one call on each device before any stream capture. Calls on a device
  * share the array, so calls that overlap on the GPU race: serialise them on one
- * stream. Jobs whose scratch does not fit (e.g. a 1024^2 grid with many slices)
- * are rejected with PTYRO_ERR_WORKSPACE before anything is launched. */
+ * stream. The batch is the largest that fits; when not one probe fits with the
+ * default variant's optional interleaved transmission tables, they are left out
+ * (bit-identical results). Jobs whose scratch still does not fit (e.g. a 1024^2 grid
+ * with many slices) are rejected with PTYRO_ERR_WORKSPACE before anything is
+ * launched. The call has no way to return the device status word, so if a bounded
+ * wait inside the forward gave up, `patterns` is filled with NaN. */
 int ptyro_ms_forward_noalloc(const ptyro_ms_params* p, const float* potential, const float* modes,
                              const float* weights, const double* positions, float* patterns, void* stream);
 

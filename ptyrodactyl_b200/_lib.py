@@ -19,6 +19,8 @@ PTYRO_ERR_WORKSPACE = 2
 PTYRO_ERR_CUDA = 3
 PTYRO_ERR_UNSUPPORTED = 4
 STATIC_SCRATCH_BYTES = 64 << 20  # PTYRO_STATIC_SCRATCH_BYTES
+WS_STATUS_BYTES = 256  # PTYRO_WS_STATUS_BYTES: the status block at the start of every workspace
+STATUS_WAIT_TIMEOUT = 1  # PTYRO_STATUS_WAIT_TIMEOUT
 PTYRO_FLAG_ACCUMULATE = 1
 MAX_DETECTORS = 32
 
@@ -36,6 +38,7 @@ EXPORTED_SYMBOLS = (
     "ptyro_pass_wait_timeouts",
     "ptyro_ms_steady_pass",
     "ptyro_fp32_fma_probe",
+    "ptyro_test_wait_timeout",
     "ptyro_ms_forward_noalloc",
     "ptyro_ms_detect_workspace_bytes",
     "ptyro_ms_forward_detect",
@@ -214,6 +217,8 @@ def _declare(lib) -> None:
     lib.ptyro_atom_slices.argtypes = [i32, i32, i32, i32, vp, vp, vp, vp, vp, dbl, vp, i64, i64, i64, vp, sz, vp]
     lib.ptyro_ms_forward_noalloc.restype = ctypes.c_int
     lib.ptyro_ms_forward_noalloc.argtypes = [pp, vp, vp, vp, vp, vp, vp]
+    lib.ptyro_test_wait_timeout.restype = ctypes.c_int
+    lib.ptyro_test_wait_timeout.argtypes = [i32, i32, vp, vp, vp]
 
 
 def load(path: str | None = None):
@@ -240,3 +245,46 @@ def check(code: int) -> None:
         if code == PTYRO_ERR_INVALID or code == PTYRO_ERR_UNSUPPORTED:
             raise ValueError(msg)
         raise PtyroError(code, msg)
+
+
+class DeviceStatusError(RuntimeError):
+    """A call's kernels reported a failure through its device status word (for
+    example a bounded wait for a tile copy gave up); its outputs are invalid."""
+
+    def __init__(self, what: str, status: int):
+        reasons = []
+        if status & STATUS_WAIT_TIMEOUT:
+            reasons.append("a bounded wait for a tile copy (TMA) gave up")
+        super().__init__(f"{what}: device status {status:#x} ({'; '.join(reasons) or 'unknown bits'}); "
+                         "the results of this call are invalid")
+        self.status = status
+
+
+def new_status(device):
+    """A zeroed int32 device word that :func:`gather_status` ORs call statuses into."""
+    import torch
+    return torch.zeros(1, dtype=torch.int32, device=device)
+
+
+def gather_status(status, workspace) -> None:
+    """OR the status word at the start of ``workspace`` (a uint8 device tensor that a
+    call just used) into ``status`` on the current stream, ordered after that call.
+    Asynchronous and capturable in a CUDA graph; ``status`` None does nothing."""
+    if status is not None:
+        status.bitwise_or_(workspace[:4].view(status.dtype))
+
+
+def check_status(status, what: str) -> None:
+    """Wait for the work behind ``status`` and raise :class:`DeviceStatusError` if any
+    bit is set (a host synchronisation)."""
+    v = int(status.item())
+    if v:
+        raise DeviceStatusError(what, v)
+
+
+def check_workspace_status(workspace, what: str) -> None:
+    """:func:`check_status` of the status word at the start of ``workspace``."""
+    import torch
+    v = int(workspace[:4].view(torch.int32).item())
+    if v:
+        raise DeviceStatusError(what, v)

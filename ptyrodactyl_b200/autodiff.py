@@ -87,6 +87,7 @@ class Stem4dFunction(torch.autograd.Function):
                                           weights.data_ptr(), positions.data_ptr(), out.data_ptr(), ws.data_ptr(),
                                           ws_bytes, _stream_ptr(dev))
             _lib.check(rc)
+            _lib.check_workspace_status(ws, "stem_4d forward")
         return out, res
 
     @staticmethod
@@ -142,6 +143,7 @@ class Stem4dFunction(torch.autograd.Function):
                                                            g.data_ptr(), g_slices.data_ptr(), g_modes.data_ptr(),
                                                            g_pos.data_ptr(), ws.data_ptr(), ws_bytes,
                                                            _stream_ptr(dev)))
+            _lib.check_workspace_status(ws, "stem_4d backward")
         # the C-ABI gives JAX's convention conj(2 dL/dconj); torch wants 2 dL/dconj
         return g_slices, g_modes.conj().resolve_conj(), g_pos
 
@@ -234,6 +236,7 @@ def vjp(slices, modes, weights, positions, grad_patterns, slice_thickness, volta
     _lib.check(lib.ptyro_ms_forward_ckpt(ctypes.byref(prm), k, slices.data_ptr(), modes.data_ptr(),
                                          weights.data_ptr(), positions.data_ptr(), out.data_ptr(), res.data_ptr(),
                                          ws.data_ptr(), ws_bytes, st))
+    _lib.check_workspace_status(ws, "vjp forward")
     g_slices = torch.empty_strided(slices.shape, slices.stride(), dtype=torch.float32, device=dev)
     g_modes = torch.empty_strided(modes.shape, modes.stride(), dtype=torch.complex64, device=dev)
     bws = lib.ptyro_ms_backward_workspace_bytes(ctypes.byref(prm))
@@ -242,6 +245,7 @@ def vjp(slices, modes, weights, positions, grad_patterns, slice_thickness, volta
     _lib.check(lib.ptyro_ms_backward(ctypes.byref(prm), k, slices.data_ptr(), weights.data_ptr(),
                                      positions.data_ptr(), res.data_ptr(), g.data_ptr(), g_slices.data_ptr(),
                                      g_modes.data_ptr(), bw.data_ptr(), bws, st))
+    _lib.check_workspace_status(bw, "vjp backward")
     return out, g_slices, g_modes
 
 

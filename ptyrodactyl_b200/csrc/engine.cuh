@@ -301,7 +301,7 @@ static bool is_pow2(int n) { return n > 0 && (n & (n - 1)) == 0; }
 static int field_of(const ptyro_ms_params* p) { return p->field_n > 0 ? p->field_n : p->n; }
 
 struct Layout {
-  size_t tw, tw2, pf, trans, trans_t, trans_p, trans_pt, trans_h, trans_ht, probe_k, ramp_y, ramp_x, waves, p2,
+  size_t status, tw, tw2, pf, trans, trans_t, trans_p, trans_pt, trans_h, trans_ht, probe_k, ramp_y, ramp_x, waves, p2,
       total;
   int batch;
   bool paired_t;  // line-pair interleaved transmission tables present (tune bit 16384 at 256^2)
@@ -323,6 +323,7 @@ static Layout layout_for(const ptyro_ms_params* p) {
   L.batch = p->batch > 0 ? (p->batch < p->num_probes ? p->batch : (p->num_probes > 0 ? p->num_probes : 1))
                          : auto_batch(p);
   size_t o = 0;
+  L.status = o; o = align_up(o + PTYRO_WS_STATUS_BYTES);  // the call's device status word
   L.tw = o; o = align_up(o + 8 * (size_t)p->n);
   L.tw2 = o; o = align_up(o + 8 * (size_t)p->n);
   L.pf = o; o = align_up(o + 8 * (size_t)p->n);
@@ -368,6 +369,13 @@ static int validate(const ptyro_ms_params* p) {
     return fail(PTYRO_ERR_INVALID, "real_space_calib_ang must be > 0");
   if ((size_t)p->num_modes * p->num_probes > 65535u * 16u)
     return fail(PTYRO_ERR_INVALID, "too many probe modes");
+  return PTYRO_OK;
+}
+
+// Zero the call's device status word (a memset node when the stream is being captured).
+static int clear_status(void* status, cudaStream_t st) {
+  const cudaError_t e = cudaMemsetAsync(status, 0, sizeof(unsigned int), st);
+  if (e != cudaSuccess) return fail(PTYRO_ERR_CUDA, std::string("clearing the status word: ") + cudaGetErrorString(e));
   return PTYRO_OK;
 }
 
@@ -422,6 +430,7 @@ struct FwdPlan {
 };
 
 struct FwdBuffers {
+  unsigned int* status;
   float2* waves;
   const float2* probe_k;
   const float2 *ramp_y, *ramp_x, *trans, *trans_t, *pf, *tw, *tw2;
@@ -431,6 +440,7 @@ struct FwdBuffers {
 
 static FwdBuffers fwd_buffers(const Layout& L, char* ws) {
   FwdBuffers b;
+  b.status = (unsigned int*)(ws + L.status);
   b.waves = (float2*)(ws + L.waves);
   b.probe_k = (const float2*)(ws + L.probe_k);
   b.ramp_y = (const float2*)(ws + L.ramp_y);
@@ -471,6 +481,7 @@ static FwdPlan fwd_pass_plan(const ptyro_ms_params* p, const FwdBuffers& B, cons
   FwdPlan r;
   PassArgs& a = r.a;
   a = PassArgs{};
+  a.status = B.status;
   a.wave = B.waves;
   a.probe_k = B.probe_k;
   a.ramp_y = B.ramp_y;
@@ -620,6 +631,7 @@ static int forward_impl(const ptyro_ms_params* p, int ckpt_every, const float* p
   }
   cudaStream_t st = (cudaStream_t)stream;
   char* ws = (char*)workspace;
+  if ((rc = clear_status(ws + L.status, st))) return rc;
   rc = forward_setup(p, L, ws, potential, modes, st);
   if (rc) return rc;
   const int n = p->n, S = p->num_slices, M = p->num_modes;
@@ -788,7 +800,7 @@ static __global__ void k_write_grad_modes(const float2* __restrict__ lam_beam, i
 }
 
 struct BwdLayout {
-  size_t tw, pf, trans, trans_t, ramp_y, ramp_x, psi, lam, contrib, beam, probe_k, total;
+  size_t status, tw, pf, trans, trans_t, ramp_y, ramp_x, psi, lam, contrib, beam, probe_k, total;
   int batch;
 };
 
@@ -806,6 +818,7 @@ static BwdLayout bwd_layout_for(const ptyro_ms_params* p) {
   }
   const size_t slots = (size_t)L.batch * p->num_modes;
   size_t o = 0;
+  L.status = o; o = align_up(o + PTYRO_WS_STATUS_BYTES);  // the call's device status word
   L.tw = o; o = align_up(o + 8 * (size_t)p->n);
   L.pf = o; o = align_up(o + 8 * (size_t)p->n);
   const size_t ff = (size_t)field_of(p) * field_of(p);
@@ -890,6 +903,7 @@ struct BwdPlan {
 };
 
 struct BwdBuffers {
+  unsigned int* status;
   float2 *psi, *lam;
   float* contrib;
   const float2 *trans, *trans_t, *pf, *tw, *ramp_y, *ramp_x;
@@ -903,6 +917,7 @@ static BwdPlan bwd_pass_plan(const ptyro_ms_params* p, const BwdBuffers& B, cons
   BwdPlan r;
   BwdArgs& a = r.a;
   a = BwdArgs{};
+  a.status = B.status;
   a.psi = B.psi;
   a.lam = B.lam;
   a.weights = weights;
@@ -975,6 +990,7 @@ static int backward_impl(const ptyro_ms_params* p, int ckpt_every, const float* 
                                          std::to_string(workspace_bytes));
   cudaStream_t st = (cudaStream_t)stream;
   char* ws = (char*)workspace;
+  if ((rc = clear_status(ws + L.status, st))) return rc;
   const int n = p->n, S = p->num_slices, M = p->num_modes;
   const size_t nn = (size_t)n * n;
   const int C = (S + ckpt_every - 1) / ckpt_every;
@@ -1003,6 +1019,7 @@ static int backward_impl(const ptyro_ms_params* p, int ckpt_every, const float* 
     if ((rc = fft2_planes(n, M, false, pk, tw, st))) return rc;
   }
   BwdBuffers B;
+  B.status = (unsigned int*)(ws + L.status);
   B.psi = (float2*)(ws + L.psi);
   B.lam = (float2*)(ws + L.lam);
   B.contrib = (float*)(ws + L.contrib);

@@ -42,6 +42,7 @@ struct BwdArgs {
   int beam_epi;            // op2 / op1 ends in k-order: multiply lam by conj(ramp along this axis)
   float sigma2;            // 2 sigma
   float scale;             // 1/N after OP_IFFT
+  unsigned int* status;    // the call's device status word (PTYRO_STATUS_* bits), or null
 };
 
 // Shared memory of an adjoint pass: twiddles + max(paired exchange buffers, tile).
@@ -103,6 +104,7 @@ __device__ __forceinline__ void bwd_body(const BwdArgs& a, const int slot, const
   float2* work = smem + N;
   float2* stg = nullptr;  // TMA staging: psi block, then lambda block, [row][G]
   uint32_t bar = 0;
+  bool tile_ok = true;  // false once this warp's tile wait gave up
   if (TMA) {
     const int wp = threadIdx.x >> 5;
     const uintptr_t base = reinterpret_cast<uintptr_t>(reinterpret_cast<Pair*>(work) + (size_t)(wp * G) * PairBuf<N1, N2>::kSize);
@@ -163,7 +165,9 @@ __device__ __forceinline__ void bwd_body(const BwdArgs& a, const int slot, const
     }
     bwd_load_half<N1, N2, AXIS, 1>(Wl, v, korder_in, t, line, lc, work, pitch);
   } else if (TMA) {
-    if (!mbar_wait(bar, 0, 1 << 20) && lane == 0) atomicAdd(&g_pair_wait_timeouts, 1u);
+    // a warp whose copies never landed computes on stale shared memory but writes no
+    // wave back; it still takes part in the dV tile's block barriers below
+    tile_ok = warp_wait_tile(bar, kTileWaitPolls, a.status);
     if (a.op1 == OP_FFT) {
 #pragma unroll
       for (int r = 0; r < N2; ++r) v[r].re.x = v[r].im.x = 0.f;
@@ -260,7 +264,7 @@ __device__ __forceinline__ void bwd_body(const BwdArgs& a, const int slot, const
     for (int r = 0; r < N2; ++r) stg[G * N + (lam_k ? korder_index<N1, N2>(t, r) : t + N1 * r) * G + gl] = pair_b(v[r]);
     fence_proxy_async_smem();
     __syncwarp();
-    if (lane == 0) {
+    if (lane == 0 && tile_ok) {
       const int x = line0 + warp * G;
       if (store_psi) tma_store_3d(pmap, x, 0, slot, smem_u32(stg));
       tma_store_3d(lmap, x, 0, slot, smem_u32(stg + G * N));

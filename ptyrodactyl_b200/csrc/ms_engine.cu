@@ -187,6 +187,7 @@ int ptyro_ms_steady_pass(const ptyro_ms_params* p, int32_t axis, int32_t reps, v
   if ((rc = check_workspace(L, workspace, workspace_bytes))) return rc;
   char* ws = (char*)workspace;
   PassArgs a = {};
+  a.status = (unsigned int*)(ws + L.status);
   a.wave = (float2*)(ws + L.waves);
   a.trans = (const float2*)(ws + L.trans);
   a.trans_t = (const float2*)(ws + L.trans_t);

@@ -152,7 +152,8 @@ __device__ __forceinline__ void half_body(const PassArgs& a, const int slot, con
 #pragma unroll
     for (int j = 0; j < H; ++j) p[j] = make_pair(w[off(t + N1 * j)], w[off(t + N1 * (j + H))]);
   } else if (TMA) {
-    if (!mbar_wait(bar, 0, 1 << 20) && (threadIdx.x & 31) == 0) atomicAdd(&g_pair_wait_timeouts, 1u);
+    // a warp whose copies never landed leaves its lines untouched (no barrier follows)
+    if (!warp_wait_tile(bar, kTileWaitPolls, a.status)) return;
 #pragma unroll
     for (int j = 0; j < H; ++j) p[j] = make_pair(stg[(t + N1 * j) * G + gl], stg[(t + N1 * (j + H)) * G + gl]);
   } else {

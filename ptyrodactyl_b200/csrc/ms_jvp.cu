@@ -73,6 +73,7 @@ static int jvp_impl(const ptyro_ms_params* p, const float* potential, const floa
                                          std::to_string(workspace_bytes));
   cudaStream_t st = (cudaStream_t)stream;
   char* ws = (char*)workspace;
+  if ((rc = clear_status(ws + L.status, st))) return rc;
   if ((rc = forward_setup(p, L, ws, potential, modes, st))) return rc;
   const int n = p->n, S = p->num_slices, M = p->num_modes, F = field_of(p);
   const size_t nn = (size_t)n * n;

@@ -17,33 +17,10 @@
 #include <cuda.h>
 
 #include "ms_pass.cuh"
+#include "ms_wait.cuh"
 
 namespace ptyro {
 
-// Waits on a TMA completion that gave up after the iteration limit (this
-// translation unit's launches); read on the host by the pass launcher's accessor.
-static __device__ unsigned int g_pair_wait_timeouts = 0;
-
-__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
-__device__ __forceinline__ void mbar_init(uint32_t bar, int count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
-}
-// true once the barrier's phase `parity` has completed; false after `limit` polls
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, int limit) {
-  for (int i = 0; i < limit; ++i) {
-    uint32_t done;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(done)
-        : "r"(bar), "r"(parity)
-        : "memory");
-    if (done) return true;
-  }
-  return false;
-}
 // plain 3-D tiled TMA load of box (x, y, z) into this CTA's own shared memory only
 __device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap* map, int x, int y, int z, uint32_t bar) {
   asm volatile(
@@ -105,8 +82,8 @@ __device__ __forceinline__ Pair cmul_pp(Pair a, Pair w) {
 // rows of the slot with one tiled TMA copy (wmap: the batch's wave slots as a 3-D
 // tensor (x, y, slot) of 8-byte elements, box 2 G x N x 1), into and out of its own
 // exchange buffers, instead of 16-byte loads and stores per row and lane pair; the
-// wait on the copy's mbarrier gives up after a bounded number of polls and counts
-// the failure in g_pair_wait_timeouts.
+// wait on the copy's mbarrier gives up after a bounded number of polls, and then
+// the warp flags the call's status word and skips its lines (warp_wait_tile).
 // GEN: the first and last slice passes too: op1 may be OP_IFFT (the wave arrives
 // transformed along this axis; inverse transform and a.scale instead of finishing a
 // convolution) and op2 OP_FFT (forward transform instead of starting one). With
@@ -177,7 +154,8 @@ __device__ __forceinline__ void pair_body(const PassArgs& a, const int slot, con
     for (int j = 0; j < N2; ++j)
       v[j] = make_pair(w[(size_t)la * N + t + N1 * j], w[(size_t)lb * N + t + N1 * j]);
   } else if (TMA) {
-    if (!mbar_wait(bar, 0, 1 << 20) && lane == 0) atomicAdd(&g_pair_wait_timeouts, 1u);
+    // a warp whose copy never landed leaves its lines untouched (no barrier follows)
+    if (!warp_wait_tile(bar, kTileWaitPolls, a.status)) return;
 #pragma unroll
     for (int j = 0; j < N2; ++j) {
       const float4 q = *reinterpret_cast<const float4*>(stg + (t + N1 * j) * (2 * G) + 2 * gl);

@@ -89,6 +89,7 @@ struct PassArgs {
   // src == SRC_WAVE and op1 == OP_IFFT), or null
   const float2* tilt;
   int amp_shift;           // amp_store receives the fftshifted amplitude with plane stride res_stride
+  unsigned int* status;    // the call's device status word (PTYRO_STATUS_* bits), or null
 };
 
 template <int N1, int N2>

@@ -18,6 +18,22 @@ namespace ptyro {
 // Number of engine kernels enqueued by this process (all devices, all threads).
 extern std::atomic<unsigned long long> g_launches;
 
+// Per-device "first time" flag for state that CUDA keeps per device, such as a
+// kernel's dynamic shared memory limit (cudaFuncSetAttribute): first() is true once
+// for every device ordinal below kDevices it is called with (the current device),
+// and always for higher ordinals. Two threads may both see true; setting the
+// attribute twice is harmless.
+struct DeviceOnce {
+  static constexpr int kDevices = 64;
+  std::atomic<unsigned long long> mask{0};
+  bool first() {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kDevices) return true;
+    const unsigned long long bit = 1ull << dev;
+    return (mask.fetch_or(bit, std::memory_order_relaxed) & bit) == 0;
+  }
+};
+
 // cuTensorMapEncodeTiled from the driver (no link-time dependency on libcuda), or null.
 inline PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
   static PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
@@ -76,11 +92,10 @@ int launch_pass_s(const PassArgs& a, int grid_y, cudaStream_t st) {
   constexpr int N = Geo::N;
   constexpr int W = Geo::kWarps;
   const size_t smem = STEADY ? Geo::smem_bytes_steady(W) : Geo::smem_bytes(W);
-  static bool attr_done = false;  // once per template instance
-  if (!attr_done) {
+  static DeviceOnce attr_done;  // per device: the attribute is per-device state
+  if (attr_done.first()) {
     cudaFuncSetAttribute(ms_pass_kernel<N1, N2, AXIS, W, MINB, STEADY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)smem);
-    attr_done = true;
   }
   dim3 grid(N / Geo::kLines, grid_y);
   ms_pass_kernel<N1, N2, AXIS, W, MINB, STEADY><<<grid, W * 32, smem, st>>>(a);
@@ -96,11 +111,10 @@ int launch_bwd_w(const BwdArgs& a, int grid_y, cudaStream_t st, const CUtensorMa
   constexpr int W = Geo::kWarps;
   constexpr int MINB = N2 <= 16 ? 2 : 1;  // two resident CTAs where the register budget allows
   const size_t smem = bwd_smem_bytes<N1, N2>(W);
-  static bool attr_done = false;
-  if (!attr_done) {
+  static DeviceOnce attr_done;  // per device: the attribute is per-device state
+  if (attr_done.first()) {
     cudaFuncSetAttribute(ms_bwd_pass_kernel<N1, N2, AXIS, W, MINB, TMA>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)smem);
-    attr_done = true;
   }
   static const CUtensorMap kNoMap = {};
   dim3 grid(N / Geo::kLines, grid_y);
@@ -129,11 +143,10 @@ int launch_jvp_t(const JvpArgs& a, int grid_y, cudaStream_t st) {
   constexpr int W = Geo::kWarps;
   constexpr int MINB = N2 <= 16 ? 2 : 1;
   const size_t smem = bwd_smem_bytes<N1, N2>(W);
-  static bool attr_done = false;
-  if (!attr_done) {
+  static DeviceOnce attr_done;  // per device: the attribute is per-device state
+  if (attr_done.first()) {
     cudaFuncSetAttribute(ms_jvp_pass_kernel<N1, N2, AXIS, W, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)smem);
-    attr_done = true;
   }
   dim3 grid(N / Geo::kLines, grid_y);
   ms_jvp_pass_kernel<N1, N2, AXIS, W, MINB><<<grid, W * 32, smem, st>>>(a);
@@ -149,16 +162,19 @@ int launch_pipe_t(const PassArgs& a, int nslots, cudaStream_t st) {
   constexpr int W = Geo::kWarps;
   using PG = PipeGeom<N1, N2, AXIS, W>;
   const size_t smem = PG::smem_bytes();
-  static int resident = 0;  // CTAs of this kernel per SM x SMs
+  static int resident_of[DeviceOnce::kDevices] = {};  // CTAs of this kernel per SM x SMs, per device
+  int dev = 0;
+  cudaGetDevice(&dev);
+  int resident = dev >= 0 && dev < DeviceOnce::kDevices ? resident_of[dev] : 0;
   if (!resident) {
     cudaFuncSetAttribute(ms_pass_pipe_kernel<N1, N2, AXIS, W, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)smem);
-    int per_sm = 0, dev = 0, sms = 0;
+    int per_sm = 0, sms = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ms_pass_pipe_kernel<N1, N2, AXIS, W, MINB>, W * 32,
                                                   smem);
-    cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     resident = (per_sm > 0 ? per_sm : 1) * (sms > 0 ? sms : 1);
+    if (dev >= 0 && dev < DeviceOnce::kDevices) resident_of[dev] = resident;
   }
   const int tiles = Geo::N / Geo::kLines;
   int rows = resident / tiles;
@@ -176,11 +192,10 @@ template <int N1, int N2, int AXIS, int W, int MINB, bool PRE, bool DIRECT = fal
 int launch_pair_w(const PassArgs& a, int grid_y, cudaStream_t st, const CUtensorMap* wmap = nullptr) {
   using PG = PairGeom<N1, N2, W, PRE>;
   const size_t smem = PG::smem_bytes();
-  static bool attr_done = false;
-  if (!attr_done) {
+  static DeviceOnce attr_done;  // per device: the attribute is per-device state
+  if (attr_done.first()) {
     cudaFuncSetAttribute(ms_pass_pair_kernel<N1, N2, AXIS, W, MINB, PRE, DIRECT, TMA, GEN>,
                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    attr_done = true;
   }
   static const CUtensorMap kNoMap = {};
   dim3 grid(PG::N / PG::kLines, grid_y);
@@ -223,11 +238,10 @@ int launch_half_w(const PassArgs& a, int grid_y, cudaStream_t st, const CUtensor
   using Geo = PassGeom<N1, N2>;
   constexpr int W = Geo::kWarps;
   const size_t smem = Geo::smem_bytes(W);
-  static bool attr_done = false;
-  if (!attr_done) {
+  static DeviceOnce attr_done;  // per device: the attribute is per-device state
+  if (attr_done.first()) {
     cudaFuncSetAttribute(ms_pass_half_kernel<N1, N2, AXIS, W, MINB, TMA>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)smem);
-    attr_done = true;
   }
   static const CUtensorMap kNoMap = {};
   dim3 grid(Geo::N / Geo::kLines, grid_y);
@@ -290,11 +304,10 @@ int launch_pass_multi_t(const PassArgs* descs, const int2* rows, int nrows, cuda
   using Geo = PassGeom<N1, N2>;
   constexpr int W = Geo::kWarps;
   const size_t smem = Geo::smem_bytes(W);
-  static bool attr_done = false;
-  if (!attr_done) {
+  static DeviceOnce attr_done;  // per device: the attribute is per-device state
+  if (attr_done.first()) {
     cudaFuncSetAttribute(ms_pass_multi_kernel<N1, N2, AXIS, W, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)smem);
-    attr_done = true;
   }
   dim3 grid(Geo::N / Geo::kLines, nrows);
   ms_pass_multi_kernel<N1, N2, AXIS, W, MINB><<<grid, W * 32, smem, st>>>(descs, rows);
@@ -311,11 +324,10 @@ int launch_pass_pair_multi_t(const PassArgs* descs, const int2* rows, int nrows,
     using Geo = PassGeom<N1, N2>;
     constexpr int W = Geo::kWarps;
     const size_t smem = Geo::smem_bytes(W);
-    static bool attr_done = false;
-    if (!attr_done) {
+    static DeviceOnce attr_done;  // per device: the attribute is per-device state
+    if (attr_done.first()) {
       cudaFuncSetAttribute(ms_pass_half_multi_kernel<N1, N2, AXIS, W, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)smem);
-      attr_done = true;
     }
     dim3 grid(Geo::N / Geo::kLines, nrows);
     ms_pass_half_multi_kernel<N1, N2, AXIS, W, 2><<<grid, W * 32, smem, st>>>(descs, rows);
@@ -330,11 +342,10 @@ int launch_pass_pair_multi_t(const PassArgs* descs, const int2* rows, int nrows,
     constexpr int MINB = 16 / W;
     using PG = PairGeom<N1, N2, W, false>;
     const size_t smem = PG::smem_bytes();
-    static bool attr_done = false;
-    if (!attr_done) {
+    static DeviceOnce attr_done;  // per device: the attribute is per-device state
+    if (attr_done.first()) {
       cudaFuncSetAttribute(ms_pass_pair_multi_kernel<N1, N2, AXIS, W, MINB>,
                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      attr_done = true;
     }
     dim3 grid(N / PG::kLines, nrows);
     ms_pass_pair_multi_kernel<N1, N2, AXIS, W, MINB><<<grid, W * 32, smem, st>>>(descs, rows);
@@ -349,11 +360,10 @@ int launch_bwd_multi_t(const BwdArgs* descs, const int2* rows, int nrows, cudaSt
   constexpr int W = Geo::kWarps;
   constexpr int MINB = N2 <= 16 ? 2 : 1;
   const size_t smem = bwd_smem_bytes<N1, N2>(W);
-  static bool attr_done = false;
-  if (!attr_done) {
+  static DeviceOnce attr_done;  // per device: the attribute is per-device state
+  if (attr_done.first()) {
     cudaFuncSetAttribute(ms_bwd_multi_kernel<N1, N2, AXIS, W, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)smem);
-    attr_done = true;
   }
   dim3 grid(Geo::N / Geo::kLines, nrows);
   ms_bwd_multi_kernel<N1, N2, AXIS, W, MINB><<<grid, W * 32, smem, st>>>(descs, rows);

@@ -7,6 +7,8 @@ reconstruction — :class:`GraphedForward` captures that sequence once into a CU
 graph on static input/output buffers and replays it, so the host issues one
 graph launch instead of thousands of kernel launches. Inputs are updated in place
 (``copy_`` into :attr:`slices`, :attr:`modes`, :attr:`positions`...) between replays.
+Each replay zeroes and then fills the device status words at the start of its
+workspaces; :meth:`check` reads them after a replay.
 """
 
 from __future__ import annotations
@@ -91,3 +93,16 @@ class GraphedForward:
         """Run the captured forward on the current stream; returns the static output."""
         self.graph.replay()
         return self.out
+
+    def status(self) -> int:
+        """OR of the device status words the last replay left (waits for the replay)."""
+        v = 0
+        for part in self.parts:
+            v |= int(part[3][:4].view(torch.int32).item())
+        return v
+
+    def check(self) -> None:
+        """Raise ``DeviceStatusError`` if the last replay's kernels reported a failure."""
+        v = self.status()
+        if v:
+            raise _lib.DeviceStatusError("graphed forward", v)

@@ -154,7 +154,7 @@ def run_forward(slices: torch.Tensor, slice_thickness: float, modes: torch.Tenso
                 positions: torch.Tensor, voltage_kv: float, calib_ang: float, shift_calib_ang: float,
                 out: Optional[torch.Tensor] = None, batch: int = 0, plain: bool = False,
                 tune: Optional[int] = None, windows: Optional[torch.Tensor] = None, accumulate: bool = False,
-                lanes: int = 0) -> torch.Tensor:
+                lanes: int = 0, status: Optional[torch.Tensor] = None) -> torch.Tensor:
     """Device-level forward: all tensors already on one CUDA device.
 
     slices (F, F, S) float32 (any strides), modes (n, n, M) complex64 (any strides),
@@ -164,6 +164,9 @@ def run_forward(slices: torch.Tensor, slice_thickness: float, modes: torch.Tenso
     ``accumulate`` the intensities are added into ``out`` instead. ``lanes`` > 1
     runs contiguous probe ranges as concurrent forwards on side streams (0: two
     lanes when the probes' waves exceed 256 MiB); results do not depend on it.
+    ``status`` (an int32 device word from ``_lib.new_status``) collects the call's
+    device status bits asynchronously; nothing here synchronises, so the caller checks
+    it (``_lib.check_status``) once it needs the results.
     """
     lib = _lib.load()
     dev = slices.device
@@ -179,14 +182,20 @@ def run_forward(slices: torch.Tensor, slice_thickness: float, modes: torch.Tenso
         main = torch.cuda.current_stream(dev)
         bounds = [num_probes * i // lanes for i in range(lanes + 1)]
         streams = _side_streams(dev, lanes)
-        for (lo, hi), st in zip(zip(bounds[:-1], bounds[1:]), streams):
+        # one status word per lane: the lanes run concurrently
+        lane_status = [None if status is None else _lib.new_status(dev) for _ in streams]
+        for (lo, hi), st, ls in zip(zip(bounds[:-1], bounds[1:]), streams, lane_status):
             st.wait_stream(main)
             with torch.cuda.stream(st):
                 run_forward(slices, slice_thickness, modes, weights, positions[lo:hi], voltage_kv, calib_ang,
                             shift_calib_ang, out=out[lo:hi], batch=batch, plain=plain, tune=tune,
-                            windows=None if windows is None else windows[lo:hi], accumulate=accumulate, lanes=1)
+                            windows=None if windows is None else windows[lo:hi], accumulate=accumulate, lanes=1,
+                            status=ls)
         for st in streams:
             main.wait_stream(st)
+        for ls in lane_status:
+            if ls is not None:
+                status.bitwise_or_(ls)
         return out
     prm = ms_params(n, slices.shape[2], modes.shape[2], num_probes, voltage_kv, slice_thickness,
                     calib_ang, shift_calib_ang, slices.stride(), modes.stride(), batch, tune, f, windows,
@@ -203,13 +212,16 @@ def run_forward(slices: torch.Tensor, slice_thickness: float, modes: torch.Tenso
     rc = fn(ctypes.byref(prm), slices.data_ptr(), modes.data_ptr(), weights.data_ptr(),
             positions.data_ptr(), out.data_ptr(), ws.data_ptr(), ws_bytes, _stream_ptr(dev))
     _lib.check(rc)
+    if not plain:
+        _lib.gather_status(status, ws)
     return out
 
 
 def run_forward_to_host(slices: torch.Tensor, slice_thickness: float, modes: torch.Tensor, weights: torch.Tensor,
                         positions: torch.Tensor, voltage_kv: float, calib_ang: float, shift_calib_ang: float,
                         host_out: torch.Tensor, chunks: int = 8, lanes: int = 2, tune: Optional[int] = None,
-                        windows: Optional[torch.Tensor] = None) -> torch.Tensor:
+                        windows: Optional[torch.Tensor] = None,
+                        status: Optional[torch.Tensor] = None) -> torch.Tensor:
     """``run_forward`` whose patterns land in a host tensor (pinned for overlap): the
     probes run as ``chunks`` consecutive ranges on ``lanes`` compute streams, and
     each range's patterns are copied to the host on a copy stream as soon as the
@@ -227,6 +239,7 @@ def run_forward_to_host(slices: torch.Tensor, slice_thickness: float, modes: tor
     copy = _side_streams(dev, 1 + max(1, lanes))[-1]
     chunks = max(1, min(int(chunks), num_probes))
     bounds = [num_probes * i // chunks for i in range(chunks + 1)]
+    lane_status = [None if status is None else _lib.new_status(dev) for _ in streams]
     for st in streams + [copy]:
         st.wait_stream(main)
     for i, (lo, hi) in enumerate(zip(bounds[:-1], bounds[1:])):
@@ -234,7 +247,8 @@ def run_forward_to_host(slices: torch.Tensor, slice_thickness: float, modes: tor
         with torch.cuda.stream(st):
             run_forward(slices, slice_thickness, modes, weights, positions[lo:hi], voltage_kv, calib_ang,
                         shift_calib_ang, out=dev_out[lo:hi], tune=tune,
-                        windows=None if windows is None else windows[lo:hi], lanes=1)
+                        windows=None if windows is None else windows[lo:hi], lanes=1,
+                        status=lane_status[i % len(streams)])
         done = torch.cuda.Event()
         done.record(st)
         copy.wait_event(done)
@@ -242,6 +256,9 @@ def run_forward_to_host(slices: torch.Tensor, slice_thickness: float, modes: tor
             host_out[lo:hi].copy_(dev_out[lo:hi], non_blocking=True)
     for st in streams + [copy]:
         main.wait_stream(st)
+    for ls in lane_status:
+        if ls is not None:
+            status.bitwise_or_(ls)
     return host_out
 
 
@@ -274,7 +291,8 @@ def stem_4d(pot_slice: PotentialSlices, beam: ProbeModes, microscope: Microscope
     field is ``positions * real_space_calib_ang`` as in the reference. ``data`` is a
     float32 CUDA tensor (P, H, W), or ``out`` when given: a CUDA tensor is written in
     place; a host tensor (pinned) receives the patterns chunk by chunk while the
-    remaining probes compute.
+    remaining probes compute. The call waits for its kernels and raises
+    ``DeviceStatusError`` if they reported a failure (a bounded wait that gave up).
     """
     if detector.scan_positions_px is None:
         raise ValueError("detector.scan_positions_px is required")
@@ -298,11 +316,15 @@ def stem_4d(pot_slice: PotentialSlices, beam: ProbeModes, microscope: Microscope
         data = stem_4d_patterns(slices, modes, weights, positions, pot_slice.slice_thickness,
                                 microscope.voltage_kv, calib, detector.real_space_calib_ang)
     elif out is not None and not out.is_cuda:
+        status = _lib.new_status(dev)
         data = run_forward_to_host(slices, pot_slice.slice_thickness, modes, weights, positions,
-                                   microscope.voltage_kv, calib, detector.real_space_calib_ang, out)
+                                   microscope.voltage_kv, calib, detector.real_space_calib_ang, out, status=status)
+        _lib.check_status(status, "stem_4d")
     else:
+        status = _lib.new_status(dev)
         data = run_forward(slices, pot_slice.slice_thickness, modes, weights, positions,
-                           microscope.voltage_kv, calib, detector.real_space_calib_ang, out=out)
+                           microscope.voltage_kv, calib, detector.real_space_calib_ang, out=out, status=status)
+        _lib.check_status(status, "stem_4d")
     if out is not None and data is not out:
         out.copy_(data)
         data = out
@@ -332,8 +354,10 @@ def stem_4d_windowed(pot_slice: PotentialSlices, beam: ProbeModes, microscope: M
         data = stem_4d_patterns(slices, modes, weights, positions, pot_slice.slice_thickness,
                                 microscope.voltage_kv, calib, detector.real_space_calib_ang, windows=win)
     else:
+        status = _lib.new_status(dev)
         data = run_forward(slices, pot_slice.slice_thickness, modes, weights, positions, microscope.voltage_kv,
-                           calib, detector.real_space_calib_ang, windows=win)
+                           calib, detector.real_space_calib_ang, windows=win, status=status)
+        _lib.check_status(status, "stem_4d_windowed")
     fourier_calib = 1.0 / (modes.shape[0] * calib)
     scan_positions = detector.scan_positions_px.to(torch.float64) * detector.real_space_calib_ang
     return create_stem4d(data, detector.real_space_calib_ang, fourier_calib, scan_positions, microscope.voltage_kv)
@@ -355,10 +379,12 @@ def stem_4d_frozen_phonon(pot_slices: list, beam: ProbeModes, microscope: Micros
     n = modes.shape[0]
     out = torch.zeros((positions.shape[0], n, n), dtype=torch.float32, device=dev)
     calib = min(float(pot_slices[0].calib), float(beam.calib))
+    status = _lib.new_status(dev)
     for ps in pot_slices:
         slices = as_tensor(ps.slices, torch.float32, dev)
         run_forward(slices, ps.slice_thickness, modes, wscaled, positions, microscope.voltage_kv, calib,
-                    detector.real_space_calib_ang, out=out, accumulate=True)
+                    detector.real_space_calib_ang, out=out, accumulate=True, status=status)
+    _lib.check_status(status, "stem_4d_frozen_phonon")
     fourier_calib = 1.0 / (n * calib)
     scan_positions = detector.scan_positions_px.to(torch.float64) * detector.real_space_calib_ang
     return create_stem4d(out, detector.real_space_calib_ang, fourier_calib, scan_positions, microscope.voltage_kv)
@@ -407,7 +433,10 @@ def stem4d_sharded(probe_modes: ProbeModes, sample: AtomicSliceData, microscope:
     bounds = as_tensor(sample.slice_z_bounds, torch.float64)
     thickness = float(bounds[0, 1] - bounds[0, 0])
     positions = as_tensor(detector.scan_positions_ang, torch.float64, dev).reshape(-1, 2).contiguous()
-    data = run_forward(slices, thickness, modes, weights, positions, microscope.voltage_kv, calib, calib)
+    status = _lib.new_status(dev)
+    data = run_forward(slices, thickness, modes, weights, positions, microscope.voltage_kv, calib, calib,
+                       status=status)
+    _lib.check_status(status, "stem4d_sharded")
     return create_stem4d(data, calib, 1.0 / (n * calib), detector.scan_positions_ang.to(torch.float64),
                          microscope.voltage_kv)
 
@@ -428,8 +457,10 @@ def cbed_image(pot_slices: PotentialSlices, beam: ProbeModes, microscope: Micros
         data = ensemble_patterns(slices, pot_slices.slice_thickness, beam, microscope.ensemble,
                                  microscope.voltage_kv, calib, zero, calib)[0]
     else:
+        status = _lib.new_status(dev)
         data = run_forward(slices, pot_slices.slice_thickness, modes, weights, zero,
-                           microscope.voltage_kv, calib, calib)[0]
+                           microscope.voltage_kv, calib, calib, status=status)[0]
+        _lib.check_status(status, "cbed_image")
     inv = 1.0 / (modes.shape[0] * calib)
     return create_calibrated_array(data, inv, inv, False)
 

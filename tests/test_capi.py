@@ -138,3 +138,19 @@ def test_atomic_slice_data_validation():
     for kw, msg in bad:
         with pytest.raises(ValueError, match=msg):
             pb.create_atomic_slice_data(**{**base, **kw})
+
+
+def test_device_status_host_logic():
+    """Status words are ORed per call and any set bit raises (host side, no GPU)."""
+    import torch
+    st = torch.zeros(1, dtype=torch.int32)
+    ws = torch.zeros(_lib.WS_STATUS_BYTES, dtype=torch.uint8)
+    _lib.gather_status(st, ws)
+    _lib.check_status(st, "clean")
+    ws[:4] = torch.tensor([_lib.STATUS_WAIT_TIMEOUT, 0, 0, 0], dtype=torch.uint8)
+    _lib.gather_status(st, ws)
+    _lib.gather_status(None, ws)  # no status tensor: nothing to do
+    with pytest.raises(_lib.DeviceStatusError, match="bounded wait"):
+        _lib.check_status(st, "failed")
+    with pytest.raises(_lib.DeviceStatusError):
+        _lib.check_workspace_status(ws, "failed")

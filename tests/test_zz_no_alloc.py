@@ -88,3 +88,54 @@ def test_noalloc_rejects_jobs_beyond_its_scratch(case):
                                       torch.cuda.current_stream().cuda_stream)
     assert rc == _lib.PTYRO_ERR_WORKSPACE
     assert "no-alloc forward has a fixed" in lib.ptyro_last_error().decode()
+
+
+def _case_256(num_slices, num_probes):
+    w = synth.CONFIG2
+    dev = torch.device("cuda")
+    pot = torch.as_tensor(synth.potential_slices(w, num_slices=num_slices), device=dev)
+    probe = R.make_probe(w.voltage_kv, w.aperture_mrad, (w.n, w.n), w.calib * 100.0, w.defocus_ang, w.c3_ang)
+    modes = torch.as_tensor(probe[..., None].astype(np.complex64), device=dev)
+    weights = torch.ones(1, dtype=torch.float32, device=dev)
+    pos = torch.as_tensor(synth.raster_positions(w)[::613][:num_probes], device=dev).contiguous()
+    from ptyrodactyl_b200.simulations import default_tune
+    prm = ms_params(w.n, num_slices, 1, pos.shape[0], w.voltage_kv, synth.SLICE_DZ, w.calib, w.calib, pot.stride(),
+                    modes.stride(), batch=0, tune=default_tune(w.n))
+    return prm, pot, modes, weights, pos
+
+
+def _noalloc(lib, prm, pot, modes, weights, pos):
+    out = torch.full((prm.num_probes, prm.n, prm.n), float("nan"), dtype=torch.float32, device=pot.device)
+    rc = lib.ptyro_ms_forward_noalloc(ctypes.byref(prm), pot.data_ptr(), modes.data_ptr(), weights.data_ptr(),
+                                      pos.data_ptr(), out.data_ptr(), torch.cuda.current_stream().cuda_stream)
+    _lib.check(rc)
+    torch.cuda.synchronize()
+    return out.cpu().numpy()
+
+
+def test_noalloc_default_variant_256_bit_identical(case):
+    """The default 256^2 launch variant (TMA column blocks, paired passes, line-pair
+    transmission tables) on the static scratch: 8 slices keep every table, and the
+    patterns equal the workspace forward's bit for bit, twice, with no wait given up."""
+    lib = case[0]
+    prm, pot, modes, weights, pos = _case_256(8, 5)
+    assert lib.ptyro_ms_workspace_bytes(ctypes.byref(prm)) <= _lib.STATIC_SCRATCH_BYTES
+    want = _workspace_forward(lib, prm, pot, modes, weights, pos)
+    t0 = lib.ptyro_pass_wait_timeouts()
+    for _ in range(2):
+        assert np.array_equal(_noalloc(lib, prm, pot, modes, weights, pos), want)
+    assert lib.ptyro_pass_wait_timeouts() == t0
+
+
+def test_noalloc_runs_the_full_256_workload_depth(case):
+    """256^2 with all 50 slices under the default variant: the interleaved tables do not
+    fit the fixed scratch, so the call drops them (bit-identical results) instead of
+    rejecting the job."""
+    lib = case[0]
+    prm, pot, modes, weights, pos = _case_256(50, 3)
+    one = ms_params(prm.n, prm.num_slices, 1, 1, prm.voltage_kv, prm.slice_thickness_ang, prm.calib_ang,
+                    prm.shift_calib_ang, pot.stride(), modes.stride(), batch=1, tune=prm.tune)
+    assert lib.ptyro_ms_workspace_bytes(ctypes.byref(one)) > _lib.STATIC_SCRATCH_BYTES
+    got = _noalloc(lib, prm, pot, modes, weights, pos)
+    want = _workspace_forward(lib, prm, pot, modes, weights, pos)
+    assert np.array_equal(got, want)
