@@ -59,9 +59,12 @@ def _cpu_worker(task):
                                            w.defocus_ang, w.c3_ang)
         _CPU_STATE["pos"] = synth.raster_positions(w)
     pos = _CPU_STATE["pos"][np.asarray(idx)]
+    args = (_CPU_STATE["pot"], synth.SLICE_DZ, w.calib, _CPU_STATE["probe"][..., None], [1.0], w.calib,
+            w.voltage_kv, pos, w.calib)
+    if name == "check":  # the checker: the float32 and float64 restatements' patterns
+        return (R.stem_4d(*args, dtype=np.complex64)["data"], R.stem_4d(*args, dtype=np.complex128)["data"])
     t0 = time.perf_counter()
-    R.stem_4d(_CPU_STATE["pot"], synth.SLICE_DZ, w.calib, _CPU_STATE["probe"][..., None], [1.0], w.calib,
-              w.voltage_kv, pos, w.calib, dtype=np.complex128)
+    R.stem_4d(*args, dtype=np.complex128)
     return time.perf_counter() - t0
 
 
@@ -93,6 +96,10 @@ class CpuOracle:
         self.pool.map(_cpu_worker, tasks)
         wall = time.perf_counter() - t0
         return self.procs * probes_per_proc * WORKLOAD.num_slices, wall
+
+    def check(self, idx) -> tuple:
+        """Oracle patterns (float32 path, float64 path) of the probes ``idx`` of the workload."""
+        return self.pool.apply(_cpu_worker, (("check", list(idx)),))
 
     def close(self):
         self.pool.close()
@@ -349,12 +356,24 @@ def run_ours(args, rank, world, local_rank):
     del pws
 
     cpu_baseline = None
+    parity = None
     if cpu is not None:
         upd, wall = 0, 0.0
         while wall < args.cpu_seconds:
             u, t = cpu.step(1)
             upd += u
             wall += t
+        # parity of the timed forward's patterns on a sample of probes (first, middle, last)
+        idx = [0, P // 2, P - 1]
+        want32, want64 = cpu.check(idx)
+        got = out_d[idx].double().cpu().numpy()
+
+        def rel(a, b):
+            return float(np.linalg.norm((a - b).ravel()) / np.linalg.norm(b.ravel()))
+
+        parity = {"probes": idx, "rel_l2_vs_float32_restatement": rel(got, want32),
+                  "rel_l2_vs_float64_oracle": rel(got, want64),
+                  "float32_restatement_vs_float64_oracle": rel(want32, want64)}
         cpu.close()
         cpu_baseline = {"value": upd / wall, "unit": UNIT, "cores": cpu.procs, "kind": "port",
                         "sample": f"{upd // S} probes of this workload (all 50 slices each), NumPy complex128 "
@@ -385,8 +404,22 @@ def run_ours(args, rank, world, local_rank):
             "clocks": clk,
             "cpu_baseline": cpu_baseline,
             "checks": {"pattern_sum_max_rel_err": max_sum_err,
-                       "tma_wait_timeouts": int(lib.ptyro_pass_wait_timeouts())},
+                       "tma_wait_timeouts": int(lib.ptyro_pass_wait_timeouts()),
+                       "device_status": graphed.status() if graphed is not None else None,
+                       "sampled_parity": parity},
         }
+        if world == 1 and not args.no_extras:
+            # the other two halves of the metric, on the same GPU after the headline
+            g = run_grad(argparse.Namespace(**{**vars(args), "steps": 12, "warmup": 3}), rank, world, local_rank)
+            line["adjoint_over_forward"] = g["adjoint_over_forward"]
+            line["gradient"] = {k: g[k] for k in ("metric", "value", "unit", "forward_ms",
+                                                  "forward_with_residuals_ms", "adjoint_ms",
+                                                  "adjoint_over_forward", "value_and_grad_over_forward",
+                                                  "config")}
+            sv = run_serve(argparse.Namespace(**{**vars(args), "requests": 48}), rank, world, local_rank)
+            line["p50_ms"], line["p99_ms"] = sv["p50_ms"], sv["p99_ms"]
+            line["serving"] = {k: sv[k] for k in ("metric", "value", "unit", "p50_ms", "p99_ms", "mean_ms",
+                                                  "requests", "completed", "makespan_s", "config")}
         print(json.dumps(line), flush=True)
 
 
@@ -525,8 +558,8 @@ def run_grad(args, rank, world, local_rank):
                    "residual_bytes": int(res.numel() * 4), "backward_batch": bprm.batch,
                    "targets": f"Poisson noise at {w.dose:g} e- per pattern", "loss": "amplitude"},
     }
-    if rank == 0:
-        print(json.dumps(line), flush=True)
+    del res, ws, bws
+    return line
 
 
 # ----------------------------------------------------------------------------- 512^2 leg
@@ -661,8 +694,53 @@ def run_serve(args, rank, world, local_rank):
                    "admission": "HBM footprint (arena) + wave-slot budget",
                    "targets": "uniform random patterns (gradient cost does not depend on them)"},
     }
-    if rank == 0:
-        print(json.dumps(line), flush=True)
+    return line
+
+
+# ----------------------------------------------------------------------------- profiling case
+def run_profile_case(args, rank, world, local_rank):
+    """A small, self-checking case of the forward engine for profilers: one batched
+    forward over ``--probes`` scan positions of the perovskite workload (``--grid``
+    edge, 2 slices, one batch), then ``--reps`` steady-state passes per axis
+    (``ptyro_ms_steady_pass``) on the wave slots the forward left in the workspace.
+    Pass-kernel launches: 6 in the forward (setup kernels aside), then ``--reps`` row
+    passes and ``--reps`` column passes. Exits non-zero if the patterns are not finite
+    or the device status word is set."""
+    import torch
+    from ptyrodactyl_b200 import _lib
+    from ptyrodactyl_b200.simulations import make_probe, ms_params
+    from ptyrodactyl_b200.types import create_detector_config, create_microscope_config
+
+    n, probes, reps = args.grid, args.probes, args.reps
+    tune = default_tune(n) if args.tune < 0 else args.tune
+    w = synth.CONFIG2
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    lib = _lib.load()
+    if n == w.n:
+        pot = torch.as_tensor(synth.potential_slices(w, num_slices=2), device=dev)
+    else:
+        pot = torch.rand((n, n, 2), generator=torch.Generator(device=dev).manual_seed(1), device=dev) * 50
+    mic = create_microscope_config(w.voltage_kv, w.aperture_mrad, probe_shape=(n, n))
+    probe = make_probe(mic, create_detector_config(w.calib))[..., None].contiguous()
+    pos = torch.as_tensor(synth.raster_positions(w), device=dev)[:probes].contiguous()
+    probes = pos.shape[0]
+    wt = torch.ones(1, device=dev)
+    prm = ms_params(n, 2, 1, probes, w.voltage_kv, synth.SLICE_DZ, w.calib, w.calib, pot.stride(), probe.stride(),
+                    probes, tune)
+    nb = lib.ptyro_ms_workspace_bytes(ctypes.byref(prm))
+    ws = torch.empty(nb, dtype=torch.uint8, device=dev)
+    out = torch.empty((probes, n, n), device=dev)
+    st = torch.cuda.current_stream().cuda_stream
+    _lib.check(lib.ptyro_ms_forward(ctypes.byref(prm), pot.data_ptr(), probe.data_ptr(), wt.data_ptr(),
+                                    pos.data_ptr(), out.data_ptr(), ws.data_ptr(), nb, st))
+    for axis in (0, 1):
+        _lib.check(lib.ptyro_ms_steady_pass(ctypes.byref(prm), axis, reps, ws.data_ptr(), nb, st))
+    torch.cuda.synchronize()
+    total = float(out.sum())
+    status = int(ws[:4].view(torch.int32).item())
+    print(f"profile case n={n} probes={probes} reps={reps} tune={tune}: pattern sum {total:.6g}, status {status}")
+    return 0 if (total == total and abs(total) != float("inf") and status == 0) else 1
 
 
 # ----------------------------------------------------------------------------- reference arm
@@ -708,8 +786,13 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--mode", choices=("forward", "grad", "serve", "config3"), default="forward")
-    ap.add_argument("--probes", type=int, default=2048, help="config3 mode: scan positions sampled")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="forward mode: skip the gradient and serving legs that follow the headline")
+    ap.add_argument("--mode", choices=("forward", "grad", "serve", "config3", "profile-case"), default="forward")
+    ap.add_argument("--probes", type=int, default=2048,
+                    help="config3 mode: scan positions sampled; profile-case mode: probes in the one batch")
+    ap.add_argument("--grid", type=int, default=256, help="profile-case mode: grid edge")
+    ap.add_argument("--reps", type=int, default=1, help="profile-case mode: steady passes per axis")
     ap.add_argument("--requests", type=int, default=64, help="serve mode: requests in the mix")
     ap.add_argument("--rate", type=float, default=20.0, help="serve mode: Poisson arrival rate (1/s)")
     ap.add_argument("--seed", type=int, default=5, help="serve mode: mix seed")
@@ -732,12 +815,14 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                 device_id=torch.device("cuda", local_rank))
     try:
-        if args.mode == "grad":
-            run_grad(args, rank, world, local_rank)
-        elif args.mode == "serve":
-            run_serve(args, rank, world, local_rank)
+        if args.mode in ("grad", "serve"):
+            line = (run_grad if args.mode == "grad" else run_serve)(args, rank, world, local_rank)
+            if rank == 0:
+                print(json.dumps(line), flush=True)
         elif args.mode == "config3":
             run_config3(args, rank, world, local_rank)
+        elif args.mode == "profile-case":
+            sys.exit(run_profile_case(args, rank, world, local_rank))
         else:
             run_ours(args, rank, world, local_rank)
     finally:

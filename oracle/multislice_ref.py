@@ -13,7 +13,7 @@ scalars evaluated in float64 and rounded where they enter an array).
 
 Pinned against the reference's golden file
 ``tests/test_data/plan01_ug_reference.npz`` (see ``tests/golden/make_golden.py``
-and ``tests/test_oracle_golden.py``).
+and ``tests/test_oracle.py``).
 """
 
 from __future__ import annotations

@@ -78,17 +78,23 @@ class Stem4dFunction(torch.autograd.Function):
         if P:
             ws_bytes = lib.ptyro_ms_workspace_bytes(ctypes.byref(prm))
             ws = _workspace(ws_bytes, dev)
-            if record:
-                rc = lib.ptyro_ms_forward_ckpt(ctypes.byref(prm), k, slices.data_ptr(), modes.data_ptr(),
-                                               weights.data_ptr(), positions.data_ptr(), out.data_ptr(),
-                                               res.data_ptr(), ws.data_ptr(), ws_bytes, _stream_ptr(dev))
-            else:
-                rc = lib.ptyro_ms_forward(ctypes.byref(prm), slices.data_ptr(), modes.data_ptr(),
-                                          weights.data_ptr(), positions.data_ptr(), out.data_ptr(), ws.data_ptr(),
-                                          ws_bytes, _stream_ptr(dev))
-            _lib.check(rc)
+            with torch.cuda.device(dev):
+                Stem4dFunction._forward_call(lib, prm, k, record, slices, modes, weights, positions, out, res, ws,
+                                             ws_bytes, dev)
             _lib.check_workspace_status(ws, "stem_4d forward")
         return out, res
+
+    @staticmethod
+    def _forward_call(lib, prm, k, record, slices, modes, weights, positions, out, res, ws, ws_bytes, dev):
+        if record:
+            rc = lib.ptyro_ms_forward_ckpt(ctypes.byref(prm), k, slices.data_ptr(), modes.data_ptr(),
+                                           weights.data_ptr(), positions.data_ptr(), out.data_ptr(),
+                                           res.data_ptr(), ws.data_ptr(), ws_bytes, _stream_ptr(dev))
+        else:
+            rc = lib.ptyro_ms_forward(ctypes.byref(prm), slices.data_ptr(), modes.data_ptr(),
+                                      weights.data_ptr(), positions.data_ptr(), out.data_ptr(), ws.data_ptr(),
+                                      ws_bytes, _stream_ptr(dev))
+        _lib.check(rc)
 
     @staticmethod
     def setup_context(ctx, inputs, output):
@@ -108,7 +114,7 @@ class Stem4dFunction(torch.autograd.Function):
             raise RuntimeError("stem_4d was evaluated without residuals (record=False); no backward")
         # under torch.func the rule sees functorch wrappers; the kernels need storage
         saved = [_plain(t) for t in ctx.saved_tensors]
-        with torch._C._DisableFuncTorch():
+        with torch._C._DisableFuncTorch(), torch.cuda.device(saved[0].device):
             g_slices, g_modes, g_pos = Stem4dFunction._adjoint(ctx, saved, _plain(grad_out))
         return (g_slices if ctx.needs_input_grad[0] else None, g_modes if ctx.needs_input_grad[1] else None,
                 None, g_pos, None, None, None, None, None, None, None, None, None)

@@ -209,8 +209,9 @@ def run_forward(slices: torch.Tensor, slice_thickness: float, modes: torch.Tenso
         _lib.check(_lib.PTYRO_ERR_INVALID)
     ws = _workspace(ws_bytes, dev)
     fn = lib.ptyro_ms_forward_plain if plain else lib.ptyro_ms_forward
-    rc = fn(ctypes.byref(prm), slices.data_ptr(), modes.data_ptr(), weights.data_ptr(),
-            positions.data_ptr(), out.data_ptr(), ws.data_ptr(), ws_bytes, _stream_ptr(dev))
+    with torch.cuda.device(dev):  # the engine launches on, and keeps per-device state for, the current device
+        rc = fn(ctypes.byref(prm), slices.data_ptr(), modes.data_ptr(), weights.data_ptr(),
+                positions.data_ptr(), out.data_ptr(), ws.data_ptr(), ws_bytes, _stream_ptr(dev))
     _lib.check(rc)
     if not plain:
         _lib.gather_status(status, ws)

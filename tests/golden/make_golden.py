@@ -10,7 +10,7 @@ capture's scalar parameters, so the tests need neither JAX nor the reference
 tree at run time.
 
 Run from the repository root (needs the reference checkout):
-    python tests/golden/make_golden.py [REFERENCE_ROOT]
+    python tests/golden/make_golden.py REFERENCE_ROOT
 """
 
 from __future__ import annotations
@@ -27,7 +27,9 @@ from oracle.jax_prng import prng_key, uniform_f64  # noqa: E402
 
 
 def main() -> None:
-    ref_root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_golden.py <reference project root>")
+    ref_root = sys.argv[1]
     ref = np.load(os.path.join(ref_root, "tests/test_data/plan01_ug_reference.npz"))
     pot = uniform_f64(prng_key(42), (32, 32, 2)) * 10.0
     out = {
