@@ -616,6 +616,71 @@ def run_config3(args, rank, world, local_rank):
         print(json.dumps(line), flush=True)
 
 
+# ----------------------------------------------------------------------------- 128^2 leg
+def run_config1(args, rank, world, local_rank):
+    """128^2 grid, 8x8 cell, 20 slices: the pass engine (wave slots through L2 once per
+    slice) against the wave-resident kernel (tune bit 32768: one CTA per probe, the
+    wave in shared memory across all slices), both replayed from CUDA graphs, on the
+    16x16 scan (256 probes) and on a 8192-probe sample (the scan at 32 sub-pixel
+    offsets) that fills the GPU; one JSON line."""
+    import torch
+    import ptyrodactyl_b200 as pb
+    from ptyrodactyl_b200.graphs import GraphedForward
+
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    w = synth.CONFIG1
+    n, S = w.n, w.num_slices
+    slices = torch.as_tensor(synth.potential_slices(w), device=dev)
+    mic = pb.create_microscope_config(w.voltage_kv, w.aperture_mrad, probe_shape=(n, n))
+    modes = pb.make_probe(mic, pb.create_detector_config(w.calib))[..., None].contiguous()
+    wts = torch.ones(1, dtype=torch.float32, device=dev)
+    scan = synth.raster_positions(w)
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
+    base = default_tune(n) if args.tune < 0 else args.tune
+    result = {}
+    for label, reps_pos in (("scan_256", 1), ("sample_8192", 32)):
+        pos = np.concatenate([scan + 0.031 * i for i in range(reps_pos)])
+        pos_d = torch.as_tensor(pos, device=dev).contiguous()
+        P = pos.shape[0]
+        row = {"probes": P}
+        outs = {}
+        for kind, tune in (("pass_engine", base & ~32768), ("resident", base | 32768)):
+            g = GraphedForward(slices, modes, wts, pos_d, synth.SLICE_DZ, w.voltage_kv, w.calib, tune=tune,
+                               batch=P if kind == "resident" else 0)
+            for _ in range(args.warmup):
+                g.replay()
+            torch.cuda.synchronize()
+            reps = max(5, args.steps)
+            ts = []
+            for _ in range(reps):
+                flush.zero_()
+                s_, e_ = _events(torch, 2)
+                s_.record()
+                g.replay()
+                e_.record()
+                torch.cuda.synchronize()
+                ts.append(s_.elapsed_time(e_))
+            g.check()
+            ms = statistics.median(ts)
+            upd = float(P) * S / (ms * 1e-3)
+            row[kind] = {"ms_per_forward": ms, "updates_per_s": upd,
+                         "tflops_algorithmic": upd * synth.algorithmic_flops_per_update(n) / 1e12,
+                         "launches_per_forward": g.launches_per_replay, "tune": tune}
+            outs[kind] = g.out.clone()
+        row["bit_identical"] = bool(torch.equal(outs["pass_engine"], outs["resident"]))
+        row["resident_over_pass_engine"] = row["resident"]["updates_per_s"] / row["pass_engine"]["updates_per_s"]
+        result[label] = row
+    line = {"metric": "probe-slice updates/s at 128^2 (20 slices): pass engine vs wave-resident kernel",
+            "mode": "config1", "unit": UNIT, "n_gpus": world, "dtype": "f32", "data": "synthetic",
+            "value": max(result["sample_8192"]["pass_engine"]["updates_per_s"],
+                         result["sample_8192"]["resident"]["updates_per_s"]),
+            "results": result,
+            "config": {"workload": w.name, "grid": n, "slices": S, "voltage_kv": w.voltage_kv,
+                       "aperture_mrad": w.aperture_mrad, "l2": "flushed (256 MB write) before every timed forward"}}
+    return line
+
+
 # ----------------------------------------------------------------------------- serving leg
 def run_serve(args, rank, world, local_rank):
     """Poisson-arrival mix of simulations and gradient solves through the server;
@@ -788,7 +853,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-extras", action="store_true",
                     help="forward mode: skip the gradient and serving legs that follow the headline")
-    ap.add_argument("--mode", choices=("forward", "grad", "serve", "config3", "profile-case"), default="forward")
+    ap.add_argument("--mode", choices=("forward", "grad", "serve", "config1", "config3", "profile-case"),
+                    default="forward")
     ap.add_argument("--probes", type=int, default=2048,
                     help="config3 mode: scan positions sampled; profile-case mode: probes in the one batch")
     ap.add_argument("--grid", type=int, default=256, help="profile-case mode: grid edge")
@@ -815,8 +881,9 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                 device_id=torch.device("cuda", local_rank))
     try:
-        if args.mode in ("grad", "serve"):
-            line = (run_grad if args.mode == "grad" else run_serve)(args, rank, world, local_rank)
+        if args.mode in ("grad", "serve", "config1"):
+            line = {"grad": run_grad, "serve": run_serve, "config1": run_config1}[args.mode](args, rank, world,
+                                                                                      local_rank)
             if rank == 0:
                 print(json.dumps(line), flush=True)
         elif args.mode == "config3":

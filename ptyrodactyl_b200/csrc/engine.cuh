@@ -14,6 +14,7 @@
 
 #include "../../include/ptyro_b200.h"
 #include "ms_pass.cuh"
+#include "ms_resident.cuh"
 #include "pass_launch.cuh"
 
 namespace ptyro {
@@ -295,6 +296,9 @@ static int fft2_planes(int n, int count, bool inverse, float2* data, const float
 
 // ---------------------------------------------------------------- workspace layout
 static size_t align_up(size_t v) { return (v + 255) & ~(size_t)255; }
+
+// ptyro_ms_params.tune bit of the wave-resident kernel (ms_resident.cuh)
+constexpr int kTuneResident = 32768;
 
 static bool is_pow2(int n) { return n > 0 && (n & (n - 1)) == 0; }
 
@@ -639,12 +643,35 @@ static int forward_impl(const ptyro_ms_params* p, int ckpt_every, const float* p
   const int C = residuals ? (S + ckpt_every - 1) / ckpt_every : 0;
   const size_t res_stride = (size_t)(C + 1) * nn;
   const FwdBuffers B = fwd_buffers(L, ws);
+  // tune bit 32768: the wave-resident kernel (one CTA per probe, wave in shared memory
+  // across all slices) where it applies: N <= 128, one mode, no field windows, no
+  // residuals, detectors, tilts or amplitude output
+  const bool resident = (p->tune & kTuneResident) && resident_smem_bytes(n) > 0 && M == 1 && !residuals &&
+                        !has_det && !ex && !p->windows && field_of(p) == n;
   for (int b0 = 0; b0 < p->num_probes; b0 += L.batch) {
     const int nb = p->num_probes - b0 < L.batch ? p->num_probes - b0 : L.batch;
     float2* res_base = residuals ? residuals + (size_t)b0 * M * res_stride : nullptr;
     k_ramps<<<(nb * n + 255) / 256, 256, 0, st>>>(positions + 2 * (size_t)b0, nb, n, p->shift_calib_ang,
                                                   (float2*)B.ramp_y, (float2*)B.ramp_x);
     if ((rc = check_launch("k_ramps"))) return rc;
+    if (resident) {
+      ResidentArgs ra = {};
+      ra.probe_k = B.probe_k;
+      ra.ramp_y = B.ramp_y;
+      ra.ramp_x = B.ramp_x;
+      ra.trans = B.trans;
+      ra.trans_t = B.trans_t;
+      ra.pf = B.pf;
+      ra.tw = B.tw;
+      ra.weights = weights;
+      ra.pattern = patterns + (size_t)b0 * nn;
+      ra.num_slices = S;
+      ra.accumulate = (p->flags & PTYRO_FLAG_ACCUMULATE) != 0;
+      ra.scale = 1.0f / (float)n;
+      const int e = launch_resident(n, ra, nb, st);
+      if (e != 0) return fail(PTYRO_ERR_CUDA, std::string("ms_resident_kernel: ") + cudaGetErrorString((cudaError_t)e));
+      continue;
+    }
     for (int k = 0; k <= S + 1; ++k) {
       const FwdPlan f = fwd_pass_plan(p, B, weights, patterns, res_base, ckpt_every, C, b0, nb, k,
                                       has_det ? &det : nullptr, ex);

@@ -128,9 +128,10 @@ def check_windows(slices: torch.Tensor, modes: torch.Tensor, windows: Optional[t
 # 64 eight warps per CTA, 128 direct column access, 256 half-paired lines of N2 = 2 N1,
 # 2048 column blocks moved by TMA at 256^2 and 512^2, 4096 first and last slice
 # passes paired at 256^2, 16384 interleaved transmission tables: line pairs at 256^2,
-# line halves at 512^2);
+# line halves at 512^2, 32768 the wave-resident kernel at 128^2 for the forwards it
+# applies to);
 # the autotuner refines it.
-DEFAULT_TUNE = {16: 147, 32: 147, 64: 147, 128: 147, 256: 22739, 512: 18691, 1024: 0}
+DEFAULT_TUNE = {16: 147, 32: 147, 64: 147, 128: 32915, 256: 22739, 512: 18691, 1024: 0}
 
 
 def default_tune(n: int) -> int:

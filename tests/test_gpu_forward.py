@@ -16,6 +16,7 @@ import torch
 import ptyrodactyl_b200 as pb
 from oracle import multislice_ref as R
 from ptyrodactyl_b200 import synth
+from ptyrodactyl_b200.simulations import default_tune
 from tests.conftest import rel_l2
 
 pytestmark = pytest.mark.gpu
@@ -292,3 +293,49 @@ def test_stem_4d_streams_patterns_to_host():
     assert s4.data is host and torch.equal(host, ref)
     dev_out = torch.empty((p, n, n), dtype=torch.float32, device="cuda")
     assert torch.equal(pb.stem_4d(pots, beam, mic, det, out=dev_out).data.cpu(), ref)
+
+
+@pytest.mark.parametrize("n,num_slices", [(16, 1), (32, 3), (64, 2), (64, 7), (128, 1), (128, 20)])
+def test_resident_kernel_is_bit_identical_to_the_pass_engine(n, num_slices):
+    """The wave-resident kernel (tune bit 32768: one CTA per probe, the wave in shared
+    memory across all slices) runs the pass engine's operations in the same order, so
+    the patterns match the default variant bit for bit; the oracle checks both."""
+    rng = np.random.default_rng(n + num_slices)
+    pot = rng.uniform(0, 60, (n, n, num_slices))
+    probe = R.make_probe(300.0, 20.0, (n, n), 24.4, defocus_ang=20.0)
+    pos = rng.uniform(-3, 3, (37, 2))
+    dev = torch.device("cuda")
+    args = (torch.as_tensor(pot, dtype=torch.float32, device=dev), synth.SLICE_DZ,
+            torch.as_tensor(probe[..., None].astype(np.complex64), device=dev), torch.ones(1, device=dev),
+            torch.as_tensor(pos, device=dev), 300.0, 0.244, 0.244)
+    engine = pb.run_forward(*args, tune=default_tune(n) & ~32768).cpu().numpy()
+    resident = pb.run_forward(*args, tune=default_tune(n) | 32768).cpu().numpy()
+    assert np.array_equal(resident, engine)
+    # several batches, and accumulation into the output (frozen-phonon averaging)
+    small = pb.run_forward(*args, tune=default_tune(n) | 32768, batch=5).cpu().numpy()
+    assert np.array_equal(small, engine)
+    acc = torch.as_tensor(engine, device=dev).clone()
+    pb.run_forward(*args, tune=32768, out=acc, accumulate=True)
+    assert np.array_equal(acc.cpu().numpy(), engine + engine)
+    want = R.stem_4d(pot, synth.SLICE_DZ, 0.244, probe[..., None], [1.0], 0.244, 300.0, pos, 0.244,
+                     dtype=np.complex128)["data"]
+    assert rel_l2(resident, want) < TOL_F64
+
+
+def test_resident_kernel_at_the_128_workload_full_depth():
+    """The 128^2 perovskite workload (20 slices, 300 kV, 20 mrad) through the resident
+    kernel: bit-identical to the pass engine and within the float32 tolerance of the
+    float32 restatement."""
+    w = synth.CONFIG1
+    pot, probe, pos = _workload_case(w, 6)
+    dev = torch.device("cuda")
+    args = (torch.as_tensor(pot, dtype=torch.float32, device=dev), synth.SLICE_DZ,
+            torch.as_tensor(probe[..., None].astype(np.complex64), device=dev), torch.ones(1, device=dev),
+            torch.as_tensor(pos, device=dev), w.voltage_kv, w.calib, w.calib)
+    engine = pb.run_forward(*args, tune=default_tune(w.n) & ~32768).cpu().numpy()
+    resident = pb.run_forward(*args, tune=default_tune(w.n) | 32768).cpu().numpy()
+    assert default_tune(w.n) & 32768  # the 128^2 default runs the resident kernel
+    assert np.array_equal(resident, engine)
+    want32 = R.stem_4d(pot, synth.SLICE_DZ, w.calib, probe[..., None], [1.0], w.calib, w.voltage_kv, pos, w.calib,
+                       dtype=np.complex64)["data"]
+    assert rel_l2(resident, want32) < TOL_F32
