@@ -33,12 +33,20 @@ from .simulations import (
     relativistic_wavelength_ang,
 )
 
-DEFAULT_CKPT = 0  # 0: ceil(sqrt(S))
+DEFAULT_CKPT = 0  # 0: every slice when the residuals fit RESIDUAL_BUDGET_BYTES, else ceil(sqrt(S))
+# The default forward keeps the wave at every slice when that costs at most this many
+# bytes: the adjoint then carries only lambda (half the transform work of the lockstep
+# adjoint, which rebuilds the forward wave between sparser checkpoints).
+RESIDUAL_BUDGET_BYTES = 16 << 30
 
 
-def _ckpt_for(num_slices: int, ckpt_every: int) -> int:
+def _ckpt_for(num_slices: int, ckpt_every: int, n: int = 0, planes: int = 0) -> int:
+    """Checkpoint spacing: ``ckpt_every`` if given, else 1 when the S + 1 residual planes
+    of all ``planes`` (probe, mode) slots of an n x n grid fit the budget, else ceil(sqrt(S))."""
     if ckpt_every and ckpt_every > 0:
         return int(ckpt_every)
+    if n and planes and (num_slices + 1) * planes * 8 * n * n <= RESIDUAL_BUDGET_BYTES:
+        return 1
     return max(1, int(math.ceil(math.sqrt(num_slices))))
 
 
@@ -69,7 +77,7 @@ class Stem4dFunction(torch.autograd.Function):
         dev = slices.device
         S, M, P = slices.shape[2], modes.shape[2], positions.shape[0]
         n, f = check_windows(slices, modes, windows, P)
-        k = _ckpt_for(S, ckpt_every)
+        k = _ckpt_for(S, ckpt_every, n, P * M)
         prm = ms_params(n, S, M, P, voltage_kv, slice_thickness, calib_ang, shift_calib_ang, slices.stride(),
                         modes.stride(), batch, tune, f, windows)
         out = torch.empty((P, n, n), dtype=torch.float32, device=dev)
@@ -105,7 +113,8 @@ class Stem4dFunction(torch.autograd.Function):
         ctx.save_for_backward(slices, modes, weights, positions, res, windows)
         ctx.save_for_forward(slices, modes, weights, positions, windows)
         n = modes.shape[0]
-        ctx.cfg = (slice_thickness, voltage_kv, calib_ang, shift_calib_ang, _ckpt_for(slices.shape[2], ckpt_every),
+        ctx.cfg = (slice_thickness, voltage_kv, calib_ang, shift_calib_ang,
+                   _ckpt_for(slices.shape[2], ckpt_every, n, positions.shape[0] * modes.shape[2]),
                    batch, tune, n, slices.shape[0], record)
 
     @staticmethod
@@ -229,7 +238,7 @@ def vjp(slices, modes, weights, positions, grad_patterns, slice_thickness, volta
     dev = slices.device
     S, M, P = slices.shape[2], modes.shape[2], positions.shape[0]
     n, f = check_windows(slices, modes, windows, P)
-    k = _ckpt_for(S, ckpt_every)
+    k = _ckpt_for(S, ckpt_every, n, P * M)
     sc = float(calib_ang if shift_calib_ang is None else shift_calib_ang)
     prm = ms_params(n, S, M, P, voltage_kv, slice_thickness, calib_ang, sc, slices.stride(), modes.stride(), batch,
                     default_tune(n) if tune is None else int(tune), f, windows)

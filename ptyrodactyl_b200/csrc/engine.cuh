@@ -299,6 +299,9 @@ static size_t align_up(size_t v) { return (v + 255) & ~(size_t)255; }
 
 // ptyro_ms_params.tune bit of the wave-resident kernel (ms_resident.cuh)
 constexpr int kTuneResident = 32768;
+// tune bit: keep the lockstep adjoint (psi and lambda together) even when every slice
+// point has a checkpoint, instead of the lambda-only pass (ms_bwd_lam.cuh)
+constexpr int kTuneLockstepAdjoint = 65536;
 
 static bool is_pow2(int n) { return n > 0 && (n & (n - 1)) == 0; }
 
@@ -983,6 +986,8 @@ static BwdPlan bwd_pass_plan(const ptyro_ms_params* p, const BwdBuffers& B, cons
     a.op1 = OP_FFT; a.t_slice = -1; a.op2 = OP_NONE; a.psi_done = 1; a.beam_epi = 1;
     r.axis = (S + 1) % 2;
   }
+  // a checkpoint at every slice point: the lambda-only pass (tune bit 65536 keeps the lockstep one)
+  a.lam_only = ckpt_every == 1 && n <= 256 && !(p->tune & kTuneLockstepAdjoint);
   return r;
 }
 

@@ -43,6 +43,7 @@ struct BwdArgs {
   float sigma2;            // 2 sigma
   float scale;             // 1/N after OP_IFFT
   unsigned int* status;    // the call's device status word (PTYRO_STATUS_* bits), or null
+  int lam_only;            // every slice point has a checkpoint: carry lambda only (ms_bwd_lam.cuh)
 };
 
 // Shared memory of an adjoint pass: twiddles + max(paired exchange buffers, tile).

@@ -1,0 +1,160 @@
+// Adjoint pass that carries only the adjoint wave, for gradients whose forward kept
+// the wave at every slice (checkpoint spacing 1), grids up to 256^2.
+//
+// The lockstep adjoint (ms_bwd.cuh) pairs the forward wave psi and the adjoint lambda
+// of one line and runs psi backward through U^H conj(T) alongside lambda, replacing
+// it by the stored wave wherever a checkpoint exists. With a checkpoint at every
+// slice point psi is never needed between slice points: lambda's recursion does not
+// involve psi, and the dV contribution 2 sigma Im(conj(phi_s) lambda_s) takes phi_s
+// straight from the stored residual. This pass therefore pairs the adjoints of two
+// neighbouring lines (like the forward's paired pass), which halves the transform work
+// of every adjoint pass; each paired operation rounds as the lockstep kernel's lambda
+// half does, so the gradients are bit-identical to the lockstep adjoint at spacing 1.
+// Row passes read and write lines directly; column passes read and write the two
+// neighbouring columns of a lane pair as 16-byte pieces.
+#pragma once
+#include "ms_bwd.cuh"
+#include "ms_pair.cuh"
+
+namespace ptyro {
+
+// a * conj(w) with a different w per line: the operations of cmulc(Pair, w) per lane
+__device__ __forceinline__ Pair cmulc(Pair a, float2 wa, float2 wb) {
+  const float2 wx = make_float2(wa.x, wb.x), wy = make_float2(wa.y, wb.y);
+  return {__ffma2_rn(a.re, wx, __fmul2_rn(a.im, wy)), __ffma2_rn(a.im, wx, __fmul2_rn(a.re, make_float2(-wa.y, -wb.y)))};
+}
+
+template <int N1, int N2, int AXIS, int WARPS>
+__device__ __forceinline__ void bwd_lam_body(const BwdArgs& a, const int slot) {
+  using PG = PairGeom<N1, N2, WARPS>;
+  using PB = PairBuf<N1, N2>;
+  constexpr int N = PG::N, G = PG::G, lines = PG::kLines;
+  extern __shared__ float4 smem4[];
+  float2* tw = reinterpret_cast<float2*>(smem4);  // tw[k2 * N1 + t] = W_N^{t k2}
+  float2* pfs = tw + N;                           // propagator factor / N
+  Pair* xbuf = reinterpret_cast<Pair*>(pfs + N);
+  for (int i = threadIdx.x; i < N; i += blockDim.x) {
+    const int k2 = i / N1, tt = i % N1;
+    tw[i] = a.tw[(tt * k2) % N];
+    pfs[i] = a.pf[i];
+  }
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int t = AXIS == 0 ? (lane % N1) : (lane / G);
+  const int gl = AXIS == 0 ? (lane / N1) : (lane % G);
+  const int lp = warp * G + gl;
+  const int la = blockIdx.x * lines + 2 * lp, lb = la + 1;
+  Pair* buf = xbuf + lp * PB::kSize;
+  const size_t NN = (size_t)N * N;
+  const int b = slot / a.n_modes, m = slot % a.n_modes;
+  float2* Wl = a.lam + (size_t)slot * NN;
+  const bool korder_in = a.init || a.op1 == OP_IFFT;
+  Pair v[N2];
+
+  // ---- load lambda of both lines
+  if (a.init) {  // lam = N^2 w_m g(shifted) A in k-space
+    const float2* A = a.amp + (size_t)slot * a.res_stride;
+    const float* g = a.gpat + (size_t)b * NN;
+    const float s = (float)N * (float)N * a.weights[m];
+    const int ksa = (la + N / 2) % N, ksb = (lb + N / 2) % N;
+#pragma unroll
+    for (int r = 0; r < N2; ++r) {
+      const int k = korder_index<N1, N2>(t, r), kq = (k + N / 2) % N;
+      const float2 aa = A[AXIS == 0 ? (size_t)la * N + k : (size_t)k * N + la];
+      const float2 ab = A[AXIS == 0 ? (size_t)lb * N + k : (size_t)k * N + lb];
+      const float ga = AXIS == 0 ? g[(size_t)ksa * N + kq] : g[(size_t)kq * N + ksa];
+      const float gb = AXIS == 0 ? g[(size_t)ksb * N + kq] : g[(size_t)kq * N + ksb];
+      v[r] = make_pair(cscale(aa, s * ga), cscale(ab, s * gb));
+    }
+  } else {
+#pragma unroll
+    for (int r = 0; r < N2; ++r) {
+      const int e = korder_in ? korder_index<N1, N2>(t, r) : t + N1 * r;
+      if (AXIS == 0) {
+        v[r] = make_pair(Wl[(size_t)la * N + e], Wl[(size_t)lb * N + e]);
+      } else {
+        const float4 q = *reinterpret_cast<const float4*>(Wl + (size_t)e * N + la);
+        v[r] = {make_float2(q.x, q.z), make_float2(q.y, q.w)};
+      }
+    }
+  }
+
+  // ---- op1
+  if (a.op1 == OP_IFFT) {
+    line_k_to_nat<N1, N2, +1>(v, t, buf, tw);
+#pragma unroll
+    for (int j = 0; j < N2; ++j) v[j] = cscale(v[j], a.scale);
+  } else if (a.op1 == OP_CONV_CONJ || a.op1 == OP_FFT) {
+    apply_op<N1, N2>(a.op1, v, t, buf, tw, pfs);
+  }
+
+  // ---- slice point: dV contribution from the stored wave phi_s (stored at once, so
+  // it holds no registers through the second transform), then conj(T_s)
+  if (a.t_slice >= 0) {
+    const float2* ck = a.ckpt + (size_t)slot * a.res_stride;
+    float* C = a.contrib ? a.contrib + (size_t)slot * NN : nullptr;
+#pragma unroll
+    for (int j = 0; j < N2; ++j) {
+      const int e = t + N1 * j;
+      float2 pa, pb;
+      if (AXIS == 0) {
+        pa = ck[(size_t)la * N + e];
+        pb = ck[(size_t)lb * N + e];
+      } else {
+        const float4 q = *reinterpret_cast<const float4*>(ck + (size_t)e * N + la);
+        pa = make_float2(q.x, q.y);
+        pb = make_float2(q.z, q.w);
+      }
+      const float cva = a.sigma2 * (pa.x * v[j].im.x - pa.y * v[j].re.x);
+      const float cvb = a.sigma2 * (pb.x * v[j].im.y - pb.y * v[j].re.y);
+      if (C) {
+        if (AXIS == 0) {
+          C[(size_t)la * N + e] = cva;
+          C[(size_t)lb * N + e] = cvb;
+        } else {
+          *reinterpret_cast<float2*>(C + (size_t)e * N + la) = make_float2(cva, cvb);
+        }
+      }
+    }
+    int oa, ob;
+    const float2* Ta = trans_row<AXIS>(a.trans, a.trans_t, a.field_n, a.t_slice, a.win, b, la, &oa);
+    const float2* Tb = trans_row<AXIS>(a.trans, a.trans_t, a.field_n, a.t_slice, a.win, b, lb, &ob);
+    const int fm = a.field_n - 1;
+#pragma unroll
+    for (int j = 0; j < N2; ++j)
+      v[j] = cmulc(v[j], __ldg(Ta + ((t + N1 * j + oa) & fm)), __ldg(Tb + ((t + N1 * j + ob) & fm)));
+  }
+
+  // ---- op2, and the beam-gradient epilogue (lambda k-order along this axis times conj(ramp))
+  bool lam_k = a.op1 == OP_FFT;
+  if (a.op2 == OP_CONV_CONJ) {
+    apply_op<N1, N2>(OP_CONV_CONJ, v, t, buf, tw, pfs);
+  } else if (a.op2 == OP_FFT) {
+    apply_op<N1, N2>(OP_FFT, v, t, buf, tw, pfs);
+    lam_k = true;
+  }
+  if (a.beam_epi) {
+    const float2* ra = (AXIS == 0 ? a.ramp_x : a.ramp_y) + (size_t)b * N;
+#pragma unroll
+    for (int r = 0; r < N2; ++r) v[r] = cmulc(v[r], ra[korder_index<N1, N2>(t, r)]);
+  }
+
+  // ---- store lambda
+#pragma unroll
+  for (int r = 0; r < N2; ++r) {
+    const int e = lam_k ? korder_index<N1, N2>(t, r) : t + N1 * r;
+    if (AXIS == 0) {
+      Wl[(size_t)la * N + e] = pair_a(v[r]);
+      Wl[(size_t)lb * N + e] = pair_b(v[r]);
+    } else {
+      *reinterpret_cast<float4*>(Wl + (size_t)e * N + la) = make_float4(v[r].re.x, v[r].im.x, v[r].re.y, v[r].im.y);
+    }
+  }
+}
+
+template <int N1, int N2, int AXIS, int WARPS, int MINB>
+__global__ void __launch_bounds__(WARPS * 32, MINB) ms_bwd_lam_kernel(BwdArgs a) {
+  bwd_lam_body<N1, N2, AXIS, WARPS>(a, blockIdx.y);
+}
+
+}  // namespace ptyro

@@ -8,6 +8,7 @@
 #include <mutex>
 
 #include "ms_bwd.cuh"
+#include "ms_bwd_lam.cuh"
 #include "ms_jvp.cuh"
 #include "ms_half.cuh"
 #include "ms_pair.cuh"
@@ -124,9 +125,29 @@ int launch_bwd_w(const BwdArgs& a, int grid_y, cudaStream_t st, const CUtensorMa
   return (int)cudaGetLastError();
 }
 
+// The lambda-only adjoint pass (ms_bwd_lam.cuh): two lines per thread, direct access.
+template <int N1, int N2, int AXIS>
+int launch_bwd_lam_t(const BwdArgs& a, int grid_y, cudaStream_t st) {
+  constexpr int N = N1 * N2, G = 32 / N1;
+  constexpr int W = N / (2 * G) < 8 ? N / (2 * G) : 8;  // line pairs per CTA tile the grid
+  using PG = PairGeom<N1, N2, W>;
+  const size_t smem = sizeof(float2) * 2 * (size_t)N + PG::kXbuf;
+  static DeviceOnce attr_done;  // per device: the attribute is per-device state
+  if (attr_done.first())
+    cudaFuncSetAttribute(ms_bwd_lam_kernel<N1, N2, AXIS, W, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)smem);
+  dim3 grid(N / PG::kLines, grid_y);
+  ms_bwd_lam_kernel<N1, N2, AXIS, W, 2><<<grid, W * 32, smem, st>>>(a);
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  return (int)cudaGetLastError();
+}
+
 // variant bit 11 (2048): 256^2 adjoint column passes move their column blocks by TMA
 template <int N1, int N2, int AXIS>
 int launch_bwd_t(const BwdArgs& a, int grid_y, cudaStream_t st, int variant) {
+  if constexpr (N2 <= 16) {  // two lines of lambda fit in a thread's registers
+    if (a.lam_only) return launch_bwd_lam_t<N1, N2, AXIS>(a, grid_y, st);
+  }
   if constexpr (AXIS == 1 && N1 * N2 == 256) {
     CUtensorMap pmap, lmap;
     if ((variant & 2048) && !a.init && wave_tensor_map(a.psi, N1 * N2, grid_y, 32 / N1, &pmap) &&

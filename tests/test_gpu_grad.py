@@ -198,3 +198,42 @@ def test_position_gradient_matches_oracle(n, s, m, p):
     (pat * torch.as_tensor(g, dtype=torch.float32, device=dev)).sum().backward()
     _, _, dpos = R.stem_4d_vjp(pot, 1.7, 0.3, modes, w, 0.3, 200.0, pos, 0.3, g, with_positions=True)
     assert rel_l2(ps.grad.cpu().numpy(), dpos) < TOL, rel_l2(ps.grad.cpu().numpy(), dpos)
+
+
+@pytest.mark.parametrize("n,s,m,p", [(16, 3, 1, 3), (32, 1, 1, 2), (64, 5, 2, 3), (128, 4, 1, 5), (256, 6, 1, 3)])
+def test_lambda_only_adjoint_is_bit_identical_to_lockstep(n, s, m, p):
+    """With a checkpoint at every slice point the adjoint pass carries only lambda,
+    two lines per thread (ms_bwd_lam.cuh); the lockstep adjoint (tune bit 65536) runs
+    psi alongside and replaces it by the checkpoint at every slice point, so both give
+    the same gradients bit for bit, and both match the oracle."""
+    pot, modes, w, pos, g = _case(n, s, m, p, seed=n + s)
+    dev = torch.device("cuda")
+    args = [torch.as_tensor(pot, dtype=torch.float32, device=dev), torch.as_tensor(modes.astype(np.complex64), device=dev),
+            torch.as_tensor(w, dtype=torch.float32, device=dev), torch.as_tensor(pos, dtype=torch.float64, device=dev),
+            torch.as_tensor(g, dtype=torch.float32, device=dev), 1.7, 200.0, 0.3]
+    base = pb.simulations.default_tune(n)
+    lam = pb.vjp(*args, ckpt_every=1, tune=base, batch=2)
+    lock = pb.vjp(*args, ckpt_every=1, tune=base | 65536, batch=2)
+    for a, b in zip(lam, lock):
+        assert torch.equal(a, b)
+    dv_ref, dm_ref = R.stem_4d_vjp(pot, 1.7, 0.3, modes, w, 0.3, 200.0, pos, 0.3, g)
+    assert rel_l2(lam[1].cpu().numpy(), dv_ref) < TOL
+    assert rel_l2(lam[2].cpu().numpy(), dm_ref) < TOL
+
+
+def test_lambda_only_adjoint_windowed_field():
+    """The lambda-only adjoint on 64^2 windows of a periodic 128^2 field (one window
+    wraps) equals the lockstep adjoint bit for bit."""
+    rng = np.random.default_rng(17)
+    n, f, s = 64, 128, 4
+    dev = torch.device("cuda")
+    field = torch.as_tensor(rng.uniform(0.0, 50.0, (f, f, s)), dtype=torch.float32, device=dev)
+    probe = R.make_probe(200.0, 25.0, (n, n), 30.0, defocus_ang=-20.0)
+    windows = torch.as_tensor(np.array([[0, 0], [8, 40], [64, 64], [100, 90], [120, 3]], np.int32), device=dev)
+    args = [field, torch.as_tensor(probe[..., None].astype(np.complex64), device=dev), torch.ones(1, device=dev),
+            torch.as_tensor(rng.uniform(-1, 1, (5, 2)), device=dev),
+            torch.as_tensor(rng.normal(size=(5, n, n)), dtype=torch.float32, device=dev), 1.7, 200.0, 0.3]
+    lam = pb.vjp(*args, ckpt_every=1, windows=windows, batch=3)
+    lock = pb.vjp(*args, ckpt_every=1, windows=windows, batch=3, tune=pb.simulations.default_tune(n) | 65536)
+    for a, b in zip(lam, lock):
+        assert torch.equal(a, b)
