@@ -14,12 +14,20 @@ third-party dependency absent here (pinned ``jax==0.9.2`` in the reference's
   ("partitionable", the default since JAX 0.5, and the original
   split-in-halves layout);
 * ``uniform``'s mantissa-fill rule: keep the top ``nmant`` random bits, OR in the
-  exponent of 1.0, reinterpret, subtract 1.
+  exponent of 1.0, reinterpret, subtract 1;
+* ``split`` in the partitionable ("fold-like") layout: key i is the Threefry block of
+  the counter (0, i) under the parent key;
+* ``normal``: ``sqrt(2) * erf_inv(u)`` with ``u`` uniform on
+  [nextafter(-1, 0), 1). XLA evaluates ``erf_inv`` with its own polynomial; here the
+  inverse error function is computed to full double precision by Halley's method
+  (so the draws agree with JAX's to a few units in the last place).
 
 Only ``tests/golden/make_golden.py`` and the tests use this module.
 """
 
 from __future__ import annotations
+
+import math
 
 import numpy as np
 
@@ -96,3 +104,53 @@ def uniform_f64(key: tuple[int, int], shape, minval: float = 0.0, maxval: float 
     fbits = (bits >> np.uint64(64 - 52)) | one_bits
     floats = fbits.view(np.float64) - 1.0
     return np.maximum(minval, floats * (maxval - minval) + minval)
+
+
+def split(key: tuple[int, int], num: int = 2) -> list[tuple[int, int]]:
+    """``jax.random.split(key, num)`` (partitionable layout): key i = Threefry-2x32 of
+    the 64-bit counter i, as (high, low) words, under ``key``."""
+    idx = np.arange(int(num), dtype=np.uint64)
+    b1, b2 = threefry2x32(key, (idx >> np.uint64(32)).astype(np.uint32),
+                          (idx & np.uint64(0xFFFFFFFF)).astype(np.uint32))
+    return [(int(a), int(b)) for a, b in zip(b1, b2)]
+
+
+def erfinv(y: float) -> float:
+    """Inverse error function in double precision.
+
+    Starting value: Winitzki's closed-form approximation (S. Winitzki, "A handy
+    approximation for the error function and its inverse", 2008; a = 0.147, relative
+    error ~2e-3). Refinement: Halley's method on f(x) = erf(x) - y, with
+    f' = 2/sqrt(pi) exp(-x^2) and f'' = -2 x f', written through erfc in the tails so
+    that 1 - |y| keeps its precision; three steps reach rounding level.
+    """
+    y = float(y)
+    if y <= -1.0:
+        return -math.inf
+    if y >= 1.0:
+        return math.inf
+    if y == 0.0:
+        return 0.0
+    a = 0.147
+    ln = math.log1p(-y * y)
+    t = 2.0 / (math.pi * a) + 0.5 * ln
+    x = math.copysign(math.sqrt(math.sqrt(t * t - ln / a) - t), y)
+    ay = abs(y)
+    for _ in range(4):
+        if ay > 0.5:  # f = sign(y) (1 - |y| - erfc(|x|)) without cancellation
+            f = ((1.0 - ay) - math.erfc(abs(x))) * (1.0 if y > 0 else -1.0)
+        else:
+            f = math.erf(x) - y
+        d = 2.0 / math.sqrt(math.pi) * math.exp(-x * x)
+        if d == 0.0:
+            break
+        step = f / d
+        x = x - step / (1.0 + x * step)  # Halley: f'' / f' = -2 x
+    return x
+
+
+def normal_f64(key: tuple[int, int], shape) -> np.ndarray:
+    """``jax.random.normal(key, shape, dtype=float64)``."""
+    lo = np.nextafter(np.float64(-1.0), np.float64(0.0))
+    u = uniform_f64(key, shape, minval=float(lo), maxval=1.0)
+    return np.sqrt(np.float64(2.0)) * np.vectorize(erfinv, otypes=[np.float64])(u)

@@ -603,3 +603,81 @@ def single_slice_poscorrected(data, positions, voltage_kv, calib_ang, pot0, beam
         step, s_pos = _adam_step(dpos, s_pos, lr_pos)
         pos = pos + step
     return pot, beam, pos, losses
+
+
+def _optax_adam(g, state, lr, b1=0.9, b2=0.999, eps=1e-8):
+    """optax 0.2.3 ``adam`` (``scale_by_adam`` then ``scale_by_learning_rate``), in its
+    operation order: mu = (1 - b1) g + b1 mu; nu = (1 - b2) |g|^2 + b2 nu; bias
+    corrections 1 - b^count; update = -lr * mu_hat / (sqrt(nu_hat) + eps)."""
+    sq = np.real(np.conj(g) * g) if np.iscomplexobj(g) else g ** 2
+    mu = (1 - b1) * g + b1 * state["mu"]
+    nu = (1 - b2) * sq + b2 * state["nu"]
+    count = state["count"] + 1
+    mu_hat = mu / (1 - b1 ** count)
+    nu_hat = nu / (1 - b2 ** count)
+    return -lr * (mu_hat / (np.sqrt(nu_hat) + eps)), {"mu": mu, "nu": nu, "count": count}
+
+
+def _loss_grad(model, data, loss):
+    """``_reduce_loss`` (multislice/multislice_recon.py:127-147) and its derivative."""
+    diff = model - data
+    if loss == "mae":
+        return float(np.mean(np.abs(diff))), np.sign(diff) / diff.size
+    mse = float(np.mean(diff ** 2))
+    if loss == "mse":
+        return mse, 2.0 * diff / diff.size
+    rmse = np.sqrt(mse)
+    return float(rmse), diff / (diff.size * rmse)
+
+
+def recon_loop(data, positions, voltage_kv, calib_ang, pot0, modes0, weights, slice_thickness, num_iterations,
+               lr, lr_pos=None, save_every=1, loss="mse"):
+    """The reference's reconstruction loops in float64 with optax's Adam
+    (multislice/multislice_recon.py): ``single_slice_ptychography`` (:243-668,
+    ``lr_pos`` None: positions fixed), ``single_slice_poscorrected`` (:671-1221),
+    ``single_slice_multi_modal`` (:1224-1737; several modes with fixed weights) and
+    ``multi_slice_multi_modal`` (:1740-2227) all follow it.
+
+    Each iteration: patterns = stem_4d(real(pot) as one slice, modes, weights,
+    positions) (:392-420), the loss of ``_reduce_loss``, JAX's gradients (the VJP of
+    ``stem_4d``: dL/dV real, the modes' and positions' gradients), then one optimizer
+    step per parameter. Potential and modes step with conj of JAX's gradient
+    (``_apply_optimizer_step`` :166-207), positions with their real gradient and
+    ``optax.apply_updates``. Snapshots: after the first update at index 0, then after
+    iteration ii at index ii // save_every when ii % save_every == 0 (:590-636),
+    out-of-range indices dropped. Returns a dict of the final values, snapshots
+    (trailing axis) and losses."""
+    pot = np.asarray(pot0).astype(np.complex128)
+    modes = np.atleast_3d(np.asarray(modes0)).astype(np.complex128)
+    w = np.asarray(weights, np.float64)
+    pos = np.asarray(positions, np.float64).copy()
+    refine = lr_pos is not None
+    zero = lambda x: {"mu": np.zeros_like(x), "nu": np.zeros(x.shape), "count": 0}
+    s_pot, s_modes, s_pos = zero(pot), zero(modes), zero(pos)
+    count = num_iterations // save_every
+    snap = {"pot": np.zeros(pot.shape + (count,), np.complex128),
+            "modes": np.zeros(modes.shape + (count,), np.complex128),
+            "pos": np.zeros(pos.shape + (count,), np.float64)}
+    losses = []
+    for ii in range(num_iterations):
+        slices = np.real(pot)[..., None]
+        model = stem_4d(slices, slice_thickness, calib_ang, modes, w, calib_ang, voltage_kv, pos,
+                        calib_ang)["data"]
+        value, g = _loss_grad(model, np.asarray(data, np.float64), loss)
+        losses.append(value)
+        out = stem_4d_vjp(slices, slice_thickness, calib_ang, modes, w, calib_ang, voltage_kv, pos, calib_ang, g,
+                          with_positions=refine)
+        dv, dm = out[0], out[1]
+        step, s_pot = _optax_adam(dv[:, :, 0].astype(np.complex128), s_pot, lr)
+        pot = pot + step
+        step, s_modes = _optax_adam(np.conj(dm), s_modes, lr)
+        modes = modes + step
+        if refine:
+            step, s_pos = _optax_adam(out[2], s_pos, lr_pos)
+            pos = pos + step
+        if ii % save_every == 0 and ii // save_every < count:
+            snap["pot"][..., ii // save_every] = pot
+            snap["modes"][..., ii // save_every] = modes
+            snap["pos"][..., ii // save_every] = pos
+    return {"pot": pot, "modes": modes, "pos": pos, "snap_pot": snap["pot"], "snap_modes": snap["modes"],
+            "snap_pos": snap["pos"], "losses": losses}

@@ -91,3 +91,48 @@ def test_unknown_optimizer_and_loss():
         MR.multi_slice_multi_modal(s4, pot0, beam0, 2.0, num_iterations=1, optimizer_name="sgd")
     with pytest.raises(ValueError):
         MR.multi_slice_multi_modal(s4, pot0, beam0, 2.0, num_iterations=1, loss_type="huber")
+
+
+@pytest.mark.parametrize("fn", ["single_slice_ptychography", "single_slice_poscorrected", "single_slice_multi_modal",
+                                "multi_slice_multi_modal"])
+def test_engine_loops_match_the_pinned_oracle_loop(fn):
+    """The setting of the reference's pinned regressions (PRNGKey(11) draws, two
+    positions, 80 kV, unit calibration, two Adam steps at lr 0.001; the oracle's loop
+    reproduces those pins on the reference's 4 x 4 grid, tests/test_oracle_recon_pins.py)
+    on the engine's smallest grid, 16 x 16, against the same float64 oracle loop.
+    Adam's first steps are lr * sign(g) up to 1e-8, so float32 gradients give the same
+    iterates to float32 rounding unless a gradient sits at noise level."""
+    from oracle.jax_prng import normal_f64, prng_key, split
+    n = 16
+    keys = split(prng_key(11), 5)
+    pot = (normal_f64(keys[0], (n, n)) * 0.01).astype(np.complex128)
+    beam = normal_f64(keys[1], (n, n)) + 1j * normal_f64(keys[2], (n, n))
+    modes = np.stack([beam, beam * (0.5 + 0.1j)], axis=-1)
+    data = np.ones((2, n, n))
+    pos = np.array([[0.0, 0.0], [1.0, 0.0]])
+    s4 = pb.create_stem4d(torch.as_tensor(data, dtype=torch.float32, device="cuda"), 1.0, 1.0 / n, pos, 80.0)
+    pot_c = pb.create_calibrated_array(pot, 1.0, 1.0, True)
+    beam_c = pb.create_calibrated_array(beam, 1.0, 1.0, True)
+    if fn == "single_slice_ptychography":
+        out = MR.single_slice_ptychography(s4, pot_c, beam_c, 1.0, save_every=1, num_iterations=2,
+                                           learning_rate=0.001)
+        got = (out[0].data_array, out[1].data_array[..., None], None)
+        want = R.recon_loop(data, pos, 80.0, 1.0, pot, beam, [1.0], 1.0, 2, 0.001)
+    elif fn == "single_slice_poscorrected":
+        out = MR.single_slice_poscorrected(s4, pot_c, beam_c, 1.0, save_every=1, num_iterations=2,
+                                           learning_rate=0.001)
+        got = (out[0].data_array, out[1].data_array[..., None], out[2])
+        want = R.recon_loop(data, pos, 80.0, 1.0, pot, beam, [1.0], 1.0, 2, 0.001, lr_pos=0.001)
+    elif fn == "single_slice_multi_modal":
+        probe = pb.create_probe_modes(modes, [0.7, 0.3], 1.0)
+        out = MR.single_slice_multi_modal(s4, pot, probe, 1.0, save_every=1, num_iterations=2, learning_rate=0.001)
+        got = (out[0], out[1].modes, out[2])
+        want = R.recon_loop(data, pos, 80.0, 1.0, pot, modes, [0.7, 0.3], 1.0, 2, 0.001, lr_pos=0.001)
+    else:
+        out = MR.multi_slice_multi_modal(s4, pot, beam, 1.0, save_every=1, num_iterations=2, learning_rate=0.001)
+        got = (out[0], out[1][..., None], out[2])
+        want = R.recon_loop(data, pos, 80.0, 1.0, pot, beam, [1.0], 1.0, 2, 0.001, lr_pos=0.01)
+    assert rel_l2(got[0].cpu().numpy(), want["pot"]) < 1e-5
+    assert rel_l2(got[1].cpu().numpy(), want["modes"]) < 1e-5
+    if got[2] is not None:
+        assert np.allclose(got[2].cpu().numpy(), want["pos"], rtol=1e-5, atol=1e-9)
