@@ -101,7 +101,13 @@ def test_engine_loops_match_the_pinned_oracle_loop(fn):
     reproduces those pins on the reference's 4 x 4 grid, tests/test_oracle_recon_pins.py)
     on the engine's smallest grid, 16 x 16, against the same float64 oracle loop.
     Adam's first steps are lr * sign(g) up to 1e-8, so float32 gradients give the same
-    iterates to float32 rounding unless a gradient sits at noise level."""
+    iterates to float32 rounding unless a gradient sits at noise level. That is the
+    case for the scan positions here: the object is nearly transparent (|T - 1| ~ 1e-5),
+    so the patterns hardly depend on position and the position gradient is a small
+    difference of large terms (the oracle's own complex64 and complex128 values of it
+    differ by 4-8 %). The positions are therefore held to the first step's direction
+    and the second step to 5 % of a step; well-conditioned position gradients are
+    checked against the oracle at 1e-4 in test_gpu_grad.py."""
     from oracle.jax_prng import normal_f64, prng_key, split
     n = 16
     keys = split(prng_key(11), 5)
@@ -113,6 +119,7 @@ def test_engine_loops_match_the_pinned_oracle_loop(fn):
     s4 = pb.create_stem4d(torch.as_tensor(data, dtype=torch.float32, device="cuda"), 1.0, 1.0 / n, pos, 80.0)
     pot_c = pb.create_calibrated_array(pot, 1.0, 1.0, True)
     beam_c = pb.create_calibrated_array(beam, 1.0, 1.0, True)
+    lr_pos = 0.01 if fn == "multi_slice_multi_modal" else 0.001
     if fn == "single_slice_ptychography":
         out = MR.single_slice_ptychography(s4, pot_c, beam_c, 1.0, save_every=1, num_iterations=2,
                                            learning_rate=0.001)
@@ -135,4 +142,4 @@ def test_engine_loops_match_the_pinned_oracle_loop(fn):
     assert rel_l2(got[0].cpu().numpy(), want["pot"]) < 1e-5
     assert rel_l2(got[1].cpu().numpy(), want["modes"]) < 1e-5
     if got[2] is not None:
-        assert np.allclose(got[2].cpu().numpy(), want["pos"], rtol=1e-5, atol=1e-9)
+        assert np.abs(got[2].cpu().numpy() - want["pos"]).max() < 0.05 * lr_pos
