@@ -274,6 +274,22 @@ int ptyro_fp32_fma_probe(float* out, int32_t blocks, int32_t iters, void* stream
 int ptyro_test_wait_timeout(int32_t warps, int32_t polls, uint32_t* status, int32_t* skipped_warps,
                             void* stream);
 
+/* Projected potential of one atom, averaged from a supersampled grid: replaces
+ * single_atom_potential (src/ptyrodactyl/multislice/atom_potentials.py:588-681) with
+ * lobato_projected_potential / kirkland_projected_potential
+ * (src/ptyrodactyl/multislice/form_factors.py:322-439).
+ *   parameterization  0 = Lobato--Van Dyck, 1 = Kirkland
+ *   coeffs            HOST double: Lobato a1..a5, b1..b5 (10 values); Kirkland a1, b1,
+ *                     a2, b2, a3, b3 (Lorentzian), c1, d1, c2, d2, c3, d3 (Gaussian) (12)
+ *   pixel_size        Angstrom; the supersampled step is pixel_size / supersampling
+ *   h, w              output grid; supersampled point k of an axis of K = edge *
+ *                     supersampling points sits at (k - K/2) * step
+ *   center_x, center_y  the atom's position, Angstrom (0, 0: the supersampled grid's centre)
+ *   out               DEVICE float64 (h, w), volt-Angstrom: the mean of each pixel's
+ *                     supersampling^2 values */
+int ptyro_atom_potential(int32_t parameterization, const double* coeffs, double pixel_size, int32_t h, int32_t w,
+                         double center_x, double center_y, int32_t supersampling, double* out, void* stream);
+
 /* Workspace bytes of ptyro_atom_slices for edge n and num_types atom types. */
 size_t ptyro_atom_slices_workspace_bytes(int32_t n, int32_t num_types);
 

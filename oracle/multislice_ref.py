@@ -681,3 +681,83 @@ def recon_loop(data, positions, voltage_kv, calib_ang, pot0, modes0, weights, sl
             snap["pos"][..., ii // save_every] = pos
     return {"pot": pot, "modes": modes, "pos": pos, "snap_pot": snap["pot"], "snap_modes": snap["modes"],
             "snap_pos": snap["pos"], "losses": losses}
+
+
+# ---------------------------------------------------------------------------
+# Single-atom projected potentials (multislice/atom_potentials.py:95-681,
+# multislice/form_factors.py:322-439), float64.
+# ---------------------------------------------------------------------------
+
+def _bessel_k0_ref(x):
+    """The reference's K0 (atom_potentials.py:95-140, :377-408): Abramowitz & Stegun
+    9.8.5 for x <= 2 (with I0), 9.8.6 above."""
+    from scipy.special import i0
+    x = np.asarray(x, np.float64)
+    x2 = (x * x) / 4.0
+    c = np.array([-0.57721566, 0.42278420, 0.23069756, 0.03488590, 0.00262698, 0.00010750, 0.00000740])
+    small = -np.log(x / 2.0) * i0(x) + np.sum(c * np.power(x2[..., None], np.arange(7)), axis=-1)
+    y = 2.0 / x
+    poly = 1.25331414 + y * (-0.07832358 + y * (0.02189568 + y * (-0.01062446 + y * (
+        0.00587872 + y * (-0.00251540 + y * 0.00053208)))))
+    return np.where(x <= 2.0, small, np.exp(-x) / np.sqrt(x) * poly)
+
+
+def _bessel_k1_ref(x):
+    """The reference's K1 (atom_potentials.py:279-297, :409-421): A&S 9.8.7 for x <= 2
+    (with I1), 9.8.8 above."""
+    from scipy.special import i1
+    x = np.asarray(x, np.float64)
+    x2 = (x * x) / 4.0
+    d = np.array([1.0, 0.15443144, -0.67278579, -0.18156897, -0.01919402, -0.00110404, -0.00004686])
+    small = np.log(x / 2.0) * i1(x) + np.sum(d * np.power(x2[..., None], np.arange(7)), axis=-1) / x
+    y = 2.0 / x
+    poly = 1.25331414 + y * (0.23498619 + y * (-0.03655620 + y * (0.01504268 + y * (
+        -0.00780353 + y * (0.00325614 + y * -0.00068245)))))
+    return np.where(x <= 2.0, small, np.exp(-x) / np.sqrt(x) * poly)
+
+
+def element_coefficients(atom_no, parameterization):
+    """Row of the coefficient table the package ships (lobato: a1..a5, b1..b5;
+    kirkland: a1, b1, ..., c3, d3)."""
+    import os
+    data = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "ptyrodactyl_b200", "data")
+    if parameterization == "lobato":
+        tab = np.loadtxt(os.path.join(data, "lobato_van_dyck.csv"), delimiter=",", skiprows=1, usecols=range(2, 12))
+    else:
+        tab = np.loadtxt(os.path.join(data, "kirkland_potentials.csv"), delimiter=",")
+    return tab[int(atom_no) - 1]
+
+
+def projected_potential(coeffs, r, parameterization):
+    """lobato_projected_potential (form_factors.py:322-371, Lobato & Van Dyck Eq. 16,
+    C_MB = 47.87801) or kirkland_projected_potential (:374-439, a0 = 0.5292, e_k = 14.4)."""
+    r = np.maximum(np.asarray(r, np.float64), 1e-10)[..., None]
+    if parameterization == "lobato":
+        a, b = np.asarray(coeffs[:5]), np.asarray(coeffs[5:10])
+        arg = 2.0 * np.pi * r / np.sqrt(b)
+        terms = a / b * _bessel_k0_ref(arg) + a * np.pi * r / np.power(b, 1.5) * _bessel_k1_ref(arg)
+        return 2.0 * np.pi * 47.87801 * np.sum(terms, axis=-1)
+    c = np.asarray(coeffs)
+    la, lb, ga, gb = c[[0, 2, 4]], c[[1, 3, 5]], c[[6, 8, 10]], c[[7, 9, 11]]
+    lt = la * _bessel_k0_ref(2.0 * np.pi * r * np.sqrt(lb))
+    gt = ga / gb * np.exp(-(np.pi ** 2) * np.square(r) / gb)
+    lpre = 4.0 * np.pi ** 2 * 0.5292 * 14.4
+    gpre = 2.0 * np.pi ** 2 * 0.5292 * 14.4
+    return lpre * (lt[..., 0] + lt[..., 1] + lt[..., 2]) + gpre * (gt[..., 0] + gt[..., 1] + gt[..., 2])
+
+
+def single_atom_potential(atom_no, pixel_size, grid_shape, center_coords=None, supersampling=4,
+                          parameterization="lobato"):
+    """atom_potentials.py:588-681: the potential on a supersampled grid (point k of an
+    axis at (k - K/2) * pixel / s), r = sqrt(dx^2 + dy^2 + 1e-10), then the mean of each
+    pixel's s x s block (``_downsample_potential`` :537-583)."""
+    s = int(supersampling)
+    step = pixel_size / s
+    gh, gw = grid_shape[0] * s, grid_shape[1] * s
+    cx, cy = (0.0, 0.0) if center_coords is None else (center_coords[0], center_coords[1])
+    yc = (np.arange(gh) - gh // 2) * step
+    xc = (np.arange(gw) - gw // 2) * step
+    ya, xa = np.meshgrid(yc, xc, indexing="ij")
+    r = np.sqrt((xa - cx) ** 2 + (ya - cy) ** 2 + 1e-10)
+    fine = projected_potential(element_coefficients(atom_no, parameterization), r, parameterization)
+    return fine.reshape(grid_shape[0], s, grid_shape[1], s).mean(axis=(1, 3))

@@ -67,6 +67,7 @@ from .multislice_recon import (  # noqa: F401
     single_slice_ptychography,
 )
 from .crystal import CrystalData, create_crystal_data, crystal_potential_slices  # noqa: F401
+from .elements import kirkland_parameters, lobato_parameters, single_atom_potential  # noqa: F401
 from .ensemble import (  # noqa: F401
     coherence_to_distribution,
     ensemble_axes_for_cbed,

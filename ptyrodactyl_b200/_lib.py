@@ -67,6 +67,7 @@ EXPORTED_SYMBOLS = (
     "ptyro_sched_memory",
     "ptyro_atom_slices_workspace_bytes",
     "ptyro_atom_slices",
+    "ptyro_atom_potential",
 )
 
 PTYRO_JOB_FORWARD = 0
@@ -219,6 +220,8 @@ def _declare(lib) -> None:
     lib.ptyro_ms_forward_noalloc.argtypes = [pp, vp, vp, vp, vp, vp, vp]
     lib.ptyro_test_wait_timeout.restype = ctypes.c_int
     lib.ptyro_test_wait_timeout.argtypes = [i32, i32, vp, vp, vp]
+    lib.ptyro_atom_potential.restype = ctypes.c_int
+    lib.ptyro_atom_potential.argtypes = [i32, vp, dbl, i32, i32, dbl, dbl, i32, vp, vp]
 
 
 def load(path: str | None = None):

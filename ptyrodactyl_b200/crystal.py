@@ -8,11 +8,10 @@ device places every atom: per slice and atom type a structure factor (a product 
 per-atom phase tables), times the spectrum of the type's projected potential, one
 inverse FFT (``ptyro_place_atoms``; ``_process_all_slices`` :826-994).
 
-The reference builds each element's projected potential from the Lobato or
-Kirkland parametrisation (``single_atom_potential`` :588-681). Those coefficient
-tables are not part of this engine: callers pass the per-element lookup potentials
-(``atom_potentials``: atomic number -> (H, W) array, the atom at the grid centre),
-for instance computed once by the reference's own ``single_atom_potential``.
+Each element's projected potential comes from the Lobato or Kirkland parametrisation
+(``single_atom_potential`` :588-681, evaluated on the device by ``elements.py``) on the
+padded grid with the atom at its centre; callers may instead pass their own lookups
+(``atom_potentials``: atomic number -> (H, W) array, the atom at the grid centre).
 """
 
 from __future__ import annotations
@@ -126,15 +125,13 @@ def crystal_potential_slices(crystal_data: CrystalData, pixel_size: float, slice
                              atom_potentials: Optional[Mapping[int, object]] = None) -> PotentialSlices:
     """Potential slices of ``crystal_data`` (atom_potentials.py:1364-1510) on a padded
     grid, cropped by ``padding``. The padded grid must be square with a power-of-two
-    edge in [16, 1024] (pass ``grid_shape``); ``atom_potentials`` maps each atomic
-    number to its (H, W) projected potential at the grid centre. ``supersampling``
-    and ``parameterization`` describe how those lookups were made and are not used."""
-    del supersampling, parameterization
+    edge in [16, 1024] (pass ``grid_shape``). Each element's lookup is its projected
+    potential (``parameterization``, ``supersampling``) at the grid centre, or
+    ``atom_potentials[Z]`` when given."""
+    from .elements import _check_parameterization
+    _check_parameterization(parameterization)
     if crystal_data.lattice is None:
         raise ValueError("CrystalData.lattice must not be None")
-    if atom_potentials is None:
-        raise NotImplementedError("pass atom_potentials: the element parametrisations are not built into this "
-                                  "engine")
     positions, numbers = _apply_repeats(crystal_data.positions, crystal_data.atomic_numbers, crystal_data.lattice,
                                         repeats)
     z = positions[:, 2]
@@ -149,6 +146,9 @@ def crystal_potential_slices(crystal_data: CrystalData, pixel_size: float, slice
                          " pass grid_shape")
     num_slices = ns if ns is not None else int(slice_idx.max()) + 1
     elements = sorted(set(int(v) for v in numbers))
+    if atom_potentials is None:
+        from .elements import atom_lookup
+        atom_potentials = atom_lookup(elements, pixel_size, (height, width), supersampling, parameterization)
     missing = [e for e in elements if e not in atom_potentials]
     if missing:
         raise ValueError(f"atom_potentials has no entry for atomic numbers {missing}")

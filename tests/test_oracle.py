@@ -263,3 +263,14 @@ def test_oracle_position_gradient_matches_finite_differences():
             e[i, c] = 1e-5
             fd = (loss(pos + e) - loss(pos - e)) / 2e-5
             assert abs(fd - dpos[i, c]) <= 1e-6 * max(1.0, abs(fd))
+
+
+@pytest.mark.parametrize("z,expected_sum,expected_max", [(6, 3304.630500664369, 599.0660669230273),
+                                                         (14, 7467.50633667953, 1309.8209272295387),
+                                                         (79, 16835.066119859865, 6296.83419348897)])
+def test_oracle_single_atom_potential_matches_captured_reference(z, expected_sum, expected_max):
+    """The reference's captured Kirkland C/Si/Au values (test_atom_potentials.py:31-63,
+    rtol 2e-15 there): the oracle restates the reference's Bessel approximations."""
+    pot = R.single_atom_potential(z, 0.2, (16, 16), supersampling=2, parameterization="kirkland")
+    assert abs(pot.sum() - expected_sum) <= 2e-15 * expected_sum
+    assert abs(pot.max() - expected_max) <= 2e-15 * expected_max
