@@ -105,9 +105,10 @@ def test_engine_loops_match_the_pinned_oracle_loop(fn):
     case for the scan positions here: the object is nearly transparent (|T - 1| ~ 1e-5),
     so the patterns hardly depend on position and the position gradient is a small
     difference of large terms (the oracle's own complex64 and complex128 values of it
-    differ by 4-8 %). The positions are therefore held to the first step's direction
-    and the second step to 5 % of a step; well-conditioned position gradients are
-    checked against the oracle at 1e-4 in test_gpu_grad.py."""
+    differ by 4-8 %, and the second Adam step with them). The positions are therefore
+    held to a quarter of a step: every first step must go the oracle's way (a wrong
+    direction is two steps off); well-conditioned position gradients are checked
+    against the oracle at 1e-4 in test_gpu_grad.py."""
     from oracle.jax_prng import normal_f64, prng_key, split
     n = 16
     keys = split(prng_key(11), 5)
@@ -142,4 +143,4 @@ def test_engine_loops_match_the_pinned_oracle_loop(fn):
     assert rel_l2(got[0].cpu().numpy(), want["pot"]) < 1e-5
     assert rel_l2(got[1].cpu().numpy(), want["modes"]) < 1e-5
     if got[2] is not None:
-        assert np.abs(got[2].cpu().numpy() - want["pos"]).max() < 0.05 * lr_pos
+        assert np.abs(got[2].cpu().numpy() - want["pos"]).max() < 0.25 * lr_pos
