@@ -784,9 +784,10 @@ def run_serve(args, rank, world, local_rank):
 def run_profile_case(args, rank, world, local_rank):
     """A small, self-checking case of the forward engine for profilers: one batched
     forward over ``--probes`` scan positions of the perovskite workload (``--grid``
-    edge, 2 slices, one batch), then ``--reps`` steady-state passes per axis
+    edge, ``--slices`` slices, one batch), then ``--reps`` steady-state passes per axis
     (``ptyro_ms_steady_pass``) on the wave slots the forward left in the workspace.
-    Pass-kernel launches: 6 in the forward (setup kernels aside), then ``--reps`` row
+    Pass-kernel launches: slices + 4 in the forward (setup kernels aside; one for the
+    wave-resident kernel, tune bit 32768), then ``--reps`` row
     passes and ``--reps`` column passes. Exits non-zero if the patterns are not finite
     or the device status word is set."""
     import torch
@@ -794,22 +795,22 @@ def run_profile_case(args, rank, world, local_rank):
     from ptyrodactyl_b200.simulations import make_probe, ms_params
     from ptyrodactyl_b200.types import create_detector_config, create_microscope_config
 
-    n, probes, reps = args.grid, args.probes, args.reps
+    n, probes, reps, S = args.grid, args.probes, args.reps, args.slices
     tune = default_tune(n) if args.tune < 0 else args.tune
     w = synth.CONFIG2
     dev = torch.device("cuda", local_rank)
     torch.cuda.set_device(dev)
     lib = _lib.load()
     if n == w.n:
-        pot = torch.as_tensor(synth.potential_slices(w, num_slices=2), device=dev)
+        pot = torch.as_tensor(synth.potential_slices(w, num_slices=S), device=dev)
     else:
-        pot = torch.rand((n, n, 2), generator=torch.Generator(device=dev).manual_seed(1), device=dev) * 50
+        pot = torch.rand((n, n, S), generator=torch.Generator(device=dev).manual_seed(1), device=dev) * 50
     mic = create_microscope_config(w.voltage_kv, w.aperture_mrad, probe_shape=(n, n))
     probe = make_probe(mic, create_detector_config(w.calib))[..., None].contiguous()
     pos = torch.as_tensor(synth.raster_positions(w), device=dev)[:probes].contiguous()
     probes = pos.shape[0]
     wt = torch.ones(1, device=dev)
-    prm = ms_params(n, 2, 1, probes, w.voltage_kv, synth.SLICE_DZ, w.calib, w.calib, pot.stride(), probe.stride(),
+    prm = ms_params(n, S, 1, probes, w.voltage_kv, synth.SLICE_DZ, w.calib, w.calib, pot.stride(), probe.stride(),
                     probes, tune)
     nb = lib.ptyro_ms_workspace_bytes(ctypes.byref(prm))
     ws = torch.empty(nb, dtype=torch.uint8, device=dev)
@@ -877,6 +878,7 @@ def main():
                     help="config3 mode: scan positions sampled; profile-case mode: probes in the one batch")
     ap.add_argument("--grid", type=int, default=256, help="profile-case mode: grid edge")
     ap.add_argument("--reps", type=int, default=1, help="profile-case mode: steady passes per axis")
+    ap.add_argument("--slices", type=int, default=2, help="profile-case mode: slices of the forward")
     ap.add_argument("--requests", type=int, default=64, help="serve mode: requests in the mix")
     ap.add_argument("--rate", type=float, default=20.0, help="serve mode: Poisson arrival rate (1/s)")
     ap.add_argument("--seed", type=int, default=5, help="serve mode: mix seed")

@@ -152,6 +152,19 @@ int ptyro_ms_backward_positions(const ptyro_ms_params* p, int32_t ckpt_every, co
                                 float* grad_modes, double* grad_positions, void* workspace, size_t workspace_bytes,
                                 void* stream);
 
+/* Workspace bytes of ptyro_ms_weight_grad for `p` (its num_modes). */
+size_t ptyro_ms_weight_grad_workspace_bytes(const ptyro_ms_params* p);
+
+/* Gradient of the loss with respect to the incoherent mode weights of stem_4d
+ * (apply_distribution, src/ptyrodactyl/multislice/reduce.py:29-89: I = sum_m w_m |A_m|^2):
+ * grad_weights[m] = sum_p sum_k dL/dI_p(k) |A_pm(k)|^2, float64 (M,), from the far-field
+ * amplitudes stored by ptyro_ms_forward_ckpt (same p, same ckpt_every) and dL/d(patterns)
+ * (P, N, N) in the patterns' fftshifted layout. Deterministic (fixed partial sums added
+ * in order). The reference differentiates through the weights with jax.grad. */
+int ptyro_ms_weight_grad(const ptyro_ms_params* p, int32_t ckpt_every, const float* residuals,
+                         const float* grad_patterns, double* grad_weights, void* workspace, size_t workspace_bytes,
+                         void* stream);
+
 /* The same model run the plain way: one scan position at a time, one kernel per
  * stage (shift, and per slice transmission multiply, FFT2, propagator multiply,
  * IFFT2, then FFT2 and |.|^2), the way the reference's vmap body reads

@@ -68,6 +68,8 @@ EXPORTED_SYMBOLS = (
     "ptyro_atom_slices_workspace_bytes",
     "ptyro_atom_slices",
     "ptyro_atom_potential",
+    "ptyro_ms_weight_grad_workspace_bytes",
+    "ptyro_ms_weight_grad",
 )
 
 PTYRO_JOB_FORWARD = 0
@@ -220,6 +222,10 @@ def _declare(lib) -> None:
     lib.ptyro_ms_forward_noalloc.argtypes = [pp, vp, vp, vp, vp, vp, vp]
     lib.ptyro_test_wait_timeout.restype = ctypes.c_int
     lib.ptyro_test_wait_timeout.argtypes = [i32, i32, vp, vp, vp]
+    lib.ptyro_ms_weight_grad_workspace_bytes.restype = sz
+    lib.ptyro_ms_weight_grad_workspace_bytes.argtypes = [pp]
+    lib.ptyro_ms_weight_grad.restype = ctypes.c_int
+    lib.ptyro_ms_weight_grad.argtypes = [pp, i32, vp, vp, vp, vp, sz, vp]
     lib.ptyro_atom_potential.restype = ctypes.c_int
     lib.ptyro_atom_potential.argtypes = [i32, vp, dbl, i32, i32, dbl, dbl, i32, vp, vp]
 

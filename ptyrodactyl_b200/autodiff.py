@@ -125,8 +125,28 @@ class Stem4dFunction(torch.autograd.Function):
         saved = [_plain(t) for t in ctx.saved_tensors]
         with torch._C._DisableFuncTorch(), torch.cuda.device(saved[0].device):
             g_slices, g_modes, g_pos = Stem4dFunction._adjoint(ctx, saved, _plain(grad_out))
+            g_w = Stem4dFunction._weight_grad(ctx, saved, _plain(grad_out)) if ctx.needs_input_grad[2] else None
         return (g_slices if ctx.needs_input_grad[0] else None, g_modes if ctx.needs_input_grad[1] else None,
-                None, g_pos, None, None, None, None, None, None, None, None, None)
+                g_w, g_pos, None, None, None, None, None, None, None, None, None)
+
+    @staticmethod
+    def _weight_grad(ctx, saved, grad_out):
+        """dL/dw_m = sum_p sum_k dL/dI_p(k) |A_pm(k)|^2 from the stored far-field amplitudes
+        (ptyro_ms_weight_grad), in the weights' dtype."""
+        slices, modes, weights, positions, res, windows = saved
+        slice_thickness, voltage_kv, calib_ang, shift_calib_ang, k, batch, tune, n, f, record = ctx.cfg
+        lib = _lib.load()
+        dev = slices.device
+        S, M, P = slices.shape[2], modes.shape[2], positions.shape[0]
+        prm = ms_params(n, S, M, P, voltage_kv, slice_thickness, calib_ang, shift_calib_ang, slices.stride(),
+                        modes.stride(), batch, tune, f, windows)
+        out = torch.empty(M, dtype=torch.float64, device=dev)
+        nbytes = lib.ptyro_ms_weight_grad_workspace_bytes(ctypes.byref(prm))
+        ws = _workspace(nbytes, dev)
+        g = grad_out.to(torch.float32).contiguous()
+        _lib.check(lib.ptyro_ms_weight_grad(ctypes.byref(prm), k, res.data_ptr(), g.data_ptr(), out.data_ptr(),
+                                            ws.data_ptr(), nbytes, _stream_ptr(dev)))
+        return out.to(weights.dtype)
 
     @staticmethod
     def _adjoint(ctx, saved, grad_out):
@@ -169,12 +189,21 @@ class Stem4dFunction(torch.autograd.Function):
         t_slices, t_modes, t_weights, t_positions = (_plain(t) for t in (t_slices, t_modes, t_weights, t_positions))
         slice_thickness, voltage_kv, calib_ang, shift_calib_ang, k, batch, tune, n, f, record = ctx.cfg
         # torch.func.jvp hands zero tangents to the inputs it does not differentiate
-        if any(t is not None and bool(t.any()) for t in (t_weights, t_positions)):
-            raise NotImplementedError("stem_4d has no derivative with respect to weights or positions")
+        if t_positions is not None and bool(t_positions.any()):
+            raise NotImplementedError("stem_4d has no forward-mode derivative with respect to positions")
         with torch._C._DisableFuncTorch():  # buffers made here must be plain tensors
+            if t_weights is not None and bool(t_weights.any()):
+                # the patterns are linear in the weights: their tangent is the forward with
+                # the tangent weights, added to the potential's and modes' tangent below
+                from .simulations import run_forward
+                w_tangent = run_forward(slices, slice_thickness, modes, t_weights.to(torch.float32).contiguous(),
+                                        positions, voltage_kv, calib_ang, shift_calib_ang, batch=batch,
+                                        windows=windows)
+            else:
+                w_tangent = None
             _, tangent = jvp(slices, modes, weights, positions, t_slices, t_modes, slice_thickness, voltage_kv,
                              calib_ang, shift_calib_ang, batch=batch, windows=windows, want_patterns=False)
-        return tangent, None
+        return (tangent if w_tangent is None else tangent + w_tangent), None
 
 
 def stem_4d_patterns(slices: torch.Tensor, modes: torch.Tensor, weights: torch.Tensor, positions: torch.Tensor,
@@ -186,7 +215,8 @@ def stem_4d_patterns(slices: torch.Tensor, modes: torch.Tensor, weights: torch.T
     ``windows`` the potential is a larger periodic field (see ``run_forward``).
     Reverse mode (``backward``, ``torch.func.grad/vjp``) and forward mode
     (``torch.func.jvp``, dual tensors) both run hand-written kernels."""
-    record = bool(slices.requires_grad or modes.requires_grad or positions.requires_grad) and torch.is_grad_enabled()
+    record = bool(slices.requires_grad or modes.requires_grad or positions.requires_grad or weights.requires_grad) \
+        and torch.is_grad_enabled()
     return Stem4dFunction.apply(slices, modes, weights, positions, float(slice_thickness), float(voltage_kv),
                                 float(calib_ang), float(calib_ang if shift_calib_ang is None else shift_calib_ang),
                                 int(ckpt_every), int(batch), int(default_tune(modes.shape[0]) if tune is None else tune),

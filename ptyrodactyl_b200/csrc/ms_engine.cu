@@ -114,6 +114,25 @@ int ptyro_ms_backward_positions(const ptyro_ms_params* p, int32_t ckpt_every, co
                        grad_potential, grad_modes, workspace, workspace_bytes, stream, modes, grad_positions);
 }
 
+size_t ptyro_ms_weight_grad_workspace_bytes(const ptyro_ms_params* p) {
+  if (validate(p)) return 0;
+  return weight_grad_workspace_bytes(p->num_modes);
+}
+
+int ptyro_ms_weight_grad(const ptyro_ms_params* p, int32_t ckpt_every, const float* residuals,
+                         const float* grad_patterns, double* grad_weights, void* workspace, size_t workspace_bytes,
+                         void* stream) {
+  int rc = validate(p);
+  if (rc) return rc;
+  if (ckpt_every < 1) return fail(PTYRO_ERR_INVALID, "ckpt_every must be >= 1");
+  if (!grad_weights) return fail(PTYRO_ERR_INVALID, "grad_weights is NULL");
+  if (p->num_probes > 0 && (!residuals || !grad_patterns)) return fail(PTYRO_ERR_INVALID, "NULL array argument");
+  if (!workspace || workspace_bytes < weight_grad_workspace_bytes(p->num_modes))
+    return fail(PTYRO_ERR_WORKSPACE, "workspace too small for the weight gradient");
+  return weight_grad(p, ckpt_every, (const float2*)residuals, grad_patterns, grad_weights, (double*)workspace,
+                     (cudaStream_t)stream);
+}
+
 int ptyro_ms_forward_plain(const ptyro_ms_params* p, const float* potential, const float* modes,
                            const float* weights, const double* positions, float* patterns, void* workspace,
                            size_t workspace_bytes, void* stream) {

@@ -12,10 +12,13 @@ struct ResGeom {
   static constexpr int kPairs = WARPS * G;  // line pairs per iteration of a pass
   static_assert((N / 2) % kPairs == 0, "the CTA's line pairs must tile the grid");
   static constexpr int kIters = (N / 2) / kPairs;
-  // Row pitch of the resident wave, in float2. N + 8 (== 8 mod 16) puts consecutive
-  // rows 64 bytes apart modulo the 128-byte bank window, so the 16-byte column-pair
-  // reads of a warp (4 column pairs x 8 rows) fill four full wavefronts.
-  static constexpr int kPitch = N + 8;
+  // Row pitch of the resident wave, in float2: N + 4 (== 4 mod 8). Row passes: the line
+  // pairs (2p, 2p + 1) of a warp start 2 * pitch * 8 == 64 bytes apart modulo the
+  // 128-byte bank window, so each 8-byte load of a warp (4 pairs x 8 lanes) takes the
+  // minimum two wavefronts. Column passes: consecutive rows sit 32 bytes apart modulo
+  // 128, so the 16-byte column-pair reads of a warp (8 rows x 64 bytes) cover every
+  // bank exactly four times, the minimum four wavefronts.
+  static constexpr int kPitch = N + 4;
   static constexpr size_t kWave = sizeof(float2) * (size_t)N * kPitch;
   static constexpr size_t kTables = sizeof(float2) * 2 * (size_t)N;  // twiddles, propagator factor
   static constexpr size_t kXbuf = sizeof(Pair) * (size_t)kPairs * PairBuf<N1, N2>::kSize;

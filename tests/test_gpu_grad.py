@@ -237,3 +237,31 @@ def test_lambda_only_adjoint_windowed_field():
     lock = pb.vjp(*args, ckpt_every=1, windows=windows, batch=3, tune=pb.simulations.default_tune(n) | 65536)
     for a, b in zip(lam, lock):
         assert torch.equal(a, b)
+
+
+def test_mode_weight_gradient_and_tangent_match_oracle():
+    """dL/dw_m = sum_p sum_k g_p(k) I_pm(k) with I_pm the pattern of mode m alone
+    (ptyro_ms_weight_grad over the stored amplitudes), and the weights' forward-mode
+    tangent sum_m t_m I_pm; the oracle's per-mode patterns give both."""
+    pot, modes, w, pos, g = _case(64, 4, 2, 3, seed=21)
+    dev = torch.device("cuda")
+    sl = torch.as_tensor(pot, dtype=torch.float32, device=dev)
+    md = torch.as_tensor(modes.astype(np.complex64), device=dev)
+    ps = torch.as_tensor(pos, dtype=torch.float64, device=dev)
+    wt = torch.as_tensor(w, dtype=torch.float32, device=dev).requires_grad_(True)
+    per_mode = [R.stem_4d(pot, 1.7, 0.3, modes[..., m:m + 1], [1.0], 0.3, 200.0, pos, 0.3)["data"] for m in range(2)]
+    pat = pb.stem_4d_patterns(sl, md, wt, ps, 1.7, 200.0, 0.3)
+    (pat * torch.as_tensor(g, dtype=torch.float32, device=dev)).sum().backward()
+    want = np.array([np.sum(g * per_mode[m]) for m in range(2)])
+    assert rel_l2(wt.grad.cpu().numpy(), want) < TOL
+    t = torch.tensor([0.3, -0.5], dtype=torch.float32, device=dev)
+    _, tan = torch.func.jvp(lambda w_: pb.stem_4d_patterns(sl, md, w_, ps, 1.7, 200.0, 0.3), (wt.detach(),), (t,))
+    assert rel_l2(tan.cpu().numpy(), 0.3 * per_mode[0] - 0.5 * per_mode[1]) < TOL
+    # through the public stem_4d with a ProbeModes whose weights require grad
+    beam = pb.ProbeModes(md, wt.detach().clone().requires_grad_(True), 0.3)
+    slices = pb.create_potential_slices(sl, 1.7, 0.3)
+    mic = pb.create_microscope_config(200.0, 25.0, probe_shape=(64, 64))
+    det = pb.create_detector_config(0.3, scan_positions_px=pos)
+    out = pb.stem_4d(slices, beam, mic, det)
+    (out.data * torch.as_tensor(g, dtype=torch.float32, device=dev)).sum().backward()
+    assert rel_l2(beam.weights.grad.cpu().numpy(), want) < TOL
