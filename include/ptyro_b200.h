@@ -303,6 +303,57 @@ int ptyro_test_wait_timeout(int32_t warps, int32_t polls, uint32_t* status, int3
 int ptyro_atom_potential(int32_t parameterization, const double* coeffs, double pixel_size, int32_t h, int32_t w,
                          double center_x, double center_y, int32_t supersampling, double* out, void* stream);
 
+/* ---- Any grid size. The entry points above take square power-of-two grids 16..1024
+ * (p->n). These take any height x width (each 1..4096), as the reference does
+ * (fftfreq of any size, simulations.py:162-225; any probe_shape), with p->n ignored,
+ * no potential-field windows, and every slice's wave kept as a residual (checkpoint
+ * spacing 1). The 1-D transforms are four-step DFTs with direct sums (N1 + N2 complex
+ * multiply-adds per point for N = N1 N2), slower than the fused path; results follow
+ * the same arithmetic (stem_4d, simulations.py:1330-1443, and its jax.grad). */
+size_t ptyro_gm_workspace_bytes(const ptyro_ms_params* p, int32_t height, int32_t width);
+
+/* Residual bytes ptyro_gm_forward writes when `residuals` is not NULL: per (probe,
+ * mode) the wave after each of the S transmission multiplies and the far-field
+ * amplitude, (P, M, S + 1, height, width) complex64. */
+size_t ptyro_gm_residual_bytes(const ptyro_ms_params* p, int32_t height, int32_t width);
+
+/* ptyro_ms_forward / ptyro_ms_forward_ckpt on a height x width grid: patterns (P, H, W)
+ * fftshifted (odd sizes shift by floor(N/2), as numpy's fftshift); residuals NULL or
+ * ptyro_gm_residual_bytes. p->flags PTYRO_FLAG_ACCUMULATE adds into patterns. */
+int ptyro_gm_forward(const ptyro_ms_params* p, int32_t height, int32_t width, const float* potential,
+                     const float* modes, const float* weights, const double* positions, float* patterns,
+                     float* residuals, void* workspace, size_t workspace_bytes, void* stream);
+
+size_t ptyro_gm_backward_workspace_bytes(const ptyro_ms_params* p, int32_t height, int32_t width);
+
+/* ptyro_ms_backward(_positions) on a height x width grid, from ptyro_gm_forward's
+ * residuals: dL/dV (potential strides), the modes' gradient in JAX's convention, and
+ * dL/d(positions) (P, 2) when grad_positions is not NULL (then modes is needed). */
+int ptyro_gm_backward(const ptyro_ms_params* p, int32_t height, int32_t width, const float* potential,
+                      const float* modes, const float* weights, const double* positions, const float* residuals,
+                      const float* grad_patterns, float* grad_potential, float* grad_modes, double* grad_positions,
+                      void* workspace, size_t workspace_bytes, void* stream);
+
+/* numpy fft2 / ifft2 of `count` contiguous height x width complex64 planes in place,
+ * any height and width in [1, 4096] (inverse scaled by 1 / (height width)). */
+size_t ptyro_gm_fft_workspace_bytes(int32_t height, int32_t width);
+int ptyro_gm_fft2(int32_t height, int32_t width, int32_t count, int32_t inverse, float* data, void* workspace,
+                  size_t workspace_bytes, void* stream);
+
+/* make_probe (simulations.py:334-431) for any probe_shape (height x width, 1..4096 each):
+ * the aperture and aberration on the reference's rolled-arange frequency grid, ifft2
+ * and ifftshift; probe (height, width) complex64. */
+size_t ptyro_gm_make_probe_workspace_bytes(int32_t height, int32_t width);
+int ptyro_gm_make_probe(int32_t height, int32_t width, double voltage_kv, double aperture_mrad,
+                        double probe_calibration_pm, double defocus_ang, double c3_ang, double c5_ang, float* probe,
+                        void* workspace, size_t workspace_bytes, void* stream);
+
+/* ptyro_ms_weight_grad from ptyro_gm_forward's residuals. */
+size_t ptyro_gm_weight_grad_workspace_bytes(const ptyro_ms_params* p, int32_t height, int32_t width);
+int ptyro_gm_weight_grad(const ptyro_ms_params* p, int32_t height, int32_t width, const float* residuals,
+                         const float* grad_patterns, double* grad_weights, void* workspace, size_t workspace_bytes,
+                         void* stream);
+
 /* Workspace bytes of ptyro_atom_slices for edge n and num_types atom types. */
 size_t ptyro_atom_slices_workspace_bytes(int32_t n, int32_t num_types);
 

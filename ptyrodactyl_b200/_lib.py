@@ -70,6 +70,17 @@ EXPORTED_SYMBOLS = (
     "ptyro_atom_potential",
     "ptyro_ms_weight_grad_workspace_bytes",
     "ptyro_ms_weight_grad",
+    "ptyro_gm_workspace_bytes",
+    "ptyro_gm_residual_bytes",
+    "ptyro_gm_forward",
+    "ptyro_gm_backward_workspace_bytes",
+    "ptyro_gm_backward",
+    "ptyro_gm_fft_workspace_bytes",
+    "ptyro_gm_fft2",
+    "ptyro_gm_make_probe_workspace_bytes",
+    "ptyro_gm_make_probe",
+    "ptyro_gm_weight_grad_workspace_bytes",
+    "ptyro_gm_weight_grad",
 )
 
 PTYRO_JOB_FORWARD = 0
@@ -226,6 +237,25 @@ def _declare(lib) -> None:
     lib.ptyro_ms_weight_grad_workspace_bytes.argtypes = [pp]
     lib.ptyro_ms_weight_grad.restype = ctypes.c_int
     lib.ptyro_ms_weight_grad.argtypes = [pp, i32, vp, vp, vp, vp, sz, vp]
+    for name in ("ptyro_gm_workspace_bytes", "ptyro_gm_residual_bytes", "ptyro_gm_backward_workspace_bytes"):
+        getattr(lib, name).restype = sz
+        getattr(lib, name).argtypes = [pp, i32, i32]
+    lib.ptyro_gm_fft_workspace_bytes.restype = sz
+    lib.ptyro_gm_fft_workspace_bytes.argtypes = [i32, i32]
+    lib.ptyro_gm_fft2.restype = ctypes.c_int
+    lib.ptyro_gm_fft2.argtypes = [i32, i32, i32, i32, vp, vp, sz, vp]
+    lib.ptyro_gm_make_probe_workspace_bytes.restype = sz
+    lib.ptyro_gm_make_probe_workspace_bytes.argtypes = [i32, i32]
+    lib.ptyro_gm_make_probe.restype = ctypes.c_int
+    lib.ptyro_gm_make_probe.argtypes = [i32, i32, dbl, dbl, dbl, dbl, dbl, dbl, vp, vp, sz, vp]
+    lib.ptyro_gm_weight_grad_workspace_bytes.restype = sz
+    lib.ptyro_gm_weight_grad_workspace_bytes.argtypes = [pp, i32, i32]
+    lib.ptyro_gm_weight_grad.restype = ctypes.c_int
+    lib.ptyro_gm_weight_grad.argtypes = [pp, i32, i32, vp, vp, vp, vp, sz, vp]
+    lib.ptyro_gm_forward.restype = ctypes.c_int
+    lib.ptyro_gm_forward.argtypes = [pp, i32, i32, vp, vp, vp, vp, vp, vp, vp, sz, vp]
+    lib.ptyro_gm_backward.restype = ctypes.c_int
+    lib.ptyro_gm_backward.argtypes = [pp, i32, i32, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, sz, vp]
     lib.ptyro_atom_potential.restype = ctypes.c_int
     lib.ptyro_atom_potential.argtypes = [i32, vp, dbl, i32, i32, dbl, dbl, i32, vp, vp]
 

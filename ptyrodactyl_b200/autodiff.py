@@ -24,13 +24,16 @@ import torch
 
 from . import _lib
 from .simulations import (
-    _check_edge,
     _stream_ptr,
     _workspace,
+    any_grid_params,
+    check_any_grid,
     check_windows,
     default_tune,
+    engine_grid,
     ms_params,
     relativistic_wavelength_ang,
+    run_forward_any,
 )
 
 DEFAULT_CKPT = 0  # 0: every slice when the residuals fit RESIDUAL_BUDGET_BYTES, else ceil(sqrt(S))
@@ -76,6 +79,9 @@ class Stem4dFunction(torch.autograd.Function):
         lib = _lib.load()
         dev = slices.device
         S, M, P = slices.shape[2], modes.shape[2], positions.shape[0]
+        if not engine_grid(modes.shape[0], modes.shape[1]):
+            return Stem4dFunction._forward_any(lib, slices, modes, weights, positions, slice_thickness, voltage_kv,
+                                               calib_ang, shift_calib_ang, batch, windows, record)
         n, f = check_windows(slices, modes, windows, P)
         k = _ckpt_for(S, ckpt_every, n, P * M)
         prm = ms_params(n, S, M, P, voltage_kv, slice_thickness, calib_ang, shift_calib_ang, slices.stride(),
@@ -90,6 +96,22 @@ class Stem4dFunction(torch.autograd.Function):
                 Stem4dFunction._forward_call(lib, prm, k, record, slices, modes, weights, positions, out, res, ws,
                                              ws_bytes, dev)
             _lib.check_workspace_status(ws, "stem_4d forward")
+        return out, res
+
+    @staticmethod
+    def _forward_any(lib, slices, modes, weights, positions, slice_thickness, voltage_kv, calib_ang,
+                     shift_calib_ang, batch, windows, record):
+        """Any height x width (ptyro_gm_forward): the residuals hold every slice's wave
+        and the far-field amplitudes, the any-size adjoint's only input."""
+        h, w = check_any_grid(slices, modes, windows)
+        P = positions.shape[0]
+        prm = any_grid_params(slices, modes, P, voltage_kv, slice_thickness, calib_ang, shift_calib_ang, batch)
+        nres = lib.ptyro_gm_residual_bytes(ctypes.byref(prm), h, w) // 4 if (P and record) else 0
+        res = torch.empty(nres, dtype=torch.float32, device=slices.device)
+        status = _lib.new_status(slices.device)
+        out = run_forward_any(slices, slice_thickness, modes, weights, positions, voltage_kv, calib_ang,
+                              shift_calib_ang, batch=batch, status=status, residuals=res if nres else None)
+        _lib.check_status(status, "stem_4d forward")
         return out, res
 
     @staticmethod
@@ -113,6 +135,7 @@ class Stem4dFunction(torch.autograd.Function):
         ctx.save_for_backward(slices, modes, weights, positions, res, windows)
         ctx.save_for_forward(slices, modes, weights, positions, windows)
         n = modes.shape[0]
+        ctx.any_grid = not engine_grid(modes.shape[0], modes.shape[1])
         ctx.cfg = (slice_thickness, voltage_kv, calib_ang, shift_calib_ang,
                    _ckpt_for(slices.shape[2], ckpt_every, n, positions.shape[0] * modes.shape[2]),
                    batch, tune, n, slices.shape[0], record)
@@ -138,12 +161,20 @@ class Stem4dFunction(torch.autograd.Function):
         lib = _lib.load()
         dev = slices.device
         S, M, P = slices.shape[2], modes.shape[2], positions.shape[0]
+        out = torch.empty(M, dtype=torch.float64, device=dev)
+        g = grad_out.to(torch.float32).contiguous()
+        if ctx.any_grid:
+            h, w = modes.shape[0], modes.shape[1]
+            prm = any_grid_params(slices, modes, P, voltage_kv, slice_thickness, calib_ang, shift_calib_ang, batch)
+            nbytes = lib.ptyro_gm_weight_grad_workspace_bytes(ctypes.byref(prm), h, w)
+            ws = _workspace(nbytes, dev)
+            _lib.check(lib.ptyro_gm_weight_grad(ctypes.byref(prm), h, w, res.data_ptr(), g.data_ptr(),
+                                                out.data_ptr(), ws.data_ptr(), nbytes, _stream_ptr(dev)))
+            return out.to(weights.dtype)
         prm = ms_params(n, S, M, P, voltage_kv, slice_thickness, calib_ang, shift_calib_ang, slices.stride(),
                         modes.stride(), batch, tune, f, windows)
-        out = torch.empty(M, dtype=torch.float64, device=dev)
         nbytes = lib.ptyro_ms_weight_grad_workspace_bytes(ctypes.byref(prm))
         ws = _workspace(nbytes, dev)
-        g = grad_out.to(torch.float32).contiguous()
         _lib.check(lib.ptyro_ms_weight_grad(ctypes.byref(prm), k, res.data_ptr(), g.data_ptr(), out.data_ptr(),
                                             ws.data_ptr(), nbytes, _stream_ptr(dev)))
         return out.to(weights.dtype)
@@ -161,6 +192,9 @@ class Stem4dFunction(torch.autograd.Function):
         if P == 0:
             g_slices.zero_()
             g_modes.zero_()
+        elif ctx.any_grid:
+            Stem4dFunction._adjoint_any(lib, slices, modes, weights, positions, res, grad_out, slice_thickness,
+                                        voltage_kv, calib_ang, shift_calib_ang, batch, g_slices, g_modes, g_pos)
         else:
             g = grad_out.to(torch.float32).contiguous()
             prm = ms_params(n, S, M, P, voltage_kv, slice_thickness, calib_ang, shift_calib_ang, slices.stride(),
@@ -183,11 +217,34 @@ class Stem4dFunction(torch.autograd.Function):
         return g_slices, g_modes.conj().resolve_conj(), g_pos
 
     @staticmethod
+    def _adjoint_any(lib, slices, modes, weights, positions, res, grad_out, slice_thickness, voltage_kv, calib_ang,
+                     shift_calib_ang, batch, g_slices, g_modes, g_pos):
+        """ptyro_gm_backward: dL/dV, the modes' gradient (JAX's convention) and, when
+        g_pos is given, dL/d(positions), from the any-size forward's residuals."""
+        dev = slices.device
+        h, w = modes.shape[0], modes.shape[1]
+        P = positions.shape[0]
+        prm = any_grid_params(slices, modes, P, voltage_kv, slice_thickness, calib_ang, shift_calib_ang, batch)
+        g = grad_out.to(torch.float32).contiguous()
+        ws_bytes = lib.ptyro_gm_backward_workspace_bytes(ctypes.byref(prm), h, w)
+        if ws_bytes == 0:
+            _lib.check(_lib.PTYRO_ERR_INVALID)
+        ws = _workspace(ws_bytes, dev)
+        _lib.check(lib.ptyro_gm_backward(ctypes.byref(prm), h, w, slices.data_ptr(), modes.data_ptr(),
+                                         weights.data_ptr(), positions.data_ptr(), res.data_ptr(), g.data_ptr(),
+                                         g_slices.data_ptr(), g_modes.data_ptr(),
+                                         None if g_pos is None else g_pos.data_ptr(), ws.data_ptr(), ws_bytes,
+                                         _stream_ptr(dev)))
+        _lib.check_workspace_status(ws, "stem_4d backward")
+
+    @staticmethod
     def jvp(ctx, t_slices, t_modes, t_weights, t_positions, *rest):
         # under torch.func the rule sees functorch wrappers; the kernels need storage
         slices, modes, weights, positions, windows = (_plain(t) for t in ctx.saved_tensors)
         t_slices, t_modes, t_weights, t_positions = (_plain(t) for t in (t_slices, t_modes, t_weights, t_positions))
         slice_thickness, voltage_kv, calib_ang, shift_calib_ang, k, batch, tune, n, f, record = ctx.cfg
+        if ctx.any_grid:
+            raise NotImplementedError("forward-mode derivatives need a square grid with a power-of-two edge")
         # torch.func.jvp hands zero tangents to the inputs it does not differentiate
         if t_positions is not None and bool(t_positions.any()):
             raise NotImplementedError("stem_4d has no forward-mode derivative with respect to positions")
@@ -243,6 +300,8 @@ def jvp(slices, modes, weights, positions, tangent_slices, tangent_modes, slice_
     lib = _lib.load()
     dev = slices.device
     S, M, P = slices.shape[2], modes.shape[2], positions.shape[0]
+    if not engine_grid(modes.shape[0], modes.shape[1]):
+        raise NotImplementedError("forward-mode derivatives need a square grid with a power-of-two edge")
     n, f = check_windows(slices, modes, windows, P)
     sc = float(calib_ang if shift_calib_ang is None else shift_calib_ang)
     prm = ms_params(n, S, M, P, voltage_kv, slice_thickness, calib_ang, sc, slices.stride(), modes.stride(), batch,
@@ -267,9 +326,27 @@ def vjp(slices, modes, weights, positions, grad_patterns, slice_thickness, volta
     lib = _lib.load()
     dev = slices.device
     S, M, P = slices.shape[2], modes.shape[2], positions.shape[0]
+    sc = float(calib_ang if shift_calib_ang is None else shift_calib_ang)
+    if not engine_grid(modes.shape[0], modes.shape[1]):
+        h, w = check_any_grid(slices, modes, windows)
+        prm = any_grid_params(slices, modes, P, voltage_kv, slice_thickness, calib_ang, sc, batch)
+        res = torch.empty(max(1, lib.ptyro_gm_residual_bytes(ctypes.byref(prm), h, w) // 4), dtype=torch.float32,
+                          device=dev)
+        status = _lib.new_status(dev)
+        out = run_forward_any(slices, slice_thickness, modes, weights, positions, voltage_kv, calib_ang, sc,
+                              batch=batch, status=status, residuals=res)
+        _lib.check_status(status, "vjp forward")
+        g_slices = torch.empty_strided(slices.shape, slices.stride(), dtype=torch.float32, device=dev)
+        g_modes = torch.empty_strided(modes.shape, modes.stride(), dtype=torch.complex64, device=dev)
+        if P == 0:
+            g_slices.zero_()
+            g_modes.zero_()
+        else:
+            Stem4dFunction._adjoint_any(lib, slices, modes, weights, positions, res, grad_patterns, slice_thickness,
+                                        voltage_kv, calib_ang, sc, batch, g_slices, g_modes, None)
+        return out, g_slices, g_modes
     n, f = check_windows(slices, modes, windows, P)
     k = _ckpt_for(S, ckpt_every, n, P * M)
-    sc = float(calib_ang if shift_calib_ang is None else shift_calib_ang)
     prm = ms_params(n, S, M, P, voltage_kv, slice_thickness, calib_ang, sc, slices.stride(), modes.stride(), batch,
                     default_tune(n) if tune is None else int(tune), f, windows)
     out = torch.empty((P, n, n), dtype=torch.float32, device=dev)
@@ -326,11 +403,15 @@ def make_probe_differentiable(voltage_kv: float, aperture_mrad: float, probe_sha
     """
     dev = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
     h, w = int(probe_shape[0]), int(probe_shape[1])
-    n = _check_edge(h, w)
+    if not engine_grid(h, w) and not (1 <= h <= 4096 and 1 <= w <= 4096):
+        raise ValueError(f"probe_shape must be in [1, 4096]^2, got ({h}, {w})")
     lam = relativistic_wavelength_ang(voltage_kv)
-    fov = n * 0.01 * float(probe_calibration_pm)
-    f = torch.fft.fftfreq(n, d=1.0 / n, dtype=torch.float64, device=dev) / fov
-    ly, lx = torch.meshgrid(f, f, indexing="ij")
+
+    def axis(m: int) -> torch.Tensor:
+        # the reference's grid: arange(-m/2, m/2) rolled by m // 2, over the field of view
+        a = torch.arange(m, dtype=torch.float64, device=dev) - m / 2.0
+        return torch.roll(a, m // 2) / (m * 0.01 * float(probe_calibration_pm))
+    ly, lx = torch.meshgrid(axis(h), axis(w), indexing="ij")
     q = torch.sqrt(lx * lx + ly * ly)
     mask = (q <= (aperture_mrad / 1000.0) / lam).to(torch.float64)
     p = lam * q
@@ -344,4 +425,4 @@ def make_probe_differentiable(voltage_kv: float, aperture_mrad: float, probe_sha
     chi = 2 * math.pi * chi / lam
     a = torch.polar(mask, -chi).to(torch.complex64)
     probe = _Fft2Fn.apply(a, True)
-    return torch.roll(probe, shifts=(n // 2, n // 2), dims=(0, 1))
+    return torch.roll(probe, shifts=(-(h // 2), -(w // 2)), dims=(0, 1))  # ifftshift

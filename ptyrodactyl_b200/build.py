@@ -15,8 +15,8 @@ PKG = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 LIB = os.path.join(PKG, "libptyro_b200.so")
-SOURCES = ["ms_engine.cu", "diag.cu", "ms_static.cu", "ms_sched.cu", "atoms.cu", "ms_jvp.cu", "ms_resident.cu", "elements.cu"] + [f"pass_{n}.cu" for n in (16, 32, 64, 128, 256, 512, 1024)]
-HEADERS = ["fft_core.cuh", "unit_consts.cuh", "ms_pass.cuh", "ms_pair.cuh", "ms_half.cuh", "ms_bwd.cuh",
+SOURCES = ["ms_engine.cu", "diag.cu", "ms_static.cu", "ms_sched.cu", "atoms.cu", "ms_jvp.cu", "ms_resident.cu", "elements.cu", "ms_generic.cu"] + [f"pass_{n}.cu" for n in (16, 32, 64, 128, 256, 512, 1024)]
+HEADERS = ["fft_core.cuh", "unit_consts.cuh", "ms_pass.cuh", "ms_pair.cuh", "ms_half.cuh", "ms_bwd.cuh", "ms_bwd_lam.cuh",
            "ms_jvp.cuh", "ms_pipe.cuh", "ms_wait.cuh", "ms_resident.cuh", "pass_launch.cuh", "engine.cuh"]
 
 NVCC_FLAGS = [

@@ -1002,38 +1002,9 @@ static size_t weight_grad_workspace_bytes(int num_modes) {
   return align_up(sizeof(double) * (size_t)kWeightGradBlocks * (size_t)num_modes);
 }
 
-static __global__ void __launch_bounds__(256) k_weight_grad_part(const float2* __restrict__ res,
-                                                                const float* __restrict__ g, int P, int M, int n,
-                                                                size_t slot_stride, size_t amp_off,
-                                                                double* __restrict__ part) {
-  __shared__ double red[8];
-  const int m = blockIdx.y;
-  const size_t nn = (size_t)n * n, total = (size_t)P * nn;
-  double acc = 0.0;
-  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
-    const size_t pr = i / nn, px = i % nn;
-    const int ky = (int)(px / n), kx = (int)(px % n);
-    const float2 a = res[((size_t)pr * M + m) * slot_stride + amp_off + px];
-    const float gv = g[pr * nn + (size_t)((ky + n / 2) % n) * n + (kx + n / 2) % n];
-    acc += (double)gv * ((double)a.x * a.x + (double)a.y * a.y);
-  }
-  for (int o = 16; o >= 1; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double s = 0.0;
-    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += red[w];
-    part[(size_t)m * gridDim.x + blockIdx.x] = s;
-  }
-}
-
-static __global__ void k_weight_grad_final(const double* __restrict__ part, int blocks, int M, double* out) {
-  const int m = blockIdx.x * blockDim.x + threadIdx.x;
-  if (m >= M) return;
-  double s = 0.0;
-  for (int b = 0; b < blocks; ++b) s += part[(size_t)m * blocks + b];
-  out[m] = s;
-}
+// the reduction itself (ms_generic.cu), for any H x W: sum_p sum_k g_p(fftshift k) |A_pm(k)|^2
+int weight_grad_hw(int P, int M, int H, int W, size_t slot_stride, size_t amp_off, const float2* res, const float* g,
+                   double* out, double* part, int blocks, cudaStream_t st);
 
 static int weight_grad(const ptyro_ms_params* p, int ckpt_every, const float2* residuals, const float* g,
                        double* out, double* part, cudaStream_t st) {
@@ -1044,10 +1015,9 @@ static int weight_grad(const ptyro_ms_params* p, int ckpt_every, const float2* r
     const cudaError_t e = cudaMemsetAsync(out, 0, sizeof(double) * (size_t)M, st);
     return e == cudaSuccess ? PTYRO_OK : fail(PTYRO_ERR_CUDA, cudaGetErrorString(e));
   }
-  k_weight_grad_part<<<dim3(kWeightGradBlocks, M), 256, 0, st>>>(residuals, g, P, M, n, (size_t)(C + 1) * nn,
-                                                                (size_t)C * nn, part);
-  k_weight_grad_final<<<(M + 63) / 64, 64, 0, st>>>(part, kWeightGradBlocks, M, out);
-  return check_launch("mode-weight gradient", 2);
+  const int rc = weight_grad_hw(P, M, n, n, (size_t)(C + 1) * nn, (size_t)C * nn, residuals, g, out, part,
+                                kWeightGradBlocks, st);
+  return rc ? fail(rc, "mode-weight gradient: launch failed") : PTYRO_OK;
 }
 
 static int launch_reduce_dv_any(const ptyro_ms_params* p, const float* contrib, int nb, int b0, float* dv, int s,

@@ -80,6 +80,66 @@ def _check_edge(h: int, w: int) -> int:
     return h
 
 
+ANY_GRID_MAX = 4096  # height and width limit of the any-size path
+
+
+def engine_grid(h: int, w: int) -> bool:
+    """True for the pass engine's square power-of-two grids; every other height x
+    width in [1, 4096] runs the any-size path (ptyro_gm_*)."""
+    return int(h) == int(w) and int(h) in SUPPORTED_EDGES
+
+
+def check_any_grid(slices: torch.Tensor, modes: torch.Tensor, windows: Optional[torch.Tensor] = None):
+    """(H, W) of an any-size forward: the potential covers the beam's grid exactly."""
+    h, w = int(modes.shape[0]), int(modes.shape[1])
+    if not (1 <= h <= ANY_GRID_MAX and 1 <= w <= ANY_GRID_MAX):
+        raise ValueError(f"grid height and width must be in [1, {ANY_GRID_MAX}], got ({h}, {w})")
+    if windows is not None:
+        raise ValueError(f"potential-field windows need a square grid with edge in {SUPPORTED_EDGES}, got ({h}, {w})")
+    if tuple(slices.shape[:2]) != (h, w):
+        raise ValueError(f"potential slices {tuple(slices.shape[:2])} must cover the beam grid ({h}, {w})")
+    return h, w
+
+
+def any_grid_params(slices: torch.Tensor, modes: torch.Tensor, num_probes: int, voltage_kv: float,
+                    slice_thickness: float, calib_ang: float, shift_calib_ang: float, batch: int = 0,
+                    accumulate: bool = False) -> _lib.MsParams:
+    return ms_params(0, slices.shape[2], modes.shape[2], num_probes, voltage_kv, slice_thickness, calib_ang,
+                     shift_calib_ang, slices.stride(), modes.stride(), batch, 0, 0, None,
+                     _lib.PTYRO_FLAG_ACCUMULATE if accumulate else 0)
+
+
+def run_forward_any(slices: torch.Tensor, slice_thickness: float, modes: torch.Tensor, weights: torch.Tensor,
+                    positions: torch.Tensor, voltage_kv: float, calib_ang: float, shift_calib_ang: float,
+                    out: Optional[torch.Tensor] = None, batch: int = 0, accumulate: bool = False,
+                    status: Optional[torch.Tensor] = None, residuals: Optional[torch.Tensor] = None,
+                    windows: Optional[torch.Tensor] = None) -> torch.Tensor:
+    """``run_forward`` on any height x width grid (ptyro_gm_forward): the potential
+    covers the beam's grid, no windows. ``residuals`` (ptyro_gm_residual_bytes) keeps
+    the waves the any-size adjoint reads."""
+    lib = _lib.load()
+    dev = slices.device
+    h, w = check_any_grid(slices, modes, windows)
+    num_probes = positions.shape[0]
+    prm = any_grid_params(slices, modes, num_probes, voltage_kv, slice_thickness, calib_ang, shift_calib_ang,
+                          batch, accumulate)
+    if out is None:
+        out = (torch.zeros if accumulate else torch.empty)((num_probes, h, w), dtype=torch.float32, device=dev)
+    if num_probes == 0:
+        return out
+    ws_bytes = lib.ptyro_gm_workspace_bytes(ctypes.byref(prm), h, w)
+    if ws_bytes == 0:
+        _lib.check(_lib.PTYRO_ERR_INVALID)
+    ws = _workspace(ws_bytes, dev)
+    with torch.cuda.device(dev):
+        rc = lib.ptyro_gm_forward(ctypes.byref(prm), h, w, slices.data_ptr(), modes.data_ptr(), weights.data_ptr(),
+                                  positions.data_ptr(), out.data_ptr(), _ptr(residuals), ws.data_ptr(), ws_bytes,
+                                  _stream_ptr(dev))
+    _lib.check(rc)
+    _lib.gather_status(status, ws)
+    return out
+
+
 def _workspace(nbytes: int, device: torch.device) -> torch.Tensor:
     # torch's caching allocator hands out 512-byte aligned blocks
     return torch.empty(max(int(nbytes), 256), dtype=torch.uint8, device=device)
@@ -169,6 +229,10 @@ def run_forward(slices: torch.Tensor, slice_thickness: float, modes: torch.Tenso
     device status bits asynchronously; nothing here synchronises, so the caller checks
     it (``_lib.check_status``) once it needs the results.
     """
+    if not engine_grid(modes.shape[0], modes.shape[1]):
+        return run_forward_any(slices, slice_thickness, modes, weights, positions, voltage_kv, calib_ang,
+                               shift_calib_ang, out=out, batch=batch, accumulate=accumulate, status=status,
+                               windows=windows)
     lib = _lib.load()
     dev = slices.device
     num_probes = positions.shape[0]
@@ -230,12 +294,21 @@ def run_forward_to_host(slices: torch.Tensor, slice_thickness: float, modes: tor
     range is done, so the device-to-host transfer overlaps the remaining compute."""
     dev = slices.device
     num_probes = positions.shape[0]
-    n, _ = check_windows(slices, modes, windows, num_probes)
-    if tuple(host_out.shape) != (num_probes, n, n) or host_out.dtype != torch.float32:
-        raise ValueError(f"host_out must be a float32 tensor of shape {(num_probes, n, n)}")
+    any_grid = not engine_grid(modes.shape[0], modes.shape[1])
+    if any_grid:
+        h, w = check_any_grid(slices, modes, windows)
+    else:
+        h, _ = check_windows(slices, modes, windows, num_probes)
+        w = h
+    if tuple(host_out.shape) != (num_probes, h, w) or host_out.dtype != torch.float32:
+        raise ValueError(f"host_out must be a float32 tensor of shape {(num_probes, h, w)}")
     if num_probes == 0:
         return host_out
-    dev_out = torch.empty((num_probes, n, n), dtype=torch.float32, device=dev)
+    if any_grid:  # one forward, then one copy
+        host_out.copy_(run_forward_any(slices, slice_thickness, modes, weights, positions, voltage_kv, calib_ang,
+                                       shift_calib_ang, status=status), non_blocking=True)
+        return host_out
+    dev_out = torch.empty((num_probes, h, w), dtype=torch.float32, device=dev)
     main = torch.cuda.current_stream(dev)
     streams = _side_streams(dev, max(1, lanes))
     copy = _side_streams(dev, 1 + max(1, lanes))[-1]
@@ -477,8 +550,21 @@ def cbed_amplitude(pot_slices: PotentialSlices, beam: ProbeModes, microscope: Mi
         slices = slices[..., None]
     modes, _ = _beam_on(beam, dev)
     calib = min(float(pot_slices.calib), float(beam.calib))
-    n, f = check_windows(slices, modes, None, 1)
     zero = torch.zeros((1, 2), dtype=torch.float64, device=dev)
+    if not engine_grid(modes.shape[0], modes.shape[1]):
+        # the far-field amplitude planes of the any-size forward's residuals, fftshifted
+        h, w = check_any_grid(slices, modes)
+        S, M = slices.shape[2], modes.shape[2]
+        prm = any_grid_params(slices, modes, 1, microscope.voltage_kv, pot_slices.slice_thickness, calib, calib)
+        res = torch.empty(lib.ptyro_gm_residual_bytes(ctypes.byref(prm), h, w) // 8, dtype=torch.complex64,
+                          device=dev)
+        status = _lib.new_status(dev)
+        run_forward_any(slices, pot_slices.slice_thickness, modes, torch.ones(M, dtype=torch.float32, device=dev),
+                        zero, microscope.voltage_kv, calib, calib, status=status, residuals=res)
+        _lib.check_status(status, "cbed_amplitude")
+        amps = res.view(M, S + 1, h, w)[:, S]
+        return torch.roll(amps, shifts=(h // 2, w // 2), dims=(1, 2)).permute(1, 2, 0)
+    n, f = check_windows(slices, modes, None, 1)
     prm = ms_params(n, slices.shape[2], modes.shape[2], 1, microscope.voltage_kv, pot_slices.slice_thickness, calib,
                     calib, slices.stride(), modes.stride(), 0, 0, f)
     amps = torch.empty((1, modes.shape[2], n, n), dtype=torch.complex64, device=dev)
@@ -494,10 +580,23 @@ def make_probe(microscope: MicroscopeConfig, detector: DetectorConfig) -> torch.
     complex64 (H, W) CUDA tensor, centred at (H/2, W/2), unnormalised."""
     if microscope.probe_shape is None:
         raise ValueError("microscope.probe_shape is required")
-    h, w = microscope.probe_shape
-    n = _check_edge(h, w)
+    h, w = (int(v) for v in microscope.probe_shape)
     lib = _lib.load()
     dev = _device()
+    if not engine_grid(h, w):
+        if not (1 <= h <= ANY_GRID_MAX and 1 <= w <= ANY_GRID_MAX):
+            raise ValueError(f"probe_shape must be in [1, {ANY_GRID_MAX}]^2, got ({h}, {w})")
+        probe = torch.empty((h, w), dtype=torch.complex64, device=dev)
+        ws_bytes = lib.ptyro_gm_make_probe_workspace_bytes(h, w)
+        ws = _workspace(ws_bytes, dev)
+        with torch.cuda.device(dev):
+            rc = lib.ptyro_gm_make_probe(h, w, microscope.voltage_kv, microscope.aperture_mrad,
+                                         detector.probe_calibration_pm, microscope.defocus_ang, microscope.c3_ang,
+                                         microscope.c5_ang, probe.data_ptr(), ws.data_ptr(), ws_bytes,
+                                         _stream_ptr(dev))
+        _lib.check(rc)
+        return probe
+    n = h
     probe = torch.empty((n, n), dtype=torch.complex64, device=dev)
     ws_bytes = lib.ptyro_fft_workspace_bytes(n)
     ws = _workspace(ws_bytes, dev)
@@ -513,6 +612,17 @@ def fft2(x: torch.Tensor, inverse: bool = False) -> torch.Tensor:
     lib = _lib.load()
     dev = _device(x.device if x.is_cuda else None)
     y = as_tensor(x, torch.complex64, dev).contiguous().clone()
+    if not engine_grid(y.shape[-2], y.shape[-1]):
+        h, w = int(y.shape[-2]), int(y.shape[-1])
+        ws_bytes = lib.ptyro_gm_fft_workspace_bytes(h, w)
+        if ws_bytes == 0:
+            raise ValueError(f"fft2 height and width must be in [1, {ANY_GRID_MAX}], got ({h}, {w})")
+        ws = _workspace(ws_bytes, dev)
+        with torch.cuda.device(dev):
+            rc = lib.ptyro_gm_fft2(h, w, y.numel() // (h * w) if h * w else 0, 1 if inverse else 0, y.data_ptr(),
+                                   ws.data_ptr(), ws_bytes, _stream_ptr(dev))
+        _lib.check(rc)
+        return y
     n = _check_edge(y.shape[-2], y.shape[-1])
     count = y.numel() // (n * n)
     ws_bytes = lib.ptyro_fft_workspace_bytes(n)

@@ -154,3 +154,60 @@ def test_device_status_host_logic():
         _lib.check_status(st, "failed")
     with pytest.raises(_lib.DeviceStatusError):
         _lib.check_workspace_status(ws, "failed")
+
+
+def test_any_size_entry_points_validate_before_launch(lib):
+    p = _p(n=0, num_probes=4, num_modes=2, num_slices=3)
+    ws = lib.ptyro_gm_workspace_bytes(ctypes.byref(p), 45, 77)
+    assert ws > 0
+    assert lib.ptyro_gm_backward_workspace_bytes(ctypes.byref(p), 45, 77) > ws  # plus the beam sum
+    assert lib.ptyro_gm_residual_bytes(ctypes.byref(p), 45, 77) == 8 * 45 * 77 * 4 * 2 * 4
+    for h, w in ((0, 77), (45, 0), (4097, 3), (3, 4097)):
+        assert lib.ptyro_gm_workspace_bytes(ctypes.byref(p), h, w) == 0
+    rc = lib.ptyro_gm_forward(ctypes.byref(p), 45, 77, None, None, None, None, None, None, None, 0, None)
+    assert rc == _lib.PTYRO_ERR_INVALID and "NULL" in lib.ptyro_last_error().decode()
+    buf = ctypes.create_string_buffer(64)
+    fake = ctypes.addressof(buf)
+    rc = lib.ptyro_gm_forward(ctypes.byref(p), 45, 77, fake, fake, fake, fake, fake, None, None, 0, None)
+    assert rc == _lib.PTYRO_ERR_WORKSPACE
+    p.windows = fake
+    rc = lib.ptyro_gm_forward(ctypes.byref(p), 45, 77, fake, fake, fake, fake, fake, None, None, 0, None)
+    assert rc == _lib.PTYRO_ERR_UNSUPPORTED and "windows" in lib.ptyro_last_error().decode()
+    p.windows = None
+    assert lib.ptyro_gm_forward(ctypes.byref(_p(n=0, num_probes=0)), 45, 77, None, None, None, None, None, None,
+                                None, 0, None) == 0
+    rc = lib.ptyro_gm_backward(ctypes.byref(p), 45, 77, None, None, None, None, None, None, None, None, None,
+                               None, 0, None)
+    assert rc == _lib.PTYRO_ERR_INVALID
+    rc = lib.ptyro_gm_weight_grad(ctypes.byref(p), 45, 77, None, None, None, None, 0, None)
+    assert rc == _lib.PTYRO_ERR_INVALID
+
+
+def test_any_size_transforms_and_probe_validate(lib):
+    assert lib.ptyro_gm_fft_workspace_bytes(45, 77) > 0
+    assert lib.ptyro_gm_fft_workspace_bytes(0, 77) == 0
+    assert lib.ptyro_gm_fft2(4097, 3, 1, 0, None, None, 0, None) == _lib.PTYRO_ERR_INVALID
+    assert lib.ptyro_gm_fft2(5, 3, -1, 0, None, None, 0, None) == _lib.PTYRO_ERR_INVALID
+    assert lib.ptyro_gm_fft2(5, 3, 0, 0, None, None, 0, None) == 0  # nothing to transform
+    assert lib.ptyro_gm_make_probe_workspace_bytes(7, 5) > 0
+    rc = lib.ptyro_gm_make_probe(7, 5, -1.0, 25.0, 30.0, 0.0, 0.0, 0.0, None, None, 0, None)
+    assert rc == _lib.PTYRO_ERR_INVALID and "voltage" in lib.ptyro_last_error().decode()
+    rc = lib.ptyro_gm_make_probe(7, 5, 200.0, 25.0, 30.0, float("inf"), 0.0, 0.0, None, None, 0, None)
+    assert rc == _lib.PTYRO_ERR_INVALID
+
+
+def test_any_size_routing_host_logic():
+    import torch
+
+    from ptyrodactyl_b200.simulations import check_any_grid, engine_grid
+    assert engine_grid(64, 64) and engine_grid(1024, 1024)
+    for h, w in ((64, 128), (4, 4), (100, 100), (2048, 2048), (45, 77)):
+        assert not engine_grid(h, w)
+    sl, md = torch.zeros(45, 77, 2), torch.zeros(45, 77, 1, dtype=torch.complex64)
+    assert check_any_grid(sl, md) == (45, 77)
+    with pytest.raises(ValueError, match="windows"):
+        check_any_grid(sl, md, torch.zeros(1, 2, dtype=torch.int32))
+    with pytest.raises(ValueError, match="cover the beam grid"):
+        check_any_grid(torch.zeros(45, 78, 2), md)
+    with pytest.raises(ValueError, match="4096"):
+        check_any_grid(torch.zeros(5000, 3, 1), torch.zeros(5000, 3, 1, dtype=torch.complex64))

@@ -93,13 +93,28 @@ def test_unknown_optimizer_and_loss():
         MR.multi_slice_multi_modal(s4, pot0, beam0, 2.0, num_iterations=1, loss_type="huber")
 
 
+# The reference's pinned values after two Adam steps on its 4 x 4 grid
+# (tests/test_ptyrodactyl/test_multislice/test_multislice_recon.py:185-285):
+# potential[0, 0], beam (mode 0)[0, 0], position[0, 0].
+PINS = {
+    "single_slice_ptychography": (0.02866302842954916, -1.4996974690426799 - 1.4814616332191217j, None),
+    "single_slice_poscorrected": (0.02866303668627853, -1.4996974690390232 - 1.4814616332263657j,
+                                  0.002001176434824531),
+    "single_slice_multi_modal": (0.0286630285066058, -1.4996968965393802 - 1.481462648068354j, 0.0020011719351587594),
+    "multi_slice_multi_modal": (0.028663098749764054, -1.4996974690074887 - 1.4814616332889121j, 0.02000915293273863),
+}
+
+
+@pytest.mark.parametrize("n", [4, 16])
 @pytest.mark.parametrize("fn", ["single_slice_ptychography", "single_slice_poscorrected", "single_slice_multi_modal",
                                 "multi_slice_multi_modal"])
-def test_engine_loops_match_the_pinned_oracle_loop(fn):
+def test_engine_loops_match_the_pinned_oracle_loop(fn, n):
     """The setting of the reference's pinned regressions (PRNGKey(11) draws, two
     positions, 80 kV, unit calibration, two Adam steps at lr 0.001; the oracle's loop
     reproduces those pins on the reference's 4 x 4 grid, tests/test_oracle_recon_pins.py)
-    on the engine's smallest grid, 16 x 16, against the same float64 oracle loop.
+    against the same float64 oracle loop: on the reference's own 4 x 4 grid (the
+    any-size path), where the reference's pinned scalars are checked as well, and on
+    the pass engine's smallest grid, 16 x 16.
     Adam's first steps are lr * sign(g) up to 1e-8, so float32 gradients give the same
     iterates to float32 rounding unless a gradient sits at noise level. That is the
     case for the scan positions here: the object is nearly transparent (|T - 1| ~ 1e-5),
@@ -110,7 +125,6 @@ def test_engine_loops_match_the_pinned_oracle_loop(fn):
     direction is two steps off); well-conditioned position gradients are checked
     against the oracle at 1e-4 in test_gpu_grad.py."""
     from oracle.jax_prng import normal_f64, prng_key, split
-    n = 16
     keys = split(prng_key(11), 5)
     pot = (normal_f64(keys[0], (n, n)) * 0.01).astype(np.complex128)
     beam = normal_f64(keys[1], (n, n)) + 1j * normal_f64(keys[2], (n, n))
@@ -144,3 +158,9 @@ def test_engine_loops_match_the_pinned_oracle_loop(fn):
     assert rel_l2(got[1].cpu().numpy(), want["modes"]) < 1e-5
     if got[2] is not None:
         assert np.abs(got[2].cpu().numpy() - want["pos"]).max() < 0.25 * lr_pos
+    if n == 4:
+        pin_pot, pin_beam, pin_pos = PINS[fn]
+        assert abs(complex(got[0][0, 0].item()) - pin_pot) <= 1e-5 * abs(pin_pot)
+        assert abs(complex(got[1][0, 0, 0].item()) - pin_beam) <= 1e-5 * abs(pin_beam)
+        if pin_pos is not None:
+            assert abs(float(got[2][0, 0]) - pin_pos) < 0.25 * lr_pos
