@@ -468,6 +468,26 @@ int ptyro_sched_release(ptyro_sched* s, int64_t id);
 /* Free arena bytes and free wave slots. */
 int ptyro_sched_memory(ptyro_sched* s, size_t* free_bytes, int32_t* free_slots);
 
+/* Recorded batch plans: a fixed set of jobs (any mix of grid edges, slice counts,
+ * scan sizes, forward and gradient; no ready events) run as the scheduler runs them,
+ * every job advancing one pass per tick in the same multi-job launches, but
+ * recorded once. ptyro_plan_create simulates the ticks on the host and copies every
+ * tick's descriptors into the arena (a synchronous copy: call it outside stream
+ * capture); ptyro_plan_launch then only enqueues kernels and memsets on `stream`,
+ * so it can be captured into a CUDA graph and replayed; each launch recomputes every
+ * job from its current inputs. Results are bit-identical to the same jobs run
+ * through ptyro_sched_*. The arena (DEVICE, 256-byte aligned, ptyro_plan_bytes)
+ * holds every job's scratch at once; one launch at a time per plan. */
+typedef struct ptyro_plan ptyro_plan;
+size_t ptyro_plan_bytes(const ptyro_job_desc* jobs, int32_t num_jobs);
+int ptyro_plan_create(int32_t device, const ptyro_job_desc* jobs, int32_t num_jobs, void* arena, size_t arena_bytes,
+                      ptyro_plan** out);
+int ptyro_plan_launch(ptyro_plan* plan, void* stream);
+/* Device address of job `job`'s status word (uint32, PTYRO_STATUS_* bits; cleared by
+ * every launch of the plan). */
+int ptyro_plan_job_status(const ptyro_plan* plan, int32_t job, void** status_word);
+int ptyro_plan_destroy(ptyro_plan* plan);
+
 /* Bytes of the fixed device scratch array behind ptyro_ms_forward_noalloc. */
 #define PTYRO_STATIC_SCRATCH_BYTES (64u * 1024u * 1024u)
 

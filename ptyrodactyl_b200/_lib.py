@@ -65,6 +65,11 @@ EXPORTED_SYMBOLS = (
     "ptyro_sched_job_state",
     "ptyro_sched_release",
     "ptyro_sched_memory",
+    "ptyro_plan_bytes",
+    "ptyro_plan_create",
+    "ptyro_plan_launch",
+    "ptyro_plan_job_status",
+    "ptyro_plan_destroy",
     "ptyro_atom_slices_workspace_bytes",
     "ptyro_atom_slices",
     "ptyro_atom_potential",
@@ -202,6 +207,16 @@ def _declare(lib) -> None:
     lib.ptyro_sched_release.argtypes = [vp, ctypes.c_int64]
     lib.ptyro_sched_memory.restype = ctypes.c_int
     lib.ptyro_sched_memory.argtypes = [vp, ctypes.POINTER(sz), ctypes.POINTER(i32)]
+    lib.ptyro_plan_bytes.restype = sz
+    lib.ptyro_plan_bytes.argtypes = [jd, i32]
+    lib.ptyro_plan_create.restype = ctypes.c_int
+    lib.ptyro_plan_create.argtypes = [i32, jd, i32, vp, sz, ctypes.POINTER(vp)]
+    lib.ptyro_plan_launch.restype = ctypes.c_int
+    lib.ptyro_plan_launch.argtypes = [vp, vp]
+    lib.ptyro_plan_job_status.restype = ctypes.c_int
+    lib.ptyro_plan_job_status.argtypes = [vp, i32, ctypes.POINTER(vp)]
+    lib.ptyro_plan_destroy.restype = ctypes.c_int
+    lib.ptyro_plan_destroy.argtypes = [vp]
     i64 = ctypes.c_int64
     lib.ptyro_ms_detect_workspace_bytes.restype = sz
     lib.ptyro_ms_detect_workspace_bytes.argtypes = [pp, i32]

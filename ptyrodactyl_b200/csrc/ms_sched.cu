@@ -291,32 +291,46 @@ static BwdBuffers job_bwd_buffers(Job& j) {
   return b;
 }
 
-static int admit(ptyro_sched* s, Job& j, GridClass& c) {
+// the job's status word cleared, its tables and probe spectra built, gradient sums zeroed
+static int job_setup(Job& j, cudaStream_t st) {
   const ptyro_ms_params* p = &j.plan.p;
   int rc;
-  if (j.d.ready_event && cudaStreamWaitEvent(c.stream, (cudaEvent_t)j.d.ready_event, 0) != cudaSuccess)
-    return fail(PTYRO_ERR_CUDA, "cudaStreamWaitEvent on the job's ready event failed");
-  if ((rc = forward_setup(p, j.plan.L, j.base + j.plan.off_fwd, j.d.potential, j.d.modes, c.stream))) return rc;
+  if ((rc = clear_status(j.base + j.plan.off_fwd + j.plan.L.status, st))) return rc;
+  if ((rc = forward_setup(p, j.plan.L, j.base + j.plan.off_fwd, j.d.potential, j.d.modes, st))) return rc;
   if (j.plan.grad) {
     const int F = field_of(p);
     const size_t nn = (size_t)p->n * p->n;
-    k_zero_pot<<<blocks_for((size_t)F * F * p->num_slices, 256), 256, 0, c.stream>>>(
+    k_zero_pot<<<blocks_for((size_t)F * F * p->num_slices, 256), 256, 0, st>>>(
         j.d.grad_potential, p->pot_stride_y, p->pot_stride_x, p->pot_stride_s, F, p->num_slices);
-    k_zero2<<<blocks_for(nn * p->num_modes, 256), 256, 0, c.stream>>>((float2*)(j.base + j.plan.off_beam),
-                                                                       nn * p->num_modes);
+    k_zero2<<<blocks_for(nn * p->num_modes, 256), 256, 0, st>>>((float2*)(j.base + j.plan.off_beam),
+                                                                 nn * p->num_modes);
     if ((rc = check_launch("gradient job setup", 2))) return rc;
   }
-  j.state = PTYRO_JOB_RUNNING;
-  j.phase = 0;
-  j.b0 = 0;
-  j.nb = std::min(j.plan.L.batch, p->num_probes);
-  j.k = 0;
-  if (p->num_probes == 0) j.issued_all = true;
   return PTYRO_OK;
 }
 
-// the last kernels of a job, then its completion event
-static int finish_job(Job& j, GridClass& c) {
+// the pass counters of a job that starts
+static void job_start(Job& j) {
+  j.state = PTYRO_JOB_RUNNING;
+  j.phase = 0;
+  j.b0 = 0;
+  j.nb = std::min(j.plan.L.batch, j.plan.p.num_probes);
+  j.k = 0;
+  if (j.plan.p.num_probes == 0) j.issued_all = true;
+}
+
+static int admit(ptyro_sched* s, Job& j, GridClass& c) {
+  (void)s;
+  int rc;
+  if (j.d.ready_event && cudaStreamWaitEvent(c.stream, (cudaEvent_t)j.d.ready_event, 0) != cudaSuccess)
+    return fail(PTYRO_ERR_CUDA, "cudaStreamWaitEvent on the job's ready event failed");
+  if ((rc = job_setup(j, c.stream))) return rc;
+  job_start(j);
+  return PTYRO_OK;
+}
+
+// the last kernels of a job (gradient jobs: the probe gradient and the loss)
+static int job_epilogue(Job& j, cudaStream_t st) {
   const ptyro_ms_params* p = &j.plan.p;
   int rc = PTYRO_OK;
   if (j.plan.grad && p->num_probes > 0) {
@@ -324,12 +338,19 @@ static int finish_job(Job& j, GridClass& c) {
     const int n = p->n, M = p->num_modes;
     const size_t nn = (size_t)n * n;
     float2* beam = (float2*)(j.base + j.plan.off_beam);
-    if ((rc = fft2_planes(n, M, true, beam, f.tw, c.stream))) return rc;
-    k_write_grad_modes<<<(unsigned)((nn * M + 255) / 256), 256, 0, c.stream>>>(
+    if ((rc = fft2_planes(n, M, true, beam, f.tw, st))) return rc;
+    k_write_grad_modes<<<(unsigned)((nn * M + 255) / 256), 256, 0, st>>>(
         beam, n, M, (float2*)j.d.grad_modes, p->mode_stride_y, p->mode_stride_x, p->mode_stride_m);
-    k_sum_partials<<<1, 256, 0, c.stream>>>((const float*)(j.base + j.plan.off_lossp), p->num_probes, j.d.loss);
+    k_sum_partials<<<1, 256, 0, st>>>((const float*)(j.base + j.plan.off_lossp), p->num_probes, j.d.loss);
     if ((rc = check_launch("gradient job epilogue", 2))) return rc;
   }
+  return PTYRO_OK;
+}
+
+// the epilogue, then the job's completion event
+static int finish_job(Job& j, GridClass& c) {
+  int rc = job_epilogue(j, c.stream);
+  if (rc) return rc;
   if (cudaEventCreateWithFlags(&j.done, cudaEventDisableTiming) != cudaSuccess ||
       cudaEventRecord(j.done, c.stream) != cudaSuccess)
     return fail(PTYRO_ERR_CUDA, "cudaEventRecord failed");
@@ -345,27 +366,28 @@ struct TickRows {
   std::vector<int2> rows[6];
 };
 
-// one pass of every running job of grid class c
-static int tick_class(ptyro_sched* s, GridClass& c, std::vector<Job*>& jobs) {
-  TickRows t;
-  struct Follow {
-    Job* j;
-    int slice;
-    bool loss, beam;
-  };
-  std::vector<Follow> follow;
-  int rc;
+// the per-job kernels that follow a tick's multi-job launches
+struct Follow {
+  Job* j;
+  int b0, nb, slice;
+  bool loss, beam;
+};
+
+struct RampReq {
+  Job* j;
+  int b0, nb;
+};
+
+// One pass of every job in `jobs`: the descriptors and CTA rows of the multi-job
+// launches, the probe batches whose shift ramps must be built first, and the
+// follow-up kernels.
+static void build_tick(std::vector<Job*>& jobs, TickRows& t, std::vector<RampReq>& ramps,
+                       std::vector<Follow>& follow) {
   for (Job* j : jobs) {
     const ptyro_ms_params* p = &j->plan.p;
     const int S = p->num_slices;
-    if (j->k == 0 && j->phase == 0) {
-      const FwdBuffers f = job_fwd_buffers(*j);
-      k_ramps<<<(j->nb * p->n + 255) / 256, 256, 0, c.stream>>>(j->d.positions + 2 * (size_t)j->b0, j->nb, p->n,
-                                                                p->shift_calib_ang, (float2*)f.ramp_y,
-                                                                (float2*)f.ramp_x);
-      if ((rc = check_launch("k_ramps"))) return rc;
-    }
-    Follow fl{j, -1, false, false};
+    if (j->k == 0 && j->phase == 0) ramps.push_back({j, j->b0, j->nb});
+    Follow fl{j, j->b0, j->nb, -1, false, false};
     if (j->phase == 0) {
       float2* res = j->plan.grad ? (float2*)(j->base + j->plan.off_res) : nullptr;
       const FwdPlan f = fwd_pass_plan(p, job_fwd_buffers(*j), j->d.weights, j->d.patterns, res, j->plan.K,
@@ -390,71 +412,215 @@ static int tick_class(ptyro_sched* s, GridClass& c, std::vector<Job*>& jobs) {
     }
     follow.push_back(fl);
   }
-  // upload descriptors and rows through the staging ring
+}
+
+static int launch_ramps(const RampReq& r, cudaStream_t st) {
+  const ptyro_ms_params* p = &r.j->plan.p;
+  const FwdBuffers f = job_fwd_buffers(*r.j);
+  k_ramps<<<(r.nb * p->n + 255) / 256, 256, 0, st>>>(r.j->d.positions + 2 * (size_t)r.b0, r.nb, p->n,
+                                                      p->shift_calib_ang, (float2*)f.ramp_y, (float2*)f.ramp_x);
+  return check_launch("k_ramps");
+}
+
+// bytes of one tick's descriptors and row tables as laid out by pack_tick
+static size_t tick_bytes(const TickRows& t) {
   size_t bytes = align_up(t.fdesc.size() * sizeof(PassArgs)) + align_up(t.bdesc.size() * sizeof(BwdArgs));
   for (int i = 0; i < 6; ++i) bytes += align_up(t.rows[i].size() * sizeof(int2));
+  return bytes;
+}
+
+// the device addresses a tick's launches read, for a packed copy at `dptr`
+struct TickPtrs {
+  const PassArgs* fd;
+  const BwdArgs* bd;
+  const int2* rows[6];
+  int nrows[6];
+};
+
+static TickPtrs pack_tick(const TickRows& t, char* h, char* dptr) {
+  TickPtrs q;
+  size_t o = 0;
+  q.fd = (const PassArgs*)(dptr + o);
+  if (h) memcpy(h + o, t.fdesc.data(), t.fdesc.size() * sizeof(PassArgs));
+  o += align_up(t.fdesc.size() * sizeof(PassArgs));
+  q.bd = (const BwdArgs*)(dptr + o);
+  if (h) memcpy(h + o, t.bdesc.data(), t.bdesc.size() * sizeof(BwdArgs));
+  o += align_up(t.bdesc.size() * sizeof(BwdArgs));
+  for (int i = 0; i < 6; ++i) {
+    q.rows[i] = (const int2*)(dptr + o);
+    q.nrows[i] = (int)t.rows[i].size();
+    if (h) memcpy(h + o, t.rows[i].data(), t.rows[i].size() * sizeof(int2));
+    o += align_up(t.rows[i].size() * sizeof(int2));
+  }
+  return q;
+}
+
+static int launch_tick(int n, const TickPtrs& q, cudaStream_t st) {
+  const int tune = 3;
+  int rc;
+  if ((rc = launch_pass_multi(n, 0, q.fd, q.rows[0], q.nrows[0], st, tune))) return rc;
+  if ((rc = launch_pass_multi(n, 1, q.fd, q.rows[1], q.nrows[1], st, tune))) return rc;
+  if ((rc = launch_pass_pair_multi(n, 0, q.fd, q.rows[4], q.nrows[4], st))) return rc;
+  if ((rc = launch_pass_pair_multi(n, 1, q.fd, q.rows[5], q.nrows[5], st))) return rc;
+  if ((rc = launch_bwd_multi(n, 0, q.bd, q.rows[2], q.nrows[2], st))) return rc;
+  return launch_bwd_multi(n, 1, q.bd, q.rows[3], q.nrows[3], st);
+}
+
+static int launch_follow(const Follow& fl, cudaStream_t st) {
+  Job& j = *fl.j;
+  const ptyro_ms_params* p = &j.plan.p;
+  const int n = p->n, M = p->num_modes;
+  const size_t nn = (size_t)n * n;
+  int rc;
+  if (fl.loss) {
+    k_amp_loss<<<fl.nb, 256, 0, st>>>(j.d.patterns + (size_t)fl.b0 * nn, j.d.targets + (size_t)fl.b0 * nn, (int)nn,
+                                       kLossEps, (float*)(j.base + j.plan.off_g),
+                                       (float*)(j.base + j.plan.off_lossp) + fl.b0);
+    if ((rc = check_launch("k_amp_loss"))) return rc;
+  }
+  if (fl.slice >= 0 &&
+      (rc = launch_reduce_dv_any(p, (const float*)(j.base + j.plan.off_contrib), fl.nb, fl.b0, j.d.grad_potential,
+                                 fl.slice, st)))
+    return rc;
+  if (fl.beam) {
+    k_reduce_beam<<<(unsigned)((nn * M + 255) / 256), 256, 0, st>>>((const float2*)(j.base + j.plan.off_lam), fl.nb,
+                                                                     M, n, (float2*)(j.base + j.plan.off_beam));
+    if ((rc = check_launch("k_reduce_beam"))) return rc;
+  }
+  return PTYRO_OK;
+}
+
+// past one pass: returns true when the job has issued its last pass
+static bool job_advance(Job& j) {
+  const ptyro_ms_params* p = &j.plan.p;
+  if (++j.k <= p->num_slices + 1) return false;
+  j.k = 0;
+  if (j.phase == 0 && j.plan.grad) {
+    j.phase = 1;
+    return false;
+  }
+  j.phase = 0;
+  j.b0 += j.nb;
+  if (j.b0 >= p->num_probes) return true;
+  j.nb = std::min(j.plan.L.batch, p->num_probes - j.b0);
+  return false;
+}
+
+// one pass of every running job of grid class c
+static int tick_class(ptyro_sched* s, GridClass& c, std::vector<Job*>& jobs) {
+  TickRows t;
+  std::vector<RampReq> ramps;
+  std::vector<Follow> follow;
+  int rc;
+  build_tick(jobs, t, ramps, follow);
+  for (const RampReq& r : ramps)
+    if ((rc = launch_ramps(r, c.stream))) return rc;
+  // upload descriptors and rows through the staging ring
+  const size_t bytes = tick_bytes(t);
   if (bytes > s->stage_bytes) return fail(PTYRO_ERR_INVALID, "tick descriptors exceed the staging buffer");
   const int slot = c.next;
   c.next = (c.next + 1) % GridClass::kRing;
   cudaEventSynchronize(c.used[slot]);  // the copy that last used this slot has finished
-  char* h = c.host[slot];
-  char* dptr = c.dev[slot];
-  size_t o = 0;
-  const PassArgs* fd = (const PassArgs*)(dptr + o);
-  memcpy(h + o, t.fdesc.data(), t.fdesc.size() * sizeof(PassArgs));
-  o += align_up(t.fdesc.size() * sizeof(PassArgs));
-  const BwdArgs* bd = (const BwdArgs*)(dptr + o);
-  memcpy(h + o, t.bdesc.data(), t.bdesc.size() * sizeof(BwdArgs));
-  o += align_up(t.bdesc.size() * sizeof(BwdArgs));
-  const int2* rows[6];
-  for (int i = 0; i < 6; ++i) {
-    rows[i] = (const int2*)(dptr + o);
-    memcpy(h + o, t.rows[i].data(), t.rows[i].size() * sizeof(int2));
-    o += align_up(t.rows[i].size() * sizeof(int2));
-  }
-  if (cudaMemcpyAsync(dptr, h, o, cudaMemcpyHostToDevice, c.stream) != cudaSuccess)
+  const TickPtrs q = pack_tick(t, c.host[slot], c.dev[slot]);
+  if (cudaMemcpyAsync(c.dev[slot], c.host[slot], bytes, cudaMemcpyHostToDevice, c.stream) != cudaSuccess)
     return fail(PTYRO_ERR_CUDA, "descriptor upload failed");
   cudaEventRecord(c.used[slot], c.stream);
-  const int tune = 3;
-  if ((rc = launch_pass_multi(c.n, 0, fd, rows[0], (int)t.rows[0].size(), c.stream, tune))) return rc;
-  if ((rc = launch_pass_multi(c.n, 1, fd, rows[1], (int)t.rows[1].size(), c.stream, tune))) return rc;
-  if ((rc = launch_pass_pair_multi(c.n, 0, fd, rows[4], (int)t.rows[4].size(), c.stream))) return rc;
-  if ((rc = launch_pass_pair_multi(c.n, 1, fd, rows[5], (int)t.rows[5].size(), c.stream))) return rc;
-  if ((rc = launch_bwd_multi(c.n, 0, bd, rows[2], (int)t.rows[2].size(), c.stream))) return rc;
-  if ((rc = launch_bwd_multi(c.n, 1, bd, rows[3], (int)t.rows[3].size(), c.stream))) return rc;
-  // per-job follow-up kernels, then advance
-  for (Follow& fl : follow) {
-    Job& j = *fl.j;
-    const ptyro_ms_params* p = &j.plan.p;
-    const int n = p->n, S = p->num_slices, M = p->num_modes;
-    const size_t nn = (size_t)n * n;
-    if (fl.loss) {
-      k_amp_loss<<<j.nb, 256, 0, c.stream>>>(j.d.patterns + (size_t)j.b0 * nn, j.d.targets + (size_t)j.b0 * nn,
-                                             (int)nn, kLossEps, (float*)(j.base + j.plan.off_g),
-                                             (float*)(j.base + j.plan.off_lossp) + j.b0);
-      if ((rc = check_launch("k_amp_loss"))) return rc;
-    }
-    if (fl.slice >= 0 &&
-        (rc = launch_reduce_dv_any(p, (const float*)(j.base + j.plan.off_contrib), j.nb, j.b0, j.d.grad_potential,
-                                   fl.slice, c.stream)))
-      return rc;
-    if (fl.beam) {
-      k_reduce_beam<<<(unsigned)((nn * M + 255) / 256), 256, 0, c.stream>>>(
-          (const float2*)(j.base + j.plan.off_lam), j.nb, M, n, (float2*)(j.base + j.plan.off_beam));
-      if ((rc = check_launch("k_reduce_beam"))) return rc;
-    }
-    // advance
-    if (++j.k > S + 1) {
-      j.k = 0;
-      if (j.phase == 0 && j.plan.grad) {
-        j.phase = 1;
-      } else {
-        j.phase = 0;
-        j.b0 += j.nb;
-        if (j.b0 >= p->num_probes) {
-          if ((rc = finish_job(j, c))) return rc;
-        } else {
-          j.nb = std::min(j.plan.L.batch, p->num_probes - j.b0);
+  if ((rc = launch_tick(c.n, q, c.stream))) return rc;
+  for (const Follow& fl : follow) {
+    if ((rc = launch_follow(fl, c.stream))) return rc;
+    if (job_advance(*fl.j) && (rc = finish_job(*fl.j, c))) return rc;
+  }
+  return PTYRO_OK;
+}
+
+// ---------------------------------------------------------------- recorded batch plans
+// A fixed set of jobs (any mix of grid edges, slice counts, scan sizes, forward and
+// gradient) as one recorded sequence of launches: the scheduler's lockstep ticks are
+// simulated once on the host and every tick's descriptors and row tables are copied
+// once into the plan's arena, so launching the plan only enqueues kernels and memsets
+// on the caller's stream (no host synchronisation, copies or events) and can be
+// captured in a CUDA graph and replayed.
+struct PlanOp {
+  enum Kind { SETUP, RAMPS, TICK, FOLLOW, EPILOGUE } kind;
+  int job = -1;  // SETUP, EPILOGUE
+  RampReq ramp{};
+  Follow follow{};
+  int n = 0;  // TICK: grid edge
+  TickPtrs q{};
+};
+
+struct PlanJobs {
+  std::vector<Job> jobs;  // reserved up front: ops hold pointers into it
+  std::vector<PlanOp> ops;
+  std::vector<char> blob;  // the packed ticks
+  size_t job_bytes = 0;
+};
+
+static int plan_record(const ptyro_job_desc* descs, int num_jobs, char* arena, PlanJobs& pj) {
+  if (num_jobs < 1 || !descs) return fail(PTYRO_ERR_INVALID, "a plan needs at least one job");
+  pj.jobs.clear();
+  pj.jobs.reserve((size_t)num_jobs);
+  pj.ops.clear();
+  pj.blob.clear();
+  size_t o = 0;
+  for (int i = 0; i < num_jobs; ++i) {
+    pj.jobs.emplace_back();
+    Job& j = pj.jobs.back();
+    int rc = plan_job(&descs[i], &j.plan);
+    if (rc) return rc;
+    if (descs[i].ready_event)
+      return fail(PTYRO_ERR_INVALID, "plan jobs take no ready events: order their inputs on the launch stream");
+    j.d = descs[i];
+    j.id = i;
+    j.arena_off = o;
+    j.base = arena ? arena + o : nullptr;
+    o = align_up(o + j.plan.bytes);
+  }
+  pj.job_bytes = o;
+  char* desc_base = arena ? arena + o : nullptr;
+  std::map<int, std::vector<Job*>> classes;
+  for (Job& j : pj.jobs) {
+    PlanOp op;
+    op.kind = PlanOp::SETUP;
+    op.job = (int)j.id;
+    pj.ops.push_back(op);
+    job_start(j);
+    if (!j.issued_all) classes[j.plan.p.n].push_back(&j);
+  }
+  for (auto& kv : classes) {
+    for (;;) {
+      std::vector<Job*> running;
+      for (Job* j : kv.second)
+        if (!j->issued_all) running.push_back(j);
+      if (running.empty()) break;
+      TickRows t;
+      std::vector<RampReq> ramps;
+      std::vector<Follow> follow;
+      build_tick(running, t, ramps, follow);
+      for (const RampReq& r : ramps) {
+        PlanOp op;
+        op.kind = PlanOp::RAMPS;
+        op.ramp = r;
+        pj.ops.push_back(op);
+      }
+      const size_t off = pj.blob.size();  // a multiple of 256: every packed piece is
+      pj.blob.resize(off + tick_bytes(t));
+      PlanOp tick;
+      tick.kind = PlanOp::TICK;
+      tick.n = kv.first;
+      tick.q = pack_tick(t, pj.blob.data() + off, desc_base + off);
+      pj.ops.push_back(tick);
+      for (const Follow& fl : follow) {
+        PlanOp op;
+        op.kind = PlanOp::FOLLOW;
+        op.follow = fl;
+        pj.ops.push_back(op);
+        if (job_advance(*fl.j)) {
+          fl.j->issued_all = true;
+          PlanOp ep;
+          ep.kind = PlanOp::EPILOGUE;
+          ep.job = (int)fl.j->id;
+          pj.ops.push_back(ep);
         }
       }
     }
@@ -464,7 +630,77 @@ static int tick_class(ptyro_sched* s, GridClass& c, std::vector<Job*>& jobs) {
 
 }  // namespace ptyro
 
+struct ptyro_plan {
+  int device = 0;
+  ptyro::PlanJobs pj;
+};
+
 extern "C" {
+
+size_t ptyro_plan_bytes(const ptyro_job_desc* jobs, int32_t num_jobs) {
+  ptyro::PlanJobs pj;
+  if (ptyro::plan_record(jobs, num_jobs, nullptr, pj)) return 0;
+  return pj.job_bytes + ptyro::align_up(pj.blob.size());
+}
+
+int ptyro_plan_create(int32_t device, const ptyro_job_desc* jobs, int32_t num_jobs, void* arena, size_t arena_bytes,
+                      ptyro_plan** out) {
+  using namespace ptyro;
+  if (!out) return fail(PTYRO_ERR_INVALID, "out is NULL");
+  *out = nullptr;
+  if (!arena || ((uintptr_t)arena & 255)) return fail(PTYRO_ERR_WORKSPACE, "arena must be 256-byte aligned");
+  int cur = -1;
+  cudaGetDevice(&cur);
+  if (cur != device) return fail(PTYRO_ERR_INVALID, "create the plan with its device current");
+  auto plan = std::make_unique<ptyro_plan>();
+  plan->device = device;
+  int rc = plan_record(jobs, num_jobs, (char*)arena, plan->pj);
+  if (rc) return rc;
+  const size_t need = plan->pj.job_bytes + align_up(plan->pj.blob.size());
+  if (arena_bytes < need)
+    return fail(PTYRO_ERR_WORKSPACE, "plan needs " + std::to_string(need) + " arena bytes; got " +
+                                         std::to_string(arena_bytes));
+  if (!plan->pj.blob.empty() &&
+      cudaMemcpy((char*)arena + plan->pj.job_bytes, plan->pj.blob.data(), plan->pj.blob.size(),
+                 cudaMemcpyHostToDevice) != cudaSuccess)
+    return fail(PTYRO_ERR_CUDA, "plan descriptor upload failed");
+  *out = plan.release();
+  return PTYRO_OK;
+}
+
+int ptyro_plan_launch(ptyro_plan* plan, void* stream) {
+  using namespace ptyro;
+  if (!plan) return fail(PTYRO_ERR_INVALID, "plan is NULL");
+  int cur = -1;
+  cudaGetDevice(&cur);
+  if (cur != plan->device) return fail(PTYRO_ERR_INVALID, "launch the plan with its device current");
+  cudaStream_t st = (cudaStream_t)stream;
+  int rc = PTYRO_OK;
+  for (const PlanOp& op : plan->pj.ops) {
+    switch (op.kind) {
+      case PlanOp::SETUP: rc = job_setup(plan->pj.jobs[op.job], st); break;
+      case PlanOp::RAMPS: rc = launch_ramps(op.ramp, st); break;
+      case PlanOp::TICK: rc = launch_tick(op.n, op.q, st); break;
+      case PlanOp::FOLLOW: rc = launch_follow(op.follow, st); break;
+      case PlanOp::EPILOGUE: rc = job_epilogue(plan->pj.jobs[op.job], st); break;
+    }
+    if (rc) return rc;
+  }
+  return PTYRO_OK;
+}
+
+int ptyro_plan_job_status(const ptyro_plan* plan, int32_t job, void** status_word) {
+  if (!plan || !status_word) return ptyro::fail(PTYRO_ERR_INVALID, "plan or status_word is NULL");
+  if (job < 0 || job >= (int)plan->pj.jobs.size()) return ptyro::fail(PTYRO_ERR_INVALID, "job index out of range");
+  const ptyro::Job& j = plan->pj.jobs[job];
+  *status_word = j.base + j.plan.off_fwd + j.plan.L.status;
+  return PTYRO_OK;
+}
+
+int ptyro_plan_destroy(ptyro_plan* plan) {
+  delete plan;
+  return PTYRO_OK;
+}
 
 size_t ptyro_sched_job_bytes(const ptyro_job_desc* d) {
   JobPlan jp;

@@ -100,8 +100,10 @@ def probe_modes_to_distribution(probe: ProbeModes) -> Distribution:
     """The incoherent mode axis with the beam's weights (simulations.py:682-711)."""
     m = probe.modes.shape[2] if probe.modes.ndim == 3 else 1
     samples = np.arange(m, dtype=np.float64)[:, None]
-    return create_distribution(samples, as_tensor(probe.weights, torch.float64).cpu(), ReductionMode.INCOHERENT,
-                               AXIS_PROBE_MODES)
+    # a constant copy: derivatives with respect to the beam weights flow through the
+    # engine calls, which take the weights themselves
+    return create_distribution(samples, as_tensor(probe.weights, torch.float64).detach().cpu(),
+                               ReductionMode.INCOHERENT, AXIS_PROBE_MODES)
 
 
 # ----------------------------------------------------------------------------- axes
@@ -265,6 +267,65 @@ def run_forward_ensemble(slices: torch.Tensor, slice_thickness: float, groups: L
                                              g.weights.data_ptr(), positions.data_ptr(), g.tilts.data_ptr(),
                                              out.data_ptr(), ws.data_ptr(), nbytes, _stream_ptr(dev))
         _lib.check(rc)
+    return out
+
+
+def ensemble_patterns_differentiable(slices: torch.Tensor, slice_thickness: float, beam: ProbeModes,
+                                     ensemble: EnsembleAxes, modes: torch.Tensor, weights: torch.Tensor,
+                                     voltage_kv: float, calib_ang: float, positions: torch.Tensor,
+                                     shift_calib_ang: float) -> torch.Tensor:
+    """The ensemble patterns as a reverse-mode differentiable function of the
+    potential, the beam modes, the beam weights and the scan positions, for
+    INCOHERENT axes of probe modes, position jitter and energy spread.
+
+    The axes form a Cartesian product (at most one axis of each kind,
+    ``ensemble_axes_for_cbed``), so the patterns are
+    sum_c w_c sum_j w_j stem_4d(modes, w_modes, positions + delta_j * s, voltage + dE_c),
+    with s = shift_calib_ang / calib_ang: the jitter's Fourier shift at the ensemble
+    calibration composes with the scan shift into one shift of the scan position.
+    Each energy is one differentiable engine call over all jitter copies of the scan.
+    Tilted coherence samples and COHERENT axes raise ``NotImplementedError``."""
+    axes = ensemble_axes_for_cbed(ensemble, beam)
+    mode_count = modes.shape[2]
+    maps = _axis_maps(axes, mode_count)
+    if any(a.reduction is not ReductionMode.INCOHERENT for a in axes):
+        raise NotImplementedError("derivatives through COHERENT ensemble axes are not supported")
+    dev = slices.device
+    sel, w_modes = None, weights
+    jit, w_jit = np.zeros((1, 2)), np.ones(1)
+    energies: dict = {0.0: 1.0}
+    for axis, kind in zip(axes, maps):
+        smp, wts = axis.samples.detach().numpy(), axis.weights.detach().numpy()
+        if kind == AXIS_PROBE_MODES:
+            idx = smp[:, 0].astype(np.int64)
+            if np.any(idx < 0) or np.any(idx >= mode_count):
+                raise ValueError("probe mode index out of range")
+            if ensemble.probe_modes is not None:  # an explicit axis: its own constant weights
+                sel = torch.as_tensor(idx, device=dev)
+                w_modes = torch.as_tensor(wts, dtype=torch.float32, device=dev)
+            elif not np.array_equal(idx, np.arange(mode_count)):
+                raise ValueError("the beam's mode axis must list every mode once")
+        elif kind == AXIS_POSITION_JITTER:
+            jit, w_jit = smp, wts
+        else:
+            if np.any(smp[:, 1:3] != 0.0):
+                raise NotImplementedError("derivatives through tilted coherence samples are not supported")
+            energies = {}
+            for de, w in zip(smp[:, 0], wts):
+                energies[float(de)] = energies.get(float(de), 0.0) + float(w)
+    use_modes = modes if sel is None else modes.index_select(2, sel)
+    scale = float(shift_calib_ang) / float(calib_ang)
+    offsets = torch.as_tensor(jit * scale, dtype=torch.float64, device=dev)  # (J, 2)
+    J, P = offsets.shape[0], positions.shape[0]
+    pos_all = (positions[None, :, :] + offsets[:, None, :]).reshape(J * P, 2)
+    wj = torch.as_tensor(w_jit, dtype=torch.float32, device=dev)
+    from .autodiff import stem_4d_patterns
+    out = None
+    for de, w_e in energies.items():
+        pat = stem_4d_patterns(slices, use_modes, w_modes.to(torch.float32), pos_all, slice_thickness,
+                               voltage_kv + de / 1000.0, calib_ang, shift_calib_ang)
+        part = float(w_e) * torch.einsum("j,jpyx->pyx", wj, pat.reshape((J, P) + tuple(pat.shape[1:])))
+        out = part if out is None else out + part
     return out
 
 

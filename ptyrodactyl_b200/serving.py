@@ -94,6 +94,85 @@ class Scheduler:
             pass
 
 
+class BatchPlan:
+    """A fixed batch of jobs (uneven grid edges, slice counts and scan sizes, forward
+    and gradient) recorded once as the scheduler would run them (``ptyro_plan_*``):
+    every tick one multi-job launch per pass kind, all descriptors in device memory.
+    :meth:`launch` enqueues the whole batch on the current stream with no host
+    synchronisation; :meth:`capture` records that into a CUDA graph and
+    :meth:`replay` reruns every job on the current contents of its input buffers.
+    Inputs must be ready on the launching stream; the arena holds all jobs' scratch."""
+
+    def __init__(self, descs: List[_lib.JobDesc], keep: tuple = (), device=None):
+        self.lib = _lib.load()
+        self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+        self._descs = (_lib.JobDesc * len(descs))(*descs)
+        self.num_jobs = len(descs)
+        nbytes = int(self.lib.ptyro_plan_bytes(self._descs, self.num_jobs))
+        if nbytes == 0:
+            _lib.check(_lib.PTYRO_ERR_INVALID)
+        self.arena = torch.empty(nbytes, dtype=torch.uint8, device=self.device)
+        handle = ctypes.c_void_p()
+        with torch.cuda.device(self.device):
+            _lib.check(self.lib.ptyro_plan_create(self.device.index or 0, self._descs, self.num_jobs,
+                                                  self.arena.data_ptr(), nbytes, ctypes.byref(handle)))
+        self.handle = handle
+        self._keep = keep
+        self.graph: Optional[torch.cuda.CUDAGraph] = None
+
+    def launch(self, stream: Optional[torch.cuda.Stream] = None) -> None:
+        st = stream if stream is not None else torch.cuda.current_stream(self.device)
+        with torch.cuda.device(self.device):
+            _lib.check(self.lib.ptyro_plan_launch(self.handle, st.cuda_stream))
+
+    def capture(self) -> torch.cuda.CUDAGraph:
+        """Record one launch into a CUDA graph (after one plain launch, which sets the
+        kernels' per-device attributes outside the capture)."""
+        main = torch.cuda.current_stream(self.device)
+        self.launch(main)
+        side = torch.cuda.Stream(device=self.device)
+        side.wait_stream(main)
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, stream=side):
+            self.launch(side)
+        main.wait_stream(side)
+        self.graph = g
+        return g
+
+    def replay(self) -> None:
+        if self.graph is None:
+            raise RuntimeError("capture() the plan first")
+        self.graph.replay()
+
+    def status(self) -> int:
+        """OR of the jobs' device status words after the last launch (synchronises)."""
+        base = self.arena.data_ptr()
+        word = 0
+        for i in range(self.num_jobs):
+            ptr = ctypes.c_void_p()
+            _lib.check(self.lib.ptyro_plan_job_status(self.handle, i, ctypes.byref(ptr)))
+            off = int(ptr.value) - base
+            word |= int(self.arena[off:off + 4].view(torch.int32).item())
+        return word
+
+    def check(self, what: str = "batch plan") -> None:
+        word = self.status()
+        if word:
+            raise _lib.DeviceStatusError(f"{what}: device status {word:#x} (a bounded wait gave up)")
+
+    def close(self) -> None:
+        if getattr(self, "handle", None):
+            self.graph = None
+            self.lib.ptyro_plan_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 @dataclass
 class Request:
     """One simulation (kind "forward") or gradient solve (kind "grad")."""
@@ -166,6 +245,25 @@ class Server:
 
     # ---- requests
     def submit(self, req: Request) -> int:
+        d, res, keep = self._job(req)
+        # the inputs above were written on torch's stream; the scheduler's streams wait for them
+        ready = torch.cuda.Event()
+        ready.record(torch.cuda.current_stream(self.device))
+        d.ready_event = ready.cuda_event
+        keep = keep + (ready,)
+        res.submit_s = time.perf_counter()
+        jid = self.sched.submit(d, keep)
+        self.active[jid] = res
+        return jid
+
+    def plan(self, requests: List[Request]) -> Tuple["BatchPlan", List[Result]]:
+        """The requests as one recorded :class:`BatchPlan` (not submitted to the
+        scheduler) and their result buffers, filled by every launch or replay."""
+        jobs = [self._job(r) for r in requests]
+        plan = BatchPlan([d for d, _, _ in jobs], keep=tuple(k for _, _, k in jobs), device=self.device)
+        return plan, [r for _, r, _ in jobs]
+
+    def _job(self, req: Request) -> Tuple[_lib.JobDesc, Result, tuple]:
         pot = self.potentials[req.potential_key]
         if pot.shape[0] != req.n or pot.shape[1] != req.n or pot.shape[2] < req.num_slices:
             raise ValueError("the cached potential must be (n, n, S_max) with S_max >= the request's slices")
@@ -199,15 +297,7 @@ class Server:
             d.grad_modes = res.grad_modes.data_ptr()
             d.loss = res.loss.data_ptr()
             keep = keep + (tg, gbase, res.grad_modes, res.loss)
-        # the inputs above were written on torch's stream; the scheduler's streams wait for them
-        ready = torch.cuda.Event()
-        ready.record(torch.cuda.current_stream(self.device))
-        d.ready_event = ready.cuda_event
-        keep = keep + (ready,)
-        res.submit_s = time.perf_counter()
-        jid = self.sched.submit(d, keep)
-        self.active[jid] = res
-        return jid
+        return d, res, keep
 
     def poll(self) -> int:
         """One scheduler tick; move finished jobs to :attr:`finished`. Returns jobs in flight."""

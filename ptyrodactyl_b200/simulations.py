@@ -381,10 +381,14 @@ def stem_4d(pot_slice: PotentialSlices, beam: ProbeModes, microscope: Microscope
     if not microscope.ensemble.is_empty():
         # per position, cbed_image's ensemble branch (simulations.py:1163-1193)
         if _needs_autodiff(slices, modes, positions, weights):
-            raise NotImplementedError("derivatives through ensemble axes are not supported by the B200 engine")
-        from .ensemble import ensemble_patterns
-        data = ensemble_patterns(slices, pot_slice.slice_thickness, beam, microscope.ensemble,
-                                 microscope.voltage_kv, calib, positions, detector.real_space_calib_ang)
+            from .ensemble import ensemble_patterns_differentiable
+            data = ensemble_patterns_differentiable(slices, pot_slice.slice_thickness, beam, microscope.ensemble,
+                                                    modes, weights, microscope.voltage_kv, calib, positions,
+                                                    detector.real_space_calib_ang)
+        else:
+            from .ensemble import ensemble_patterns
+            data = ensemble_patterns(slices, pot_slice.slice_thickness, beam, microscope.ensemble,
+                                     microscope.voltage_kv, calib, positions, detector.real_space_calib_ang)
     elif _needs_autodiff(slices, modes, positions, weights):
         # differentiable path: checkpointed forward + hand-written adjoint kernel
         from .autodiff import stem_4d_patterns

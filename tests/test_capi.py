@@ -211,3 +211,21 @@ def test_any_size_routing_host_logic():
         check_any_grid(torch.zeros(45, 78, 2), md)
     with pytest.raises(ValueError, match="4096"):
         check_any_grid(torch.zeros(5000, 3, 1), torch.zeros(5000, 3, 1, dtype=torch.complex64))
+
+
+def test_batch_plan_bytes_validate(lib):
+    p = _p(num_probes=5, num_slices=4, batch=2)
+    jobs = (_lib.JobDesc * 2)()
+    buf = ctypes.create_string_buffer(64)
+    fake = ctypes.addressof(buf)
+    for j in jobs:
+        j.p = p
+        j.kind = _lib.PTYRO_JOB_FORWARD
+        j.potential = j.modes = j.weights = j.positions = j.patterns = fake
+    assert lib.ptyro_plan_bytes(jobs, 2) >= 2 * lib.ptyro_sched_job_bytes(ctypes.byref(jobs[0]))
+    assert lib.ptyro_plan_bytes(jobs, 0) == 0
+    jobs[1].ready_event = fake  # plans order their inputs on the launch stream
+    assert lib.ptyro_plan_bytes(jobs, 2) == 0 and "ready" in lib.ptyro_last_error().decode()
+    jobs[1].ready_event = None
+    jobs[1].kind = _lib.PTYRO_JOB_GRADIENT  # without targets and gradient buffers
+    assert lib.ptyro_plan_bytes(jobs, 2) == 0

@@ -2,6 +2,8 @@
 amplitudes on the GPU, against the oracle's restatement of cbed_image's ensemble
 branch."""
 
+import dataclasses
+
 import numpy as np
 import pytest
 import torch
@@ -85,3 +87,58 @@ def test_coherent_mode_axis_and_unsupported_coherent_tilts():
     mic2 = pb.create_microscope_config(200.0, 25.0, ensemble=ens2, probe_shape=(64, 64))
     with pytest.raises(NotImplementedError, match="coherent sums over energy or tilt"):
         pb.cbed_image(pb.create_potential_slices(pot, 1.7, 0.25), beam, mic2)
+
+
+@pytest.mark.parametrize("jitter,energy", [(0.08, 0.0), (0.0, 0.6), (0.1, 0.5)])
+def test_stem_4d_ensemble_gradients_match_oracle(jitter, energy):
+    """Reverse mode through incoherent jitter and energy-spread axes and a two-mode
+    beam: the patterns against the oracle's ensemble branch, and dL/dV, dL/dbeam,
+    dL/d(weights) and dL/d(positions) against the oracle's adjoint summed over the
+    (energy, jitter) samples, each at the scan positions moved by the jitter (the
+    jitter's Fourier shift at the beam calibration composed with the scan shift)."""
+    pot, modes, w = _setup(n=64, s=3, m=2, seed=12)
+    rng = np.random.default_rng(4)
+    pos = rng.uniform(-2, 2, (4, 2))
+    g = rng.normal(size=(4, 64, 64))
+    ens = pb.create_ensemble_axes(position_jitter=pb.position_jitter_to_distribution(jitter, 2),
+                                  coherence=pb.coherence_to_distribution(energy, 0.0, 2))
+    mic = pb.create_microscope_config(200.0, 25.0, ensemble=ens, probe_shape=(64, 64))
+    det = pb.create_detector_config(0.3, scan_positions_px=pos)
+    dev = torch.device("cuda")
+    V = torch.tensor(pot, dtype=torch.float32, device=dev, requires_grad=True)
+    md = torch.tensor(modes.astype(np.complex64), device=dev, requires_grad=True)
+    wt = torch.tensor(w, dtype=torch.float32, device=dev, requires_grad=True)
+    ps = torch.tensor(pos, dtype=torch.float64, device=dev, requires_grad=True)
+    det_t = dataclasses.replace(det, scan_positions_px=ps)
+    s4 = pb.stem_4d(pb.PotentialSlices(V, 1.7, 0.25), pb.ProbeModes(md, wt, 0.25), mic, det_t)
+    (s4.data * torch.as_tensor(g, dtype=torch.float32, device=dev)).sum().backward()
+    beam = pb.create_probe_modes(modes, w, 0.25)
+    axes = [_axes_oracle(a) for a in pb.ensemble_axes_for_cbed(ens, beam)]
+    want = R.stem_4d_ensemble(pot, 1.7, 0.25, modes, 0.25, 200.0, pos, 0.3, axes)
+    assert rel_l2(s4.data.detach().cpu().numpy(), want) < TOL
+    jit = pb.position_jitter_to_distribution(jitter, 2)
+    coh = pb.coherence_to_distribution(energy, 0.0, 2)
+    dv, dm, dpos, dw = 0.0, 0.0, 0.0, np.zeros(2)
+    for (de, _, _), wc in zip(coh.samples.numpy(), coh.weights.numpy()):
+        for delta, wj in zip(jit.samples.numpy(), jit.weights.numpy()):
+            pj = pos + delta * (0.3 / 0.25)
+            kv = 200.0 + de / 1000.0
+            a, b, c = R.stem_4d_vjp(pot, 1.7, 0.25, modes, w, 0.25, kv, pj, 0.3, g * wc * wj, with_positions=True)
+            dv, dm, dpos = dv + a, dm + b, dpos + c
+            for k in range(2):
+                per = R.stem_4d(pot, 1.7, 0.25, modes[..., k:k + 1], [1.0], 0.25, kv, pj, 0.3)["data"]
+                dw[k] += wc * wj * np.sum(g * per)
+    assert rel_l2(V.grad.cpu().numpy(), dv) < TOL
+    assert rel_l2(md.grad.cpu().numpy(), np.conj(dm)) < TOL
+    assert rel_l2(wt.grad.cpu().numpy(), dw) < TOL
+    assert rel_l2(ps.grad.cpu().numpy(), dpos) < TOL
+
+
+def test_ensemble_derivatives_refuse_tilts():
+    pot, modes, w = _setup(n=32, s=2, m=1, seed=2)
+    ens = pb.create_ensemble_axes(coherence=pb.coherence_to_distribution(0.3, 0.2, 2))
+    mic = pb.create_microscope_config(200.0, 25.0, ensemble=ens, probe_shape=(32, 32))
+    det = pb.create_detector_config(0.3, scan_positions_px=np.zeros((1, 2)))
+    V = torch.tensor(pot, dtype=torch.float32, device="cuda", requires_grad=True)
+    with pytest.raises(NotImplementedError, match="tilted"):
+        pb.stem_4d(pb.PotentialSlices(V, 1.7, 0.25), pb.create_probe_modes(modes, w, 0.25), mic, det)

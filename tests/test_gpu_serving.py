@@ -147,3 +147,56 @@ def test_cancel_queued_and_admission_waits_for_memory():
         want = _alone(srv, r)
         assert torch.equal(by_id[id(r)].patterns, want)
     srv.close()
+
+
+def test_batch_plan_launch_and_graph_replay_equal_the_scheduler(server):
+    """Uneven jobs (four grid edges, 2-6 slices, 1-7 probes, forward and gradient) as
+    one recorded plan: a plain launch and a CUDA-graph replay give the scheduler's
+    results bit for bit, and a replay reads the current contents of the inputs."""
+    rng = np.random.default_rng(21)
+    reqs = [_req(64, 5, 7, seed=31), _req(128, 3, 2, seed=32), _req(256, 2, 2, seed=33), _req(512, 2, 1, seed=35)]
+    for n, s, p, seed in ((64, 4, 3, 34), (128, 6, 5, 36)):
+        tg = torch.as_tensor(rng.uniform(0, 1e-3, (p, n, n)), dtype=torch.float32, device=server.device)
+        reqs.append(_req(n, s, p, kind="grad", seed=seed, targets=tg))
+    n0 = len(server.finished)
+    for r in reqs:
+        server.submit(r)
+    server.drain()
+    want = {id(res.request): res for res in server.finished[n0:]}
+    assert all(res.state == _lib.JOB_DONE for res in want.values())
+
+    def same(results):
+        for r, res in zip(reqs, results):
+            w = want[id(r)]
+            assert torch.equal(res.patterns, w.patterns)
+            if r.kind == "grad":
+                assert torch.equal(res.grad_potential, w.grad_potential)
+                assert torch.equal(res.grad_modes, w.grad_modes)
+                assert torch.equal(res.loss, w.loss)
+
+    plan, results = server.plan(reqs)
+    plan.launch()
+    torch.cuda.synchronize()
+    plan.check()
+    same(results)
+    plan.capture()
+    for res in results:
+        res.patterns.zero_()
+        if res.grad_potential is not None:
+            res.grad_modes.zero_()
+            res.loss.zero_()
+    plan.replay()
+    torch.cuda.synchronize()
+    plan.check()
+    same(results)
+    # a replay recomputes from the inputs' current contents: move the first job's scan
+    pos = plan._keep[0][2]
+    pos.add_(0.75)
+    plan.replay()
+    torch.cuda.synchronize()
+    r0 = reqs[0]
+    moved = Request(n=r0.n, num_slices=r0.num_slices, positions=pos.cpu().numpy(), voltage_kv=r0.voltage_kv,
+                    aperture_mrad=r0.aperture_mrad, defocus_ang=r0.defocus_ang, potential_key=r0.potential_key,
+                    calib_ang=r0.calib_ang)
+    assert torch.equal(results[0].patterns, _alone(server, moved))
+    plan.close()
