@@ -583,7 +583,7 @@ def run_grad(args, rank, world, local_rank):
 # ----------------------------------------------------------------------------- 512^2 leg
 def run_config3(args, rank, world, local_rank):
     """512^2 grid, 32x32 cell, 100 slices, frozen-phonon average of 4 configurations,
-    on a sample of the 128x128 scan (``--probes``); one JSON line."""
+    on the 128x128 scan (or a sample of ``--probes`` positions); one JSON line."""
     import torch
     import ptyrodactyl_b200 as pb
     from ptyrodactyl_b200 import _lib
@@ -593,13 +593,14 @@ def run_config3(args, rank, world, local_rank):
     w = synth.CONFIG3
     n, S = w.n, w.num_slices
     pos_all = synth.raster_positions(w)
-    idx = np.linspace(0, pos_all.shape[0] - 1, args.probes).astype(np.int64)
+    probes = args.probes or pos_all.shape[0]  # default: the full 128x128 scan
+    idx = np.linspace(0, pos_all.shape[0] - 1, probes).astype(np.int64)
     pos = torch.as_tensor(pos_all[idx], device=dev).contiguous()
     pots = [torch.as_tensor(synth.potential_slices(w, phonon=k), device=dev) for k in range(w.phonon_configs)]
     mic = pb.create_microscope_config(w.voltage_kv, w.aperture_mrad, probe_shape=(n, n))
     modes = pb.make_probe(mic, pb.create_detector_config(w.calib))[..., None].contiguous()
     wq = torch.full((1,), 1.0 / len(pots), dtype=torch.float32, device=dev)
-    out = torch.zeros((args.probes, n, n), dtype=torch.float32, device=dev)
+    out = torch.zeros((probes, n, n), dtype=torch.float32, device=dev)
 
     def step():
         out.zero_()
@@ -618,7 +619,7 @@ def run_config3(args, rank, world, local_rank):
     e.record()
     torch.cuda.synchronize()
     ms = s.elapsed_time(e) / reps
-    updates = float(args.probes) * S * len(pots)
+    updates = float(probes) * S * len(pots)
     sums = out.sum(dim=(1, 2))
     n_ap = float(_aperture_mask(w).sum())
     line = {"metric": "probe-slice updates/s at 512^2 (100 slices, 4 frozen-phonon configurations averaged)",
@@ -627,7 +628,7 @@ def run_config3(args, rank, world, local_rank):
             "n_gpus": world, "dtype": "f32", "data": "synthetic",
             "checks": {"pattern_sum_max_rel_err": float(((sums - n_ap).abs().max() / n_ap).item()),
                        "tma_wait_timeouts": int(_lib.load().ptyro_pass_wait_timeouts())},
-            "config": {"workload": w.name, "grid": n, "slices": S, "probes_sampled": args.probes,
+            "config": {"workload": w.name, "grid": n, "slices": S, "probes_sampled": probes,
                        "probes_full_scan": w.num_probes, "phonon_configs": len(pots), "batch": args.batch,
                        "tune": default_tune(w.n) if args.tune < 0 else args.tune}}
     if rank == 0:
@@ -795,7 +796,7 @@ def run_profile_case(args, rank, world, local_rank):
     from ptyrodactyl_b200.simulations import make_probe, ms_params
     from ptyrodactyl_b200.types import create_detector_config, create_microscope_config
 
-    n, probes, reps, S = args.grid, args.probes, args.reps, args.slices
+    n, probes, reps, S = args.grid, args.probes or 2048, args.reps, args.slices
     tune = default_tune(n) if args.tune < 0 else args.tune
     w = synth.CONFIG2
     dev = torch.device("cuda", local_rank)
@@ -874,8 +875,9 @@ def main():
                     help="forward mode: skip the gradient and serving legs that follow the headline")
     ap.add_argument("--mode", choices=("forward", "grad", "serve", "config1", "config3", "profile-case"),
                     default="forward")
-    ap.add_argument("--probes", type=int, default=2048,
-                    help="config3 mode: scan positions sampled; profile-case mode: probes in the one batch")
+    ap.add_argument("--probes", type=int, default=0,
+                    help="config3 mode: scan positions sampled (0: the full 128x128 scan); profile-case mode: "
+                         "probes in the one batch (0: 2048)")
     ap.add_argument("--grid", type=int, default=256, help="profile-case mode: grid edge")
     ap.add_argument("--reps", type=int, default=1, help="profile-case mode: steady passes per axis")
     ap.add_argument("--slices", type=int, default=2, help="profile-case mode: slices of the forward")

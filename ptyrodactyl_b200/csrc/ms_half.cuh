@@ -7,8 +7,11 @@
 //   in-thread DFT:   decimation in frequency, a_j = x_j + x_{j+N1},
 //                    b_j = (x_j - x_{j+N1}) W_{2 N1}^j, then one paired N1-point DFT
 //                    gives (X[2k], X[2k+1]) in Pair k
-//   exchange:        as the one-line kernel; the k-order groups g = 0, 1 of the
-//                    second stage form the Pairs, so the N1-point group DFTs pair too
+//   exchange:        thread t of the second stage takes rows k2 = 2t and 2t + 1 of
+//                    every column, exactly the Pairs the first stage produced, so the
+//                    exchange moves whole Pairs (16 bytes) and the N1-point DFTs of
+//                    the second stage pair too: thread t ends with
+//                    Pair k1 = (X[2t + N2 k1], X[2t + 1 + N2 k1])
 //   inverse:         the mirror image (paired group DFTs, exchange, paired N1-point
 //                    DFT of (even, odd) inputs, decimation-in-time final stage), which
 //                    returns each value to the thread and the pairing it came from.
@@ -26,10 +29,46 @@ struct HalfLine {
   static constexpr int H = N1;  // Pairs per thread
 };
 
-// forward, natural (j, j + H) pairs -> k-order Pairs (g = 0, g = 1 of k1); DIR = -1
+// a * conj(w) with w = ((wA.x, wB.x), (wA.y, wB.y)): the operations of
+// cmul(Pair, conj(wA), conj(wB))
+__device__ __forceinline__ Pair cmulc_pp(Pair a, Pair w) {
+  return {__ffma2_rn(a.re, w.re, __fmul2_rn(a.im, w.im)),
+          __ffma2_rn(a.re, make_float2(-w.im.x, -w.im.y), __fmul2_rn(a.im, w.re))};
+}
+
+// Exchange buffer of one line: Pair entry (m, n1) holds rows 2m and 2m + 1 (of the
+// N2 rows k2) of column n1 at m * (N1 + 1) + n1, so one 16-byte store and one
+// 16-byte load move a Pair between the two stages without repacking; both access
+// patterns (m fixed, n1 = lane; n1 fixed, m = lane) put the 8 lanes of each
+// quarter-warp phase in distinct banks. It fits in the line's LineBuf region.
+template <int N1, int N2>
+struct HalfBuf {
+  static constexpr int kRow = N1 + 1;
+  static_assert(N2 == 2 * N1 && sizeof(Pair) * (N2 / 2) * kRow <= sizeof(float2) * LineBuf<N1, N2>::kSize,
+                "the Pair exchange buffer must fit in the line's buffer");
+  __device__ static __forceinline__ int at(int m, int n1) { return m * kRow + n1; }
+};
+
+// Tables of the half-paired kernel, Pair-shaped so that each lookup is one 16-byte
+// load: twiddles twp[m * N1 + t] = (W_N^{2m t}, W_N^{(2m+1) t}) and propagator factors
+// pfp[k1 * N1 + t] = (P[2t + N2 k1], P[2t + 1 + N2 k1]), the factors of the k-order
+// Pair k1 of thread t.
+template <int N1, int N2>
+__device__ __forceinline__ void half_tables(const float2* __restrict__ tw_g, const float2* __restrict__ pf_g,
+                                            Pair* twp, Pair* pfp) {
+  constexpr int N = N1 * N2;
+  for (int i = threadIdx.x; i < N / 2; i += blockDim.x) {
+    const int m = i / N1, t = i % N1;
+    twp[i] = make_pair(tw_g[(t * 2 * m) % N], tw_g[(t * (2 * m + 1)) % N]);
+    pfp[i] = make_pair(pf_g[2 * t + N2 * m], pf_g[2 * t + 1 + N2 * m]);
+  }
+}
+
+// forward, natural (j, j + H) pairs -> k-order Pairs; DIR = -1. Thread t ends with
+// Pair k1 = (X[2t + N2 k1], X[2t + 1 + N2 k1]).
 template <int N1, int N2, int DIR>
-__device__ __forceinline__ void half_nat_to_k(Pair (&p)[N1], int t, float2* buf, const float2* tw) {
-  using LB = LineBuf<N1, N2>;
+__device__ __forceinline__ void half_nat_to_k(Pair (&p)[N1], int t, Pair* buf, const Pair* twp) {
+  using HB = HalfBuf<N1, N2>;
   constexpr int H = N1;
   // decimation in frequency: a_j = x_j + x_{j+H}, b_j = (x_j - x_{j+H}) W_{2H}^j
 #pragma unroll
@@ -39,48 +78,36 @@ __device__ __forceinline__ void half_nat_to_k(Pair (&p)[N1], int t, float2* buf,
     const float2 b = twmul64<DIR>(csub(xa, xb), j * (64 / (2 * H)));
     p[j] = make_pair(a, b);
   }
-  dft<H, DIR, 1, 0, H>(p);  // Pair k = (X[2k], X[2k+1])
+  dft<H, DIR, 1, 0, H>(p);  // Pair k = (Y[2k], Y[2k+1])
   // twiddles W_N^{t k2}, k2 = 2k and 2k + 1
   if (t != 0) {
 #pragma unroll
-    for (int k = 0; k < H; ++k) {
-      const float2 wa = tw[(2 * k) * N1 + t], wb = tw[(2 * k + 1) * N1 + t];
-      p[k] = DIR < 0 ? cmul(p[k], wa, wb) : cmul(p[k], cconj(wa), cconj(wb));
-    }
+    for (int k = 0; k < H; ++k) p[k] = DIR < 0 ? cmul_pp(p[k], twp[k * N1 + t]) : cmulc_pp(p[k], twp[k * N1 + t]);
   }
   __syncwarp();
 #pragma unroll
-  for (int k = 0; k < H; ++k) {
-    buf[LB::at(2 * k, t)] = pair_a(p[k]);
-    buf[LB::at(2 * k + 1, t)] = pair_b(p[k]);
-  }
+  for (int k = 0; k < H; ++k) buf[HB::at(k, t)] = p[k];
   __syncwarp();
 #pragma unroll
-  for (int n1 = 0; n1 < N1; ++n1) p[n1] = make_pair(buf[LB::at(t, n1)], buf[LB::at(t + N1, n1)]);
-  dft<N1, DIR, 1, 0, N1>(p);  // Pair k1 = (r = k1, r = N1 + k1) of the k-order layout
+  for (int n1 = 0; n1 < N1; ++n1) p[n1] = buf[HB::at(t, n1)];  // (Y_{n1}[2t], Y_{n1}[2t+1])
+  dft<N1, DIR, 1, 0, N1>(p);
 }
 
 // inverse, k-order Pairs -> natural (j, j + H) pairs; DIR = +1
 template <int N1, int N2, int DIR>
-__device__ __forceinline__ void half_k_to_nat(Pair (&p)[N1], int t, float2* buf, const float2* tw) {
-  using LB = LineBuf<N1, N2>;
+__device__ __forceinline__ void half_k_to_nat(Pair (&p)[N1], int t, Pair* buf, const Pair* twp) {
+  using HB = HalfBuf<N1, N2>;
   constexpr int H = N1;
-  dft<N1, DIR, 1, 0, N1>(p);
+  dft<N1, DIR, 1, 0, N1>(p);  // Pair n1 = (rows 2t, 2t + 1 of column n1)
   __syncwarp();
 #pragma unroll
-  for (int n1 = 0; n1 < N1; ++n1) {
-    buf[LB::at(t, n1)] = pair_a(p[n1]);
-    buf[LB::at(t + N1, n1)] = pair_b(p[n1]);
-  }
+  for (int n1 = 0; n1 < N1; ++n1) buf[HB::at(t, n1)] = p[n1];
   __syncwarp();
 #pragma unroll
-  for (int m = 0; m < H; ++m) p[m] = make_pair(buf[LB::at(2 * m, t)], buf[LB::at(2 * m + 1, t)]);
+  for (int m = 0; m < H; ++m) p[m] = buf[HB::at(m, t)];
   if (t != 0) {
 #pragma unroll
-    for (int m = 0; m < H; ++m) {
-      const float2 wa = tw[(2 * m) * N1 + t], wb = tw[(2 * m + 1) * N1 + t];
-      p[m] = DIR < 0 ? cmul(p[m], wa, wb) : cmul(p[m], cconj(wa), cconj(wb));
-    }
+    for (int m = 0; m < H; ++m) p[m] = DIR < 0 ? cmul_pp(p[m], twp[m * N1 + t]) : cmulc_pp(p[m], twp[m * N1 + t]);
   }
   dft<H, DIR, 1, 0, H>(p);  // Pair j = (E_j, O_j): transforms of the even and odd inputs
   // decimation in time: x_j = E_j + W_{2H}^j O_j, x_{j+H} = E_j - W_{2H}^j O_j
@@ -111,8 +138,8 @@ __device__ __forceinline__ void half_body(const PassArgs& a, const int slot, con
                 "the warp's exchange buffers must hold its column block at 128-byte alignment");
   __shared__ __align__(8) uint64_t half_bar[TMA ? WARPS : 1];
   extern __shared__ float2 smem[];
-  float2* tw = smem;
-  float2* pfs = smem + N;
+  Pair* twp = reinterpret_cast<Pair*>(smem);          // N / 2 Pairs
+  Pair* pfp = reinterpret_cast<Pair*>(smem + N);      // N / 2 Pairs
   float2* work = smem + 2 * N;
   float2* stg = nullptr;  // TMA staging: [row][G]
   uint32_t bar = 0;
@@ -130,11 +157,7 @@ __device__ __forceinline__ void half_body(const PassArgs& a, const int slot, con
         tma_load_3d(smem_u32(stg + (size_t)y * G), &wmap, blockIdx.x * lines + wp * G, y, slot, bar);
     }
   }
-  for (int i = threadIdx.x; i < N; i += blockDim.x) {
-    const int k2 = i / N1, tt = i % N1;
-    tw[i] = a.tw[(tt * k2) % N];
-    pfs[i] = a.pf[i];
-  }
+  half_tables<N1, N2>(a.tw, a.pf, twp, pfp);
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int t = AXIS == 0 ? (lane % N1) : (lane / G);
@@ -142,7 +165,7 @@ __device__ __forceinline__ void half_body(const PassArgs& a, const int slot, con
   const int lc = warp * G + gl;
   const int line0 = blockIdx.x * lines;
   const int line = line0 + lc;
-  float2* buf = work + lc * LB::kSize;
+  Pair* buf = reinterpret_cast<Pair*>(work + lc * LB::kSize);
   float2* w = a.wave + (size_t)slot * N * N;
   auto off = [&](int e) -> size_t { return AXIS == 0 ? (size_t)line * N + e : (size_t)e * N + line; };
   Pair p[H];
@@ -166,11 +189,10 @@ __device__ __forceinline__ void half_body(const PassArgs& a, const int slot, con
   }
 
   // ---- finish slice s-1's convolution along this axis
-  half_nat_to_k<N1, N2, -1>(p, t, buf, tw);
+  half_nat_to_k<N1, N2, -1>(p, t, buf, twp);
 #pragma unroll
-  for (int k1 = 0; k1 < N1; ++k1)
-    p[k1] = cmul(p[k1], pfs[korder_index<N1, N2>(t, k1)], pfs[korder_index<N1, N2>(t, N1 + k1)]);
-  half_k_to_nat<N1, N2, +1>(p, t, buf, tw);
+  for (int k1 = 0; k1 < N1; ++k1) p[k1] = cmul_pp(p[k1], pfp[k1 * N1 + t]);
+  half_k_to_nat<N1, N2, +1>(p, t, buf, twp);
 
   // ---- transmission (and the gradient-mode checkpoint)
   {
@@ -202,11 +224,10 @@ __device__ __forceinline__ void half_body(const PassArgs& a, const int slot, con
   }
 
   // ---- start slice s's convolution along this axis
-  half_nat_to_k<N1, N2, -1>(p, t, buf, tw);
+  half_nat_to_k<N1, N2, -1>(p, t, buf, twp);
 #pragma unroll
-  for (int k1 = 0; k1 < N1; ++k1)
-    p[k1] = cmul(p[k1], pfs[korder_index<N1, N2>(t, k1)], pfs[korder_index<N1, N2>(t, N1 + k1)]);
-  half_k_to_nat<N1, N2, +1>(p, t, buf, tw);
+  for (int k1 = 0; k1 < N1; ++k1) p[k1] = cmul_pp(p[k1], pfp[k1 * N1 + t]);
+  half_k_to_nat<N1, N2, +1>(p, t, buf, twp);
 
   // ---- store
   if (AXIS == 0) {
