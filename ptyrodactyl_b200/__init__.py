@@ -68,6 +68,7 @@ from .multislice_recon import (  # noqa: F401
 )
 from .crystal import CrystalData, create_crystal_data, crystal_potential_slices  # noqa: F401
 from .elements import kirkland_parameters, lobato_parameters, single_atom_potential  # noqa: F401
+from .hdf5 import HDF5SchemaError, load_from_h5, save_to_h5  # noqa: F401
 from .ensemble import (  # noqa: F401
     coherence_to_distribution,
     ensemble_axes_for_cbed,
