@@ -766,6 +766,8 @@ def run_serve(args, rank, world, local_rank):
     lat = np.array([r.latency_s for r in srv.finished]) * 1e3
     upd = sum(r.request.updates for r in srv.finished)
     ok = sum(1 for r in srv.finished if r.state == 2)
+    plan = {"probes_64": run_plan_leg(srv, build, mix, dev, max_probes=64),
+            "probes_4": run_plan_leg(srv, build, mix, dev, max_probes=4)}
     srv.close()
     line = {
         "metric": "serving mix: p50/p99 latency and aggregate probe-slice updates/s", "mode": "serve",
@@ -777,8 +779,70 @@ def run_serve(args, rank, world, local_rank):
                    "seed": args.seed, "arena_gb": args.arena_gb, "max_slots": args.max_slots,
                    "admission": "HBM footprint (arena) + wave-slot budget",
                    "targets": "uniform random patterns (gradient cost does not depend on them)"},
+        "batch_plan": plan,
     }
     return line
+
+
+def run_plan_leg(srv, build, mix, dev, jobs=16, max_probes=64, reps=3):
+    """A fixed batch of uneven requests (the first ``jobs`` of the serving mix, each
+    cut to at most ``max_probes`` probes, so the batch is launch-bound like small
+    serving traffic) run twice: through the stepped scheduler (host ticks, staging
+    copies, events; wall time) and as one CUDA-graph replay of the same jobs recorded
+    as a batch plan (``ptyro_plan_*``; device time and wall time). The replay's
+    results are checked bit for bit against the scheduler's."""
+    import torch
+    from ptyrodactyl_b200 import _lib
+
+    lib = _lib.load()
+    specs = [dict(m, num_probes=min(m["num_probes"], max_probes)) for m in mix[:jobs]]
+    reqs = [build(sp, 0.0) for sp in specs]
+    updates = sum(r.updates for r in reqs)
+
+    def scheduled():
+        srv.finished.clear()
+        for r in reqs:
+            srv.submit(r)
+        srv.drain()
+        return {id(res.request): res for res in srv.finished}
+
+    scheduled()  # warm-up
+    walls = []
+    for _ in range(reps):
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        want = scheduled()
+        torch.cuda.synchronize()
+        walls.append(time.perf_counter() - t)
+    plan, results = srv.plan(reqs)
+    before = lib.ptyro_launch_count()
+    plan.launch()
+    torch.cuda.synchronize()
+    launches = int(lib.ptyro_launch_count() - before)
+    plan.capture()
+    plan.replay()
+    torch.cuda.synchronize()
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    dev_ms, plan_walls = [], []
+    for _ in range(reps):
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        s.record()
+        plan.replay()
+        e.record()
+        torch.cuda.synchronize()
+        plan_walls.append(time.perf_counter() - t)
+        dev_ms.append(s.elapsed_time(e))
+    identical = all(torch.equal(res.patterns, want[id(r)].patterns) for r, res in zip(reqs, results))
+    status = plan.status()
+    plan.close()
+    sched_s, plan_s = float(np.median(walls)), float(np.median(plan_walls))
+    return {"jobs": len(reqs), "grad_jobs": sum(1 for r in reqs if r.kind == "grad"),
+            "grids": sorted({r.n for r in reqs}), "probes_per_job_max": max_probes, "updates": updates,
+            "scheduler_wall_ms": sched_s * 1e3, "plan_replay_wall_ms": plan_s * 1e3,
+            "plan_replay_device_ms": float(np.median(dev_ms)), "replay_over_scheduler": sched_s / plan_s,
+            "plan_updates_per_s": updates / plan_s, "kernel_launches_per_replay": launches,
+            "bit_identical_to_scheduler": bool(identical), "device_status": int(status)}
 
 
 # ----------------------------------------------------------------------------- profiling case

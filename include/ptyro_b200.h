@@ -475,7 +475,9 @@ int ptyro_sched_memory(ptyro_sched* s, size_t* free_bytes, int32_t* free_slots);
  * tick's descriptors into the arena (a synchronous copy: call it outside stream
  * capture); ptyro_plan_launch then only enqueues kernels and memsets on `stream`,
  * so it can be captured into a CUDA graph and replayed; each launch recomputes every
- * job from its current inputs. Results are bit-identical to the same jobs run
+ * job from its current inputs. The jobs of each grid edge run on a stream of the
+ * plan's own, forked from `stream` and joined back to it with events (a captured
+ * graph gets one branch per grid edge). Results are bit-identical to the same jobs run
  * through ptyro_sched_*. The arena (DEVICE, 256-byte aligned, ptyro_plan_bytes)
  * holds every job's scratch at once; one launch at a time per plan. */
 typedef struct ptyro_plan ptyro_plan;

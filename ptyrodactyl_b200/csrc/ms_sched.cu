@@ -542,6 +542,7 @@ static int tick_class(ptyro_sched* s, GridClass& c, std::vector<Job*>& jobs) {
 // captured in a CUDA graph and replayed.
 struct PlanOp {
   enum Kind { SETUP, RAMPS, TICK, FOLLOW, EPILOGUE } kind;
+  int cls = 0;   // grid class: the op goes on that class's stream
   int job = -1;  // SETUP, EPILOGUE
   RampReq ramp{};
   Follow follow{};
@@ -553,6 +554,7 @@ struct PlanJobs {
   std::vector<Job> jobs;  // reserved up front: ops hold pointers into it
   std::vector<PlanOp> ops;
   std::vector<char> blob;  // the packed ticks
+  std::vector<int> class_edges;  // grid edge of each class, ascending
   size_t job_bytes = 0;
 };
 
@@ -578,16 +580,24 @@ static int plan_record(const ptyro_job_desc* descs, int num_jobs, char* arena, P
   }
   pj.job_bytes = o;
   char* desc_base = arena ? arena + o : nullptr;
+  std::map<int, int> cls_of;  // grid edge -> class index
+  for (Job& j : pj.jobs) cls_of.emplace(j.plan.p.n, 0);
+  for (auto& kv : cls_of) {
+    kv.second = (int)pj.class_edges.size();
+    pj.class_edges.push_back(kv.first);
+  }
   std::map<int, std::vector<Job*>> classes;
   for (Job& j : pj.jobs) {
     PlanOp op;
     op.kind = PlanOp::SETUP;
+    op.cls = cls_of[j.plan.p.n];
     op.job = (int)j.id;
     pj.ops.push_back(op);
     job_start(j);
     if (!j.issued_all) classes[j.plan.p.n].push_back(&j);
   }
   for (auto& kv : classes) {
+    const int cls = cls_of[kv.first];
     for (;;) {
       std::vector<Job*> running;
       for (Job* j : kv.second)
@@ -600,6 +610,7 @@ static int plan_record(const ptyro_job_desc* descs, int num_jobs, char* arena, P
       for (const RampReq& r : ramps) {
         PlanOp op;
         op.kind = PlanOp::RAMPS;
+        op.cls = cls;
         op.ramp = r;
         pj.ops.push_back(op);
       }
@@ -607,18 +618,21 @@ static int plan_record(const ptyro_job_desc* descs, int num_jobs, char* arena, P
       pj.blob.resize(off + tick_bytes(t));
       PlanOp tick;
       tick.kind = PlanOp::TICK;
+      tick.cls = cls;
       tick.n = kv.first;
       tick.q = pack_tick(t, pj.blob.data() + off, desc_base + off);
       pj.ops.push_back(tick);
       for (const Follow& fl : follow) {
         PlanOp op;
         op.kind = PlanOp::FOLLOW;
+        op.cls = cls;
         op.follow = fl;
         pj.ops.push_back(op);
         if (job_advance(*fl.j)) {
           fl.j->issued_all = true;
           PlanOp ep;
           ep.kind = PlanOp::EPILOGUE;
+          ep.cls = cls;
           ep.job = (int)fl.j->id;
           pj.ops.push_back(ep);
         }
@@ -630,9 +644,21 @@ static int plan_record(const ptyro_job_desc* descs, int num_jobs, char* arena, P
 
 }  // namespace ptyro
 
+// Grid classes run on their own streams, forked from and joined back to the launch
+// stream with events (under stream capture the graph gets one branch per class).
 struct ptyro_plan {
   int device = 0;
   ptyro::PlanJobs pj;
+  std::vector<cudaStream_t> streams;  // one per grid class
+  std::vector<cudaEvent_t> joins;     // one per grid class
+  cudaEvent_t fork = nullptr;
+  ~ptyro_plan() {
+    for (cudaStream_t s : streams)
+      if (s) cudaStreamDestroy(s);
+    for (cudaEvent_t e : joins)
+      if (e) cudaEventDestroy(e);
+    if (fork) cudaEventDestroy(fork);
+  }
 };
 
 extern "C" {
@@ -664,6 +690,18 @@ int ptyro_plan_create(int32_t device, const ptyro_job_desc* jobs, int32_t num_jo
       cudaMemcpy((char*)arena + plan->pj.job_bytes, plan->pj.blob.data(), plan->pj.blob.size(),
                  cudaMemcpyHostToDevice) != cudaSuccess)
     return fail(PTYRO_ERR_CUDA, "plan descriptor upload failed");
+  if (cudaEventCreateWithFlags(&plan->fork, cudaEventDisableTiming) != cudaSuccess)
+    return fail(PTYRO_ERR_CUDA, "cudaEventCreateWithFlags failed");
+  for (size_t c = 0; c < plan->pj.class_edges.size(); ++c) {
+    cudaStream_t cs = nullptr;
+    cudaEvent_t ev = nullptr;
+    if (cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) != cudaSuccess)
+      return fail(PTYRO_ERR_CUDA, "cudaStreamCreateWithFlags failed");
+    plan->streams.push_back(cs);
+    if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess)
+      return fail(PTYRO_ERR_CUDA, "cudaEventCreateWithFlags failed");
+    plan->joins.push_back(ev);
+  }
   *out = plan.release();
   return PTYRO_OK;
 }
@@ -675,18 +713,29 @@ int ptyro_plan_launch(ptyro_plan* plan, void* stream) {
   cudaGetDevice(&cur);
   if (cur != plan->device) return fail(PTYRO_ERR_INVALID, "launch the plan with its device current");
   cudaStream_t st = (cudaStream_t)stream;
+  if (cudaEventRecord(plan->fork, st) != cudaSuccess) return fail(PTYRO_ERR_CUDA, "plan fork: cudaEventRecord failed");
+  for (cudaStream_t cs : plan->streams)
+    if (cudaStreamWaitEvent(cs, plan->fork, 0) != cudaSuccess)
+      return fail(PTYRO_ERR_CUDA, "plan fork: cudaStreamWaitEvent failed");
   int rc = PTYRO_OK;
   for (const PlanOp& op : plan->pj.ops) {
+    cudaStream_t cs = plan->streams[op.cls];
     switch (op.kind) {
-      case PlanOp::SETUP: rc = job_setup(plan->pj.jobs[op.job], st); break;
-      case PlanOp::RAMPS: rc = launch_ramps(op.ramp, st); break;
-      case PlanOp::TICK: rc = launch_tick(op.n, op.q, st); break;
-      case PlanOp::FOLLOW: rc = launch_follow(op.follow, st); break;
-      case PlanOp::EPILOGUE: rc = job_epilogue(plan->pj.jobs[op.job], st); break;
+      case PlanOp::SETUP: rc = job_setup(plan->pj.jobs[op.job], cs); break;
+      case PlanOp::RAMPS: rc = launch_ramps(op.ramp, cs); break;
+      case PlanOp::TICK: rc = launch_tick(op.n, op.q, cs); break;
+      case PlanOp::FOLLOW: rc = launch_follow(op.follow, cs); break;
+      case PlanOp::EPILOGUE: rc = job_epilogue(plan->pj.jobs[op.job], cs); break;
     }
-    if (rc) return rc;
+    if (rc) break;
   }
-  return PTYRO_OK;
+  // join every class stream back to the launch stream, also after a failed launch
+  for (size_t c = 0; c < plan->streams.size(); ++c) {
+    if (cudaEventRecord(plan->joins[c], plan->streams[c]) != cudaSuccess ||
+        cudaStreamWaitEvent(st, plan->joins[c], 0) != cudaSuccess)
+      return rc ? rc : fail(PTYRO_ERR_CUDA, "plan join failed");
+  }
+  return rc;
 }
 
 int ptyro_plan_job_status(const ptyro_plan* plan, int32_t job, void** status_word) {
