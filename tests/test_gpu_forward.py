@@ -225,8 +225,13 @@ def test_errors_raise_value_error():
     mic = pb.create_microscope_config(100.0, 20.0, probe_shape=(48, 48))
     det = pb.create_detector_config(0.2, scan_positions_px=np.zeros((1, 2)))
     beam = pb.create_probe_modes(np.ones((48, 48, 1), np.complex64), [1.0], 0.2)
-    with pytest.raises(ValueError):
-        pb.stem_4d(slices, beam, mic, det)
+    assert tuple(pb.stem_4d(slices, beam, mic, det).data.shape) == (1, 48, 48)  # any grid runs
+    beam64 = pb.create_probe_modes(np.ones((64, 64, 1), np.complex64), [1.0], 0.2)
+    with pytest.raises(ValueError):  # a potential smaller than the beam's grid
+        pb.stem_4d(slices, beam64, mic, det)
+    wide = pb.create_potential_slices(np.zeros((5000, 3, 1)), 1.0, 0.2)
+    with pytest.raises(ValueError, match="4096"):
+        pb.stem_4d(wide, pb.create_probe_modes(np.ones((5000, 3, 1), np.complex64), [1.0], 0.2), mic, det)
     det2 = pb.create_detector_config(0.2)
     with pytest.raises(ValueError, match="scan_positions_px is required"):
         pb.stem_4d(slices, beam, mic, det2)
