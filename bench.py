@@ -469,7 +469,8 @@ def run_grad(args, rank, world, local_rank):
     lib = _lib.load()
     w = synth.CONFIG4
     n, S, P, F = w.n, w.num_slices, w.num_probes, w.field_n
-    win = torch.as_tensor(w.windows(), device=dev)
+    P = min(P, args.probes) if args.probes else P  # --probes: the first P scan windows (profiling cases)
+    win = torch.as_tensor(w.windows()[:P], device=dev).contiguous()
     pos = torch.zeros((P, 2), dtype=torch.float64, device=dev)
     mic = pb.create_microscope_config(w.voltage_kv, w.aperture_mrad, w.defocus_ang, w.c3_ang, probe_shape=(n, n))
     probe = pb.make_probe(mic, pb.create_detector_config(w.calib))[..., None].contiguous()
@@ -941,7 +942,7 @@ def main():
                     default="forward")
     ap.add_argument("--probes", type=int, default=0,
                     help="config3 mode: scan positions sampled (0: the full 128x128 scan); profile-case mode: "
-                         "probes in the one batch (0: 2048)")
+                         "probes in the one batch (0: 2048); grad mode: the first scan windows (0: all 1024)")
     ap.add_argument("--grid", type=int, default=256, help="profile-case mode: grid edge")
     ap.add_argument("--reps", type=int, default=1, help="profile-case mode: steady passes per axis")
     ap.add_argument("--slices", type=int, default=2, help="profile-case mode: slices of the forward")

@@ -711,71 +711,99 @@ static __global__ void k_reduce_dv(const float* __restrict__ contrib, int nslots
   const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nn) return;
   float acc = 0.f;
-  for (int w = 0; w < nslots; ++w) acc += contrib[(size_t)w * nn + i];
+  for (int w = 0; w < nslots; ++w) acc += __ldcs(contrib + (size_t)w * nn + i);  // read once
   const int y = (int)(i / n), x = (int)(i % n);
   dv[(long long)y * sy + (long long)x * sx + (long long)s * ss] += acc;
 }
 
 // Windowed runs: field pixel (fy, fx) of dV_s collects the contribution of every
-// slot whose n x n window (origin modulo F) covers it, added in slot order (no
-// atomics). A CTA covers a TX x TY tile of the field (TX, TY <= n); warp 0 first
-// lists, in slot order, the slots whose window meets the tile (rows and columns;
-// both lengths are at most n, so a window meets the tile iff it holds one of the
-// tile's corner rows and one of its corner columns), then every pixel adds the
-// listed slots whose window covers it. Loads of 8 listed slots are issued together,
-// and neighbouring threads read neighbouring pixels of the same slot plane.
+// slot whose n x n window (origin modulo F) covers it, added in a fixed order (no
+// atomics, deterministic). A CTA covers a TX x TY tile of the field (TX, TY <= n,
+// TX TY = 64). First every thread classifies some of the slots (a window meets the
+// tile iff it holds one of the tile's corner rows and one of its corner columns, both
+// lengths being at most n; it covers the whole tile iff the tile's first row and
+// column sit at least TY rows and TX columns before the window's end), then warp 0
+// lists the meeting slots in slot order with, for a covering slot, the offset of the
+// tile's corner in its contribution plane: its pixels then load at corner + (ty n +
+// tx) with no per-pixel test. A batch's windows cluster (neighbouring scan positions),
+// so central pixels collect many contributions: each pixel's list is split into
+// kReduceQ contiguous parts summed by kReduceQ threads, 8 loads in flight each, and
+// the parts are added in order. Neighbouring threads read neighbouring pixels of the
+// same plane.
+constexpr int kReduceQ = 4;
+
 static __global__ void __launch_bounds__(256) k_reduce_dv_win(const float* __restrict__ contrib, int nb, int M, int n,
                                                        int F, const int* __restrict__ win, float* dv, long long sy,
                                                        long long sx, long long ss, int s, int tx_log2) {
-  extern __shared__ int sh[];
-  int* swx = sh;           // window column origin of each listed slot
-  int* swy = sh + nb;      // window row origin
-  int* sslot = sh + 2 * nb;  // listed slots, ascending
+  extern __shared__ long long shl[];
+  long long* scorner = shl;                                  // listed: plane base (+ tile corner if covering)
+  int2* sorg = reinterpret_cast<int2*>(shl + nb);            // listed: window origin (wy, wx)
+  int2* sall = sorg + nb;                                    // per slot: window origin
+  int* sflag = reinterpret_cast<int*>(sall + nb);            // per slot: 0 misses, 1 meets, 2 covers the tile
+  int* sfull = sflag + nb;                                   // listed: covers the tile
   __shared__ int count;
-  const int TX = 1 << tx_log2, TY = (int)blockDim.x >> tx_log2;
+  __shared__ float part[256];
+  constexpr int kPix = 256 / kReduceQ;  // pixels per tile
+  const int TX = 1 << tx_log2, TY = kPix >> tx_log2;
   const int fx0 = (int)blockIdx.x * TX, fy0 = (int)blockIdx.y * TY;
   const int fm = F - 1;
+  for (int bb = (int)threadIdx.x; bb < nb; bb += (int)blockDim.x) {
+    const int wy = win ? win[2 * bb] : 0, wx = win ? win[2 * bb + 1] : 0;
+    const int ly0 = (fy0 - wy) & fm, lx0 = (fx0 - wx) & fm;
+    const bool rows = ly0 < n || ((fy0 + TY - 1 - wy) & fm) < n;
+    const bool cols = lx0 < n || ((fx0 + TX - 1 - wx) & fm) < n;
+    sall[bb] = make_int2(wy, wx);
+    sflag[bb] = !(rows && cols) ? 0 : (ly0 + TY <= n && lx0 + TX <= n ? 2 : 1);
+  }
+  __syncthreads();
+  const size_t nn = (size_t)n * n;
   if (threadIdx.x < 32) {
     int c = 0;
     for (int b0 = 0; b0 < nb; b0 += 32) {
       const int bb = b0 + (int)threadIdx.x;
-      int wy = 0, wx = 0;
-      if (bb < nb && win) {
-        wy = win[2 * bb];
-        wx = win[2 * bb + 1];
-      }
-      const bool rows = ((fy0 - wy) & fm) < n || ((fy0 + TY - 1 - wy) & fm) < n;
-      const bool cols = ((fx0 - wx) & fm) < n || ((fx0 + TX - 1 - wx) & fm) < n;
-      const bool in = bb < nb && rows && cols;
-      const unsigned mask = __ballot_sync(0xffffffffu, in);
-      if (in) {
+      const int f = bb < nb ? sflag[bb] : 0;
+      const unsigned mask = __ballot_sync(0xffffffffu, f != 0);
+      if (f) {
         const int pos = c + __popc(mask & ((1u << threadIdx.x) - 1u));
-        sslot[pos] = bb;
-        swx[pos] = wx;
-        swy[pos] = wy;
+        const int2 o = sall[bb];
+        long long base = (long long)bb * M * (long long)nn;
+        if (f == 2) base += (long long)((fy0 - o.x) & fm) * n + ((fx0 - o.y) & fm);
+        scorner[pos] = base;
+        sorg[pos] = o;
+        sfull[pos] = f == 2;
       }
       c += __popc(mask);
     }
     if (threadIdx.x == 0) count = c;
   }
   __syncthreads();
-  const int fx = fx0 + ((int)threadIdx.x & (TX - 1));
-  const int fy = fy0 + ((int)threadIdx.x >> tx_log2);
-  const size_t nn = (size_t)n * n;
+  const int pix = (int)threadIdx.x & (kPix - 1), q = (int)threadIdx.x / kPix;
+  const int tx = pix & (TX - 1), ty = pix >> tx_log2;
+  const int fx = fx0 + tx, fy = fy0 + ty;
+  const int toff = ty * n + tx;
   const int cnt = count;
+  const int kb = (int)(((long long)cnt * q) / kReduceQ), ke = (int)(((long long)cnt * (q + 1)) / kReduceQ);
   float acc = 0.f;
-  for (int k0 = 0; k0 < cnt; k0 += 8) {
+  for (int k0 = kb; k0 < ke; k0 += 8) {
     float v[8];
 #pragma unroll
     for (int u = 0; u < 8; ++u) {
       const int k = k0 + u;
       v[u] = 0.f;
-      if (k < cnt) {
-        const int ly = (fy - swy[k]) & fm, lx = (fx - swx[k]) & fm;
-        if (ly < n && lx < n) {
-          const float* cp = contrib + (size_t)sslot[k] * M * nn + (size_t)ly * n + lx;
-          float t = cp[0];
-          for (int m = 1; m < M; ++m) t += cp[(size_t)m * nn];
+      if (k < ke) {
+        const float* cp;
+        bool ok = true;
+        if (sfull[k]) {
+          cp = contrib + scorner[k] + toff;
+        } else {
+          const int2 o = sorg[k];
+          const int ly = (fy - o.x) & fm, lx = (fx - o.y) & fm;
+          ok = (ly | lx) < n;  // n is a power of two
+          cp = contrib + scorner[k] + (long long)ly * n + lx;
+        }
+        if (ok) {  // contributions are read once
+          float t = __ldcs(cp);
+          for (int m = 1; m < M; ++m) t += __ldcs(cp + (size_t)m * nn);
           v[u] = t;
         }
       }
@@ -783,23 +811,30 @@ static __global__ void __launch_bounds__(256) k_reduce_dv_win(const float* __res
 #pragma unroll
     for (int u = 0; u < 8; ++u) acc += v[u];
   }
-  dv[(long long)fy * sy + (long long)fx * sx + (long long)s * ss] += acc;
+  part[threadIdx.x] = acc;
+  __syncthreads();
+  if (q == 0) {
+    float sum = part[pix];
+#pragma unroll
+    for (int r = 1; r < kReduceQ; ++r) sum += part[r * kPix + pix];
+    dv[(long long)fy * sy + (long long)fx * sx + (long long)s * ss] += sum;
+  }
 }
 
 static int launch_reduce_dv_win(const float* contrib, int nb, int M, int n, int F, const int* win, float* dv,
                                 long long sy, long long sx, long long ss, int s, cudaStream_t st) {
-  // tile TX x TY = 256 pixels with TX, TY <= n (n and F are powers of two, n >= 16)
+  // tile TX x TY = 256 / kReduceQ pixels with TX, TY <= n (n and F are powers of two, n >= 16)
   const int tx = n < 32 ? n : 32;
   int tx_log2 = 0;
   while ((1 << tx_log2) < tx) ++tx_log2;
-  const int ty = 256 / tx;
-  constexpr int kChunk = 2048;  // probes listed per launch (24 KB of shared memory)
+  const int ty = (256 / kReduceQ) / tx;
+  constexpr int kChunk = 1024;  // probes listed per launch (32 bytes of shared memory each)
   const dim3 grid((unsigned)(F / tx), (unsigned)(F / ty));
   for (int c0 = 0; c0 < nb; c0 += kChunk) {  // chunks add into dv in probe order
     const int cn = nb - c0 < kChunk ? nb - c0 : kChunk;
-    k_reduce_dv_win<<<grid, 256, 3 * sizeof(int) * (size_t)cn, st>>>(
-        contrib + (size_t)c0 * M * n * n, cn, M, n, F, win ? win + 2 * (size_t)c0 : nullptr, dv, sy, sx, ss, s,
-        tx_log2);
+    k_reduce_dv_win<<<grid, 256, 32 * (size_t)cn, st>>>(contrib + (size_t)c0 * M * n * n, cn, M, n, F,
+                                                         win ? win + 2 * (size_t)c0 : nullptr, dv, sy, sx, ss, s,
+                                                         tx_log2);
     int rc = check_launch("k_reduce_dv_win");
     if (rc) return rc;
   }

@@ -18,6 +18,12 @@
 
 namespace ptyro {
 
+// Asynchronous prefetch of `bytes` (a multiple of 16, 16-byte aligned) of global
+// memory into L2; nothing is written to shared memory and nothing waits on it.
+__device__ __forceinline__ void prefetch_l2_bulk(const void* src, uint32_t bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes) : "memory");
+}
+
 // a * conj(w) with a different w per line: the operations of cmulc(Pair, w) per lane
 __device__ __forceinline__ Pair cmulc(Pair a, float2 wa, float2 wb) {
   const float2 wx = make_float2(wa.x, wb.x), wy = make_float2(wa.y, wb.y);
@@ -48,6 +54,22 @@ __device__ __forceinline__ void bwd_lam_body(const BwdArgs& a, const int slot) {
   const size_t NN = (size_t)N * N;
   const int b = slot / a.n_modes, m = slot % a.n_modes;
   float2* Wl = a.lam + (size_t)slot * NN;
+  // the stored wave phi_s of the CTA's lines, wanted after the first transform: its
+  // DRAM latency overlaps that transform (rows: one contiguous block; columns: one
+  // row segment of the CTA's columns per thread)
+  if (a.t_slice >= 0) {
+    const float2* ck0 = a.ckpt + (size_t)slot * a.res_stride;
+    const int line0 = blockIdx.x * lines;
+    if (AXIS == 0) {
+      constexpr uint32_t kChunk = 4096;
+      constexpr uint32_t kBytes = sizeof(float2) * (uint32_t)lines * N;
+      if (threadIdx.x < kBytes / kChunk)
+        prefetch_l2_bulk(reinterpret_cast<const char*>(ck0 + (size_t)line0 * N) + threadIdx.x * kChunk, kChunk);
+    } else {
+      for (int e = threadIdx.x; e < N; e += blockDim.x)
+        prefetch_l2_bulk(ck0 + (size_t)e * N + line0, sizeof(float2) * lines);
+    }
+  }
   const bool korder_in = a.init || a.op1 == OP_IFFT;
   Pair v[N2];
 
@@ -60,8 +82,8 @@ __device__ __forceinline__ void bwd_lam_body(const BwdArgs& a, const int slot) {
 #pragma unroll
     for (int r = 0; r < N2; ++r) {
       const int k = korder_index<N1, N2>(t, r), kq = (k + N / 2) % N;
-      const float2 aa = A[AXIS == 0 ? (size_t)la * N + k : (size_t)k * N + la];
-      const float2 ab = A[AXIS == 0 ? (size_t)lb * N + k : (size_t)k * N + lb];
+      const float2 aa = __ldcs(A + (AXIS == 0 ? (size_t)la * N + k : (size_t)k * N + la));
+      const float2 ab = __ldcs(A + (AXIS == 0 ? (size_t)lb * N + k : (size_t)k * N + lb));
       const float ga = AXIS == 0 ? g[(size_t)ksa * N + kq] : g[(size_t)kq * N + ksa];
       const float gb = AXIS == 0 ? g[(size_t)ksb * N + kq] : g[(size_t)kq * N + ksb];
       v[r] = make_pair(cscale(aa, s * ga), cscale(ab, s * gb));
@@ -89,7 +111,9 @@ __device__ __forceinline__ void bwd_lam_body(const BwdArgs& a, const int slot) {
   }
 
   // ---- slice point: dV contribution from the stored wave phi_s (stored at once, so
-  // it holds no registers through the second transform), then conj(T_s)
+  // it holds no registers through the second transform), then conj(T_s). phi_s is
+  // read and the contribution written with streaming hints (each is touched once), so
+  // that the batch's lambda slots stay in L2 between passes.
   if (a.t_slice >= 0) {
     const float2* ck = a.ckpt + (size_t)slot * a.res_stride;
     float* C = a.contrib ? a.contrib + (size_t)slot * NN : nullptr;
@@ -98,10 +122,10 @@ __device__ __forceinline__ void bwd_lam_body(const BwdArgs& a, const int slot) {
       const int e = t + N1 * j;
       float2 pa, pb;
       if (AXIS == 0) {
-        pa = ck[(size_t)la * N + e];
-        pb = ck[(size_t)lb * N + e];
+        pa = __ldcs(ck + (size_t)la * N + e);
+        pb = __ldcs(ck + (size_t)lb * N + e);
       } else {
-        const float4 q = *reinterpret_cast<const float4*>(ck + (size_t)e * N + la);
+        const float4 q = __ldcs(reinterpret_cast<const float4*>(ck + (size_t)e * N + la));
         pa = make_float2(q.x, q.y);
         pb = make_float2(q.z, q.w);
       }
@@ -109,10 +133,10 @@ __device__ __forceinline__ void bwd_lam_body(const BwdArgs& a, const int slot) {
       const float cvb = a.sigma2 * (pb.x * v[j].im.y - pb.y * v[j].re.y);
       if (C) {
         if (AXIS == 0) {
-          C[(size_t)la * N + e] = cva;
-          C[(size_t)lb * N + e] = cvb;
+          __stcs(C + (size_t)la * N + e, cva);
+          __stcs(C + (size_t)lb * N + e, cvb);
         } else {
-          *reinterpret_cast<float2*>(C + (size_t)e * N + la) = make_float2(cva, cvb);
+          __stcs(reinterpret_cast<float2*>(C + (size_t)e * N + la), make_float2(cva, cvb));
         }
       }
     }

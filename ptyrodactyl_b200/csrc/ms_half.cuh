@@ -217,8 +217,8 @@ __device__ __forceinline__ void half_body(const PassArgs& a, const int slot, con
       float2* ck = a.ckpt_store + (size_t)slot * a.res_stride;
 #pragma unroll
       for (int j = 0; j < H; ++j) {
-        ck[off(t + N1 * j)] = pair_a(p[j]);
-        ck[off(t + N1 * (j + H))] = pair_b(p[j]);
+        __stcs(ck + off(t + N1 * j), pair_a(p[j]));  // read once, by the adjoint
+        __stcs(ck + off(t + N1 * (j + H)), pair_b(p[j]));
       }
     }
   }

@@ -229,12 +229,14 @@ __device__ __forceinline__ void pair_body(const PassArgs& a, const int slot, con
     float2* ck = a.ckpt_store + (size_t)slot * a.res_stride;
 #pragma unroll
     for (int j = 0; j < N2; ++j) {
+      // streaming stores: the residuals are read once, by the adjoint, and must not
+      // push the batch's wave slots out of L2
       if (AXIS == 0) {
-        ck[(size_t)la * N + t + N1 * j] = pair_a(v[j]);
-        ck[(size_t)lb * N + t + N1 * j] = pair_b(v[j]);
+        __stcs(ck + (size_t)la * N + t + N1 * j, pair_a(v[j]));
+        __stcs(ck + (size_t)lb * N + t + N1 * j, pair_b(v[j]));
       } else {
-        *reinterpret_cast<float4*>(ck + (size_t)(t + N1 * j) * N + la) =
-            make_float4(v[j].re.x, v[j].im.x, v[j].re.y, v[j].im.y);
+        __stcs(reinterpret_cast<float4*>(ck + (size_t)(t + N1 * j) * N + la),
+               make_float4(v[j].re.x, v[j].im.x, v[j].re.y, v[j].im.y));
       }
     }
   }

@@ -319,7 +319,7 @@ __device__ __forceinline__ void pass_body(const PassArgs& a, const int yslot) {
       if (a.ckpt_store) {
         float2* ck = a.ckpt_store + (size_t)slot * a.res_stride;
 #pragma unroll
-        for (int j = 0; j < N2; ++j) ck[off(t + N1 * j)] = v[j];
+        for (int j = 0; j < N2; ++j) __stcs(ck + off(t + N1 * j), v[j]);  // read once, by the adjoint
       }
     }
     // ---- op2
