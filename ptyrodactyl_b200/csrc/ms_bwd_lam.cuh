@@ -11,7 +11,10 @@
 // of every adjoint pass; each paired operation rounds as the lockstep kernel's lambda
 // half does, so the gradients are bit-identical to the lockstep adjoint at spacing 1.
 // Row passes read and write lines directly; column passes read and write the two
-// neighbouring columns of a lane pair as 16-byte pieces.
+// neighbouring columns of a lane pair as 16-byte pieces, or (TMA, 256^2, as the
+// forward's paired column pass) move each warp's block of 2 G columns x N rows of
+// lambda with one tiled TMA copy into and out of its own exchange buffers, with the
+// bounded mbarrier wait of warp_wait_tile.
 #pragma once
 #include "ms_bwd.cuh"
 #include "ms_pair.cuh"
@@ -30,15 +33,35 @@ __device__ __forceinline__ Pair cmulc(Pair a, float2 wa, float2 wb) {
   return {__ffma2_rn(a.re, wx, __fmul2_rn(a.im, wy)), __ffma2_rn(a.im, wx, __fmul2_rn(a.re, make_float2(-wa.y, -wb.y)))};
 }
 
-template <int N1, int N2, int AXIS, int WARPS>
-__device__ __forceinline__ void bwd_lam_body(const BwdArgs& a, const int slot) {
+template <int N1, int N2, int AXIS, int WARPS, bool TMA>
+__device__ __forceinline__ void bwd_lam_body(const BwdArgs& a, const int slot, const CUtensorMap& lmap) {
   using PG = PairGeom<N1, N2, WARPS>;
   using PB = PairBuf<N1, N2>;
   constexpr int N = PG::N, G = PG::G, lines = PG::kLines;
+  static_assert(!TMA || (AXIS == 1 && N <= 256), "TMA moves whole columns of a column pass");
+  constexpr uint32_t kWarpBytes = sizeof(float2) * 2 * G * N;  // one warp's column block
+  static_assert(!TMA || sizeof(Pair) * G * PB::kSize >= kWarpBytes + 127,
+                "the warp's exchange buffers must hold its column block at 128-byte alignment");
+  __shared__ __align__(8) uint64_t tma_bar[TMA ? WARPS : 1];
   extern __shared__ float4 smem4[];
   float2* tw = reinterpret_cast<float2*>(smem4);  // tw[k2 * N1 + t] = W_N^{t k2}
   float2* pfs = tw + N;                           // propagator factor / N
   Pair* xbuf = reinterpret_cast<Pair*>(pfs + N);
+  // TMA staging: this warp's exchange buffers, rounded up to 128 bytes; [row][2 G columns]
+  float2* stg = nullptr;
+  uint32_t bar = 0;
+  if (TMA) {
+    const int wp = threadIdx.x >> 5;
+    const uintptr_t base = reinterpret_cast<uintptr_t>(xbuf + (size_t)(wp * G) * PB::kSize);
+    stg = reinterpret_cast<float2*>((base + 127) & ~(uintptr_t)127);
+    bar = smem_u32(&tma_bar[wp]);
+    if ((threadIdx.x & 31) == 0) {
+      mbar_init(bar, 1);
+      asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+      mbar_expect_tx(bar, kWarpBytes);
+      tma_load_3d(smem_u32(stg), &lmap, blockIdx.x * lines + wp * 2 * G, 0, slot, bar);
+    }
+  }
   for (int i = threadIdx.x; i < N; i += blockDim.x) {
     const int k2 = i / N1, tt = i % N1;
     tw[i] = a.tw[(tt * k2) % N];
@@ -89,13 +112,16 @@ __device__ __forceinline__ void bwd_lam_body(const BwdArgs& a, const int slot) {
       v[r] = make_pair(cscale(aa, s * ga), cscale(ab, s * gb));
     }
   } else {
+    // a warp whose copy never landed leaves its lines untouched (no barrier follows)
+    if (TMA && !warp_wait_tile(bar, kTileWaitPolls, a.status)) return;
 #pragma unroll
     for (int r = 0; r < N2; ++r) {
       const int e = korder_in ? korder_index<N1, N2>(t, r) : t + N1 * r;
       if (AXIS == 0) {
         v[r] = make_pair(Wl[(size_t)la * N + e], Wl[(size_t)lb * N + e]);
       } else {
-        const float4 q = *reinterpret_cast<const float4*>(Wl + (size_t)e * N + la);
+        const float4 q = TMA ? *reinterpret_cast<const float4*>(stg + (size_t)e * (2 * G) + 2 * gl)
+                             : *reinterpret_cast<const float4*>(Wl + (size_t)e * N + la);
         v[r] = {make_float2(q.x, q.z), make_float2(q.y, q.w)};
       }
     }
@@ -164,6 +190,22 @@ __device__ __forceinline__ void bwd_lam_body(const BwdArgs& a, const int slot) {
   }
 
   // ---- store lambda
+  if (TMA) {
+    __syncwarp();  // every lane has read the last exchange
+#pragma unroll
+    for (int r = 0; r < N2; ++r) {
+      const int e = lam_k ? korder_index<N1, N2>(t, r) : t + N1 * r;
+      *reinterpret_cast<float4*>(stg + (size_t)e * (2 * G) + 2 * gl) =
+          make_float4(v[r].re.x, v[r].im.x, v[r].re.y, v[r].im.y);
+    }
+    fence_proxy_async_smem();
+    __syncwarp();
+    if (lane == 0) {
+      tma_store_3d(&lmap, la, 0, slot, smem_u32(stg));
+      tma_store_wait_read();
+    }
+    return;
+  }
 #pragma unroll
   for (int r = 0; r < N2; ++r) {
     const int e = lam_k ? korder_index<N1, N2>(t, r) : t + N1 * r;
@@ -176,9 +218,9 @@ __device__ __forceinline__ void bwd_lam_body(const BwdArgs& a, const int slot) {
   }
 }
 
-template <int N1, int N2, int AXIS, int WARPS, int MINB>
-__global__ void __launch_bounds__(WARPS * 32, MINB) ms_bwd_lam_kernel(BwdArgs a) {
-  bwd_lam_body<N1, N2, AXIS, WARPS>(a, blockIdx.y);
+template <int N1, int N2, int AXIS, int WARPS, int MINB, bool TMA = false>
+__global__ void __launch_bounds__(WARPS * 32, MINB) ms_bwd_lam_kernel(BwdArgs a, const __grid_constant__ CUtensorMap lmap) {
+  bwd_lam_body<N1, N2, AXIS, WARPS, TMA>(a, blockIdx.y, lmap);
 }
 
 }  // namespace ptyro

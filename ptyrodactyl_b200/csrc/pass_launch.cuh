@@ -126,27 +126,40 @@ int launch_bwd_w(const BwdArgs& a, int grid_y, cudaStream_t st, const CUtensorMa
 }
 
 // The lambda-only adjoint pass (ms_bwd_lam.cuh): two lines per thread, direct access.
-template <int N1, int N2, int AXIS>
-int launch_bwd_lam_t(const BwdArgs& a, int grid_y, cudaStream_t st) {
+template <int N1, int N2, int AXIS, bool TMA>
+int launch_bwd_lam_w(const BwdArgs& a, int grid_y, cudaStream_t st, const CUtensorMap* lmap = nullptr) {
   constexpr int N = N1 * N2, G = 32 / N1;
   constexpr int W = N / (2 * G) < 8 ? N / (2 * G) : 8;  // line pairs per CTA tile the grid
   using PG = PairGeom<N1, N2, W>;
   const size_t smem = sizeof(float2) * 2 * (size_t)N + PG::kXbuf;
   static DeviceOnce attr_done;  // per device: the attribute is per-device state
   if (attr_done.first())
-    cudaFuncSetAttribute(ms_bwd_lam_kernel<N1, N2, AXIS, W, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaFuncSetAttribute(ms_bwd_lam_kernel<N1, N2, AXIS, W, 2, TMA>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)smem);
+  static const CUtensorMap kNoMap = {};
   dim3 grid(N / PG::kLines, grid_y);
-  ms_bwd_lam_kernel<N1, N2, AXIS, W, 2><<<grid, W * 32, smem, st>>>(a);
+  ms_bwd_lam_kernel<N1, N2, AXIS, W, 2, TMA><<<grid, W * 32, smem, st>>>(a, lmap ? *lmap : kNoMap);
   g_launches.fetch_add(1, std::memory_order_relaxed);
   return (int)cudaGetLastError();
+}
+
+// lambda-only adjoint passes; variant bit 11 (2048): 256^2 column passes move lambda's
+// column blocks by TMA (not the initial pass, which reads the amplitudes)
+template <int N1, int N2, int AXIS>
+int launch_bwd_lam_t(const BwdArgs& a, int grid_y, cudaStream_t st, int variant) {
+  if constexpr (AXIS == 1 && N1 * N2 == 256) {
+    CUtensorMap lmap;
+    if ((variant & 2048) && !a.init && wave_tensor_map(a.lam, N1 * N2, grid_y, 2 * (32 / N1), &lmap))
+      return launch_bwd_lam_w<N1, N2, AXIS, true>(a, grid_y, st, &lmap);
+  }
+  return launch_bwd_lam_w<N1, N2, AXIS, false>(a, grid_y, st);
 }
 
 // variant bit 11 (2048): 256^2 adjoint column passes move their column blocks by TMA
 template <int N1, int N2, int AXIS>
 int launch_bwd_t(const BwdArgs& a, int grid_y, cudaStream_t st, int variant) {
   if constexpr (N2 <= 16) {  // two lines of lambda fit in a thread's registers
-    if (a.lam_only) return launch_bwd_lam_t<N1, N2, AXIS>(a, grid_y, st);
+    if (a.lam_only) return launch_bwd_lam_t<N1, N2, AXIS>(a, grid_y, st, variant);
   }
   if constexpr (AXIS == 1 && N1 * N2 == 256) {
     CUtensorMap pmap, lmap;
