@@ -704,16 +704,27 @@ static __global__ void k_zero2(float2* d, size_t count) {
     d[i] = make_float2(0.f, 0.f);
 }
 
-// dV_s += sum over slots of the per-slot contributions, in slot order (deterministic).
+// dV_s += sum over slots of the per-slot contributions, in slot order (deterministic),
+// for a group of `planes` contribution planes (plane j, `pstride` floats apart, holds
+// slice s0 - j); four planes are summed together so that their loads overlap.
 static __global__ void k_reduce_dv(const float* __restrict__ contrib, int nslots, int n, float* dv, long long sy,
-                            long long sx, long long ss, int s) {
+                                   long long sx, long long ss, int s0, int planes, long long pstride) {
   const size_t nn = (size_t)n * n;
   const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nn) return;
-  float acc = 0.f;
-  for (int w = 0; w < nslots; ++w) acc += __ldcs(contrib + (size_t)w * nn + i);  // read once
   const int y = (int)(i / n), x = (int)(i % n);
-  dv[(long long)y * sy + (long long)x * sx + (long long)s * ss] += acc;
+  for (int j0 = 0; j0 < planes; j0 += 4) {
+    const int jn = planes - j0 < 4 ? planes - j0 : 4;
+    float acc[4] = {0.f, 0.f, 0.f, 0.f};
+    for (int w = 0; w < nslots; ++w) {
+#pragma unroll
+      for (int jj = 0; jj < 4; ++jj)
+        if (jj < jn) acc[jj] += __ldcs(contrib + (j0 + jj) * pstride + (size_t)w * nn + i);  // read once
+    }
+#pragma unroll
+    for (int jj = 0; jj < 4; ++jj)
+      if (jj < jn) dv[(long long)y * sy + (long long)x * sx + (long long)(s0 - j0 - jj) * ss] += acc[jj];
+  }
 }
 
 // Windowed runs: field pixel (fy, fx) of dV_s collects the contribution of every
@@ -734,7 +745,8 @@ constexpr int kReduceQ = 4;
 
 static __global__ void __launch_bounds__(256) k_reduce_dv_win(const float* __restrict__ contrib, int nb, int M, int n,
                                                        int F, const int* __restrict__ win, float* dv, long long sy,
-                                                       long long sx, long long ss, int s, int tx_log2) {
+                                                       long long sx, long long ss, int s0, int planes,
+                                                       long long pstride, int tx_log2) {
   extern __shared__ long long shl[];
   long long* scorner = shl;                                  // listed: plane base (+ tile corner if covering)
   int2* sorg = reinterpret_cast<int2*>(shl + nb);            // listed: window origin (wy, wx)
@@ -742,7 +754,7 @@ static __global__ void __launch_bounds__(256) k_reduce_dv_win(const float* __res
   int* sflag = reinterpret_cast<int*>(sall + nb);            // per slot: 0 misses, 1 meets, 2 covers the tile
   int* sfull = sflag + nb;                                   // listed: covers the tile
   __shared__ int count;
-  __shared__ float part[256];
+  __shared__ float part[4][256];
   constexpr int kPix = 256 / kReduceQ;  // pixels per tile
   const int TX = 1 << tx_log2, TY = kPix >> tx_log2;
   const int fx0 = (int)blockIdx.x * TX, fy0 = (int)blockIdx.y * TY;
@@ -783,46 +795,66 @@ static __global__ void __launch_bounds__(256) k_reduce_dv_win(const float* __res
   const int toff = ty * n + tx;
   const int cnt = count;
   const int kb = (int)(((long long)cnt * q) / kReduceQ), ke = (int)(((long long)cnt * (q + 1)) / kReduceQ);
-  float acc = 0.f;
-  for (int k0 = kb; k0 < ke; k0 += 8) {
-    float v[8];
+  // planes (slices) four at a time: one listing serves every plane, and each thread
+  // keeps one independent sum per plane in flight
+  for (int j0 = 0; j0 < planes; j0 += 4) {
+    const int jn = planes - j0 < 4 ? planes - j0 : 4;
+    const float* cplane = contrib + j0 * pstride;
+    float acc[4] = {0.f, 0.f, 0.f, 0.f};
+    for (int k0 = kb; k0 < ke; k0 += 8) {
+      float v[8][4];
 #pragma unroll
-    for (int u = 0; u < 8; ++u) {
-      const int k = k0 + u;
-      v[u] = 0.f;
-      if (k < ke) {
-        const float* cp;
-        bool ok = true;
-        if (sfull[k]) {
-          cp = contrib + scorner[k] + toff;
-        } else {
-          const int2 o = sorg[k];
-          const int ly = (fy - o.x) & fm, lx = (fx - o.y) & fm;
-          ok = (ly | lx) < n;  // n is a power of two
-          cp = contrib + scorner[k] + (long long)ly * n + lx;
-        }
-        if (ok) {  // contributions are read once
-          float t = __ldcs(cp);
-          for (int m = 1; m < M; ++m) t += __ldcs(cp + (size_t)m * nn);
-          v[u] = t;
+      for (int u = 0; u < 8; ++u) {
+        const int k = k0 + u;
+#pragma unroll
+        for (int jj = 0; jj < 4; ++jj) v[u][jj] = 0.f;
+        if (k < ke) {
+          long long off;
+          bool ok = true;
+          if (sfull[k]) {
+            off = scorner[k] + toff;
+          } else {
+            const int2 o = sorg[k];
+            const int ly = (fy - o.x) & fm, lx = (fx - o.y) & fm;
+            ok = (ly | lx) < n;  // n is a power of two
+            off = scorner[k] + (long long)ly * n + lx;
+          }
+          if (ok) {
+#pragma unroll
+            for (int jj = 0; jj < 4; ++jj) {
+              if (jj < jn) {  // contributions are read once
+                const float* cp = cplane + jj * pstride + off;
+                float t = __ldcs(cp);
+                for (int m = 1; m < M; ++m) t += __ldcs(cp + (size_t)m * nn);
+                v[u][jj] = t;
+              }
+            }
+          }
         }
       }
+#pragma unroll
+      for (int u = 0; u < 8; ++u)
+#pragma unroll
+        for (int jj = 0; jj < 4; ++jj) acc[jj] += v[u][jj];
     }
 #pragma unroll
-    for (int u = 0; u < 8; ++u) acc += v[u];
-  }
-  part[threadIdx.x] = acc;
-  __syncthreads();
-  if (q == 0) {
-    float sum = part[pix];
+    for (int jj = 0; jj < 4; ++jj) part[jj][threadIdx.x] = acc[jj];
+    __syncthreads();
+    if (q == 0) {
+      for (int jj = 0; jj < jn; ++jj) {
+        float sum = part[jj][pix];
 #pragma unroll
-    for (int r = 1; r < kReduceQ; ++r) sum += part[r * kPix + pix];
-    dv[(long long)fy * sy + (long long)fx * sx + (long long)s * ss] += sum;
+        for (int r = 1; r < kReduceQ; ++r) sum += part[jj][r * kPix + pix];
+        dv[(long long)fy * sy + (long long)fx * sx + (long long)(s0 - j0 - jj) * ss] += sum;
+      }
+    }
+    __syncthreads();  // part is refilled by the next planes
   }
 }
 
 static int launch_reduce_dv_win(const float* contrib, int nb, int M, int n, int F, const int* win, float* dv,
-                                long long sy, long long sx, long long ss, int s, cudaStream_t st) {
+                                long long sy, long long sx, long long ss, int s0, int planes, long long pstride,
+                                cudaStream_t st) {
   // tile TX x TY = 256 / kReduceQ pixels with TX, TY <= n (n and F are powers of two, n >= 16)
   const int tx = n < 32 ? n : 32;
   int tx_log2 = 0;
@@ -833,8 +865,8 @@ static int launch_reduce_dv_win(const float* contrib, int nb, int M, int n, int 
   for (int c0 = 0; c0 < nb; c0 += kChunk) {  // chunks add into dv in probe order
     const int cn = nb - c0 < kChunk ? nb - c0 : kChunk;
     k_reduce_dv_win<<<grid, 256, 32 * (size_t)cn, st>>>(contrib + (size_t)c0 * M * n * n, cn, M, n, F,
-                                                         win ? win + 2 * (size_t)c0 : nullptr, dv, sy, sx, ss, s,
-                                                         tx_log2);
+                                                         win ? win + 2 * (size_t)c0 : nullptr, dv, sy, sx, ss, s0,
+                                                         planes, pstride, tx_log2);
     int rc = check_launch("k_reduce_dv_win");
     if (rc) return rc;
   }
@@ -867,7 +899,12 @@ static __global__ void k_write_grad_modes(const float2* __restrict__ lam_beam, i
 struct BwdLayout {
   size_t status, tw, pf, trans, trans_t, ramp_y, ramp_x, psi, lam, contrib, beam, probe_k, total;
   int batch;
+  int dgroup;  // slices whose dV contributions are kept before one reduction adds them
 };
+
+// Contribution planes kept per batch: the reduction of a group of slices lists each
+// tile's windows once and overlaps the slices' loads.
+constexpr size_t kContribGroupBytes = (size_t)512 << 20;
 
 static BwdLayout bwd_layout_for(const ptyro_ms_params* p) {
   BwdLayout L = {};
@@ -893,7 +930,11 @@ static BwdLayout bwd_layout_for(const ptyro_ms_params* p) {
   L.ramp_x = o; o = align_up(o + 8 * (size_t)p->n * L.batch);
   L.psi = o; o = align_up(o + 8 * nn * slots);
   L.lam = o; o = align_up(o + 8 * nn * slots);
-  L.contrib = o; o = align_up(o + 4 * nn * slots);
+  const size_t plane = 4 * nn * slots;
+  size_t d = kContribGroupBytes / plane;
+  d = d < 1 ? 1 : (d > (size_t)p->num_slices ? (size_t)p->num_slices : d);
+  L.dgroup = (int)(d < 1 ? 1 : d);
+  L.contrib = o; o = align_up(o + plane * L.dgroup);
   L.beam = o; o = align_up(o + 8 * nn * p->num_modes);
   L.probe_k = o; o = align_up(o + 8 * nn * p->num_modes);  // position gradients only
   L.total = o;
@@ -972,6 +1013,8 @@ struct BwdBuffers {
   float2 *psi, *lam;
   float* contrib;
   const float2 *trans, *trans_t, *pf, *tw, *ramp_y, *ramp_x;
+  int dgroup = 1;             // contribution planes: slice point i (in adjoint order) writes plane i % dgroup
+  size_t contrib_plane = 0;   // floats between planes
 };
 
 static BwdPlan bwd_pass_plan(const ptyro_ms_params* p, const BwdBuffers& B, const float* weights,
@@ -1011,7 +1054,7 @@ static BwdPlan bwd_pass_plan(const ptyro_ms_params* p, const BwdBuffers& B, cons
     a.op1 = k == 1 ? OP_IFFT : OP_CONV_CONJ;
     a.t_slice = s;
     a.ckpt = (s % ckpt_every == 0) ? res_base + (size_t)(s / ckpt_every) * nn : nullptr;
-    a.contrib = B.contrib;
+    a.contrib = B.contrib + (size_t)((k - 1) % B.dgroup) * B.contrib_plane;
     a.op2 = k == S ? OP_FFT : OP_CONV_CONJ;
     a.psi_done = k == S;
     a.beam_epi = k == S;
@@ -1055,18 +1098,25 @@ static int weight_grad(const ptyro_ms_params* p, int ckpt_every, const float2* r
   return rc ? fail(rc, "mode-weight gradient: launch failed") : PTYRO_OK;
 }
 
-static int launch_reduce_dv_any(const ptyro_ms_params* p, const float* contrib, int nb, int b0, float* dv, int s,
-                                cudaStream_t st) {
+// dV of a group of `planes` slices (plane j: slice s0 - j, pstride floats apart)
+static int launch_reduce_dv_group(const ptyro_ms_params* p, const float* contrib, int planes, size_t pstride, int nb,
+                                  int b0, float* dv, int s0, cudaStream_t st) {
   const int n = p->n, M = p->num_modes, F = field_of(p);
   const size_t nn = (size_t)n * n;
   if (p->windows != nullptr || F != n) {
     const int* win = p->windows ? (const int*)p->windows + 2 * (size_t)b0 : nullptr;
     return launch_reduce_dv_win(contrib, nb, M, n, F, win, dv, p->pot_stride_y, p->pot_stride_x, p->pot_stride_s,
-                                s, st);
+                                s0, planes, (long long)pstride, st);
   }
   k_reduce_dv<<<(unsigned)((nn + 255) / 256), 256, 0, st>>>(contrib, nb * M, n, dv, p->pot_stride_y,
-                                                             p->pot_stride_x, p->pot_stride_s, s);
+                                                             p->pot_stride_x, p->pot_stride_s, s0, planes,
+                                                             (long long)pstride);
   return check_launch("k_reduce_dv");
+}
+
+static int launch_reduce_dv_any(const ptyro_ms_params* p, const float* contrib, int nb, int b0, float* dv, int s,
+                                cudaStream_t st) {
+  return launch_reduce_dv_group(p, contrib, 1, 0, nb, b0, dv, s, st);
 }
 
 static int backward_impl(const ptyro_ms_params* p, int ckpt_every, const float* potential, const float* weights,
@@ -1119,6 +1169,8 @@ static int backward_impl(const ptyro_ms_params* p, int ckpt_every, const float* 
   B.psi = (float2*)(ws + L.psi);
   B.lam = (float2*)(ws + L.lam);
   B.contrib = (float*)(ws + L.contrib);
+  B.dgroup = L.dgroup;
+  B.contrib_plane = nn * (size_t)L.batch * M;
   B.trans = (const float2*)(ws + L.trans);
   B.trans_t = (const float2*)(ws + L.trans_t);
   B.pf = (const float2*)(ws + L.pf);
@@ -1135,7 +1187,14 @@ static int backward_impl(const ptyro_ms_params* p, int ckpt_every, const float* 
       const BwdPlan b = bwd_pass_plan(p, B, weights, res_base, grad_patterns + (size_t)b0 * nn, ckpt_every, C, b0,
                                       nb, k);
       if ((rc = launch_bwd(n, b.axis, b.a, b.rows, st, p->tune))) return rc;
-      if (b.slice >= 0 && (rc = launch_reduce_dv_any(p, B.contrib, nb, b0, grad_potential, b.slice, st))) return rc;
+      // slice points k = 1 .. S (slice S - k) fill planes (k - 1) % dgroup; a full group,
+      // or the last slice point, is reduced into dV in one launch
+      if (b.slice >= 0 && ((k - 1) % L.dgroup == L.dgroup - 1 || k == S)) {
+        const int i0 = (k - 1) - (k - 1) % L.dgroup;
+        if ((rc = launch_reduce_dv_group(p, B.contrib, k - i0, B.contrib_plane, nb, b0, grad_potential, S - 1 - i0,
+                                         st)))
+          return rc;
+      }
     }
     if (grad_positions) {
       k_position_grad<<<nb, 256, 0, st>>>(B.lam, (const float2*)(ws + L.probe_k), n, M, p->shift_calib_ang,
