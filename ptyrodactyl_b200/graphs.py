@@ -19,7 +19,7 @@ from typing import Optional
 import torch
 
 from . import _lib
-from .simulations import check_windows, ms_params
+from .simulations import check_windows, lane_batch, ms_params
 
 
 class GraphedForward:
@@ -47,6 +47,7 @@ class GraphedForward:
         self.out = torch.empty((num_probes, n, n), dtype=torch.float32, device=dev)
         lanes = max(1, min(int(lanes), max(1, num_probes)))
         bounds = [num_probes * i // lanes for i in range(lanes + 1)]
+        batch = lane_batch(n, modes.shape[2], lanes, batch)  # concurrent lanes share the L2 budget
         self.parts = []  # (lo, hi, params, workspace, bytes)
         for lo, hi in zip(bounds[:-1], bounds[1:]):
             prm = ms_params(n, slices.shape[2], modes.shape[2], hi - lo, voltage_kv, slice_thickness, calib_ang, sc,
