@@ -392,7 +392,8 @@ def run_ours(args, rank, world, local_rank):
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": w.name, "grid": n, "slices": S, "probes_per_gpu": P, "modes": 1,
-                       "batch": batch, "tune": tune, "cuda_graph": bool(args.graph), "lanes": args.lanes if args.graph else 1, "voltage_kv": w.voltage_kv, "aperture_mrad": w.aperture_mrad,
+                       "batch": _batch_of(lib, parts[0][2], n), "tune": tune, "cuda_graph": bool(args.graph),
+                       "lanes": args.lanes if args.graph else 1, "voltage_kv": w.voltage_kv, "aperture_mrad": w.aperture_mrad,
                        "defocus_ang": w.defocus_ang, "c3_ang": w.c3_ang,
                        "l2": "flushed (256 MB write) before every timed step",
                        "parallelism": f"dp{world} (probe shards, no collective)"},
