@@ -105,6 +105,17 @@ int ptyro_ms_forward(const ptyro_ms_params* p, const float* potential, const flo
                      const float* weights, const double* positions, float* patterns,
                      void* workspace, size_t workspace_bytes, void* stream);
 
+/* ptyro_ms_forward whose patterns also stream to host memory: after each probe batch's
+ * pattern pass, the batch's patterns (in `patterns`, device) are copied into
+ * host_patterns ((P, n, n) float32; page-locked for the copies to overlap) on
+ * copy_stream while later batches compute; `stream` waits for the last copy, so work
+ * ordered after the call on `stream` sees every pattern on the host. One setup for all
+ * batches, and only the last batch's copy is not hidden. copy_stream: a stream of its
+ * own (not NULL, not stream); no PTYRO_FLAG_ACCUMULATE; not for stream capture. */
+int ptyro_ms_forward_to_host(const ptyro_ms_params* p, const float* potential, const float* modes,
+                             const float* weights, const double* positions, float* patterns, float* host_patterns,
+                             void* workspace, size_t workspace_bytes, void* stream, void* copy_stream);
+
 /* Residual bytes ptyro_ms_forward_ckpt writes for `p`: per (probe, mode) one
  * complex64 N x N plane per checkpoint (slices 0, K, 2K, ... for K = ckpt_every)
  * plus one plane for the far-field amplitude. */

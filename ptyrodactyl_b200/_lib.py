@@ -30,6 +30,7 @@ EXPORTED_SYMBOLS = (
     "ptyro_last_error",
     "ptyro_ms_workspace_bytes",
     "ptyro_ms_forward",
+    "ptyro_ms_forward_to_host",
     "ptyro_ms_forward_plain",
     "ptyro_make_probe",
     "ptyro_fft_workspace_bytes",
@@ -160,6 +161,8 @@ def _declare(lib) -> None:
     lib.ptyro_last_error.argtypes = []
     lib.ptyro_ms_workspace_bytes.restype = sz
     lib.ptyro_ms_workspace_bytes.argtypes = [pp]
+    lib.ptyro_ms_forward_to_host.restype = ctypes.c_int
+    lib.ptyro_ms_forward_to_host.argtypes = [pp, vp, vp, vp, vp, vp, vp, vp, sz, vp, vp]
     for name in ("ptyro_ms_forward", "ptyro_ms_forward_plain"):
         f = getattr(lib, name)
         f.restype = ctypes.c_int

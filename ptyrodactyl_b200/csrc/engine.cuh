@@ -609,10 +609,35 @@ static int detect_patterns(const float* patterns, int count, int n, const uint32
   return check_launch("k_detect_patterns");
 }
 
+// Patterns streamed to host memory (ptyro_ms_forward_to_host): after each probe batch
+// the batch's patterns are copied on `copy` once `ready` (recorded after the batch's
+// pattern pass) has fired, while later batches compute; at the end the call's stream
+// waits for `copied`, recorded after the last copy. Waits take the event's latest
+// record at the time of the call, so one `ready` event serves every batch.
+struct HostStream {
+  float* host = nullptr;
+  cudaStream_t copy = nullptr;
+  cudaEvent_t ready = nullptr, copied = nullptr;
+  ~HostStream() {
+    if (ready) cudaEventDestroy(ready);
+    if (copied) cudaEventDestroy(copied);
+  }
+};
+
+static int copy_batch_to_host(const HostStream* hs, const float* patterns, int b0, int nb, size_t nn,
+                              cudaStream_t st) {
+  if (!hs) return PTYRO_OK;
+  if (cudaEventRecord(hs->ready, st) != cudaSuccess || cudaStreamWaitEvent(hs->copy, hs->ready, 0) != cudaSuccess ||
+      cudaMemcpyAsync(hs->host + (size_t)b0 * nn, patterns + (size_t)b0 * nn, sizeof(float) * nn * (size_t)nb,
+                      cudaMemcpyDeviceToHost, hs->copy) != cudaSuccess)
+    return fail(PTYRO_ERR_CUDA, "streaming the patterns to host memory failed");
+  return PTYRO_OK;
+}
+
 static int forward_impl(const ptyro_ms_params* p, int ckpt_every, const float* potential, const float* modes,
                         const float* weights, const double* positions, float* patterns, float2* residuals,
                         void* workspace, size_t workspace_bytes, void* stream, const DetOut* det_in = nullptr,
-                        const FwdExtras* ex = nullptr) {
+                        const FwdExtras* ex = nullptr, const HostStream* hs = nullptr) {
   int rc = validate(p);
   if (rc) return rc;
   if (p->num_probes == 0) return PTYRO_OK;
@@ -673,6 +698,7 @@ static int forward_impl(const ptyro_ms_params* p, int ckpt_every, const float* p
       ra.scale = 1.0f / (float)n;
       const int e = launch_resident(n, ra, nb, st);
       if (e != 0) return fail(PTYRO_ERR_CUDA, std::string("ms_resident_kernel: ") + cudaGetErrorString((cudaError_t)e));
+      if ((rc = copy_batch_to_host(hs, patterns, b0, nb, nn, st))) return rc;
       continue;
     }
     for (int k = 0; k <= S + 1; ++k) {
@@ -686,7 +712,10 @@ static int forward_impl(const ptyro_ms_params* p, int ckpt_every, const float* p
                                                                   (p->flags & PTYRO_FLAG_ACCUMULATE) != 0);
       if ((rc = check_launch("k_det_reduce"))) return rc;
     }
+    if ((rc = copy_batch_to_host(hs, patterns, b0, nb, nn, st))) return rc;
   }
+  if (hs && (cudaEventRecord(hs->copied, hs->copy) != cudaSuccess || cudaStreamWaitEvent(st, hs->copied, 0) != cudaSuccess))
+    return fail(PTYRO_ERR_CUDA, "joining the pattern copies failed");
   return PTYRO_OK;
 }
 

@@ -27,6 +27,24 @@ int ptyro_ms_forward(const ptyro_ms_params* p, const float* potential, const flo
                       stream);
 }
 
+int ptyro_ms_forward_to_host(const ptyro_ms_params* p, const float* potential, const float* modes,
+                             const float* weights, const double* positions, float* patterns, float* host_patterns,
+                             void* workspace, size_t workspace_bytes, void* stream, void* copy_stream) {
+  if (!host_patterns) return fail(PTYRO_ERR_INVALID, "host_patterns is NULL");
+  if (p && (p->flags & PTYRO_FLAG_ACCUMULATE))
+    return fail(PTYRO_ERR_INVALID, "an accumulating forward cannot stream its patterns to the host");
+  if (!copy_stream || copy_stream == stream)
+    return fail(PTYRO_ERR_INVALID, "copy_stream must be a stream of its own (not NULL, not stream)");
+  HostStream hs;
+  hs.host = host_patterns;
+  hs.copy = (cudaStream_t)copy_stream;
+  if (cudaEventCreateWithFlags(&hs.ready, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&hs.copied, cudaEventDisableTiming) != cudaSuccess)
+    return fail(PTYRO_ERR_CUDA, "cudaEventCreateWithFlags failed");
+  return forward_impl(p, 0, potential, modes, weights, positions, patterns, nullptr, workspace, workspace_bytes,
+                      stream, nullptr, nullptr, &hs);
+}
+
 size_t ptyro_ms_detect_workspace_bytes(const ptyro_ms_params* p, int32_t num_det) {
   if (validate(p) || num_det < 1 || num_det > PTYRO_MAX_DETECTORS) return 0;
   const Layout L = layout_for(p);

@@ -19,6 +19,7 @@
 #include <math.h>
 
 #include <atomic>
+#include <mutex>
 #include <string>
 
 #include "../../include/ptyro_b200.h"
@@ -164,13 +165,15 @@ int dft_axis(float2* data, int planes, int H, int W, int axis, bool inverse, con
   int L = 6144 / N;  // lines per CTA: two [L][N] buffers of 8 bytes stay within 96 KB
   L = L < 1 ? 1 : (L > 32 ? 32 : L);
   const size_t smem = sizeof(float2) * ((size_t)2 * L * N + N);
-  static bool attr[64] = {};
+  static std::once_flag attr[64];  // per device; concurrent callers wait for the first
   int dev = 0;
   cudaGetDevice(&dev);
-  if (dev >= 0 && dev < 64 && !attr[dev]) {
+  if (dev >= 0 && dev < 64)
+    std::call_once(attr[dev], [] {
+      cudaFuncSetAttribute(k_dft_lines, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    });
+  else
     cudaFuncSetAttribute(k_dft_lines, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    attr[dev] = true;
-  }
   const long long total = (long long)planes * lines;
   k_dft_lines<<<(unsigned)((total + L - 1) / L), 256, smem, st>>>(data, planes, lines, (long long)H * W, ls, es, N,
                                                                   divisor_near_sqrt(N), L, inverse ? 1 : 0, tw);

@@ -164,9 +164,8 @@ template <int N1, int N2, int WARPS>
 static int launch_resident_t(const ResidentArgs& a, int nb, cudaStream_t st) {
   using RG = ResGeom<N1, N2, WARPS>;
   static DeviceOnce attr_done;  // per device: the attribute is per-device state
-  if (attr_done.first())
-    cudaFuncSetAttribute(ms_resident_kernel<N1, N2, WARPS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)RG::kSmem);
+  attr_done.once([&] { cudaFuncSetAttribute(ms_resident_kernel<N1, N2, WARPS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)RG::kSmem); });
   ms_resident_kernel<N1, N2, WARPS><<<nb, WARPS * 32, RG::kSmem, st>>>(a);
   g_launches.fetch_add(1, std::memory_order_relaxed);
   return (int)cudaGetLastError();

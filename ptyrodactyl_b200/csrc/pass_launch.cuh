@@ -19,19 +19,24 @@ namespace ptyro {
 // Number of engine kernels enqueued by this process (all devices, all threads).
 extern std::atomic<unsigned long long> g_launches;
 
-// Per-device "first time" flag for state that CUDA keeps per device, such as a
-// kernel's dynamic shared memory limit (cudaFuncSetAttribute): first() is true once
-// for every device ordinal below kDevices it is called with (the current device),
-// and always for higher ordinals. Two threads may both see true; setting the
-// attribute twice is harmless.
+// Per-device one-time setup for state that CUDA keeps per device, such as a kernel's
+// dynamic shared memory limit (cudaFuncSetAttribute): once(f) runs f once for every
+// device ordinal below kDevices (the current device), and every time for higher
+// ordinals. Threads that launch on the same device at once (one per lane) wait for
+// the first call to finish, so none launches before the attribute is set.
 struct DeviceOnce {
   static constexpr int kDevices = 64;
-  std::atomic<unsigned long long> mask{0};
-  bool first() {
+  std::once_flag flag[kDevices];
+  // runs f once per device; callers on that device that arrive meanwhile wait until it
+  // has returned (so no thread launches before the attribute is set)
+  template <class F>
+  void once(F&& f) {
     int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kDevices) return true;
-    const unsigned long long bit = 1ull << dev;
-    return (mask.fetch_or(bit, std::memory_order_relaxed) & bit) == 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kDevices) {
+      f();
+      return;
+    }
+    std::call_once(flag[dev], f);
   }
 };
 
@@ -94,10 +99,10 @@ int launch_pass_s(const PassArgs& a, int grid_y, cudaStream_t st) {
   constexpr int W = Geo::kWarps;
   const size_t smem = STEADY ? Geo::smem_bytes_steady(W) : Geo::smem_bytes(W);
   static DeviceOnce attr_done;  // per device: the attribute is per-device state
-  if (attr_done.first()) {
+  attr_done.once([&] {
     cudaFuncSetAttribute(ms_pass_kernel<N1, N2, AXIS, W, MINB, STEADY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)smem);
-  }
+  });
   dim3 grid(N / Geo::kLines, grid_y);
   ms_pass_kernel<N1, N2, AXIS, W, MINB, STEADY><<<grid, W * 32, smem, st>>>(a);
   g_launches.fetch_add(1, std::memory_order_relaxed);
@@ -113,10 +118,10 @@ int launch_bwd_w(const BwdArgs& a, int grid_y, cudaStream_t st, const CUtensorMa
   constexpr int MINB = N2 <= 16 ? 2 : 1;  // two resident CTAs where the register budget allows
   const size_t smem = bwd_smem_bytes<N1, N2>(W);
   static DeviceOnce attr_done;  // per device: the attribute is per-device state
-  if (attr_done.first()) {
+  attr_done.once([&] {
     cudaFuncSetAttribute(ms_bwd_pass_kernel<N1, N2, AXIS, W, MINB, TMA>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)smem);
-  }
+  });
   static const CUtensorMap kNoMap = {};
   dim3 grid(N / Geo::kLines, grid_y);
   ms_bwd_pass_kernel<N1, N2, AXIS, W, MINB, TMA>
@@ -133,9 +138,8 @@ int launch_bwd_lam_w(const BwdArgs& a, int grid_y, cudaStream_t st, const CUtens
   using PG = PairGeom<N1, N2, W>;
   const size_t smem = sizeof(float2) * 2 * (size_t)N + PG::kXbuf;
   static DeviceOnce attr_done;  // per device: the attribute is per-device state
-  if (attr_done.first())
-    cudaFuncSetAttribute(ms_bwd_lam_kernel<N1, N2, AXIS, W, 2, TMA>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)smem);
+  attr_done.once([&] { cudaFuncSetAttribute(ms_bwd_lam_kernel<N1, N2, AXIS, W, 2, TMA>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)smem); });
   static const CUtensorMap kNoMap = {};
   dim3 grid(N / PG::kLines, grid_y);
   ms_bwd_lam_kernel<N1, N2, AXIS, W, 2, TMA><<<grid, W * 32, smem, st>>>(a, lmap ? *lmap : kNoMap);
@@ -178,10 +182,10 @@ int launch_jvp_t(const JvpArgs& a, int grid_y, cudaStream_t st) {
   constexpr int MINB = N2 <= 16 ? 2 : 1;
   const size_t smem = bwd_smem_bytes<N1, N2>(W);
   static DeviceOnce attr_done;  // per device: the attribute is per-device state
-  if (attr_done.first()) {
+  attr_done.once([&] {
     cudaFuncSetAttribute(ms_jvp_pass_kernel<N1, N2, AXIS, W, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)smem);
-  }
+  });
   dim3 grid(N / Geo::kLines, grid_y);
   ms_jvp_pass_kernel<N1, N2, AXIS, W, MINB><<<grid, W * 32, smem, st>>>(a);
   g_launches.fetch_add(1, std::memory_order_relaxed);
@@ -227,10 +231,10 @@ int launch_pair_w(const PassArgs& a, int grid_y, cudaStream_t st, const CUtensor
   using PG = PairGeom<N1, N2, W, PRE>;
   const size_t smem = PG::smem_bytes();
   static DeviceOnce attr_done;  // per device: the attribute is per-device state
-  if (attr_done.first()) {
+  attr_done.once([&] {
     cudaFuncSetAttribute(ms_pass_pair_kernel<N1, N2, AXIS, W, MINB, PRE, DIRECT, TMA, GEN>,
                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  }
+  });
   static const CUtensorMap kNoMap = {};
   dim3 grid(PG::N / PG::kLines, grid_y);
   ms_pass_pair_kernel<N1, N2, AXIS, W, MINB, PRE, DIRECT, TMA, GEN>
@@ -273,10 +277,10 @@ int launch_half_w(const PassArgs& a, int grid_y, cudaStream_t st, const CUtensor
   constexpr int W = Geo::kWarps;
   const size_t smem = Geo::smem_bytes(W);
   static DeviceOnce attr_done;  // per device: the attribute is per-device state
-  if (attr_done.first()) {
+  attr_done.once([&] {
     cudaFuncSetAttribute(ms_pass_half_kernel<N1, N2, AXIS, W, MINB, TMA>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)smem);
-  }
+  });
   static const CUtensorMap kNoMap = {};
   dim3 grid(Geo::N / Geo::kLines, grid_y);
   ms_pass_half_kernel<N1, N2, AXIS, W, MINB, TMA><<<grid, W * 32, smem, st>>>(a, wmap ? *wmap : kNoMap);
@@ -339,10 +343,10 @@ int launch_pass_multi_t(const PassArgs* descs, const int2* rows, int nrows, cuda
   constexpr int W = Geo::kWarps;
   const size_t smem = Geo::smem_bytes(W);
   static DeviceOnce attr_done;  // per device: the attribute is per-device state
-  if (attr_done.first()) {
+  attr_done.once([&] {
     cudaFuncSetAttribute(ms_pass_multi_kernel<N1, N2, AXIS, W, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)smem);
-  }
+  });
   dim3 grid(Geo::N / Geo::kLines, nrows);
   ms_pass_multi_kernel<N1, N2, AXIS, W, MINB><<<grid, W * 32, smem, st>>>(descs, rows);
   g_launches.fetch_add(1, std::memory_order_relaxed);
@@ -359,10 +363,10 @@ int launch_pass_pair_multi_t(const PassArgs* descs, const int2* rows, int nrows,
     constexpr int W = Geo::kWarps;
     const size_t smem = Geo::smem_bytes(W);
     static DeviceOnce attr_done;  // per device: the attribute is per-device state
-    if (attr_done.first()) {
+    attr_done.once([&] {
       cudaFuncSetAttribute(ms_pass_half_multi_kernel<N1, N2, AXIS, W, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)smem);
-    }
+    });
     dim3 grid(Geo::N / Geo::kLines, nrows);
     ms_pass_half_multi_kernel<N1, N2, AXIS, W, 2><<<grid, W * 32, smem, st>>>(descs, rows);
     g_launches.fetch_add(1, std::memory_order_relaxed);
@@ -377,10 +381,10 @@ int launch_pass_pair_multi_t(const PassArgs* descs, const int2* rows, int nrows,
     using PG = PairGeom<N1, N2, W, false>;
     const size_t smem = PG::smem_bytes();
     static DeviceOnce attr_done;  // per device: the attribute is per-device state
-    if (attr_done.first()) {
+    attr_done.once([&] {
       cudaFuncSetAttribute(ms_pass_pair_multi_kernel<N1, N2, AXIS, W, MINB>,
                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    }
+    });
     dim3 grid(N / PG::kLines, nrows);
     ms_pass_pair_multi_kernel<N1, N2, AXIS, W, MINB><<<grid, W * 32, smem, st>>>(descs, rows);
     g_launches.fetch_add(1, std::memory_order_relaxed);
@@ -395,10 +399,10 @@ int launch_bwd_multi_t(const BwdArgs* descs, const int2* rows, int nrows, cudaSt
   constexpr int MINB = N2 <= 16 ? 2 : 1;
   const size_t smem = bwd_smem_bytes<N1, N2>(W);
   static DeviceOnce attr_done;  // per device: the attribute is per-device state
-  if (attr_done.first()) {
+  attr_done.once([&] {
     cudaFuncSetAttribute(ms_bwd_multi_kernel<N1, N2, AXIS, W, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)smem);
-  }
+  });
   dim3 grid(Geo::N / Geo::kLines, nrows);
   ms_bwd_multi_kernel<N1, N2, AXIS, W, MINB><<<grid, W * 32, smem, st>>>(descs, rows);
   g_launches.fetch_add(1, std::memory_order_relaxed);

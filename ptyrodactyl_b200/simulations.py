@@ -10,6 +10,7 @@ from __future__ import annotations
 
 import ctypes
 import math
+import threading
 from typing import Optional
 
 import torch
@@ -302,20 +303,23 @@ def run_forward(slices: torch.Tensor, slice_thickness: float, modes: torch.Tenso
 
 def run_forward_to_host(slices: torch.Tensor, slice_thickness: float, modes: torch.Tensor, weights: torch.Tensor,
                         positions: torch.Tensor, voltage_kv: float, calib_ang: float, shift_calib_ang: float,
-                        host_out: torch.Tensor, chunks: int = 8, lanes: int = 2, tune: Optional[int] = None,
+                        host_out: torch.Tensor, lanes: int = 2, tune: Optional[int] = None,
                         windows: Optional[torch.Tensor] = None,
                         status: Optional[torch.Tensor] = None) -> torch.Tensor:
     """``run_forward`` whose patterns land in a host tensor (pinned for overlap): the
-    probes run as ``chunks`` consecutive ranges on ``lanes`` compute streams, and
-    each range's patterns are copied to the host on a copy stream as soon as the
-    range is done, so the device-to-host transfer overlaps the remaining compute."""
+    probes run as ``lanes`` contiguous ranges, each one forward on a compute stream of
+    its own (``ptyro_ms_forward_to_host``) that copies every probe batch's patterns to
+    the host on a copy stream of its own as soon as the batch is done, so the
+    device-to-host transfer overlaps the remaining compute and only the last batch's
+    copy is exposed."""
     dev = slices.device
     num_probes = positions.shape[0]
     any_grid = not engine_grid(modes.shape[0], modes.shape[1])
     if any_grid:
         h, w = check_any_grid(slices, modes, windows)
+        f = h
     else:
-        h, _ = check_windows(slices, modes, windows, num_probes)
+        h, f = check_windows(slices, modes, windows, num_probes)
         w = h
     if tuple(host_out.shape) != (num_probes, h, w) or host_out.dtype != torch.float32:
         raise ValueError(f"host_out must be a float32 tensor of shape {(num_probes, h, w)}")
@@ -325,34 +329,71 @@ def run_forward_to_host(slices: torch.Tensor, slice_thickness: float, modes: tor
         host_out.copy_(run_forward_any(slices, slice_thickness, modes, weights, positions, voltage_kv, calib_ang,
                                        shift_calib_ang, status=status), non_blocking=True)
         return host_out
+    lib = _lib.load()
+    if tune is None:
+        tune = default_tune(h)
     dev_out = torch.empty((num_probes, h, w), dtype=torch.float32, device=dev)
     main = torch.cuda.current_stream(dev)
-    streams = _side_streams(dev, max(1, lanes))
-    copy = _side_streams(dev, 1 + max(1, lanes))[-1]
-    chunks = max(1, min(int(chunks), num_probes))
-    bounds = [num_probes * i // chunks for i in range(chunks + 1)]
-    lb = lane_batch(h, modes.shape[2], len(streams))
+    lanes = max(1, min(int(lanes), num_probes))
+    streams = _side_streams(dev, lanes)
+    copies = _copy_streams(dev, lanes)
+    bounds = [num_probes * i // lanes for i in range(lanes + 1)]
+    lb = lane_batch(h, modes.shape[2], lanes)
     lane_status = [None if status is None else _lib.new_status(dev) for _ in streams]
-    for st in streams + [copy]:
+    calls = []  # (params, workspace, bytes, lo, hi, compute stream, copy stream)
+    for (lo, hi), st, cp in zip(zip(bounds[:-1], bounds[1:]), streams, copies):
         st.wait_stream(main)
-    for i, (lo, hi) in enumerate(zip(bounds[:-1], bounds[1:])):
-        st = streams[i % len(streams)]
+        cp.wait_stream(main)
+        prm = ms_params(h, slices.shape[2], modes.shape[2], hi - lo, voltage_kv, slice_thickness, calib_ang,
+                        shift_calib_ang, slices.stride(), modes.stride(), lb, tune, f,
+                        None if windows is None else windows[lo:hi])
+        ws_bytes = lib.ptyro_ms_workspace_bytes(ctypes.byref(prm))
+        if ws_bytes == 0:
+            _lib.check(_lib.PTYRO_ERR_INVALID)
         with torch.cuda.stream(st):
-            run_forward(slices, slice_thickness, modes, weights, positions[lo:hi], voltage_kv, calib_ang,
-                        shift_calib_ang, out=dev_out[lo:hi], tune=tune, batch=lb,
-                        windows=None if windows is None else windows[lo:hi], lanes=1,
-                        status=lane_status[i % len(streams)])
-        done = torch.cuda.Event()
-        done.record(st)
-        copy.wait_event(done)
-        with torch.cuda.stream(copy):
-            host_out[lo:hi].copy_(dev_out[lo:hi], non_blocking=True)
-    for st in streams + [copy]:
+            ws = _workspace(ws_bytes, dev)  # allocated for the lane's stream
+        calls.append((prm, ws, ws_bytes, lo, hi, st, cp))
+    results = [None] * len(calls)
+
+    def issue(i):
+        prm, ws, ws_bytes, lo, hi, st, cp = calls[i]
+        with torch.cuda.device(dev):
+            rc = lib.ptyro_ms_forward_to_host(ctypes.byref(prm), slices.data_ptr(), modes.data_ptr(),
+                                              weights.data_ptr(), positions[lo:hi].data_ptr(),
+                                              dev_out[lo:hi].data_ptr(), host_out[lo:hi].data_ptr(), ws.data_ptr(),
+                                              ws_bytes, st.cuda_stream, cp.cuda_stream)
+            # the library's error message is per thread
+            results[i] = (rc, lib.ptyro_last_error().decode() if rc else "")
+
+    # each lane's launches are issued from a host thread of its own (the call releases
+    # the interpreter lock), so both lanes reach the GPU from the start
+    threads = [threading.Thread(target=issue, args=(i,)) for i in range(1, len(calls))]
+    for t in threads:
+        t.start()
+    issue(0)
+    for t in threads:
+        t.join()
+    for rc, msg in results:
+        if rc in (_lib.PTYRO_ERR_INVALID, _lib.PTYRO_ERR_UNSUPPORTED):
+            raise ValueError(msg)
+        if rc:
+            raise _lib.PtyroError(rc, msg)
+    for (prm, ws, ws_bytes, lo, hi, st, cp), ls in zip(calls, lane_status):
+        with torch.cuda.stream(st):
+            _lib.gather_status(ls, ws)  # one status word per lane: the lanes run concurrently
+    for st in streams:
         main.wait_stream(st)
     for ls in lane_status:
         if ls is not None:
             status.bitwise_or_(ls)
     return host_out
+
+
+def _copy_streams(dev: torch.device, count: int) -> list:
+    key = ("copy", dev.index, count)
+    if key not in _STREAMS:
+        _STREAMS[key] = [torch.cuda.Stream(device=dev) for _ in range(count)]
+    return _STREAMS[key]
 
 
 def _needs_autodiff(*tensors) -> bool:

@@ -229,3 +229,19 @@ def test_batch_plan_bytes_validate(lib):
     jobs[1].ready_event = None
     jobs[1].kind = _lib.PTYRO_JOB_GRADIENT  # without targets and gradient buffers
     assert lib.ptyro_plan_bytes(jobs, 2) == 0
+
+
+def test_forward_to_host_validates_before_launch(lib):
+    p = _p(num_probes=4)
+    buf = ctypes.create_string_buffer(64)
+    fake = ctypes.addressof(buf)
+    args = [fake] * 5
+    rc = lib.ptyro_ms_forward_to_host(ctypes.byref(p), *args, None, fake, 64, fake, fake + 8)
+    assert rc == _lib.PTYRO_ERR_INVALID and "host_patterns" in lib.ptyro_last_error().decode()
+    rc = lib.ptyro_ms_forward_to_host(ctypes.byref(p), *args, fake, fake, 64, fake, fake)
+    assert rc == _lib.PTYRO_ERR_INVALID and "copy_stream" in lib.ptyro_last_error().decode()
+    rc = lib.ptyro_ms_forward_to_host(ctypes.byref(p), *args, fake, fake, 64, fake, None)
+    assert rc == _lib.PTYRO_ERR_INVALID
+    acc = _p(num_probes=4, flags=_lib.PTYRO_FLAG_ACCUMULATE)
+    rc = lib.ptyro_ms_forward_to_host(ctypes.byref(acc), *args, fake, fake, 64, fake, fake + 8)
+    assert rc == _lib.PTYRO_ERR_INVALID and "accumulating" in lib.ptyro_last_error().decode()

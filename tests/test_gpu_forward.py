@@ -344,3 +344,35 @@ def test_resident_kernel_at_the_128_workload_full_depth():
     want32 = R.stem_4d(pot, synth.SLICE_DZ, w.calib, probe[..., None], [1.0], w.calib, w.voltage_kv, pos, w.calib,
                        dtype=np.complex64)["data"]
     assert rel_l2(resident, want32) < TOL_F32
+
+
+@pytest.mark.parametrize("n", [64, 128])
+def test_forward_to_host_streams_every_batch(n):
+    """ptyro_ms_forward_to_host with 5-probe batches (a ragged last batch; the pass
+    engine at 64^2, the wave-resident kernel at 128^2) copies every batch's patterns
+    to pinned host memory on its copy stream: the host patterns equal the device
+    forward's bit for bit once the call's stream is synchronised."""
+    import ctypes
+    from ptyrodactyl_b200.simulations import default_tune, ms_params, run_forward
+    rng = np.random.default_rng(n)
+    s, p = 4, 23
+    dev = torch.device("cuda")
+    slices = torch.as_tensor(rng.uniform(0, 30, (n, n, s)), dtype=torch.float32, device=dev)
+    probe = R.make_probe(200.0, 25.0, (n, n), 20.0)
+    modes = torch.as_tensor(probe[..., None].astype(np.complex64), device=dev)
+    wt = torch.ones(1, device=dev)
+    pos = torch.as_tensor(rng.uniform(-2, 2, (p, 2)), dtype=torch.float64, device=dev)
+    ref = run_forward(slices, 1.5, modes, wt, pos, 200.0, 0.2, 0.2, lanes=1).cpu()
+    lib = pb._lib.load()
+    prm = ms_params(n, s, 1, p, 200.0, 1.5, 0.2, 0.2, slices.stride(), modes.stride(), 5, default_tune(n))
+    ws_bytes = lib.ptyro_ms_workspace_bytes(ctypes.byref(prm))
+    ws = torch.empty(ws_bytes, dtype=torch.uint8, device=dev)
+    out = torch.empty((p, n, n), dtype=torch.float32, device=dev)
+    host = torch.full((p, n, n), -1.0, dtype=torch.float32).pin_memory()
+    st, cp = torch.cuda.Stream(), torch.cuda.Stream()
+    pb._lib.check(lib.ptyro_ms_forward_to_host(ctypes.byref(prm), slices.data_ptr(), modes.data_ptr(),
+                                               wt.data_ptr(), pos.data_ptr(), out.data_ptr(), host.data_ptr(),
+                                               ws.data_ptr(), ws_bytes, st.cuda_stream, cp.cuda_stream))
+    st.synchronize()  # the call's stream waits for the last copy
+    assert torch.equal(host, ref)
+    assert int(ws[:4].view(torch.int32).item()) == 0
