@@ -345,6 +345,15 @@ int ptyro_gm_backward(const ptyro_ms_params* p, int32_t height, int32_t width, c
                       const float* grad_patterns, float* grad_potential, float* grad_modes, double* grad_positions,
                       void* workspace, size_t workspace_bytes, void* stream);
 
+/* ptyro_ms_jvp on a height x width grid: patterns (NULL or (P, H, W)) and their
+ * directional derivative `tangent` (P, H, W) along (tangent_potential, tangent_modes),
+ * either of which may be NULL (zero); tangents have the potential's / modes' strides. */
+size_t ptyro_gm_jvp_workspace_bytes(const ptyro_ms_params* p, int32_t height, int32_t width);
+int ptyro_gm_jvp(const ptyro_ms_params* p, int32_t height, int32_t width, const float* potential,
+                 const float* tangent_potential, const float* modes, const float* tangent_modes, const float* weights,
+                 const double* positions, float* patterns, float* tangent, void* workspace, size_t workspace_bytes,
+                 void* stream);
+
 /* numpy fft2 / ifft2 of `count` contiguous height x width complex64 planes in place,
  * any height and width in [1, 4096] (inverse scaled by 1 / (height width)). */
 size_t ptyro_gm_fft_workspace_bytes(int32_t height, int32_t width);

@@ -81,6 +81,8 @@ EXPORTED_SYMBOLS = (
     "ptyro_gm_forward",
     "ptyro_gm_backward_workspace_bytes",
     "ptyro_gm_backward",
+    "ptyro_gm_jvp_workspace_bytes",
+    "ptyro_gm_jvp",
     "ptyro_gm_fft_workspace_bytes",
     "ptyro_gm_fft2",
     "ptyro_gm_make_probe_workspace_bytes",
@@ -258,6 +260,10 @@ def _declare(lib) -> None:
     for name in ("ptyro_gm_workspace_bytes", "ptyro_gm_residual_bytes", "ptyro_gm_backward_workspace_bytes"):
         getattr(lib, name).restype = sz
         getattr(lib, name).argtypes = [pp, i32, i32]
+    lib.ptyro_gm_jvp_workspace_bytes.restype = sz
+    lib.ptyro_gm_jvp_workspace_bytes.argtypes = [pp, i32, i32]
+    lib.ptyro_gm_jvp.restype = ctypes.c_int
+    lib.ptyro_gm_jvp.argtypes = [pp, i32, i32, vp, vp, vp, vp, vp, vp, vp, vp, vp, sz, vp]
     lib.ptyro_gm_fft_workspace_bytes.restype = sz
     lib.ptyro_gm_fft_workspace_bytes.argtypes = [i32, i32]
     lib.ptyro_gm_fft2.restype = ctypes.c_int

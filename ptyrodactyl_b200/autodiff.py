@@ -243,8 +243,6 @@ class Stem4dFunction(torch.autograd.Function):
         slices, modes, weights, positions, windows = (_plain(t) for t in ctx.saved_tensors)
         t_slices, t_modes, t_weights, t_positions = (_plain(t) for t in (t_slices, t_modes, t_weights, t_positions))
         slice_thickness, voltage_kv, calib_ang, shift_calib_ang, k, batch, tune, n, f, record = ctx.cfg
-        if ctx.any_grid:
-            raise NotImplementedError("forward-mode derivatives need a square grid with a power-of-two edge")
         # torch.func.jvp hands zero tangents to the inputs it does not differentiate
         if t_positions is not None and bool(t_positions.any()):
             raise NotImplementedError("stem_4d has no forward-mode derivative with respect to positions")
@@ -301,7 +299,9 @@ def jvp(slices, modes, weights, positions, tangent_slices, tangent_modes, slice_
     dev = slices.device
     S, M, P = slices.shape[2], modes.shape[2], positions.shape[0]
     if not engine_grid(modes.shape[0], modes.shape[1]):
-        raise NotImplementedError("forward-mode derivatives need a square grid with a power-of-two edge")
+        return _jvp_any(lib, slices, modes, weights, positions, tangent_slices, tangent_modes, slice_thickness,
+                        voltage_kv, calib_ang, calib_ang if shift_calib_ang is None else shift_calib_ang, batch,
+                        windows, want_patterns)
     n, f = check_windows(slices, modes, windows, P)
     sc = float(calib_ang if shift_calib_ang is None else shift_calib_ang)
     prm = ms_params(n, S, M, P, voltage_kv, slice_thickness, calib_ang, sc, slices.stride(), modes.stride(), batch,
@@ -317,6 +317,32 @@ def jvp(slices, modes, weights, positions, tangent_slices, tangent_modes, slice_
                                     modes.data_ptr(), None if tm is None else tm.data_ptr(), weights.data_ptr(),
                                     positions.data_ptr(), None if out is None else out.data_ptr(), tan.data_ptr(),
                                     ws.data_ptr(), ws_bytes, _stream_ptr(dev)))
+    return out, tan
+
+
+def _jvp_any(lib, slices, modes, weights, positions, tangent_slices, tangent_modes, slice_thickness, voltage_kv,
+             calib_ang, shift_calib_ang, batch, windows, want_patterns):
+    """``jvp`` on any height x width grid (ptyro_gm_jvp)."""
+    dev = slices.device
+    h, w = check_any_grid(slices, modes, windows)
+    P = positions.shape[0]
+    prm = any_grid_params(slices, modes, P, voltage_kv, slice_thickness, calib_ang, float(shift_calib_ang), batch)
+    ts = _like(tangent_slices, slices, torch.float32)
+    tm = _like(tangent_modes, modes, torch.complex64)
+    out = torch.empty((P, h, w), dtype=torch.float32, device=dev) if want_patterns else None
+    tan = torch.empty((P, h, w), dtype=torch.float32, device=dev)
+    if P:
+        ws_bytes = lib.ptyro_gm_jvp_workspace_bytes(ctypes.byref(prm), h, w)
+        if ws_bytes == 0:
+            _lib.check(_lib.PTYRO_ERR_INVALID)
+        ws = _workspace(ws_bytes, dev)
+        with torch.cuda.device(dev):
+            _lib.check(lib.ptyro_gm_jvp(ctypes.byref(prm), h, w, slices.data_ptr(),
+                                        None if ts is None else ts.data_ptr(), modes.data_ptr(),
+                                        None if tm is None else tm.data_ptr(), weights.data_ptr(),
+                                        positions.data_ptr(), None if out is None else out.data_ptr(), tan.data_ptr(),
+                                        ws.data_ptr(), ws_bytes, _stream_ptr(dev)))
+        _lib.check_workspace_status(ws, "jvp")
     return out, tan
 
 

@@ -563,6 +563,129 @@ int gm_backward(const ptyro_ms_params* p, int H, int W, const float* V, const fl
   return launched("k_gm_write_modes");
 }
 
+// ---------------------------------------------------------------- forward mode
+// The forward with its tangent (ptyro_ms_jvp on any grid): per slot the wave psi and its
+// tangent dpsi go through the same slice operators, the tangent picking up the
+// potential's tangent at each transmission: dphi = T (dpsi + i sigma dV psi), phi = T psi
+// (stem_4d's jvp). Both waves sit in one array (psi planes first, then dpsi planes), so
+// every transform runs on all of them at once.
+__global__ void k_gm_jvp_slice(float2* __restrict__ wave, float2* __restrict__ dwave, size_t slots, int H, int W,
+                               const float2* __restrict__ T, const float* __restrict__ dV, long long sy, long long sx,
+                               long long ss, int s, float sigma) {
+  const size_t hw = (size_t)H * W, total = slots * hw;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+    const size_t px = i % hw;
+    const float2 t = T[px], v = wave[i];
+    float2 d = dwave[i];
+    if (dV) {  // dpsi + i sigma dV psi
+      const float a = sigma * dV[(long long)(px / W) * sy + (long long)(px % W) * sx + (long long)s * ss];
+      d = make_float2(fmaf(-a, v.y, d.x), fmaf(a, v.x, d.y));
+    }
+    dwave[i] = cmul(d, t);
+    wave[i] = cmul(v, t);
+  }
+}
+
+// I = sum_m w_m |A|^2 and dI = sum_m w_m 2 Re(conj(A) dA), fftshifted like k_gm_intensity
+__global__ void k_gm_jvp_out(const float2* __restrict__ wave, const float2* __restrict__ dwave,
+                             const float* __restrict__ w, int nb, int M, int H, int W, float* __restrict__ out,
+                             float* __restrict__ tangent) {
+  const size_t hw = (size_t)H * W, total = (size_t)nb * hw;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+    const size_t b = i / hw, px = i % hw;
+    const int ky = (int)(px / W), kx = (int)(px % W);
+    float acc = 0.f, dacc = 0.f;
+    for (int m = 0; m < M; ++m) {
+      const float2 a = wave[(b * M + m) * hw + px], da = dwave[(b * M + m) * hw + px];
+      acc = fmaf(w[m], fmaf(a.x, a.x, a.y * a.y), acc);
+      dacc = fmaf(w[m], 2.f * fmaf(a.x, da.x, a.y * da.y), dacc);
+    }
+    const size_t o = b * hw + (size_t)((ky + H / 2) % H) * W + (kx + W / 2) % W;
+    if (out) out[o] = acc;
+    tangent[o] = dacc;
+  }
+}
+
+struct GmJvpLayout {
+  GmLayout L;      // status, roots, tables, probe spectra and the batch
+  size_t dprobe_k;  // tangent probe spectra (M planes)
+  size_t waves2;    // psi and dpsi of the batch's slots
+  size_t total;
+};
+
+GmJvpLayout gm_jvp_layout(const ptyro_ms_params* p, int H, int W) {
+  GmJvpLayout J;
+  J.L = gm_layout(p, H, W, false);
+  const size_t hw = (size_t)H * W;
+  size_t o = J.L.total;
+  J.dprobe_k = o; o = align_up(o + 8 * hw * p->num_modes);
+  J.waves2 = o; o = align_up(o + 2 * 8 * hw * p->num_modes * (size_t)J.L.batch);
+  J.total = o;
+  return J;
+}
+
+int gm_jvp(const ptyro_ms_params* p, int H, int W, const float* V, const float* dV, const float* modes,
+           const float* dmodes, const float* weights, const double* positions, float* patterns, float* tangent,
+           void* workspace, size_t bytes, cudaStream_t st) {
+  int rc = gm_validate(p, H, W);
+  if (rc) return rc;
+  if (p->num_probes == 0) return PTYRO_OK;
+  if (!V || !modes || !weights || !positions || !tangent) return err(PTYRO_ERR_INVALID, "NULL array argument");
+  if (p->flags & PTYRO_FLAG_ACCUMULATE) return err(PTYRO_ERR_INVALID, "the tangent forward does not accumulate");
+  const GmJvpLayout J = gm_jvp_layout(p, H, W);
+  GmLayout Lw = J.L;
+  Lw.total = J.total;
+  if ((rc = gm_workspace(Lw, workspace, bytes))) return rc;
+  char* ws = (char*)workspace;
+  const GmLayout& L = J.L;
+  if ((rc = gm_setup(p, H, W, L, ws, V, false, st))) return rc;
+  const int S = p->num_slices, M = p->num_modes;
+  const size_t hw = (size_t)H * W;
+  const float2 *twH = (const float2*)(ws + L.twH), *twW = (const float2*)(ws + L.twW);
+  const float2 *T = (const float2*)(ws + L.trans), *P = (const float2*)(ws + L.prop);
+  float2* pk = (float2*)(ws + L.probe_k);
+  float2* dpk = (float2*)(ws + J.dprobe_k);
+  k_gm_gather_modes<<<blocks(hw * M), 256, 0, st>>>((const float2*)modes, p->mode_stride_y, p->mode_stride_x,
+                                                    p->mode_stride_m, H, W, M, pk);
+  if (dmodes)
+    k_gm_gather_modes<<<blocks(hw * M), 256, 0, st>>>((const float2*)dmodes, p->mode_stride_y, p->mode_stride_x,
+                                                      p->mode_stride_m, H, W, M, dpk);
+  else if (cudaMemsetAsync(dpk, 0, 8 * hw * M, st) != cudaSuccess)
+    return err(PTYRO_ERR_CUDA, "clearing the tangent probe spectra");
+  if ((rc = launched("k_gm_gather_modes", dmodes ? 2 : 1))) return rc;
+  if ((rc = fft2_planes(pk, M, H, W, false, twH, twW, st))) return rc;
+  if ((rc = fft2_planes(dpk, M, H, W, false, twH, twW, st))) return rc;
+  const float sigma = (float)sigma_of(p->voltage_kv);
+  for (int b0 = 0; b0 < p->num_probes; b0 += L.batch) {
+    const int nb = p->num_probes - b0 < L.batch ? p->num_probes - b0 : L.batch;
+    const size_t slots = (size_t)nb * M;
+    float2* wave = (float2*)(ws + J.waves2);
+    float2* dwave = wave + slots * hw;  // both waves contiguous: one transform call for all planes
+    k_gm_shift<<<blocks(slots * hw), 256, 0, st>>>(pk, positions + 2 * (size_t)b0, nb, M, H, W, p->shift_calib_ang,
+                                                   wave);
+    k_gm_shift<<<blocks(slots * hw), 256, 0, st>>>(dpk, positions + 2 * (size_t)b0, nb, M, H, W,
+                                                   p->shift_calib_ang, dwave);
+    if ((rc = launched("k_gm_shift", 2))) return rc;
+    if ((rc = fft2_planes(wave, (int)(2 * slots), H, W, true, twH, twW, st))) return rc;
+    for (int s = 0; s < S; ++s) {
+      k_gm_jvp_slice<<<blocks(slots * hw), 256, 0, st>>>(wave, dwave, slots, H, W, T + (size_t)s * hw, dV,
+                                                         p->pot_stride_y, p->pot_stride_x, p->pot_stride_s, s, sigma);
+      if ((rc = launched("k_gm_jvp_slice"))) return rc;
+      if (s == S - 1) break;
+      if ((rc = fft2_planes(wave, (int)(2 * slots), H, W, false, twH, twW, st))) return rc;
+      k_gm_mul<<<blocks(2 * slots * hw), 256, 0, st>>>(wave, 2 * slots, hw, P, 0, nullptr, 0);
+      if ((rc = launched("k_gm_mul"))) return rc;
+      if ((rc = fft2_planes(wave, (int)(2 * slots), H, W, true, twH, twW, st))) return rc;
+    }
+    if ((rc = fft2_planes(wave, (int)(2 * slots), H, W, false, twH, twW, st))) return rc;
+    k_gm_jvp_out<<<blocks((size_t)nb * hw), 256, 0, st>>>(wave, dwave, weights, nb, M, H, W,
+                                                          patterns ? patterns + (size_t)b0 * hw : nullptr,
+                                                          tangent + (size_t)b0 * hw);
+    if ((rc = launched("k_gm_jvp_out"))) return rc;
+  }
+  return PTYRO_OK;
+}
+
 // ---------------------------------------------------------------- make_probe, any shape
 // make_probe (simulations.py:395-431) on an H x W grid: the aperture |q| <= alpha/lambda
 // times exp(-i chi) on the reference's grid, q along x = (arange(-W/2, W/2) rolled by
@@ -729,6 +852,19 @@ int ptyro_gm_weight_grad(const ptyro_ms_params* p, int32_t height, int32_t width
                       (size_t)p->num_slices * hw, (const float2*)residuals, grad_patterns, grad_weights,
                       (double*)workspace, 296, (cudaStream_t)stream);
   return rc ? err(rc, "mode-weight gradient: launch failed") : PTYRO_OK;
+}
+
+size_t ptyro_gm_jvp_workspace_bytes(const ptyro_ms_params* p, int32_t height, int32_t width) {
+  if (ptyro::gm_validate(p, height, width)) return 0;
+  return ptyro::gm_jvp_layout(p, height, width).total;
+}
+
+int ptyro_gm_jvp(const ptyro_ms_params* p, int32_t height, int32_t width, const float* potential,
+                 const float* tangent_potential, const float* modes, const float* tangent_modes, const float* weights,
+                 const double* positions, float* patterns, float* tangent, void* workspace, size_t workspace_bytes,
+                 void* stream) {
+  return ptyro::gm_jvp(p, height, width, potential, tangent_potential, modes, tangent_modes, weights, positions,
+                       patterns, tangent, workspace, workspace_bytes, (cudaStream_t)stream);
 }
 
 size_t ptyro_gm_workspace_bytes(const ptyro_ms_params* p, int32_t height, int32_t width) {

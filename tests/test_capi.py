@@ -183,6 +183,15 @@ def test_any_size_entry_points_validate_before_launch(lib):
     assert rc == _lib.PTYRO_ERR_INVALID
 
 
+def test_any_size_jvp_validates(lib):
+    p = _p(n=0, num_probes=3, num_modes=1, num_slices=2)
+    assert lib.ptyro_gm_jvp_workspace_bytes(ctypes.byref(p), 45, 77) > lib.ptyro_gm_workspace_bytes(
+        ctypes.byref(p), 45, 77)
+    assert lib.ptyro_gm_jvp_workspace_bytes(ctypes.byref(p), 0, 77) == 0
+    rc = lib.ptyro_gm_jvp(ctypes.byref(p), 45, 77, *([None] * 8), None, 0, None)
+    assert rc == _lib.PTYRO_ERR_INVALID and "NULL" in lib.ptyro_last_error().decode()
+
+
 def test_any_size_transforms_and_probe_validate(lib):
     assert lib.ptyro_gm_fft_workspace_bytes(45, 77) > 0
     assert lib.ptyro_gm_fft_workspace_bytes(0, 77) == 0

@@ -122,12 +122,25 @@ def test_autograd_position_and_weight_gradients(h, w, s, m, p):
     assert rel_l2(ww.grad.cpu().numpy(), want_w) < TOL
 
 
-def test_forward_mode_is_refused_off_the_engine_grids():
-    pot, modes, wt, pos, _ = _case(12, 20, 2, 1, 2)
-    sl, md, ww = _dev(pot, modes, wt)
+@pytest.mark.parametrize("h,w,s,m,p", [(48, 80, 3, 2, 3), (33, 27, 2, 1, 2), (4, 4, 2, 1, 2)])
+def test_forward_mode_matches_oracle(h, w, s, m, p):
+    """ptyro_gm_jvp against the oracle's stem_4d_jvp for potential and mode tangents,
+    directly and through torch.func.jvp of the public differentiable forward."""
+    pot, modes, wt, pos, _ = _case(h, w, s, m, p, seed=5 * h + w)
+    rng = np.random.default_rng(h * w)
+    dpot = rng.normal(size=pot.shape)
+    dmodes = 0.1 * (rng.normal(size=modes.shape) + 1j * rng.normal(size=modes.shape))
+    sl, md, ww, dsl, dmd = _dev(pot, modes, wt, dpot, dmodes)
     ps = torch.as_tensor(pos, dtype=torch.float64, device="cuda")
-    with pytest.raises(NotImplementedError):
-        torch.func.jvp(lambda v: pb.stem_4d_patterns(v, md, ww, ps, DZ, KV, CALIB), (sl,), (torch.ones_like(sl),))
+    want, dwant = R.stem_4d_jvp(pot, DZ, CALIB, modes, wt, CALIB, KV, pos, CALIB, dslices=dpot, dbeam=dmodes)
+    out, tan = pb.jvp(sl, md, ww, ps, dsl, dmd, DZ, KV, CALIB)
+    assert rel_l2(out.cpu().numpy(), want) < TOL
+    assert rel_l2(tan.cpu().numpy(), dwant) < TOL, rel_l2(tan.cpu().numpy(), dwant)
+    _, tan_v = pb.jvp(sl, md, ww, ps, dsl, None, DZ, KV, CALIB, want_patterns=False)
+    _, dwant_v = R.stem_4d_jvp(pot, DZ, CALIB, modes, wt, CALIB, KV, pos, CALIB, dslices=dpot)
+    assert rel_l2(tan_v.cpu().numpy(), dwant_v) < TOL
+    _, tan_f = torch.func.jvp(lambda v, b: pb.stem_4d_patterns(v, b, ww, ps, DZ, KV, CALIB), (sl, md), (dsl, dmd))
+    assert rel_l2(tan_f.cpu().numpy(), dwant) < TOL
 
 
 @pytest.mark.parametrize("h,w", [(96, 160), (45, 77), (64, 128), (7, 5), (100, 100)])
