@@ -33,9 +33,11 @@ from .simulations import (
     _stream_ptr,
     _workspace,
     check_windows,
+    engine_grid,
     fft2,
     ms_params,
     relativistic_wavelength_ang,
+    run_forward_any,
 )
 from .types import (
     Distribution,
@@ -158,10 +160,10 @@ class VirtualModes:
 def _jitter_shift(spectra: torch.Tensor, delta, calib: float) -> torch.Tensor:
     """ifft2(fft2(mode) exp(-2 pi i (qy dy + qx dx))) of (M, n, n) spectra
     (shift_beam_fourier, simulations.py:1236-1327)."""
-    n = spectra.shape[-1]
-    q = np.fft.fftfreq(n, d=calib)
-    ry = np.exp(-2j * np.pi * q * float(delta[0]))
-    rx = np.exp(-2j * np.pi * q * float(delta[1]))
+    qy = np.fft.fftfreq(spectra.shape[-2], d=calib)
+    qx = np.fft.fftfreq(spectra.shape[-1], d=calib)
+    ry = np.exp(-2j * np.pi * qy * float(delta[0]))
+    rx = np.exp(-2j * np.pi * qx * float(delta[1]))
     ramp = torch.as_tensor(np.outer(ry, rx).astype(np.complex64), device=spectra.device)
     return fft2(spectra * ramp, inverse=True)
 
@@ -246,10 +248,18 @@ def run_forward_ensemble(slices: torch.Tensor, slice_thickness: float, groups: L
     lib = _lib.load()
     dev = slices.device
     num_probes = positions.shape[0]
-    n = groups[0].modes.shape[0]
-    out = torch.zeros((num_probes, n, n), dtype=torch.float32, device=dev)
+    h, w = groups[0].modes.shape[0], groups[0].modes.shape[1]
+    out = torch.zeros((num_probes, h, w), dtype=torch.float32, device=dev)
     if num_probes == 0:
         return out
+    if not engine_grid(h, w):  # the any-size forward, accumulating each energy's group
+        for g in groups:
+            if g.tilts is not None:
+                raise NotImplementedError("tilted coherence samples need a square grid with a power-of-two edge")
+            run_forward_any(slices, slice_thickness, g.modes.contiguous(), g.weights, positions, g.voltage_kv,
+                            calib_ang, shift_calib_ang, out=out, accumulate=True)
+        return out
+    n = h
     for g in groups:
         _, f = check_windows(slices, g.modes, None, num_probes)
         prm = ms_params(n, slices.shape[2], g.modes.shape[2], num_probes, g.voltage_kv, slice_thickness, calib_ang,

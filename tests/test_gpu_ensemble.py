@@ -142,3 +142,30 @@ def test_ensemble_derivatives_refuse_tilts():
     V = torch.tensor(pot, dtype=torch.float32, device="cuda", requires_grad=True)
     with pytest.raises(NotImplementedError, match="tilted"):
         pb.stem_4d(pb.PotentialSlices(V, 1.7, 0.25), pb.create_probe_modes(modes, w, 0.25), mic, det)
+
+
+def test_ensemble_on_a_rectangular_grid():
+    """Jitter and energy-spread axes on a 40 x 56 grid (the any-size path, one
+    accumulating forward per energy) against the oracle's ensemble branch; tilted
+    samples need the engine's square grids."""
+    rng = np.random.default_rng(6)
+    h, w, s = 40, 56, 3
+    pot = rng.uniform(0.0, 40.0, (h, w, s))
+    probe = R.make_probe(200.0, 25.0, (h, w), 25.0, defocus_ang=-30.0)
+    modes = np.stack([probe, np.roll(probe, 2, axis=1) * (0.8 - 0.2j)], -1)
+    wts = np.array([0.65, 0.35])
+    pos = rng.uniform(-2, 2, (3, 2))
+    ens = pb.create_ensemble_axes(position_jitter=pb.position_jitter_to_distribution(0.08, 2),
+                                  coherence=pb.coherence_to_distribution(0.5, 0.0, 2))
+    mic = pb.create_microscope_config(200.0, 25.0, ensemble=ens, probe_shape=(h, w))
+    beam = pb.create_probe_modes(modes, wts, 0.25)
+    det = pb.create_detector_config(0.3, scan_positions_px=pos)
+    s4 = pb.stem_4d(pb.create_potential_slices(pot, 1.7, 0.25), beam, mic, det)
+    axes = [_axes_oracle(a) for a in pb.ensemble_axes_for_cbed(ens, beam)]
+    want = R.stem_4d_ensemble(pot, 1.7, 0.25, modes, 0.25, 200.0, pos, 0.3, axes)
+    assert tuple(s4.data.shape) == (3, h, w)
+    assert rel_l2(s4.data.cpu().numpy(), want) < TOL
+    tilted = pb.create_ensemble_axes(coherence=pb.coherence_to_distribution(0.5, 0.2, 2))
+    mic_t = pb.create_microscope_config(200.0, 25.0, ensemble=tilted, probe_shape=(h, w))
+    with pytest.raises(NotImplementedError, match="tilted"):
+        pb.stem_4d(pb.create_potential_slices(pot, 1.7, 0.25), beam, mic_t, det)
