@@ -357,13 +357,16 @@ def run_forward_to_host(slices: torch.Tensor, slice_thickness: float, modes: tor
 
     def issue(i):
         prm, ws, ws_bytes, lo, hi, st, cp = calls[i]
-        with torch.cuda.device(dev):
-            rc = lib.ptyro_ms_forward_to_host(ctypes.byref(prm), slices.data_ptr(), modes.data_ptr(),
-                                              weights.data_ptr(), positions[lo:hi].data_ptr(),
-                                              dev_out[lo:hi].data_ptr(), host_out[lo:hi].data_ptr(), ws.data_ptr(),
-                                              ws_bytes, st.cuda_stream, cp.cuda_stream)
-            # the library's error message is per thread
-            results[i] = (rc, lib.ptyro_last_error().decode() if rc else "")
+        try:
+            with torch.cuda.device(dev):
+                rc = lib.ptyro_ms_forward_to_host(ctypes.byref(prm), slices.data_ptr(), modes.data_ptr(),
+                                                  weights.data_ptr(), positions[lo:hi].data_ptr(),
+                                                  dev_out[lo:hi].data_ptr(), host_out[lo:hi].data_ptr(),
+                                                  ws.data_ptr(), ws_bytes, st.cuda_stream, cp.cuda_stream)
+                # the library's error message is per thread
+                results[i] = (rc, lib.ptyro_last_error().decode() if rc else "")
+        except Exception as error:  # reported on the calling thread below
+            results[i] = (_lib.PTYRO_ERR_CUDA, f"issuing lane {i}: {error!r}")
 
     # each lane's launches are issued from a host thread of its own (the call releases
     # the interpreter lock), so both lanes reach the GPU from the start
