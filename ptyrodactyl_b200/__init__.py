@@ -27,6 +27,7 @@ from .types import (  # noqa: F401
     create_stem4d,
 )
 from .simulations import (  # noqa: F401
+    aberration,
     cbed_amplitude,
     cbed_image,
     fft2,

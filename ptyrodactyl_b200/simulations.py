@@ -641,6 +641,24 @@ def cbed_amplitude(pot_slices: PotentialSlices, beam: ProbeModes, microscope: Mi
     return amps[0].permute(1, 2, 0)
 
 
+def aberration(fourier_coord, lambda_angstrom, defocus=0.0, c3=0.0, c5=0.0) -> torch.Tensor:
+    """Aberration phase chi = 2 pi / lambda (C1 p^2 / 2 + 1e7 C3 p^4 / 4 + 1e7 C5 p^6 / 6),
+    p = lambda |q| (simulations.py:434-498; the 1e7 factor makes the C3 and C5 fields act
+    as mm). ``fourier_coord`` is |q| in 1/Angstrom (any shape); float64 on its device,
+    differentiable in every argument given as a tensor. ``make_probe`` evaluates the
+    same phase inside its aperture kernel."""
+    q = as_tensor(fourier_coord, torch.float64)
+    dev = q.device
+
+    def t(v):
+        return v.to(device=dev, dtype=torch.float64) if isinstance(v, torch.Tensor) else torch.tensor(
+            float(v), dtype=torch.float64, device=dev)
+    lam = t(lambda_angstrom)
+    p = lam * q
+    chi = (t(defocus) * p ** 2) / 2 + (t(c3) * 1e7 * p ** 4) / 4 + (t(c5) * 1e7 * p ** 6) / 6
+    return (2 * math.pi * chi) / lam
+
+
 def make_probe(microscope: MicroscopeConfig, detector: DetectorConfig) -> torch.Tensor:
     """Real-space probe from aperture and aberrations (simulations.py:334-431):
     complex64 (H, W) CUDA tensor, centred at (H/2, W/2), unnormalised."""

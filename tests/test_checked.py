@@ -76,3 +76,26 @@ def test_checked_entries_match_unchecked_on_valid_inputs():
     det_ang = pb.create_detector_config(0.2, scan_positions_ang=rng.uniform(0, n * 0.2 - 0.5, (5, 2)))
     got = pb.checked_stem4d_sharded(beam, sample, mic, det_ang).data.cpu()
     assert torch.equal(got, pb.stem4d_sharded(beam, sample, mic, det_ang).data.cpu())
+
+
+def test_public_integrator_signatures_have_at_most_six_parameters():
+    """The reference's contract on its public integrators (test_simulations.py:59-81)."""
+    import inspect
+    for f in (pb.aberration, pb.annular_detector, pb.cbed_amplitude, pb.cbed_image, pb.checked_cbed_image,
+              pb.checked_make_probe, pb.checked_stem4d_sharded, pb.checked_stem_4d, pb.make_probe,
+              pb.stem4d_sharded, pb.stem_4d):
+        assert len(inspect.signature(f).parameters) <= 6, f
+
+
+def test_aberration_matches_oracle_and_differentiates():
+    import numpy as np
+    import torch
+    from oracle import multislice_ref as R
+    q = np.linspace(0.0, 1.2, 50).reshape(5, 10)
+    lam = R.relativistic_wavelength_ang(200.0)
+    want = R.aberration(q, lam, -35.0, 2e-3, 0.5)
+    got = pb.aberration(q, lam, -35.0, 2e-3, 0.5)
+    assert got.dtype == torch.float64 and np.allclose(got.numpy(), want, rtol=1e-14, atol=1e-12)
+    c1 = torch.tensor(-35.0, dtype=torch.float64, requires_grad=True)
+    pb.aberration(torch.as_tensor(q), lam, c1).sum().backward()
+    assert abs(float(c1.grad) - float(np.sum(2 * np.pi / lam * (lam * q) ** 2 / 2))) < 1e-9 * abs(float(c1.grad))
