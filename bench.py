@@ -429,7 +429,7 @@ def run_ours(args, rank, world, local_rank):
             sv = run_serve(argparse.Namespace(**{**vars(args), "requests": 48}), rank, world, local_rank)
             line["p50_ms"], line["p99_ms"] = sv["p50_ms"], sv["p99_ms"]
             line["serving"] = {k: sv[k] for k in ("metric", "value", "unit", "p50_ms", "p99_ms", "mean_ms",
-                                                  "requests", "completed", "makespan_s", "config")}
+                                                  "requests", "completed", "makespan_s", "config", "batch_plan")}
         print(json.dumps(line), flush=True)
 
 
