@@ -928,8 +928,9 @@ static __global__ void k_write_grad_modes(const float2* __restrict__ lam_beam, i
 }
 
 struct BwdLayout {
-  size_t status, tw, pf, trans, trans_t, ramp_y, ramp_x, psi, lam, contrib, beam, probe_k, total;
+  size_t status, tw, pf, trans, trans_t, trans_p, trans_pt, ramp_y, ramp_x, psi, lam, contrib, beam, probe_k, total;
   int batch;
+  bool paired_t;  // line-pair interleaved transmission tables (as the forward's, 256^2)
   int dgroup;  // slices whose dV contributions are kept before one reduction adds them
 };
 
@@ -957,6 +958,11 @@ static BwdLayout bwd_layout_for(const ptyro_ms_params* p) {
   const size_t ff = (size_t)field_of(p) * field_of(p);
   L.trans = o; o = align_up(o + 8 * ff * p->num_slices);
   L.trans_t = o; o = align_up(o + 8 * ff * p->num_slices);
+  L.paired_t = p->n == 256 && (p->tune & 16384) && (p->tune & 16) && (p->tune & 64);
+  if (L.paired_t) {
+    L.trans_p = o; o = align_up(o + 8 * ff * p->num_slices);
+    L.trans_pt = o; o = align_up(o + 8 * ff * p->num_slices);
+  }
   L.ramp_y = o; o = align_up(o + 8 * (size_t)p->n * L.batch);
   L.ramp_x = o; o = align_up(o + 8 * (size_t)p->n * L.batch);
   L.psi = o; o = align_up(o + 8 * nn * slots);
@@ -1044,6 +1050,7 @@ struct BwdBuffers {
   float2 *psi, *lam;
   float* contrib;
   const float2 *trans, *trans_t, *pf, *tw, *ramp_y, *ramp_x;
+  const float4 *trans_p = nullptr, *trans_pt = nullptr;  // interleaved tables, or null
   int dgroup = 1;             // contribution planes: slice point i (in adjoint order) writes plane i % dgroup
   size_t contrib_plane = 0;   // floats between planes
 };
@@ -1063,6 +1070,8 @@ static BwdPlan bwd_pass_plan(const ptyro_ms_params* p, const BwdBuffers& B, cons
   a.res_stride = (size_t)(C + 1) * nn;
   a.trans = B.trans;
   a.trans_t = B.trans_t;
+  a.trans_p = B.trans_p;
+  a.trans_pt = B.trans_pt;
   a.pf = B.pf;
   a.tw = B.tw;
   a.ramp_y = B.ramp_y;
@@ -1182,7 +1191,9 @@ static int backward_impl(const ptyro_ms_params* p, int ckpt_every, const float* 
   k_transmission<<<blocks_for((size_t)F * F * S, 256), 256, 0, st>>>(potential, p->pot_stride_y, p->pot_stride_x,
                                                                      p->pot_stride_s, F, S,
                                                                      interaction_sigma(p->voltage_kv),
-                                                                     (float2*)(ws + L.trans), (float2*)(ws + L.trans_t));
+                                                                     (float2*)(ws + L.trans), (float2*)(ws + L.trans_t),
+                                                                     L.paired_t ? (float*)(ws + L.trans_p) : nullptr,
+                                                                     L.paired_t ? (float*)(ws + L.trans_pt) : nullptr);
   k_zero_pot<<<blocks_for((size_t)F * F * S, 256), 256, 0, st>>>(grad_potential, p->pot_stride_y, p->pot_stride_x,
                                                                  p->pot_stride_s, F, S);
   k_zero2<<<blocks_for(nn * M, 256), 256, 0, st>>>(beam, nn * M);
@@ -1204,6 +1215,8 @@ static int backward_impl(const ptyro_ms_params* p, int ckpt_every, const float* 
   B.contrib_plane = nn * (size_t)L.batch * M;
   B.trans = (const float2*)(ws + L.trans);
   B.trans_t = (const float2*)(ws + L.trans_t);
+  B.trans_p = L.paired_t ? (const float4*)(ws + L.trans_p) : nullptr;
+  B.trans_pt = L.paired_t ? (const float4*)(ws + L.trans_pt) : nullptr;
   B.pf = (const float2*)(ws + L.pf);
   B.tw = tw;
   B.ramp_y = (const float2*)(ws + L.ramp_y);

@@ -28,6 +28,8 @@ struct BwdArgs {
   size_t res_stride;
   const float2* trans;     // (S, F, F) T, row-major
   const float2* trans_t;   // transposed
+  const float4* trans_p;   // T interleaved by line pairs (rows), or null: the lambda-only pass's one
+  const float4* trans_pt;  // 16-byte load per element pair; and the transposed table's column pairs
   const int* win;          // (B, 2) window origins in the field, or null
   int field_n;             // F (== N without windows)
   const float2* pf;        // (N) propagator factor / N (conjugated in use)

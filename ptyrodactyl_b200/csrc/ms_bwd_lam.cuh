@@ -166,13 +166,34 @@ __device__ __forceinline__ void bwd_lam_body(const BwdArgs& a, const int slot, c
         }
       }
     }
-    int oa, ob;
-    const float2* Ta = trans_row<AXIS>(a.trans, a.trans_t, a.field_n, a.t_slice, a.win, b, la, &oa);
-    const float2* Tb = trans_row<AXIS>(a.trans, a.trans_t, a.field_n, a.t_slice, a.win, b, lb, &ob);
+    // the pair's lines sit at field lines la + lo, la + 1 + lo: one interleaved entry
+    // (T[2p].re, T[2p+1].re, T[2p].im, T[2p+1].im) serves both when lo is even, and
+    // multiplies with the same operations as the two plain loads
+    const float4* TP = AXIS == 0 ? a.trans_p : a.trans_pt;
+    int lo = 0, eo = 0;
+    if (a.win) {
+      lo = AXIS == 0 ? a.win[2 * b] : a.win[2 * b + 1];
+      eo = AXIS == 0 ? a.win[2 * b + 1] : a.win[2 * b];
+    }
     const int fm = a.field_n - 1;
+    if (TP != nullptr && (lo & 1) == 0) {
+      const float4* row =
+          TP + ((size_t)a.t_slice * (a.field_n / 2) + (size_t)(((la + lo) & fm) >> 1)) * a.field_n;
 #pragma unroll
-    for (int j = 0; j < N2; ++j)
-      v[j] = cmulc(v[j], __ldg(Ta + ((t + N1 * j + oa) & fm)), __ldg(Tb + ((t + N1 * j + ob) & fm)));
+      for (int j = 0; j < N2; ++j) {
+        const float4 q = __ldg(row + ((t + N1 * j + eo) & fm));
+        const float2 wx = make_float2(q.x, q.y), wy = make_float2(q.z, q.w);
+        v[j] = {__ffma2_rn(v[j].re, wx, __fmul2_rn(v[j].im, wy)),
+                __ffma2_rn(v[j].im, wx, __fmul2_rn(v[j].re, make_float2(-q.z, -q.w)))};
+      }
+    } else {
+      int oa, ob;
+      const float2* Ta = trans_row<AXIS>(a.trans, a.trans_t, a.field_n, a.t_slice, a.win, b, la, &oa);
+      const float2* Tb = trans_row<AXIS>(a.trans, a.trans_t, a.field_n, a.t_slice, a.win, b, lb, &ob);
+#pragma unroll
+      for (int j = 0; j < N2; ++j)
+        v[j] = cmulc(v[j], __ldg(Ta + ((t + N1 * j + oa) & fm)), __ldg(Tb + ((t + N1 * j + ob) & fm)));
+    }
   }
 
   // ---- op2, and the beam-gradient epilogue (lambda k-order along this axis times conj(ramp))
