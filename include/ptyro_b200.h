@@ -248,6 +248,14 @@ int ptyro_ms_forward_detect(const ptyro_ms_params* p, const float* potential, co
 int ptyro_detect_patterns(const float* patterns, int64_t num_patterns, int32_t n, const uint32_t* det_mask,
                           int32_t num_det, double* det_out, void* stream);
 
+/* Masked sums of stored patterns of any height x width, (P, height, width) float32:
+ * det_out[p][d] = sum of the pixels i of pattern p with bit d set in det_mask[i],
+ * the mask in the stored patterns' own (fftshifted) pixel order, (height, width).
+ * annular_detector (simulations.py:1539-1656) at every probe_shape, including the
+ * any-size grids of ptyro_gm_forward. height, width in [1, 8192]. No workspace. */
+int ptyro_detect_patterns_hw(const float* patterns, int64_t num_patterns, int32_t height, int32_t width,
+                             const uint32_t* det_mask, int32_t num_det, double* det_out, void* stream);
+
 /* Probe formation. Replaces make_probe (src/ptyrodactyl/multislice/simulations.py:334-431)
  * with aberration (:434-498): aperture |q| <= alpha/lambda times exp(-i chi),
  * ifftshift(ifft2(.)). Writes a complex64 (n, n) probe to `probe`.

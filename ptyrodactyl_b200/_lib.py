@@ -44,6 +44,7 @@ EXPORTED_SYMBOLS = (
     "ptyro_ms_detect_workspace_bytes",
     "ptyro_ms_forward_detect",
     "ptyro_detect_patterns",
+    "ptyro_detect_patterns_hw",
     "ptyro_ms_jvp_workspace_bytes",
     "ptyro_ms_jvp",
     "ptyro_ms_forward_tilted",
@@ -229,6 +230,8 @@ def _declare(lib) -> None:
     lib.ptyro_ms_forward_detect.argtypes = [pp, vp, vp, vp, vp, vp, i32, vp, vp, vp, sz, vp]
     lib.ptyro_detect_patterns.restype = ctypes.c_int
     lib.ptyro_detect_patterns.argtypes = [vp, i64, i32, vp, i32, vp, vp]
+    lib.ptyro_detect_patterns_hw.restype = ctypes.c_int
+    lib.ptyro_detect_patterns_hw.argtypes = [vp, i64, i32, i32, vp, i32, vp, vp]
     lib.ptyro_ms_jvp_workspace_bytes.restype = sz
     lib.ptyro_ms_jvp_workspace_bytes.argtypes = [pp]
     lib.ptyro_ms_jvp.restype = ctypes.c_int

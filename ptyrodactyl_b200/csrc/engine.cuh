@@ -568,6 +568,28 @@ static size_t det_part_bytes(const Layout& L, int n, int n_det) {
 // accumulation, the warps' sums added in warp order (deterministic). Pixel (y, x)
 // of a stored pattern holds frequency ((y + n/2) mod n, (x + n/2) mod n).
 constexpr int kDetThreads = 256;
+
+// Per-detector CTA totals: each warp's shuffle sum, then the warps' sums in warp
+// order (deterministic), written to row[0 .. n_det).
+__device__ __forceinline__ void det_block_sums(const double (&acc)[PTYRO_MAX_DETECTORS], int n_det,
+                                               double (*red)[PTYRO_MAX_DETECTORS], double* row) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+#pragma unroll
+  for (int d = 0; d < PTYRO_MAX_DETECTORS; ++d) {
+    if (d >= n_det) break;
+    double s = acc[d];
+#pragma unroll
+    for (int o = 16; o >= 1; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) red[warp][d] = s;
+  }
+  __syncthreads();
+  if (threadIdx.x < n_det) {
+    double s = 0.0;
+    for (int w = 0; w < kDetThreads / 32; ++w) s += red[w][threadIdx.x];
+    row[threadIdx.x] = s;
+  }
+}
+
 static __global__ void __launch_bounds__(kDetThreads) k_detect_patterns(const float* __restrict__ pat, int n,
                                                                         const uint32_t* __restrict__ mask,
                                                                         int n_det, double* out) {
@@ -586,21 +608,29 @@ static __global__ void __launch_bounds__(kDetThreads) k_detect_patterns(const fl
     for (int d = 0; d < PTYRO_MAX_DETECTORS; ++d)
       if (d < n_det && ((b >> d) & 1u)) acc[d] += (double)v;
   }
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  det_block_sums(acc, n_det, red, out + (size_t)blockIdx.x * n_det);
+}
+
+// The same sums for patterns of any height x width, the mask given in the stored
+// patterns' own (fftshifted) pixel order: pixel i of every pattern against mask[i],
+// as the reference's annular_detector multiplies each pattern by its mask.
+static __global__ void __launch_bounds__(kDetThreads) k_detect_patterns_stored(const float* __restrict__ pat,
+                                                                               int hw,
+                                                                               const uint32_t* __restrict__ mask,
+                                                                               int n_det, double* out) {
+  __shared__ double red[kDetThreads / 32][PTYRO_MAX_DETECTORS];
+  const float* p = pat + (size_t)blockIdx.x * hw;
+  double acc[PTYRO_MAX_DETECTORS];
 #pragma unroll
-  for (int d = 0; d < PTYRO_MAX_DETECTORS; ++d) {
-    if (d >= n_det) break;
-    double s = acc[d];
+  for (int d = 0; d < PTYRO_MAX_DETECTORS; ++d) acc[d] = 0.0;
+  for (int i = threadIdx.x; i < hw; i += kDetThreads) {
+    const float v = p[i];
+    const uint32_t b = __ldg(mask + i);
 #pragma unroll
-    for (int o = 16; o >= 1; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-    if (lane == 0) red[warp][d] = s;
+    for (int d = 0; d < PTYRO_MAX_DETECTORS; ++d)
+      if (d < n_det && ((b >> d) & 1u)) acc[d] += (double)v;
   }
-  __syncthreads();
-  if (threadIdx.x < n_det) {
-    double s = 0.0;
-    for (int w = 0; w < kDetThreads / 32; ++w) s += red[w][threadIdx.x];
-    out[(size_t)blockIdx.x * n_det + threadIdx.x] = s;
-  }
+  det_block_sums(acc, n_det, red, out + (size_t)blockIdx.x * n_det);
 }
 
 static int detect_patterns(const float* patterns, int count, int n, const uint32_t* mask, int n_det, double* out,

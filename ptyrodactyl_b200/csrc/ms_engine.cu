@@ -74,6 +74,20 @@ int ptyro_detect_patterns(const float* patterns, int64_t num_patterns, int32_t n
   return detect_patterns(patterns, (int)num_patterns, n, det_mask, num_det, det_out, (cudaStream_t)stream);
 }
 
+int ptyro_detect_patterns_hw(const float* patterns, int64_t num_patterns, int32_t height, int32_t width,
+                             const uint32_t* det_mask, int32_t num_det, double* det_out, void* stream) {
+  if (height < 1 || width < 1 || height > 8192 || width > 8192)
+    return fail(PTYRO_ERR_INVALID, "pattern height and width must be in [1, 8192]");
+  if (num_patterns < 0 || num_patterns > 0x7fffffffLL) return fail(PTYRO_ERR_INVALID, "num_patterns out of range");
+  if (num_det < 1 || num_det > PTYRO_MAX_DETECTORS)
+    return fail(PTYRO_ERR_INVALID, "num_det must be in [1, " + std::to_string(PTYRO_MAX_DETECTORS) + "]");
+  if (num_patterns == 0) return PTYRO_OK;
+  if (!patterns || !det_mask || !det_out) return fail(PTYRO_ERR_INVALID, "NULL array argument");
+  k_detect_patterns_stored<<<(unsigned)num_patterns, kDetThreads, 0, (cudaStream_t)stream>>>(
+      patterns, height * width, det_mask, num_det, det_out);
+  return check_launch("k_detect_patterns_stored");
+}
+
 int ptyro_ms_forward_tilted(const ptyro_ms_params* p, const float* potential, const float* modes,
                             const float* weights, const double* positions, const float* tilts, float* patterns,
                             void* workspace, size_t workspace_bytes, void* stream) {

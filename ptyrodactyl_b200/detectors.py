@@ -29,6 +29,7 @@ from .simulations import (
     _stream_ptr,
     _workspace,
     check_windows,
+    engine_grid,
     ms_params,
     relativistic_wavelength_ang,
 )
@@ -74,6 +75,22 @@ def detector_mask_bits(n: int, fourier_calib: float, voltage_kv: float, annuli: 
     return torch.from_numpy(unshifted.view(np.int32).copy()).to(_device(device))
 
 
+def stored_mask_bits(shape, fourier_calib: float, voltage_kv: float, annuli: Sequence[Annulus],
+                     device=None) -> torch.Tensor:
+    """uint32 (h, w) per-pixel detector bits in the stored patterns' own
+    (fftshifted) order, bit d for annulus d, as an int32 CUDA tensor (same bits):
+    the reference's annular mask (simulations.py:1590-1618) at any height x width."""
+    if not 1 <= len(annuli) <= _lib.MAX_DETECTORS:
+        raise ValueError(f"between 1 and {_lib.MAX_DETECTORS} detectors are supported, got {len(annuli)}")
+    hh, ww = int(shape[0]), int(shape[1])
+    bits = np.zeros((hh, ww), dtype=np.uint32)
+    for d, (inner, outer) in enumerate(annuli):
+        if not (np.isfinite(inner) and np.isfinite(outer) and 0 <= inner <= outer):
+            raise ValueError("annuli must satisfy 0 <= inner <= outer")
+        bits |= annular_mask((hh, ww), fourier_calib, voltage_kv, inner, outer).astype(np.uint32) << np.uint32(d)
+    return torch.from_numpy(bits.view(np.int32).copy()).to(_device(device))
+
+
 def _annuli_of(detector: DetectorConfig, annuli: Optional[Sequence[Annulus]]) -> list:
     if annuli is None:
         return [(detector.collection_inner_mrad, detector.collection_outer_mrad)]
@@ -81,20 +98,27 @@ def _annuli_of(detector: DetectorConfig, annuli: Optional[Sequence[Annulus]]) ->
 
 
 def virtual_detectors(stem4d_data: STEM4D, annuli: Sequence[Annulus]) -> torch.Tensor:
-    """(P, K) float64 masked sums of the stored patterns, one column per annulus."""
+    """(P, K) float64 masked sums of the stored (P, H, W) patterns, one column per
+    annulus, at any pattern height x width."""
     data = stem4d_data.data
-    if data.ndim != 3 or data.shape[1] != data.shape[2]:
-        raise ValueError("stem4d_data.data must be (P, N, N)")
-    n = data.shape[1]
-    if n < 2 or n & (n - 1):
-        raise ValueError(f"pattern edge must be a power of two, got {n}")
+    if data.ndim != 3:
+        raise ValueError("stem4d_data.data must be (P, H, W)")
+    hh, ww = int(data.shape[1]), int(data.shape[2])
+    if not (1 <= hh <= 8192 and 1 <= ww <= 8192):
+        raise ValueError(f"pattern height and width must be in [1, 8192], got ({hh}, {ww})")
     dev = _device(data.device if data.is_cuda else None)
     pats = as_tensor(data, torch.float32, dev).contiguous()
-    mask = detector_mask_bits(n, stem4d_data.fourier_space_calib, stem4d_data.voltage_kv, annuli, dev)
     out = torch.empty((pats.shape[0], len(annuli)), dtype=torch.float64, device=dev)
     lib = _lib.load()
-    _lib.check(lib.ptyro_detect_patterns(pats.data_ptr(), pats.shape[0], n, mask.data_ptr(), len(annuli),
-                                         out.data_ptr(), _stream_ptr(dev)))
+    if hh == ww and hh >= 2 and not hh & (hh - 1):
+        mask = detector_mask_bits(hh, stem4d_data.fourier_space_calib, stem4d_data.voltage_kv, annuli, dev)
+        rc = lib.ptyro_detect_patterns(pats.data_ptr(), pats.shape[0], hh, mask.data_ptr(), len(annuli),
+                                       out.data_ptr(), _stream_ptr(dev))
+    else:
+        mask = stored_mask_bits((hh, ww), stem4d_data.fourier_space_calib, stem4d_data.voltage_kv, annuli, dev)
+        rc = lib.ptyro_detect_patterns_hw(pats.data_ptr(), pats.shape[0], hh, ww, mask.data_ptr(), len(annuli),
+                                          out.data_ptr(), _stream_ptr(dev))
+    _lib.check(rc)
     return out
 
 
@@ -146,23 +170,41 @@ def stem_4d_detectors(pot_slice: PotentialSlices, beam: ProbeModes, microscope: 
                       detector: DetectorConfig, annuli: Optional[Sequence[Annulus]] = None) -> torch.Tensor:
     """``virtual_detectors(stem_4d(...), annuli)`` in one fused forward: (P, K)
     float64, no pattern stored. ``annuli`` defaults to the detector's own
-    (collection_inner_mrad, collection_outer_mrad)."""
+    (collection_inner_mrad, collection_outer_mrad). With ensemble axes, or on a grid
+    other than the pass engine's square power-of-two edges, the integration runs on
+    stem_4d's patterns instead, 1024 probes at a time (same values)."""
     if detector.scan_positions_px is None:
         raise ValueError("detector.scan_positions_px is required")
-    if not microscope.ensemble.is_empty():
-        raise NotImplementedError("ensemble axes are not supported by the B200 engine")
     dev = _device(pot_slice.slices.device if pot_slice.slices.is_cuda else None)
     slices = as_tensor(pot_slice.slices, torch.float32, dev)
     if slices.ndim == 2:
         slices = slices[..., None]
     modes, weights = _beam_on(beam, dev)
     n = modes.shape[0]
+    if not microscope.ensemble.is_empty() or not engine_grid(modes.shape[0], modes.shape[1]):
+        # ensemble axes and any-size grids: stem_4d's own path, then the masked sums
+        # of its patterns, a chunk of probes at a time
+        return _detectors_unfused(pot_slice, beam, microscope, detector, _annuli_of(detector, annuli))
     positions = as_tensor(detector.scan_positions_px, torch.float64, dev).reshape(-1, 2).contiguous()
     calib = min(float(pot_slice.calib), float(beam.calib))
     rings = _annuli_of(detector, annuli)
     mask = detector_mask_bits(n, 1.0 / (n * calib), microscope.voltage_kv, rings, dev)
     return run_forward_detect(slices, pot_slice.slice_thickness, modes, weights, positions, microscope.voltage_kv,
                               calib, detector.real_space_calib_ang, mask, len(rings))
+
+
+def _detectors_unfused(pot_slice: PotentialSlices, beam: ProbeModes, microscope: MicroscopeConfig,
+                       detector: DetectorConfig, rings: list, chunk: int = 1024) -> torch.Tensor:
+    from .simulations import stem_4d
+    from .types import create_detector_config
+    pos = detector.scan_positions_px
+    parts = []
+    for c0 in range(0, pos.shape[0], int(chunk)):
+        sub = create_detector_config(detector.real_space_calib_ang, detector.probe_calibration_pm,
+                                     detector.collection_inner_mrad, detector.collection_outer_mrad,
+                                     scan_positions_px=pos[c0:c0 + int(chunk)])
+        parts.append(virtual_detectors(stem_4d(pot_slice, beam, microscope, sub), rings))
+    return torch.cat(parts, dim=0)
 
 
 def stem_4d_annular(pot_slice: PotentialSlices, beam: ProbeModes, microscope: MicroscopeConfig,

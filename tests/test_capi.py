@@ -254,3 +254,31 @@ def test_forward_to_host_validates_before_launch(lib):
     acc = _p(num_probes=4, flags=_lib.PTYRO_FLAG_ACCUMULATE)
     rc = lib.ptyro_ms_forward_to_host(ctypes.byref(acc), *args, fake, fake, 64, fake, fake + 8)
     assert rc == _lib.PTYRO_ERR_INVALID and "accumulating" in lib.ptyro_last_error().decode()
+
+
+def test_detect_patterns_hw_validates_before_launch(lib):
+    call = lib.ptyro_detect_patterns_hw
+    assert call(None, 4, 0, 8, None, 1, None, None) == _lib.PTYRO_ERR_INVALID
+    assert call(None, 4, 8, 8193, None, 1, None, None) == _lib.PTYRO_ERR_INVALID
+    assert call(None, 4, 8, 8, None, 0, None, None) == _lib.PTYRO_ERR_INVALID
+    assert call(None, 4, 8, 8, None, _lib.MAX_DETECTORS + 1, None, None) == _lib.PTYRO_ERR_INVALID
+    assert call(None, -1, 8, 8, None, 1, None, None) == _lib.PTYRO_ERR_INVALID
+    assert call(None, 0, 7, 5, None, 1, None, None) == _lib.PTYRO_OK
+    rc = call(None, 3, 7, 5, None, 1, None, None)
+    assert rc == _lib.PTYRO_ERR_INVALID and "NULL" in lib.ptyro_last_error().decode()
+
+
+def test_stored_mask_bits_is_the_reference_mask():
+    """Shifted-order bits for any (H, W): bit d is the reference's annulus d."""
+    import numpy as np
+    from ptyrodactyl_b200 import detectors as D
+    annuli = [(0.0, 5.0), (5.0, 12.0)]
+    for shape in [(7, 5), (48, 80), (16, 16)]:
+        bits = D.np.zeros(shape, dtype=np.uint32)
+        for d, (a, b) in enumerate(annuli):
+            bits |= D.annular_mask(shape, 0.05, 200.0, a, b).astype(np.uint32) << np.uint32(d)
+        qy = np.arange(shape[0]) - shape[0] // 2
+        qx = np.arange(shape[1]) - shape[1] // 2
+        q = np.hypot(qy[:, None], qx[None, :]) * 0.05
+        lam = D.relativistic_wavelength_ang(200.0)
+        assert np.array_equal(bits & 1, ((q >= 0.0) & (q <= 5e-3 / lam)).astype(np.uint32))

@@ -134,3 +134,58 @@ def test_stem_4d_clipped_matches_clipped_stem_4d():
     assert torch.equal(clipped.data, want)
     lam = R.relativistic_wavelength_ang(kv)
     assert abs(clipped.fourier_space_calib - (80.0 / 64) / (lam * 1000.0)) < 1e-15
+
+
+@pytest.mark.parametrize("shape", [(48, 80), (33, 33), (7, 5), (64, 64)])
+def test_virtual_detectors_any_pattern_shape(shape):
+    """annular_detector at any (H, W), odd and rectangular, as the reference integrates
+    any pattern shape (simulations.py:1600-1636)."""
+    rng = np.random.default_rng(shape[0] * 7 + shape[1])
+    pats = rng.uniform(0.0, 1.0, (6,) + shape).astype(np.float32)
+    fc, kv = 0.05, 200.0
+    s4 = pb.create_stem4d(torch.from_numpy(pats).cuda(), 0.3, fc, np.zeros((6, 2)), kv)
+    annuli = [(0.0, 5.0), (5.0, 12.0), (12.0, 40.0), (0.0, 1e6)]
+    got = pb.virtual_detectors(s4, annuli).cpu().numpy()
+    for d, (a, b) in enumerate(annuli):
+        want = R.annular_detector(pats, fc, kv, a, b, (6,))
+        assert np.allclose(got[:, d], want, rtol=1e-12, atol=1e-9), (shape, d)
+    det = pb.create_detector_config(0.3, collection_inner_mrad=5.0, collection_outer_mrad=12.0, scan_shape=(2, 3))
+    img = pb.annular_detector(s4, det).data_array.cpu().numpy()
+    assert np.allclose(img, R.annular_detector(pats, fc, kv, 5.0, 12.0, (2, 3)), rtol=1e-12, atol=1e-9)
+
+
+def test_detectors_on_any_size_grid_and_with_ensemble():
+    """stem_4d_detectors where the fused epilogue does not apply (an any-size grid; an
+    ensemble microscope): stem_4d's own path, then the masked sums, equal to
+    annular_detector(stem_4d(...))."""
+    calib, kv = 0.25, 200.0
+    annuli = [(0.0, 12.0), (12.0, 40.0)]
+    rng = np.random.default_rng(5)
+    # any-size grid: 40 x 56
+    h, w = 40, 56
+    pot = rng.uniform(0.0, 20.0, (h, w, 3))
+    probe = R.make_probe(kv, 25.0, (h, w), calib * 100.0, defocus_ang=-30.0)
+    pos = rng.uniform(-2, 2, (5, 2))
+    pots = pb.create_potential_slices(pot, 1.5, calib)
+    beam = pb.create_probe_modes(probe[..., None], np.array([1.0]), calib)
+    mic = pb.create_microscope_config(kv, 25.0, probe_shape=(h, w))
+    det = pb.create_detector_config(calib, scan_positions_px=pos, scan_shape=(5, 1))
+    got = pb.stem_4d_detectors(pots, beam, mic, det, annuli).cpu().numpy()
+    pats = R.stem_4d(pot, 1.5, calib, probe[..., None], np.array([1.0]), calib, kv, pos, calib,
+                     dtype=np.complex128)["data"]
+    for d, (a, b) in enumerate(annuli):
+        assert rel_l2(got[:, d], R.annular_detector(pats, 1.0 / (h * calib), kv, a, b, (5,))) < 1e-5
+    # ensemble axes on the engine grid
+    n = 64
+    pot = rng.uniform(0.0, 20.0, (n, n, 3))
+    probe = R.make_probe(kv, 25.0, (n, n), calib * 100.0, defocus_ang=-30.0)
+    ens = pb.create_ensemble_axes(position_jitter=pb.position_jitter_to_distribution(0.08, 2),
+                                  coherence=pb.coherence_to_distribution(0.5, 0.0, 2))
+    mic = pb.create_microscope_config(kv, 25.0, ensemble=ens, probe_shape=(n, n))
+    pots = pb.create_potential_slices(pot, 1.5, calib)
+    beam = pb.create_probe_modes(probe[..., None], np.array([1.0]), calib)
+    det = pb.create_detector_config(calib, collection_inner_mrad=12.0, collection_outer_mrad=40.0,
+                                    scan_positions_px=pos, scan_shape=(5, 1))
+    fused = pb.stem_4d_annular(pots, beam, mic, det).data_array
+    unfused = pb.annular_detector(pb.stem_4d(pots, beam, mic, det), det).data_array
+    assert torch.allclose(fused, unfused, rtol=1e-12, atol=0.0)
