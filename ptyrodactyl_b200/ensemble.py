@@ -15,6 +15,14 @@ their weights (they must share one energy and tilt), with the combination's
 product weight as the mode weight and its tilt applied by the engine after the scan
 shift (``ptyro_ms_forward_tilted``). Virtual modes are grouped by energy; each group
 is one engine call at its voltage, accumulating into the same patterns.
+
+A tilt is also exactly a change of the first slice's potential: the ramp
+exp(i phi(r)) multiplies the shifted wave just before the first transmission
+exp(i sigma V_0(r)), so it equals the transmission of V_0 + phi / sigma
+(``tilt_folded_slices``, phi wrapped to [-pi, pi) so the float32 sum keeps its
+precision). The derivatives through tilted samples, and tilted samples on the
+any-size grids, run that way: one call per tilt, the adjoint unchanged, and
+dL/dV_0 the same for the folded slice as for V_0.
 """
 
 from __future__ import annotations
@@ -34,6 +42,7 @@ from .simulations import (
     _workspace,
     check_windows,
     engine_grid,
+    interaction_sigma,
     fft2,
     ms_params,
     relativistic_wavelength_ang,
@@ -150,11 +159,29 @@ def _axis_maps(axes, mode_count: int) -> Tuple[str, ...]:
 
 
 class VirtualModes:
-    """Virtual modes of one energy: (n, n, K) complex64 input waves, (K,) weights,
-    (K, 2, n) tilt factors (or None when no sample is tilted), and the voltage."""
+    """Virtual modes of one energy: (H, W, K) complex64 input waves, (K,) weights,
+    (K, 2, n) tilt factors of the square engine grids (or None when no sample is
+    tilted or the grid is not one), (K, 2) tilts in mrad (x, y), and the voltage."""
 
-    def __init__(self, modes: torch.Tensor, weights: torch.Tensor, tilts: Optional[torch.Tensor], voltage_kv: float):
+    def __init__(self, modes: torch.Tensor, weights: torch.Tensor, tilts: Optional[torch.Tensor], voltage_kv: float,
+                 angles: Optional[np.ndarray] = None):
         self.modes, self.weights, self.tilts, self.voltage_kv = modes, weights, tilts, voltage_kv
+        self.angles = np.zeros((modes.shape[2], 2)) if angles is None else np.asarray(angles, dtype=np.float64)
+
+
+def tilt_folded_slices(slices: torch.Tensor, tilt_mrad, voltage_kv: float, calib: float) -> torch.Tensor:
+    """(H, W, S) slices whose first slice carries the beam tilt: V_0 + phi / sigma with
+    phi the phase of _apply_tilt_phase_ramp (simulations.py:891-946; coordinates
+    (index - (size - 1) / 2) * calib, tilt (x, y) in mrad at ``voltage_kv``) wrapped to
+    [-pi, pi). Out of place, so autograd passes dL/dV_0 through unchanged."""
+    h, w = int(slices.shape[0]), int(slices.shape[1])
+    k = 2.0 * np.pi / relativistic_wavelength_ang(voltage_kv)
+    cy = (np.arange(h, dtype=np.float64) - (h - 1) / 2.0) * float(calib)
+    cx = (np.arange(w, dtype=np.float64) - (w - 1) / 2.0) * float(calib)
+    phase = k * ((float(tilt_mrad[0]) / 1000.0) * cx[None, :] + (float(tilt_mrad[1]) / 1000.0) * cy[:, None])
+    phase = phase - 2.0 * np.pi * np.round(phase / (2.0 * np.pi))
+    dv = torch.as_tensor((phase / interaction_sigma(voltage_kv)).astype(np.float32), device=slices.device)
+    return torch.cat([slices[:, :, :1] + dv[:, :, None], slices[:, :, 1:]], dim=2)
 
 
 def _jitter_shift(spectra: torch.Tensor, delta, calib: float) -> torch.Tensor:
@@ -229,16 +256,18 @@ def virtual_modes(ensemble: EnsembleAxes, beam_modes: torch.Tensor, beam: ProbeM
         groups.setdefault(de, []).append((wave, w_inc, tilt))
 
     out = []
+    square = engine_grid(beam_modes.shape[0], beam_modes.shape[1])
     for de, members in groups.items():
         volt = voltage_kv + de / 1000.0
         modes = torch.stack([m[0] for m in members], dim=2).to(torch.complex64)
         wts = torch.tensor([m[1] for m in members], dtype=torch.float32, device=dev)
-        tilted = any(any(t != 0.0 for t in m[2]) for m in members)
+        angles = np.array([np.asarray(m[2], dtype=np.float64) for m in members]).reshape(-1, 2)
+        tilted = bool(np.any(angles != 0.0))
         tilts = None
-        if tilted:
+        if tilted and square:
             tf = np.stack([_tilt_factors(m[2], volt, calib, n) for m in members]).astype(np.complex64)
             tilts = torch.as_tensor(tf, device=dev).contiguous()
-        out.append(VirtualModes(modes, wts, tilts, volt))
+        out.append(VirtualModes(modes, wts, tilts, volt, angles))
     return out
 
 
@@ -252,12 +281,15 @@ def run_forward_ensemble(slices: torch.Tensor, slice_thickness: float, groups: L
     out = torch.zeros((num_probes, h, w), dtype=torch.float32, device=dev)
     if num_probes == 0:
         return out
-    if not engine_grid(h, w):  # the any-size forward, accumulating each energy's group
+    if not engine_grid(h, w):  # the any-size forward, accumulating each energy's group, one call per tilt
         for g in groups:
-            if g.tilts is not None:
-                raise NotImplementedError("tilted coherence samples need a square grid with a power-of-two edge")
-            run_forward_any(slices, slice_thickness, g.modes.contiguous(), g.weights, positions, g.voltage_kv,
-                            calib_ang, shift_calib_ang, out=out, accumulate=True)
+            for tilt in np.unique(g.angles, axis=0):
+                idx = np.flatnonzero(np.all(g.angles == tilt, axis=1))
+                sl = slices if not np.any(tilt != 0.0) else tilt_folded_slices(slices, tilt, g.voltage_kv, calib_ang)
+                sel = torch.as_tensor(idx, device=dev)
+                run_forward_any(sl, slice_thickness, g.modes.index_select(2, sel).contiguous(),
+                                g.weights.index_select(0, sel).contiguous(), positions, g.voltage_kv,
+                                calib_ang, shift_calib_ang, out=out, accumulate=True)
         return out
     n = h
     for g in groups:
@@ -280,6 +312,15 @@ def run_forward_ensemble(slices: torch.Tensor, slice_thickness: float, groups: L
     return out
 
 
+def _host(t: torch.Tensor) -> np.ndarray:
+    """A constant tensor's values as float64 NumPy, also inside a torch.func transform
+    (where operations on it would be wrapped and have no storage)."""
+    while torch._C._functorch.is_functorch_wrapped_tensor(t):
+        t = torch._C._functorch.get_unwrapped(t)
+    with torch._C._DisableFuncTorch():
+        return t.detach().cpu().numpy().astype(np.float64)
+
+
 def ensemble_patterns_differentiable(slices: torch.Tensor, slice_thickness: float, beam: ProbeModes,
                                      ensemble: EnsembleAxes, modes: torch.Tensor, weights: torch.Tensor,
                                      voltage_kv: float, calib_ang: float, positions: torch.Tensor,
@@ -293,8 +334,10 @@ def ensemble_patterns_differentiable(slices: torch.Tensor, slice_thickness: floa
     sum_c w_c sum_j w_j stem_4d(modes, w_modes, positions + delta_j * s, voltage + dE_c),
     with s = shift_calib_ang / calib_ang: the jitter's Fourier shift at the ensemble
     calibration composes with the scan shift into one shift of the scan position.
-    Each energy is one differentiable engine call over all jitter copies of the scan.
-    Tilted coherence samples and COHERENT axes raise ``NotImplementedError``."""
+    Each coherence sample is one differentiable engine call over all jitter copies of
+    the scan, at its energy, a tilted sample with its tilt folded into the first
+    slice's potential (``tilt_folded_slices``). COHERENT axes raise
+    ``NotImplementedError``."""
     axes = ensemble_axes_for_cbed(ensemble, beam)
     mode_count = modes.shape[2]
     maps = _axis_maps(axes, mode_count)
@@ -303,9 +346,9 @@ def ensemble_patterns_differentiable(slices: torch.Tensor, slice_thickness: floa
     dev = slices.device
     sel, w_modes = None, weights
     jit, w_jit = np.zeros((1, 2)), np.ones(1)
-    energies: dict = {0.0: 1.0}
+    energies: dict = {(0.0, 0.0, 0.0): 1.0}  # (dE eV, tilt x mrad, tilt y mrad) -> weight
     for axis, kind in zip(axes, maps):
-        smp, wts = axis.samples.detach().numpy(), axis.weights.detach().numpy()
+        smp, wts = _host(axis.samples), _host(axis.weights)
         if kind == AXIS_PROBE_MODES:
             idx = smp[:, 0].astype(np.int64)
             if np.any(idx < 0) or np.any(idx >= mode_count):
@@ -318,11 +361,10 @@ def ensemble_patterns_differentiable(slices: torch.Tensor, slice_thickness: floa
         elif kind == AXIS_POSITION_JITTER:
             jit, w_jit = smp, wts
         else:
-            if np.any(smp[:, 1:3] != 0.0):
-                raise NotImplementedError("derivatives through tilted coherence samples are not supported")
             energies = {}
-            for de, w in zip(smp[:, 0], wts):
-                energies[float(de)] = energies.get(float(de), 0.0) + float(w)
+            for row, w in zip(smp, wts):
+                key = (float(row[0]), float(row[1]), float(row[2]))
+                energies[key] = energies.get(key, 0.0) + float(w)
     use_modes = modes if sel is None else modes.index_select(2, sel)
     scale = float(shift_calib_ang) / float(calib_ang)
     offsets = torch.as_tensor(jit * scale, dtype=torch.float64, device=dev)  # (J, 2)
@@ -331,9 +373,11 @@ def ensemble_patterns_differentiable(slices: torch.Tensor, slice_thickness: floa
     wj = torch.as_tensor(w_jit, dtype=torch.float32, device=dev)
     from .autodiff import stem_4d_patterns
     out = None
-    for de, w_e in energies.items():
-        pat = stem_4d_patterns(slices, use_modes, w_modes.to(torch.float32), pos_all, slice_thickness,
-                               voltage_kv + de / 1000.0, calib_ang, shift_calib_ang)
+    for (de, tx, ty), w_e in energies.items():
+        volt = voltage_kv + de / 1000.0
+        sl = slices if tx == 0.0 and ty == 0.0 else tilt_folded_slices(slices, (tx, ty), volt, calib_ang)
+        pat = stem_4d_patterns(sl, use_modes, w_modes.to(torch.float32), pos_all, slice_thickness,
+                               volt, calib_ang, shift_calib_ang)
         part = float(w_e) * torch.einsum("j,jpyx->pyx", wj, pat.reshape((J, P) + tuple(pat.shape[1:])))
         out = part if out is None else out + part
     return out

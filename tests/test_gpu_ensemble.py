@@ -134,20 +134,68 @@ def test_stem_4d_ensemble_gradients_match_oracle(jitter, energy):
     assert rel_l2(ps.grad.cpu().numpy(), dpos) < TOL
 
 
-def test_ensemble_derivatives_refuse_tilts():
-    pot, modes, w = _setup(n=32, s=2, m=1, seed=2)
-    ens = pb.create_ensemble_axes(coherence=pb.coherence_to_distribution(0.3, 0.2, 2))
-    mic = pb.create_microscope_config(200.0, 25.0, ensemble=ens, probe_shape=(32, 32))
-    det = pb.create_detector_config(0.3, scan_positions_px=np.zeros((1, 2)))
-    V = torch.tensor(pot, dtype=torch.float32, device="cuda", requires_grad=True)
-    with pytest.raises(NotImplementedError, match="tilted"):
-        pb.stem_4d(pb.PotentialSlices(V, 1.7, 0.25), pb.create_probe_modes(modes, w, 0.25), mic, det)
+@pytest.mark.parametrize("h,w", [(32, 32), (24, 40)])
+def test_ensemble_derivatives_through_tilts(h, w):
+    """Reverse mode through tilted coherence samples (energy spread and angular
+    divergence together), on the engine's square grid and on a rectangular any-size
+    grid: the patterns against the oracle's ensemble branch (which applies the tilt
+    ramp to the shifted wave), and the directional derivatives of L = sum(g * I)
+    along random directions in V, the beam modes and the scan positions against
+    central differences of the float64 oracle."""
+    rng = np.random.default_rng(h + w)
+    pot = rng.uniform(0.0, 30.0, (h, w, 2))
+    probe = R.make_probe(200.0, 25.0, (h, w), 25.0, defocus_ang=-30.0)
+    modes, wts = probe[..., None], np.array([1.0])
+    pos = rng.uniform(-1.5, 1.5, (3, 2))
+    g = rng.normal(size=(3, h, w))
+    ens = pb.create_ensemble_axes(coherence=pb.coherence_to_distribution(0.4, 0.25, 2))
+    mic = pb.create_microscope_config(200.0, 25.0, ensemble=ens, probe_shape=(h, w))
+    det = pb.create_detector_config(0.3, scan_positions_px=pos)
+    dev = torch.device("cuda")
+    V = torch.tensor(pot, dtype=torch.float32, device=dev, requires_grad=True)
+    md = torch.tensor(modes.astype(np.complex64), device=dev, requires_grad=True)
+    ps = torch.tensor(pos, dtype=torch.float64, device=dev, requires_grad=True)
+    det_t = dataclasses.replace(det, scan_positions_px=ps)
+    s4 = pb.stem_4d(pb.PotentialSlices(V, 1.7, 0.25), pb.ProbeModes(md, torch.ones(1, device=dev), 0.25), mic,
+                    det_t)
+    (s4.data * torch.as_tensor(g, dtype=torch.float32, device=dev)).sum().backward()
+    beam = pb.create_probe_modes(modes, wts, 0.25)
+    axes = [_axes_oracle(a) for a in pb.ensemble_axes_for_cbed(ens, beam)]
+
+    def loss(pot_, modes_, pos_):
+        return float(np.sum(g * R.stem_4d_ensemble(pot_, 1.7, 0.25, modes_, 0.25, 200.0, pos_, 0.3, axes)))
+
+    want = R.stem_4d_ensemble(pot, 1.7, 0.25, modes, 0.25, 200.0, pos, 0.3, axes)
+    assert rel_l2(s4.data.detach().cpu().numpy(), want) < TOL
+    dV = rng.normal(size=pot.shape)
+    dM = rng.normal(size=modes.shape) + 1j * rng.normal(size=modes.shape)
+    dP = rng.normal(size=pos.shape)
+    eps = 1e-4
+    fd_v = (loss(pot + eps * dV, modes, pos) - loss(pot - eps * dV, modes, pos)) / (2 * eps)
+    fd_m = (loss(pot, modes + eps * dM * np.abs(modes).max(), pos)
+            - loss(pot, modes - eps * dM * np.abs(modes).max(), pos)) / (2 * eps * np.abs(modes).max())
+    fd_p = (loss(pot, modes, pos + eps * dP) - loss(pot, modes, pos - eps * dP)) / (2 * eps)
+    got_v = float(np.sum(V.grad.cpu().numpy() * dV))
+    # torch's complex gradient is dL/d(re) + i dL/d(im): the directional derivative is Re(conj(grad) * d)
+    got_m = float(np.sum(np.real(np.conj(md.grad.cpu().numpy()) * dM)))
+    got_p = float(np.sum(ps.grad.cpu().numpy() * dP))
+    for got, fd in [(got_v, fd_v), (got_m, fd_m), (got_p, fd_p)]:
+        assert abs(got - fd) <= 2e-3 * abs(fd) + 1e-6 * abs(want).sum(), (got, fd)
+    # forward mode through the same ensemble: torch.func.jvp along dV
+    beam_c = pb.ProbeModes(md.detach(), torch.ones(1, device=dev), 0.25)
+
+    def fwd(v):
+        return pb.stem_4d(pb.PotentialSlices(v, 1.7, 0.25), beam_c, mic, det).data
+
+    _, tan = torch.func.jvp(fwd, (V.detach(),), (torch.as_tensor(dV, dtype=torch.float32, device=dev),))
+    got_jv = float(np.sum(g * tan.cpu().numpy()))
+    assert abs(got_jv - fd_v) <= 2e-3 * abs(fd_v) + 1e-6 * abs(want).sum(), (got_jv, fd_v)
 
 
 def test_ensemble_on_a_rectangular_grid():
     """Jitter and energy-spread axes on a 40 x 56 grid (the any-size path, one
-    accumulating forward per energy) against the oracle's ensemble branch; tilted
-    samples need the engine's square grids."""
+    accumulating forward per energy) against the oracle's ensemble branch, with
+    and without tilted coherence samples."""
     rng = np.random.default_rng(6)
     h, w, s = 40, 56, 3
     pot = rng.uniform(0.0, 40.0, (h, w, s))
@@ -165,7 +213,11 @@ def test_ensemble_on_a_rectangular_grid():
     want = R.stem_4d_ensemble(pot, 1.7, 0.25, modes, 0.25, 200.0, pos, 0.3, axes)
     assert tuple(s4.data.shape) == (3, h, w)
     assert rel_l2(s4.data.cpu().numpy(), want) < TOL
-    tilted = pb.create_ensemble_axes(coherence=pb.coherence_to_distribution(0.5, 0.2, 2))
+    # tilted samples: the tilt folded into the first slice's potential, one call per tilt
+    tilted = pb.create_ensemble_axes(position_jitter=pb.position_jitter_to_distribution(0.08, 2),
+                                     coherence=pb.coherence_to_distribution(0.5, 0.2, 2))
     mic_t = pb.create_microscope_config(200.0, 25.0, ensemble=tilted, probe_shape=(h, w))
-    with pytest.raises(NotImplementedError, match="tilted"):
-        pb.stem_4d(pb.create_potential_slices(pot, 1.7, 0.25), beam, mic_t, det)
+    s4t = pb.stem_4d(pb.create_potential_slices(pot, 1.7, 0.25), beam, mic_t, det)
+    axes_t = [_axes_oracle(a) for a in pb.ensemble_axes_for_cbed(tilted, beam)]
+    want_t = R.stem_4d_ensemble(pot, 1.7, 0.25, modes, 0.25, 200.0, pos, 0.3, axes_t)
+    assert rel_l2(s4t.data.cpu().numpy(), want_t) < TOL
