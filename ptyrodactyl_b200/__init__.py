@@ -10,8 +10,11 @@ from .types import (  # noqa: F401
     AtomicSliceData,
     Distribution,
     ReductionMode,
+    TRIVIAL,
+    TRIVIAL_DISTRIBUTION,
     create_distribution,
     create_ensemble_axes,
+    create_trivial_distribution,
     CalibratedArray,
     DetectorConfig,
     EnsembleAxes,
@@ -26,6 +29,7 @@ from .types import (  # noqa: F401
     create_probe_modes,
     create_stem4d,
 )
+from .reduce import apply_distribution, apply_distributions  # noqa: F401
 from .simulations import (  # noqa: F401
     aberration,
     cbed_amplitude,

@@ -336,49 +336,59 @@ def ensemble_patterns_differentiable(slices: torch.Tensor, slice_thickness: floa
     calibration composes with the scan shift into one shift of the scan position.
     Each coherence sample is one differentiable engine call over all jitter copies of
     the scan, at its energy, a tilted sample with its tilt folded into the first
-    slice's potential (``tilt_folded_slices``). COHERENT axes raise
-    ``NotImplementedError``."""
+    slice's potential (``tilt_folded_slices``). An explicit probe-mode axis may be
+    COHERENT (its modes summed with its weights into one wave); COHERENT jitter and
+    coherence axes raise ``NotImplementedError``. The axes' weights are
+    differentiable too (the reduction's weighted sums run in torch)."""
     axes = ensemble_axes_for_cbed(ensemble, beam)
     mode_count = modes.shape[2]
     maps = _axis_maps(axes, mode_count)
-    if any(a.reduction is not ReductionMode.INCOHERENT for a in axes):
-        raise NotImplementedError("derivatives through COHERENT ensemble axes are not supported")
+    if any(a.reduction is not ReductionMode.INCOHERENT and kind != AXIS_PROBE_MODES for a, kind in zip(axes, maps)):
+        raise NotImplementedError("derivatives through COHERENT jitter or coherence axes are not supported")
     dev = slices.device
-    sel, w_modes = None, weights
-    jit, w_jit = np.zeros((1, 2)), np.ones(1)
-    energies: dict = {(0.0, 0.0, 0.0): 1.0}  # (dE eV, tilt x mrad, tilt y mrad) -> weight
+    sel, w_modes, coherent_modes = None, weights, False
+    jit, w_jit = np.zeros((1, 2)), torch.ones(1, dtype=torch.float64)
+    # (dE eV, tilt x mrad, tilt y mrad) -> rows of the coherence axis
+    energies: dict = {(0.0, 0.0, 0.0): None}
+    w_coh = torch.ones(1, dtype=torch.float64)
     for axis, kind in zip(axes, maps):
-        smp, wts = _host(axis.samples), _host(axis.weights)
+        smp = _host(axis.samples)
         if kind == AXIS_PROBE_MODES:
             idx = smp[:, 0].astype(np.int64)
             if np.any(idx < 0) or np.any(idx >= mode_count):
                 raise ValueError("probe mode index out of range")
-            if ensemble.probe_modes is not None:  # an explicit axis: its own constant weights
+            if ensemble.probe_modes is not None:  # an explicit axis: its own weights
                 sel = torch.as_tensor(idx, device=dev)
-                w_modes = torch.as_tensor(wts, dtype=torch.float32, device=dev)
+                w_modes = axis.weights.to(device=dev, dtype=torch.float32)
+                coherent_modes = axis.reduction is ReductionMode.COHERENT
             elif not np.array_equal(idx, np.arange(mode_count)):
                 raise ValueError("the beam's mode axis must list every mode once")
         elif kind == AXIS_POSITION_JITTER:
-            jit, w_jit = smp, wts
+            jit, w_jit = smp, axis.weights
         else:
-            energies = {}
-            for row, w in zip(smp, wts):
-                key = (float(row[0]), float(row[1]), float(row[2]))
-                energies[key] = energies.get(key, 0.0) + float(w)
+            energies, w_coh = {}, axis.weights
+            for r, row in enumerate(smp):
+                energies.setdefault((float(row[0]), float(row[1]), float(row[2])), []).append(r)
     use_modes = modes if sel is None else modes.index_select(2, sel)
+    if coherent_modes:
+        # a COHERENT mode axis: one wave, the weighted sum of the selected modes
+        use_modes = (use_modes * w_modes.to(use_modes.dtype)).sum(dim=2, keepdim=True)
+        w_modes = torch.ones(1, dtype=torch.float32, device=dev)
     scale = float(shift_calib_ang) / float(calib_ang)
     offsets = torch.as_tensor(jit * scale, dtype=torch.float64, device=dev)  # (J, 2)
     J, P = offsets.shape[0], positions.shape[0]
     pos_all = (positions[None, :, :] + offsets[:, None, :]).reshape(J * P, 2)
-    wj = torch.as_tensor(w_jit, dtype=torch.float32, device=dev)
+    wj = w_jit.to(device=dev, dtype=torch.float32)
+    w_coh = w_coh.to(device=dev, dtype=torch.float32)
     from .autodiff import stem_4d_patterns
     out = None
-    for (de, tx, ty), w_e in energies.items():
+    for (de, tx, ty), rows in energies.items():
         volt = voltage_kv + de / 1000.0
         sl = slices if tx == 0.0 and ty == 0.0 else tilt_folded_slices(slices, (tx, ty), volt, calib_ang)
         pat = stem_4d_patterns(sl, use_modes, w_modes.to(torch.float32), pos_all, slice_thickness,
                                volt, calib_ang, shift_calib_ang)
-        part = float(w_e) * torch.einsum("j,jpyx->pyx", wj, pat.reshape((J, P) + tuple(pat.shape[1:])))
+        w_e = w_coh[0] if rows is None else w_coh[torch.as_tensor(rows, device=dev)].sum()
+        part = w_e * torch.einsum("j,jpyx->pyx", wj, pat.reshape((J, P) + tuple(pat.shape[1:])))
         out = part if out is None else out + part
     return out
 

@@ -411,6 +411,13 @@ def _needs_autodiff(*tensors) -> bool:
     return False
 
 
+def _ensemble_weights(microscope: MicroscopeConfig) -> list:
+    """The weight tensors of the microscope's ensemble axes (a derivative may be taken
+    with respect to them)."""
+    ens = microscope.ensemble
+    return [d.weights for d in (ens.probe_modes, ens.position_jitter, ens.coherence) if d is not None]
+
+
 def _beam_on(beam: ProbeModes, dev) -> tuple:
     modes = beam.modes if beam.modes.ndim == 3 else beam.modes[..., None]
     modes = as_tensor(modes, torch.complex64, dev)
@@ -442,7 +449,7 @@ def stem_4d(pot_slice: PotentialSlices, beam: ProbeModes, microscope: Microscope
     calib = min(float(pot_slice.calib), float(beam.calib))
     if not microscope.ensemble.is_empty():
         # per position, cbed_image's ensemble branch (simulations.py:1163-1193)
-        if _needs_autodiff(slices, modes, positions, weights):
+        if _needs_autodiff(slices, modes, positions, weights, *_ensemble_weights(microscope)):
             from .ensemble import ensemble_patterns_differentiable
             data = ensemble_patterns_differentiable(slices, pot_slice.slice_thickness, beam, microscope.ensemble,
                                                     modes, weights, microscope.voltage_kv, calib, positions,
@@ -594,9 +601,19 @@ def cbed_image(pot_slices: PotentialSlices, beam: ProbeModes, microscope: Micros
     calib = min(float(pot_slices.calib), float(beam.calib))
     zero = torch.zeros((1, 2), dtype=torch.float64, device=dev)
     if not microscope.ensemble.is_empty():
-        from .ensemble import ensemble_patterns
-        data = ensemble_patterns(slices, pot_slices.slice_thickness, beam, microscope.ensemble,
-                                 microscope.voltage_kv, calib, zero, calib)[0]
+        if _needs_autodiff(slices, modes, weights, *_ensemble_weights(microscope)):
+            from .ensemble import ensemble_patterns_differentiable
+            data = ensemble_patterns_differentiable(slices, pot_slices.slice_thickness, beam, microscope.ensemble,
+                                                    modes, weights, microscope.voltage_kv, calib, zero, calib)[0]
+        else:
+            from .ensemble import ensemble_patterns
+            data = ensemble_patterns(slices, pot_slices.slice_thickness, beam, microscope.ensemble,
+                                     microscope.voltage_kv, calib, zero, calib)[0]
+    elif _needs_autodiff(slices, modes, weights):
+        # the same engine call at the one zero position, through the adjoint kernels
+        from .autodiff import stem_4d_patterns
+        data = stem_4d_patterns(slices, modes, weights, zero, pot_slices.slice_thickness, microscope.voltage_kv,
+                                calib, calib)[0]
     else:
         status = _lib.new_status(dev)
         data = run_forward(slices, pot_slices.slice_thickness, modes, weights, zero,

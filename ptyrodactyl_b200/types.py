@@ -118,12 +118,26 @@ def create_distribution(samples, weights, reduction=ReductionMode.INCOHERENT, ax
         raise ValueError("weights must be finite")
     if bool((wts < 0).any()):
         raise ValueError("weights must be non-negative")
-    if float(wts.sum()) <= 0.0:
+    if float(wts.detach().sum()) <= 0.0:
         raise ValueError("weights must have positive total probability")
     clipped = wts.clamp(min=0.0)
-    total = float(clipped.sum())
-    norm = clipped / total if total > 0 else torch.full_like(clipped, 1.0 / clipped.shape[0])
+    norm = clipped / clipped.sum()  # a tensor total: the normalisation's full derivative
     return Distribution(smp, norm, mode, axis_id)
+
+
+def create_trivial_distribution(sample_dim: int = 1, reduction=ReductionMode.INCOHERENT,
+                                axis_id: Optional[str] = "trivial") -> Distribution:
+    """types/distributions.py:190-242: one zero sample of width ``sample_dim`` with unit
+    weight."""
+    dim = int(sample_dim)
+    if dim <= 0:
+        raise ValueError("sample_dim must be positive")
+    return create_distribution(torch.zeros((1, dim), dtype=torch.float64), torch.ones(1, dtype=torch.float64),
+                               reduction, axis_id)
+
+
+TRIVIAL_DISTRIBUTION = create_trivial_distribution()
+TRIVIAL = TRIVIAL_DISTRIBUTION
 
 
 @dataclass(frozen=True)

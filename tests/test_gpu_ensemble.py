@@ -221,3 +221,74 @@ def test_ensemble_on_a_rectangular_grid():
     axes_t = [_axes_oracle(a) for a in pb.ensemble_axes_for_cbed(tilted, beam)]
     want_t = R.stem_4d_ensemble(pot, 1.7, 0.25, modes, 0.25, 200.0, pos, 0.3, axes_t)
     assert rel_l2(s4t.data.cpu().numpy(), want_t) < TOL
+
+
+def test_cbed_image_is_differentiable():
+    """cbed_image under reverse mode: the engine's adjoint at the one zero position,
+    against the oracle's adjoint of stem_4d there (cbed_image's unshifted beam)."""
+    pot, modes, w = _setup(n=64, s=3, m=2, seed=5)
+    g = np.random.default_rng(2).normal(size=(64, 64))
+    dev = torch.device("cuda")
+    V = torch.tensor(pot, dtype=torch.float32, device=dev, requires_grad=True)
+    md = torch.tensor(modes.astype(np.complex64), device=dev, requires_grad=True)
+    wt = torch.tensor(w, dtype=torch.float32, device=dev)
+    mic = pb.create_microscope_config(200.0, 25.0, probe_shape=(64, 64))
+    img = pb.cbed_image(pb.PotentialSlices(V, 1.7, 0.25), pb.ProbeModes(md, wt, 0.25), mic).data_array
+    (img * torch.as_tensor(g, dtype=torch.float32, device=dev)).sum().backward()
+    want = R.stem_4d(pot, 1.7, 0.25, modes, w, 0.25, 200.0, np.zeros((1, 2)), 0.25)["data"][0]
+    assert rel_l2(img.detach().cpu().numpy(), want) < TOL
+    dv, dm = R.stem_4d_vjp(pot, 1.7, 0.25, modes, w, 0.25, 200.0, np.zeros((1, 2)), 0.25, g[None])
+    assert rel_l2(V.grad.cpu().numpy(), dv) < TOL
+    assert rel_l2(md.grad.cpu().numpy(), np.conj(dm)) < TOL
+
+
+def test_ensemble_axis_weights_and_coherent_modes_are_differentiable():
+    """Reverse mode through an explicit COHERENT probe-mode axis (its modes summed with
+    its weights into one wave), an explicit jitter axis and an energy-spread axis,
+    with respect to the potential and the two explicit axes' raw weights (through
+    create_distribution's normalisation): directional derivatives against float64
+    central differences of the oracle's ensemble branch."""
+    pot, modes, w = _setup(n=32, s=2, m=2, seed=21)
+    rng = np.random.default_rng(9)
+    pos = rng.uniform(-1.5, 1.5, (3, 2))
+    g = rng.normal(size=(3, 32, 32))
+    jsmp = np.array([[0.05, -0.03], [-0.04, 0.06]])
+    dev = torch.device("cuda")
+    wm = torch.tensor([0.7, 0.3], dtype=torch.float64, requires_grad=True)
+    wj = torch.tensor([0.45, 0.55], dtype=torch.float64, requires_grad=True)
+    mode_axis = pb.create_distribution(np.arange(2.0)[:, None], wm, pb.ReductionMode.COHERENT, "probe_modes")
+    jit_axis = pb.create_distribution(jsmp, wj, pb.ReductionMode.INCOHERENT, "position_jitter")
+    coh = pb.coherence_to_distribution(0.4, 0.0, 2)
+    ens = pb.create_ensemble_axes(probe_modes=mode_axis, position_jitter=jit_axis, coherence=coh)
+    mic = pb.create_microscope_config(200.0, 25.0, ensemble=ens, probe_shape=(32, 32))
+    det = pb.create_detector_config(0.3, scan_positions_px=pos)
+    V = torch.tensor(pot, dtype=torch.float32, device=dev, requires_grad=True)
+    beam = pb.ProbeModes(torch.tensor(modes.astype(np.complex64), device=dev),
+                         torch.tensor(w, dtype=torch.float32, device=dev), 0.25)
+    s4 = pb.stem_4d(pb.PotentialSlices(V, 1.7, 0.25), beam, mic, det)
+    (s4.data * torch.as_tensor(g, dtype=torch.float32, device=dev)).sum().backward()
+
+    def axes_of(wm_, wj_):
+        return [(np.arange(2.0)[:, None], wm_ / wm_.sum(), "coherent", "probe_modes"),
+                (jsmp, wj_ / wj_.sum(), "incoherent", "position_jitter"), _axes_oracle(coh)]
+
+    def loss(pot_, wm_, wj_):
+        return float(np.sum(g * R.stem_4d_ensemble(pot_, 1.7, 0.25, modes, 0.25, 200.0, pos, 0.3,
+                                                    axes_of(wm_, wj_))))
+
+    wm0, wj0 = np.array([0.7, 0.3]), np.array([0.45, 0.55])
+    want = R.stem_4d_ensemble(pot, 1.7, 0.25, modes, 0.25, 200.0, pos, 0.3, axes_of(wm0, wj0))
+    assert rel_l2(s4.data.detach().cpu().numpy(), want) < TOL
+    dV, dwm, dwj = rng.normal(size=pot.shape), rng.normal(size=2), rng.normal(size=2)
+    eps = 1e-5
+    checks = [
+        (float(np.sum(V.grad.cpu().numpy() * dV)),
+         (loss(pot + eps * dV, wm0, wj0) - loss(pot - eps * dV, wm0, wj0)) / (2 * eps)),
+        (float(np.sum(wm.grad.numpy() * dwm)),
+         (loss(pot, wm0 + eps * dwm, wj0) - loss(pot, wm0 - eps * dwm, wj0)) / (2 * eps)),
+        (float(np.sum(wj.grad.numpy() * dwj)),
+         (loss(pot, wm0, wj0 + eps * dwj) - loss(pot, wm0, wj0 - eps * dwj)) / (2 * eps)),
+    ]
+    scale = float(np.abs(g * want).sum())
+    for got, fd in checks:
+        assert abs(got - fd) <= 2e-3 * abs(fd) + 1e-5 * scale, (got, fd)
