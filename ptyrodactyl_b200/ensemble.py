@@ -206,8 +206,11 @@ def _tilt_factors(tilt_mrad, voltage_kv: float, calib: float, n: int) -> np.ndar
 
 
 def virtual_modes(ensemble: EnsembleAxes, beam_modes: torch.Tensor, beam: ProbeModes, voltage_kv: float,
-                  calib: float) -> List[VirtualModes]:
-    """Expand the ensemble of ``beam`` into engine calls (one per energy)."""
+                  calib: float, mixed: Optional[list] = None) -> List[VirtualModes]:
+    """Expand the ensemble of ``beam`` into engine calls (one per energy). An
+    incoherent combination whose coherent samples differ in energy or tilt is
+    appended to ``mixed`` as (weight, [(wave, weight, dE, tilt), ...]) when a list is
+    given, and raises ``NotImplementedError`` otherwise."""
     axes = ensemble_axes_for_cbed(ensemble, beam)
     n = beam_modes.shape[0]
     mode_count = beam_modes.shape[2]
@@ -236,24 +239,28 @@ def virtual_modes(ensemble: EnsembleAxes, beam_modes: torch.Tensor, beam: ProbeM
     groups = {}  # energy -> list of (wave, weight, tilt)
     for inc in itertools.product(*[range(samples[i].shape[0]) for i in incoherent]):
         w_inc = float(np.prod([weights[i][k] for i, k in zip(incoherent, inc)])) if incoherent else 1.0
-        wave = None
-        shared = None
+        parts = []  # the coherent samples of this incoherent combination: (wave, weight, dE, tilt)
         for coh in itertools.product(*[range(samples[i].shape[0]) for i in coherent]):
             choice = dict(zip(incoherent, inc))
             choice.update(zip(coherent, coh))
             mode, delta, de, tilt = update(choice)
-            if shared is None:
-                shared = (de, tuple(tilt))
-            elif shared != (de, tuple(tilt)):
-                raise NotImplementedError("coherent sums over energy or tilt samples are not supported")
             w_coh = float(np.prod([weights[i][k] for i, k in zip(coherent, coh)])) if coherent else 1.0
             if np.any(delta != 0.0):
                 part = _jitter_shift(spectra[mode], delta, calib)
             else:
                 part = beam_modes[:, :, mode]
+            parts.append((part, w_coh, de, tuple(tilt)))
+        if len({(p[2], p[3]) for p in parts}) > 1:
+            # a coherent sum across energies or tilts: separate operators per sample,
+            # summed as amplitudes (mixed_coherent_patterns)
+            if mixed is None:
+                raise NotImplementedError("coherent sums over energy or tilt samples are not supported")
+            mixed.append((w_inc, parts))
+            continue
+        wave = None
+        for part, w_coh, _, _ in parts:
             wave = part * w_coh if wave is None else wave + part * w_coh
-        de, tilt = shared
-        groups.setdefault(de, []).append((wave, w_inc, tilt))
+        groups.setdefault(parts[0][2], []).append((wave, w_inc, parts[0][3]))
 
     out = []
     square = engine_grid(beam_modes.shape[0], beam_modes.shape[1])
@@ -402,5 +409,57 @@ def ensemble_patterns(slices: torch.Tensor, slice_thickness: float, beam: ProbeM
     dev = _device(slices.device)
     modes = beam.modes if beam.modes.ndim == 3 else beam.modes[..., None]
     modes = as_tensor(modes, torch.complex64, dev).contiguous()
-    groups = virtual_modes(ensemble, modes, beam, voltage_kv, calib_ang)
-    return run_forward_ensemble(slices, slice_thickness, groups, positions, calib_ang, shift_calib_ang)
+    mixed: list = []
+    groups = virtual_modes(ensemble, modes, beam, voltage_kv, calib_ang, mixed)
+    if groups:
+        out = run_forward_ensemble(slices, slice_thickness, groups, positions, calib_ang, shift_calib_ang)
+    else:
+        out = torch.zeros((positions.shape[0],) + tuple(modes.shape[:2]), dtype=torch.float32, device=dev)
+    if mixed:
+        mixed_coherent_patterns(out, slices, slice_thickness, mixed, voltage_kv, positions, calib_ang,
+                                shift_calib_ang)
+    return out
+
+
+def mixed_coherent_patterns(out: torch.Tensor, slices: torch.Tensor, slice_thickness: float, mixed: list,
+                            voltage_kv: float, positions: torch.Tensor, calib_ang: float, shift_calib_ang: float,
+                            chunk_bytes: int = 1 << 30) -> torch.Tensor:
+    """Adds sum_i w_i |sum_c w_c A(wave_c; V + dE_c, tilt_c)|^2 to ``out`` (P, n, n):
+    the incoherent combinations whose coherent samples differ in energy or tilt
+    (apply_distributions, reduce.py:93-201). Every coherent sample is one amplitude
+    forward (``ptyro_ms_amplitudes``, fftshifted complex64, with the sample's tilt
+    after the scan shift) at its voltage; the weighted amplitudes are summed and
+    squared on the device, ``chunk_bytes`` of amplitudes at a time."""
+    lib = _lib.load()
+    dev = slices.device
+    n, w = int(out.shape[1]), int(out.shape[2])
+    if not engine_grid(n, w):
+        raise NotImplementedError("coherent sums over energy or tilt samples need a square grid with a "
+                                  "power-of-two edge")
+    num_probes = positions.shape[0]
+    chunk = max(1, min(num_probes, int(chunk_bytes) // (8 * n * n)))
+    for w_inc, parts in mixed:
+        for c0 in range(0, num_probes, chunk):
+            pos = positions[c0:c0 + chunk].contiguous()
+            field = None
+            for wave, w_coh, de, tilt in parts:
+                volt = voltage_kv + de / 1000.0
+                mode = wave[:, :, None].to(torch.complex64).contiguous()
+                tilts = None
+                if any(t != 0.0 for t in tilt):
+                    tilts = torch.as_tensor(_tilt_factors(tilt, volt, calib_ang, n)[None].astype(np.complex64),
+                                            device=dev).contiguous()
+                _, f = check_windows(slices, mode, None, pos.shape[0])
+                prm = ms_params(n, slices.shape[2], 1, pos.shape[0], volt, slice_thickness, calib_ang,
+                                shift_calib_ang, slices.stride(), mode.stride(), 0, 0, f)
+                amps = torch.empty((pos.shape[0], 1, n, n), dtype=torch.complex64, device=dev)
+                nbytes = lib.ptyro_ms_workspace_bytes(ctypes.byref(prm))
+                if nbytes == 0:
+                    _lib.check(_lib.PTYRO_ERR_INVALID)
+                ws = _workspace(nbytes, dev)
+                _lib.check(lib.ptyro_ms_amplitudes(ctypes.byref(prm), slices.data_ptr(), mode.data_ptr(),
+                                                   pos.data_ptr(), None if tilts is None else tilts.data_ptr(),
+                                                   amps.data_ptr(), ws.data_ptr(), nbytes, _stream_ptr(dev)))
+                field = amps[:, 0] * w_coh if field is None else field + amps[:, 0] * w_coh
+            out[c0:c0 + chunk] += float(w_inc) * (field.real ** 2 + field.imag ** 2)
+    return out

@@ -72,7 +72,7 @@ def test_stem_4d_ensemble_matches_oracle():
     assert rel_l2(s4.data.cpu().numpy(), want) < TOL
 
 
-def test_coherent_mode_axis_and_unsupported_coherent_tilts():
+def test_coherent_mode_axis_and_coherent_energy_tilt_sums():
     pot, modes, w = _setup(m=2)
     coh = pb.create_distribution(np.arange(2.0)[:, None], w, pb.ReductionMode.COHERENT, "probe_modes")
     ens = pb.create_ensemble_axes(probe_modes=coh)
@@ -81,12 +81,33 @@ def test_coherent_mode_axis_and_unsupported_coherent_tilts():
     got = pb.cbed_image(pb.create_potential_slices(pot, 1.7, 0.25), beam, mic).data_array.cpu().numpy()
     want = R.ensemble_cbed(pot, 1.7, 0.25, modes, 0.25, 200.0, [_axes_oracle(coh)])
     assert rel_l2(got, want) < TOL
+    # a COHERENT coherence axis (energy and tilt samples summed as amplitudes), with
+    # the coherent mode axis, in cbed_image; and with an incoherent jitter axis in stem_4d
     c = pb.coherence_to_distribution(0.5, 0.2, 2)
     coherent_tilts = pb.create_distribution(c.samples, c.weights, pb.ReductionMode.COHERENT, "coherence")
     ens2 = pb.create_ensemble_axes(probe_modes=coh, coherence=coherent_tilts)
     mic2 = pb.create_microscope_config(200.0, 25.0, ensemble=ens2, probe_shape=(64, 64))
+    got2 = pb.cbed_image(pb.create_potential_slices(pot, 1.7, 0.25), beam, mic2).data_array.cpu().numpy()
+    axes2 = [_axes_oracle(a) for a in pb.ensemble_axes_for_cbed(ens2, beam)]
+    want2 = R.ensemble_cbed(pot, 1.7, 0.25, modes, 0.25, 200.0, axes2)
+    assert rel_l2(got2, want2) < TOL
+    ens3 = pb.create_ensemble_axes(position_jitter=pb.position_jitter_to_distribution(0.06, 2),
+                                   coherence=coherent_tilts)
+    mic3 = pb.create_microscope_config(200.0, 25.0, ensemble=ens3, probe_shape=(64, 64))
+    beam1 = pb.create_probe_modes(modes[..., :1], np.array([1.0]), 0.25)
+    pos = np.random.default_rng(3).uniform(-2, 2, (4, 2))
+    det = pb.create_detector_config(0.3, scan_positions_px=pos)
+    s4 = pb.stem_4d(pb.create_potential_slices(pot, 1.7, 0.25), beam1, mic3, det)
+    axes3 = [_axes_oracle(a) for a in pb.ensemble_axes_for_cbed(ens3, beam1)]
+    want3 = R.stem_4d_ensemble(pot, 1.7, 0.25, modes[..., :1], 0.25, 200.0, pos, 0.3, axes3)
+    assert rel_l2(s4.data.cpu().numpy(), want3) < TOL
+    # any-size grids have no amplitude forward at scan positions: refused by name
+    mic4 = pb.create_microscope_config(200.0, 25.0, ensemble=ens2, probe_shape=(40, 56))
+    rect = np.random.default_rng(1).uniform(0.0, 20.0, (40, 56, 2))
+    probe = R.make_probe(200.0, 25.0, (40, 56), 25.0)
+    beam2 = pb.create_probe_modes(np.stack([probe, probe * 0.5j], -1), w, 0.25)
     with pytest.raises(NotImplementedError, match="coherent sums over energy or tilt"):
-        pb.cbed_image(pb.create_potential_slices(pot, 1.7, 0.25), beam, mic2)
+        pb.cbed_image(pb.create_potential_slices(rect, 1.7, 0.25), beam2, mic4)
 
 
 @pytest.mark.parametrize("jitter,energy", [(0.08, 0.0), (0.0, 0.6), (0.1, 0.5)])
