@@ -20,6 +20,7 @@ import ctypes
 import math
 from typing import Optional
 
+import numpy as np
 import torch
 
 from . import _lib
@@ -244,9 +245,10 @@ class Stem4dFunction(torch.autograd.Function):
         t_slices, t_modes, t_weights, t_positions = (_plain(t) for t in (t_slices, t_modes, t_weights, t_positions))
         slice_thickness, voltage_kv, calib_ang, shift_calib_ang, k, batch, tune, n, f, record = ctx.cfg
         # torch.func.jvp hands zero tangents to the inputs it does not differentiate
-        if t_positions is not None and bool(t_positions.any()):
-            raise NotImplementedError("stem_4d has no forward-mode derivative with respect to positions")
+        moved = t_positions is not None and bool(t_positions.any())
         with torch._C._DisableFuncTorch():  # buffers made here must be plain tensors
+            p_tangent = _position_tangent(slices, modes, weights, positions, t_positions, slice_thickness,
+                                          voltage_kv, calib_ang, shift_calib_ang, batch, windows) if moved else None
             if t_weights is not None and bool(t_weights.any()):
                 # the patterns are linear in the weights: their tangent is the forward with
                 # the tangent weights, added to the potential's and modes' tangent below
@@ -258,7 +260,35 @@ class Stem4dFunction(torch.autograd.Function):
                 w_tangent = None
             _, tangent = jvp(slices, modes, weights, positions, t_slices, t_modes, slice_thickness, voltage_kv,
                              calib_ang, shift_calib_ang, batch=batch, windows=windows, want_patterns=False)
-        return (tangent if w_tangent is None else tangent + w_tangent), None
+        if w_tangent is not None:
+            tangent = tangent + w_tangent
+        if p_tangent is not None:
+            tangent = tangent + p_tangent
+        return tangent, None
+
+
+def _position_tangent(slices, modes, weights, positions, t_positions, slice_thickness, voltage_kv, calib_ang,
+                      shift_calib_ang, batch, windows) -> torch.Tensor:
+    """dI along scan-position tangents (P, 2). Probe p's first wave is
+    ifft2(fft2(beam) R_p) with R_p = exp(-2 pi i (qy y_p + qx x_p)) (shift_beam_fourier,
+    simulations.py:1236-1327), so d psi_p / dy_p = shift_p(ifft2(fft2(beam) (-2 pi i qy))):
+    the tangent kernel with that fixed tangent beam, once per axis, gives every
+    probe's derivative along its own y (x), and dI = dy_p dI/dy_p + dx_p dI/dx_p."""
+    from .simulations import fft2
+    dev = modes.device
+    h, w = int(modes.shape[0]), int(modes.shape[1])
+    spectra = fft2(modes.permute(2, 0, 1).contiguous())  # (M, H, W)
+    qy = np.fft.fftfreq(h, d=float(shift_calib_ang))
+    qx = np.fft.fftfreq(w, d=float(shift_calib_ang))
+    out = None
+    for c, q in enumerate((np.broadcast_to(qy[:, None], (h, w)), np.broadcast_to(qx[None, :], (h, w)))):
+        factor = torch.as_tensor((-2j * np.pi * q).astype(np.complex64), device=dev)
+        d_modes = fft2(spectra * factor, inverse=True).permute(1, 2, 0).contiguous()
+        _, tan = jvp(slices, modes, weights, positions, None, d_modes, slice_thickness, voltage_kv, calib_ang,
+                     shift_calib_ang, batch=batch, windows=windows, want_patterns=False)
+        part = t_positions[:, c].to(device=dev, dtype=torch.float32)[:, None, None] * tan
+        out = part if out is None else out + part
+    return out
 
 
 def stem_4d_patterns(slices: torch.Tensor, modes: torch.Tensor, weights: torch.Tensor, positions: torch.Tensor,

@@ -2,6 +2,8 @@
 the transpose identity with the adjoint kernels, and torch.func / Gauss-Newton
 through the public stem_4d."""
 
+import dataclasses
+
 import numpy as np
 import pytest
 import torch
@@ -133,3 +135,35 @@ def test_jtj_operator_is_symmetric_and_gauss_newton_descends():
     r0 = float(torch.linalg.norm(forward_fn(start) - data))
     _, rn = pb.jacobian.gauss_newton_step(forward_fn, start, data, cg_max_iterations=10, cg_tolerance=1e-8)
     assert float(rn) < 0.5 * r0
+
+
+@pytest.mark.parametrize("h,w", [(64, 64), (24, 40)])
+def test_forward_mode_along_scan_positions(h, w):
+    """torch.func.jvp through stem_4d along a scan-position tangent (two tangent-kernel
+    runs, one per axis of the shifted beam's derivative): <dI, g> against the oracle's
+    position gradient, on the engine's grid and on a rectangular any-size grid."""
+    rng = np.random.default_rng(h * w)
+    pot = rng.uniform(0.0, 30.0, (h, w, 3))
+    probe = R.make_probe(200.0, 25.0, (h, w), 30.0, defocus_ang=-30.0)
+    pos = rng.uniform(-2, 2, (5, 2))
+    g = rng.normal(size=(5, h, w))
+    tpos = rng.normal(size=(5, 2))
+    mic = pb.create_microscope_config(200.0, 25.0, probe_shape=(h, w))
+    pots = pb.create_potential_slices(pot, 1.7, 0.3)
+    beam = pb.create_probe_modes(probe[..., None], np.array([1.0]), 0.3)
+    dev = torch.device("cuda")
+
+    det0 = pb.create_detector_config(0.3, scan_positions_px=pos)
+
+    def fwd(p):
+        return pb.stem_4d(pots, beam, mic, dataclasses.replace(det0, scan_positions_px=p)).data
+
+    p0 = torch.tensor(pos, dtype=torch.float64, device=dev)
+    out, tan = torch.func.jvp(fwd, (p0,), (torch.tensor(tpos, dtype=torch.float64, device=dev),))
+    want = R.stem_4d(pot, 1.7, 0.3, probe[..., None], [1.0], 0.3, 200.0, pos, 0.3)["data"]
+    assert rel_l2(out.cpu().numpy(), want) < TOL
+    _, _, dpos = R.stem_4d_vjp(pot, 1.7, 0.3, probe[..., None], [1.0], 0.3, 200.0, pos, 0.3, g,
+                               with_positions=True)
+    got = float(np.sum(tan.cpu().numpy() * g))
+    ref = float(np.sum(dpos * tpos))
+    assert abs(got - ref) <= 1e-3 * abs(ref) + 1e-4 * float(np.abs(g * want).sum()) * 1e-2, (got, ref)
