@@ -33,11 +33,18 @@ from .reduce import apply_distribution, apply_distributions  # noqa: F401
 from .simulations import (  # noqa: F401
     aberration,
     cbed_amplitude,
+    cbed_amplitude_from_atoms,
     cbed_image,
+    cbed_image_from_atoms,
     fft2,
+    fourier_calib,
+    fourier_coords,
     interaction_sigma,
     make_probe,
+    propagation_func,
     relativistic_wavelength_ang,
+    shift_beam_fourier,
+    transmission_func,
     run_forward,
     slices_from_atoms,
     stem4d_sharded,

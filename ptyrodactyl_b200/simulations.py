@@ -13,6 +13,7 @@ import math
 import threading
 from typing import Optional
 
+import numpy as np
 import torch
 
 from . import _lib
@@ -589,6 +590,34 @@ def stem4d_sharded(probe_modes: ProbeModes, sample: AtomicSliceData, microscope:
                          microscope.voltage_kv)
 
 
+def cbed_amplitude_from_atoms(beam, atom_coords, atom_types, slice_z_bounds, atom_potentials, voltage_kv,
+                              calib_ang, atom_mask=None) -> torch.Tensor:
+    """Detector-plane amplitudes (H, W, M) complex64 of the unshifted beam modes through
+    slices built on the device from atoms (multislice/parallelized.py:174-261); every
+    calibration is ``calib_ang`` and the slice thickness is that of the first z bound."""
+    from .types import create_atomic_slice_data
+    dev = _device()
+    modes = as_tensor(beam, torch.complex64, dev)
+    if modes.ndim == 2:
+        modes = modes[..., None]
+    sample = create_atomic_slice_data(atom_coords, atom_types, slice_z_bounds, atom_potentials, atom_mask)
+    slices = slices_from_atoms(sample, tuple(modes.shape[:2]), float(calib_ang), dev)
+    bounds = as_tensor(sample.slice_z_bounds, torch.float64)
+    thickness = float(bounds[0, 1] - bounds[0, 0])
+    return _amplitudes_at_origin(slices, thickness, modes.contiguous(), float(voltage_kv), float(calib_ang))
+
+
+def cbed_image_from_atoms(beam, mode_distribution, atom_coords, atom_types, slice_z_bounds, atom_potentials,
+                          voltage_kv, calib_ang, atom_mask=None) -> torch.Tensor:
+    """CBED intensity (H, W) of the atom-backed amplitudes reduced over
+    ``mode_distribution`` (sample = mode index) by apply_distribution
+    (multislice/parallelized.py:264-347)."""
+    from .reduce import apply_distribution
+    amps = cbed_amplitude_from_atoms(beam, atom_coords, atom_types, slice_z_bounds, atom_potentials, voltage_kv,
+                                     calib_ang, atom_mask)
+    return apply_distribution(mode_distribution, lambda sample: amps[..., int(sample[0])])
+
+
 def cbed_image(pot_slices: PotentialSlices, beam: ProbeModes, microscope: MicroscopeConfig) -> CalibratedArray:
     """Single-position CBED intensity (simulations.py:1130-1233): the unshifted beam
     through the slices, sum_m w_m |fftshift(fft2(exit wave))|^2, or, when the
@@ -626,29 +655,37 @@ def cbed_image(pot_slices: PotentialSlices, beam: ProbeModes, microscope: Micros
 def cbed_amplitude(pot_slices: PotentialSlices, beam: ProbeModes, microscope: MicroscopeConfig) -> torch.Tensor:
     """Complex detector-plane amplitudes (H, W, M) of every beam mode at the probe's
     own place: fftshift(fft2(exit wave)) (simulations.py:606-679), complex64 CUDA."""
-    lib = _lib.load()
     dev = _device(pot_slices.slices.device if pot_slices.slices.is_cuda else None)
     slices = as_tensor(pot_slices.slices, torch.float32, dev)
     if slices.ndim == 2:
         slices = slices[..., None]
     modes, _ = _beam_on(beam, dev)
     calib = min(float(pot_slices.calib), float(beam.calib))
+    return _amplitudes_at_origin(slices, pot_slices.slice_thickness, modes, microscope.voltage_kv, calib)
+
+
+def _amplitudes_at_origin(slices: torch.Tensor, slice_thickness: float, modes: torch.Tensor, voltage_kv: float,
+                          calib: float) -> torch.Tensor:
+    """fftshifted far-field amplitudes (H, W, M) complex64 of the unshifted modes."""
+    lib = _lib.load()
+    dev = slices.device
+    microscope_kv = float(voltage_kv)
     zero = torch.zeros((1, 2), dtype=torch.float64, device=dev)
     if not engine_grid(modes.shape[0], modes.shape[1]):
         # the far-field amplitude planes of the any-size forward's residuals, fftshifted
         h, w = check_any_grid(slices, modes)
         S, M = slices.shape[2], modes.shape[2]
-        prm = any_grid_params(slices, modes, 1, microscope.voltage_kv, pot_slices.slice_thickness, calib, calib)
+        prm = any_grid_params(slices, modes, 1, microscope_kv, slice_thickness, calib, calib)
         res = torch.empty(lib.ptyro_gm_residual_bytes(ctypes.byref(prm), h, w) // 8, dtype=torch.complex64,
                           device=dev)
         status = _lib.new_status(dev)
-        run_forward_any(slices, pot_slices.slice_thickness, modes, torch.ones(M, dtype=torch.float32, device=dev),
-                        zero, microscope.voltage_kv, calib, calib, status=status, residuals=res)
+        run_forward_any(slices, slice_thickness, modes, torch.ones(M, dtype=torch.float32, device=dev),
+                        zero, microscope_kv, calib, calib, status=status, residuals=res)
         _lib.check_status(status, "cbed_amplitude")
         amps = res.view(M, S + 1, h, w)[:, S]
         return torch.roll(amps, shifts=(h // 2, w // 2), dims=(1, 2)).permute(1, 2, 0)
     n, f = check_windows(slices, modes, None, 1)
-    prm = ms_params(n, slices.shape[2], modes.shape[2], 1, microscope.voltage_kv, pot_slices.slice_thickness, calib,
+    prm = ms_params(n, slices.shape[2], modes.shape[2], 1, microscope_kv, slice_thickness, calib,
                     calib, slices.stride(), modes.stride(), 0, 0, f)
     amps = torch.empty((1, modes.shape[2], n, n), dtype=torch.complex64, device=dev)
     nbytes = lib.ptyro_ms_workspace_bytes(ctypes.byref(prm))
@@ -656,6 +693,67 @@ def cbed_amplitude(pot_slices: PotentialSlices, beam: ProbeModes, microscope: Mi
     _lib.check(lib.ptyro_ms_amplitudes(ctypes.byref(prm), slices.data_ptr(), modes.data_ptr(), zero.data_ptr(),
                                        None, amps.data_ptr(), ws.data_ptr(), nbytes, _stream_ptr(dev)))
     return amps[0].permute(1, 2, 0)
+
+
+# ----------------------------------------------------------------------------- building blocks
+# The reference's public per-step functions, float64/complex128 torch on the input's
+# device and differentiable like the reference's. The engine evaluates the same
+# quantities inside its kernels (k_transmission, k_propagator, k_ramps); these are for
+# callers who compose their own steps.
+
+
+def transmission_func(pot_slice, voltage_kv) -> torch.Tensor:
+    """exp(i sigma V) of a potential slice (simulations.py:107-161), complex128."""
+    v = as_tensor(pot_slice, torch.float64)
+    return torch.polar(torch.ones_like(v), interaction_sigma(float(voltage_kv)) * v)
+
+
+def propagation_func(imsize_y: int, imsize_x: int, thickness_ang, voltage_kv, calib_ang,
+                     device=None) -> torch.Tensor:
+    """Fresnel propagator exp(-i pi lambda dz (qx^2 + qy^2)) on the fftfreq grid
+    (simulations.py:164-226), complex128 (imsize_y, imsize_x)."""
+    dev = torch.device("cpu") if device is None else torch.device(device)
+    qy = torch.fft.fftfreq(int(imsize_y), d=float(calib_ang), dtype=torch.float64, device=dev)
+    qx = torch.fft.fftfreq(int(imsize_x), d=float(calib_ang), dtype=torch.float64, device=dev)
+    l_sq = qx[None, :] ** 2 + qy[:, None] ** 2
+    phase = -math.pi * relativistic_wavelength_ang(float(voltage_kv)) * float(thickness_ang) * l_sq
+    return torch.polar(torch.ones_like(phase), phase)
+
+
+def fourier_coords(calibration, image_size) -> CalibratedArray:
+    """Radial spatial frequencies of a centred-then-rolled grid (simulations.py:229-294):
+    |q| in 1/Angstrom (h, w) float64 with the inverse calibrations."""
+    size = np.asarray(image_size, dtype=np.int64).reshape(-1)
+    cal = np.broadcast_to(np.asarray(calibration, dtype=np.float64), (2,))
+    fov = size * cal
+    ay = np.arange(-size[0] / 2, size[0] / 2, 1) / fov[0]
+    ax = np.arange(-size[1] / 2, size[1] / 2, 1) / fov[1]
+    ry, rx = np.roll(ay, int(size[0] // 2)), np.roll(ax, int(size[1] // 2))
+    xx, yy = np.meshgrid(rx, ry)
+    radius = torch.from_numpy(np.sqrt(yy * yy + xx * xx))
+    return create_calibrated_array(radius, float(ay[1] - ay[0]), float(ax[1] - ax[0]), False)
+
+
+def fourier_calib(real_space_calib, sizebeam) -> torch.Tensor:
+    """1 / (size x calibration) per axis (simulations.py:297-331), float64 (2,)."""
+    return 1.0 / (as_tensor(np.asarray(sizebeam, dtype=np.float64), torch.float64)
+                  * as_tensor(real_space_calib, torch.float64))
+
+
+def shift_beam_fourier(beam, pos, calib_ang) -> torch.Tensor:
+    """ifft2(fft2(beam) exp(-2 pi i (qy y + qx x))) per position (simulations.py:
+    1238-1327): beam (H, W) or (H, W, M), pos (P, 2) -> complex128 (P, H, W, M)."""
+    b = as_tensor(beam, torch.complex128)
+    if b.ndim == 2:
+        b = b[..., None]
+    dev = b.device
+    p = as_tensor(pos, torch.float64, dev).reshape(-1, 2)
+    qy = torch.fft.fftfreq(b.shape[0], d=float(calib_ang), dtype=torch.float64, device=dev)
+    qx = torch.fft.fftfreq(b.shape[1], d=float(calib_ang), dtype=torch.float64, device=dev)
+    bk = torch.fft.fft2(b, dim=(0, 1))
+    phase = -2.0 * math.pi * (qy[None, :, None] * p[:, 0, None, None] + qx[None, None, :] * p[:, 1, None, None])
+    ramp = torch.polar(torch.ones_like(phase), phase)
+    return torch.fft.ifft2(bk[None] * ramp[..., None], dim=(1, 2))
 
 
 def aberration(fourier_coord, lambda_angstrom, defocus=0.0, c3=0.0, c5=0.0) -> torch.Tensor:

@@ -280,6 +280,30 @@ def test_slices_from_atoms_match_oracle():
     assert rel_l2(got, want) < 1e-5
 
 
+def test_cbed_from_atoms_matches_oracle():
+    """cbed_amplitude_from_atoms / cbed_image_from_atoms (parallelized.py:174-347):
+    slices from atoms on the device, the unshifted modes through them, the image
+    reduced over a mode distribution."""
+    rng = np.random.default_rng(13)
+    n, calib, kv = 64, 0.25, 200.0
+    atoms = np.column_stack([rng.uniform(0, 16, 60), rng.uniform(0, 16, 60), rng.uniform(0, 4, 60)])
+    types = rng.integers(0, 2, 60)
+    r = np.hypot(*np.meshgrid(np.fft.fftfreq(n) * n, np.fft.fftfreq(n) * n, indexing="ij"))
+    kern = np.stack([20.0 * np.exp(-r / 2.0), 35.0 * np.exp(-r / 1.5)])
+    bounds = [[0.0, 2.0], [2.0, 4.0]]
+    probe = R.make_probe(kv, 25.0, (n, n), calib * 100.0, defocus_ang=-20.0)
+    modes = np.stack([probe, np.roll(probe, 3, axis=0) * (0.6 + 0.3j)], -1)
+    amps = pb.cbed_amplitude_from_atoms(modes, atoms, types, bounds, kern, kv, calib)
+    slices = np.stack([R.slice_potential_from_atoms(atoms, types, b[0], b[1], kern, (n, n), calib)
+                       for b in bounds], axis=-1)
+    want = R.cbed_amplitude(slices, 2.0, kv, calib, modes)
+    assert tuple(amps.shape) == (n, n, 2) and rel_l2(amps.cpu().numpy(), want) < TOL_F64
+    dist = pb.create_distribution(np.arange(2.0)[:, None], [0.7, 0.3], pb.ReductionMode.INCOHERENT, "probe_modes")
+    img = pb.cbed_image_from_atoms(modes, dist, atoms, types, bounds, kern, kv, calib)
+    want_img = 0.7 * np.abs(want[..., 0]) ** 2 + 0.3 * np.abs(want[..., 1]) ** 2
+    assert rel_l2(img.cpu().numpy(), want_img) < TOL_F64
+
+
 def test_stem_4d_streams_patterns_to_host():
     """out= a pinned host tensor: chunked compute with overlapped copies gives the
     device result exactly."""
