@@ -36,6 +36,7 @@ from .simulations import (  # noqa: F401
     cbed_amplitude_from_atoms,
     cbed_image,
     cbed_image_from_atoms,
+    decompose_beam_to_modes,
     fft2,
     fourier_calib,
     fourier_coords,

@@ -27,6 +27,7 @@ from .types import (
     STEM4D,
     as_tensor,
     create_calibrated_array,
+    create_probe_modes,
     create_stem4d,
 )
 
@@ -738,6 +739,27 @@ def fourier_calib(real_space_calib, sizebeam) -> torch.Tensor:
     """1 / (size x calibration) per axis (simulations.py:297-331), float64 (2,)."""
     return 1.0 / (as_tensor(np.asarray(sizebeam, dtype=np.float64), torch.float64)
                   * as_tensor(real_space_calib, torch.float64))
+
+
+def decompose_beam_to_modes(beam: CalibratedArray, num_modes: int, key, first_mode_weight: float = 0.6) -> ProbeModes:
+    """Orthogonal modes that together keep the beam's intensity (simulations.py:
+    1447-1536): the reduced QR factor of an (H W, M) complex normal matrix drawn with
+    ``key`` (two JAX key words or an int seed, split into the real and imaginary
+    draws), each column scaled by the beam's pixel amplitudes |beam|; weights
+    (first_mode_weight, then the rest shared equally). Modes complex128 on the host,
+    as the reference returns them; the engine reads them as complex64."""
+    from . import prng
+    data = as_tensor(beam.data_array, torch.complex128).detach().cpu().numpy()
+    hh, ww = data.shape
+    m = int(num_modes)
+    k1, k2 = prng.split(key)
+    draws = prng.normal(k1, (hh * ww, m)) + 1j * prng.normal(k2, (hh * ww, m))
+    q, _ = np.linalg.qr(draws, mode="reduced")
+    weights = np.full(m, (1.0 - float(first_mode_weight)) / (m - 1) if m > 1 else 0.0)
+    weights[0] = float(first_mode_weight)
+    modes = (q * np.sqrt(np.abs(data.reshape(-1)) ** 2)[:, None]).reshape(hh, ww, m)
+    checked = create_probe_modes(modes, weights, beam.calib_y)
+    return ProbeModes(torch.from_numpy(modes), checked.weights, checked.calib)
 
 
 def shift_beam_fourier(beam, pos, calib_ang) -> torch.Tensor:
