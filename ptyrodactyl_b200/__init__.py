@@ -83,6 +83,7 @@ from .crystal import CrystalData, create_crystal_data, crystal_potential_slices 
 from .elements import kirkland_parameters, lobato_parameters, single_atom_potential  # noqa: F401
 from .hdf5 import HDF5SchemaError, load_from_h5, save_to_h5  # noqa: F401
 from .ensemble import (  # noqa: F401
+    bind_cbed_axes,
     coherence_to_distribution,
     ensemble_axes_for_cbed,
     position_jitter_to_distribution,

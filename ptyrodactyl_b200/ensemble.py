@@ -140,22 +140,84 @@ def ensemble_axes_for_cbed(ensemble: EnsembleAxes, beam: ProbeModes) -> Tuple[Di
     return tuple(axes)
 
 
-def _axis_maps(axes, mode_count: int) -> Tuple[str, ...]:
-    """simulations.py:1032-1127: axis ids, sample widths, probe-mode axis first."""
+def _axis_maps(axes, mode_count: int, column_maps: Tuple[str, ...] = ()) -> Tuple[str, ...]:
+    """simulations.py:1032-1127: the column map of each axis (its axis_id unless
+    ``column_maps`` names them all), sample widths, probe-mode axis first."""
+    if len(column_maps) not in (0, len(axes)):
+        raise ValueError("column_maps must be empty or match axes length")
     maps = []
     for i, axis in enumerate(axes):
-        if axis.axis_id is None:
+        name = column_maps[i] if column_maps else axis.axis_id
+        if name is None:
             raise ValueError("distribution axis_id is required")
-        if axis.axis_id not in _AXIS_DIM:
-            raise ValueError(f"unknown axis_id {axis.axis_id!r}")
-        if axis.samples.shape[1] != _AXIS_DIM[axis.axis_id]:
-            raise ValueError(f"{axis.axis_id!r} axis must have sample width {_AXIS_DIM[axis.axis_id]}")
-        if axis.axis_id == AXIS_PROBE_MODES and i != 0:
+        if name not in _AXIS_DIM:
+            raise ValueError(f"unknown axis_id {name!r}")
+        if axis.samples.shape[1] != _AXIS_DIM[name]:
+            raise ValueError(f"{name!r} axis must have sample width {_AXIS_DIM[name]}")
+        if name == AXIS_PROBE_MODES and i != 0:
             raise ValueError("probe_modes axis must be first")
-        maps.append(axis.axis_id)
+        maps.append(name)
     if AXIS_PROBE_MODES not in maps and mode_count != 1:
         raise ValueError("multimode probes require a first probe_modes axis")
     return tuple(maps)
+
+
+def bind_cbed_axes(pot_slices, probe_modes: ProbeModes, microscope, detector, axes,
+                   column_maps: Tuple[str, ...] = ()):
+    """The per-sample amplitude of cbed_image's ensemble branch (simulations.py:
+    769-888): a function of one concatenated sample row (one row of each axis, in
+    order) returning the complex (H, W) detector field of the selected mode, shifted
+    by the jitter at ``detector.real_space_calib_ang``, with the coherence sample's
+    tilt ramp (after the shift) and energy (voltage + dE / 1000). Each call runs the
+    engine's amplitude pass once. ``apply_distributions(axes, bound)`` is the ensemble
+    CBED intensity."""
+    from .simulations import _amplitudes_at_origin
+    axes = tuple(axes)
+    modes_all = probe_modes.modes if probe_modes.modes.ndim == 3 else probe_modes.modes[..., None]
+    maps = _axis_maps(axes, int(modes_all.shape[2]), tuple(column_maps))
+    widths = [int(a.samples.shape[1]) for a in axes]
+    expected = sum(widths)
+    dev = _device(pot_slices.slices.device if pot_slices.slices.is_cuda else None)
+    slices = as_tensor(pot_slices.slices, torch.float32, dev)
+    if slices.ndim == 2:
+        slices = slices[..., None]
+    modes = as_tensor(modes_all, torch.complex64, dev).contiguous()
+    calib = float(detector.real_space_calib_ang)
+    pot_calib = min(float(pot_slices.calib), float(probe_modes.calib))
+    kv = float(microscope.voltage_kv)
+    h, w = int(modes.shape[0]), int(modes.shape[1])
+
+    def bound(sample) -> torch.Tensor:
+        row = _host(torch.as_tensor(sample)).reshape(-1)
+        if row.shape[0] != expected:
+            raise ValueError("sample width does not match bound axes")
+        mode, delta, de, tilt, c = 0, np.zeros(2), 0.0, np.zeros(2), 0
+        for name, wd in zip(maps, widths):
+            part = row[c:c + wd]
+            c += wd
+            if name == AXIS_PROBE_MODES:
+                mode = int(part[0])
+            elif name == AXIS_POSITION_JITTER:
+                delta = delta + part
+            else:
+                de, tilt = de + float(part[0]), tilt + part[1:3]
+        if not 0 <= mode < modes.shape[2]:
+            raise ValueError(f"probe mode index {mode} out of range")
+        volt = kv + de / 1000.0
+        wave = modes[:, :, mode]
+        if np.any(delta != 0.0):
+            wave = _jitter_shift(fft2(wave[None]), delta, calib)[0]
+        if np.any(tilt != 0.0):
+            k = 2.0 * np.pi / relativistic_wavelength_ang(volt)
+            cy = (np.arange(h, dtype=np.float64) - (h - 1) / 2.0) * calib
+            cx = (np.arange(w, dtype=np.float64) - (w - 1) / 2.0) * calib
+            ramp = np.exp(1j * k * ((tilt[0] / 1000.0) * cx[None, :] + (tilt[1] / 1000.0) * cy[:, None]))
+            wave = wave * torch.as_tensor(ramp.astype(np.complex64), device=dev)
+        amps = _amplitudes_at_origin(slices, float(pot_slices.slice_thickness), wave[:, :, None].contiguous(), volt,
+                                     pot_calib)
+        return amps[:, :, 0]
+
+    return bound
 
 
 class VirtualModes:

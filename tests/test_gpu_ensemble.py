@@ -313,3 +313,31 @@ def test_ensemble_axis_weights_and_coherent_modes_are_differentiable():
     scale = float(np.abs(g * want).sum())
     for got, fd in checks:
         assert abs(got - fd) <= 2e-3 * abs(fd) + 1e-5 * scale, (got, fd)
+
+
+@pytest.mark.parametrize("with_modes", [False, True])
+def test_bind_cbed_axes_explicit_composition_matches_cbed_image(with_modes):
+    """apply_distributions(axes, bind_cbed_axes(...)) against cbed_image's ensemble
+    branch (the reference's test_cbed_image_ensemble_axes_match_explicit_composition,
+    widened to jitter, energy and tilt, and a two-mode beam with its mode axis), and
+    against the oracle's ensemble branch."""
+    m = 2 if with_modes else 1
+    pot, modes, w = _setup(n=32, s=2, m=m, seed=17)
+    beam = pb.create_probe_modes(modes, w, 0.25)
+    ens = pb.create_ensemble_axes(position_jitter=pb.position_jitter_to_distribution(0.15, 2),
+                                  coherence=pb.coherence_to_distribution(0.5, 0.2, 2))
+    mic = pb.create_microscope_config(200.0, 25.0, ensemble=ens, probe_shape=(32, 32))
+    pots = pb.create_potential_slices(pot, 1.7, 0.25)
+    det = pb.create_detector_config(0.25, probe_calibration_pm=25.0)
+    axes = pb.ensemble_axes_for_cbed(ens, beam)
+    bound = pb.bind_cbed_axes(pots, beam, mic, det, axes)
+    explicit = pb.apply_distributions(axes, bound)
+    carried = pb.cbed_image(pots, beam, mic).data_array
+    assert rel_l2(explicit.cpu().numpy(), carried.cpu().numpy()) < 1e-5
+    want = R.ensemble_cbed(pot, 1.7, 0.25, modes, 0.25, 200.0, [_axes_oracle(a) for a in axes])
+    assert rel_l2(explicit.cpu().numpy(), want) < TOL
+    # the binder's contract: sample width and explicit column maps
+    with pytest.raises(ValueError, match="sample width"):
+        bound(torch.zeros(1, dtype=torch.float64))
+    with pytest.raises(ValueError, match="column_maps"):
+        pb.bind_cbed_axes(pots, beam, mic, det, axes, column_maps=("coherence",))
