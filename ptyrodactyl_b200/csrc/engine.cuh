@@ -791,29 +791,28 @@ static __global__ void k_reduce_dv(const float* __restrict__ contrib, int nslots
 // atomics, deterministic). A CTA covers a TX x TY tile of the field (TX, TY <= n,
 // TX TY = 64). First every thread classifies some of the slots (a window meets the
 // tile iff it holds one of the tile's corner rows and one of its corner columns, both
-// lengths being at most n; it covers the whole tile iff the tile's first row and
-// column sit at least TY rows and TX columns before the window's end), then warp 0
-// lists the meeting slots in slot order with, for a covering slot, the offset of the
-// tile's corner in its contribution plane: its pixels then load at corner + (ty n +
-// tx) with no per-pixel test. A batch's windows cluster (neighbouring scan positions),
-// so central pixels collect many contributions: each pixel's list is split into
-// kReduceQ contiguous parts summed by kReduceQ threads, 8 loads in flight each, and
-// the parts are added in order. Neighbouring threads read neighbouring pixels of the
-// same plane.
+// lengths being at most n), then warp 0 lists the meeting slots in slot order with
+// their plane base and window origin. A batch's windows cluster (neighbouring scan
+// positions), so central pixels collect many contributions: each pixel's list is
+// split into kReduceQ contiguous parts summed by kReduceQ threads, 8 loads in flight
+// each, and the parts are added in order. Neighbouring threads read neighbouring
+// pixels of the same plane. Every listed slot takes the same path (local row and
+// column from the window origin, one bounds test), and a single-mode run (M1) drops
+// the mode loop: the loop body stays small, since instruction fetch, not DRAM, is
+// what this kernel waits on most.
 constexpr int kReduceQ = 4;
 
-// 4 CTAs per SM (64 registers): its loads are latency-bound, so more resident warps
-// pay (149 against 201 us per 10-plane launch at the gradient workload, same results)
+// 4 CTAs per SM (64 registers): more resident warps pay for its short loads
+template <bool M1>
 static __global__ void __launch_bounds__(256, 4) k_reduce_dv_win(const float* __restrict__ contrib, int nb, int M, int n,
                                                        int F, const int* __restrict__ win, float* dv, long long sy,
                                                        long long sx, long long ss, int s0, int planes,
                                                        long long pstride, int tx_log2) {
   extern __shared__ long long shl[];
-  long long* scorner = shl;                                  // listed: plane base (+ tile corner if covering)
+  long long* sbase = shl;                                    // listed: plane base of the slot
   int2* sorg = reinterpret_cast<int2*>(shl + nb);            // listed: window origin (wy, wx)
   int2* sall = sorg + nb;                                    // per slot: window origin
-  int* sflag = reinterpret_cast<int*>(sall + nb);            // per slot: 0 misses, 1 meets, 2 covers the tile
-  int* sfull = sflag + nb;                                   // listed: covers the tile
+  int* sflag = reinterpret_cast<int*>(sall + nb);            // per slot: meets the tile
   __shared__ int count;
   __shared__ float part[4][256];
   constexpr int kPix = 256 / kReduceQ;  // pixels per tile
@@ -822,11 +821,10 @@ static __global__ void __launch_bounds__(256, 4) k_reduce_dv_win(const float* __
   const int fm = F - 1;
   for (int bb = (int)threadIdx.x; bb < nb; bb += (int)blockDim.x) {
     const int wy = win ? win[2 * bb] : 0, wx = win ? win[2 * bb + 1] : 0;
-    const int ly0 = (fy0 - wy) & fm, lx0 = (fx0 - wx) & fm;
-    const bool rows = ly0 < n || ((fy0 + TY - 1 - wy) & fm) < n;
-    const bool cols = lx0 < n || ((fx0 + TX - 1 - wx) & fm) < n;
+    const bool rows = ((fy0 - wy) & fm) < n || ((fy0 + TY - 1 - wy) & fm) < n;
+    const bool cols = ((fx0 - wx) & fm) < n || ((fx0 + TX - 1 - wx) & fm) < n;
     sall[bb] = make_int2(wy, wx);
-    sflag[bb] = !(rows && cols) ? 0 : (ly0 + TY <= n && lx0 + TX <= n ? 2 : 1);
+    sflag[bb] = rows && cols;
   }
   __syncthreads();
   const size_t nn = (size_t)n * n;
@@ -838,12 +836,8 @@ static __global__ void __launch_bounds__(256, 4) k_reduce_dv_win(const float* __
       const unsigned mask = __ballot_sync(0xffffffffu, f != 0);
       if (f) {
         const int pos = c + __popc(mask & ((1u << threadIdx.x) - 1u));
-        const int2 o = sall[bb];
-        long long base = (long long)bb * M * (long long)nn;
-        if (f == 2) base += (long long)((fy0 - o.x) & fm) * n + ((fx0 - o.y) & fm);
-        scorner[pos] = base;
-        sorg[pos] = o;
-        sfull[pos] = f == 2;
+        sbase[pos] = (long long)bb * (M1 ? 1 : M) * (long long)nn;
+        sorg[pos] = sall[bb];
       }
       c += __popc(mask);
     }
@@ -853,7 +847,6 @@ static __global__ void __launch_bounds__(256, 4) k_reduce_dv_win(const float* __
   const int pix = (int)threadIdx.x & (kPix - 1), q = (int)threadIdx.x / kPix;
   const int tx = pix & (TX - 1), ty = pix >> tx_log2;
   const int fx = fx0 + tx, fy = fy0 + ty;
-  const int toff = ty * n + tx;
   const int cnt = count;
   const int kb = (int)(((long long)cnt * q) / kReduceQ), ke = (int)(((long long)cnt * (q + 1)) / kReduceQ);
   // planes (slices) four at a time: one listing serves every plane, and each thread
@@ -867,30 +860,20 @@ static __global__ void __launch_bounds__(256, 4) k_reduce_dv_win(const float* __
 #pragma unroll
       for (int u = 0; u < 8; ++u) {
         const int k = k0 + u;
+        const bool in = k < ke;
+        const int2 o = in ? sorg[k] : make_int2(0, 0);
+        const int ly = (fy - o.x) & fm, lx = (fx - o.y) & fm;
+        const bool ok = in && (ly | lx) < n;  // n is a power of two
+        const float* cp = cplane + (ok ? sbase[k] + (long long)ly * n + lx : 0);
 #pragma unroll
-        for (int jj = 0; jj < 4; ++jj) v[u][jj] = 0.f;
-        if (k < ke) {
-          long long off;
-          bool ok = true;
-          if (sfull[k]) {
-            off = scorner[k] + toff;
-          } else {
-            const int2 o = sorg[k];
-            const int ly = (fy - o.x) & fm, lx = (fx - o.y) & fm;
-            ok = (ly | lx) < n;  // n is a power of two
-            off = scorner[k] + (long long)ly * n + lx;
+        for (int jj = 0; jj < 4; ++jj) {
+          float t = 0.f;
+          if (ok && jj < jn) {  // contributions are read once
+            t = __ldcs(cp + jj * pstride);
+            if (!M1)
+              for (int m = 1; m < M; ++m) t += __ldcs(cp + jj * pstride + (size_t)m * nn);
           }
-          if (ok) {
-#pragma unroll
-            for (int jj = 0; jj < 4; ++jj) {
-              if (jj < jn) {  // contributions are read once
-                const float* cp = cplane + jj * pstride + off;
-                float t = __ldcs(cp);
-                for (int m = 1; m < M; ++m) t += __ldcs(cp + (size_t)m * nn);
-                v[u][jj] = t;
-              }
-            }
-          }
+          v[u][jj] = t;
         }
       }
 #pragma unroll
@@ -925,9 +908,14 @@ static int launch_reduce_dv_win(const float* contrib, int nb, int M, int n, int 
   const dim3 grid((unsigned)(F / tx), (unsigned)(F / ty));
   for (int c0 = 0; c0 < nb; c0 += kChunk) {  // chunks add into dv in probe order
     const int cn = nb - c0 < kChunk ? nb - c0 : kChunk;
-    k_reduce_dv_win<<<grid, 256, 32 * (size_t)cn, st>>>(contrib + (size_t)c0 * M * n * n, cn, M, n, F,
-                                                         win ? win + 2 * (size_t)c0 : nullptr, dv, sy, sx, ss, s0,
-                                                         planes, pstride, tx_log2);
+    const float* cbase = contrib + (size_t)c0 * M * n * n;
+    const int* wbase = win ? win + 2 * (size_t)c0 : nullptr;
+    if (M == 1)
+      k_reduce_dv_win<true><<<grid, 256, 32 * (size_t)cn, st>>>(cbase, cn, M, n, F, wbase, dv, sy, sx, ss, s0, planes,
+                                                                 pstride, tx_log2);
+    else
+      k_reduce_dv_win<false><<<grid, 256, 32 * (size_t)cn, st>>>(cbase, cn, M, n, F, wbase, dv, sy, sx, ss, s0, planes,
+                                                                  pstride, tx_log2);
     int rc = check_launch("k_reduce_dv_win");
     if (rc) return rc;
   }
