@@ -801,6 +801,7 @@ static __global__ void k_reduce_dv(const float* __restrict__ contrib, int nslots
 // the mode loop: the loop body stays small, since instruction fetch, not DRAM, is
 // what this kernel waits on most.
 constexpr int kReduceQ = 4;
+constexpr int kPartPlanes = 12;  // planes whose parts are staged between two barriers
 
 // 4 CTAs per SM (64 registers): more resident warps pay for its short loads
 template <bool M1>
@@ -814,7 +815,7 @@ static __global__ void __launch_bounds__(256, 4) k_reduce_dv_win(const float* __
   int2* sall = sorg + nb;                                    // per slot: window origin
   int* sflag = reinterpret_cast<int*>(sall + nb);            // per slot: meets the tile
   __shared__ int count;
-  __shared__ float part[4][256];
+  __shared__ float part[kPartPlanes][256];
   constexpr int kPix = 256 / kReduceQ;  // pixels per tile
   const int TX = 1 << tx_log2, TY = kPix >> tx_log2;
   const int fx0 = (int)blockIdx.x * TX, fy0 = (int)blockIdx.y * TY;
@@ -850,46 +851,51 @@ static __global__ void __launch_bounds__(256, 4) k_reduce_dv_win(const float* __
   const int cnt = count;
   const int kb = (int)(((long long)cnt * q) / kReduceQ), ke = (int)(((long long)cnt * (q + 1)) / kReduceQ);
   // planes (slices) four at a time: one listing serves every plane, and each thread
-  // keeps one independent sum per plane in flight
-  for (int j0 = 0; j0 < planes; j0 += 4) {
-    const int jn = planes - j0 < 4 ? planes - j0 : 4;
-    const float* cplane = contrib + j0 * pstride;
-    float acc[4] = {0.f, 0.f, 0.f, 0.f};
-    for (int k0 = kb; k0 < ke; k0 += 8) {
-      float v[8][4];
+  // keeps one independent sum per plane in flight; the parts of up to kPartPlanes
+  // planes wait in shared memory, so the threads meet once per kPartPlanes planes
+  for (int g0 = 0; g0 < planes; g0 += kPartPlanes) {
+    const int gn = planes - g0 < kPartPlanes ? planes - g0 : kPartPlanes;
+    for (int j0 = g0; j0 < g0 + gn; j0 += 4) {
+      const int jn = g0 + gn - j0 < 4 ? g0 + gn - j0 : 4;
+      const float* cplane = contrib + j0 * pstride;
+      float acc[4] = {0.f, 0.f, 0.f, 0.f};
+      for (int k0 = kb; k0 < ke; k0 += 8) {
+        float v[8][4];
 #pragma unroll
-      for (int u = 0; u < 8; ++u) {
-        const int k = k0 + u;
-        const bool in = k < ke;
-        const int2 o = in ? sorg[k] : make_int2(0, 0);
-        const int ly = (fy - o.x) & fm, lx = (fx - o.y) & fm;
-        const bool ok = in && (ly | lx) < n;  // n is a power of two
-        const float* cp = cplane + (ok ? sbase[k] + (long long)ly * n + lx : 0);
+        for (int u = 0; u < 8; ++u) {
+          const int k = k0 + u;
+          const bool in = k < ke;
+          const int2 o = in ? sorg[k] : make_int2(0, 0);
+          const int ly = (fy - o.x) & fm, lx = (fx - o.y) & fm;
+          const bool ok = in && (ly | lx) < n;  // n is a power of two
+          const float* cp = cplane + (ok ? sbase[k] + (long long)ly * n + lx : 0);
 #pragma unroll
-        for (int jj = 0; jj < 4; ++jj) {
-          float t = 0.f;
-          if (ok && jj < jn) {  // contributions are read once
-            t = __ldcs(cp + jj * pstride);
-            if (!M1)
-              for (int m = 1; m < M; ++m) t += __ldcs(cp + jj * pstride + (size_t)m * nn);
+          for (int jj = 0; jj < 4; ++jj) {
+            float t = 0.f;
+            if (ok && jj < jn) {  // contributions are read once
+              t = __ldcs(cp + jj * pstride);
+              if (!M1)
+                for (int m = 1; m < M; ++m) t += __ldcs(cp + jj * pstride + (size_t)m * nn);
+            }
+            v[u][jj] = t;
           }
-          v[u][jj] = t;
         }
+#pragma unroll
+        for (int u = 0; u < 8; ++u)
+#pragma unroll
+          for (int jj = 0; jj < 4; ++jj) acc[jj] += v[u][jj];
       }
 #pragma unroll
-      for (int u = 0; u < 8; ++u)
-#pragma unroll
-        for (int jj = 0; jj < 4; ++jj) acc[jj] += v[u][jj];
+      for (int jj = 0; jj < 4; ++jj)
+        if (jj < jn) part[j0 - g0 + jj][threadIdx.x] = acc[jj];
     }
-#pragma unroll
-    for (int jj = 0; jj < 4; ++jj) part[jj][threadIdx.x] = acc[jj];
     __syncthreads();
     if (q == 0) {
-      for (int jj = 0; jj < jn; ++jj) {
+      for (int jj = 0; jj < gn; ++jj) {
         float sum = part[jj][pix];
 #pragma unroll
         for (int r = 1; r < kReduceQ; ++r) sum += part[jj][r * kPix + pix];
-        dv[(long long)fy * sy + (long long)fx * sx + (long long)(s0 - j0 - jj) * ss] += sum;
+        dv[(long long)fy * sy + (long long)fx * sx + (long long)(s0 - g0 - jj) * ss] += sum;
       }
     }
     __syncthreads();  // part is refilled by the next planes
