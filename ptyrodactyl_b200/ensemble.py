@@ -381,6 +381,38 @@ def run_forward_ensemble(slices: torch.Tensor, slice_thickness: float, groups: L
     return out
 
 
+class _FourierFilter(torch.autograd.Function):
+    """y = ifft2(fft2(x) H) over the first two axes of (H, W, M) complex64 CUDA modes
+    with a shared (H, W) filter, on the engine's transforms. Backward (torch's complex
+    convention): dx = ifft2(fft2(dy) conj(H)); dH = sum_m conj(fft2(x)) fft2(dy) / (H W)."""
+
+    @staticmethod
+    def forward(ctx, x, filt):
+        xk = fft2(x.permute(2, 0, 1).contiguous())
+        ctx.save_for_backward(xk, filt)
+        return fft2(xk * filt, inverse=True).permute(1, 2, 0).contiguous()
+
+    @staticmethod
+    def backward(ctx, gy):
+        xk, filt = ctx.saved_tensors
+        gk = fft2(gy.to(torch.complex64).permute(2, 0, 1).contiguous())
+        gx = fft2(gk * filt.conj(), inverse=True).permute(1, 2, 0).contiguous() if ctx.needs_input_grad[0] else None
+        gf = (xk.conj() * gk).sum(dim=0) / float(xk.shape[-1] * xk.shape[-2]) if ctx.needs_input_grad[1] else None
+        return gx, gf
+
+
+def _coherent_jitter_filter(samples: np.ndarray, weights: torch.Tensor, h: int, w: int, calib: float,
+                            dev) -> torch.Tensor:
+    """sum_j w_j exp(-2 pi i (qy dy_j + qx dx_j)), q = fftfreq(., calib): the coherent
+    jitter sum of shift_beam_fourier's ramps as one filter (differentiable in w)."""
+    qy = np.fft.fftfreq(h, d=float(calib))
+    qx = np.fft.fftfreq(w, d=float(calib))
+    ramps = np.exp(-2j * np.pi * (qy[None, :, None] * samples[:, 0, None, None]
+                                  + qx[None, None, :] * samples[:, 1, None, None]))
+    r = torch.as_tensor(ramps.astype(np.complex64), device=dev)
+    return (weights.to(device=dev, dtype=torch.float32).to(torch.complex64)[:, None, None] * r).sum(dim=0)
+
+
 def _host(t: torch.Tensor) -> np.ndarray:
     """A constant tensor's values as float64 NumPy, also inside a torch.func transform
     (where operations on it would be wrapped and have no storage)."""
@@ -406,14 +438,16 @@ def ensemble_patterns_differentiable(slices: torch.Tensor, slice_thickness: floa
     Each coherence sample is one differentiable engine call over all jitter copies of
     the scan, at its energy, a tilted sample with its tilt folded into the first
     slice's potential (``tilt_folded_slices``). An explicit probe-mode axis may be
-    COHERENT (its modes summed with its weights into one wave); COHERENT jitter and
-    coherence axes raise ``NotImplementedError``. The axes' weights are
+    COHERENT (its modes summed with its weights into one wave), and so may the jitter
+    axis (its weighted shifts are one Fourier filter of each mode, ``_FourierFilter``);
+    COHERENT coherence axes raise ``NotImplementedError``. The axes' weights are
     differentiable too (the reduction's weighted sums run in torch)."""
     axes = ensemble_axes_for_cbed(ensemble, beam)
     mode_count = modes.shape[2]
     maps = _axis_maps(axes, mode_count)
-    if any(a.reduction is not ReductionMode.INCOHERENT and kind != AXIS_PROBE_MODES for a, kind in zip(axes, maps)):
-        raise NotImplementedError("derivatives through COHERENT jitter or coherence axes are not supported")
+    if any(a.reduction is not ReductionMode.INCOHERENT and kind == AXIS_COHERENCE for a, kind in zip(axes, maps)):
+        raise NotImplementedError("derivatives through COHERENT coherence axes are not supported")
+    coherent_jitter = None
     dev = slices.device
     sel, w_modes, coherent_modes = None, weights, False
     jit, w_jit = np.zeros((1, 2)), torch.ones(1, dtype=torch.float64)
@@ -433,7 +467,10 @@ def ensemble_patterns_differentiable(slices: torch.Tensor, slice_thickness: floa
             elif not np.array_equal(idx, np.arange(mode_count)):
                 raise ValueError("the beam's mode axis must list every mode once")
         elif kind == AXIS_POSITION_JITTER:
-            jit, w_jit = smp, axis.weights
+            if axis.reduction is ReductionMode.COHERENT:
+                coherent_jitter = (smp, axis.weights)
+            else:
+                jit, w_jit = smp, axis.weights
         else:
             energies, w_coh = {}, axis.weights
             for r, row in enumerate(smp):
@@ -443,6 +480,12 @@ def ensemble_patterns_differentiable(slices: torch.Tensor, slice_thickness: floa
         # a COHERENT mode axis: one wave, the weighted sum of the selected modes
         use_modes = (use_modes * w_modes.to(use_modes.dtype)).sum(dim=2, keepdim=True)
         w_modes = torch.ones(1, dtype=torch.float32, device=dev)
+    if coherent_jitter is not None:
+        # a COHERENT jitter axis: the weighted sum of the shifted waves is one Fourier
+        # filter of each mode (the shifts' ramps at the ensemble calibration)
+        filt = _coherent_jitter_filter(coherent_jitter[0], coherent_jitter[1], int(use_modes.shape[0]),
+                                       int(use_modes.shape[1]), calib_ang, dev)
+        use_modes = _FourierFilter.apply(use_modes.to(torch.complex64).contiguous(), filt)
     scale = float(shift_calib_ang) / float(calib_ang)
     offsets = torch.as_tensor(jit * scale, dtype=torch.float64, device=dev)  # (J, 2)
     J, P = offsets.shape[0], positions.shape[0]

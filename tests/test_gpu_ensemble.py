@@ -341,3 +341,51 @@ def test_bind_cbed_axes_explicit_composition_matches_cbed_image(with_modes):
         bound(torch.zeros(1, dtype=torch.float64))
     with pytest.raises(ValueError, match="column_maps"):
         pb.bind_cbed_axes(pots, beam, mic, det, axes, column_maps=("coherence",))
+
+
+def test_coherent_jitter_axis_is_differentiable():
+    """Reverse mode through a COHERENT jitter axis (the weighted shifts as one Fourier
+    filter of the mode) with an energy-spread axis: patterns against the oracle's
+    ensemble branch, and directional derivatives along V, the beam mode and the raw
+    jitter weights against float64 central differences of it."""
+    pot, modes, w = _setup(n=32, s=2, m=1, seed=23)
+    rng = np.random.default_rng(10)
+    pos = rng.uniform(-1.5, 1.5, (3, 2))
+    g = rng.normal(size=(3, 32, 32))
+    jsmp = np.array([[0.3, -0.2], [-0.25, 0.35], [0.1, 0.1]])
+    dev = torch.device("cuda")
+    wj = torch.tensor([0.5, 0.3, 0.2], dtype=torch.float64, requires_grad=True)
+    jit_axis = pb.create_distribution(jsmp, wj, pb.ReductionMode.COHERENT, "position_jitter")
+    coh = pb.coherence_to_distribution(0.4, 0.0, 2)
+    ens = pb.create_ensemble_axes(position_jitter=jit_axis, coherence=coh)
+    mic = pb.create_microscope_config(200.0, 25.0, ensemble=ens, probe_shape=(32, 32))
+    det = pb.create_detector_config(0.3, scan_positions_px=pos)
+    V = torch.tensor(pot, dtype=torch.float32, device=dev, requires_grad=True)
+    md = torch.tensor(modes.astype(np.complex64), device=dev, requires_grad=True)
+    beam = pb.ProbeModes(md, torch.ones(1, dtype=torch.float32, device=dev), 0.25)
+    s4 = pb.stem_4d(pb.PotentialSlices(V, 1.7, 0.25), beam, mic, det)
+    (s4.data * torch.as_tensor(g, dtype=torch.float32, device=dev)).sum().backward()
+
+    def axes_of(wj_):
+        return [(jsmp, wj_ / wj_.sum(), "coherent", "position_jitter"), _axes_oracle(coh)]
+
+    def loss(pot_, modes_, wj_):
+        return float(np.sum(g * R.stem_4d_ensemble(pot_, 1.7, 0.25, modes_, 0.25, 200.0, pos, 0.3, axes_of(wj_))))
+
+    wj0 = np.array([0.5, 0.3, 0.2])
+    want = R.stem_4d_ensemble(pot, 1.7, 0.25, modes, 0.25, 200.0, pos, 0.3, axes_of(wj0))
+    assert rel_l2(s4.data.detach().cpu().numpy(), want) < TOL
+    dV, dwj = rng.normal(size=pot.shape), rng.normal(size=3)
+    dM = (rng.normal(size=modes.shape) + 1j * rng.normal(size=modes.shape)) * np.abs(modes).max()
+    eps = 1e-5
+    checks = [
+        (float(np.sum(V.grad.cpu().numpy() * dV)),
+         (loss(pot + eps * dV, modes, wj0) - loss(pot - eps * dV, modes, wj0)) / (2 * eps)),
+        (float(np.sum(np.real(np.conj(md.grad.cpu().numpy()) * dM))),
+         (loss(pot, modes + eps * dM, wj0) - loss(pot, modes - eps * dM, wj0)) / (2 * eps)),
+        (float(np.sum(wj.grad.numpy() * dwj)),
+         (loss(pot, modes, wj0 + eps * dwj) - loss(pot, modes, wj0 - eps * dwj)) / (2 * eps)),
+    ]
+    scale = float(np.abs(g * want).sum())
+    for got, fd in checks:
+        assert abs(got - fd) <= 2e-3 * abs(fd) + 1e-5 * scale, (got, fd)
