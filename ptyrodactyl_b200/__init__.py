@@ -81,6 +81,21 @@ from .multislice_recon import (  # noqa: F401
 )
 from .crystal import CrystalData, create_crystal_data, crystal_potential_slices  # noqa: F401
 from .elements import kirkland_parameters, lobato_parameters, single_atom_potential  # noqa: F401
+from .form_factors import (  # noqa: F401
+    KirklandParameters,
+    LobatoParameters,
+    atomic_form_factor,
+    bessel_kv,
+    create_kirkland_parameters,
+    create_lobato_parameters,
+    kirkland_form_factor,
+    kirkland_projected_potential,
+    lobato_bandlimited_peak,
+    lobato_form_factor,
+    lobato_projected_potential,
+    projected_atom_potential,
+)
+from .multislice_recon import OPTIMIZERS  # noqa: F401
 from .hdf5 import HDF5SchemaError, load_from_h5, save_to_h5  # noqa: F401
 from .ensemble import (  # noqa: F401
     bind_cbed_axes,
