@@ -31,7 +31,18 @@ from .types import (  # noqa: F401
 )
 from .reduce import apply_distribution, apply_distributions  # noqa: F401
 from .simulations import (  # noqa: F401
+    A_BOHR,
+    C_LIGHT,
+    E_CHARGE,
+    H_PLANCK,
+    HBAR,
+    M0C2_EV,
+    M_E,
+    MOTT_BETHE_VOLT_ANGSTROM_SQ,
     aberration,
+    helmholtz_coupling,
+    phase_interaction_parameter,
+    relativistic_mass,
     cbed_amplitude,
     cbed_amplitude_from_atoms,
     cbed_image,

@@ -31,11 +31,15 @@ from .types import (
     create_stem4d,
 )
 
-# CODATA 2018 (types/constants.py:60-96)
+# CODATA 2018 (types/constants.py:60-104)
 H_PLANCK = 6.62607015e-34
+HBAR = 1.054571817e-34
 M_E = 9.1093837015e-31
 E_CHARGE = 1.602176634e-19
 C_LIGHT = 2.99792458e8
+A_BOHR = 0.529177210903  # Angstrom
+M0C2_EV = 510998.95
+MOTT_BETHE_VOLT_ANGSTROM_SQ = 47.87801
 
 SUPPORTED_EDGES = (16, 32, 64, 128, 256, 512, 1024)
 
@@ -54,6 +58,25 @@ def interaction_sigma(voltage_kv: float) -> float:
     einstein = M_E * (C_LIGHT * C_LIGHT)
     lam = relativistic_wavelength_ang(voltage_kv)
     return ((2 * math.pi / (lam * volt)) * (einstein + ev)) / ((2 * einstein) + ev)
+
+
+def relativistic_mass(voltage_kv: float) -> float:
+    """m = m_e (1 + e V / (m_e c^2)) in kg (types/constants.py:249-288)."""
+    ev = float(voltage_kv) * 1000.0 * E_CHARGE
+    return M_E * (1.0 + ev / (M_E * C_LIGHT * C_LIGHT))
+
+
+def phase_interaction_parameter(voltage_kv: float) -> float:
+    """sigma = 2 pi m e lambda / h^2 with the relativistic mass, in rad / (V Angstrom)
+    (types/constants.py:181-246); the same quantity as ``interaction_sigma``."""
+    lam_m = relativistic_wavelength_ang(voltage_kv) * 1e-10
+    return 2.0 * math.pi * relativistic_mass(voltage_kv) * E_CHARGE * lam_m / (H_PLANCK * H_PLANCK) * 1e-10
+
+
+def helmholtz_coupling(voltage_kv: float) -> float:
+    """sigma_H = 2 m e / hbar^2 = 8 pi^2 m_0 e (1 + e U / (m_0 c^2)) / h^2, in
+    1 / (V Angstrom^2) (types/constants.py:119-178); equals 2 k_0 sigma."""
+    return 8.0 * math.pi ** 2 * relativistic_mass(voltage_kv) * E_CHARGE / (H_PLANCK * H_PLANCK) * 1e-20
 
 
 def _device(device=None) -> torch.device:

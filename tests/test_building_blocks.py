@@ -60,3 +60,18 @@ def test_building_blocks_are_differentiable():
     beam = torch.randn(8, 8, dtype=torch.complex128)
     pb.shift_beam_fourier(beam, pos, 0.3).abs().pow(2).sum().backward()
     assert pos.grad is not None and bool(torch.isfinite(pos.grad).all())
+
+
+def test_physics_helpers_match_the_reference_values():
+    """types/constants.py:119-288: sigma 0.92440e-3 / 0.65262e-3 rad/(V A) and sigma_H
+    0.31383 / 0.41656 1/(V A^2) at 100 / 300 kV; sigma_H = 2 k0 sigma; sigma is the
+    transmission's interaction constant."""
+    for kv, sig, sh in [(100.0, 0.92440e-3, 0.31383), (300.0, 0.65262e-3, 0.41656)]:
+        s = pb.phase_interaction_parameter(kv)
+        h = pb.helmholtz_coupling(kv)
+        assert abs(s - sig) < 5e-9 and abs(h - sh) < 5e-6
+        k0 = 2.0 * np.pi / pb.relativistic_wavelength_ang(kv)
+        assert np.isclose(h, 2.0 * k0 * s, rtol=1e-14, atol=0.0)
+        assert np.isclose(s, pb.interaction_sigma(kv), rtol=1e-14, atol=0.0)
+    assert np.isclose(pb.relativistic_mass(0.0), pb.M_E, rtol=0, atol=0)
+    assert np.isclose(pb.relativistic_mass(pb.M0C2_EV / 1000.0), 2.0 * pb.M_E, rtol=1e-8)
