@@ -12,6 +12,9 @@ from .types import (  # noqa: F401
     ReductionMode,
     TRIVIAL,
     TRIVIAL_DISTRIBUTION,
+    AxisUpdate,
+    combine_axis_updates,
+    create_axis_update,
     create_distribution,
     create_ensemble_axes,
     create_trivial_distribution,

@@ -125,6 +125,43 @@ def create_distribution(samples, weights, reduction=ReductionMode.INCOHERENT, ax
     return Distribution(smp, norm, mode, axis_id)
 
 
+@dataclass(frozen=True)
+class AxisUpdate:
+    """The perturbation one ensemble sample applies (electron_types.py:227-268):
+    position shift in Angstrom (dy, dx), energy change in eV, tilt (x, y) in mrad;
+    samples of several axes add."""
+
+    position_delta_ang: torch.Tensor
+    energy_delta_ev: torch.Tensor
+    tilt_delta_mrad: torch.Tensor
+
+
+def _update_field(value, shape, name: str) -> torch.Tensor:
+    t = torch.zeros(shape, dtype=torch.float64) if value is None else as_tensor(value, torch.float64).cpu()
+    if tuple(t.shape) != tuple(shape):
+        raise ValueError(f"{name} must have shape {tuple(shape)}")
+    if not bool(torch.isfinite(t).all()):
+        raise ValueError(f"{name} must be finite")
+    return t
+
+
+def create_axis_update(position_delta_ang=None, energy_delta_ev=None, tilt_delta_mrad=None) -> AxisUpdate:
+    """electron_types.py:417-480: missing fields are zero; shapes (2,), (), (2,); finite."""
+    return AxisUpdate(_update_field(position_delta_ang, (2,), "position_delta_ang"),
+                      _update_field(energy_delta_ev, (), "energy_delta_ev"),
+                      _update_field(tilt_delta_mrad, (2,), "tilt_delta_mrad"))
+
+
+def combine_axis_updates(updates) -> AxisUpdate:
+    """electron_types.py:377-414: the field-wise sum (the zero update for none)."""
+    updates = tuple(updates)
+    if not updates:
+        return create_axis_update()
+    return create_axis_update(torch.stack([u.position_delta_ang for u in updates]).sum(0),
+                              torch.stack([u.energy_delta_ev for u in updates]).sum(),
+                              torch.stack([u.tilt_delta_mrad for u in updates]).sum(0))
+
+
 def create_trivial_distribution(sample_dim: int = 1, reduction=ReductionMode.INCOHERENT,
                                 axis_id: Optional[str] = "trivial") -> Distribution:
     """types/distributions.py:190-242: one zero sample of width ``sample_dim`` with unit

@@ -118,3 +118,17 @@ def test_single_axis_agrees(mode):
 def test_no_axes_rejected():
     with pytest.raises(ValueError, match="at least one axis"):
         pb.apply_distributions((), _scalar_field)
+
+
+def test_axis_updates_add_field_by_field():
+    a = pb.create_axis_update(position_delta_ang=[0.1, -0.2], energy_delta_ev=0.5)
+    b = pb.create_axis_update(tilt_delta_mrad=[1.0, 2.0], energy_delta_ev=-0.25)
+    c = pb.combine_axis_updates((a, b))
+    assert torch.equal(c.position_delta_ang, _t([0.1, -0.2]))
+    assert float(c.energy_delta_ev) == 0.25 and torch.equal(c.tilt_delta_mrad, _t([1.0, 2.0]))
+    z = pb.combine_axis_updates(())
+    assert float(z.energy_delta_ev) == 0.0 and not bool(z.position_delta_ang.any())
+    with pytest.raises(ValueError, match="shape"):
+        pb.create_axis_update(position_delta_ang=[1.0, 2.0, 3.0])
+    with pytest.raises(ValueError, match="finite"):
+        pb.create_axis_update(energy_delta_ev=float("nan"))
