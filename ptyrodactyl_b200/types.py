@@ -138,6 +138,8 @@ class AxisUpdate:
 
 def _update_field(value, shape, name: str) -> torch.Tensor:
     t = torch.zeros(shape, dtype=torch.float64) if value is None else as_tensor(value, torch.float64).cpu()
+    if tuple(shape) == () and t.numel() == 1:
+        t = t.reshape(())
     if tuple(t.shape) != tuple(shape):
         raise ValueError(f"{name} must have shape {tuple(shape)}")
     if not bool(torch.isfinite(t).all()):
