@@ -491,7 +491,7 @@ def run_grad(args, rank, world, local_rank):
     rng = np.random.default_rng(w.seed)
     targets = torch.as_tensor(synth.poisson_targets(clean.cpu().numpy().astype(np.float64), w.dose, rng),
                               dtype=torch.float32, device=dev)
-    from ptyrodactyl_b200.autodiff import _ckpt_for
+    from ptyrodactyl_b200.autodiff import _ckpt_for, run_backward
     k = _ckpt_for(S, args.ckpt, n, P)  # the library's default: every slice when the residuals fit
     prm = ms_params(n, S, 1, P, w.voltage_kv, synth.SLICE_DZ, w.calib, w.calib, model.stride(), probe.stride(),
                     0, default_tune(n) if args.tune < 0 else args.tune, F, win)
@@ -499,8 +499,6 @@ def run_grad(args, rank, world, local_rank):
                      args.bwd_batch, prm.tune, F, win)
     ws_b = lib.ptyro_ms_workspace_bytes(ctypes.byref(prm))
     ws = torch.empty(ws_b, dtype=torch.uint8, device=dev)
-    bws_b = lib.ptyro_ms_backward_workspace_bytes(ctypes.byref(bprm))
-    bws = torch.empty(bws_b, dtype=torch.uint8, device=dev)
     res = torch.empty(lib.ptyro_ms_residual_bytes(ctypes.byref(prm), k) // 4, dtype=torch.float32, device=dev)
     out = torch.empty((P, n, n), dtype=torch.float32, device=dev)
     g_field = torch.empty_like(model)
@@ -508,9 +506,9 @@ def run_grad(args, rank, world, local_rank):
     st = torch.cuda.current_stream(dev).cuda_stream
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
 
-    def fwd():
-        _lib.check(lib.ptyro_ms_forward(ctypes.byref(prm), model.data_ptr(), probe.data_ptr(), wts.data_ptr(),
-                                        pos.data_ptr(), out.data_ptr(), ws.data_ptr(), ws_b, st))
+    def fwd():  # the library's forward (concurrent probe lanes, as stem_4d runs it)
+        pb.run_forward(model, synth.SLICE_DZ, probe, wts, pos, w.voltage_kv, w.calib, w.calib, out=out,
+                       tune=prm.tune, windows=win)
 
     def fwd_ckpt():
         _lib.check(lib.ptyro_ms_forward_ckpt(ctypes.byref(prm), k, model.data_ptr(), probe.data_ptr(),
@@ -526,10 +524,9 @@ def run_grad(args, rank, world, local_rank):
         gbuf["g"] = o.grad.contiguous()
         gbuf["loss"] = loss.detach()
 
-    def bwd():
-        _lib.check(lib.ptyro_ms_backward(ctypes.byref(bprm), k, model.data_ptr(), wts.data_ptr(), pos.data_ptr(),
-                                         res.data_ptr(), gbuf["g"].data_ptr(), g_field.data_ptr(),
-                                         g_modes.data_ptr(), bws.data_ptr(), bws_b, st))
+    def bwd():  # the library's adjoint (concurrent probe lanes, as stem_4d's backward runs it)
+        run_backward(model, probe, wts, pos, res, gbuf["g"], k, synth.SLICE_DZ, w.voltage_kv, w.calib, w.calib,
+                     args.bwd_batch, prm.tune, win, g_field, g_modes)
         if world > 1:  # each rank holds its probes' share of dL/dV: one NCCL all-reduce sums them
             import torch.distributed as dist
             dist.all_reduce(g_field)
@@ -585,9 +582,10 @@ def run_grad(args, rank, world, local_rank):
         "loss": float(gbuf["loss"]), "dtype": "f32", "data": "synthetic",
         "config": {"workload": w.name, "grid": n, "field": F, "slices": S, "probes": P, "ckpt_every": k,
                    "residual_bytes": int(res.numel() * 4), "backward_batch": bprm.batch,
+                   "lanes": "forward and adjoint as the library runs them: two concurrent probe lanes",
                    "targets": f"Poisson noise at {w.dose:g} e- per pattern", "loss": "amplitude"},
     }
-    del res, ws, bws
+    del res, ws
     return line
 
 

@@ -25,6 +25,8 @@ import torch
 
 from . import _lib
 from .simulations import (
+    _LANE_MIN_WAVE_BYTES,
+    _side_streams,
     _stream_ptr,
     _workspace,
     any_grid_params,
@@ -32,6 +34,7 @@ from .simulations import (
     check_windows,
     default_tune,
     engine_grid,
+    lane_batch,
     ms_params,
     relativistic_wavelength_ang,
     run_forward_any,
@@ -197,23 +200,8 @@ class Stem4dFunction(torch.autograd.Function):
             Stem4dFunction._adjoint_any(lib, slices, modes, weights, positions, res, grad_out, slice_thickness,
                                         voltage_kv, calib_ang, shift_calib_ang, batch, g_slices, g_modes, g_pos)
         else:
-            g = grad_out.to(torch.float32).contiguous()
-            prm = ms_params(n, S, M, P, voltage_kv, slice_thickness, calib_ang, shift_calib_ang, slices.stride(),
-                            modes.stride(), batch, tune, f, windows)
-            ws_bytes = lib.ptyro_ms_backward_workspace_bytes(ctypes.byref(prm))
-            ws = _workspace(ws_bytes, dev)
-            if g_pos is None:
-                _lib.check(lib.ptyro_ms_backward(ctypes.byref(prm), k, slices.data_ptr(), weights.data_ptr(),
-                                                 positions.data_ptr(), res.data_ptr(), g.data_ptr(),
-                                                 g_slices.data_ptr(), g_modes.data_ptr(), ws.data_ptr(), ws_bytes,
-                                                 _stream_ptr(dev)))
-            else:
-                _lib.check(lib.ptyro_ms_backward_positions(ctypes.byref(prm), k, slices.data_ptr(), modes.data_ptr(),
-                                                           weights.data_ptr(), positions.data_ptr(), res.data_ptr(),
-                                                           g.data_ptr(), g_slices.data_ptr(), g_modes.data_ptr(),
-                                                           g_pos.data_ptr(), ws.data_ptr(), ws_bytes,
-                                                           _stream_ptr(dev)))
-            _lib.check_workspace_status(ws, "stem_4d backward")
+            run_backward(slices, modes, weights, positions, res, grad_out, k, slice_thickness, voltage_kv, calib_ang,
+                         shift_calib_ang, batch, tune, windows, g_slices, g_modes, g_pos)
         # the C-ABI gives JAX's convention conj(2 dL/dconj); torch wants 2 dL/dconj
         return g_slices, g_modes.conj().resolve_conj(), g_pos
 
@@ -289,6 +277,89 @@ def _position_tangent(slices, modes, weights, positions, t_positions, slice_thic
         part = t_positions[:, c].to(device=dev, dtype=torch.float32)[:, None, None] * tan
         out = part if out is None else out + part
     return out
+
+
+def _backward_call(lib, prm, k, slices, modes, weights, positions, res_ptr, g, g_slices, g_modes, g_pos, ws,
+                   ws_bytes, stream_ptr):
+    if g_pos is None:
+        _lib.check(lib.ptyro_ms_backward(ctypes.byref(prm), k, slices.data_ptr(), weights.data_ptr(),
+                                         positions.data_ptr(), res_ptr, g.data_ptr(), g_slices.data_ptr(),
+                                         g_modes.data_ptr(), ws.data_ptr(), ws_bytes, stream_ptr))
+    else:
+        _lib.check(lib.ptyro_ms_backward_positions(ctypes.byref(prm), k, slices.data_ptr(), modes.data_ptr(),
+                                                   weights.data_ptr(), positions.data_ptr(), res_ptr, g.data_ptr(),
+                                                   g_slices.data_ptr(), g_modes.data_ptr(), g_pos.data_ptr(),
+                                                   ws.data_ptr(), ws_bytes, stream_ptr))
+
+
+def run_backward(slices: torch.Tensor, modes: torch.Tensor, weights: torch.Tensor, positions: torch.Tensor,
+                 residuals: torch.Tensor, grad_patterns: torch.Tensor, ckpt_every: int, slice_thickness: float,
+                 voltage_kv: float, calib_ang: float, shift_calib_ang: float, batch: int, tune: int,
+                 windows: Optional[torch.Tensor], g_slices: torch.Tensor, g_modes: torch.Tensor,
+                 g_pos: Optional[torch.Tensor] = None, lanes: int = 0) -> None:
+    """The engine's adjoint (ptyro_ms_backward, or _positions with ``g_pos``) over the
+    residuals a ptyro_ms_forward_ckpt of the same probes recorded, into g_slices (the
+    slices' strides) and g_modes (JAX's convention). ``lanes`` > 1 runs contiguous probe
+    ranges as concurrent adjoints on side streams, each over its own residual range
+    (the residuals are probe-major) with the lane's share of the L2 wave budget, their
+    dL/dV and dL/dmodes added in lane order afterwards (0: two lanes when the probes'
+    waves exceed 256 MiB, as the forward). The sums are deterministic for a given lane
+    count; different lane counts agree to float32 rounding."""
+    lib = _lib.load()
+    dev = slices.device
+    S, M, P = slices.shape[2], modes.shape[2], positions.shape[0]
+    n, f = check_windows(slices, modes, windows, P)
+    g = grad_patterns.to(torch.float32).contiguous()
+    k = int(ckpt_every)
+    if lanes == 0:
+        lanes = 2 if P * n * n * M * 8 >= _LANE_MIN_WAVE_BYTES else 1
+    lanes = max(1, min(int(lanes), P))
+    per_probe = M * ((S + k - 1) // k + 1) * n * n * 8  # residual bytes of one probe's (mode, plane) slots
+    if lanes > 1:
+        full = ms_params(n, S, M, P, voltage_kv, slice_thickness, calib_ang, shift_calib_ang, slices.stride(),
+                         modes.stride(), batch, tune, f, windows)
+        if lib.ptyro_ms_residual_bytes(ctypes.byref(full), k) != P * per_probe or \
+                residuals.numel() * residuals.element_size() < P * per_probe:
+            lanes = 1  # not the probe-major layout this split assumes: one call
+    if lanes == 1:
+        prm = ms_params(n, S, M, P, voltage_kv, slice_thickness, calib_ang, shift_calib_ang, slices.stride(),
+                        modes.stride(), batch, tune, f, windows)
+        ws_bytes = lib.ptyro_ms_backward_workspace_bytes(ctypes.byref(prm))
+        ws = _workspace(ws_bytes, dev)
+        _backward_call(lib, prm, k, slices, modes, weights, positions, residuals.data_ptr(), g, g_slices, g_modes,
+                       g_pos, ws, ws_bytes, _stream_ptr(dev))
+        _lib.check_workspace_status(ws, "stem_4d backward")
+        return
+    main = torch.cuda.current_stream(dev)
+    bounds = [P * i // lanes for i in range(lanes + 1)]
+    streams = _side_streams(dev, lanes)
+    lb = lane_batch(n, M, lanes, batch)
+    outs = [(g_slices, g_modes)] + [(torch.empty_strided(g_slices.shape, g_slices.stride(), dtype=g_slices.dtype,
+                                                         device=dev),
+                                     torch.empty_strided(g_modes.shape, g_modes.stride(), dtype=g_modes.dtype,
+                                                         device=dev)) for _ in range(lanes - 1)]
+    keep = []
+    for (lo, hi), st, (gs, gm) in zip(zip(bounds[:-1], bounds[1:]), streams, outs):
+        win = None if windows is None else windows[lo:hi].contiguous()
+        prm = ms_params(n, S, M, hi - lo, voltage_kv, slice_thickness, calib_ang, shift_calib_ang, slices.stride(),
+                        modes.stride(), lb, tune, f, win)
+        ws_bytes = lib.ptyro_ms_backward_workspace_bytes(ctypes.byref(prm))
+        ws = _workspace(ws_bytes, dev)
+        st.wait_stream(main)
+        with torch.cuda.stream(st):
+            _backward_call(lib, prm, k, slices, modes, weights, positions[lo:hi],
+                           residuals.data_ptr() + lo * per_probe, g[lo:hi], gs, gm,
+                           None if g_pos is None else g_pos[lo:hi], ws, ws_bytes, _stream_ptr(dev))
+        for t in (ws, gs, gm) + (() if win is None else (win,)):
+            t.record_stream(st)
+        keep.append(ws)
+    for st in streams:
+        main.wait_stream(st)
+    for gs, gm in outs[1:]:
+        g_slices.add_(gs)
+        g_modes.add_(gm)
+    for ws in keep:
+        _lib.check_workspace_status(ws, "stem_4d backward")
 
 
 def stem_4d_patterns(slices: torch.Tensor, modes: torch.Tensor, weights: torch.Tensor, positions: torch.Tensor,

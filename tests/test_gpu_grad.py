@@ -265,3 +265,49 @@ def test_mode_weight_gradient_and_tangent_match_oracle():
     out = pb.stem_4d(slices, beam, mic, det)
     (out.data * torch.as_tensor(g, dtype=torch.float32, device=dev)).sum().backward()
     assert rel_l2(beam.weights.grad.cpu().numpy(), want) < TOL
+
+
+@pytest.mark.parametrize("windowed", [False, True])
+def test_adjoint_lanes_agree_with_one_call(windowed):
+    """run_backward over two and three concurrent probe lanes (each its own residual
+    range and side stream, dL/dV and dL/dmodes added in lane order) against one call,
+    with scan-position gradients; the lanes' sums differ only by float32 rounding."""
+    import ctypes
+    from ptyrodactyl_b200 import _lib
+    from ptyrodactyl_b200.autodiff import run_backward
+    from ptyrodactyl_b200.simulations import default_tune, ms_params
+    rng = np.random.default_rng(31 + windowed)
+    n, S, P, M = 64, 3, 37, 2
+    F = 128 if windowed else n
+    dev = torch.device("cuda")
+    pot = torch.as_tensor(rng.uniform(0.0, 30.0, (F, F, S)), dtype=torch.float32, device=dev)
+    probe = R.make_probe(200.0, 25.0, (n, n), 25.0, defocus_ang=-30.0)
+    modes = torch.as_tensor(np.stack([probe, np.roll(probe, 3, axis=0) * (0.5 + 0.2j)], -1).astype(np.complex64),
+                            device=dev)
+    wts = torch.tensor([0.7, 0.3], dtype=torch.float32, device=dev)
+    pos = torch.as_tensor(rng.uniform(-2, 2, (P, 2)), dtype=torch.float64, device=dev)
+    win = torch.as_tensor(rng.integers(0, F, (P, 2)), dtype=torch.int32, device=dev) if windowed else None
+    lib = _lib.load()
+    k = 1
+    from ptyrodactyl_b200.simulations import check_windows
+    _, f = check_windows(pot, modes, win, P)
+    prm = ms_params(n, S, M, P, 200.0, 1.7, 0.25, 0.25, pot.stride(), modes.stride(), 0, default_tune(n), f, win)
+    ws_b = lib.ptyro_ms_workspace_bytes(ctypes.byref(prm))
+    ws = torch.empty(ws_b, dtype=torch.uint8, device=dev)
+    res = torch.empty(lib.ptyro_ms_residual_bytes(ctypes.byref(prm), k) // 4, dtype=torch.float32, device=dev)
+    out = torch.empty((P, n, n), dtype=torch.float32, device=dev)
+    _lib.check(lib.ptyro_ms_forward_ckpt(ctypes.byref(prm), k, pot.data_ptr(), modes.data_ptr(), wts.data_ptr(),
+                                         pos.data_ptr(), out.data_ptr(), res.data_ptr(), ws.data_ptr(), ws_b,
+                                         torch.cuda.current_stream().cuda_stream))
+    g = torch.as_tensor(rng.normal(size=(P, n, n)), dtype=torch.float32, device=dev)
+    results = []
+    for lanes in (1, 2, 3):
+        gs, gm = torch.empty_like(pot), torch.empty_like(modes)
+        gp = torch.zeros((P, 2), dtype=torch.float64, device=dev)
+        run_backward(pot, modes, wts, pos, res, g, k, 1.7, 200.0, 0.25, 0.25, 0, default_tune(n), win, gs, gm, gp,
+                     lanes=lanes)
+        results.append((gs, gm, gp))
+    for gs, gm, gp in results[1:]:
+        assert torch.linalg.norm(gs - results[0][0]) <= 1e-6 * torch.linalg.norm(results[0][0])
+        assert torch.linalg.norm(gm - results[0][1]) <= 1e-6 * torch.linalg.norm(results[0][1])
+        assert torch.equal(gp, results[0][2])  # per-probe: the same kernels on the same probes
