@@ -491,29 +491,25 @@ def run_grad(args, rank, world, local_rank):
     rng = np.random.default_rng(w.seed)
     targets = torch.as_tensor(synth.poisson_targets(clean.cpu().numpy().astype(np.float64), w.dose, rng),
                               dtype=torch.float32, device=dev)
-    from ptyrodactyl_b200.autodiff import _ckpt_for, run_backward
+    from ptyrodactyl_b200.autodiff import _ckpt_for, run_backward, run_forward_ckpt
     k = _ckpt_for(S, args.ckpt, n, P)  # the library's default: every slice when the residuals fit
     prm = ms_params(n, S, 1, P, w.voltage_kv, synth.SLICE_DZ, w.calib, w.calib, model.stride(), probe.stride(),
                     0, default_tune(n) if args.tune < 0 else args.tune, F, win)
     bprm = ms_params(n, S, 1, P, w.voltage_kv, synth.SLICE_DZ, w.calib, w.calib, model.stride(), probe.stride(),
                      args.bwd_batch, prm.tune, F, win)
-    ws_b = lib.ptyro_ms_workspace_bytes(ctypes.byref(prm))
-    ws = torch.empty(ws_b, dtype=torch.uint8, device=dev)
     res = torch.empty(lib.ptyro_ms_residual_bytes(ctypes.byref(prm), k) // 4, dtype=torch.float32, device=dev)
     out = torch.empty((P, n, n), dtype=torch.float32, device=dev)
     g_field = torch.empty_like(model)
     g_modes = torch.empty_like(probe)
-    st = torch.cuda.current_stream(dev).cuda_stream
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
 
     def fwd():  # the library's forward (concurrent probe lanes, as stem_4d runs it)
         pb.run_forward(model, synth.SLICE_DZ, probe, wts, pos, w.voltage_kv, w.calib, w.calib, out=out,
                        tune=prm.tune, windows=win)
 
-    def fwd_ckpt():
-        _lib.check(lib.ptyro_ms_forward_ckpt(ctypes.byref(prm), k, model.data_ptr(), probe.data_ptr(),
-                                             wts.data_ptr(), pos.data_ptr(), out.data_ptr(), res.data_ptr(),
-                                             ws.data_ptr(), ws_b, st))
+    def fwd_ckpt():  # the library's residual-recording forward (concurrent probe lanes, as stem_4d records)
+        run_forward_ckpt(model, probe, wts, pos, k, synth.SLICE_DZ, w.voltage_kv, w.calib, w.calib, 0, prm.tune, win,
+                         out, res)
 
     gbuf = {}
 
@@ -582,10 +578,11 @@ def run_grad(args, rank, world, local_rank):
         "loss": float(gbuf["loss"]), "dtype": "f32", "data": "synthetic",
         "config": {"workload": w.name, "grid": n, "field": F, "slices": S, "probes": P, "ckpt_every": k,
                    "residual_bytes": int(res.numel() * 4), "backward_batch": bprm.batch,
-                   "lanes": "forward and adjoint as the library runs them: two concurrent probe lanes",
+                   "lanes": "forward, recording forward and adjoint as the library runs them: two concurrent "
+                            "probe lanes",
                    "targets": f"Poisson noise at {w.dose:g} e- per pattern", "loss": "amplitude"},
     }
-    del res, ws
+    del res
     return line
 
 

@@ -93,7 +93,11 @@ class Stem4dFunction(torch.autograd.Function):
         out = torch.empty((P, n, n), dtype=torch.float32, device=dev)
         nres = lib.ptyro_ms_residual_bytes(ctypes.byref(prm), k) // 4 if (P and record) else 0
         res = torch.empty(nres, dtype=torch.float32, device=dev)
-        if P:
+        if P and record:
+            with torch.cuda.device(dev):
+                run_forward_ckpt(slices, modes, weights, positions, k, slice_thickness, voltage_kv, calib_ang,
+                                 shift_calib_ang, batch, tune, windows, out, res)
+        elif P:
             ws_bytes = lib.ptyro_ms_workspace_bytes(ctypes.byref(prm))
             ws = _workspace(ws_bytes, dev)
             with torch.cuda.device(dev):
@@ -279,6 +283,65 @@ def _position_tangent(slices, modes, weights, positions, t_positions, slice_thic
     return out
 
 
+def _lanes_for(lib, P: int, n: int, S: int, M: int, k: int, lanes: int, prm_full, residuals) -> tuple:
+    """(lanes, residual bytes per probe): two lanes when the probes' waves exceed
+    256 MiB (as the forward), one when the residuals are not the probe-major layout the
+    split assumes."""
+    if lanes == 0:
+        lanes = 2 if P * n * n * M * 8 >= _LANE_MIN_WAVE_BYTES else 1
+    lanes = max(1, min(int(lanes), P))
+    per_probe = M * ((S + k - 1) // k + 1) * n * n * 8
+    if lanes > 1 and (lib.ptyro_ms_residual_bytes(ctypes.byref(prm_full), k) != P * per_probe
+                      or residuals.numel() * residuals.element_size() < P * per_probe):
+        lanes = 1
+    return lanes, per_probe
+
+
+def run_forward_ckpt(slices: torch.Tensor, modes: torch.Tensor, weights: torch.Tensor, positions: torch.Tensor,
+                     ckpt_every: int, slice_thickness: float, voltage_kv: float, calib_ang: float,
+                     shift_calib_ang: float, batch: int, tune: int, windows: Optional[torch.Tensor],
+                     out: torch.Tensor, residuals: torch.Tensor, lanes: int = 0) -> None:
+    """The residual-recording forward (ptyro_ms_forward_ckpt) into ``out`` (P, n, n) and
+    ``residuals`` (ptyro_ms_residual_bytes); ``lanes`` > 1 runs contiguous probe ranges
+    concurrently on side streams, each writing its own (probe-major) residual range, as
+    ``run_backward`` reads them. The results do not depend on the lane count."""
+    lib = _lib.load()
+    dev = slices.device
+    S, M, P = slices.shape[2], modes.shape[2], positions.shape[0]
+    n, f = check_windows(slices, modes, windows, P)
+    k = int(ckpt_every)
+    full = ms_params(n, S, M, P, voltage_kv, slice_thickness, calib_ang, shift_calib_ang, slices.stride(),
+                     modes.stride(), batch, tune, f, windows)
+    lanes, per_probe = _lanes_for(lib, P, n, S, M, k, lanes, full, residuals)
+    main = torch.cuda.current_stream(dev)
+    bounds = [P * i // lanes for i in range(lanes + 1)]
+    streams = [main] if lanes == 1 else _side_streams(dev, lanes)
+    lb = batch if lanes == 1 else lane_batch(n, M, lanes, batch)
+    keep = []
+    for (lo, hi), st in zip(zip(bounds[:-1], bounds[1:]), streams):
+        win = None if windows is None else windows[lo:hi].contiguous()
+        prm = full if lanes == 1 else ms_params(n, S, M, hi - lo, voltage_kv, slice_thickness, calib_ang,
+                                                 shift_calib_ang, slices.stride(), modes.stride(), lb, tune, f, win)
+        ws_bytes = lib.ptyro_ms_workspace_bytes(ctypes.byref(prm))
+        ws = _workspace(ws_bytes, dev)
+        if st is not main:
+            st.wait_stream(main)
+        with torch.cuda.stream(st):
+            _lib.check(lib.ptyro_ms_forward_ckpt(ctypes.byref(prm), k, slices.data_ptr(), modes.data_ptr(),
+                                                 weights.data_ptr(), positions[lo:hi].data_ptr(),
+                                                 out[lo:hi].data_ptr(), residuals.data_ptr() + lo * per_probe,
+                                                 ws.data_ptr(), ws_bytes, _stream_ptr(dev)))
+        if st is not main:
+            for t in (ws,) + (() if win is None else (win,)):
+                t.record_stream(st)
+        keep.append(ws)
+    for st in streams:
+        if st is not main:
+            main.wait_stream(st)
+    for ws in keep:
+        _lib.check_workspace_status(ws, "stem_4d forward")
+
+
 def _backward_call(lib, prm, k, slices, modes, weights, positions, res_ptr, g, g_slices, g_modes, g_pos, ws,
                    ws_bytes, stream_ptr):
     if g_pos is None:
@@ -311,16 +374,9 @@ def run_backward(slices: torch.Tensor, modes: torch.Tensor, weights: torch.Tenso
     n, f = check_windows(slices, modes, windows, P)
     g = grad_patterns.to(torch.float32).contiguous()
     k = int(ckpt_every)
-    if lanes == 0:
-        lanes = 2 if P * n * n * M * 8 >= _LANE_MIN_WAVE_BYTES else 1
-    lanes = max(1, min(int(lanes), P))
-    per_probe = M * ((S + k - 1) // k + 1) * n * n * 8  # residual bytes of one probe's (mode, plane) slots
-    if lanes > 1:
-        full = ms_params(n, S, M, P, voltage_kv, slice_thickness, calib_ang, shift_calib_ang, slices.stride(),
-                         modes.stride(), batch, tune, f, windows)
-        if lib.ptyro_ms_residual_bytes(ctypes.byref(full), k) != P * per_probe or \
-                residuals.numel() * residuals.element_size() < P * per_probe:
-            lanes = 1  # not the probe-major layout this split assumes: one call
+    full = ms_params(n, S, M, P, voltage_kv, slice_thickness, calib_ang, shift_calib_ang, slices.stride(),
+                     modes.stride(), batch, tune, f, windows)
+    lanes, per_probe = _lanes_for(lib, P, n, S, M, k, lanes, full, residuals)
     if lanes == 1:
         prm = ms_params(n, S, M, P, voltage_kv, slice_thickness, calib_ang, shift_calib_ang, slices.stride(),
                         modes.stride(), batch, tune, f, windows)

@@ -269,7 +269,7 @@ def test_mode_weight_gradient_and_tangent_match_oracle():
 
 @pytest.mark.parametrize("windowed", [False, True])
 def test_adjoint_lanes_agree_with_one_call(windowed):
-    """run_backward over two and three concurrent probe lanes (each its own residual
+    """run_forward_ckpt and run_backward over two and three concurrent probe lanes (each its own residual
     range and side stream, dL/dV and dL/dmodes added in lane order) against one call,
     with scan-position gradients; the lanes' sums differ only by float32 rounding."""
     import ctypes
@@ -299,6 +299,13 @@ def test_adjoint_lanes_agree_with_one_call(windowed):
     _lib.check(lib.ptyro_ms_forward_ckpt(ctypes.byref(prm), k, pot.data_ptr(), modes.data_ptr(), wts.data_ptr(),
                                          pos.data_ptr(), out.data_ptr(), res.data_ptr(), ws.data_ptr(), ws_b,
                                          torch.cuda.current_stream().cuda_stream))
+    # the recording forward over lanes writes the same patterns and residuals
+    from ptyrodactyl_b200.autodiff import run_forward_ckpt
+    for lanes in (2, 3):
+        out_l, res_l = torch.empty_like(out), torch.empty_like(res)
+        run_forward_ckpt(pot, modes, wts, pos, k, 1.7, 200.0, 0.25, 0.25, 0, default_tune(n), win, out_l, res_l,
+                         lanes=lanes)
+        assert torch.equal(out_l, out) and torch.equal(res_l, res)
     g = torch.as_tensor(rng.normal(size=(P, n, n)), dtype=torch.float32, device=dev)
     results = []
     for lanes in (1, 2, 3):
