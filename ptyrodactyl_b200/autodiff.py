@@ -535,22 +535,13 @@ def vjp(slices, modes, weights, positions, grad_patterns, slice_thickness, volta
     out = torch.empty((P, n, n), dtype=torch.float32, device=dev)
     res = torch.empty(max(1, lib.ptyro_ms_residual_bytes(ctypes.byref(prm), k) // 4), dtype=torch.float32,
                       device=dev)
-    ws_bytes = lib.ptyro_ms_workspace_bytes(ctypes.byref(prm))
-    ws = _workspace(ws_bytes, dev)
-    st = _stream_ptr(dev)
-    _lib.check(lib.ptyro_ms_forward_ckpt(ctypes.byref(prm), k, slices.data_ptr(), modes.data_ptr(),
-                                         weights.data_ptr(), positions.data_ptr(), out.data_ptr(), res.data_ptr(),
-                                         ws.data_ptr(), ws_bytes, st))
-    _lib.check_workspace_status(ws, "vjp forward")
+    tn = prm.tune
+    run_forward_ckpt(slices, modes, weights, positions, k, slice_thickness, voltage_kv, calib_ang, sc, batch, tn,
+                     windows, out, res)
     g_slices = torch.empty_strided(slices.shape, slices.stride(), dtype=torch.float32, device=dev)
     g_modes = torch.empty_strided(modes.shape, modes.stride(), dtype=torch.complex64, device=dev)
-    bws = lib.ptyro_ms_backward_workspace_bytes(ctypes.byref(prm))
-    bw = _workspace(bws, dev)
-    g = grad_patterns.to(torch.float32).contiguous()
-    _lib.check(lib.ptyro_ms_backward(ctypes.byref(prm), k, slices.data_ptr(), weights.data_ptr(),
-                                     positions.data_ptr(), res.data_ptr(), g.data_ptr(), g_slices.data_ptr(),
-                                     g_modes.data_ptr(), bw.data_ptr(), bws, st))
-    _lib.check_workspace_status(bw, "vjp backward")
+    run_backward(slices, modes, weights, positions, res, grad_patterns, k, slice_thickness, voltage_kv, calib_ang, sc,
+                 batch, tn, windows, g_slices, g_modes)
     return out, g_slices, g_modes
 
 
