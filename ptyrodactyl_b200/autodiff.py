@@ -448,7 +448,7 @@ def _like(t: Optional[torch.Tensor], primal: torch.Tensor, dtype) -> Optional[to
 
 
 def jvp(slices, modes, weights, positions, tangent_slices, tangent_modes, slice_thickness, voltage_kv, calib_ang,
-        shift_calib_ang=None, batch: int = 0, windows=None, want_patterns: bool = True):
+        shift_calib_ang=None, batch: int = 0, windows=None, want_patterns: bool = True, lanes: int = 0):
     """(patterns or None, dI) for the tangent (tangent_slices, tangent_modes), either
     of which may be None (zero). Runs ``ptyro_ms_jvp``: the wave and its tangent go
     through the forward's passes together."""
@@ -461,19 +461,41 @@ def jvp(slices, modes, weights, positions, tangent_slices, tangent_modes, slice_
                         windows, want_patterns)
     n, f = check_windows(slices, modes, windows, P)
     sc = float(calib_ang if shift_calib_ang is None else shift_calib_ang)
-    prm = ms_params(n, S, M, P, voltage_kv, slice_thickness, calib_ang, sc, slices.stride(), modes.stride(), batch,
-                    0, f, windows)
     ts = _like(tangent_slices, slices, torch.float32)
     tm = _like(tangent_modes, modes, torch.complex64)
     out = torch.empty((P, n, n), dtype=torch.float32, device=dev) if want_patterns else None
     tan = torch.empty((P, n, n), dtype=torch.float32, device=dev)
-    if P:
+    if not P:
+        return out, tan
+    # contiguous probe ranges as concurrent tangent forwards on side streams (every
+    # output is per probe, so the lanes change nothing but the overlap)
+    if lanes == 0:
+        lanes = 2 if P * n * n * M * 8 >= _LANE_MIN_WAVE_BYTES else 1
+    lanes = max(1, min(int(lanes), P))
+    main = torch.cuda.current_stream(dev)
+    bounds = [P * i // lanes for i in range(lanes + 1)]
+    streams = [main] if lanes == 1 else _side_streams(dev, lanes)
+    # a slot holds the wave and its tangent: half the lane's share of the L2 wave budget
+    lb = batch if (lanes == 1 or batch) else max(1, lane_batch(n, M, lanes) // 2)
+    for (lo, hi), st in zip(zip(bounds[:-1], bounds[1:]), streams):
+        win = None if windows is None else windows[lo:hi].contiguous()
+        prm = ms_params(n, S, M, hi - lo, voltage_kv, slice_thickness, calib_ang, sc, slices.stride(), modes.stride(),
+                        lb, 0, f, win)
         ws_bytes = lib.ptyro_ms_jvp_workspace_bytes(ctypes.byref(prm))
         ws = _workspace(ws_bytes, dev)
-        _lib.check(lib.ptyro_ms_jvp(ctypes.byref(prm), slices.data_ptr(), None if ts is None else ts.data_ptr(),
-                                    modes.data_ptr(), None if tm is None else tm.data_ptr(), weights.data_ptr(),
-                                    positions.data_ptr(), None if out is None else out.data_ptr(), tan.data_ptr(),
-                                    ws.data_ptr(), ws_bytes, _stream_ptr(dev)))
+        if st is not main:
+            st.wait_stream(main)
+        with torch.cuda.stream(st):
+            _lib.check(lib.ptyro_ms_jvp(ctypes.byref(prm), slices.data_ptr(), None if ts is None else ts.data_ptr(),
+                                        modes.data_ptr(), None if tm is None else tm.data_ptr(), weights.data_ptr(),
+                                        positions[lo:hi].data_ptr(), None if out is None else out[lo:hi].data_ptr(),
+                                        tan[lo:hi].data_ptr(), ws.data_ptr(), ws_bytes, _stream_ptr(dev)))
+        if st is not main:
+            for t in (ws,) + (() if win is None else (win,)):
+                t.record_stream(st)
+    for st in streams:
+        if st is not main:
+            main.wait_stream(st)
     return out, tan
 
 

@@ -167,3 +167,15 @@ def test_forward_mode_along_scan_positions(h, w):
     got = float(np.sum(tan.cpu().numpy() * g))
     ref = float(np.sum(dpos * tpos))
     assert abs(got - ref) <= 1e-3 * abs(ref) + 1e-4 * float(np.abs(g * want).sum()) * 1e-2, (got, ref)
+
+
+def test_jvp_lanes_are_bit_identical():
+    """The tangent forward over two and three concurrent probe lanes writes exactly
+    the patterns and tangents of one call (every output is per probe)."""
+    pot, modes, w, pos, dv, dm = _case(64, 3, 2, 23, seed=4)
+    sl, md, ps, tsl, tmd = _dev(pot, modes, pos, dv, dm)
+    wt = torch.as_tensor(w, dtype=torch.float32, device="cuda")
+    ref = pb.jvp(sl, md, wt, ps, tsl, tmd, 1.7, 200.0, 0.3, lanes=1)
+    for lanes in (2, 3):
+        got = pb.jvp(sl, md, wt, ps, tsl, tmd, 1.7, 200.0, 0.3, lanes=lanes)
+        assert torch.equal(got[0], ref[0]) and torch.equal(got[1], ref[1])
